@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Walker-steps/s of the batched phaseless AFQMC walker step on B200.
+
+Workload: M=200 orbitals, N_up=N_dn=50 (CLOSED walkers), N_chol=1600 (decay 0.995^n), 1024 walkers
+per GPU, dt=0.005, Taylor order 6, seeded synthetic Hamiltonian and RHF trial (no public input:
+the reference reads pyscf-generated HDF5 files that are not available here).
+
+One bench "step" is one block of the reference's production loop (run_afqmc.cpp:69-113) at its
+cadence: 10 propagation steps, QR re-orthogonalisation every 5, comb population control every 10
+and one mixed-estimator energy measurement every 10.  value = walker-steps/s over all ranks
+(= W * 10 * K * N_gpus / max-over-ranks device time).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BLOCK = 10  # AFQMC steps per bench step
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=6)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--walkers", type=int, default=1024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def metric_name():
+    return "walker-steps/s at M=200, 1024 walkers: mixed vs FP64 on B200 at |dE|<0.5 mHa"
+
+
+# ------------------------------------------------------------------------------------------
+# CPU leg: the oracle (restatement of the reference CPU path) on the host cores
+# ------------------------------------------------------------------------------------------
+def cpu_sample(wl, n_walkers, n_blocks=1):
+    """Time the oracle on n_walkers walkers of the workload; returns (walker-steps/s, seconds,
+    description).  One block = 10 propagations + 2 orthogonalisations + 1 energy measurement."""
+    import numpy as np
+    from oracle import afqmc as O
+    oham = O.Real3IndexFactorization(wl.walker_type, wl.M, wl.nup, wl.ndn, wl.Likn, wl.hij, wl.E0,
+                                     wl.PsiT)
+    owfn = O.NOMSD(oham, wl.PsiT)
+    prop = O.Propagator(owfn, O.PropagatorParams(dt=wl.dt))
+    ws = O.WalkerSet.from_trial(owfn, n_walkers)
+    E, ov = owfn.Energy(ws.SA, ws.SB)
+    ws.props[:, O.OVLP] = ov
+    ws.props[:, O.PSEUDO_ELOC] = E.sum(axis=1)
+    Eshift = float(np.mean(E.sum(axis=1)).real)
+    rng = O.HostRandomGenerator(O.split_seed(0, 0, 1))
+    wrng = O.HostRandomGenerator(O.split_seed(0, 0, 0))
+    t0 = time.perf_counter()
+    for b in range(n_blocks):
+        for s in range(BLOCK):
+            u = rng.sample_uniform(n_walkers * wl.Nc).reshape(n_walkers, wl.Nc)
+            prop.propagate(ws, Eshift, u)
+            if s % 5 == 0:
+                prop.orthogonalize(ws)
+            if s == 0:
+                O.population_control_single_rank(wrng, ws)
+        O.energy_measure(owfn, ws)
+    dt = time.perf_counter() - t0
+    ws_s = n_walkers * BLOCK * n_blocks / dt
+    desc = (f"oracle (numpy/scipy, OpenBLAS) on {n_walkers} walkers x {BLOCK * n_blocks} steps "
+            f"of the same workload, incl. orthogonalisation, comb and one energy measurement per "
+            f"{BLOCK} steps")
+    return ws_s, dt, desc
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = host_cores()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", str(cores))
+    from safire_b200.synth import make_workload
+    wl = make_workload("cfg2")
+    n_walkers = 16
+    for _ in range(args.warmup):
+        cpu_sample(wl, n_walkers, 0)
+    tot_ws, tot_t = 0.0, 0.0
+    for _ in range(args.steps):
+        v, t, desc = cpu_sample(wl, n_walkers, 1)
+        tot_ws += n_walkers * BLOCK
+        tot_t += t
+    value = tot_ws / tot_t
+    line = {
+        "impl": "reference", "metric": metric_name(), "value": value, "unit": "walker-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * tot_t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": "M=200 N=50+50 Nc=1600 W=1024 dt=0.005 (sampled on 16 walkers)",
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "walker-steps/s", "cores": cores, "kind": "port",
+                         "sample": desc},
+        "e2e": {"value": value, "unit": "walker-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------------------
+# GPU leg
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    def __init__(self, device_index):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+        self.dev = device_index
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.strip().split(",") for r in self.file.read().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+                for k, n in enumerate(names):
+                    if r[3 + k].strip().lower() in ("active", "1"):
+                        reasons.add(n)
+            except Exception:
+                continue
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def fp64_peak_tflops(torch):
+    """Dense FP64 throughput of cuBLAS DGEMM on this GPU (the FP64 roofline denominator)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1000)
+    del a, b
+    return 2 * n ** 3 / best / 1e12
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from safire_b200 import afqmc as A
+    from safire_b200 import capi
+    from safire_b200.driver import RunParams, Simulation
+    from safire_b200.synth import make_workload
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    prec = A.PREC_MIXED if args.precision == "mixed" else A.PREC_FP64
+    W = args.walkers
+    wl = make_workload("cfg2")
+    rp = RunParams(equilibration_steps=0, seed=rank)
+    sim = Simulation.from_workload(wl, W=W, precision=prec, rp=rp)
+    stream = torch.cuda.current_stream()
+
+    def block():
+        for _ in range(BLOCK):
+            sim.step()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        block()
+    torch.cuda.synchronize()
+    barrier()
+    launches0 = capi.lib().afqmc_kernel_launches()
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        block()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = capi.lib().afqmc_kernel_launches() - launches0
+    t_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+    value = W * world * BLOCK * args.steps / (t_ms / 1000)
+
+    # per-phase timing of one step and of one energy measurement (untimed region)
+    sim.prop.set_timing(True)
+    sim.prop.Propagate(sim.wset, sim.Eshift)
+    phases = sim.prop.timings()
+    sim.prop.set_timing(False)
+    torch.cuda.synchronize()
+    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0.record(stream)
+    sim.measure()
+    m1.record(stream)
+    torch.cuda.synchronize()
+    phases["energy_measurement"] = m0.elapsed_time(m1)
+    o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    o0.record(stream)
+    sim.prop.Orthogonalize(sim.wset)
+    o1.record(stream)
+    torch.cuda.synchronize()
+    phases["orthogonalize"] = o0.elapsed_time(o1)
+
+    # roofline of the dominant kernel: the FP64 contraction with the largest share of a block
+    M, N, Nc = wl.M, wl.nup, wl.Nc
+    flops = {  # flops the kernels execute per call (real trial: Lnak, L and P1 are real)
+        "vHS": 4.0 * M * M * Nc * W,
+        "vbias": 4.0 * N * M * Nc * W,
+        "propagate": W * (2 * 4.0 * M * M * N + 6 * 8.0 * M * M * N),
+        "energy_measurement": W * (4.0 * N * N * M * Nc + 8.0 * N * N * Nc),
+    }
+    block_share = {k: (phases[k] * (1 if k == "energy_measurement" else BLOCK)) for k in flops}
+    top = max(block_share, key=block_share.get)
+    achieved = flops[top] / (phases[top] / 1000) / 1e12
+    peak = fp64_peak_tflops(torch) if prec == A.PREC_FP64 else None
+    peaks = measured_peaks()
+    roofline = {"kernel": top, "bound": "tensor", "achieved": achieved,
+                "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if peak else None, "traffic": None,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64)",
+                "flops_per_launch": flops[top]}
+
+    # e2e: the same loop through the public API with host uniforms copied in from pinned memory
+    # and the weights + energy estimate read back every block
+    e2e = None
+    if not args.no_e2e:
+        host_u = torch.rand((BLOCK, W, Nc), dtype=torch.float64).pin_memory()
+        dev_u = torch.empty((BLOCK, W, Nc), dtype=torch.float64, device="cuda")
+        host_w = torch.empty((W,), dtype=torch.complex128).pin_memory()
+        host_e = torch.empty((4,), dtype=torch.complex128).pin_memory()
+
+        def block_e2e():
+            dev_u.copy_(host_u, non_blocking=True)
+            for s in range(BLOCK):
+                st = sim.step_index
+                sim.prop.Propagate(sim.wset, sim.Eshift, dev_u[s])
+                if st % 5 == 0:
+                    sim.prop.Orthogonalize(sim.wset)
+                if st % 10 == 0:
+                    A.population_control(sim.wset, sim.walker_rng)
+                sim.step_index += 1
+            E, _ = sim.wfn.Energy(sim.wset, set_properties=False, precision=prec)
+            sums = A.energy_sums(sim.wset, E)
+            host_e.copy_(sums, non_blocking=True)
+            host_w.copy_(sim.wset.properties()[:, 0], non_blocking=True)
+
+        block_e2e()
+        torch.cuda.synchronize()
+        barrier()
+        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k0.record(stream)
+        for _ in range(args.steps):
+            block_e2e()
+        k1.record(stream)
+        torch.cuda.synchronize()
+        te = k0.elapsed_time(k1)
+        if world > 1:
+            t = torch.tensor([te], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        e2e = {"value": W * world * BLOCK * args.steps / (te / 1000), "unit": "walker-steps/s",
+               "h2d_bytes_per_step": int(host_u.numel() * 8),
+               "d2h_bytes_per_step": int((host_w.numel() + host_e.numel()) * 16)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = host_cores()
+        os.environ.setdefault("OPENBLAS_NUM_THREADS", str(cores))
+        v, t, desc = cpu_sample(wl, 16, 1)
+        cpu = {"value": v, "unit": "walker-steps/s", "cores": cores, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": metric_name(), "value": value, "unit": "walker-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128" if prec == A.PREC_FP64 else "c128+tf32x3",
+            "data": "synthetic",
+            "config": {"workload": "M=200 N=50+50 Nc=1600 W=1024/GPU dt=0.005 taylor=6, "
+                                   "block of 10 steps (ortho/5, comb/10, energy/10)",
+                       "precision": args.precision, "global_walkers": W * world,
+                       "parallelism": f"walker dp{world}",
+                       "l2": "inputs larger than L2 (V 655 MB, Likn 512 MB per step)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clk, "phases_ms": phases,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

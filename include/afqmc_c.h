@@ -1,0 +1,301 @@
+/*
+ * afqmc_c.h — C ABI of the B200-native batched AFQMC walker step.
+ *
+ * Drop-in boundary for the hot path of bkesk/SAFIRE (paths below are relative to that repository):
+ *   - HamiltonianOperations (Real3IndexFactorization alternative):
+ *       src/AFQMC/HamiltonianOperations/HamiltonianOperations.h:33-103,
+ *       src/AFQMC/HamiltonianOperations/Real3IndexFactorization.hpp
+ *   - det_ops free functions: src/AFQMC/SlaterDeterminantOperations/{density_matrix,orthogonalize,
+ *       propagate}.hpp
+ *   - the single-determinant NOMSD trial: src/AFQMC/Wavefunctions/NOMSD.{hpp,cpp}
+ *   - the hybrid phaseless propagator step and comb population control:
+ *       src/AFQMC/Propagators/AFQMCBasePropagator.{h,cpp}, Propagators/WalkerSetUpdate.hpp,
+ *       src/AFQMC/Walkers/population_control.hpp
+ *
+ * Conventions
+ *   - complex128 is afqmc_c128 {re, im}, layout-compatible with std::complex<double>.
+ *   - All arrays are C-ordered (row-major) like the reference's nda views.  Device arrays are
+ *     caller-owned device pointers unless a parameter says "host".
+ *   - Every function returns an AFQMC_* status; 0 is success.  afqmc_last_error() gives a
+ *     human-readable detail for the calling thread.  No C++ exception crosses the ABI.
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).  Calls are asynchronous with
+ *     respect to the host unless documented otherwise.
+ *   - Where the reference accumulates into an output (log-overlaps), so do these functions.
+ */
+#ifndef AFQMC_C_H
+#define AFQMC_C_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct afqmc_c128 {
+  double re, im;
+} afqmc_c128;
+
+typedef struct CUstream_st* afqmc_stream; /* == cudaStream_t */
+
+/* status codes (the reference throws; these replace its utils::check / APP_ABORT paths) */
+#define AFQMC_OK 0
+#define AFQMC_ERR_ARG 1         /* invalid argument / null pointer */
+#define AFQMC_ERR_SHAPE 2       /* shape or size mismatch (utils::check "Size mismatch") */
+#define AFQMC_ERR_CUDA 3        /* CUDA runtime error */
+#define AFQMC_ERR_NONFINITE 4   /* non-finite value where the reference would abort */
+#define AFQMC_ERR_TIMEOUT 5     /* a bounded device wait gave up */
+#define AFQMC_ERR_ALLOC 6       /* device allocation failed */
+#define AFQMC_ERR_UNSUPPORTED 7 /* configuration outside what this build implements */
+#define AFQMC_ERR_COLLAPSE 8    /* total walker weight collapsed (population_control.hpp:39) */
+
+/* walker types (reference enum WALKER_TYPES, src/AFQMC/config.h:46-52) */
+#define AFQMC_CLOSED 1
+#define AFQMC_COLLINEAR 2
+
+/* precision of the contraction kernels */
+#define AFQMC_PREC_FP64 0  /* complex128 throughout (the drop-in) */
+#define AFQMC_PREC_MIXED 1 /* 3xTF32 tensor-core contractions, FP64 LU/QR/weights/energy sums */
+
+/* walker_data scalar properties, in walker-row order (src/AFQMC/Walkers/WalkerConfig.hpp:28-48,
+ * WalkerSetBase.cpp:88-110) */
+#define AFQMC_WEIGHT 0
+#define AFQMC_PHASE 1
+#define AFQMC_PSEUDO_ELOC 2
+#define AFQMC_E1 3
+#define AFQMC_EXX 4
+#define AFQMC_EJ 5
+#define AFQMC_OVLP 6
+#define AFQMC_LOGSCL_UP 7
+#define AFQMC_LOGSCL_DN 8
+#define AFQMC_IS_UNITARY 9
+#define AFQMC_THETA 10
+#define AFQMC_NPROP 11
+
+const char* afqmc_status_string(int status);
+const char* afqmc_last_error(void);
+int afqmc_version(void);
+/* number of kernels this library has launched in the process (instrumentation) */
+unsigned long long afqmc_kernel_launches(void);
+
+/* =========================================================================================
+ * det_ops (src/AFQMC/SlaterDeterminantOperations/density_matrix.hpp, orthogonalize.hpp,
+ * propagate.hpp).  S is [W][M][N] with a walker stride of ldS elements (>= M*N), so a walker
+ * buffer row (Slater block followed by properties) can be passed directly.
+ * ========================================================================================= */
+
+/* det_ops::Log_Overlap(A=PsiT [N][M], B=S, ovlp) — density_matrix.hpp:431-447.
+ * ovlp[w] += log det(PsiT * S_w), imaginary part wrapped to [-pi, pi] after accumulation
+ * (numerics/operations/determinants_impl.hpp:32-75). */
+int afqmc_log_overlap(const afqmc_c128* PsiT, const afqmc_c128* S, long ldS, afqmc_c128* ovlp,
+                      int W, int M, int N, afqmc_stream stream);
+
+/* det_ops::MixedDensityMatrix(A=PsiT, B=S, C=G, ovlp, compact, herm=true) —
+ * density_matrix.hpp:535-601.  compact != 0: G [W][N][M] = (PsiT S_w)^{-T} S_w^T;
+ * compact == 0: G [W][M][M] = PsiT^T (PsiT S_w)^{-T} S_w^T.  ldG = walker stride of G.
+ * A singular PsiT S_w gives a zero inverse (getri_or_zero, numerics/nda_functions.hpp:422). */
+int afqmc_mixed_density_matrix(const afqmc_c128* PsiT, const afqmc_c128* S, long ldS,
+                               afqmc_c128* G, long ldG, afqmc_c128* ovlp, int W, int M, int N,
+                               int compact, afqmc_stream stream);
+
+/* det_ops::detail::inverse_logdet (batched) — density_matrix.hpp:80-111.
+ * Ainv [W][N][N] = A^{-1} (zero if singular), logdet[w] += log det A_w. */
+int afqmc_inverse_logdet(const afqmc_c128* A, afqmc_c128* Ainv, afqmc_c128* logdet, int W, int N,
+                         afqmc_stream stream);
+
+/* det_ops::orthogonalize(A=S, log_detR) — orthogonalize.hpp:131-169.  In place: S_w <- Q_w with
+ * R's diagonal made real-positive; logdetR[w] += sum_i log(|R_ii|) (the sign-fixed QR log det). */
+int afqmc_orthogonalize(afqmc_c128* S, long ldS, afqmc_c128* logdetR, int W, int M, int N,
+                        afqmc_stream stream);
+
+/* det_ops::detail::propagate_impl<'N'>(npol=1, S, P1, V, order) — propagate.hpp:238-298.
+ * S_w <- P1 * sum_{n=0..order} (i V_w)^n/n! * P1 * S_w.  P1 [M][M] (shared), V [W][M][M]. */
+int afqmc_propagate(const afqmc_c128* P1, const afqmc_c128* V, afqmc_c128* S, long ldS, int W,
+                    int M, int N, int order, afqmc_stream stream);
+
+/* =========================================================================================
+ * HamiltonianOperations, Real3IndexFactorization alternative (ndet = 1, npol = 1).
+ * ========================================================================================= */
+typedef struct afqmc_ham_s* afqmc_ham;
+
+/* Builds the device tensors of RealDenseHamiltonian::getHamiltonianOperations
+ * (src/AFQMC/Hamiltonians/RealDenseHamiltonian.cpp:36-184): Likn, Lnak = PsiT L, haj = PsiT h
+ * (HamiltonianOperations/detail/one_body.hpp:124-153) and v0 = -1/2 sum L L.
+ *   Likn  host float64 [nspin_H2][M][M][Nc]   (Hamiltonian/DenseFactorized/L)
+ *   hij   host complex [nspin_H1][M][M]       (Hamiltonian/hcore)
+ *   PsiT  host complex [nup][M] (+ [ndn][M] for COLLINEAR): the trial's conjugate transpose
+ * The handle is bound to the device current at creation. */
+int afqmc_ham_create(int walker_type, int M, int nup, int ndn, int Nc, const double* Likn,
+                     int nspin_H2, const afqmc_c128* hij, int nspin_H1, double E0,
+                     const afqmc_c128* PsiT, afqmc_ham* out);
+int afqmc_ham_destroy(afqmc_ham ham);
+/* number_of_cholesky_vectors / energy_offset / walker type (Real3IndexFactorization.hpp:432-438) */
+int afqmc_ham_info(afqmc_ham ham, int* walker_type, int* M, int* nup, int* ndn, int* Nc,
+                   double* E0);
+/* Copies of the built tensors (for tests): Lnak [nspin][Nc][N_s][M], haj [nel][M],
+ * vexx [nspin_H2][M][M] (all host). Any pointer may be NULL. */
+int afqmc_ham_get_tensors(afqmc_ham ham, afqmc_c128* Lnak, afqmc_c128* haj, double* vexx);
+
+/* Real3IndexFactorization::vbias — Real3IndexFactorization.hpp:328-428 (half-rotated G).
+ * G [W][nel*M], v [W][Nc]: v = sqrt(dt) (x2 if CLOSED) sum_{a,k} G[w,a,k] Lnak[n,a,k]. */
+int afqmc_ham_vbias(afqmc_ham ham, const afqmc_c128* G, afqmc_c128* v, int W, double dt,
+                    int precision, afqmc_stream stream);
+
+/* Real3IndexFactorization::vHS — Real3IndexFactorization.hpp:282-326.  X [W][Nc];
+ * V [nspin_vHS][W][M][M] (caller-owned; the reference returns a pooled buffer):
+ * V[s,w,i,k] = sqrt(dt) sum_n L_s[i,k,n] X[w,n]. */
+int afqmc_ham_vhs(afqmc_ham ham, const afqmc_c128* X, afqmc_c128* V, int W, double dt,
+                  int precision, afqmc_stream stream);
+
+/* Real3IndexFactorization::energy — Real3IndexFactorization.hpp:138-174, 476-590.
+ * E [W][3] = (E1, EXX, EJ) from the half-rotated G [W][nel*M]. */
+int afqmc_ham_energy(afqmc_ham ham, const afqmc_c128* G, afqmc_c128* E, int W, int addH1,
+                     int addEJ, int addEXX, int precision, afqmc_stream stream);
+
+/* getOneBodyPropagatorMatrix — Real3IndexFactorization.hpp:99-124 with add_one_body_shifts
+ * (detail/one_body.hpp:65-85).  vMF host [Nc]; H1 host [nspin][M][M] = dt (h + v0) + vHS(vMF).
+ * Synchronous. */
+int afqmc_ham_one_body_propagator(afqmc_ham ham, double dt, const afqmc_c128* vMF,
+                                  afqmc_c128* H1);
+
+/* =========================================================================================
+ * Walker set: device buffer of rows [S_alpha (M*nup) | S_beta (M*ndn) | 11 properties]
+ * (WalkerSetBase.cpp:44-125).  For CLOSED walkers ndn is not stored.
+ * ========================================================================================= */
+typedef struct afqmc_wset_s* afqmc_wset;
+
+int afqmc_wset_create(int walker_type, int M, int nup, int ndn, int W, afqmc_wset* out);
+int afqmc_wset_destroy(afqmc_wset ws);
+/* device pointer to the walker buffer and the row length in complex elements */
+int afqmc_wset_buffer(afqmc_wset ws, afqmc_c128** data, long* walker_size, int* W);
+/* property column <-> host [W] (WalkerSetBase.h:463-481 getProperty/setProperty); synchronous */
+int afqmc_wset_get_property(afqmc_wset ws, int prop, afqmc_c128* host_out);
+int afqmc_wset_set_property(afqmc_wset ws, int prop, const afqmc_c128* host_in);
+/* every walker = the trial (NOMSD::initial_guess, NOMSD.cpp:131-153), weight = phase = 1 */
+int afqmc_wset_init_from_trial(afqmc_wset ws, afqmc_ham ham, afqmc_stream stream);
+
+/* =========================================================================================
+ * Single-determinant NOMSD trial on a walker set (Wavefunctions/NOMSD.cpp)
+ * ========================================================================================= */
+
+/* NOMSD::MixedDensityMatrix / DensityMatrix (compact) — NOMSD.hpp:293-343:
+ * G [W][nel*M], ovlp [W] (overwritten; CLOSED doubles the single-spin log overlap). */
+int afqmc_wfn_density_matrix(afqmc_ham ham, afqmc_wset ws, afqmc_c128* G, afqmc_c128* ovlp,
+                             afqmc_stream stream);
+/* NOMSD::Log_Overlap — NOMSD.cpp:280-301 (+ log conj(ci), ci = 1). ovlp [W] overwritten. */
+int afqmc_wfn_log_overlap(afqmc_ham ham, afqmc_wset ws, afqmc_c128* ovlp, afqmc_stream stream);
+/* NOMSD::Energy — NOMSD.cpp:159-182: E [W][3], ovlp [W] (device, overwritten).
+ * set_properties != 0 also stores OVLP, E1, EXX, EJ on the walkers (NOMSD.cpp:67-79). */
+int afqmc_wfn_energy(afqmc_ham ham, afqmc_wset ws, afqmc_c128* E, afqmc_c128* ovlp,
+                     int set_properties, int precision, afqmc_stream stream);
+/* NOMSD::vMF — NOMSD.cpp:437-465: vbias of the trial's own density matrix.  host [Nc]. */
+int afqmc_wfn_vmf(afqmc_ham ham, double dt, afqmc_c128* vMF_host);
+
+/* =========================================================================================
+ * Propagator (AFQMCBasePropagator, hybrid force bias, dense vHS, single determinant)
+ * ========================================================================================= */
+typedef struct afqmc_prop_params {
+  double dt;
+  int taylor_n;                 /* 6 */
+  double vbias_bound;           /* 50 */
+  double upper_cutoff_scale;    /* 10 */
+  double lower_cutoff_scale;    /* 1 */
+  double weight_bound_floor;    /* 100 */
+  double weight_bound_fraction; /* 0.1 */
+  int denseP1;                  /* 0: P1 truncated at |x| > 1e-8 like the reference's CSR copy */
+  int precision;                /* AFQMC_PREC_* */
+} afqmc_prop_params;
+
+typedef struct afqmc_prop_s* afqmc_prop;
+
+/* Fills the reference defaults for a non-model Hamiltonian (parameters.hpp:103-131,
+ * parameter_defaults.cpp:274-289). */
+void afqmc_prop_params_default(afqmc_prop_params* p);
+
+/* AFQMCBasePropagator construction + generateP1 (AFQMCBasePropagator.cpp:42-214):
+ * vMF (imag zeroed), H1, hermitize, P1 = exp(-H1/2), CSR-like truncation.  Allocates the step
+ * workspace for up to max_walkers walkers.  Synchronous. */
+int afqmc_prop_create(afqmc_ham ham, const afqmc_prop_params* params, int max_walkers,
+                      afqmc_prop* out);
+int afqmc_prop_destroy(afqmc_prop prop);
+/* host copies: P1 [nspin][M][M], vMF [Nc] (either may be NULL) */
+int afqmc_prop_get_p1(afqmc_prop prop, afqmc_c128* P1, afqmc_c128* vMF);
+
+/* One phaseless step, AFQMCBasePropagator::Propagate (AFQMCBasePropagator.cpp:289-392):
+ * vbias -> X (construct_X) -> vHS -> propagate -> Log_Overlap -> walker_update ->
+ * bound_walker_weights, all on the device (the walker update is the reference's host loop,
+ * restated as a kernel with the same formula).
+ *   uniforms: device [W][Nc] field uniforms (the reference's RNGbuff, rng_block_size = Nc), or
+ *             NULL to draw them on the device from the propagator's counter-based generator.
+ * Capturable in a CUDA graph when uniforms == NULL or points to a fixed device buffer. */
+int afqmc_prop_step(afqmc_prop prop, afqmc_wset ws, double Eshift, const double* uniforms,
+                    afqmc_stream stream);
+/* Same as afqmc_prop_step but Eshift is read from device memory at run time (graph friendly). */
+int afqmc_prop_step_dev(afqmc_prop prop, afqmc_wset ws, const double* Eshift_dev,
+                        const double* uniforms, afqmc_stream stream);
+/* AFQMCBasePropagator::Orthogonalize (cpp:735-741): QR re-orthonormalisation then OVLP refresh. */
+int afqmc_prop_orthogonalize(afqmc_prop prop, afqmc_wset ws, afqmc_stream stream);
+/* Seeds / advances the device field generator (Philox4x32-10, counter = step). */
+int afqmc_prop_set_field_seed(afqmc_prop prop, unsigned long long seed);
+/* Last step's intermediates, device pointers valid until the next step: vbias [W][Nc],
+ * X [W][Nc], HW [W], mf [W], new_ovlp [W].  Any output may be NULL. */
+int afqmc_prop_last_step(afqmc_prop prop, const afqmc_c128** vbias, const afqmc_c128** X,
+                         const afqmc_c128** hw, const afqmc_c128** mf,
+                         const afqmc_c128** new_ovlp);
+/* Per-phase device timing of a step, the analogue of the reference's AFQMCTimers
+ * (src/AFQMC/Utilities/AFQMCTimer.h:25-63): phases G_for_vbias, vbias, assemble_X, vHS,
+ * propagate, pseudo_energy (overlap), extra (walker update).  afqmc_prop_timings waits for and
+ * returns the milliseconds of the last step run with timing enabled. */
+#define AFQMC_NPHASE 7
+int afqmc_prop_set_timing(afqmc_prop prop, int enable);
+int afqmc_prop_timings(afqmc_prop prop, double* ms);
+/* bound statistics (AFQMCBasePropagator.h:199-237): counts[6] = eloc {total, upper, lower},
+ * weight {total, upper, lower}; synchronous */
+int afqmc_prop_bound_stats(afqmc_prop prop, long long* counts);
+
+/* =========================================================================================
+ * Population control and estimators (host + device)
+ * ========================================================================================= */
+typedef struct afqmc_host_rng_s* afqmc_host_rng;
+
+/* split_seed (src/utilities/Random.cpp:7-20) */
+unsigned long long afqmc_split_seed(int seed, int rank, unsigned stream);
+/* HostRandomGenerator (src/utilities/Random.hpp:37-51): std::mt19937 + uniform_real_distribution */
+int afqmc_host_rng_create(unsigned long long seed, afqmc_host_rng* out);
+int afqmc_host_rng_destroy(afqmc_host_rng rng);
+int afqmc_host_rng_uniform(afqmc_host_rng rng, double* out, long n);
+
+/* comb (population_control.hpp:34-65): host arrays; draws one uniform from rng. */
+int afqmc_comb(afqmc_host_rng rng, const double* weights, int n, int num_target, int* offspring);
+/* plan_walker_exchange (population_control.hpp:87-133): pure host logic. plan holds up to
+ * max_plan entries of {src, walker, dst, copies}; *nplan receives the count. */
+int afqmc_plan_walker_exchange(const int* offspring, const int* counts, int nranks, int* plan,
+                               int max_plan, int* nplan);
+/* population_control on one rank (population_control.hpp:218-255): |w| to host, comb, row
+ * copies on the device in the reference's slot order, weights <- w/|w|.  Synchronous.
+ * offspring (host [W]) may be NULL. */
+int afqmc_population_control(afqmc_wset ws, afqmc_host_rng rng, int* offspring,
+                             afqmc_stream stream);
+/* Row gather: dst row j <- src row src_index[j] (device int array) for j in [0, n); rows of
+ * walker_size elements.  Building block for the multi-rank exchange. */
+int afqmc_wset_copy_rows(afqmc_wset ws, const int* dst_slots, const int* src_slots, int n,
+                         afqmc_stream stream);
+/* pack rows idx[0..n) into buf [n][walker_size] / unpack buf rows into slots idx (device) */
+int afqmc_wset_pack_rows(afqmc_wset ws, const int* idx, int n, afqmc_c128* buf,
+                         afqmc_stream stream);
+int afqmc_wset_unpack_rows(afqmc_wset ws, const int* idx, int n, const afqmc_c128* buf,
+                           afqmc_stream stream);
+/* weights <- w/|w| for all walkers (end of population_control) */
+int afqmc_wset_normalize_weights(afqmc_wset ws, afqmc_stream stream);
+
+/* EnergyEstimator::measure sums (EnergyEstimator.h:51-100): out4 (device) =
+ * {sum_w w E1, sum_w w EXX, sum_w w EJ, sum_w w} */
+int afqmc_energy_sums(afqmc_wset ws, const afqmc_c128* E, afqmc_c128* out4, afqmc_stream stream);
+/* averagePseudoEnergy numerator/denominator (Drivers/average_energy.hpp:53-63): out2 (device) =
+ * {sum w exp(dt*eloc), sum w} */
+int afqmc_pseudo_energy_sums(afqmc_wset ws, double dt, afqmc_c128* out2, afqmc_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AFQMC_C_H */

@@ -1,0 +1,399 @@
+"""Python mirror of the reference's operator API for the walker step, on top of the C ABI.
+
+Names follow bkesk/SAFIRE so that tests and drivers read like the reference's own:
+
+  det_ops.Log_Overlap / MixedDensityMatrix / orthogonalize / Propagate / inverse_logdet
+        (src/AFQMC/SlaterDeterminantOperations/*.hpp)
+  HamiltonianOperations (Real3IndexFactorization): vbias, vHS, energy,
+        getOneBodyPropagatorMatrix, number_of_cholesky_vectors, energy_offset
+        (src/AFQMC/HamiltonianOperations/Real3IndexFactorization.hpp)
+  NOMSD: MixedDensityMatrix, Log_Overlap, Energy, vMF  (src/AFQMC/Wavefunctions/NOMSD.cpp)
+  WalkerSet: getProperty / setProperty / SlaterMatrices  (src/AFQMC/Walkers/WalkerSetBase.h)
+  Propagator: Propagate(wset, Eshift), Orthogonalize(wset)  (Propagators/AFQMCBasePropagator.cpp)
+  population_control(wset, rng)  (src/AFQMC/Walkers/population_control.hpp)
+
+Device arrays are torch CUDA tensors (complex128 / float64), used only as device memory and
+streams; every computation runs in the CUDA library.  Errors raise capi.AfqmcError, the analogue
+of the reference's utils::check exceptions.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from types import SimpleNamespace
+
+import numpy as np
+import torch
+
+from . import capi
+from .capi import call, lib, vp
+
+CLOSED, COLLINEAR = capi.CLOSED, capi.COLLINEAR
+PREC_FP64, PREC_MIXED = capi.PREC_FP64, capi.PREC_MIXED
+
+
+def _stream(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return vp(s.cuda_stream)
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if isinstance(t, torch.Tensor):
+        if not t.is_cuda and t.numel() > 0:
+            raise ValueError("expected a CUDA tensor")
+        return vp(t.data_ptr())
+    return vp(t)
+
+
+def _host_ptr(a: np.ndarray):
+    return vp(a.ctypes.data)
+
+
+class _DevView:
+    """__cuda_array_interface__ wrapper so torch can view library-owned device memory."""
+
+    def __init__(self, ptr, shape, typestr, strides=None):
+        self.__cuda_array_interface__ = dict(shape=tuple(shape), typestr=typestr,
+                                             data=(int(ptr), False), version=3,
+                                             strides=strides)
+
+
+def device_view(ptr, shape, dtype=torch.complex128, strides_bytes=None):
+    typestr = {torch.complex128: "<c16", torch.float64: "<f8", torch.int32: "<i4"}[dtype]
+    return torch.as_tensor(_DevView(ptr, shape, typestr, strides_bytes), device="cuda")
+
+
+# --------------------------------------------------------------------------------------------
+# det_ops
+# --------------------------------------------------------------------------------------------
+class det_ops:  # noqa: N801 (reference namespace name)
+    @staticmethod
+    def Log_Overlap(A, B, ovlp, stream=None):
+        """A = PsiT [N, M], B = S [W, M, N] (walker stride B.stride(0)), ovlp [W] accumulated."""
+        W, M, N = B.shape
+        call("afqmc_log_overlap", _ptr(A), _ptr(B), B.stride(0), _ptr(ovlp), W, M, N,
+             _stream(stream))
+
+    @staticmethod
+    def MixedDensityMatrix(A, B, C_, ovlp, compact=True, stream=None):
+        W, M, N = B.shape
+        call("afqmc_mixed_density_matrix", _ptr(A), _ptr(B), B.stride(0), _ptr(C_), C_.stride(0),
+             _ptr(ovlp), W, M, N, int(bool(compact)), _stream(stream))
+
+    @staticmethod
+    def inverse_logdet(A, Ainv, logdet, stream=None):
+        W, N, _ = A.shape
+        call("afqmc_inverse_logdet", _ptr(A), _ptr(Ainv), _ptr(logdet), W, N, _stream(stream))
+
+    @staticmethod
+    def orthogonalize(A, log_detR, stream=None):
+        W, M, N = A.shape
+        call("afqmc_orthogonalize", _ptr(A), A.stride(0), _ptr(log_detR), W, M, N,
+             _stream(stream))
+
+    @staticmethod
+    def Propagate(S, P1, V, order=6, stream=None):
+        W, M, N = S.shape
+        call("afqmc_propagate", _ptr(P1), _ptr(V), _ptr(S), S.stride(0), W, M, N, order,
+             _stream(stream))
+
+
+# --------------------------------------------------------------------------------------------
+# HamiltonianOperations (Real3IndexFactorization)
+# --------------------------------------------------------------------------------------------
+class HamiltonianOperations:
+    def __init__(self, walker_type, M, nup, ndn, Likn, hij, E0, PsiT):
+        """Likn float64 [nspin_H2, M, M, Nc]; hij complex [nspin_H1, M, M]; PsiT list of complex
+        [N_s, M] (numpy, host)."""
+        Likn = np.ascontiguousarray(Likn, dtype=np.float64)
+        hij = np.ascontiguousarray(hij, dtype=np.complex128)
+        psi = np.ascontiguousarray(np.concatenate([np.asarray(p) for p in PsiT], axis=0),
+                                   dtype=np.complex128)
+        self.walker_type, self.M, self.nup, self.ndn = walker_type, M, nup, ndn
+        self.Nc = Likn.shape[3]
+        self.E0 = float(E0)
+        self.nel = nup + (ndn if walker_type == COLLINEAR else 0)
+        h = vp()
+        call("afqmc_ham_create", walker_type, M, nup, ndn, self.Nc, _host_ptr(Likn), Likn.shape[0],
+             _host_ptr(hij), hij.shape[0], float(E0), _host_ptr(psi), C.byref(h))
+        self.handle = h
+        self.nspin_H2 = Likn.shape[0]
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and capi._lib is not None:
+            capi._lib.afqmc_ham_destroy(h)
+            self.handle = None
+
+    def number_of_cholesky_vectors(self):
+        return self.Nc
+
+    def energy_offset(self):
+        return self.E0
+
+    def vbias(self, G, v, dt, precision=PREC_FP64, stream=None):
+        call("afqmc_ham_vbias", self.handle, _ptr(G), _ptr(v), G.shape[0], float(dt), precision,
+             _stream(stream))
+
+    def vHS(self, X, dt, precision=PREC_FP64, stream=None, out=None):
+        W = X.shape[0]
+        nst = self.nspin_H2 if self.walker_type == COLLINEAR else 1
+        V = out if out is not None else torch.empty((nst, W, self.M, self.M),
+                                                    dtype=torch.complex128, device=X.device)
+        call("afqmc_ham_vhs", self.handle, _ptr(X), _ptr(V), W, float(dt), precision,
+             _stream(stream))
+        return V
+
+    def energy(self, E, G, addH1=True, addEJ=True, addEXX=True, precision=PREC_FP64,
+               stream=None):
+        call("afqmc_ham_energy", self.handle, _ptr(G), _ptr(E), G.shape[0], int(addH1),
+             int(addEJ), int(addEXX), precision, _stream(stream))
+
+    def getOneBodyPropagatorMatrix(self, dt, vMF):
+        nspin = 2 if self.walker_type == COLLINEAR else 1
+        vm = np.ascontiguousarray(vMF, dtype=np.complex128)
+        H1 = np.zeros((nspin, self.M, self.M), dtype=np.complex128)
+        call("afqmc_ham_one_body_propagator", self.handle, float(dt), _host_ptr(vm), _host_ptr(H1))
+        return H1
+
+    def tensors(self):
+        nspin = 2 if self.walker_type == COLLINEAR else 1
+        nel = [self.nup, self.ndn if self.walker_type == COLLINEAR else 0]
+        Lnak = np.zeros(sum(self.Nc * n * self.M for n in nel[:nspin]), dtype=np.complex128)
+        haj = np.zeros((self.nel, self.M), dtype=np.complex128)
+        vexx = np.zeros((self.nspin_H2, self.M, self.M), dtype=np.float64)
+        call("afqmc_ham_get_tensors", self.handle, _host_ptr(Lnak), _host_ptr(haj),
+             _host_ptr(vexx))
+        out, off = [], 0
+        for s in range(nspin):
+            n = self.Nc * nel[s] * self.M
+            out.append(Lnak[off:off + n].reshape(self.Nc, nel[s], self.M))
+            off += n
+        return SimpleNamespace(Lnak=out, haj=haj, vexx=vexx)
+
+
+Real3IndexFactorization = HamiltonianOperations
+
+
+# --------------------------------------------------------------------------------------------
+# Walker set
+# --------------------------------------------------------------------------------------------
+class WalkerSet:
+    def __init__(self, walker_type, M, nup, ndn, W):
+        h = vp()
+        call("afqmc_wset_create", walker_type, M, nup, ndn, W, C.byref(h))
+        self.handle = h
+        self.walker_type, self.M, self.nup, self.W = walker_type, M, nup, W
+        self.ndn = ndn if walker_type == COLLINEAR else 0
+        data, ws, nw = vp(), C.c_long(), C.c_int()
+        call("afqmc_wset_buffer", h, C.byref(data), C.byref(ws), C.byref(nw))
+        self.walker_size = ws.value
+        self.buffer = device_view(data.value, (W, self.walker_size))
+        self.prop0 = M * (self.nup + self.ndn)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and capi._lib is not None:
+            capi._lib.afqmc_wset_destroy(h)
+            self.handle = None
+
+    def size(self):
+        return self.W
+
+    def SlaterMatrices(self, spin=0):
+        """[W, M, N_s] view with the walker stride (WalkerSetBase.h:255-275)."""
+        off = 0 if spin == 0 else self.M * self.nup
+        n = self.nup if spin == 0 else self.ndn
+        return self.buffer[:, off:off + self.M * n].unflatten(1, (self.M, n))
+
+    def getProperty(self, prop):
+        out = np.zeros(self.W, dtype=np.complex128)
+        call("afqmc_wset_get_property", self.handle, prop, _host_ptr(out))
+        return out
+
+    def setProperty(self, prop, values):
+        v = np.ascontiguousarray(np.broadcast_to(np.asarray(values, dtype=np.complex128),
+                                                 (self.W,)))
+        call("afqmc_wset_set_property", self.handle, prop, _host_ptr(v))
+
+    def properties(self):
+        return self.buffer[:, self.prop0:self.prop0 + capi.NPROP]
+
+    def init_from_trial(self, ham: HamiltonianOperations, stream=None):
+        call("afqmc_wset_init_from_trial", self.handle, ham.handle, _stream(stream))
+
+
+# --------------------------------------------------------------------------------------------
+# NOMSD single-determinant trial
+# --------------------------------------------------------------------------------------------
+class NOMSD:
+    def __init__(self, ham: HamiltonianOperations):
+        self.ham = ham
+
+    def MixedDensityMatrix(self, wset: WalkerSet, G=None, ovlp=None, stream=None):
+        dev = wset.buffer.device
+        G = G if G is not None else torch.empty((wset.W, self.ham.nel * self.ham.M),
+                                                dtype=torch.complex128, device=dev)
+        ovlp = ovlp if ovlp is not None else torch.empty(wset.W, dtype=torch.complex128,
+                                                         device=dev)
+        call("afqmc_wfn_density_matrix", self.ham.handle, wset.handle, _ptr(G), _ptr(ovlp),
+             _stream(stream))
+        return G, ovlp
+
+    def Log_Overlap(self, wset: WalkerSet, ovlp=None, stream=None):
+        ovlp = ovlp if ovlp is not None else torch.empty(wset.W, dtype=torch.complex128,
+                                                         device=wset.buffer.device)
+        call("afqmc_wfn_log_overlap", self.ham.handle, wset.handle, _ptr(ovlp), _stream(stream))
+        return ovlp
+
+    def Energy(self, wset: WalkerSet, set_properties=True, precision=PREC_FP64, stream=None):
+        dev = wset.buffer.device
+        E = torch.empty((wset.W, 3), dtype=torch.complex128, device=dev)
+        ov = torch.empty(wset.W, dtype=torch.complex128, device=dev)
+        call("afqmc_wfn_energy", self.ham.handle, wset.handle, _ptr(E), _ptr(ov),
+             int(set_properties), precision, _stream(stream))
+        return E, ov
+
+    def vMF(self, dt):
+        v = np.zeros(self.ham.Nc, dtype=np.complex128)
+        call("afqmc_wfn_vmf", self.ham.handle, float(dt), _host_ptr(v))
+        return v
+
+
+# --------------------------------------------------------------------------------------------
+# Propagator
+# --------------------------------------------------------------------------------------------
+def default_params(**kw):
+    p = capi.PropParams()
+    lib().afqmc_prop_params_default(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class Propagator:
+    def __init__(self, ham: HamiltonianOperations, params: capi.PropParams, max_walkers):
+        h = vp()
+        call("afqmc_prop_create", ham.handle, C.byref(params), int(max_walkers), C.byref(h))
+        self.handle = h
+        self.ham = ham
+        self.params = params
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and capi._lib is not None:
+            capi._lib.afqmc_prop_destroy(h)
+            self.handle = None
+
+    def P1_vMF(self):
+        nspin = 2 if self.ham.walker_type == COLLINEAR else 1
+        P1 = np.zeros((nspin, self.ham.M, self.ham.M), dtype=np.complex128)
+        vMF = np.zeros(self.ham.Nc, dtype=np.complex128)
+        call("afqmc_prop_get_p1", self.handle, _host_ptr(P1), _host_ptr(vMF))
+        return P1, vMF
+
+    def set_field_seed(self, seed):
+        call("afqmc_prop_set_field_seed", self.handle, int(seed))
+
+    def Propagate(self, wset: WalkerSet, Eshift, uniforms=None, stream=None):
+        """One step.  uniforms: device float64 [W, Nc] or None (device Philox generator)."""
+        call("afqmc_prop_step", self.handle, wset.handle, float(Eshift), _ptr(uniforms),
+             _stream(stream))
+
+    def Propagate_dev(self, wset: WalkerSet, Eshift_dev, uniforms=None, stream=None):
+        call("afqmc_prop_step_dev", self.handle, wset.handle, _ptr(Eshift_dev), _ptr(uniforms),
+             _stream(stream))
+
+    def Orthogonalize(self, wset: WalkerSet, stream=None):
+        call("afqmc_prop_orthogonalize", self.handle, wset.handle, _stream(stream))
+
+    def last_step(self, W):
+        ptrs = [vp() for _ in range(5)]
+        call("afqmc_prop_last_step", self.handle, *[C.byref(p) for p in ptrs])
+        Nc = self.ham.Nc
+        vb, X, hw, mf, nov = (p.value for p in ptrs)
+        return SimpleNamespace(vbias=device_view(vb, (W, Nc)), X=device_view(X, (W, Nc)),
+                               HW=device_view(hw, (W,)), mf=device_view(mf, (W,)),
+                               new_ovlp=device_view(nov, (W,)))
+
+    PHASES = ("G_for_vbias", "vbias", "assemble_X", "vHS", "propagate", "pseudo_energy", "extra")
+
+    def set_timing(self, enable=True):
+        call("afqmc_prop_set_timing", self.handle, int(enable))
+
+    def timings(self):
+        ms = (C.c_double * len(self.PHASES))()
+        call("afqmc_prop_timings", self.handle, ms)
+        return dict(zip(self.PHASES, list(ms)))
+
+    def bound_stats(self):
+        c = (C.c_longlong * 6)()
+        call("afqmc_prop_bound_stats", self.handle, c)
+        return list(c)
+
+
+# --------------------------------------------------------------------------------------------
+# population control and estimators
+# --------------------------------------------------------------------------------------------
+def split_seed(seed, rank, stream):
+    return int(lib().afqmc_split_seed(seed, rank, stream))
+
+
+class HostRandomGenerator:
+    """std::mt19937 + uniform_real_distribution<double> (src/utilities/Random.hpp:37-51)."""
+
+    def __init__(self, seed64):
+        h = vp()
+        call("afqmc_host_rng_create", int(seed64), C.byref(h))
+        self.handle = h
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and capi._lib is not None:
+            capi._lib.afqmc_host_rng_destroy(h)
+            self.handle = None
+
+    def sample_uniform(self, n):
+        out = np.empty(n, dtype=np.float64)
+        call("afqmc_host_rng_uniform", self.handle, _host_ptr(out), int(n))
+        return out
+
+
+def comb(rng: HostRandomGenerator, weights, num_target):
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    off = np.zeros(w.size, dtype=np.int32)
+    call("afqmc_comb", rng.handle, _host_ptr(w), w.size, int(num_target), _host_ptr(off))
+    return off
+
+
+def plan_walker_exchange(offspring, counts):
+    off = np.ascontiguousarray(offspring, dtype=np.int32)
+    cnt = np.ascontiguousarray(counts, dtype=np.int32)
+    n = C.c_int()
+    call("afqmc_plan_walker_exchange", _host_ptr(off), _host_ptr(cnt), cnt.size, None, 0,
+         C.byref(n))
+    plan = np.zeros((max(n.value, 1), 4), dtype=np.int32)
+    call("afqmc_plan_walker_exchange", _host_ptr(off), _host_ptr(cnt), cnt.size, _host_ptr(plan),
+         n.value, C.byref(n))
+    return [tuple(int(x) for x in r) for r in plan[:n.value]]
+
+
+def population_control(wset: WalkerSet, rng: HostRandomGenerator, stream=None):
+    off = np.zeros(wset.W, dtype=np.int32)
+    call("afqmc_population_control", wset.handle, rng.handle, _host_ptr(off), _stream(stream))
+    return off
+
+
+def energy_sums(wset: WalkerSet, E, out=None, stream=None):
+    out = out if out is not None else torch.empty(4, dtype=torch.complex128,
+                                                  device=wset.buffer.device)
+    call("afqmc_energy_sums", wset.handle, _ptr(E), _ptr(out), _stream(stream))
+    return out
+
+
+def pseudo_energy_sums(wset: WalkerSet, dt, out=None, stream=None):
+    out = out if out is not None else torch.empty(2, dtype=torch.complex128,
+                                                  device=wset.buffer.device)
+    call("afqmc_pseudo_energy_sums", wset.handle, float(dt), _ptr(out), _stream(stream))
+    return out
