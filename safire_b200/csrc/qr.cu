@@ -61,9 +61,10 @@ __global__ void __launch_bounds__(QR_THREADS)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int pitch = N | 1;  // odd pitch: conflict-free column walks of 16-byte elements
   c128* a = reinterpret_cast<c128*>(smem_raw);
-  c128* tau = a + size_t(M) * pitch;  // [N]
-  double* rdiag = reinterpret_cast<double*>(tau + N);  // [N]
-  c128* wbuf = reinterpret_cast<c128*>(rdiag + N);     // [N]
+  // 16-byte arrays first, the 8-byte diagonal last (keeps every c128 16-byte aligned)
+  c128* tau = a + size_t(M) * pitch;                    // [N]
+  c128* wbuf = tau + N;                                 // [N]
+  double* rdiag = reinterpret_cast<double*>(wbuf + N);  // [N]
   __shared__ double red[QR_WARPS + 1];
 
   const long w = blockIdx.x;

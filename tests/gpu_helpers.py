@@ -5,12 +5,16 @@ import torch
 from oracle import afqmc as O
 
 
-def rel_err(a, b):
-    """||a-b||_inf / max(||a||_inf, ||b||_inf) (the reference's Approx metric)."""
+def rel_err(a, b, atol=1e-13):
+    """||a-b||_inf / max(||a||_inf, ||b||_inf, atol/rtol-floor): the reference's Approx metric
+    (tests/test_common.hpp:384-438) with an absolute floor, so roundoff-level values (1e-17) that
+    one side computes as exact zeros do not count as relative errors of 1."""
     a = np.asarray(a).ravel()
     b = np.asarray(b).ravel()
     d = np.max(np.abs(a - b)) if a.size else 0.0
     v = max(np.max(np.abs(a)) if a.size else 0.0, np.max(np.abs(b)) if b.size else 0.0)
+    if d <= atol:
+        return 0.0
     return d / v if v > 0 else d
 
 
