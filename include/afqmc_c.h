@@ -151,6 +151,11 @@ int afqmc_ham_vhs(afqmc_ham ham, const afqmc_c128* X, afqmc_c128* V, int W, doub
 int afqmc_ham_energy(afqmc_ham ham, const afqmc_c128* G, afqmc_c128* E, int W, int addH1,
                      int addEJ, int addEXX, int precision, afqmc_stream stream);
 
+/* Error word of the tensor-core kernels' bounded device waits (bit 0: a wait on a TMA or MMA
+ * completion gave up after about 2 s and the kernel returned without finishing).  0 = none, or
+ * the mixed-precision path was never used.  Synchronous. */
+int afqmc_ham_device_error(afqmc_ham ham, unsigned* flag);
+
 /* getOneBodyPropagatorMatrix — Real3IndexFactorization.hpp:99-124 with add_one_body_shifts
  * (detail/one_body.hpp:65-85).  vMF host [Nc]; H1 host [nspin][M][M] = dt (h + v0) + vHS(vMF).
  * Synchronous. */

@@ -157,6 +157,11 @@ class HamiltonianOperations:
         call("afqmc_ham_one_body_propagator", self.handle, float(dt), _host_ptr(vm), _host_ptr(H1))
         return H1
 
+    def device_error_flag(self):
+        f = C.c_uint()
+        call("afqmc_ham_device_error", self.handle, C.byref(f))
+        return f.value
+
     def tensors(self):
         nspin = 2 if self.walker_type == COLLINEAR else 1
         nel = [self.nup, self.ndn if self.walker_type == COLLINEAR else 0]

@@ -351,6 +351,8 @@ EnergyArgs energy_args(afqmc_ham_s* h, const c128* G, long ldG) {
   a.E0 = h->E0;
   a.scl = h->walker_type == AFQMC_CLOSED ? 2.0 : 1.0;
   a.sclj = h->walker_type == AFQMC_CLOSED ? 4.0 : 1.0;
+  a.Likn = h->Likn;
+  a.nspin_H2 = h->nspin_H2;
   return a;
 }
 
@@ -368,9 +370,11 @@ long energy_chunk_elems(afqmc_ham_s* h, int W) {
 int ham_energy(afqmc_ham_s* h, cudaStream_t s, const c128* G, long ldG, c128* E, int W, bool addH1,
                bool addEJ, bool addEXX, int precision) {
   EnergyArgs a = energy_args(h, G, ldG);
+  MixedHam* tc = nullptr;
   if (precision == AFQMC_PREC_MIXED) {
     if (!h->mixed) AFQMC_TRY(mixed_ham_create(&h->mixed, a, s));
-    return energy_mixed(s, h->mixed, a, E, W, addH1, addEJ, addEXX);
+    tc = h->mixed;
+    AFQMC_TRY(mixed_prepare_G(s, tc, G, ldG, W));
   }
   Scratch wT, ex, kl;
   long chunk = energy_chunk_elems(h, W);
@@ -378,7 +382,7 @@ int ham_energy(afqmc_ham_s* h, cudaStream_t s, const c128* G, long ldG, c128* E,
   AFQMC_TRY(ex.get(sizeof(c128) * size_t(W) * h->Nc, s));
   AFQMC_TRY(kl.get(sizeof(c128) * size_t(W) * h->Nc, s));
   return energy_fp64(s, a, E, W, addH1, addEJ, addEXX, (c128*)wT.p, chunk, (c128*)ex.p,
-                     (c128*)kl.p);
+                     (c128*)kl.p, tc);
 }
 
 }  // namespace
@@ -586,6 +590,14 @@ extern "C" int afqmc_ham_energy(afqmc_ham h, const afqmc_c128* G, afqmc_c128* E,
   return ham_energy(h, reinterpret_cast<cudaStream_t>(stream), (const c128*)G,
                     long(h->nel_tot) * h->M, (c128*)E, W, addH1 != 0, addEJ != 0, addEXX != 0,
                     precision);
+}
+
+extern "C" int afqmc_ham_device_error(afqmc_ham h, unsigned* flag) {
+  AFQMC_CHECK_ARG(h && flag, "afqmc_ham_device_error: null argument");
+  DeviceGuard g(h->device);
+  *flag = 0;
+  if (h->mixed) return mixed_error_flag(h->mixed, flag);
+  return AFQMC_OK;
 }
 
 extern "C" int afqmc_ham_one_body_propagator(afqmc_ham h, double dt, const afqmc_c128* vMF,
@@ -1077,7 +1089,7 @@ int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* E
   AFQMC_TRY(mark(3));
   // 3. vHS
   if (mixed) {
-    AFQMC_TRY(vhs_mixed(s, h->mixed, pr->X, pr->V, W, std::sqrt(dt)));
+    AFQMC_TRY(vhs_mixed(s, h->mixed, pr->X, nullptr, W, std::sqrt(dt)));
   } else {
     AFQMC_TRY(ham_vhs(h, s, pr->X, pr->V, W, dt));
   }
@@ -1091,8 +1103,8 @@ int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* E
                                  : (const void*)(pr->P1 + size_t(sp % pr->nspin_P1) * MM);
     const c128* V = pr->V + size_t(sp % pr->nspin_V) * W * MM;
     if (mixed) {
-      AFQMC_TRY(propagate_mixed(s, h->mixed, P1, pr->p1_real, V, MM, ws->buf + ws->offS(sp),
-                                ws->walker_size, W, M, Ns, pr->p.taylor_n, pr->w1, pr->w2, pr->w3));
+      AFQMC_TRY(propagate_mixed(s, h->mixed, P1, pr->p1_real, ws->buf + ws->offS(sp),
+                                ws->walker_size, W, M, Ns, pr->p.taylor_n));
     } else {
       AFQMC_TRY(propagate(s, P1, pr->p1_real, V, MM, ws->buf + ws->offS(sp), ws->walker_size, W, M,
                           Ns, pr->p.taylor_n, pr->w1, pr->w2, pr->w3));

@@ -10,6 +10,7 @@
 // Cholesky vectors sized by max_memory_MB; the complex128 path here materialises it in chunks of
 // walkers (one DMMA GEMM per chunk) and reduces each N x N block of T with one CTA.
 #include "energy.cuh"
+#include "mixed.cuh"
 #include "zgemm.cuh"
 
 namespace afqmc {
@@ -122,7 +123,8 @@ __global__ void init_energy_kernel(c128* E, int W, double E0, int addH1) {
 }  // namespace
 
 int energy_fp64(cudaStream_t s, const EnergyArgs& a, c128* E, int W, bool addH1, bool addEJ,
-                bool addEXX, c128* workT, long workT_elems, c128* exx_part, c128* Kl) {
+                bool addEXX, c128* workT, long workT_elems, c128* exx_part, c128* Kl,
+                MixedHam* tc) {
   if (W <= 0) return AFQMC_OK;
   init_energy_kernel<<<ceil_div(W, 128), 128, 0, s>>>(E, W, a.E0, addH1 ? 1 : 0);
   AFQMC_TRY(launch_status("init_energy_kernel"));
@@ -156,6 +158,12 @@ int energy_fp64(cudaStream_t s, const EnergyArgs& a, c128* E, int W, bool addH1,
       const int wc = (W - w0) < Wc ? (W - w0) : Wc;
       // T[(w,b)][(n,a)] = sum_k G[w,b,k] Lnak[n,a,k]; rows of G are strided by ldG per walker,
       // so one GEMM per walker in the chunk (batched, shared Lnak)
+      if (tc) {
+        AFQMC_TRY(exchange_T_tc(s, tc, sp, w0, wc, workT));
+        exchange_block_kernel<<<dim3(a.Nc, wc), 128, smem, s>>>(workT, Ns, a.Nc, w0, exx_part, Kl);
+        AFQMC_TRY(launch_status("exchange_block_kernel"));
+        continue;
+      }
       GemmParams p{};
       p.m = Ns; p.n = a.Nc * Ns; p.k = a.M;
       p.A = Gs + long(w0) * a.ldG; p.lda = a.M; p.strideA = a.ldG;

@@ -1,29 +1,728 @@
-// Mixed-precision contractions: not built yet in this revision; every entry reports
-// AFQMC_ERR_UNSUPPORTED so that a mixed request never silently runs another path.
+// Mixed-precision contractions of the walker step on the 5th-generation tensor cores.
+//
+// Every contraction is a (batched) complex GEMM run as real tcgen05.mma kind::tf32 products with
+// the 3xTF32 split x = hi + lo (hi = TF32(x), lo = TF32(x - hi)): a*b ~ ahi*bhi + ahi*blo + alo*bhi,
+// accumulated in FP32 in tensor memory.  Complex operands are kept as planes
+// {re_hi, re_lo, im_hi, im_lo}; the -Im(A)Im(B) term uses the MMA's A-negate bit.  Operand tiles
+// arrive by TMA (128-byte swizzle) in a 2-3 stage mbarrier pipeline: warp 0 issues the TMA loads,
+// one thread of warp 1 issues the MMAs, warps 2-5 drain the accumulators from TMEM and run the
+// epilogue of the calling contraction.  FP64 stays where the method needs it (overlap LU,
+// inverse, log-det, QR, weights, energy sums); see the per-function notes below for which
+// reference contraction each call replaces.
+#include <cudaTypedefs.h>
+
+#include <memory>
+#include <mutex>
+
+#include "detops.cuh"
+#include "energy.cuh"
 #include "mixed.cuh"
+#include "tc.cuh"
+#include "zgemm.cuh"
 
 namespace afqmc {
 
-struct MixedHam {
-  int dummy;
+namespace {
+
+constexpr int TC_THREADS = 192;  // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int BK = 32;           // K elements per stage (128 bytes of FP32 = one swizzle row)
+
+enum Epi : int {
+  EPI_C128 = 0,      // out_c[z][row][col] = alpha * acc                (complex128)
+  EPI_PLANES = 1,    // out planes [z][row][col] = split(alpha * acc)    (hi/lo re/im fp32)
+  EPI_TAYLOR = 2,    // out planes [z][col][row] = split(alpha*acc); acc planes [z][col][row] (+)=
+  EPI_S64 = 3,       // out_c[z][row][col] = alpha * acc (walker Slater matrix, FP64)
+  EPI_VHS = 4,       // out planes [z=0][row][ (col/M)*ldv + col%M ] = split(alpha * acc)
 };
 
-int mixed_ham_create(MixedHam** out, const EnergyArgs&, cudaStream_t) {
-  *out = nullptr;
-  set_error_detail("mixed precision path is not available in this build");
-  return AFQMC_ERR_UNSUPPORTED;
+struct TcParams {
+  CUtensorMap a[4];
+  CUtensorMap b[4];
+  int m, n, k;
+  int a_batched, b_batched;
+  c128 alpha;
+  float* out[4];        // split planes re_hi, re_lo, im_hi, im_lo
+  long out_ld, out_bs;  // leading dim / batch stride of the output planes (elements)
+  float* acc[2];        // Taylor running sum re, im  (EPI_TAYLOR)
+  int acc_init;         // 1: acc = value (first term), 0: acc += value
+  float* acc_split[4];  // optional split copy of the updated running sum (last Taylor term)
+  c128* out_c;
+  long outc_ld, outc_bs;
+  int vhs_M;            // EPI_VHS: columns are (i, k) pairs of an M x M matrix
+  unsigned* err;
+};
+
+template <bool A_CPLX, bool B_CPLX, int BN, int STAGES>
+struct TcCfg {
+  static constexpr int NA = A_CPLX ? 4 : 2;
+  static constexpr int NB = B_CPLX ? 4 : 2;
+  static constexpr int A_TILE = 128 * BK * 4;  // bytes per plane tile
+  static constexpr int B_TILE = BN * BK * 4;
+  static constexpr int STAGE = NA * A_TILE + NB * B_TILE;
+  static constexpr int TMEM_COLS = (2 * BN <= 32) ? 32 : (2 * BN <= 64) ? 64 : (2 * BN <= 128) ? 128
+                                   : (2 * BN <= 256) ? 256 : 512;
+  static constexpr size_t SMEM = size_t(STAGES) * STAGE + 1024 /*align*/ + 256 /*barriers*/;
+  static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N for M=128");
+  static_assert(SMEM <= 232448, "shared memory");
+};
+
+__device__ __forceinline__ void split_store(float v, float* hi, float* lo, long idx) {
+  const float h = tc::tf32_hi(v);
+  hi[idx] = h;
+  lo[idx] = v - h;
 }
+
+template <bool A_CPLX, bool B_CPLX, int BN, int STAGES, int EPI>
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_cgemm_kernel(const __grid_constant__ TcParams p) {
+  using K = TcCfg<A_CPLX, B_CPLX, BN, STAGES>;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1024-byte aligned stage buffers (128-byte swizzle atoms)
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * K::STAGE);
+  uint64_t* empty = full + STAGES;
+  uint64_t* accb = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accb + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * 128, n0 = blockIdx.y * BN, z = blockIdx.z;
+  const int nk = (p.k + BK - 1) / BK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+    }
+    tc::mbar_init(accb, 1);
+    *abort_flag = 0;
+    tc::fence_mbar_init();
+#pragma unroll
+    for (int q = 0; q < K::NA; ++q) tc::prefetch_tmap(&p.a[q]);
+#pragma unroll
+    for (int q = 0; q < K::NB; ++q) tc::prefetch_tmap(&p.b[q]);
+  }
+  if (warp == 1) {
+    tc::tmem_alloc(tmem_slot, K::TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t taddr = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      const int za = p.a_batched ? z : 0, zb = p.b_batched ? z : 0;
+      for (int kc = 0; kc < nk; ++kc) {
+        const int s = kc % STAGES;
+        if (kc >= STAGES) {
+          if (!tc::mbar_wait(&empty[s], ((kc / STAGES) - 1) & 1, p.err, abort_flag)) break;
+        }
+        unsigned char* st = base + size_t(s) * K::STAGE;
+        tc::mbar_arrive_expect_tx(&full[s], K::STAGE);
+#pragma unroll
+        for (int q = 0; q < K::NA; ++q)
+          tc::tma_load_3d(st + q * K::A_TILE, &p.a[q], &full[s], kc * BK, m0, za);
+#pragma unroll
+        for (int q = 0; q < K::NB; ++q)
+          tc::tma_load_3d(st + K::NA * K::A_TILE + q * K::B_TILE, &p.b[q], &full[s], kc * BK, n0,
+                          zb);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t ID = tc::idesc_tf32(128, BN, false);
+      constexpr uint32_t IDN = tc::idesc_tf32(128, BN, true);
+      const uint32_t dr = taddr, di = taddr + BN;
+      bool ok = true;
+      for (int kc = 0; kc < nk && ok; ++kc) {
+        const int s = kc % STAGES;
+        if (!tc::mbar_wait(&full[s], (kc / STAGES) & 1, p.err, abort_flag)) {
+          ok = false;
+          break;
+        }
+        tc::tc_fence_after();
+        unsigned char* st = base + size_t(s) * K::STAGE;
+        const uint32_t sa = tc::smem_u32(st);
+        const uint32_t sb = tc::smem_u32(st + K::NA * K::A_TILE);
+#pragma unroll
+        for (int kk = 0; kk < BK / 8; ++kk) {
+          // +32 bytes per K=8 step inside the 128-byte swizzle row (descriptor units of 16 B)
+          auto A = [&](int q) { return tc::sdesc_sw128(sa + q * K::A_TILE) + uint64_t(2 * kk); };
+          auto B = [&](int q) { return tc::sdesc_sw128(sb + q * K::B_TILE) + uint64_t(2 * kk); };
+          const uint32_t acc0 = (kc > 0 || kk > 0) ? 1u : 0u;
+          if constexpr (A_CPLX && B_CPLX) {
+            // Dr = Ar Br - Ai Bi ; Di = Ar Bi + Ai Br   (planes 0 re_hi, 1 re_lo, 2 im_hi, 3 im_lo)
+            tc::mma_tf32(dr, A(0), B(0), ID, acc0);
+            tc::mma_tf32(dr, A(0), B(1), ID, 1);
+            tc::mma_tf32(dr, A(1), B(0), ID, 1);
+            tc::mma_tf32(dr, A(2), B(2), IDN, 1);
+            tc::mma_tf32(dr, A(2), B(3), IDN, 1);
+            tc::mma_tf32(dr, A(3), B(2), IDN, 1);
+            tc::mma_tf32(di, A(0), B(2), ID, acc0);
+            tc::mma_tf32(di, A(0), B(3), ID, 1);
+            tc::mma_tf32(di, A(1), B(2), ID, 1);
+            tc::mma_tf32(di, A(2), B(0), ID, 1);
+            tc::mma_tf32(di, A(2), B(1), ID, 1);
+            tc::mma_tf32(di, A(3), B(0), ID, 1);
+          } else if constexpr (A_CPLX) {
+            // real B (planes 0 hi, 1 lo)
+            tc::mma_tf32(dr, A(0), B(0), ID, acc0);
+            tc::mma_tf32(dr, A(0), B(1), ID, 1);
+            tc::mma_tf32(dr, A(1), B(0), ID, 1);
+            tc::mma_tf32(di, A(2), B(0), ID, acc0);
+            tc::mma_tf32(di, A(2), B(1), ID, 1);
+            tc::mma_tf32(di, A(3), B(0), ID, 1);
+          } else {
+            // real A, complex B
+            tc::mma_tf32(dr, A(0), B(0), ID, acc0);
+            tc::mma_tf32(dr, A(0), B(1), ID, 1);
+            tc::mma_tf32(dr, A(1), B(0), ID, 1);
+            tc::mma_tf32(di, A(0), B(2), ID, acc0);
+            tc::mma_tf32(di, A(0), B(3), ID, 1);
+            tc::mma_tf32(di, A(1), B(2), ID, 1);
+          }
+        }
+        tc::mma_commit(&empty[s]);  // stage reusable once these MMAs have read it
+      }
+      tc::mma_commit(accb);  // accumulators complete (also on an aborted run: nothing in flight)
+    }
+  } else {
+    // epilogue warps 2..5: TMEM lane quarter = warp % 4
+    const int q = warp & 3;
+    const bool ok = tc::mbar_wait(accb, 0, p.err, abort_flag);
+    tc::tc_fence_after();
+    if (ok) {
+      const int row = m0 + q * 32 + lane;
+      const uint32_t trow = taddr + (uint32_t(q * 32) << 16);
+#pragma unroll 1
+      for (int c0 = 0; c0 < BN; c0 += 16) {
+        float vr[16], vi[16];
+        tc::tmem_ld16(trow + c0, vr);
+        tc::tmem_ld16(trow + BN + c0, vi);
+        tc::tmem_ld_wait();
+        if (row >= p.m) continue;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = n0 + c0 + j;
+          if (col >= p.n) break;
+          // alpha * (vr + i vi)
+          const float ar = float(p.alpha.x), ai = float(p.alpha.y);
+          const float xr = ar * vr[j] - ai * vi[j];
+          const float xi = ar * vi[j] + ai * vr[j];
+          if constexpr (EPI == EPI_C128 || EPI == EPI_S64) {
+            const double dr = p.alpha.x * double(vr[j]) - p.alpha.y * double(vi[j]);
+            const double di = p.alpha.x * double(vi[j]) + p.alpha.y * double(vr[j]);
+            p.out_c[long(z) * p.outc_bs + long(row) * p.outc_ld + col] = cmk(dr, di);
+          } else if constexpr (EPI == EPI_PLANES) {
+            const long idx = long(z) * p.out_bs + long(row) * p.out_ld + col;
+            split_store(xr, p.out[0], p.out[1], idx);
+            split_store(xi, p.out[2], p.out[3], idx);
+          } else if constexpr (EPI == EPI_VHS) {
+            const int i = col / p.vhs_M, kq = col - i * p.vhs_M;
+            const long idx = long(row) * p.out_bs + long(i) * p.out_ld + kq;
+            split_store(xr, p.out[0], p.out[1], idx);
+            split_store(xi, p.out[2], p.out[3], idx);
+          } else if constexpr (EPI == EPI_TAYLOR) {
+            // transposed store: [z][col][row]
+            const long idx = long(z) * p.out_bs + long(col) * p.out_ld + row;
+            split_store(xr, p.out[0], p.out[1], idx);
+            split_store(xi, p.out[2], p.out[3], idx);
+            float sr = xr, si = xi;
+            if (!p.acc_init) {
+              sr += p.acc[0][idx];
+              si += p.acc[1][idx];
+            }
+            p.acc[0][idx] = sr;
+            p.acc[1][idx] = si;
+            if (p.acc_split[0]) {
+              split_store(sr, p.acc_split[0], p.acc_split[1], idx);
+              split_store(si, p.acc_split[2], p.acc_split[3], idx);
+            }
+          }
+        }
+      }
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 1) tc::tmem_dealloc(taddr, K::TMEM_COLS);
+}
+
+// ---------------------------------------------------------------------------------------------
+// host: tensor maps
+// ---------------------------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// 3D map over an FP32 plane [batch][rows][ld] (inner extent k), box {32, box_rows, 1},
+// 128-byte swizzle, zero fill outside the tensor.
+int make_map(CUtensorMap* map, const float* base, long k, long rows, long ld, long batch,
+             long batch_stride, int box_rows) {
+  auto fn = encode_fn();
+  if (!fn) {
+    set_error_detail("cuTensorMapEncodeTiled is not available");
+    return AFQMC_ERR_CUDA;
+  }
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld * 4) % 16 || (batch_stride * 4) % 16) {
+    set_error_detail("make_map: plane not 16-byte aligned (ld=%ld, batch stride=%ld)", ld,
+                     batch_stride);
+    return AFQMC_ERR_SHAPE;
+  }
+  if (batch == 1) batch_stride = rows * ld;
+  cuuint64_t dims[3] = {cuuint64_t(k), cuuint64_t(rows), cuuint64_t(batch)};
+  cuuint64_t strides[2] = {cuuint64_t(ld * 4), cuuint64_t(batch_stride * 4)};
+  cuuint32_t box[3] = {cuuint32_t(BK), cuuint32_t(box_rows), 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error_detail("cuTensorMapEncodeTiled failed (%d): k=%ld rows=%ld ld=%ld batch=%ld box=%d",
+                     int(r), k, rows, ld, batch, box_rows);
+    return AFQMC_ERR_CUDA;
+  }
+  return AFQMC_OK;
+}
+
+// FP32 planes of one operand: 4 (complex) or 2 (real) arrays [batch][rows][ld]
+struct Planes {
+  float* p[4] = {nullptr, nullptr, nullptr, nullptr};
+  int nplanes = 0;
+  long rows = 0, ld = 0, batch = 0, k = 0;
+  long bstride() const { return rows * ld; }
+  size_t elems() const { return size_t(batch) * rows * ld; }
+};
+
+int alloc_planes(Planes& P, int nplanes, long batch, long rows, long k) {
+  P.nplanes = nplanes;
+  P.batch = batch;
+  P.rows = rows;
+  P.k = k;
+  P.ld = (k + 3) / 4 * 4;
+  for (int q = 0; q < nplanes; ++q) {
+    cudaError_t e = cudaMalloc(&P.p[q], sizeof(float) * P.elems());
+    if (e != cudaSuccess) {
+      set_error_detail("alloc_planes: %s", cudaGetErrorString(e));
+      return AFQMC_ERR_ALLOC;
+    }
+    AFQMC_CUDA_TRY(cudaMemset(P.p[q], 0, sizeof(float) * P.elems()));
+  }
+  return AFQMC_OK;
+}
+
+void free_planes(Planes& P) {
+  for (auto& q : P.p)
+    if (q) {
+      cudaFree(q);
+      q = nullptr;
+    }
+}
+
+int maps_for(const Planes& P, CUtensorMap* maps, int box_rows, long batch_override = -1) {
+  const long batch = batch_override > 0 ? batch_override : P.batch;
+  for (int q = 0; q < P.nplanes; ++q)
+    AFQMC_TRY(make_map(&maps[q], P.p[q], P.k, P.rows, P.ld, batch, P.bstride(), box_rows));
+  return AFQMC_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// conversions FP64 -> split FP32 planes
+// ---------------------------------------------------------------------------------------------
+// complex src [b][r][c] (ld_src, bstride_src) -> planes [b][r][c] or transposed [b][c][r]
+template <bool TRANSPOSE>
+__global__ void split_complex_kernel(const c128* __restrict__ src, long ld_src, long bs_src,
+                                     int rows, int cols, float* __restrict__ rh,
+                                     float* __restrict__ rl, float* __restrict__ ih,
+                                     float* __restrict__ il, long ld_dst, long bs_dst) {
+  const long b = blockIdx.z;
+  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows || c >= cols) return;
+  const c128 v = src[b * bs_src + long(r) * ld_src + c];
+  const long d = TRANSPOSE ? b * bs_dst + long(c) * ld_dst + r : b * bs_dst + long(r) * ld_dst + c;
+  split_store(float(v.x), rh, rl, d);
+  split_store(float(v.y), ih, il, d);
+}
+
+__global__ void split_real_kernel(const double* __restrict__ src, long n_rows, long cols,
+                                  long ld_src, float* __restrict__ h, float* __restrict__ l,
+                                  long ld_dst) {
+  const long e = blockIdx.x * long(blockDim.x) + threadIdx.x;
+  if (e >= n_rows * cols) return;
+  const long r = e / cols, c = e % cols;
+  split_store(float(src[r * ld_src + c]), h, l, r * ld_dst + c);
+}
+
+int split_complex(cudaStream_t s, const c128* src, long ld_src, long bs_src, int batch, int rows,
+                  int cols, Planes& P, bool transpose) {
+  dim3 blk(32, 8);
+  if (transpose) {
+    // coalesce the writes along the destination's contiguous (row) index
+    dim3 grid(ceil_div(cols, 32), ceil_div(rows, 8), batch);
+    split_complex_kernel<true><<<grid, blk, 0, s>>>(src, ld_src, bs_src, rows, cols, P.p[0],
+                                                    P.p[1], P.p[2], P.p[3], P.ld, P.bstride());
+  } else {
+    dim3 grid(ceil_div(cols, 32), ceil_div(rows, 8), batch);
+    split_complex_kernel<false><<<grid, blk, 0, s>>>(src, ld_src, bs_src, rows, cols, P.p[0],
+                                                     P.p[1], P.p[2], P.p[3], P.ld, P.bstride());
+  }
+  return launch_status("split_complex_kernel");
+}
+
+int split_real_host(const double* src_dev, long rows, long cols, long ld_src, Planes& P) {
+  const long n = rows * cols;
+  split_real_kernel<<<ceil_div(n, 256), 256>>>(src_dev, rows, cols, ld_src, P.p[0], P.p[1], P.ld);
+  AFQMC_TRY(launch_status("split_real_kernel"));
+  AFQMC_CUDA_TRY(cudaDeviceSynchronize());
+  return AFQMC_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// launcher
+// ---------------------------------------------------------------------------------------------
+template <bool A_CPLX, bool B_CPLX, int BN, int STAGES, int EPI>
+int launch_tc(cudaStream_t s, TcParams& p, int batch) {
+  using K = TcCfg<A_CPLX, B_CPLX, BN, STAGES>;
+  auto kern = tc_cgemm_kernel<A_CPLX, B_CPLX, BN, STAGES, EPI>;
+  AFQMC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(K::SMEM)));
+  if (batch > 65535) {
+    set_error_detail("launch_tc: batch %d exceeds the grid limit", batch);
+    return AFQMC_ERR_SHAPE;
+  }
+  dim3 grid(ceil_div(p.m, 128), ceil_div(p.n, BN), batch);
+  kern<<<grid, TC_THREADS, K::SMEM, s>>>(p);
+  return launch_status("tc_cgemm_kernel");
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// Mixed Hamiltonian: split-TF32 copies of the static tensors
+// ---------------------------------------------------------------------------------------------
+struct MixedHam {
+  int M, Nc, nspin, nel[2], el_off[2], nel_tot;
+  bool lnak_cplx;
+  Planes Likn[2];   // [1][M*M][Nc]  (B of vHS, K = Nc)
+  Planes Lnak[2];   // [1][Nc][nel*M] (B of vbias, K = nel*M); same memory viewed [Nc*nel][M] for exchange
+  // dynamic operands, sized on demand
+  int capW = 0;
+  Planes G;         // [W][1][nel_tot*M]  (A of vbias);  exchange view [W*nel][M]
+  Planes X;         // [1][W][Nc] (A of vHS)
+  unsigned* err = nullptr;
+  // propagation buffers
+  int capP = 0;
+  Planes P1;        // [1][M][M] real (A of the P1 products)
+  const void* P1_src = nullptr;
+  Planes V;         // [W][M][M] complex (A of the Taylor products)
+  Planes T0, T1, Tacc_split, Sst;  // [W][N][M] complex (B operands)
+  float* acc[2] = {nullptr, nullptr};  // running Taylor sum [W][N][M]
+  ~MixedHam() {
+    for (int s = 0; s < 2; ++s) {
+      free_planes(Likn[s]);
+      free_planes(Lnak[s]);
+    }
+    free_planes(G);
+    free_planes(X);
+    free_planes(P1);
+    free_planes(V);
+    free_planes(T0);
+    free_planes(T1);
+    free_planes(Tacc_split);
+    free_planes(Sst);
+    for (auto& a : acc)
+      if (a) cudaFree(a);
+    if (err) cudaFree(err);
+  }
+};
+
 void mixed_ham_destroy(MixedHam* m) { delete m; }
-int vbias_mixed(cudaStream_t, MixedHam*, const c128*, long, c128*, int, double) {
-  return AFQMC_ERR_UNSUPPORTED;
+
+int mixed_ham_create(MixedHam** out, const EnergyArgs& a, cudaStream_t s) {
+  *out = nullptr;
+  if (a.M % 4 || a.Nc % 4) {
+    set_error_detail("mixed precision needs M and Nc multiples of 4 (M=%d, Nc=%d)", a.M, a.Nc);
+    return AFQMC_ERR_UNSUPPORTED;
+  }
+  if (!a.Likn) {
+    set_error_detail("mixed_ham_create: missing Likn");
+    return AFQMC_ERR_ARG;
+  }
+  std::unique_ptr<MixedHam> m(new MixedHam());
+  m->M = a.M;
+  m->Nc = a.Nc;
+  m->nspin = a.nspin;
+  m->nel_tot = 0;
+  for (int s2 = 0; s2 < 2; ++s2) {
+    m->nel[s2] = a.nel[s2];
+    m->el_off[s2] = a.el_off[s2];
+    m->nel_tot += (s2 < a.nspin) ? a.nel[s2] : 0;
+  }
+  m->lnak_cplx = (a.Lnak_real[0] == nullptr);
+  const long MM = long(a.M) * a.M;
+  AFQMC_CUDA_TRY(cudaStreamSynchronize(s));
+  for (int sp = 0; sp < a.nspin_H2; ++sp) {
+    AFQMC_TRY(alloc_planes(m->Likn[sp], 2, 1, MM, a.Nc));
+    AFQMC_TRY(split_real_host(a.Likn + size_t(sp) * MM * a.Nc, MM, a.Nc, a.Nc, m->Likn[sp]));
+  }
+  for (int sp = 0; sp < a.nspin; ++sp) {
+    const int Ns = a.nel[sp];
+    if (Ns == 0) continue;
+    const long K = long(Ns) * a.M;
+    if (m->lnak_cplx) {
+      AFQMC_TRY(alloc_planes(m->Lnak[sp], 4, 1, a.Nc, K));
+      AFQMC_TRY(split_complex(nullptr, a.Lnak[sp], K, 0, 1, a.Nc, int(K), m->Lnak[sp], false));
+    } else {
+      AFQMC_TRY(alloc_planes(m->Lnak[sp], 2, 1, a.Nc, K));
+      AFQMC_TRY(split_real_host(a.Lnak_real[sp], a.Nc, K, K, m->Lnak[sp]));
+    }
+  }
+  AFQMC_CUDA_TRY(cudaMalloc(&m->err, sizeof(unsigned)));
+  AFQMC_CUDA_TRY(cudaMemset(m->err, 0, sizeof(unsigned)));
+  AFQMC_CUDA_TRY(cudaDeviceSynchronize());
+  *out = m.release();
+  return AFQMC_OK;
 }
-int vhs_mixed(cudaStream_t, MixedHam*, const c128*, c128*, int, double) { return AFQMC_ERR_UNSUPPORTED; }
-int propagate_mixed(cudaStream_t, MixedHam*, const void*, bool, const c128*, long, c128*, long, int,
-                    int, int, int, c128*, c128*, c128*) {
-  return AFQMC_ERR_UNSUPPORTED;
+
+namespace {
+
+int ensure_walker_buffers(MixedHam* m, int W) {
+  if (m->capW >= W) return AFQMC_OK;
+  AFQMC_CUDA_TRY(cudaDeviceSynchronize());
+  free_planes(m->G);
+  free_planes(m->X);
+  AFQMC_TRY(alloc_planes(m->G, 4, 1, W, long(m->nel_tot) * m->M));
+  AFQMC_TRY(alloc_planes(m->X, 4, 1, W, m->Nc));
+  m->capW = W;
+  return AFQMC_OK;
 }
-int energy_mixed(cudaStream_t, MixedHam*, const EnergyArgs&, c128*, int, bool, bool, bool) {
-  return AFQMC_ERR_UNSUPPORTED;
+
+}  // namespace
+
+// vbias = a * G Lnak^T (Real3IndexFactorization.hpp:384): A = G planes [W][nel*M], B = Lnak
+// [Nc][nel*M] (per spin block: the K range of the spin's rows of G).
+int vbias_mixed(cudaStream_t s, MixedHam* m, const c128* G, long ldG, c128* v, int W, double a) {
+  if (m->nspin > 1) {
+    set_error_detail("vbias_mixed: COLLINEAR walkers are not supported in mixed precision");
+    return AFQMC_ERR_UNSUPPORTED;
+  }
+  AFQMC_TRY(ensure_walker_buffers(m, W));
+  const long Kt = long(m->nel_tot) * m->M;
+  AFQMC_TRY(split_complex(s, G, ldG, 0, 1, W, int(Kt), m->G, false));
+  bool first = true;
+  for (int sp = 0; sp < m->nspin; ++sp) {
+    const int Ns = m->nel[sp];
+    if (Ns == 0) continue;
+    const long K = long(Ns) * m->M;
+    const long off = long(m->el_off[sp]) * m->M;
+    TcParams p{};
+    for (int q = 0; q < 4; ++q)
+      AFQMC_TRY(make_map(&p.a[q], m->G.p[q] + off, K, W, m->G.ld, 1, long(W) * m->G.ld, 128));
+    AFQMC_TRY(maps_for(m->Lnak[sp], p.b, m->lnak_cplx ? 64 : 128));
+    p.m = W; p.n = m->Nc; p.k = int(K);
+    p.alpha = cmk(a, 0);
+    p.out_c = v; p.outc_ld = m->Nc; p.outc_bs = 0;
+    p.err = m->err;
+    if (m->lnak_cplx)
+      AFQMC_TRY((launch_tc<true, true, 64, 2, EPI_C128>(s, p, 1)));
+    else
+      AFQMC_TRY((launch_tc<true, false, 128, 2, EPI_C128>(s, p, 1)));
+    first = false;
+  }
+  return AFQMC_OK;
+}
+
+// vHS = a * X L^T (Real3IndexFactorization.hpp:321) written as split planes V[w][i][k]; the
+// propagation reads them as its A operand.  When V is a complex128 output (the C-ABI call
+// afqmc_ham_vhs) the planes are re-assembled into V afterwards.
+namespace {
+__global__ void planes_to_c128_kernel(const float* __restrict__ rh, const float* __restrict__ rl,
+                                      const float* __restrict__ ih, const float* __restrict__ il,
+                                      long n, c128* __restrict__ out) {
+  long e = blockIdx.x * long(blockDim.x) + threadIdx.x;
+  if (e < n) out[e] = cmk(double(rh[e]) + double(rl[e]), double(ih[e]) + double(il[e]));
+}
+
+int ensure_v_buffers(MixedHam* m, int W) {
+  if (m->V.batch >= W) return AFQMC_OK;
+  AFQMC_CUDA_TRY(cudaDeviceSynchronize());
+  free_planes(m->V);
+  return alloc_planes(m->V, 4, W, m->M, m->M);
+}
+
+int ensure_prop_buffers(MixedHam* m, int W, int N) {
+  if (m->capP >= W && m->T0.rows == N) return AFQMC_OK;
+  AFQMC_CUDA_TRY(cudaDeviceSynchronize());
+  free_planes(m->T0);
+  free_planes(m->T1);
+  free_planes(m->Tacc_split);
+  free_planes(m->Sst);
+  for (auto& a : m->acc)
+    if (a) {
+      cudaFree(a);
+      a = nullptr;
+    }
+  const int M = m->M;
+  AFQMC_TRY(alloc_planes(m->T0, 4, W, N, M));
+  AFQMC_TRY(alloc_planes(m->T1, 4, W, N, M));
+  AFQMC_TRY(alloc_planes(m->Tacc_split, 4, W, N, M));
+  AFQMC_TRY(alloc_planes(m->Sst, 4, W, N, M));
+  for (auto& a : m->acc) {
+    AFQMC_CUDA_TRY(cudaMalloc(&a, sizeof(float) * m->T0.elems()));
+    AFQMC_CUDA_TRY(cudaMemset(a, 0, sizeof(float) * m->T0.elems()));
+  }
+  m->capP = W;
+  return AFQMC_OK;
+}
+}  // namespace
+
+int vhs_planes(cudaStream_t s, MixedHam* m, const c128* X, int W, double a) {
+  AFQMC_TRY(ensure_walker_buffers(m, W));
+  AFQMC_TRY(ensure_v_buffers(m, W));
+  AFQMC_TRY(split_complex(s, X, m->Nc, 0, 1, W, m->Nc, m->X, false));
+  TcParams p{};
+  AFQMC_TRY(maps_for(m->X, p.a, 128));
+  AFQMC_TRY(maps_for(m->Likn[0], p.b, 128));
+  const long MM = long(m->M) * m->M;
+  p.m = W; p.n = int(MM); p.k = m->Nc;
+  p.alpha = cmk(a, 0);
+  for (int q = 0; q < 4; ++q) p.out[q] = m->V.p[q];
+  p.out_ld = m->V.ld;
+  p.out_bs = m->V.bstride();
+  p.vhs_M = m->M;
+  p.err = m->err;
+  return launch_tc<true, false, 128, 2, EPI_VHS>(s, p, 1);
+}
+
+int vhs_mixed(cudaStream_t s, MixedHam* m, const c128* X, c128* V, int W, double a) {
+  if (m->nspin > 1 && m->Likn[1].p[0]) {
+    set_error_detail("vhs_mixed: spin-dependent Cholesky vectors are not supported");
+    return AFQMC_ERR_UNSUPPORTED;
+  }
+  AFQMC_TRY(vhs_planes(s, m, X, W, a));
+  if (V) {
+    const long n = long(W) * m->M * m->M;
+    if (m->V.ld != m->M) {
+      set_error_detail("vhs_mixed: padded V planes cannot be copied out");
+      return AFQMC_ERR_UNSUPPORTED;
+    }
+    planes_to_c128_kernel<<<ceil_div(n, 256), 256, 0, s>>>(m->V.p[0], m->V.p[1], m->V.p[2],
+                                                           m->V.p[3], n, V);
+    AFQMC_TRY(launch_status("planes_to_c128_kernel"));
+  }
+  return AFQMC_OK;
+}
+
+// Taylor propagation S <- P1 sum_n (iV)^n/n! P1 S (propagate.hpp:238-298) on the split planes.
+// V must have been produced by vhs_mixed (planes kept in MixedHam) for the same walkers.
+int propagate_mixed(cudaStream_t s, MixedHam* m, const void* P1, bool p1_real, c128* S, long ldS,
+                    int W, int M, int N, int order) {
+  if (!p1_real) {
+    set_error_detail("propagate_mixed: a complex one-body propagator is not supported");
+    return AFQMC_ERR_UNSUPPORTED;
+  }
+  if (m->V.batch < W) {
+    set_error_detail("propagate_mixed: no vHS planes for %d walkers (call vhs_mixed first)", W);
+    return AFQMC_ERR_ARG;
+  }
+  AFQMC_TRY(ensure_prop_buffers(m, W, N));
+  if (m->P1_src != P1) {
+    free_planes(m->P1);
+    AFQMC_TRY(alloc_planes(m->P1, 2, 1, M, M));
+    AFQMC_TRY(split_real_host(static_cast<const double*>(P1), M, M, M, m->P1));
+    m->P1_src = P1;
+  }
+  // S^T planes [W][N][M] from the walkers' Slater matrices [W][M][N]
+  AFQMC_TRY(split_complex(s, S, N, ldS, W, M, N, m->Sst, true));
+  Planes* Tin = &m->T0;
+  Planes* Tout = &m->T1;
+  // T0 = P1 S  (acc = T0)
+  {
+    TcParams p{};
+    AFQMC_TRY(maps_for(m->P1, p.a, 128));
+    AFQMC_TRY(maps_for(m->Sst, p.b, 64, W));
+    p.m = M; p.n = N; p.k = M; p.a_batched = 0; p.b_batched = 1;
+    p.alpha = cmk(1, 0);
+    for (int q = 0; q < 4; ++q) p.out[q] = Tin->p[q];
+    p.out_ld = Tin->ld; p.out_bs = Tin->bstride();
+    p.acc[0] = m->acc[0]; p.acc[1] = m->acc[1]; p.acc_init = 1;
+    if (order == 0)
+      for (int q = 0; q < 4; ++q) p.acc_split[q] = m->Tacc_split.p[q];
+    p.err = m->err;
+    AFQMC_TRY((launch_tc<false, true, 64, 3, EPI_TAYLOR>(s, p, W)));
+  }
+  for (int n = 1; n <= order; ++n) {
+    TcParams p{};
+    AFQMC_TRY(maps_for(m->V, p.a, 128, W));
+    AFQMC_TRY(maps_for(*Tin, p.b, 64, W));
+    p.m = M; p.n = N; p.k = M; p.a_batched = 1; p.b_batched = 1;
+    p.alpha = cmk(0.0, 1.0 / double(n));
+    for (int q = 0; q < 4; ++q) p.out[q] = Tout->p[q];
+    p.out_ld = Tout->ld; p.out_bs = Tout->bstride();
+    p.acc[0] = m->acc[0]; p.acc[1] = m->acc[1]; p.acc_init = 0;
+    if (n == order)
+      for (int q = 0; q < 4; ++q) p.acc_split[q] = m->Tacc_split.p[q];
+    p.err = m->err;
+    AFQMC_TRY((launch_tc<true, true, 64, 2, EPI_TAYLOR>(s, p, W)));
+    std::swap(Tin, Tout);
+  }
+  // S = P1 * TMN
+  {
+    TcParams p{};
+    AFQMC_TRY(maps_for(m->P1, p.a, 128));
+    AFQMC_TRY(maps_for(m->Tacc_split, p.b, 64, W));
+    p.m = M; p.n = N; p.k = M; p.a_batched = 0; p.b_batched = 1;
+    p.alpha = cmk(1, 0);
+    p.out_c = S; p.outc_ld = N; p.outc_bs = ldS;
+    p.err = m->err;
+    AFQMC_TRY((launch_tc<false, true, 64, 3, EPI_S64>(s, p, W)));
+  }
+  return AFQMC_OK;
+}
+
+int mixed_prepare_G(cudaStream_t s, MixedHam* m, const c128* G, long ldG, int W) {
+  AFQMC_TRY(ensure_walker_buffers(m, W));
+  const long Kt = long(m->nel_tot) * m->M;
+  return split_complex(s, G, ldG, 0, 1, W, int(Kt), m->G, false);
+}
+
+// T chunk GEMM for the exchange energy (called from energy.cu's chunk loop through energy_tc)
+int exchange_T_tc(cudaStream_t s, MixedHam* m, int sp, int w0, int wc, c128* workT) {
+  const int Ns = m->nel[sp];
+  const long off = long(m->el_off[sp]) * m->M;
+  TcParams p{};
+  // A: rows (w, b) of G for walkers [w0, w0+wc): plane rows of nel_tot*M, spin block at off
+  for (int q = 0; q < 4; ++q)
+    AFQMC_TRY(make_map(&p.a[q], m->G.p[q] + long(w0) * m->G.ld + off, m->M, Ns, m->M, wc,
+                       m->G.ld, 128));
+  // B: Lnak viewed as [Nc*Ns][M]
+  for (int q = 0; q < m->Lnak[sp].nplanes; ++q)
+    AFQMC_TRY(make_map(&p.b[q], m->Lnak[sp].p[q], m->M, long(m->Nc) * Ns, m->M, 1, 0,
+                       m->lnak_cplx ? 64 : 128));
+  p.m = Ns; p.n = m->Nc * Ns; p.k = m->M; p.a_batched = 1; p.b_batched = 0;
+  p.alpha = cmk(1, 0);
+  p.out_c = workT; p.outc_ld = long(m->Nc) * Ns; p.outc_bs = long(Ns) * m->Nc * Ns;
+  p.err = m->err;
+  if (m->lnak_cplx) return launch_tc<true, true, 64, 2, EPI_C128>(s, p, wc);
+  return launch_tc<true, false, 128, 2, EPI_C128>(s, p, wc);
+}
+
+int mixed_error_flag(MixedHam* m, unsigned* flag) {
+  AFQMC_CUDA_TRY(cudaMemcpy(flag, m->err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  return AFQMC_OK;
 }
 
 }  // namespace afqmc

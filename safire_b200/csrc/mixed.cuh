@@ -6,16 +6,23 @@
 
 namespace afqmc {
 
-struct MixedHam;  // tensor-core copies of the Hamiltonian tensors
+struct MixedHam;  // split-TF32 copies of the Hamiltonian tensors + operand planes
 
 int mixed_ham_create(MixedHam** out, const EnergyArgs& a, cudaStream_t s);
 void mixed_ham_destroy(MixedHam* m);
+// v [W][Nc] (complex128) = a * G Lnak^T
 int vbias_mixed(cudaStream_t s, MixedHam* m, const c128* G, long ldG, c128* v, int W, double a);
+// split planes of a * X L^T kept in m; V != nullptr also receives them as complex128 [W][M][M]
 int vhs_mixed(cudaStream_t s, MixedHam* m, const c128* X, c128* V, int W, double a);
-int propagate_mixed(cudaStream_t s, MixedHam* m, const void* P1, bool p1_real, const c128* V,
-                    long strideV, c128* S, long ldS, int W, int M, int N, int order, c128* w1,
-                    c128* w2, c128* w3);
-int energy_mixed(cudaStream_t s, MixedHam* m, const EnergyArgs& a, c128* E, int W, bool addH1,
-                 bool addEJ, bool addEXX);
+// S <- P1 exp_T(iV) P1 S with V from the last vhs_mixed call (P1 real float64 [M][M])
+int propagate_mixed(cudaStream_t s, MixedHam* m, const void* P1, bool p1_real, c128* S, long ldS,
+                    int W, int M, int N, int order);
+// split planes of G for the exchange-energy GEMMs
+int mixed_prepare_G(cudaStream_t s, MixedHam* m, const c128* G, long ldG, int W);
+// T [(w,b)][(n,a)] for walkers [w0, w0+wc) of spin block sp (complex128, the chunk layout of
+// energy_fp64)
+int exchange_T_tc(cudaStream_t s, MixedHam* m, int sp, int w0, int wc, c128* workT);
+// first device-side wait timeout reported by the tensor-core kernels (0 = none)
+int mixed_error_flag(MixedHam* m, unsigned* flag);
 
 }  // namespace afqmc

@@ -1,0 +1,102 @@
+"""Mixed-precision (3xTF32 tcgen05) contractions vs the FP64 oracle.
+
+Tolerances: the 3xTF32 split keeps about 21 significant bits per operand and FP32 accumulation;
+the relative (infinity-norm) errors allowed here are 2e-5 for single contractions and 1e-4 for a
+full propagation step (several chained products)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import afqmc as O
+from safire_b200.synth import make_workload
+from tests.gpu_helpers import make_pair, rand_c, rel_err, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+TOL_ONE = 2e-5
+TOL_STEP = 1e-4
+
+
+@pytest.fixture(scope="module", params=[("cfg1", 128), ("cfg1", 40)])
+def case(request, cuda):
+    name, W = request.param
+    wl = make_workload(name, W=W)
+    dham, oham, owfn = make_pair(wl)
+    return wl, dham, oham, owfn
+
+
+def test_vbias_mixed(case):
+    from safire_b200 import afqmc as A
+    wl, dham, oham, _ = case
+    rs = np.random.default_rng(1)
+    G = rand_c(rs, wl.W, wl.nup * wl.M, scale=0.3)
+    v = torch.zeros((wl.W, wl.Nc), dtype=torch.complex128, device="cuda")
+    dham.vbias(to_dev(G), v, wl.dt, precision=A.PREC_MIXED)
+    err = rel_err(to_host(v), oham.vbias(G, wl.dt))
+    print(f"vbias mixed rel err {err:.2e}")
+    assert err < TOL_ONE
+
+
+def test_vhs_mixed(case):
+    from safire_b200 import afqmc as A
+    wl, dham, oham, _ = case
+    rs = np.random.default_rng(2)
+    X = rand_c(rs, wl.W, wl.Nc)
+    V = dham.vHS(to_dev(X), wl.dt, precision=A.PREC_MIXED)
+    err = rel_err(to_host(V), oham.vHS(X, wl.dt))
+    print(f"vHS mixed rel err {err:.2e}")
+    assert err < TOL_ONE
+
+
+def test_energy_mixed(case):
+    from safire_b200 import afqmc as A
+    wl, dham, oham, _ = case
+    rs = np.random.default_rng(3)
+    G = rand_c(rs, wl.W, wl.nup * wl.M, scale=0.2)
+    E = torch.zeros((wl.W, 3), dtype=torch.complex128, device="cuda")
+    dham.energy(E, to_dev(G), precision=A.PREC_MIXED)
+    Eo = oham.energy(G)
+    Ed = to_host(E)
+    errs = [rel_err(Ed[:, q], Eo[:, q]) for q in range(3)]
+    print("energy mixed rel errs E1/EXX/EJ", ["%.2e" % e for e in errs])
+    assert errs[0] < 1e-12  # E1 stays FP64
+    assert max(errs[1:]) < TOL_ONE
+
+
+def test_step_mixed_vs_fp64(case):
+    """One propagation step, same uniforms, FP64 vs mixed: walkers, overlaps, weights."""
+    from safire_b200 import afqmc as A
+    wl, dham, oham, owfn = case
+    W = wl.W
+    res = {}
+    for prec in (A.PREC_FP64, A.PREC_MIXED):
+        ws = A.WalkerSet(wl.walker_type, wl.M, wl.nup, wl.ndn, W)
+        ws.init_from_trial(dham)
+        wfn = A.NOMSD(dham)
+        wfn.Energy(ws, set_properties=True)
+        torch.cuda.synchronize()
+        e = sum(ws.getProperty(p) for p in (A.capi.E1, A.capi.EXX, A.capi.EJ))
+        ws.setProperty(A.capi.PSEUDO_ELOC, e)
+        prop = A.Propagator(dham, A.default_params(dt=wl.dt, precision=prec), W)
+        u = O.HostRandomGenerator(O.split_seed(0, 0, 1)).sample_uniform(W * wl.Nc)
+        ud = to_dev(u.reshape(W, wl.Nc), torch.float64)
+        for _ in range(3):
+            prop.Propagate(ws, -30.0, ud)
+        torch.cuda.synchronize()
+        res[prec] = (to_host(ws.SlaterMatrices(0)), to_host(ws.properties()))
+    S64, p64 = res[A.PREC_FP64]
+    Smx, pmx = res[A.PREC_MIXED]
+    eS = rel_err(Smx, S64)
+    eO = rel_err(pmx[:, O.OVLP], p64[:, O.OVLP])
+    eW = rel_err(pmx[:, O.WEIGHT], p64[:, O.WEIGHT])
+    print(f"3 steps mixed vs fp64: S {eS:.2e} ovlp {eO:.2e} weight {eW:.2e}")
+    assert eS < TOL_STEP and eO < TOL_STEP and eW < TOL_STEP
+
+
+def test_mixed_no_device_timeout(case):
+    """The tensor-core kernels' bounded waits never ran out in the calls above."""
+    from safire_b200 import afqmc as A
+    wl, dham, _, _ = case
+    G = torch.zeros((wl.W, wl.nup * wl.M), dtype=torch.complex128, device="cuda")
+    v = torch.zeros((wl.W, wl.Nc), dtype=torch.complex128, device="cuda")
+    dham.vbias(G, v, wl.dt, precision=A.PREC_MIXED)
+    assert dham.device_error_flag() == 0
