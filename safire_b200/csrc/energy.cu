@@ -142,6 +142,10 @@ int energy_fp64(cudaStream_t s, const EnergyArgs& a, c128* E, int W, bool addH1,
       AFQMC_TRY(launch_status("e1_kernel"));
     }
     if (!need_T) continue;
+    if (tc && exchange_fused_ok(tc, sp)) {
+      AFQMC_TRY(exchange_fused(s, tc, sp, W, exx_part, Kl));
+      continue;
+    }
     // chunk of walkers whose T [Wc*Ns][Nc*Ns] fits the workspace
     const long per_walker = long(Ns) * a.Nc * Ns;
     int Wc = int(workT_elems / per_walker);

@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_cgemm_kernel(const __grid_co
         }
         tc::mma_commit(&empty[s]);  // stage reusable once these MMAs have read it
       }
-      tc::mma_commit(accb);  // accumulators complete (also on an aborted run: nothing in flight)
+      if (ok) tc::mma_commit(accb);  // on an aborted run the epilogue leaves through the flag
     }
   } else {
     // epilogue warps 2..5: TMEM lane quarter = warp % 4
@@ -267,34 +267,44 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// 3D map over an FP32 plane [batch][rows][ld] (inner extent k), box {32, box_rows, 1},
-// 128-byte swizzle, zero fill outside the tensor.
-int make_map(CUtensorMap* map, const float* base, long k, long rows, long ld, long batch,
-             long batch_stride, int box_rows) {
+}  // namespace
+
+// 3D map over an FP32 plane: element (x, y, z) at base + z*batch_stride + y*row_stride + x for
+// x < k, y < rows, z < batch; box {32, box_rows, box_batch}, 128-byte swizzle, zero fill outside.
+int make_plane_map_3d(CUtensorMap* map, const float* base, long k, long rows, long row_stride,
+                      long batch, long batch_stride, int box_rows, int box_batch) {
   auto fn = encode_fn();
   if (!fn) {
     set_error_detail("cuTensorMapEncodeTiled is not available");
     return AFQMC_ERR_CUDA;
   }
-  if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld * 4) % 16 || (batch_stride * 4) % 16) {
-    set_error_detail("make_map: plane not 16-byte aligned (ld=%ld, batch stride=%ld)", ld,
-                     batch_stride);
+  if (batch == 1) batch_stride = rows * row_stride;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (row_stride * 4) % 16 ||
+      (batch_stride * 4) % 16) {
+    set_error_detail("make_plane_map_3d: plane not 16-byte aligned (row stride=%ld, batch "
+                     "stride=%ld)", row_stride, batch_stride);
     return AFQMC_ERR_SHAPE;
   }
-  if (batch == 1) batch_stride = rows * ld;
   cuuint64_t dims[3] = {cuuint64_t(k), cuuint64_t(rows), cuuint64_t(batch)};
-  cuuint64_t strides[2] = {cuuint64_t(ld * 4), cuuint64_t(batch_stride * 4)};
-  cuuint32_t box[3] = {cuuint32_t(BK), cuuint32_t(box_rows), 1};
+  cuuint64_t strides[2] = {cuuint64_t(row_stride * 4), cuuint64_t(batch_stride * 4)};
+  cuuint32_t box[3] = {cuuint32_t(BK), cuuint32_t(box_rows), cuuint32_t(box_batch)};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides,
                   box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
-    set_error_detail("cuTensorMapEncodeTiled failed (%d): k=%ld rows=%ld ld=%ld batch=%ld box=%d",
-                     int(r), k, rows, ld, batch, box_rows);
+    set_error_detail("cuTensorMapEncodeTiled failed (%d): k=%ld rows=%ld batch=%ld box=%dx%d",
+                     int(r), k, rows, batch, box_rows, box_batch);
     return AFQMC_ERR_CUDA;
   }
   return AFQMC_OK;
+}
+
+namespace {
+
+int make_map(CUtensorMap* map, const float* base, long k, long rows, long ld, long batch,
+             long batch_stride, int box_rows) {
+  return make_plane_map_3d(map, base, k, rows, ld, batch, batch_stride, box_rows, 1);
 }
 
 // FP32 planes of one operand: 4 (complex) or 2 (real) arrays [batch][rows][ld]
@@ -420,6 +430,7 @@ struct MixedHam {
   Planes Lnak[2];   // [1][Nc][nel*M] (B of vbias, K = nel*M); same memory viewed [Nc*nel][M] for exchange
   // dynamic operands, sized on demand
   int capW = 0;
+  int exchange_split = 3;  // TF32 products per real product in the exchange contraction
   Planes G;         // [W][1][nel_tot*M]  (A of vbias);  exchange view [W*nel][M]
   Planes X;         // [1][W][Nc] (A of vHS)
   unsigned* err = nullptr;
@@ -718,6 +729,30 @@ int exchange_T_tc(cudaStream_t s, MixedHam* m, int sp, int w0, int wc, c128* wor
   p.err = m->err;
   if (m->lnak_cplx) return launch_tc<true, true, 64, 2, EPI_C128>(s, p, wc);
   return launch_tc<true, false, 128, 2, EPI_C128>(s, p, wc);
+}
+
+int exchange_fused_tc(cudaStream_t s, const float* const Gp[4], long ldG, long off,
+                      const float* const Lp[2], int W, int N, int Nc, int M, int nsplit,
+                      c128* exx, c128* kl, unsigned* err);
+
+bool exchange_fused_ok(MixedHam* m, int sp) {
+  return !m->lnak_cplx && m->nel[sp] >= 1 && m->nel[sp] <= 50;
+}
+
+int exchange_fused(cudaStream_t s, MixedHam* m, int sp, int W, c128* exx, c128* kl) {
+  const float* Gp[4] = {m->G.p[0], m->G.p[1], m->G.p[2], m->G.p[3]};
+  const float* Lp[2] = {m->Lnak[sp].p[0], m->Lnak[sp].p[1]};
+  return exchange_fused_tc(s, Gp, m->G.ld, long(m->el_off[sp]) * m->M, Lp, W, m->nel[sp], m->Nc,
+                           m->M, m->exchange_split, exx, kl, m->err);
+}
+
+int mixed_set_exchange_split(MixedHam* m, int nsplit) {
+  if (nsplit != 1 && nsplit != 3) {
+    set_error_detail("exchange split must be 1 or 3");
+    return AFQMC_ERR_ARG;
+  }
+  m->exchange_split = nsplit;
+  return AFQMC_OK;
 }
 
 int mixed_error_flag(MixedHam* m, unsigned* flag) {

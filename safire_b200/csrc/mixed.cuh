@@ -22,6 +22,11 @@ int mixed_prepare_G(cudaStream_t s, MixedHam* m, const c128* G, long ldG, int W)
 // T [(w,b)][(n,a)] for walkers [w0, w0+wc) of spin block sp (complex128, the chunk layout of
 // energy_fp64)
 int exchange_T_tc(cudaStream_t s, MixedHam* m, int sp, int w0, int wc, c128* workT);
+// fused T-free exchange for spin block sp (real trial, N <= 50): exx/kl [W][Nc] +=
+bool exchange_fused_ok(MixedHam* m, int sp);
+int exchange_fused(cudaStream_t s, MixedHam* m, int sp, int W, c128* exx, c128* kl);
+// 3: 3xTF32 (default), 1: single TF32 product in the exchange contraction
+int mixed_set_exchange_split(MixedHam* m, int nsplit);
 // first device-side wait timeout reported by the tensor-core kernels (0 = none)
 int mixed_error_flag(MixedHam* m, unsigned* flag);
 

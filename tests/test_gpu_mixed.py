@@ -100,3 +100,20 @@ def test_mixed_no_device_timeout(case):
     v = torch.zeros((wl.W, wl.Nc), dtype=torch.complex128, device="cuda")
     dham.vbias(G, v, wl.dt, precision=A.PREC_MIXED)
     assert dham.device_error_flag() == 0
+
+
+def test_energy_mixed_large_block(cuda):
+    """The fused exchange kernel at N = 50 electrons (the benchmark's block size), M = 200."""
+    from safire_b200 import afqmc as A
+    wl = make_workload("cfg2", W=5, Nc=48)
+    dham, oham, _ = make_pair(wl)
+    rs = np.random.default_rng(4)
+    G = rand_c(rs, 5, wl.nup * wl.M, scale=0.1)
+    E = torch.zeros((5, 3), dtype=torch.complex128, device="cuda")
+    dham.energy(E, to_dev(G), precision=A.PREC_MIXED)
+    Eo = oham.energy(G)
+    Ed = to_host(E)
+    errs = [rel_err(Ed[:, q], Eo[:, q]) for q in range(3)]
+    print("energy mixed N=50 rel errs", ["%.2e" % e for e in errs])
+    assert max(errs[1:]) < TOL_ONE
+    assert dham.device_error_flag() == 0
