@@ -89,6 +89,16 @@ unsigned long long afqmc_kernel_launches(void);
 int afqmc_log_overlap(const afqmc_c128* PsiT, const afqmc_c128* S, long ldS, afqmc_c128* ovlp,
                       int W, int M, int N, afqmc_stream stream);
 
+/* afqmc_log_overlap without any device allocation.  No counterpart in the reference: it exists
+ * for callers that cannot allocate device memory (an application that reserves all device memory
+ * for its own pool and treats a later cudaMalloc as an error, or one already at its memory limit).
+ * Same arguments and result as afqmc_log_overlap; its scratch is a fixed 8 MiB device array inside
+ * the library, so W*N*N must not exceed 524288 (larger calls return AFQMC_ERR_SHAPE).  All calls on
+ * a device share that array: calls that overlap on the GPU race.  The first call on a device
+ * looks up the array's address with that device current; make it before any stream capture. */
+int afqmc_log_overlap_noalloc(const afqmc_c128* PsiT, const afqmc_c128* S, long ldS,
+                              afqmc_c128* ovlp, int W, int M, int N, afqmc_stream stream);
+
 /* det_ops::MixedDensityMatrix(A=PsiT, B=S, C=G, ovlp, compact, herm=true) —
  * density_matrix.hpp:535-601.  compact != 0: G [W][N][M] = (PsiT S_w)^{-T} S_w^T;
  * compact == 0: G [W][M][M] = PsiT^T (PsiT S_w)^{-T} S_w^T.  ldG = walker stride of G.

@@ -41,6 +41,7 @@ _SIGS = {
     "afqmc_prop_set_timing": (i32, [vp, i32]),
     "afqmc_prop_timings": (i32, [vp, C.POINTER(f64)]),
     "afqmc_log_overlap": (i32, [vp, vp, i64, vp, i32, i32, i32, vp]),
+    "afqmc_log_overlap_noalloc": (i32, [vp, vp, i64, vp, i32, i32, i32, vp]),
     "afqmc_mixed_density_matrix": (i32, [vp, vp, i64, vp, i64, vp, i32, i32, i32, i32, vp]),
     "afqmc_inverse_logdet": (i32, [vp, vp, vp, i32, i32, vp]),
     "afqmc_orthogonalize": (i32, [vp, i64, vp, i32, i32, i32, vp]),
