@@ -39,6 +39,8 @@ def parse():
     ap.add_argument("--walkers", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--exchange-split", type=int, default=3, choices=[1, 3],
+                    help="TF32 products per real product in the mixed exchange contraction")
     return ap.parse_args()
 
 
@@ -203,6 +205,29 @@ def fp64_peak_tflops(torch):
     return 2 * n ** 3 / best / 1e12
 
 
+def tf32_peak_tflops(torch):
+    """Dense TF32 tensor-core throughput of cuBLAS (FP32 GEMM with TF32 allowed) on this GPU."""
+    n = 8192
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1000)
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    return 2 * n ** 3 / best / 1e12
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -226,6 +251,8 @@ def run_ours(args):
     wl = make_workload("cfg2")
     rp = RunParams(equilibration_steps=0, seed=rank)
     sim = Simulation.from_workload(wl, W=W, precision=prec, rp=rp)
+    if prec == A.PREC_MIXED and args.exchange_split != 3:
+        sim.ham.set_exchange_split(args.exchange_split)
     stream = torch.cuda.current_stream()
 
     def block():
@@ -280,24 +307,31 @@ def run_ours(args):
     torch.cuda.synchronize()
     phases["orthogonalize"] = o0.elapsed_time(o1)
 
-    # roofline of the dominant kernel: the FP64 contraction with the largest share of a block
+    # roofline of the dominant kernel: the contraction with the largest share of a block
     M, N, Nc = wl.M, wl.nup, wl.Nc
-    flops = {  # flops the kernels execute per call (real trial: Lnak, L and P1 are real)
-        "vHS": 4.0 * M * M * Nc * W,
-        "vbias": 4.0 * N * M * Nc * W,
-        "propagate": W * (2 * 4.0 * M * M * N + 6 * 8.0 * M * M * N),
-        "energy_measurement": W * (4.0 * N * N * M * Nc + 8.0 * N * N * Nc),
-    }
+    if prec == A.PREC_FP64:
+        # flops the FP64 kernels execute (real trial: Lnak, L and P1 are real)
+        flops = {"vHS": 4.0 * M * M * Nc * W, "vbias": 4.0 * N * M * Nc * W,
+                 "propagate": W * (2 * 4.0 * M * M * N + 6 * 8.0 * M * M * N),
+                 "energy_measurement": W * (4.0 * N * N * M * Nc + 8.0 * N * N * Nc)}
+        peak = fp64_peak_tflops(torch)
+        peak_src = "cuBLAS DGEMM 8192^3 measured in this run (dense FP64)"
+    else:
+        # TF32 MMA flops of the split products (x3 for 3xTF32, unpadded tile extents)
+        sp = 3.0
+        ex = float(args.exchange_split)
+        flops = {"vHS": sp * 4.0 * M * M * Nc * W, "vbias": sp * 4.0 * N * M * Nc * W,
+                 "propagate": sp * W * (2 * 4.0 * M * M * N + 6 * 8.0 * M * M * N),
+                 "energy_measurement": ex * W * 4.0 * N * N * M * Nc}
+        peak = tf32_peak_tflops(torch)
+        peak_src = "cuBLAS TF32 GEMM 8192^3 measured in this run (dense TF32 tensor cores)"
     block_share = {k: (phases[k] * (1 if k == "energy_measurement" else BLOCK)) for k in flops}
     top = max(block_share, key=block_share.get)
     achieved = flops[top] / (phases[top] / 1000) / 1e12
-    peak = fp64_peak_tflops(torch) if prec == A.PREC_FP64 else None
-    peaks = measured_peaks()
     roofline = {"kernel": top, "bound": "tensor", "achieved": achieved,
-                "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if peak else None, "traffic": None,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64)",
-                "flops_per_launch": flops[top]}
+                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": peak_src, "flops_per_launch": flops[top],
+                "block_share_ms": block_share}
 
     # e2e: the same loop through the public API with host uniforms copied in from pinned memory
     # and the weights + energy estimate read back every block
@@ -358,10 +392,12 @@ def run_ours(args):
             "config": {"workload": "M=200 N=50+50 Nc=1600 W=1024/GPU dt=0.005 taylor=6, "
                                    "block of 10 steps (ortho/5, comb/10, energy/10)",
                        "precision": args.precision, "global_walkers": W * world,
+                       "exchange_split": args.exchange_split if prec == A.PREC_MIXED else None,
                        "parallelism": f"walker dp{world}",
                        "l2": "inputs larger than L2 (V 655 MB, Likn 512 MB per step)"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clk, "phases_ms": phases,
+            "device_error_flag": int(sim.ham.device_error_flag()),
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -161,6 +161,10 @@ int afqmc_ham_vhs(afqmc_ham ham, const afqmc_c128* X, afqmc_c128* V, int W, doub
 int afqmc_ham_energy(afqmc_ham ham, const afqmc_c128* G, afqmc_c128* E, int W, int addH1,
                      int addEJ, int addEXX, int precision, afqmc_stream stream);
 
+/* TF32 products per real product in the mixed-precision exchange contraction: 3 (3xTF32, the
+ * default) or 1 (plain TF32, for runs whose energy tolerance allows it). */
+int afqmc_ham_set_exchange_split(afqmc_ham ham, int nsplit);
+
 /* Error word of the tensor-core kernels' bounded device waits (bit 0: a wait on a TMA or MMA
  * completion gave up after about 2 s and the kernel returned without finishing).  0 = none, or
  * the mixed-precision path was never used.  Synchronous. */

@@ -157,6 +157,10 @@ class HamiltonianOperations:
         call("afqmc_ham_one_body_propagator", self.handle, float(dt), _host_ptr(vm), _host_ptr(H1))
         return H1
 
+    def set_exchange_split(self, nsplit):
+        """3: 3xTF32 exchange contraction (default); 1: plain TF32."""
+        call("afqmc_ham_set_exchange_split", self.handle, int(nsplit))
+
     def device_error_flag(self):
         f = C.c_uint()
         call("afqmc_ham_device_error", self.handle, C.byref(f))

@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <random>
 #include <string>
@@ -139,6 +140,7 @@ struct afqmc_prop_s {
   c128 *G = nullptr, *vb = nullptr, *X = nullptr, *HW = nullptr, *mf = nullptr;
   c128 *newov = nullptr, *ovtmp = nullptr, *T = nullptr, *V = nullptr;
   c128 *w1 = nullptr, *w2 = nullptr, *w3 = nullptr;
+  c128* ortho_work = nullptr;
   double* Eshift_d = nullptr;
   unsigned long long* counter = nullptr;
   unsigned long long* stats = nullptr;
@@ -152,7 +154,7 @@ struct afqmc_prop_s {
       if (e) cudaEventDestroy(e);
     dfree(P1); dfree(P1r); dfree(vMF);
     dfree(G); dfree(vb); dfree(X); dfree(HW); dfree(mf); dfree(newov); dfree(ovtmp);
-    dfree(T); dfree(V); dfree(w1); dfree(w2); dfree(w3);
+    dfree(T); dfree(V); dfree(w1); dfree(w2); dfree(w3); dfree(ortho_work);
     dfree(Eshift_d); dfree(counter); dfree(stats);
   }
 };
@@ -186,6 +188,23 @@ extern "C" unsigned long long afqmc_kernel_launches(void) { return g_launches.lo
 // det_ops
 // ---------------------------------------------------------------------------------------------
 namespace {
+// Scratch of the stream-ordered allocator.  The device's default pool keeps freed blocks for reuse
+// (release threshold raised once per device), so repeated calls do not map and unmap memory.
+void retain_pool_memory() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  done[dev] = true;
+}
+
 struct Scratch {
   void* p = nullptr;
   cudaStream_t s = nullptr;
@@ -195,6 +214,7 @@ struct Scratch {
   int get(size_t bytes, cudaStream_t st) {
     s = st;
     if (bytes == 0) return AFQMC_OK;
+    retain_pool_memory();
     cudaError_t e = cudaMallocAsync(&p, bytes, st);
     if (e != cudaSuccess) {
       set_error_detail("cudaMallocAsync(%zu) failed: %s", bytes, cudaGetErrorString(e));
@@ -377,8 +397,11 @@ int ham_energy(afqmc_ham_s* h, cudaStream_t s, const c128* G, long ldG, c128* E,
     AFQMC_TRY(mixed_prepare_G(s, tc, G, ldG, W));
   }
   Scratch wT, ex, kl;
-  long chunk = energy_chunk_elems(h, W);
-  AFQMC_TRY(wT.get(sizeof(c128) * size_t(chunk), s));
+  bool fused = tc != nullptr;
+  for (int sp = 0; sp < h->nspin && fused; ++sp)
+    if (h->nel[sp] > 0 && !exchange_fused_ok(tc, sp)) fused = false;
+  const long chunk = fused ? 0 : energy_chunk_elems(h, W);
+  if (!fused) AFQMC_TRY(wT.get(sizeof(c128) * size_t(chunk), s));
   AFQMC_TRY(ex.get(sizeof(c128) * size_t(W) * h->Nc, s));
   AFQMC_TRY(kl.get(sizeof(c128) * size_t(W) * h->Nc, s));
   return energy_fp64(s, a, E, W, addH1, addEJ, addEXX, (c128*)wT.p, chunk, (c128*)ex.p,
@@ -590,6 +613,17 @@ extern "C" int afqmc_ham_energy(afqmc_ham h, const afqmc_c128* G, afqmc_c128* E,
   return ham_energy(h, reinterpret_cast<cudaStream_t>(stream), (const c128*)G,
                     long(h->nel_tot) * h->M, (c128*)E, W, addH1 != 0, addEJ != 0, addEXX != 0,
                     precision);
+}
+
+extern "C" int afqmc_ham_set_exchange_split(afqmc_ham h, int nsplit) {
+  AFQMC_CHECK_ARG(h, "afqmc_ham_set_exchange_split: null handle");
+  AFQMC_CHECK_ARG(nsplit == 1 || nsplit == 3, "afqmc_ham_set_exchange_split: nsplit must be 1 or 3");
+  DeviceGuard g(h->device);
+  if (!h->mixed) {
+    EnergyArgs a = energy_args(h, nullptr, 0);
+    AFQMC_TRY(mixed_ham_create(&h->mixed, a, nullptr));
+  }
+  return mixed_set_exchange_split(h->mixed, nsplit);
 }
 
 extern "C" int afqmc_ham_device_error(afqmc_ham h, unsigned* flag) {
@@ -1027,6 +1061,8 @@ extern "C" int afqmc_prop_create(afqmc_ham h, const afqmc_prop_params* params, i
   AFQMC_TRY(dalloc(&pr->w1, size_t(W) * M * (nmax > 0 ? nmax : 1)));
   AFQMC_TRY(dalloc(&pr->w2, size_t(W) * M * (nmax > 0 ? nmax : 1)));
   AFQMC_TRY(dalloc(&pr->w3, size_t(W) * M * (nmax > 0 ? nmax : 1)));
+  AFQMC_TRY(dalloc(&pr->ortho_work, size_t(W) * M * (nmax > 0 ? nmax : 1) +
+                                        2 * size_t(W) * (nmax > 0 ? nmax * nmax : 1)));
   AFQMC_TRY(dalloc(&pr->Eshift_d, 1));
   AFQMC_TRY(dalloc(&pr->counter, 1));
   AFQMC_TRY(dalloc(&pr->stats, 8));
@@ -1153,7 +1189,7 @@ extern "C" int afqmc_prop_orthogonalize(afqmc_prop pr, afqmc_wset ws, afqmc_stre
   for (int sp = 0; sp < h->nspin; ++sp) {
     if (h->nel[sp] == 0) continue;
     AFQMC_TRY(orthogonalize(s, ws->buf + ws->offS(sp), ws->walker_size, pr->ovtmp, ws->W, h->M,
-                            h->nel[sp]));
+                            h->nel[sp], pr->ortho_work));
   }
   AFQMC_TRY(wfn_log_overlap(h, ws, s, pr->newov, pr->T));
   return scatter_property(s, ws->buf, ws->walker_size, ws->prop0 + AFQMC_OVLP, ws->W, pr->newov);

@@ -31,127 +31,137 @@ __device__ __forceinline__ c128 log_pivot(c128 d, bool swapped) {
 // Gauss-Jordan elimination with partial pivoting (pivot = first max |re|+|im|, as izamax) on
 // [A | I] in shared memory.  The pivots are the U diagonal of getrf with the same row
 // interchanges, so the log-determinant follows log_determinant_from_getrf; the right half ends as
-// A^{-1} (zero for a singular A, as getri_or_zero).  One CTA per matrix.
+// A^{-1} (zero for a singular A, as getri_or_zero).  Without the inverse only the trailing
+// submatrix is eliminated (plain LU) and the matrix needs a quarter of the shared memory, so more
+// matrices share an SM.  One CTA per matrix, 8 warps: warp 0 finds the pivot, the pivot row, the
+// old row k and the scaled multipliers are snapshotted, then every thread updates its
+// (rows ty+8r) x (cols k+1+tx+32c) elements from the snapshots only: three barriers per step and
+// no element read after another thread wrote it in the same phase.
 // ---------------------------------------------------------------------------------------------
+constexpr int GJ_THREADS = 256;
+
 template <bool INVERT>
-__global__ void __launch_bounds__(256) gj_logdet_kernel(const c128* __restrict__ A, long strideA,
-                                                         c128* __restrict__ Ainv, long strideInv,
-                                                         c128* __restrict__ ovlp, int N,
-                                                         c128 post_scale, c128 post_add) {
+__global__ void __launch_bounds__(GJ_THREADS) gj_logdet_kernel(const c128* __restrict__ A,
+                                                                long strideA,
+                                                                c128* __restrict__ Ainv,
+                                                                long strideInv,
+                                                                c128* __restrict__ ovlp, int N,
+                                                                c128 post_scale, c128 post_add) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int P = INVERT ? 2 * N : N;  // row length of the augmented matrix
-  c128* a = reinterpret_cast<c128*>(smem_raw);      // [N][P]
-  c128* piv_val = a + size_t(N) * P;                 // [N]
+  const int P = INVERT ? 2 * N : N;  // columns of the augmented matrix
+  const int PP = P | 1;              // odd pitch: conflict-free column walks
+  c128* a = reinterpret_cast<c128*>(smem_raw);  // [N][PP]
+  c128* rbuf = a + size_t(N) * PP;              // pivot row (post-swap row k) [P]
+  c128* kbuf = rbuf + P;                        // old row k [P]
+  c128* mbuf = kbuf + P;                        // scaled multipliers of the post-swap rows [N]
+  c128* piv_val = mbuf + N;                     // [N]
   int* piv_swapped = reinterpret_cast<int*>(piv_val + N);
   __shared__ int s_piv;
   __shared__ int s_singular;
-  __shared__ double s_red_v[8];
-  __shared__ int s_red_i[8];
+  __shared__ c128 s_dinv;
 
   const long w = blockIdx.x;
   const c128* Aw = A + w * strideA;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int e = tid; e < N * N; e += nt) {
-    int i = e / N, j = e % N;
-    a[i * P + j] = Aw[e];
-  }
-  if (INVERT) {
-    for (int e = tid; e < N * N; e += nt) {
-      int i = e / N, j = e % N;
-      a[i * P + N + j] = cmk(i == j ? 1.0 : 0.0, 0.0);
-    }
+  const int tid = threadIdx.x;
+  const int tx = tid & 31, ty = tid >> 5;
+  for (int i = ty; i < N; i += GJ_THREADS / 32) {
+    for (int j = tx; j < N; j += 32) a[i * PP + j] = Aw[long(i) * N + j];
+    if (INVERT)
+      for (int j = tx; j < N; j += 32) a[i * PP + N + j] = cmk(i == j ? 1.0 : 0.0, 0.0);
   }
   if (tid == 0) s_singular = 0;
   __syncthreads();
 
   for (int k = 0; k < N; ++k) {
-    // pivot search in column k, rows k..N-1 (first maximal |re|+|im|)
-    double best = -1.0;
-    int bi = N;
-    for (int i = k + tid; i < N; i += nt) {
-      double v = cabs1(a[i * P + k]);
-      if (v > best) {
-        best = v;
-        bi = i;
-      }
-    }
-    for (int off = 16; off > 0; off >>= 1) {
-      double ov = __shfl_down_sync(0xffffffffu, best, off);
-      int oi = __shfl_down_sync(0xffffffffu, bi, off);
-      if (ov > best || (ov == best && oi < bi)) {
-        best = ov;
-        bi = oi;
-      }
-    }
-    if ((tid & 31) == 0) {
-      s_red_v[tid >> 5] = best;
-      s_red_i[tid >> 5] = bi;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      double bv = s_red_v[0];
-      int b = s_red_i[0];
-      for (int q = 1; q < (nt + 31) / 32; ++q)
-        if (s_red_v[q] > bv || (s_red_v[q] == bv && s_red_i[q] < b)) {
-          bv = s_red_v[q];
-          b = s_red_i[q];
+    // 1. pivot search in column k, rows k..N-1 (warp 0)
+    if (ty == 0) {
+      double best = -1.0;
+      int bi = N;
+      for (int i = k + tx; i < N; i += 32) {
+        const double v = cabs1(a[i * PP + k]);
+        if (v > best) {
+          best = v;
+          bi = i;
         }
-      s_piv = b;
-      piv_swapped[k] = (b != k);
-      if (!(bv > 0.0)) s_singular = 1;
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, best, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        if (ov > best || (ov == best && oi < bi)) {
+          best = ov;
+          bi = oi;
+        }
+      }
+      if (tx == 0) {
+        s_piv = bi;
+        piv_swapped[k] = (bi != k);
+        const c128 d = a[bi * PP + k];
+        piv_val[k] = d;
+        if (!(best > 0.0)) {
+          s_singular = 1;
+          s_dinv = cmk(0, 0);
+        } else {
+          s_dinv = cdiv(cmk(1.0, 0.0), d);
+        }
+      }
     }
     __syncthreads();
     const int p = s_piv;
-    if (p != k) {
-      for (int j = tid; j < P; j += nt) {
-        c128 t = a[k * P + j];
-        a[k * P + j] = a[p * P + j];
-        a[p * P + j] = t;
-      }
-      __syncthreads();
+    const c128 dinv = s_dinv;
+    const bool zero = (dinv.x == 0.0 && dinv.y == 0.0);
+    // 2. snapshots: pivot row, old row k, multipliers (column k of the post-swap rows) * dinv
+    for (int j = k + tid; j < P; j += GJ_THREADS) {
+      rbuf[j] = a[p * PP + j];
+      kbuf[j] = a[k * PP + j];
     }
-    const c128 d = a[k * P + k];
-    if (tid == 0) piv_val[k] = d;
-    const bool zero = (d.x == 0.0 && d.y == 0.0);
-    if (!zero) {
-      // eliminate column k: below the diagonal (LU part) and, for the inverse, above it too
-      const int r0 = INVERT ? 0 : k + 1;
-      const int nrows = N - r0;
-      const int ncols = P - (k + 1);
-      const c128 dinv = cdiv(cmk(1.0, 0.0), d);
-      // multipliers stored in column k of each row before the update
-      for (int i = r0 + tid; i < N; i += nt) {
-        if (i == k) continue;
-        a[i * P + k] = cmul(a[i * P + k], dinv);
-      }
-      __syncthreads();
-      for (int e = tid; e < nrows * ncols; e += nt) {
-        int i = r0 + e / ncols, j = k + 1 + e % ncols;
-        if (i == k) continue;
-        a[i * P + j] = csub(a[i * P + j], cmul(a[i * P + k], a[k * P + j]));
-      }
-      __syncthreads();
-      if (INVERT) {
-        // row k scaled by 1/d so the left block becomes the identity
-        for (int j = k + 1 + tid; j < P; j += nt) a[k * P + j] = cmul(a[k * P + j], dinv);
-        __syncthreads();
+    for (int i = (INVERT ? 0 : k) + tid; i < N; i += GJ_THREADS) {
+      const c128 c = (i == k) ? a[p * PP + k] : ((i == p) ? a[k * PP + k] : a[i * PP + k]);
+      mbuf[i] = cmul(c, dinv);
+    }
+    __syncthreads();
+    // 3. row swap + elimination (+ pivot-row scaling for the inverse)
+    const int r0 = INVERT ? 0 : k;
+    for (int i = r0 + ty; i < N; i += GJ_THREADS / 32) {
+      if (i == k) {
+        for (int j = k + 1 + tx; j < P; j += 32)
+          a[k * PP + j] = (INVERT && !zero) ? cmul(rbuf[j], dinv) : rbuf[j];
+      } else {
+        const c128 m = mbuf[i];
+        const bool from_k = (i == p);
+        for (int j = k + 1 + tx; j < P; j += 32) {
+          const c128 src = from_k ? kbuf[j] : a[i * PP + j];
+          a[i * PP + j] = zero ? src : csub(src, cmul(m, rbuf[j]));
+        }
       }
     }
+    __syncthreads();
   }
 
-  if (tid == 0) {
-    c128 res = ovlp[w];
-    for (int k = 0; k < N; ++k) res = cadd(res, log_pivot(piv_val[k], piv_swapped[k] != 0));
-    res = wrap_imag(res);
-    ovlp[w] = cadd(cmul(post_scale, res), post_add);
+  // log det: sum_k log(+-U_kk + DBL_MIN), accumulated onto ovlp, imaginary part wrapped
+  if (ty == 0) {
+    double sr = 0.0, si = 0.0;
+    for (int k = tx; k < N; k += 32) {
+      const c128 l = log_pivot(piv_val[k], piv_swapped[k] != 0);
+      sr += l.x;
+      si += l.y;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      sr += __shfl_xor_sync(0xffffffffu, sr, off);
+      si += __shfl_xor_sync(0xffffffffu, si, off);
+    }
+    if (tx == 0) {
+      c128 res = cadd(ovlp[w], cmk(sr, si));
+      res = wrap_imag(res);
+      ovlp[w] = cadd(cmul(post_scale, res), post_add);
+    }
   }
   if (INVERT) {
     c128* Iw = Ainv + w * strideInv;
     const bool sing = s_singular != 0;
-    for (int e = tid; e < N * N; e += nt) {
-      int i = e / N, j = e % N;
-      Iw[e] = sing ? cmk(0.0, 0.0) : a[i * P + N + j];
-    }
+    for (int i = ty; i < N; i += GJ_THREADS / 32)
+      for (int j = tx; j < N; j += 32) Iw[long(i) * N + j] = sing ? cmk(0.0, 0.0) : a[i * PP + N + j];
   }
 }
 
@@ -159,21 +169,22 @@ int batched_logdet_inverse(cudaStream_t s, const c128* A, long strideA, c128* Ai
                            c128* ovlp, int W, int N, bool invert, c128 post_scale, c128 post_add) {
   if (W <= 0 || N <= 0) return AFQMC_OK;
   const int P = invert ? 2 * N : N;
-  size_t smem = size_t(N) * P * sizeof(c128) + N * sizeof(c128) + N * sizeof(int);
+  const int PP = P | 1;
+  size_t smem = (size_t(N) * PP + 2 * size_t(P) + 2 * size_t(N)) * sizeof(c128) + N * sizeof(int);
   if (smem > 227 * 1024) {
-    set_error_detail("batched_logdet_inverse: N = %d exceeds the shared-memory kernel (max 84)", N);
+    set_error_detail("batched_logdet_inverse: N = %d exceeds the shared-memory kernel", N);
     return AFQMC_ERR_UNSUPPORTED;
   }
   if (invert) {
     AFQMC_CUDA_TRY(cudaFuncSetAttribute(gj_logdet_kernel<true>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    gj_logdet_kernel<true><<<W, 256, smem, s>>>(A, strideA, Ainv, strideInv, ovlp, N, post_scale,
-                                                post_add);
+    gj_logdet_kernel<true><<<W, GJ_THREADS, smem, s>>>(A, strideA, Ainv, strideInv, ovlp, N,
+                                                       post_scale, post_add);
   } else {
     AFQMC_CUDA_TRY(cudaFuncSetAttribute(gj_logdet_kernel<false>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    gj_logdet_kernel<false><<<W, 256, smem, s>>>(A, strideA, nullptr, 0, ovlp, N, post_scale,
-                                                 post_add);
+    gj_logdet_kernel<false><<<W, GJ_THREADS, smem, s>>>(A, strideA, nullptr, 0, ovlp, N,
+                                                        post_scale, post_add);
   }
   return launch_status("gj_logdet_kernel");
 }

@@ -26,7 +26,9 @@ int mixed_density_matrix(cudaStream_t s, const c128* PsiT, const c128* S, long l
 int propagate(cudaStream_t s, const void* P1, bool p1_real, const c128* V, long strideV, c128* S,
               long ldS, int W, int M, int N, int order, c128* work1, c128* work2, c128* work3);
 
-// det_ops::orthogonalize: S_w <- Q_w diag(sign(Re R_ii)), logdetR[w] += sum log(|R_ii|)
-int orthogonalize(cudaStream_t s, c128* S, long ldS, c128* logdetR, int W, int M, int N);
+// det_ops::orthogonalize: S_w <- Q_w diag(sign(Re R_ii)), logdetR[w] += sum log(|R_ii|).
+// work: [W*M*N + 2*W*N*N] complex, or nullptr to take it from the stream-ordered allocator.
+int orthogonalize(cudaStream_t s, c128* S, long ldS, c128* logdetR, int W, int M, int N,
+                  c128* work = nullptr);
 
 }  // namespace afqmc

@@ -38,7 +38,8 @@ enum Epi : int {
 struct TcParams {
   CUtensorMap a[4];
   CUtensorMap b[4];
-  int m, n, k;
+  int m, n, k, batch;
+  int order;  // tile order (see tc_tile)
   int a_batched, b_batched;
   c128 alpha;
   float* out[4];        // split planes re_hi, re_lo, im_hi, im_lo
@@ -59,10 +60,10 @@ struct TcCfg {
   static constexpr int A_TILE = 128 * BK * 4;  // bytes per plane tile
   static constexpr int B_TILE = BN * BK * 4;
   static constexpr int STAGE = NA * A_TILE + NB * B_TILE;
-  static constexpr int TMEM_COLS = (2 * BN <= 32) ? 32 : (2 * BN <= 64) ? 64 : (2 * BN <= 128) ? 128
-                                   : (2 * BN <= 256) ? 256 : 512;
+  // two accumulators (re, im) x 2 buffers
+  static constexpr int TMEM_COLS = (4 * BN <= 128) ? 128 : (4 * BN <= 256) ? 256 : 512;
   static constexpr size_t SMEM = size_t(STAGES) * STAGE + 1024 /*align*/ + 256 /*barriers*/;
-  static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N for M=128");
+  static_assert(BN % 16 == 0 && BN >= 16 && BN <= 128, "UMMA N for M=128, double buffered");
   static_assert(SMEM <= 232448, "shared memory");
 };
 
@@ -72,21 +73,41 @@ __device__ __forceinline__ void split_store(float v, float* hi, float* lo, long 
   lo[idx] = v - h;
 }
 
+// tile t -> (m tile, n tile, batch).  order 0: m tiles fastest (consecutive tiles share the B
+// tile); order 1: n tiles fastest (consecutive tiles share the A tile).
+__device__ __forceinline__ void tc_tile(long t, int MT, int NT, int order, int& mt, int& nt,
+                                        int& z) {
+  if (order == 0) {
+    mt = int(t % MT);
+    const long r = t / MT;
+    nt = int(r % NT);
+    z = int(r / NT);
+  } else {
+    nt = int(t % NT);
+    const long r = t / NT;
+    mt = int(r % MT);
+    z = int(r / MT);
+  }
+}
+
+// Persistent tensor-core GEMM: one CTA per SM walks the tiles; the TMA ring runs ahead across
+// tiles and the epilogue of tile i overlaps the MMAs of tile i+1 (two TMEM accumulators).
 template <bool A_CPLX, bool B_CPLX, int BN, int STAGES, int EPI>
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_cgemm_kernel(const __grid_constant__ TcParams p) {
   using K = TcCfg<A_CPLX, B_CPLX, BN, STAGES>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  // 1024-byte aligned stage buffers (128-byte swizzle atoms)
   unsigned char* base = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * K::STAGE);
   uint64_t* empty = full + STAGES;
-  uint64_t* accb = empty + STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accb + 1);
+  uint64_t* acc_full = empty + STAGES;  // [2]
+  uint64_t* acc_empty = acc_full + 2;   // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * 128, n0 = blockIdx.y * BN, z = blockIdx.z;
+  const int MT = (p.m + 127) / 128, NT = (p.n + BN - 1) / BN;
+  const long ntiles = long(MT) * NT * p.batch;
   const int nk = (p.k + BK - 1) / BK;
 
   if (threadIdx.x == 0) {
@@ -94,7 +115,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_cgemm_kernel(const __grid_co
       tc::mbar_init(&full[s], 1);
       tc::mbar_init(&empty[s], 1);
     }
-    tc::mbar_init(accb, 1);
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(&acc_full[b], 1);
+      tc::mbar_init(&acc_empty[b], 128);
+    }
     *abort_flag = 0;
     tc::fence_mbar_init();
 #pragma unroll
@@ -113,101 +137,131 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_cgemm_kernel(const __grid_co
 
   if (warp == 0) {
     if (lane == 0) {
-      const int za = p.a_batched ? z : 0, zb = p.b_batched ? z : 0;
-      for (int kc = 0; kc < nk; ++kc) {
-        const int s = kc % STAGES;
-        if (kc >= STAGES) {
-          if (!tc::mbar_wait(&empty[s], ((kc / STAGES) - 1) & 1, p.err, abort_flag)) break;
+      long it = 0;
+      bool ok = true;
+      for (long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        int mt, nt, z;
+        tc_tile(t, MT, NT, p.order, mt, nt, z);
+        const int za = p.a_batched ? z : 0, zb = p.b_batched ? z : 0;
+        for (int kc = 0; kc < nk; ++kc, ++it) {
+          const int s = int(it % STAGES);
+          if (it >= STAGES) {
+            if (!tc::mbar_wait(&empty[s], unsigned((it / STAGES) - 1) & 1u, p.err, abort_flag)) {
+              ok = false;
+              break;
+            }
+          }
+          unsigned char* st = base + size_t(s) * K::STAGE;
+          tc::mbar_arrive_expect_tx(&full[s], K::STAGE);
+#pragma unroll
+          for (int q = 0; q < K::NA; ++q)
+            tc::tma_load_3d(st + q * K::A_TILE, &p.a[q], &full[s], kc * BK, mt * 128, za);
+#pragma unroll
+          for (int q = 0; q < K::NB; ++q)
+            tc::tma_load_3d(st + K::NA * K::A_TILE + q * K::B_TILE, &p.b[q], &full[s], kc * BK,
+                            nt * BN, zb);
         }
-        unsigned char* st = base + size_t(s) * K::STAGE;
-        tc::mbar_arrive_expect_tx(&full[s], K::STAGE);
-#pragma unroll
-        for (int q = 0; q < K::NA; ++q)
-          tc::tma_load_3d(st + q * K::A_TILE, &p.a[q], &full[s], kc * BK, m0, za);
-#pragma unroll
-        for (int q = 0; q < K::NB; ++q)
-          tc::tma_load_3d(st + K::NA * K::A_TILE + q * K::B_TILE, &p.b[q], &full[s], kc * BK, n0,
-                          zb);
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t ID = tc::idesc_tf32(128, BN, false);
       constexpr uint32_t IDN = tc::idesc_tf32(128, BN, true);
-      const uint32_t dr = taddr, di = taddr + BN;
+      long it = 0, ti = 0;
       bool ok = true;
-      for (int kc = 0; kc < nk && ok; ++kc) {
-        const int s = kc % STAGES;
-        if (!tc::mbar_wait(&full[s], (kc / STAGES) & 1, p.err, abort_flag)) {
-          ok = false;
-          break;
-        }
-        tc::tc_fence_after();
-        unsigned char* st = base + size_t(s) * K::STAGE;
-        const uint32_t sa = tc::smem_u32(st);
-        const uint32_t sb = tc::smem_u32(st + K::NA * K::A_TILE);
-#pragma unroll
-        for (int kk = 0; kk < BK / 8; ++kk) {
-          // +32 bytes per K=8 step inside the 128-byte swizzle row (descriptor units of 16 B)
-          auto A = [&](int q) { return tc::sdesc_sw128(sa + q * K::A_TILE) + uint64_t(2 * kk); };
-          auto B = [&](int q) { return tc::sdesc_sw128(sb + q * K::B_TILE) + uint64_t(2 * kk); };
-          const uint32_t acc0 = (kc > 0 || kk > 0) ? 1u : 0u;
-          if constexpr (A_CPLX && B_CPLX) {
-            // Dr = Ar Br - Ai Bi ; Di = Ar Bi + Ai Br   (planes 0 re_hi, 1 re_lo, 2 im_hi, 3 im_lo)
-            tc::mma_tf32(dr, A(0), B(0), ID, acc0);
-            tc::mma_tf32(dr, A(0), B(1), ID, 1);
-            tc::mma_tf32(dr, A(1), B(0), ID, 1);
-            tc::mma_tf32(dr, A(2), B(2), IDN, 1);
-            tc::mma_tf32(dr, A(2), B(3), IDN, 1);
-            tc::mma_tf32(dr, A(3), B(2), IDN, 1);
-            tc::mma_tf32(di, A(0), B(2), ID, acc0);
-            tc::mma_tf32(di, A(0), B(3), ID, 1);
-            tc::mma_tf32(di, A(1), B(2), ID, 1);
-            tc::mma_tf32(di, A(2), B(0), ID, 1);
-            tc::mma_tf32(di, A(2), B(1), ID, 1);
-            tc::mma_tf32(di, A(3), B(0), ID, 1);
-          } else if constexpr (A_CPLX) {
-            // real B (planes 0 hi, 1 lo)
-            tc::mma_tf32(dr, A(0), B(0), ID, acc0);
-            tc::mma_tf32(dr, A(0), B(1), ID, 1);
-            tc::mma_tf32(dr, A(1), B(0), ID, 1);
-            tc::mma_tf32(di, A(2), B(0), ID, acc0);
-            tc::mma_tf32(di, A(2), B(1), ID, 1);
-            tc::mma_tf32(di, A(3), B(0), ID, 1);
-          } else {
-            // real A, complex B
-            tc::mma_tf32(dr, A(0), B(0), ID, acc0);
-            tc::mma_tf32(dr, A(0), B(1), ID, 1);
-            tc::mma_tf32(dr, A(1), B(0), ID, 1);
-            tc::mma_tf32(di, A(0), B(2), ID, acc0);
-            tc::mma_tf32(di, A(0), B(3), ID, 1);
-            tc::mma_tf32(di, A(1), B(2), ID, 1);
+      for (long t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++ti) {
+        const int buf = int(ti & 1);
+        if (ti >= 2) {
+          if (!tc::mbar_wait(&acc_empty[buf], unsigned((ti / 2) - 1) & 1u, p.err, abort_flag)) {
+            ok = false;
+            break;
           }
         }
-        tc::mma_commit(&empty[s]);  // stage reusable once these MMAs have read it
+        tc::tc_fence_after();
+        const uint32_t dr = taddr + uint32_t(buf * 2 * BN), di = dr + BN;
+        for (int kc = 0; kc < nk; ++kc, ++it) {
+          const int s = int(it % STAGES);
+          if (!tc::mbar_wait(&full[s], unsigned(it / STAGES) & 1u, p.err, abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc::tc_fence_after();
+          unsigned char* st = base + size_t(s) * K::STAGE;
+          const uint32_t sa = tc::smem_u32(st);
+          const uint32_t sb = tc::smem_u32(st + K::NA * K::A_TILE);
+#pragma unroll
+          for (int kk = 0; kk < BK / 8; ++kk) {
+            // +32 bytes per K=8 step inside the 128-byte swizzle row (descriptor units of 16 B)
+            auto A = [&](int q) { return tc::sdesc_sw128(sa + q * K::A_TILE) + uint64_t(2 * kk); };
+            auto B = [&](int q) { return tc::sdesc_sw128(sb + q * K::B_TILE) + uint64_t(2 * kk); };
+            const uint32_t acc0 = (kc > 0 || kk > 0) ? 1u : 0u;
+            if constexpr (A_CPLX && B_CPLX) {
+              // Dr = Ar Br - Ai Bi ; Di = Ar Bi + Ai Br  (planes 0 re_hi, 1 re_lo, 2 im_hi, 3 im_lo)
+              tc::mma_tf32(dr, A(0), B(0), ID, acc0);
+              tc::mma_tf32(dr, A(0), B(1), ID, 1);
+              tc::mma_tf32(dr, A(1), B(0), ID, 1);
+              tc::mma_tf32(dr, A(2), B(2), IDN, 1);
+              tc::mma_tf32(dr, A(2), B(3), IDN, 1);
+              tc::mma_tf32(dr, A(3), B(2), IDN, 1);
+              tc::mma_tf32(di, A(0), B(2), ID, acc0);
+              tc::mma_tf32(di, A(0), B(3), ID, 1);
+              tc::mma_tf32(di, A(1), B(2), ID, 1);
+              tc::mma_tf32(di, A(2), B(0), ID, 1);
+              tc::mma_tf32(di, A(2), B(1), ID, 1);
+              tc::mma_tf32(di, A(3), B(0), ID, 1);
+            } else if constexpr (A_CPLX) {
+              // real B (planes 0 hi, 1 lo)
+              tc::mma_tf32(dr, A(0), B(0), ID, acc0);
+              tc::mma_tf32(dr, A(0), B(1), ID, 1);
+              tc::mma_tf32(dr, A(1), B(0), ID, 1);
+              tc::mma_tf32(di, A(2), B(0), ID, acc0);
+              tc::mma_tf32(di, A(2), B(1), ID, 1);
+              tc::mma_tf32(di, A(3), B(0), ID, 1);
+            } else {
+              // real A, complex B
+              tc::mma_tf32(dr, A(0), B(0), ID, acc0);
+              tc::mma_tf32(dr, A(0), B(1), ID, 1);
+              tc::mma_tf32(dr, A(1), B(0), ID, 1);
+              tc::mma_tf32(di, A(0), B(2), ID, acc0);
+              tc::mma_tf32(di, A(0), B(3), ID, 1);
+              tc::mma_tf32(di, A(1), B(2), ID, 1);
+            }
+          }
+          tc::mma_commit(&empty[s]);  // stage reusable once these MMAs have read it
+        }
+        if (!ok) break;
+        tc::mma_commit(&acc_full[buf]);
       }
-      if (ok) tc::mma_commit(accb);  // on an aborted run the epilogue leaves through the flag
     }
   } else {
     // epilogue warps 2..5: TMEM lane quarter = warp % 4
     const int q = warp & 3;
-    const bool ok = tc::mbar_wait(accb, 0, p.err, abort_flag);
-    tc::tc_fence_after();
-    if (ok) {
-      const int row = m0 + q * 32 + lane;
-      const uint32_t trow = taddr + (uint32_t(q * 32) << 16);
+    long ti = 0;
+    for (long t = blockIdx.x; t < ntiles; t += gridDim.x, ++ti) {
+      int mt, nt, z;
+      tc_tile(t, MT, NT, p.order, mt, nt, z);
+      const int buf = int(ti & 1);
+      const bool ok = tc::mbar_wait(&acc_full[buf], unsigned(ti / 2) & 1u, p.err, abort_flag);
+      tc::tc_fence_after();
+      if (!ok) break;
+      const int row = mt * 128 + q * 32 + lane;
+      const int n0 = nt * BN;
+      const uint32_t trow = taddr + (uint32_t(q * 32) << 16) + uint32_t(buf * 2 * BN);
 #pragma unroll 1
       for (int c0 = 0; c0 < BN; c0 += 16) {
         float vr[16], vi[16];
         tc::tmem_ld16(trow + c0, vr);
         tc::tmem_ld16(trow + BN + c0, vi);
         tc::tmem_ld_wait();
+        if (c0 + 16 >= BN) {
+          tc::tc_fence_before();
+          tc::mbar_arrive(&acc_empty[buf]);  // accumulator free for tile ti+2
+        }
         if (row >= p.m) continue;
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int col = n0 + c0 + j;
           if (col >= p.n) break;
-          // alpha * (vr + i vi)
           const float ar = float(p.alpha.x), ai = float(p.alpha.y);
           const float xr = ar * vr[j] - ai * vi[j];
           const float xi = ar * vi[j] + ai * vr[j];
@@ -409,11 +463,15 @@ int launch_tc(cudaStream_t s, TcParams& p, int batch) {
   auto kern = tc_cgemm_kernel<A_CPLX, B_CPLX, BN, STAGES, EPI>;
   AFQMC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(K::SMEM)));
-  if (batch > 65535) {
-    set_error_detail("launch_tc: batch %d exceeds the grid limit", batch);
-    return AFQMC_ERR_SHAPE;
+  p.batch = batch;
+  static int nsm = 0;
+  if (nsm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   }
-  dim3 grid(ceil_div(p.m, 128), ceil_div(p.n, BN), batch);
+  const long ntiles = long(ceil_div(p.m, 128)) * ceil_div(p.n, BN) * batch;
+  const int grid = int(ntiles < nsm ? ntiles : nsm);
   kern<<<grid, TC_THREADS, K::SMEM, s>>>(p);
   return launch_status("tc_cgemm_kernel");
 }
@@ -544,6 +602,7 @@ int vbias_mixed(cudaStream_t s, MixedHam* m, const c128* G, long ldG, c128* v, i
       AFQMC_TRY(make_map(&p.a[q], m->G.p[q] + off, K, W, m->G.ld, 1, long(W) * m->G.ld, 128));
     AFQMC_TRY(maps_for(m->Lnak[sp], p.b, m->lnak_cplx ? 64 : 128));
     p.m = W; p.n = m->Nc; p.k = int(K);
+    p.order = 1;  // a G tile (128 walkers x K) stays in L2 while the Lnak tiles stream past it
     p.alpha = cmk(a, 0);
     p.out_c = v; p.outc_ld = m->Nc; p.outc_bs = 0;
     p.err = m->err;

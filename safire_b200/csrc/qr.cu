@@ -1,156 +1,130 @@
-// Batched Householder QR re-orthonormalisation of the walkers' Slater matrices.
+// Batched re-orthonormalisation of the walkers' Slater matrices.
 //
 // Reference: det_ops::orthogonalize (src/AFQMC/SlaterDeterminantOperations/orthogonalize.hpp:
 // 131-169) calls LAPACK geqrf + ungqr on each S_w (M x N) and multiplies column i of Q by
 // scl_i = sign(Re R_ii) (log_determinant_from_geqrf, numerics/operations/determinants_impl.hpp:
 // 77-108).  The result is the unique Q whose R has a real positive diagonal, so any stable QR gives
-// the same walker; this kernel restates geqrf's reflectors (zlarfg convention: beta real,
-// H = I - tau v v^H with v_0 = 1) and ungqr's backward accumulation (zung2r) in shared memory.
-// One CTA per walker; the whole M x N matrix lives in shared memory (M*N <= 13.5k elements).
+// the same walker.  Here: CholeskyQR2 — the Gram matrices S^H S and the products S R^{-1} run as
+// batched DMMA GEMMs, the N x N Cholesky factorisations and triangular inverses in one CTA per
+// walker; two passes make Q orthonormal to rounding for the well-conditioned matrices that periodic
+// re-orthogonalisation keeps.
 #include "detops.cuh"
+#include "zgemm.cuh"
 
 namespace afqmc {
 namespace {
 
-constexpr int QR_THREADS = 256;
-constexpr int QR_WARPS = QR_THREADS / 32;
+// ---------------------------------------------------------------------------------------------
+// CholeskyQR: G = S^H S = R^H R (R upper, real positive diagonal), Rinv = R^{-1}; one CTA per
+// walker, the N x N matrices in shared memory.  logdetR[w] += sum_i log R_ii.
+// ---------------------------------------------------------------------------------------------
+constexpr int CH_THREADS = 256;
 
-__device__ __forceinline__ double block_sum(double v, double* red) {
-  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  __syncthreads();
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  double t = 0.0;
-  if (threadIdx.x == 0) {
-    for (int q = 0; q < QR_WARPS; ++q) t += red[q];
-    red[QR_WARPS] = t;
-  }
-  __syncthreads();
-  return red[QR_WARPS];
-}
-
-// A(k:M, k+1:N) <- (I - ctau v v^H) A(k:M, k+1:N), v = [1, a(k+1:M, k)]
-__device__ void apply_reflector(c128* a, int pitch, int M, int N, int k, c128 ctau, c128* wbuf) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int j = k + 1 + warp; j < N; j += QR_WARPS) {
-    c128 acc = cmk(0, 0);
-    for (int i = k + lane; i < M; i += 32) {
-      c128 v = (i == k) ? cmk(1, 0) : a[i * pitch + k];
-      acc = cadd(acc, cmul(cconj(v), a[i * pitch + j]));
-    }
-    for (int off = 16; off > 0; off >>= 1) {
-      acc.x += __shfl_down_sync(0xffffffffu, acc.x, off);
-      acc.y += __shfl_down_sync(0xffffffffu, acc.y, off);
-    }
-    if (lane == 0) wbuf[j] = cmul(ctau, acc);
-  }
-  __syncthreads();
-  const int ncol = N - k - 1, nrow = M - k;
-  for (int e = threadIdx.x; e < ncol * nrow; e += QR_THREADS) {
-    int i = k + e / ncol, j = k + 1 + e % ncol;
-    c128 v = (i == k) ? cmk(1, 0) : a[i * pitch + k];
-    a[i * pitch + j] = csub(a[i * pitch + j], cmul(v, wbuf[j]));
-  }
-  __syncthreads();
-}
-
-__global__ void __launch_bounds__(QR_THREADS)
-    qr_orthogonalize_kernel(c128* __restrict__ S, long ldS, c128* __restrict__ logdetR, int M,
-                            int N) {
+__global__ void __launch_bounds__(CH_THREADS)
+    chol_inv_kernel(const c128* __restrict__ Gram, c128* __restrict__ Rinv, c128* __restrict__ logdetR,
+                    int N) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int pitch = N | 1;  // odd pitch: conflict-free column walks of 16-byte elements
-  c128* a = reinterpret_cast<c128*>(smem_raw);
-  // 16-byte arrays first, the 8-byte diagonal last (keeps every c128 16-byte aligned)
-  c128* tau = a + size_t(M) * pitch;                    // [N]
-  c128* wbuf = tau + N;                                 // [N]
-  double* rdiag = reinterpret_cast<double*>(wbuf + N);  // [N]
-  __shared__ double red[QR_WARPS + 1];
-
+  const int PP = N | 1;
+  c128* a = reinterpret_cast<c128*>(smem_raw);  // [N][PP]  -> R (upper)
+  c128* x = a + size_t(N) * PP;                 // [N][PP]  -> R^{-1}
+  double* dg = reinterpret_cast<double*>(x + size_t(N) * PP);  // [N] R_ii
   const long w = blockIdx.x;
-  c128* Sw = S + w * ldS;
-  for (int e = threadIdx.x; e < M * N; e += QR_THREADS) a[(e / N) * pitch + e % N] = Sw[e];
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const c128* Gw = Gram + w * long(N) * N;
+  for (int i = ty; i < N; i += CH_THREADS / 32)
+    for (int j = tx; j < N; j += 32) {
+      a[i * PP + j] = Gw[long(i) * N + j];
+      x[i * PP + j] = cmk(0, 0);
+    }
   __syncthreads();
-
-  // ---- geqrf (zgeqr2): reflectors stored below the diagonal ----
-  for (int k = 0; k < N; ++k) {
-    double part = 0.0;
-    for (int i = k + 1 + threadIdx.x; i < M; i += QR_THREADS) {
-      c128 x = a[i * pitch + k];
-      part += x.x * x.x + x.y * x.y;
-    }
-    const double xnorm2 = block_sum(part, red);
-    const c128 alpha = a[k * pitch + k];
-    c128 t = cmk(0, 0);
-    double beta = alpha.x;
-    if (!(xnorm2 == 0.0 && alpha.y == 0.0)) {
-      beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2), alpha.x);
-      t = cmk((beta - alpha.x) / beta, -alpha.y / beta);
-      const c128 scal = cdiv(cmk(1, 0), cmk(alpha.x - beta, alpha.y));
-      for (int i = k + 1 + threadIdx.x; i < M; i += QR_THREADS)
-        a[i * pitch + k] = cmul(a[i * pitch + k], scal);
-    }
-    if (threadIdx.x == 0) {
-      tau[k] = t;
-      rdiag[k] = beta;
-    }
+  // right-looking Cholesky on the upper triangle: row j <- row j / sqrt(a_jj); trailing update
+  for (int j = 0; j < N; ++j) {
+    double d = a[j * PP + j].x;
+    d = d > 1e-300 ? sqrt(d) : 1e-150;
+    const double dinv = 1.0 / d;
     __syncthreads();
-    // apply H^H = I - conj(tau) v v^H to the trailing columns
-    if (k < N - 1 && (t.x != 0.0 || t.y != 0.0)) apply_reflector(a, pitch, M, N, k, cconj(t), wbuf);
-  }
-
-  // ---- log det R with the sign fix ----
-  if (threadIdx.x == 0) {
-    const double small = 2.2250738585072014e-308;
-    c128 res = logdetR[w];
-    for (int k = 0; k < N; ++k) {
-      double scl = rdiag[k] < 0.0 ? -1.0 : 1.0;
-      res = cadd(res, clog(cmk(scl * rdiag[k] + small, 0.0)));
-    }
-    logdetR[w] = res;
-  }
-
-  // ---- ungqr (zung2r): form Q in place, backward over the reflectors ----
-  for (int k = N - 1; k >= 0; --k) {
-    const c128 t = tau[k];
-    if (k < N - 1 && (t.x != 0.0 || t.y != 0.0)) apply_reflector(a, pitch, M, N, k, t, wbuf);
-    // column k of Q: [0..k-1] = 0, [k] = 1 - tau, [k+1..M-1] = -tau v
-    for (int i = threadIdx.x; i < M; i += QR_THREADS) {
-      c128 q;
-      if (i < k) q = cmk(0, 0);
-      else if (i == k) q = cmk(1.0 - t.x, -t.y);
-      else q = cmul(cmk(-t.x, -t.y), a[i * pitch + k]);
-      a[i * pitch + k] = q;
+    if (tid == 0) dg[j] = d;
+    for (int l = j + 1 + tid; l < N; l += CH_THREADS) a[j * PP + l] = cscale(a[j * PP + l], dinv);
+    __syncthreads();
+    // A_il -= conj(R_ji) R_jl  for j < i <= l
+    for (int i = j + 1 + ty; i < N; i += CH_THREADS / 32) {
+      const c128 rji = cconj(a[j * PP + i]);
+      for (int l = i + tx; l < N; l += 32) a[i * PP + l] = csub(a[i * PP + l], cmul(rji, a[j * PP + l]));
     }
     __syncthreads();
   }
-
-  // S <- Q diag(scl)
-  for (int e = threadIdx.x; e < M * N; e += QR_THREADS) {
-    int i = e / N, j = e % N;
-    double scl = rdiag[j] < 0.0 ? -1.0 : 1.0;
-    Sw[e] = cscale(a[i * pitch + j], scl);
+  // R^{-1}: back substitution row by row, thread = column c
+  for (int i = N - 1; i >= 0; --i) {
+    for (int c = i + tid; c < N; c += CH_THREADS) {
+      c128 acc = cmk(i == c ? 1.0 : 0.0, 0.0);
+      for (int l = i + 1; l <= c; ++l) acc = csub(acc, cmul(a[i * PP + l], x[l * PP + c]));
+      x[i * PP + c] = cscale(acc, 1.0 / dg[i]);
+    }
+    __syncthreads();
+  }
+  c128* Rw = Rinv + w * long(N) * N;
+  for (int i = ty; i < N; i += CH_THREADS / 32)
+    for (int j = tx; j < N; j += 32) Rw[long(i) * N + j] = x[i * PP + j];
+  if (ty == 0) {
+    double sr = 0.0;
+    for (int i = tx; i < N; i += 32) sr += log(dg[i]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sr += __shfl_xor_sync(0xffffffffu, sr, off);
+    if (tx == 0) logdetR[w] = cadd(logdetR[w], cmk(sr, 0.0));
   }
 }
 
 }  // namespace
 
-int orthogonalize(cudaStream_t s, c128* S, long ldS, c128* logdetR, int W, int M, int N) {
+// One CholeskyQR pass: Q = S R^{-1} written to Q (ldQ), R from the Gram matrix of S.
+static int cholqr_pass(cudaStream_t s, const c128* S, long ldS, c128* Q, long ldQ, c128* logdetR,
+                       int W, int M, int N, c128* gram, c128* rinv) {
+  GemmParams g{};
+  g.m = N; g.n = N; g.k = M;
+  g.A = S; g.lda = N; g.strideA = ldS;  // A^H with A stored [M][N]
+  g.B = S; g.ldb = N; g.strideB = ldS;
+  g.C = gram; g.ldc = N; g.strideC = long(N) * N;
+  g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+  AFQMC_TRY(zgemm(s, W, GH, false, GN, false, g));
+  const int PP = N | 1;
+  const size_t smem = 2 * size_t(N) * PP * sizeof(c128) + N * sizeof(double);
+  AFQMC_CUDA_TRY(cudaFuncSetAttribute(chol_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(smem)));
+  chol_inv_kernel<<<W, CH_THREADS, smem, s>>>(gram, rinv, logdetR, N);
+  AFQMC_TRY(launch_status("chol_inv_kernel"));
+  GemmParams q{};
+  q.m = M; q.n = N; q.k = N;
+  q.A = S; q.lda = N; q.strideA = ldS;
+  q.B = rinv; q.ldb = N; q.strideB = long(N) * N;
+  q.C = Q; q.ldc = N; q.strideC = ldQ;
+  q.alpha = cmk(1, 0); q.beta = cmk(0, 0);
+  return zgemm(s, W, GN, false, GN, false, q);
+}
+
+// det_ops::orthogonalize by CholeskyQR2: two passes give Q orthonormal to rounding for the
+// well-conditioned walkers that the periodic re-orthogonalisation keeps; R = R2 R1 has a real
+// positive diagonal, so Q is the same unique factor as geqrf + ungqr + sign fix.
+int orthogonalize(cudaStream_t s, c128* S, long ldS, c128* logdetR, int W, int M, int N,
+                  c128* work) {
   if (W <= 0 || N <= 0 || M <= 0) return AFQMC_OK;
   if (N > M) {
     set_error_detail("orthogonalize: N = %d > M = %d", N, M);
     return AFQMC_ERR_SHAPE;
   }
-  const int pitch = N | 1;
-  size_t smem = size_t(M) * pitch * sizeof(c128) + N * (2 * sizeof(c128) + sizeof(double));
-  if (smem > 227 * 1024) {
-    set_error_detail("orthogonalize: M*N = %d x %d exceeds the shared-memory QR kernel", M, N);
+  if (2 * size_t(N | 1) * N * sizeof(c128) > 227 * 1024) {
+    set_error_detail("orthogonalize: N = %d exceeds the shared-memory Cholesky kernel", N);
     return AFQMC_ERR_UNSUPPORTED;
   }
-  AFQMC_CUDA_TRY(cudaFuncSetAttribute(qr_orthogonalize_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  qr_orthogonalize_kernel<<<W, QR_THREADS, smem, s>>>(S, ldS, logdetR, M, N);
-  return launch_status("qr_orthogonalize_kernel");
+  const size_t nQ = size_t(W) * M * N, nG = size_t(W) * N * N;
+  void* buf = work;
+  if (!buf) AFQMC_CUDA_TRY(cudaMallocAsync(&buf, sizeof(c128) * (nQ + 2 * nG), s));
+  c128* Q = static_cast<c128*>(buf);
+  c128* gram = Q + nQ;
+  c128* rinv = gram + nG;
+  int st = cholqr_pass(s, S, ldS, Q, long(M) * N, logdetR, W, M, N, gram, rinv);
+  if (!st) st = cholqr_pass(s, Q, long(M) * N, S, ldS, logdetR, W, M, N, gram, rinv);
+  if (!work) cudaFreeAsync(buf, s);
+  return st;
 }
 
 }  // namespace afqmc

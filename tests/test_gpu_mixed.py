@@ -117,3 +117,21 @@ def test_energy_mixed_large_block(cuda):
     print("energy mixed N=50 rel errs", ["%.2e" % e for e in errs])
     assert max(errs[1:]) < TOL_ONE
     assert dham.device_error_flag() == 0
+
+
+def test_exchange_single_tf32_error(cuda):
+    """Plain-TF32 exchange (one product per real product): error reported against FP64."""
+    from safire_b200 import afqmc as A
+    wl = make_workload("cfg2", W=6, Nc=64)
+    dham, oham, _ = make_pair(wl)
+    dham.set_exchange_split(1)
+    rs = np.random.default_rng(5)
+    G = rand_c(rs, 6, wl.nup * wl.M, scale=0.1)
+    E = torch.zeros((6, 3), dtype=torch.complex128, device="cuda")
+    dham.energy(E, to_dev(G), precision=A.PREC_MIXED)
+    Eo = oham.energy(G)
+    Ed = to_host(E)
+    errs = [rel_err(Ed[:, q], Eo[:, q]) for q in range(1, 3)]
+    print("energy 1xTF32 exchange rel errs EXX/EJ", ["%.2e" % e for e in errs])
+    assert max(errs) < 2e-3
+    dham.set_exchange_split(3)
