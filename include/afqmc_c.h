@@ -165,6 +165,11 @@ int afqmc_ham_energy(afqmc_ham ham, const afqmc_c128* G, afqmc_c128* E, int W, i
  * default) or 1 (plain TF32, for runs whose energy tolerance allows it). */
 int afqmc_ham_set_exchange_split(afqmc_ham ham, int nsplit);
 
+/* Mixed-precision Taylor propagation: 1 (default) runs all order + 2 products of each walker in
+ * one persistent tensor-core kernel (M <= 256 orbitals, N <= 64 electrons per spin); 0 launches
+ * one batched GEMM per product.  Both compute the same sums. */
+int afqmc_ham_set_taylor_fused(afqmc_ham ham, int fused);
+
 /* Error word of the tensor-core kernels' bounded device waits (bit 0: a wait on a TMA or MMA
  * completion gave up after about 2 s and the kernel returned without finishing).  0 = none, or
  * the mixed-precision path was never used.  Synchronous. */

@@ -219,20 +219,24 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
       const uint32_t trow = taddr + (uint32_t(q * 32) << 16) + uint32_t(buf * 2 * XBN);
 #pragma unroll 1
       for (int nl = 0; nl < 2; ++nl) {
-        // stage this walker's row b of T_n (columns a) in shared memory, 8 columns at a time
+        // stage this walker's row b of T_n (columns a) in shared memory: all fourteen TMEM
+        // loads of the slot are issued before one wait
         const int r = (wl * N + b) * PITCH;
-#pragma unroll 1
-        for (int c = 0; c < XSLOT_B; c += 8) {
-          float vr[8], vi[8];
-          tmem_ld8(trow + nl * XSLOT_B + c, vr);
-          tmem_ld8(trow + XBN + nl * XSLOT_B + c, vi);
+        {
+          float vr[XSLOT_B], vi[XSLOT_B];
+          const uint32_t cr = trow + nl * XSLOT_B, ci = trow + XBN + nl * XSLOT_B;
+#pragma unroll
+          for (int c = 0; c < XSLOT_B; c += 8) {
+            tmem_ld8(cr + c, vr + c);
+            tmem_ld8(ci + c, vi + c);
+          }
           tc::tmem_ld_wait();
           if (valid) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
-              if (c + j < N) {
-                sre[r + c + j] = vr[j];
-                sim[r + c + j] = vi[j];
+            for (int a = 0; a < XSLOT_B; ++a)
+              if (a < N) {
+                sre[r + a] = vr[a];
+                sim[r + a] = vi[a];
               }
           }
         }

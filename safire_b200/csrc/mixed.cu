@@ -489,6 +489,7 @@ struct MixedHam {
   // dynamic operands, sized on demand
   int capW = 0;
   int exchange_split = 3;  // TF32 products per real product in the exchange contraction
+  bool taylor_unfused = false;  // true: one GEMM launch per Taylor product
   Planes G;         // [W][1][nel_tot*M]  (A of vbias);  exchange view [W*nel][M]
   Planes X;         // [1][W][Nc] (A of vHS)
   unsigned* err = nullptr;
@@ -696,6 +697,11 @@ int vhs_mixed(cudaStream_t s, MixedHam* m, const c128* X, c128* V, int W, double
   return AFQMC_OK;
 }
 
+int taylor_fused_tc(cudaStream_t s, const float* const P1p[2], const float* const Vp[4], long ldV,
+                    const float* const Sp[4], float* const Tp0[4], float* const Tp1[4],
+                    float* const Rp[4], long pl_ld, c128* S, long ldS, int W, int M, int N,
+                    int order, unsigned* err);
+
 // Taylor propagation S <- P1 sum_n (iV)^n/n! P1 S (propagate.hpp:238-298) on the split planes.
 // V must have been produced by vhs_mixed (planes kept in MixedHam) for the same walkers.
 int propagate_mixed(cudaStream_t s, MixedHam* m, const void* P1, bool p1_real, c128* S, long ldS,
@@ -717,6 +723,14 @@ int propagate_mixed(cudaStream_t s, MixedHam* m, const void* P1, bool p1_real, c
   }
   // S^T planes [W][N][M] from the walkers' Slater matrices [W][M][N]
   AFQMC_TRY(split_complex(s, S, N, ldS, W, M, N, m->Sst, true));
+  if (M <= 256 && N <= 64 && !m->taylor_unfused && m->P1.ld == m->T0.ld) {
+    // one persistent kernel runs all order + 2 products of each walker
+    const float* p1p[2] = {m->P1.p[0], m->P1.p[1]};
+    const float* vp[4] = {m->V.p[0], m->V.p[1], m->V.p[2], m->V.p[3]};
+    const float* sp[4] = {m->Sst.p[0], m->Sst.p[1], m->Sst.p[2], m->Sst.p[3]};
+    return taylor_fused_tc(s, p1p, vp, m->V.ld, sp, m->T0.p, m->T1.p, m->Tacc_split.p, m->T0.ld,
+                           S, ldS, W, M, N, order, m->err);
+  }
   Planes* Tin = &m->T0;
   Planes* Tout = &m->T1;
   // T0 = P1 S  (acc = T0)
@@ -760,6 +774,11 @@ int propagate_mixed(cudaStream_t s, MixedHam* m, const void* P1, bool p1_real, c
     p.err = m->err;
     AFQMC_TRY((launch_tc<false, true, 64, 3, EPI_S64>(s, p, W)));
   }
+  return AFQMC_OK;
+}
+
+int mixed_set_taylor_fused(MixedHam* m, bool fused) {
+  m->taylor_unfused = !fused;
   return AFQMC_OK;
 }
 

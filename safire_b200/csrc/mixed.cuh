@@ -17,6 +17,9 @@ int vhs_mixed(cudaStream_t s, MixedHam* m, const c128* X, c128* V, int W, double
 // S <- P1 exp_T(iV) P1 S with V from the last vhs_mixed call (P1 real float64 [M][M])
 int propagate_mixed(cudaStream_t s, MixedHam* m, const void* P1, bool p1_real, c128* S, long ldS,
                     int W, int M, int N, int order);
+// true (default): all Taylor products of a walker in one persistent kernel (M <= 256, N <= 64);
+// false: one batched GEMM launch per product
+int mixed_set_taylor_fused(MixedHam* m, bool fused);
 // split planes of G for the exchange-energy GEMMs
 int mixed_prepare_G(cudaStream_t s, MixedHam* m, const c128* G, long ldG, int W);
 // T [(w,b)][(n,a)] for walkers [w0, w0+wc) of spin block sp (complex128, the chunk layout of

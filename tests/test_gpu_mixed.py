@@ -135,3 +135,37 @@ def test_exchange_single_tf32_error(cuda):
     print("energy 1xTF32 exchange rel errs EXX/EJ", ["%.2e" % e for e in errs])
     assert max(errs) < 2e-3
     dham.set_exchange_split(3)
+
+
+def _mixed_steps(wl, dham, fused, nsteps=2, order=None):
+    from safire_b200 import afqmc as A
+    W = wl.W
+    dham.set_taylor_fused(fused)
+    ws = A.WalkerSet(wl.walker_type, wl.M, wl.nup, wl.ndn, W)
+    ws.init_from_trial(dham)
+    kw = {} if order is None else {"taylor_n": order}
+    prop = A.Propagator(dham, A.default_params(dt=wl.dt, precision=A.PREC_MIXED, **kw), W)
+    u = O.HostRandomGenerator(O.split_seed(0, 0, 7)).sample_uniform(W * wl.Nc)
+    ud = to_dev(u.reshape(W, wl.Nc), torch.float64)
+    for _ in range(nsteps):
+        prop.Propagate(ws, -30.0, ud)
+    torch.cuda.synchronize()
+    dham.set_taylor_fused(True)
+    return to_host(ws.SlaterMatrices(0)), to_host(ws.properties())
+
+
+@pytest.mark.parametrize("name,W,Nc,order", [("cfg1", 300, None, None), ("cfg1", 20, None, 0),
+                                             ("cfg2", 6, 40, None)])
+def test_taylor_fused_vs_per_term(cuda, name, W, Nc, order):
+    """The persistent Taylor kernel (all products of a walker in one CTA) against one GEMM launch
+    per product: same split arithmetic, different kernels; W = 300 runs several walkers per CTA."""
+    kw = {"W": W} if Nc is None else {"W": W, "Nc": Nc}
+    wl = make_workload(name, **kw)
+    dham, _, _ = make_pair(wl)
+    Sf, pf = _mixed_steps(wl, dham, True, order=order)
+    Su, pu = _mixed_steps(wl, dham, False, order=order)
+    eS = rel_err(Sf, Su)
+    eO = rel_err(pf[:, O.OVLP], pu[:, O.OVLP])
+    print(f"fused vs per-term Taylor ({name}, W={W}, order={order}): S {eS:.2e} ovlp {eO:.2e}")
+    assert eS < 1e-5 and eO < 1e-5
+    assert dham.device_error_flag() == 0
