@@ -165,9 +165,224 @@ __global__ void __launch_bounds__(GJ_THREADS) gj_logdet_kernel(const c128* __res
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Register-resident Gauss-Jordan / LU for N <= 64 (the production sizes).  One CTA of 64 C threads
+// per matrix (C = 2 column classes up to N = 32, else 4); thread t holds row i = t % 64 and the
+// columns j = h + C q of class h = t / 64 in registers (q < QMAX), so a step touches shared memory
+// only for the pivot column, the scaled pivot row and the row that moves in the interchange.
+// Step k: every warp finds the pivot p (first max |re|+|im| in column k, rows k..N-1, as izamax)
+// from the column buffer; the owners of row p write it scaled by 1/pivot (with 1/pivot in column
+// k), the owners of row k write the old row k; after one barrier every row i != k subtracts
+// f_i * (scaled pivot row), f_i being its column-k element before the interchange, and row p takes
+// the old row k first; column k, moved to the column buffer and zeroed in the registers at the end
+// of step k-1, becomes -f_i/pivot (the in-place Gauss-Jordan inverse), row k the scaled pivot row.  Without the inverse only rows below k are eliminated (plain LU; the pivots
+// are the same U diagonal).  The row interchanges permute the columns of the in-place inverse;
+// they are undone on the way out (columns swapped in reverse step order).  Two barriers a step.
+// ---------------------------------------------------------------------------------------------
+template <int QMAX, int C, bool INVERT>
+__global__ void __launch_bounds__(64 * C, C == 2 ? 3 : 2) gj_reg_kernel(const c128* __restrict__ A,
+                                                               long strideA,
+                                                               c128* __restrict__ Ainv,
+                                                               long strideInv,
+                                                               c128* __restrict__ ovlp, int N,
+                                                               c128 post_scale, c128 post_add) {
+  __shared__ c128 rowbuf[64];     // pivot row * (1/pivot), column k = 1/pivot
+  __shared__ c128 kbuf[64];       // old row k (moves to row p)
+  __shared__ c128 colbuf[2][64];  // column k of every row at step k (buffer k & 1)
+  __shared__ c128 piv_val[64];
+  __shared__ int perm[64];
+  __shared__ int pos[64];
+  __shared__ int s_singular;
+
+  const int t = threadIdx.x;
+  const int i = t & 63;
+  const int h = t >> 6;  // column class: columns j = h + C q
+  const int lane = t & 31;
+  const bool row_ok = i < N;
+  const long w = blockIdx.x;
+  const c128* Aw = A + w * strideA;
+
+  c128 a[QMAX];
+#pragma unroll
+  for (int q = 0; q < QMAX; ++q) {
+    const int j = h + C * q;
+    a[q] = (row_ok && j < N) ? Aw[long(i) * N + j] : cmk(0.0, 0.0);
+  }
+  if (h == 0) {
+    if (row_ok) colbuf[0][i] = a[0];
+    a[0] = cmk(0.0, 0.0);
+  }
+  if (t == 0) s_singular = 0;
+  __syncthreads();
+
+  for (int k = 0; k < N; ++k) {
+    const c128* col = colbuf[k & 1];
+    double best = -1.0;
+    int bi = N;
+    for (int r = k + lane; r < N; r += 32) {
+      const double v = cabs1(col[r]);
+      if (v > best) {
+        best = v;
+        bi = r;
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, best, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+      if (ov > best || (ov == best && oi < bi)) {
+        best = ov;
+        bi = oi;
+      }
+    }
+    const int p = bi;
+    const bool zero = !(best > 0.0);
+    const c128 piv = col[p];
+    if (t == 0) {
+      perm[k] = p;
+      piv_val[k] = piv;
+      if (zero) s_singular = 1;
+    }
+    if (!zero) {
+      if (i == p) {
+        const c128 dinv = cdiv(cmk(1.0, 0.0), piv);
+#pragma unroll
+        for (int q = 0; q < QMAX; ++q) {
+          const int j = h + C * q;
+          if (j < N) rowbuf[j] = cmul(a[q], dinv);
+        }
+        if (h == (k % C)) rowbuf[k] = dinv;
+      }
+      if (i == k && p != k) {
+#pragma unroll
+        for (int q = 0; q < QMAX; ++q) {
+          const int j = h + C * q;
+          if (j < N) kbuf[j] = a[q];
+        }
+      }
+    }
+    __syncthreads();
+    c128* nxt = colbuf[(k + 1) & 1];
+    const int kn = k + 1;
+    if (!zero && row_ok) {
+      if (i == k) {
+        if (INVERT) {
+#pragma unroll
+          for (int q = 0; q < QMAX; ++q) {
+            const int j = h + C * q;
+            if (j < N) a[q] = rowbuf[j];
+          }
+        }
+      } else if (INVERT || i > k) {
+        const c128 f = (i == p) ? col[k] : col[i];
+        if (i == p) {
+#pragma unroll
+          for (int q = 0; q < QMAX; ++q) {
+            const int j = h + C * q;
+            if (j < N) a[q] = kbuf[j];
+          }
+        }
+        const c128 nf = cmk(-f.x, -f.y);
+#pragma unroll
+        for (int q = 0; q < QMAX; ++q) {
+          const int j = h + C * q;
+          if (j < N) {
+            const c128 r = rowbuf[j];
+            a[q].x = fma(nf.x, r.x, fma(f.y, r.y, a[q].x));
+            a[q].y = fma(nf.x, r.y, fma(nf.y, r.x, a[q].y));
+          }
+        }
+      }
+    }
+    // column k+1 moves to the column buffer for the next pivot search and is zeroed in the
+    // registers, so that step k+1's update leaves -f/pivot there (the in-place inverse's column)
+    if (kn < N && h == (kn % C)) {
+#pragma unroll
+      for (int q = 0; q < QMAX; ++q)
+        if (h + C * q == kn) {
+          if (row_ok) nxt[i] = a[q];
+          a[q] = cmk(0.0, 0.0);
+        }
+    }
+    __syncthreads();
+  }
+
+  if (t < 32) {
+    double sr = 0.0, si = 0.0;
+    for (int k = t; k < N; k += 32) {
+      const c128 l = log_pivot(piv_val[k], perm[k] != k);
+      sr += l.x;
+      si += l.y;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      sr += __shfl_xor_sync(0xffffffffu, sr, off);
+      si += __shfl_xor_sync(0xffffffffu, si, off);
+    }
+    if (t == 0) {
+      c128 res = cadd(ovlp[w], cmk(sr, si));
+      res = wrap_imag(res);
+      ovlp[w] = cadd(cmul(post_scale, res), post_add);
+    }
+  }
+  if (INVERT) {
+    // at[c] = column of the in-place result that ends in column c (kept in kbuf's memory,
+    // free after the last step); pos is its inverse
+    int* at = reinterpret_cast<int*>(kbuf);
+    if (t < N) at[t] = t;
+    __syncthreads();
+    if (t == 0)
+      for (int k = N - 1; k >= 0; --k) {
+        const int q = perm[k];
+        const int x = at[k];
+        at[k] = at[q];
+        at[q] = x;
+      }
+    __syncthreads();
+    if (t < N) pos[at[t]] = t;
+    __syncthreads();
+    const bool sing = s_singular != 0;
+    if (row_ok) {
+      c128* Iw = Ainv + w * strideInv + long(i) * N;
+#pragma unroll
+      for (int q = 0; q < QMAX; ++q) {
+        const int j = h + C * q;
+        if (j < N) Iw[pos[j]] = sing ? cmk(0.0, 0.0) : a[q];
+      }
+    }
+  }
+}
+
+template <int QMAX, int C>
+void launch_gj_reg(cudaStream_t s, const c128* A, long strideA, c128* Ainv, long strideInv,
+                   c128* ovlp, int W, int N, bool invert, c128 post_scale, c128 post_add) {
+  if (invert)
+    gj_reg_kernel<QMAX, C, true><<<W, 64 * C, 0, s>>>(A, strideA, Ainv, strideInv, ovlp, N,
+                                                      post_scale, post_add);
+  else
+    gj_reg_kernel<QMAX, C, false><<<W, 64 * C, 0, s>>>(A, strideA, nullptr, 0, ovlp, N,
+                                                       post_scale, post_add);
+}
+
 int batched_logdet_inverse(cudaStream_t s, const c128* A, long strideA, c128* Ainv, long strideInv,
                            c128* ovlp, int W, int N, bool invert, c128 post_scale, c128 post_add) {
   if (W <= 0 || N <= 0) return AFQMC_OK;
+  if (N <= 64) {
+    if (N <= 8)
+      launch_gj_reg<4, 2>(s, A, strideA, Ainv, strideInv, ovlp, W, N, invert, post_scale, post_add);
+    else if (N <= 16)
+      launch_gj_reg<8, 2>(s, A, strideA, Ainv, strideInv, ovlp, W, N, invert, post_scale, post_add);
+    else if (N <= 32)
+      launch_gj_reg<16, 2>(s, A, strideA, Ainv, strideInv, ovlp, W, N, invert, post_scale,
+                           post_add);
+    else if (N <= 52)
+      launch_gj_reg<13, 4>(s, A, strideA, Ainv, strideInv, ovlp, W, N, invert, post_scale,
+                           post_add);
+    else
+      launch_gj_reg<16, 4>(s, A, strideA, Ainv, strideInv, ovlp, W, N, invert, post_scale,
+                           post_add);
+    return launch_status("gj_reg_kernel");
+  }
   const int P = invert ? 2 * N : N;
   const int PP = P | 1;
   size_t smem = (size_t(N) * PP + 2 * size_t(P) + 2 * size_t(N)) * sizeof(c128) + N * sizeof(int);

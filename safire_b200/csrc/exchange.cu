@@ -247,16 +247,31 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
         const int n = 2 * np + nl;
         named_bar(1, 128);
         // x = sum_a T[b][a] T[a][b];  tr = T[b][b]   (rows of one warp all belong to walker wl)
+        // The sum over a runs in FP32 with four independent accumulator pairs (50 terms of
+        // products of FP32 inputs); the partial sums are widened to FP64 for every later sum.
         double v4[4] = {0.0, 0.0, 0.0, 0.0};
         if (valid && n < p.Nc) {
           const int col0 = wl * N * PITCH + b;
-#pragma unroll 5
-          for (int a = 0; a < N; ++a) {
-            const float tr_ = sre[r + a], ti_ = sim[r + a];                 // T[b][a]
-            const float ur = sre[col0 + a * PITCH], ui = sim[col0 + a * PITCH];  // T[a][b]
-            v4[0] += double(tr_) * ur - double(ti_) * ui;
-            v4[1] += double(tr_) * ui + double(ti_) * ur;
+          float xr[4] = {0.f, 0.f, 0.f, 0.f}, xi[4] = {0.f, 0.f, 0.f, 0.f};
+          int a = 0;
+#pragma unroll 2
+          for (; a + 4 <= N; a += 4) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const float tr_ = sre[r + a + j], ti_ = sim[r + a + j];  // T[b][a]
+              const float ur = sre[col0 + (a + j) * PITCH], ui = sim[col0 + (a + j) * PITCH];  // T[a][b]
+              xr[j] = fmaf(tr_, ur, fmaf(-ti_, ui, xr[j]));
+              xi[j] = fmaf(tr_, ui, fmaf(ti_, ur, xi[j]));
+            }
           }
+          for (; a < N; ++a) {
+            const float tr_ = sre[r + a], ti_ = sim[r + a];
+            const float ur = sre[col0 + a * PITCH], ui = sim[col0 + a * PITCH];
+            xr[0] = fmaf(tr_, ur, fmaf(-ti_, ui, xr[0]));
+            xi[0] = fmaf(tr_, ui, fmaf(ti_, ur, xi[0]));
+          }
+          v4[0] = (double(xr[0]) + double(xr[1])) + (double(xr[2]) + double(xr[3]));
+          v4[1] = (double(xi[0]) + double(xi[1])) + (double(xi[2]) + double(xi[3]));
           v4[2] = sre[r + b];
           v4[3] = sim[r + b];
         }

@@ -83,6 +83,40 @@ def test_singular_inverse_is_zero(cuda):
     assert abs(to_host(ld)[0].real - ldo[0].real) < 1e-9
 
 
+@pytest.mark.parametrize("N", [1, 2, 7, 8, 9, 16, 17, 32, 33, 50, 52, 53, 64, 65, 70])
+def test_random_inverse_logdet_sizes(cuda, N):
+    """Every size class of the register-resident kernel (N <= 64) and the shared-memory kernel
+    (N > 64): inverse and accumulated log det against the oracle's getrf/getri."""
+    A = _A()
+    rs = np.random.default_rng(100 + N)
+    W = 5
+    m = rand_c(rs, W, N, N)
+    ld0 = rand_c(rs, W) * 0.5
+    Am = to_dev(m)
+    inv = torch.zeros_like(Am)
+    ld = to_dev(ld0.copy())
+    A.det_ops.inverse_logdet(Am, inv, ld)
+    ldo = ld0.copy()
+    invo = O.inverse_logdet(m, ldo)
+    assert rel_err(to_host(inv), invo) < TOL
+    assert rel_err(to_host(ld), ldo) < TOL
+
+
+@pytest.mark.parametrize("N", [3, 16, 31, 33, 52, 53, 64, 66])
+def test_random_log_overlap_sizes(cuda, N):
+    """LU-only log det (Log_Overlap) in every size class, against the oracle."""
+    A = _A()
+    rs = np.random.default_rng(300 + N)
+    W, M = 6, N + 5
+    psi = rand_c(rs, N, M) / np.sqrt(M)
+    S = rand_c(rs, W, M, N) / np.sqrt(M)
+    ov = to_dev(rand_c(rs, W, scale=0.1))
+    ovo = to_host(ov).copy()
+    A.det_ops.Log_Overlap(to_dev(psi), to_dev(S), ov)
+    O.Log_Overlap(psi, S, ovo)
+    assert rel_err(to_host(ov), ovo) < TOL
+
+
 @pytest.mark.parametrize("W,M,N", [(7, 32, 8), (33, 40, 13), (4, 200, 50)])
 def test_random_density_matrix_and_overlap(cuda, W, M, N):
     A = _A()
