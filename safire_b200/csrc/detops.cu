@@ -235,7 +235,8 @@ __global__ void __launch_bounds__(64 * C, C == 2 ? 3 : 2) gj_reg_kernel(const c1
         bi = oi;
       }
     }
-    const int p = bi;
+    // a column of NaNs finds no pivot: treated as a zero pivot at row k (no interchange)
+    const int p = bi < N ? bi : k;
     const bool zero = !(best > 0.0);
     const c128 piv = col[p];
     if (t == 0) {
