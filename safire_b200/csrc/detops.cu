@@ -94,6 +94,7 @@ __global__ void __launch_bounds__(GJ_THREADS) gj_logdet_kernel(const c128* __res
         }
       }
       if (tx == 0) {
+        if (bi >= N) bi = k;  // a column of NaNs: zero pivot at row k
         s_piv = bi;
         piv_swapped[k] = (bi != k);
         const c128 d = a[bi * PP + k];
@@ -167,26 +168,29 @@ __global__ void __launch_bounds__(GJ_THREADS) gj_logdet_kernel(const c128* __res
 
 // ---------------------------------------------------------------------------------------------
 // Register-resident Gauss-Jordan / LU for N <= 64 (the production sizes).  One CTA of 64 C threads
-// per matrix (C = 2 column classes up to N = 32, else 4); thread t holds row i = t % 64 and the
-// columns j = h + C q of class h = t / 64 in registers (q < QMAX), so a step touches shared memory
-// only for the pivot column, the scaled pivot row and the row that moves in the interchange.
+// per matrix (C = 2 column classes up to N = 32, else 4); thread t holds row
+// i = t % 64 and the columns j = h + C q of class h = t / 64 in registers (q < QMAX), so a step
+// touches shared memory only for the pivot column, the pivot row and the row that moves in the
+// interchange.
 // Step k: every warp finds the pivot p (first max |re|+|im| in column k, rows k..N-1, as izamax)
-// from the column buffer; the owners of row p write it scaled by 1/pivot (with 1/pivot in column
-// k), the owners of row k write the old row k; after one barrier every row i != k subtracts
-// f_i * (scaled pivot row), f_i being its column-k element before the interchange, and row p takes
-// the old row k first; column k, moved to the column buffer and zeroed in the registers at the end
-// of step k-1, becomes -f_i/pivot (the in-place Gauss-Jordan inverse), row k the scaled pivot row.  Without the inverse only rows below k are eliminated (plain LU; the pivots
-// are the same U diagonal).  The row interchanges permute the columns of the in-place inverse;
-// they are undone on the way out (columns swapped in reverse step order).  Two barriers a step.
+// from the column buffer; the owners of row p write it as it stands with 1 in column k, the owners
+// of row k write the old row k; after one barrier every row i != k subtracts g_i times the pivot
+// row, g_i = f_i / pivot with f_i its column-k element before the interchange (the multiplier in
+// getf2's rounding order), and row p takes the old row k first.  Column k is moved to the column
+// buffer and zeroed in the registers at the end of step k-1, so the update leaves -g_i there (the
+// in-place Gauss-Jordan inverse); row k becomes the pivot row / pivot.  Without the inverse only
+// rows below k are eliminated (plain LU, the same U diagonal).  The row interchanges permute the
+// columns of the in-place inverse; they are undone on the way out (columns swapped in reverse step
+// order).  Two barriers a step.
 // ---------------------------------------------------------------------------------------------
 template <int QMAX, int C, bool INVERT>
-__global__ void __launch_bounds__(64 * C, C == 2 ? 3 : 2) gj_reg_kernel(const c128* __restrict__ A,
+__global__ void __launch_bounds__(64 * C, C == 2 ? 3 : (QMAX <= 13 ? 2 : 1)) gj_reg_kernel(const c128* __restrict__ A,
                                                                long strideA,
                                                                c128* __restrict__ Ainv,
                                                                long strideInv,
                                                                c128* __restrict__ ovlp, int N,
                                                                c128 post_scale, c128 post_add) {
-  __shared__ c128 rowbuf[64];     // pivot row * (1/pivot), column k = 1/pivot
+  __shared__ c128 rowbuf[64];     // pivot row, column k = 1
   __shared__ c128 kbuf[64];       // old row k (moves to row p)
   __shared__ c128 colbuf[2][64];  // column k of every row at step k (buffer k & 1)
   __shared__ c128 piv_val[64];
@@ -217,42 +221,41 @@ __global__ void __launch_bounds__(64 * C, C == 2 ? 3 : 2) gj_reg_kernel(const c1
 
   for (int k = 0; k < N; ++k) {
     const c128* col = colbuf[k & 1];
-    double best = -1.0;
-    int bi = N;
-    for (int r = k + lane; r < N; r += 32) {
-      const double v = cabs1(col[r]);
-      if (v > best) {
-        best = v;
-        bi = r;
-      }
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, best, off);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-      if (ov > best || (ov == best && oi < bi)) {
-        best = ov;
-        bi = oi;
-      }
-    }
-    // a column of NaNs finds no pivot: treated as a zero pivot at row k (no interchange)
-    const int p = bi < N ? bi : k;
-    const bool zero = !(best > 0.0);
+    // pivot: first max |re|+|im| in column k, rows k..N-1.  Non-negative doubles order as their
+    // bit patterns, so the maximum is two warp max-reductions (high, then low word); NaN and rows
+    // outside k..N-1 take key 0.  The first row holding the maximum comes from two ballots.
+    const int r0 = k + lane, r1 = k + lane + 32;
+    const double v0 = r0 < N ? cabs1(col[r0]) : 0.0;
+    const double v1 = r1 < N ? cabs1(col[r1]) : 0.0;
+    const unsigned long long k0 = (v0 == v0) ? static_cast<unsigned long long>(__double_as_longlong(v0)) : 0ull;
+    const unsigned long long k1 = (v1 == v1) ? static_cast<unsigned long long>(__double_as_longlong(v1)) : 0ull;
+    const unsigned long long kl = k1 > k0 ? k1 : k0;
+    const unsigned mhi = __reduce_max_sync(0xffffffffu, unsigned(kl >> 32));
+    const unsigned mlo = __reduce_max_sync(0xffffffffu, unsigned(kl >> 32) == mhi ? unsigned(kl) : 0u);
+    const unsigned long long kmax = (static_cast<unsigned long long>(mhi) << 32) | mlo;
+    const bool zero = (kmax == 0ull);
+    const unsigned b0 = __ballot_sync(0xffffffffu, r0 < N && k0 == kmax);
+    const unsigned b1 = __ballot_sync(0xffffffffu, r1 < N && k1 == kmax);
+    // a zero (or NaN) column: zero pivot at row k, no interchange
+    const int p = zero ? k : (b0 ? k + __ffs(b0) - 1 : k + 32 + __ffs(b1) - 1);
     const c128 piv = col[p];
+    // 1/pivot = conj(pivot) / |pivot|^2
+    const double rden = 1.0 / (piv.x * piv.x + piv.y * piv.y);
+    const c128 dinv = cmk(piv.x * rden, -piv.y * rden);
     if (t == 0) {
       perm[k] = p;
       piv_val[k] = piv;
       if (zero) s_singular = 1;
     }
     if (!zero) {
+      // pivot row as it stands (its column k was zeroed in the registers) with 1 in column k
       if (i == p) {
-        const c128 dinv = cdiv(cmk(1.0, 0.0), piv);
 #pragma unroll
         for (int q = 0; q < QMAX; ++q) {
           const int j = h + C * q;
-          if (j < N) rowbuf[j] = cmul(a[q], dinv);
+          if (j < N) rowbuf[j] = a[q];
         }
-        if (h == (k % C)) rowbuf[k] = dinv;
+        if (h == (k % C)) rowbuf[k] = cmk(1.0, 0.0);
       }
       if (i == k && p != k) {
 #pragma unroll
@@ -267,15 +270,18 @@ __global__ void __launch_bounds__(64 * C, C == 2 ? 3 : 2) gj_reg_kernel(const c1
     const int kn = k + 1;
     if (!zero && row_ok) {
       if (i == k) {
+        // row k <- pivot row / pivot (column k: 1/pivot)
         if (INVERT) {
 #pragma unroll
           for (int q = 0; q < QMAX; ++q) {
             const int j = h + C * q;
-            if (j < N) a[q] = rowbuf[j];
+            if (j < N) a[q] = cmul(rowbuf[j], dinv);
           }
         }
       } else if (INVERT || i > k) {
+        // row i -= g * pivot row, g = f / pivot (column k: 0 - g = -f/pivot)
         const c128 f = (i == p) ? col[k] : col[i];
+        const c128 g = cmul(f, dinv);
         if (i == p) {
 #pragma unroll
           for (int q = 0; q < QMAX; ++q) {
@@ -283,27 +289,39 @@ __global__ void __launch_bounds__(64 * C, C == 2 ? 3 : 2) gj_reg_kernel(const c1
             if (j < N) a[q] = kbuf[j];
           }
         }
-        const c128 nf = cmk(-f.x, -f.y);
+        const c128 ng = cmk(-g.x, -g.y);
 #pragma unroll
         for (int q = 0; q < QMAX; ++q) {
           const int j = h + C * q;
           if (j < N) {
             const c128 r = rowbuf[j];
-            a[q].x = fma(nf.x, r.x, fma(f.y, r.y, a[q].x));
-            a[q].y = fma(nf.x, r.y, fma(nf.y, r.x, a[q].y));
+            a[q].x = fma(ng.x, r.x, fma(g.y, r.y, a[q].x));
+            a[q].y = fma(ng.x, r.y, fma(ng.y, r.x, a[q].y));
           }
+          // keep the pivot-row loads in groups of eight (bounds the registers they hold)
+          if ((q & 7) == 7) asm volatile("" ::: "memory");
         }
       }
     }
     // column k+1 moves to the column buffer for the next pivot search and is zeroed in the
-    // registers, so that step k+1's update leaves -f/pivot there (the in-place inverse's column)
+    // registers (warp-uniform branch to its register)
     if (kn < N && h == (kn % C)) {
-#pragma unroll
-      for (int q = 0; q < QMAX; ++q)
-        if (h + C * q == kn) {
-          if (row_ok) nxt[i] = a[q];
-          a[q] = cmk(0.0, 0.0);
-        }
+      switch (kn / C) {
+#define GR_CASE(Q)                          \
+  case Q:                                   \
+    if (Q < QMAX) {                         \
+      constexpr int QQ = Q < QMAX ? Q : 0;  \
+      if (row_ok) nxt[i] = a[QQ];           \
+      a[QQ] = cmk(0.0, 0.0);                \
+    }                                       \
+    break;
+        GR_CASE(0) GR_CASE(1) GR_CASE(2) GR_CASE(3) GR_CASE(4) GR_CASE(5) GR_CASE(6) GR_CASE(7)
+        GR_CASE(8) GR_CASE(9) GR_CASE(10) GR_CASE(11) GR_CASE(12) GR_CASE(13) GR_CASE(14)
+        GR_CASE(15)
+#undef GR_CASE
+        default:
+          break;
+      }
     }
     __syncthreads();
   }
