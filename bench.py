@@ -41,6 +41,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--exchange-split", type=int, default=3, choices=[1, 3],
                     help="TF32 products per real product in the mixed exchange contraction")
+    ap.add_argument("--taylor-mode", type=int, default=1, choices=[0, 1, 2, 3],
+                    help="mixed Taylor propagation: 0 per-term GEMMs, 1 fused (auto), 2 / 3 fused "
+                         "with one / two walkers in flight per CTA")
     return ap.parse_args()
 
 
@@ -253,6 +256,8 @@ def run_ours(args):
     sim = Simulation.from_workload(wl, W=W, precision=prec, rp=rp)
     if prec == A.PREC_MIXED and args.exchange_split != 3:
         sim.ham.set_exchange_split(args.exchange_split)
+    if prec == A.PREC_MIXED and args.taylor_mode != 1:
+        sim.ham.set_taylor_fused(args.taylor_mode)
     stream = torch.cuda.current_stream()
 
     def block():
@@ -393,6 +398,7 @@ def run_ours(args):
                                    "block of 10 steps (ortho/5, comb/10, energy/10)",
                        "precision": args.precision, "global_walkers": W * world,
                        "exchange_split": args.exchange_split if prec == A.PREC_MIXED else None,
+                       "taylor_mode": args.taylor_mode if prec == A.PREC_MIXED else None,
                        "parallelism": f"walker dp{world}",
                        "l2": "inputs larger than L2 (V 655 MB, Likn 512 MB per step)"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,

@@ -166,8 +166,9 @@ int afqmc_ham_energy(afqmc_ham ham, const afqmc_c128* G, afqmc_c128* E, int W, i
 int afqmc_ham_set_exchange_split(afqmc_ham ham, int nsplit);
 
 /* Mixed-precision Taylor propagation: 1 (default) runs all order + 2 products of each walker in
- * one persistent tensor-core kernel (M <= 256 orbitals, N <= 64 electrons per spin); 0 launches
- * one batched GEMM per product.  Both compute the same sums. */
+ * one persistent tensor-core kernel (M <= 256 orbitals, N <= 64 electrons per spin), with one or
+ * two walkers in flight per CTA chosen by the walker count; 2 / 3 force one / two walkers in
+ * flight; 0 launches one batched GEMM per product.  All compute the same sums. */
 int afqmc_ham_set_taylor_fused(afqmc_ham ham, int fused);
 
 /* Error word of the tensor-core kernels' bounded device waits (bit 0: a wait on a TMA or MMA

@@ -161,9 +161,10 @@ class HamiltonianOperations:
         """3: 3xTF32 exchange contraction (default); 1: plain TF32."""
         call("afqmc_ham_set_exchange_split", self.handle, int(nsplit))
 
-    def set_taylor_fused(self, fused):
-        """True: one persistent kernel for all Taylor products (default); False: one GEMM each."""
-        call("afqmc_ham_set_taylor_fused", self.handle, int(bool(fused)))
+    def set_taylor_fused(self, mode):
+        """1/True: one persistent kernel for all Taylor products (default); 0/False: one GEMM
+        each; 2 / 3: the persistent kernel with one / two walkers in flight per CTA."""
+        call("afqmc_ham_set_taylor_fused", self.handle, int(mode))
 
     def device_error_flag(self):
         f = C.c_uint()

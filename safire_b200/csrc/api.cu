@@ -628,13 +628,13 @@ extern "C" int afqmc_ham_set_exchange_split(afqmc_ham h, int nsplit) {
 
 extern "C" int afqmc_ham_set_taylor_fused(afqmc_ham h, int fused) {
   AFQMC_CHECK_ARG(h, "afqmc_ham_set_taylor_fused: null handle");
-  AFQMC_CHECK_ARG(fused == 0 || fused == 1, "afqmc_ham_set_taylor_fused: fused must be 0 or 1");
+  AFQMC_CHECK_ARG(fused >= 0 && fused <= 3, "afqmc_ham_set_taylor_fused: mode must be 0..3");
   DeviceGuard g(h->device);
   if (!h->mixed) {
     EnergyArgs a = energy_args(h, nullptr, 0);
     AFQMC_TRY(mixed_ham_create(&h->mixed, a, nullptr));
   }
-  return mixed_set_taylor_fused(h->mixed, fused != 0);
+  return mixed_set_taylor_mode(h->mixed, fused);
 }
 
 extern "C" int afqmc_ham_device_error(afqmc_ham h, unsigned* flag) {

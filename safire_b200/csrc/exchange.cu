@@ -176,6 +176,7 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
           const uint32_t sb = tc::smem_u32(st + K::NA * K::A_TILE);
 #pragma unroll
           for (int kk = 0; kk < XBK / 8; ++kk) {
+            if (kc * XBK + kk * 8 >= p.M) break;  // zero fill past K
             auto A = [&](int q) { return tc::sdesc_sw128(sa + q * K::A_TILE) + uint64_t(2 * kk); };
             auto B = [&](int q) { return tc::sdesc_sw128(sb + q * K::B_TILE) + uint64_t(2 * kk); };
             const uint32_t acc0 = (kc > 0 || kk > 0) ? 1u : 0u;
@@ -204,8 +205,7 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
     const int L = q * 32 + lane;
     const int wl = L / XSLOT_A, b = L % XSLOT_A;
     const int et = threadIdx.x - 64;  // 0..127
-    float* sre = stg;
-    float* sim = stg + 2 * 50 * PITCH;
+    float2* st2 = reinterpret_cast<float2*>(stg);  // [2 walkers][N][PITCH] (re, im)
     long ti = 0;
     for (long t = blockIdx.x; t < ntiles; t += gridDim.x, ++ti) {
       int wp, np;
@@ -219,11 +219,11 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
       const uint32_t trow = taddr + (uint32_t(q * 32) << 16) + uint32_t(buf * 2 * XBN);
 #pragma unroll 1
       for (int nl = 0; nl < 2; ++nl) {
-        // stage this walker's row b of T_n (columns a) in shared memory: all fourteen TMEM
-        // loads of the slot are issued before one wait
+        // row b of T_n (columns a) into registers (fourteen TMEM loads, one wait) and into the
+        // staging block, from which the other rows read it as their column
         const int r = (wl * N + b) * PITCH;
+        float vr[XSLOT_B], vi[XSLOT_B];
         {
-          float vr[XSLOT_B], vi[XSLOT_B];
           const uint32_t cr = trow + nl * XSLOT_B, ci = trow + XBN + nl * XSLOT_B;
 #pragma unroll
           for (int c = 0; c < XSLOT_B; c += 8) {
@@ -231,20 +231,26 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
             tmem_ld8(ci + c, vi + c);
           }
           tc::tmem_ld_wait();
-          if (valid) {
-#pragma unroll
-            for (int a = 0; a < XSLOT_B; ++a)
-              if (a < N) {
-                sre[r + a] = vr[a];
-                sim[r + a] = vi[a];
-              }
-          }
         }
         if (nl == 1) {
           tc::tc_fence_before();
           tc::mbar_arrive(&acc_empty[buf]);  // accumulator free for tile ti+2
         }
+        if (valid) {
+#pragma unroll
+          for (int a = 0; a < XSLOT_B; ++a)
+            if (a < N) st2[r + a] = make_float2(vr[a], vi[a]);
+        }
         const int n = 2 * np + nl;
+        // the running sums this tile adds to, fetched now so their latency hides behind the loop
+        const int ww = 2 * wp + et;
+        const bool upd = et < 2 && n < p.Nc && ww < p.W;
+        const long o = long(ww) * p.Nc + n;
+        c128 exx0 = cmk(0.0, 0.0), kl0 = cmk(0.0, 0.0);
+        if (upd) {
+          exx0 = p.exx[o];
+          kl0 = p.kl[o];
+        }
         named_bar(1, 128);
         // x = sum_a T[b][a] T[a][b];  tr = T[b][b]   (rows of one warp all belong to walker wl)
         // The sum over a runs in FP32 with four independent accumulator pairs (50 terms of
@@ -253,27 +259,18 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
         if (valid && n < p.Nc) {
           const int col0 = wl * N * PITCH + b;
           float xr[4] = {0.f, 0.f, 0.f, 0.f}, xi[4] = {0.f, 0.f, 0.f, 0.f};
-          int a = 0;
-#pragma unroll 2
-          for (; a + 4 <= N; a += 4) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              const float tr_ = sre[r + a + j], ti_ = sim[r + a + j];  // T[b][a]
-              const float ur = sre[col0 + (a + j) * PITCH], ui = sim[col0 + (a + j) * PITCH];  // T[a][b]
-              xr[j] = fmaf(tr_, ur, fmaf(-ti_, ui, xr[j]));
-              xi[j] = fmaf(tr_, ui, fmaf(ti_, ur, xi[j]));
+          for (int a = 0; a < XSLOT_B; ++a)
+            if (a < N) {
+              const float2 u = st2[col0 + a * PITCH];  // T[a][b]
+              xr[a & 3] = fmaf(vr[a], u.x, fmaf(-vi[a], u.y, xr[a & 3]));
+              xi[a & 3] = fmaf(vr[a], u.y, fmaf(vi[a], u.x, xi[a & 3]));
             }
-          }
-          for (; a < N; ++a) {
-            const float tr_ = sre[r + a], ti_ = sim[r + a];
-            const float ur = sre[col0 + a * PITCH], ui = sim[col0 + a * PITCH];
-            xr[0] = fmaf(tr_, ur, fmaf(-ti_, ui, xr[0]));
-            xi[0] = fmaf(tr_, ui, fmaf(ti_, ur, xi[0]));
-          }
           v4[0] = (double(xr[0]) + double(xr[1])) + (double(xr[2]) + double(xr[3]));
           v4[1] = (double(xi[0]) + double(xi[1])) + (double(xi[2]) + double(xi[3]));
-          v4[2] = sre[r + b];
-          v4[3] = sim[r + b];
+          const float2 d = st2[r + b];
+          v4[2] = d.x;
+          v4[3] = d.y;
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c)
@@ -284,18 +281,15 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
 #pragma unroll
           for (int c = 0; c < 4; ++c) red[q * 4 + c] = v4[c];
         named_bar(1, 128);
-        if (et < 2 && n < p.Nc) {
+        // red is rewritten only after the next barrier, which these threads reach after their
+        // reads; the staging block is rewritten only after every thread passed the one above
+        if (upd) {
           // walker slot et = lane quarters {2et, 2et+1}
-          const int ww = 2 * wp + et;
-          if (ww < p.W) {
-            const double* r0 = red + (2 * et) * 4;
-            const double* r1 = red + (2 * et + 1) * 4;
-            const long o = long(ww) * p.Nc + n;
-            p.exx[o] = cadd(p.exx[o], cmk(r0[0] + r1[0], r0[1] + r1[1]));
-            p.kl[o] = cadd(p.kl[o], cmk(r0[2] + r1[2], r0[3] + r1[3]));
-          }
+          const double* r0 = red + (2 * et) * 4;
+          const double* r1 = red + (2 * et + 1) * 4;
+          p.exx[o] = cadd(exx0, cmk(r0[0] + r1[0], r0[1] + r1[1]));
+          p.kl[o] = cadd(kl0, cmk(r0[2] + r1[2], r0[3] + r1[3]));
         }
-        named_bar(1, 128);
       }
     }
   }

@@ -191,6 +191,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_cgemm_kernel(const __grid_co
           const uint32_t sb = tc::smem_u32(st + K::NA * K::A_TILE);
 #pragma unroll
           for (int kk = 0; kk < BK / 8; ++kk) {
+            if (kc * BK + kk * 8 >= p.k) break;  // zero fill past K
             // +32 bytes per K=8 step inside the 128-byte swizzle row (descriptor units of 16 B)
             auto A = [&](int q) { return tc::sdesc_sw128(sa + q * K::A_TILE) + uint64_t(2 * kk); };
             auto B = [&](int q) { return tc::sdesc_sw128(sb + q * K::B_TILE) + uint64_t(2 * kk); };
@@ -489,7 +490,8 @@ struct MixedHam {
   // dynamic operands, sized on demand
   int capW = 0;
   int exchange_split = 3;  // TF32 products per real product in the exchange contraction
-  bool taylor_unfused = false;  // true: one GEMM launch per Taylor product
+  int taylor_mode = 1;    // 0: one GEMM launch per Taylor product; 1: fused, slots chosen by W;
+  int taylor_slots = 0;   // 2 / 3: fused with one / two walkers in flight per CTA
   Planes G;         // [W][1][nel_tot*M]  (A of vbias);  exchange view [W*nel][M]
   Planes X;         // [1][W][Nc] (A of vHS)
   unsigned* err = nullptr;
@@ -699,8 +701,8 @@ int vhs_mixed(cudaStream_t s, MixedHam* m, const c128* X, c128* V, int W, double
 
 int taylor_fused_tc(cudaStream_t s, const float* const P1p[2], const float* const Vp[4], long ldV,
                     const float* const Sp[4], float* const Tp0[4], float* const Tp1[4],
-                    float* const Rp[4], long pl_ld, c128* S, long ldS, int W, int M, int N,
-                    int order, unsigned* err);
+                    float* const Rp[4], float* const sum[2], long pl_ld, c128* S, long ldS,
+                    int W, int M, int N, int order, int nslots, unsigned* err);
 
 // Taylor propagation S <- P1 sum_n (iV)^n/n! P1 S (propagate.hpp:238-298) on the split planes.
 // V must have been produced by vhs_mixed (planes kept in MixedHam) for the same walkers.
@@ -723,13 +725,13 @@ int propagate_mixed(cudaStream_t s, MixedHam* m, const void* P1, bool p1_real, c
   }
   // S^T planes [W][N][M] from the walkers' Slater matrices [W][M][N]
   AFQMC_TRY(split_complex(s, S, N, ldS, W, M, N, m->Sst, true));
-  if (M <= 256 && N <= 64 && !m->taylor_unfused && m->P1.ld == m->T0.ld) {
+  if (M <= 256 && N <= 64 && m->taylor_mode != 0 && m->P1.ld == m->T0.ld) {
     // one persistent kernel runs all order + 2 products of each walker
     const float* p1p[2] = {m->P1.p[0], m->P1.p[1]};
     const float* vp[4] = {m->V.p[0], m->V.p[1], m->V.p[2], m->V.p[3]};
     const float* sp[4] = {m->Sst.p[0], m->Sst.p[1], m->Sst.p[2], m->Sst.p[3]};
-    return taylor_fused_tc(s, p1p, vp, m->V.ld, sp, m->T0.p, m->T1.p, m->Tacc_split.p, m->T0.ld,
-                           S, ldS, W, M, N, order, m->err);
+    return taylor_fused_tc(s, p1p, vp, m->V.ld, sp, m->T0.p, m->T1.p, m->Tacc_split.p, m->acc,
+                           m->T0.ld, S, ldS, W, M, N, order, m->taylor_slots, m->err);
   }
   Planes* Tin = &m->T0;
   Planes* Tout = &m->T1;
@@ -777,8 +779,9 @@ int propagate_mixed(cudaStream_t s, MixedHam* m, const void* P1, bool p1_real, c
   return AFQMC_OK;
 }
 
-int mixed_set_taylor_fused(MixedHam* m, bool fused) {
-  m->taylor_unfused = !fused;
+int mixed_set_taylor_mode(MixedHam* m, int mode) {
+  m->taylor_mode = mode;
+  m->taylor_slots = mode >= 2 ? mode - 1 : 0;
   return AFQMC_OK;
 }
 

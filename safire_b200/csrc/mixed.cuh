@@ -17,9 +17,10 @@ int vhs_mixed(cudaStream_t s, MixedHam* m, const c128* X, c128* V, int W, double
 // S <- P1 exp_T(iV) P1 S with V from the last vhs_mixed call (P1 real float64 [M][M])
 int propagate_mixed(cudaStream_t s, MixedHam* m, const void* P1, bool p1_real, c128* S, long ldS,
                     int W, int M, int N, int order);
-// true (default): all Taylor products of a walker in one persistent kernel (M <= 256, N <= 64);
-// false: one batched GEMM launch per product
-int mixed_set_taylor_fused(MixedHam* m, bool fused);
+// 0: one batched GEMM launch per Taylor product; 1 (default): all products of a walker in one
+// persistent kernel (M <= 256, N <= 64), one or two walkers in flight per CTA chosen by the walker
+// count; 2 / 3: the persistent kernel with one / two walkers in flight
+int mixed_set_taylor_mode(MixedHam* m, int mode);
 // split planes of G for the exchange-energy GEMMs
 int mixed_prepare_G(cudaStream_t s, MixedHam* m, const c128* G, long ldG, int W);
 // T [(w,b)][(n,a)] for walkers [w0, w0+wc) of spin block sp (complex128, the chunk layout of

@@ -150,22 +150,25 @@ def _mixed_steps(wl, dham, fused, nsteps=2, order=None):
     for _ in range(nsteps):
         prop.Propagate(ws, -30.0, ud)
     torch.cuda.synchronize()
-    dham.set_taylor_fused(True)
+    dham.set_taylor_fused(1)
     return to_host(ws.SlaterMatrices(0)), to_host(ws.properties())
 
 
+@pytest.mark.parametrize("mode", [1, 2, 3])
 @pytest.mark.parametrize("name,W,Nc,order", [("cfg1", 300, None, None), ("cfg1", 20, None, 0),
-                                             ("cfg2", 6, 40, None)])
-def test_taylor_fused_vs_per_term(cuda, name, W, Nc, order):
-    """The persistent Taylor kernel (all products of a walker in one CTA) against one GEMM launch
-    per product: same split arithmetic, different kernels; W = 300 runs several walkers per CTA."""
+                                             ("cfg2", 6, 40, None), ("cfg1", 301, None, 3)])
+def test_taylor_fused_vs_per_term(cuda, name, W, Nc, order, mode):
+    """The persistent Taylor kernel (all products of a walker in one CTA; mode 2 / 3: one / two
+    walkers in flight per CTA) against one GEMM launch per product: same split arithmetic,
+    different kernels; W = 300, 301 run several walkers per CTA (301: one slot ends early)."""
     kw = {"W": W} if Nc is None else {"W": W, "Nc": Nc}
     wl = make_workload(name, **kw)
     dham, _, _ = make_pair(wl)
-    Sf, pf = _mixed_steps(wl, dham, True, order=order)
-    Su, pu = _mixed_steps(wl, dham, False, order=order)
+    Sf, pf = _mixed_steps(wl, dham, mode, order=order)
+    Su, pu = _mixed_steps(wl, dham, 0, order=order)
     eS = rel_err(Sf, Su)
     eO = rel_err(pf[:, O.OVLP], pu[:, O.OVLP])
-    print(f"fused vs per-term Taylor ({name}, W={W}, order={order}): S {eS:.2e} ovlp {eO:.2e}")
+    print(f"fused ({mode}) vs per-term Taylor ({name}, W={W}, order={order}): S {eS:.2e} "
+          f"ovlp {eO:.2e}")
     assert eS < 1e-5 and eO < 1e-5
     assert dham.device_error_flag() == 0

@@ -105,6 +105,51 @@ def test_step_parity_fp64(cuda, W, steps):
     assert stats[1] == oprop.eloc_stats.upper and stats[2] == oprop.eloc_stats.lower
 
 
+def test_step_parity_fp64_full_size(cuda):
+    """The benchmark system itself (M=200, N=50+50, Nc=1600): 40 FP64 steps with
+    orthogonalisation, comb and Eshift relaxation track the oracle walker for walker."""
+    from safire_b200 import afqmc as A
+    from safire_b200.driver import RunParams, Simulation
+
+    W, steps = 4, 40
+    wl = make_workload("cfg2", W=W)
+    rp = RunParams(equilibration_steps=100, seed=0)
+    sim = Simulation.from_workload(wl, W=W, rp=rp)
+    oham = O.Real3IndexFactorization(wl.walker_type, wl.M, wl.nup, wl.ndn, wl.Likn, wl.hij, wl.E0,
+                                     wl.PsiT)
+    owfn = O.NOMSD(oham, wl.PsiT)
+    ows = O.WalkerSet.from_trial(owfn, W)
+    E, ov = owfn.Energy(ows.SA, ows.SB)
+    ows.props[:, O.OVLP] = ov
+    ows.props[:, O.E1], ows.props[:, O.EXX], ows.props[:, O.EJ] = E[:, 0], E[:, 1], E[:, 2]
+    ows.props[:, O.PSEUDO_ELOC] = E.sum(axis=1)
+    Eshift_o = O.average_energy(ows)
+    oprop = O.Propagator(owfn, O.PropagatorParams(dt=wl.dt))
+    walker_rng = O.HostRandomGenerator(O.split_seed(0, 0, 0))
+    field_rng = O.HostRandomGenerator(O.split_seed(0, 0, 1))
+    relax = 1 - math.exp(-10.0 / rp.equilibration_steps)
+    for step in range(steps):
+        u = field_rng.sample_uniform(W * wl.Nc).reshape(W, wl.Nc)
+        sim.prop.Propagate(sim.wset, sim.Eshift, to_dev(u, torch.float64))
+        oprop.propagate(ows, Eshift_o, u)
+        if step % rp.walker_ortho_interval == 0:
+            sim.prop.Orthogonalize(sim.wset)
+            oprop.orthogonalize(ows)
+        if step % rp.population_control_interval == 0:
+            off_d = A.population_control(sim.wset, sim.walker_rng)
+            off_o = O.population_control_single_rank(walker_rng, ows)
+            assert np.array_equal(off_d, off_o), step
+        sim.Eshift += sim.relax * (sim.average_pseudo_energy() - sim.Eshift)
+        Eshift_o += relax * (O.average_pseudo_energy(ows, wl.dt) - Eshift_o)
+        sim.step_index += 1
+        props = to_host(sim.wset.properties())
+        assert rel_err(to_host(sim.wset.SlaterMatrices(0)), ows.SA) < TOL, step
+        assert rel_err(props[:, O.WEIGHT], ows.props[:, O.WEIGHT]) < TOL, step
+        assert _cmp_complex_mod(props[:, O.PSEUDO_ELOC], ows.props[:, O.PSEUDO_ELOC],
+                                2 * np.pi / wl.dt) < TOL, step
+        assert abs(sim.Eshift - Eshift_o) < TOL * abs(Eshift_o), step
+
+
 def test_device_rng_step_runs(cuda):
     """The production path: fields from the device Philox generator, full loop with measurement."""
     from safire_b200.driver import RunParams, Simulation
