@@ -239,6 +239,7 @@ def run_ours(args):
     from safire_b200 import afqmc as A
     from safire_b200 import capi
     from safire_b200.driver import RunParams, Simulation
+    from safire_b200.population import population_control_distributed
     from safire_b200.synth import make_workload
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -252,7 +253,7 @@ def run_ours(args):
     prec = A.PREC_MIXED if args.precision == "mixed" else A.PREC_FP64
     W = args.walkers
     wl = make_workload("cfg2")
-    rp = RunParams(equilibration_steps=0, seed=rank)
+    rp = RunParams(equilibration_steps=0, seed=0)
     sim = Simulation.from_workload(wl, W=W, precision=prec, rp=rp)
     if prec == A.PREC_MIXED and args.exchange_split != 3:
         sim.ham.set_exchange_split(args.exchange_split)
@@ -355,10 +356,15 @@ def run_ours(args):
                 if st % 5 == 0:
                     sim.prop.Orthogonalize(sim.wset)
                 if st % 10 == 0:
-                    A.population_control(sim.wset, sim.walker_rng)
+                    if world > 1:
+                        population_control_distributed(sim.wset, sim.walker_rng)
+                    else:
+                        A.population_control(sim.wset, sim.walker_rng)
                 sim.step_index += 1
             E, _ = sim.wfn.Energy(sim.wset, set_properties=False, precision=prec)
             sums = A.energy_sums(sim.wset, E)
+            if world > 1:
+                dist.all_reduce(sums)
             host_e.copy_(sums, non_blocking=True)
             host_w.copy_(sim.wset.properties()[:, 0], non_blocking=True)
 
@@ -392,7 +398,8 @@ def run_ours(args):
             "metric": metric_name(), "value": value, "unit": "walker-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "c128" if prec == A.PREC_FP64 else "c128+tf32x3",
+            "dtype": "c128" if prec == A.PREC_FP64 else
+                     ("c128+tf32x3" if args.exchange_split == 3 else "c128+tf32x3 (exchange tf32)"),
             "data": "synthetic",
             "config": {"workload": "M=200 N=50+50 Nc=1600 W=1024/GPU dt=0.005 taylor=6, "
                                    "block of 10 steps (ortho/5, comb/10, energy/10)",

@@ -146,6 +146,43 @@ def single_rank_slot_map(offspring: np.ndarray) -> np.ndarray:
     return src
 
 
+def swap_walkers_slot_map(offspring, counts, me):
+    """Global source walker of every slot of rank `me` after swap_walkers_async
+    (population_control.hpp:142-209): local keepers stay, arrivals take the freed slots in plan
+    order, then the extra local copies (walker order) and the extra copies of each arrival fill
+    the remaining freed slots.  Global index = counts[0] + ... + counts[r-1] + local index."""
+    offspring = np.asarray(offspring)
+    counts = [int(c) for c in counts]
+    plan = plan_walker_exchange(offspring, counts)
+    first = int(sum(counts[:me]))
+    nw = counts[me]
+    keep = [int(x) for x in offspring[first:first + nw]]
+    for src, wk, dst, copies in plan:
+        if src == me:
+            keep[wk] -= copies
+    src_of = list(range(first, first + nw))
+    free = [i for i in range(nw) if keep[i] == 0]
+    nxt = 0
+    arrivals = []
+    for src, wk, dst, copies in plan:
+        if src != me and dst == me:
+            slot = free[nxt]
+            nxt += 1
+            src_of[slot] = int(sum(counts[:src])) + wk
+            arrivals.append((slot, copies))
+    for i in range(nw):
+        for _ in range(1, keep[i]):
+            src_of[free[nxt]] = first + i
+            nxt += 1
+    for slot, copies in arrivals:
+        for _ in range(1, copies):
+            src_of[free[nxt]] = src_of[slot]
+            nxt += 1
+    if nxt != len(free):
+        raise ValueError("swap_walkers_slot_map: %d slots left unfilled" % (len(free) - nxt))
+    return np.asarray(src_of)
+
+
 # --------------------------------------------------------------------------------------------
 # Determinants (src/numerics/operations/determinants_impl.hpp)
 # --------------------------------------------------------------------------------------------

@@ -237,6 +237,28 @@ class WalkerSet:
     def init_from_trial(self, ham: HamiltonianOperations, stream=None):
         call("afqmc_wset_init_from_trial", self.handle, ham.handle, _stream(stream))
 
+    def copy_rows(self, dst, src, stream=None):
+        """rows dst[j] <- rows src[j] (int32 device tensors)."""
+        call("afqmc_wset_copy_rows", self.handle, _ptr(dst), _ptr(src), int(dst.numel()),
+             _stream(stream))
+
+    def pack_rows(self, idx, stream=None):
+        """[n, walker_size] device tensor holding the rows idx (int32 device tensor)."""
+        out = torch.empty((int(idx.numel()), self.walker_size), dtype=torch.complex128,
+                          device=self.buffer.device)
+        call("afqmc_wset_pack_rows", self.handle, _ptr(idx), int(idx.numel()), _ptr(out),
+             _stream(stream))
+        return out
+
+    def unpack_rows(self, idx, buf, stream=None):
+        """rows idx (int32 device tensor) <- buf [n, walker_size]."""
+        call("afqmc_wset_unpack_rows", self.handle, _ptr(idx), int(idx.numel()), _ptr(buf),
+             _stream(stream))
+
+    def normalize_weights(self, stream=None):
+        """w <- w/|w| for every walker (end of population control)."""
+        call("afqmc_wset_normalize_weights", self.handle, _stream(stream))
+
 
 # --------------------------------------------------------------------------------------------
 # NOMSD single-determinant trial

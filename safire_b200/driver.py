@@ -1,5 +1,7 @@
 """run_afqmc-style step loop over the C ABI (src/AFQMC/execute.cpp:106-209,
-src/AFQMC/Drivers/run_afqmc.cpp:69-113).
+src/AFQMC/Drivers/run_afqmc.cpp:69-113).  Under an initialised torch.distributed process group
+each rank holds its own walkers: the energy and pseudo-energy sums are summed over the ranks and
+population control is the distributed comb (safire_b200.population).
 
 The per-step work (G, vbias, fields, vHS, propagation, overlaps, phaseless update) is one C-ABI
 call, afqmc_prop_step; this module only sequences steps, orthogonalisation, comb population
@@ -12,9 +14,30 @@ from dataclasses import dataclass, field
 
 import numpy as np
 import torch
+import torch.distributed as dist
 
 from . import afqmc as A
 from .capi import E1, EJ, EXX, OVLP, PSEUDO_ELOC
+
+
+def _world():
+    return dist.get_world_size() if dist.is_available() and dist.is_initialized() else 1
+
+
+def _rank():
+    return dist.get_rank() if _world() > 1 else 0
+
+
+def _sum_over_ranks(t):
+    """In-place sum over the ranks of a device (NCCL) or host (gloo) tensor."""
+    if _world() > 1:
+        if dist.get_backend() == "nccl":
+            dist.all_reduce(t)
+        else:
+            h = t.cpu()
+            dist.all_reduce(h)
+            t.copy_(h)
+    return t
 
 
 @dataclass
@@ -50,6 +73,8 @@ class Simulation:
         wfn = A.NOMSD(ham)
         wset = A.WalkerSet(wl.walker_type, wl.M, wl.nup, wl.ndn, W)
         wset.init_from_trial(ham)
+        # the comb's generator is the same on every rank (the reference's root draws it); the
+        # auxiliary fields of each rank's walkers come from that rank's own stream
         walker_rng = A.HostRandomGenerator(A.split_seed(rp.seed, 0, 0))
         # initial energy, seeded pseudo energy and Eshift (execute.cpp:171-184)
         wfn.Energy(wset, set_properties=True, precision=precision)
@@ -57,22 +82,25 @@ class Simulation:
         e1, exx, ej = (wset.getProperty(p) for p in (E1, EXX, EJ))
         wset.setProperty(PSEUDO_ELOC, e1 + exx + ej)
         w = wset.getProperty(0)
-        Eshift = float((np.sum(w * (e1 + exx + ej)) / np.sum(w)).real)
+        sums = torch.tensor([np.sum(w * (e1 + exx + ej)), np.sum(w)], dtype=torch.complex128,
+                            device=wset.buffer.device)
+        sums = _sum_over_ranks(sums).cpu().numpy()
+        Eshift = float((sums[0] / sums[1]).real)
         params = A.default_params(dt=wl.dt, precision=precision, **prop_kw)
         prop = A.Propagator(ham, params, W)
-        prop.set_field_seed(A.split_seed(rp.seed, 0, 1))
+        prop.set_field_seed(A.split_seed(rp.seed, _rank(), 1))
         n = rp.equilibration_steps
         relax = 1 - math.exp(-10.0 / n) if n > 1 else 1.0
         return Simulation(ham, wfn, wset, prop, walker_rng, rp, wl.dt, Eshift, relax, precision)
 
     def average_pseudo_energy(self):
-        s = A.pseudo_energy_sums(self.wset, self.dt)
+        s = _sum_over_ranks(A.pseudo_energy_sums(self.wset, self.dt))
         s = s.cpu().numpy()
         return math.log((s[0] / s[1]).real) / self.dt
 
     def measure(self):
         E, _ = self.wfn.Energy(self.wset, set_properties=False, precision=self.precision)
-        sums = A.energy_sums(self.wset, E).cpu().numpy()
+        sums = _sum_over_ranks(A.energy_sums(self.wset, E)).cpu().numpy()
         energy = float((np.sum(sums[:3]) / sums[3]).real)
         return energy, sums, E
 
@@ -83,7 +111,11 @@ class Simulation:
         if step % self.rp.walker_ortho_interval == 0:
             self.prop.Orthogonalize(self.wset)
         if step % self.rp.population_control_interval == 0:
-            A.population_control(self.wset, self.walker_rng)
+            if _world() > 1:
+                from .population import population_control_distributed
+                population_control_distributed(self.wset, self.walker_rng)
+            else:
+                A.population_control(self.wset, self.walker_rng)
         out = None
         if step >= self.rp.equilibration_steps:
             if measure and step % self.rp.measure_interval == 0:
