@@ -289,6 +289,28 @@ int afqmc_host_rng_create(unsigned long long seed, afqmc_host_rng* out);
 int afqmc_host_rng_destroy(afqmc_host_rng rng);
 int afqmc_host_rng_uniform(afqmc_host_rng rng, double* out, long n);
 
+/* ---------------------------------------------------------------------------------------
+ * PHMSD (particle-hole multi-determinant) energy kernels
+ * -------------------------------------------------------------------------------------- */
+/* ph_excited_2body_energy_dense_cholesky (Wavefunctions/detail/phmsd_impl.hpp:33-153): for every
+ * walker w and determinant d of one excitation shell (nex holes -> nex particles),
+ *   EX[w] -= 1/2 wgt[d][w] eX(w,d),  EJ[w] += 1/2 wgt[d][w] (sum_n KE[d][w][n]^2 - eJ0(w)),
+ * KE[d][w][n] written.  Device arrays: iexcit [ndet][2][nex] (holes = electron indices into
+ * refc, then particles = active orbitals), refc [nelec], Twina [nw][nelec][nchol][nact],
+ * R [nw][ndet][nex][nact], wgt [ndet][nw], EX/EJ [nw], KE [ndet][nw][nchol].  nex <= 8.
+ * The excitation lists are validated on the host first (synchronous copy of iexcit, refc). */
+int afqmc_ph_excited_2body_energy(const int* iexcit, const int* refc, const afqmc_c128* Twina,
+                                  const afqmc_c128* R, const afqmc_c128* wgt, int nw, int ndet,
+                                  int nex, int nact, int nelec, int nchol, afqmc_c128* EX,
+                                  afqmc_c128* EJ, afqmc_c128* KE, afqmc_stream stream);
+/* ph_excited_1body_energy (phmsd_impl.hpp:156-193): E[w] += sum_d wgt[d][w] sum_p
+ * (S[w][hole_p] . R[w][d][p] + S[w][hole_p][particle_p] - S[w][hole_p][refc[hole_p]]).
+ * S [nw][nelec][nact]; other layouts as above. */
+int afqmc_ph_excited_1body_energy(const int* iexcit, const int* refc, const afqmc_c128* S,
+                                  const afqmc_c128* R, const afqmc_c128* wgt, int nw, int ndet,
+                                  int nex, int nact, int nelec, afqmc_c128* E,
+                                  afqmc_stream stream);
+
 /* comb (population_control.hpp:34-65): host arrays; draws one uniform from rng. */
 int afqmc_comb(afqmc_host_rng rng, const double* weights, int n, int num_target, int* offspring);
 /* plan_walker_exchange (population_control.hpp:87-133): pure host logic. plan holds up to

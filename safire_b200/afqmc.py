@@ -433,3 +433,27 @@ def pseudo_energy_sums(wset: WalkerSet, dt, out=None, stream=None):
                                                   device=wset.buffer.device)
     call("afqmc_pseudo_energy_sums", wset.handle, float(dt), _ptr(out), _stream(stream))
     return out
+
+
+# --------------------------------------------------------------------------------------------
+# PHMSD energy kernels (Wavefunctions/detail/phmsd_impl.hpp)
+# --------------------------------------------------------------------------------------------
+class phmsd:  # noqa: N801 (reference namespace of the free functions)
+    @staticmethod
+    def ph_excited_2body_energy(iexcit, refc, Twina, R, wgt, EX, EJ, KE, stream=None):
+        """EX -= 1/2 wgt eX, EJ += 1/2 wgt (K.K - eJ0), KE written (device tensors; iexcit
+        [ndet][2*nex] int32, refc [nelec] int32, Twina [nw][nelec][nchol][nact],
+        R [nw][ndet][nex][nact], wgt [ndet][nw])."""
+        nw, ndet, nex, nact = R.shape
+        nelec, nchol = Twina.shape[1], Twina.shape[2]
+        call("afqmc_ph_excited_2body_energy", _ptr(iexcit), _ptr(refc), _ptr(Twina), _ptr(R),
+             _ptr(wgt), nw, ndet, nex, nact, nelec, nchol, _ptr(EX), _ptr(EJ), _ptr(KE),
+             _stream(stream))
+
+    @staticmethod
+    def ph_excited_1body_energy(iexcit, refc, S, R, wgt, E, stream=None):
+        """E += sum_d wgt sum_p (S.R + S[particle] - S[refc]) (device tensors; S [nw][nelec][nact])."""
+        nw, ndet, nex, nact = R.shape
+        nelec = S.shape[1]
+        call("afqmc_ph_excited_1body_energy", _ptr(iexcit), _ptr(refc), _ptr(S), _ptr(R),
+             _ptr(wgt), nw, ndet, nex, nact, nelec, _ptr(E), _stream(stream))

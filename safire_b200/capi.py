@@ -58,6 +58,9 @@ _SIGS = {
     "afqmc_ham_device_error": (i32, [vp, C.POINTER(C.c_uint)]),
     "afqmc_ham_set_exchange_split": (i32, [vp, i32]),
     "afqmc_ham_set_taylor_fused": (i32, [vp, i32]),
+    "afqmc_ph_excited_2body_energy": (i32, [vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, i32,
+                                            vp, vp, vp, vp]),
+    "afqmc_ph_excited_1body_energy": (i32, [vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, vp, vp]),
     "afqmc_wset_create": (i32, [i32, i32, i32, i32, i32, C.POINTER(vp)]),
     "afqmc_wset_destroy": (i32, [vp]),
     "afqmc_wset_buffer": (i32, [vp, C.POINTER(vp), C.POINTER(i64), C.POINTER(i32)]),

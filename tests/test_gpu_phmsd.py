@@ -1,0 +1,84 @@
+"""PHMSD energy kernels through the C ABI on the GPU: the reference's golden values
+(tests/test_phmsd_components.cpp:41-47) and the oracle at other sizes."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import phmsd as P
+from tests.golden import phmsd_golden as g
+from tests.gpu_helpers import rel_err, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+
+def _i32(x, cuda):
+    return torch.as_tensor(np.ascontiguousarray(x, dtype=np.int32), device=cuda)
+
+
+def _run2(cuda, iexcit, refc, T, R, wgt, EX0=None, EJ0=None):
+    from safire_b200 import afqmc as A
+    nw, ndet, nex, nact = R.shape
+    EX = to_dev(np.zeros(nw, complex) if EX0 is None else EX0)
+    EJ = to_dev(np.zeros(nw, complex) if EJ0 is None else EJ0)
+    KE = torch.zeros((ndet, nw, T.shape[2]), dtype=torch.complex128, device=cuda)
+    A.phmsd.ph_excited_2body_energy(_i32(iexcit, cuda), _i32(refc, cuda), to_dev(T), to_dev(R),
+                                    to_dev(wgt), EX, EJ, KE)
+    return to_host(EX), to_host(EJ), to_host(KE)
+
+
+@pytest.mark.parametrize("nex", [1, 2, 3, 4, 5])
+def test_ph_excited_2body_golden(cuda, nex):
+    iexcit, refc, T, R, wgt = g.fixture(nex)
+    EX, EJ, _ = _run2(cuda, iexcit, refc, T, R, wgt)
+    ref = g.EXJ_REF[nex - 1]
+    assert abs(EX[0] - ref[0]) <= 1e-8 * abs(ref[0]), (EX[0], ref[0])
+    assert abs(EJ[0] - ref[1]) <= 1e-8 * abs(ref[1]), (EJ[0], ref[1])
+
+
+def _random_case(seed, nw, ndet, nex, nact, nelec, nchol):
+    rs = np.random.default_rng(seed)
+    rc = lambda *s: rs.standard_normal(s) + 1j * rs.standard_normal(s)  # noqa: E731
+    refc = rs.permutation(nact)[:nelec].astype(np.int32)
+    virt = np.setdiff1d(np.arange(nact), refc)
+    iexcit = np.zeros((ndet, 2 * nex), dtype=np.int32)
+    for d in range(ndet):
+        iexcit[d, :nex] = rs.choice(nelec, nex, replace=False)
+        iexcit[d, nex:] = rs.choice(virt, nex, replace=False)
+    return iexcit, refc, rc(nw, nelec, nchol, nact), rc(nw, ndet, nex, nact), rc(ndet, nw)
+
+
+@pytest.mark.parametrize("nex", [1, 2, 3, 4])
+def test_ph_excited_2body_vs_oracle(cuda, nex):
+    iexcit, refc, T, R, wgt = _random_case(10 + nex, 3, 37, nex, 23, 9, 70)
+    rs = np.random.default_rng(99)
+    EX0 = rs.standard_normal(3) + 1j * rs.standard_normal(3)
+    EJ0 = rs.standard_normal(3) + 1j * rs.standard_normal(3)
+    EX, EJ, KE = _run2(cuda, iexcit, refc, T, R, wgt, EX0, EJ0)
+    EXo, EJo, KEo = P.ph_excited_2body_energy_dense_cholesky(iexcit, refc, T, R, wgt, EX0, EJ0)
+    assert rel_err(EX, EXo) < 1e-10
+    assert rel_err(EJ, EJo) < 1e-10
+    assert rel_err(KE, KEo) < 1e-12
+
+
+@pytest.mark.parametrize("nex", [1, 3])
+def test_ph_excited_1body_vs_oracle(cuda, nex):
+    from safire_b200 import afqmc as A
+    iexcit, refc, T, R, wgt = _random_case(20 + nex, 4, 29, nex, 31, 11, 8)
+    rs = np.random.default_rng(7)
+    S = rs.standard_normal((4, 11, 31)) + 1j * rs.standard_normal((4, 11, 31))
+    E0 = rs.standard_normal(4) + 1j * rs.standard_normal(4)
+    E = to_dev(E0.copy())
+    A.phmsd.ph_excited_1body_energy(_i32(iexcit, cuda), _i32(refc, cuda), to_dev(S), to_dev(R),
+                                    to_dev(wgt), E)
+    Eo = P.ph_excited_1body_energy(iexcit, refc, S, R, wgt, E0)
+    assert rel_err(to_host(E), Eo) < 1e-12
+
+
+def test_ph_excited_rejects_bad_index(cuda):
+    """A hole outside the electron range is reported before any kernel reads with it."""
+    from safire_b200 import afqmc as A
+    from safire_b200.capi import AfqmcError
+    iexcit, refc, T, R, wgt = _random_case(5, 1, 4, 2, 12, 5, 6)
+    iexcit[2, 0] = 5  # nelec = 5
+    with pytest.raises(AfqmcError):
+        _run2(cuda, iexcit, refc, T, R, wgt)
