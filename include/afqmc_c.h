@@ -311,6 +311,27 @@ int afqmc_ph_excited_1body_energy(const int* iexcit, const int* refc, const afqm
                                   int nex, int nact, int nelec, afqmc_c128* E,
                                   afqmc_stream stream);
 
+/* PHMSD trial (Wavefunctions/PHMSD.hpp:60-120, Excitations.hpp:207-554) in explicit arrays, all
+ * on the host: orbmat_s [nact_s][M] the active orbitals conjugate-transposed; refc_s [N_s] the
+ * active orbital of every electron in the reference; unique excitations u = 1..nuniq_s-1 of each
+ * spin (u = 0 is the reference): nex_s[u-1] holes/particles each, their lists concatenated in
+ * exc_s as [holes (electron indices), particles (active orbitals)]; determinant k couples unique
+ * excitations det_up[k], det_dn[k] with coefficient coef[k].  Every index is validated. */
+typedef struct afqmc_phmsd_s* afqmc_phmsd;
+int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact_dn,
+                       const afqmc_c128* orbmat_up, const afqmc_c128* orbmat_dn,
+                       const int* refc_up, const int* refc_dn, int nuniq_up, const int* nex_up,
+                       const int* exc_up, int nuniq_dn, const int* nex_dn, const int* exc_dn,
+                       int ndet, const int* det_up, const int* det_dn, const afqmc_c128* coef,
+                       afqmc_phmsd* out);
+int afqmc_phmsd_destroy(afqmc_phmsd trial);
+/* PHMSD::Log_Overlap (PHMSD.cpp:804-900), COLLINEAR walkers: ovlp[w] (device, written) =
+ * log(sum_k c_k ov_up,k ov_dn,k) + log det of the reference blocks, with the Woodbury
+ * evaluation of every excitation overlap.  wbuf: walker rows [W][ldS], S_up [M][nup] then
+ * S_dn [M][ndn] at the start of each row (the walker-buffer layout). */
+int afqmc_phmsd_log_overlap(afqmc_phmsd trial, const afqmc_c128* wbuf, long ldS,
+                            afqmc_c128* ovlp, int W, afqmc_stream stream);
+
 /* comb (population_control.hpp:34-65): host arrays; draws one uniform from rng. */
 int afqmc_comb(afqmc_host_rng rng, const double* weights, int n, int num_target, int* offspring);
 /* plan_walker_exchange (population_control.hpp:87-133): pure host logic. plan holds up to

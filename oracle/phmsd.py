@@ -91,3 +91,33 @@ def ph_excited_1body_energy(iexcit, refc, S, R, wgt, E=None):
                 e_ += np.sum(S[iw, ip] * R[iw, d, p]) + S[iw, ip, iex[d, 1, p]] - S[iw, ip, refc[ip]]
             E[iw] += wgt[d, iw] * e_
     return E
+
+
+def phmsd_log_overlap(trial, S_up, S_dn):
+    """PHMSD::Log_Overlap (Wavefunctions/PHMSD.cpp:804-900) for COLLINEAR walkers:
+    per spin Log_OverlapForWoodbury (density_matrix.hpp:487-532: TMN = A B, TNN = TMN[refc],
+    log det TNN accumulated with log_determinant_from_getrf, QQ0 = TMN TNN^{-1}), the unique
+    excitation overlaps det(QQ0[particles, holes]) (phmsd_helpers.hpp:111-193), then
+    log(sum_k c_k ov_up[k] ov_dn[k]) + log_ov.  trial: safire_b200.synth.PHMSDTrial layout;
+    S_s [W, M, N_s].  Returns (log overlap [W], [ov_up [nuniq_up, W], ov_dn [nuniq_dn, W]])."""
+    from oracle.afqmc import _getrf_ref, _getri_or_zero_ref, log_det_from_getrf
+    W = S_up.shape[0]
+    log_ov = np.zeros(W, complex)
+    ovs = []
+    for s, S in ((0, S_up), (1, S_dn)):
+        A = trial.orbmat[s]
+        refc = trial.refc[s]
+        TMN = np.einsum("am,wmn->wan", A, S)
+        QQ0 = np.empty_like(TMN)
+        for w in range(W):
+            lu, piv1, info = _getrf_ref(TMN[w][refc, :])
+            log_ov[w] = log_det_from_getrf(lu, piv1, complex(log_ov[w]))
+            QQ0[w] = TMN[w] @ _getri_or_zero_ref(lu, piv1)
+        ov = [np.ones(W, complex)]
+        for n in sorted(trial.exc[s]):
+            for e in trial.exc[s][n]:
+                holes, parts = e[:n], e[n:]
+                ov.append(np.linalg.det(QQ0[:, parts][:, :, holes]))
+        ovs.append(np.array(ov))
+    tot = np.einsum("k,kw,kw->w", trial.coef, ovs[0][trial.det_up], ovs[1][trial.det_dn])
+    return np.log(tot) + log_ov, ovs

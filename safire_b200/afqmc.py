@@ -457,3 +457,49 @@ class phmsd:  # noqa: N801 (reference namespace of the free functions)
         nelec = S.shape[1]
         call("afqmc_ph_excited_1body_energy", _ptr(iexcit), _ptr(refc), _ptr(S), _ptr(R),
              _ptr(wgt), nw, ndet, nex, nact, nelec, _ptr(E), _stream(stream))
+
+
+class PHMSD:
+    """Particle-hole multi-determinant trial (Wavefunctions/PHMSD.hpp) from a
+    safire_b200.synth.PHMSDTrial (or any object with the same fields)."""
+
+    def __init__(self, trial):
+        self.trial = trial
+        arrs = []
+
+        def keep(a, dtype):
+            a = np.ascontiguousarray(a, dtype=dtype)
+            arrs.append(a)
+            return _host_ptr(a)
+
+        nu, ne, ex = [], [], []
+        for s in (0, 1):
+            n_list, e_list = [], []
+            for n in sorted(trial.exc[s]):
+                for e in trial.exc[s][n]:
+                    n_list.append(n)
+                    e_list.extend(int(x) for x in e)
+            nu.append(1 + len(n_list))
+            ne.append(np.array(n_list or [0], dtype=np.int32))
+            ex.append(np.array(e_list or [0], dtype=np.int32))
+        self.nuniq = nu
+        h = vp()
+        call("afqmc_phmsd_create", trial.M, trial.nup, trial.ndn, trial.orbmat[0].shape[0],
+             trial.orbmat[1].shape[0], keep(trial.orbmat[0], np.complex128),
+             keep(trial.orbmat[1], np.complex128), keep(trial.refc[0], np.int32),
+             keep(trial.refc[1], np.int32), nu[0], keep(ne[0], np.int32), keep(ex[0], np.int32),
+             nu[1], keep(ne[1], np.int32), keep(ex[1], np.int32), int(trial.coef.size),
+             keep(trial.det_up, np.int32), keep(trial.det_dn, np.int32),
+             keep(trial.coef, np.complex128), C.byref(h))
+        self.handle = h
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and capi._lib is not None:
+            capi._lib.afqmc_phmsd_destroy(h)
+            self.handle = None
+
+    def Log_Overlap(self, wbuf, ovlp, stream=None):
+        """ovlp [W] (device) <- log overlap of every walker row of wbuf [W][ldS] (device)."""
+        call("afqmc_phmsd_log_overlap", self.handle, _ptr(wbuf), int(wbuf.stride(0)), _ptr(ovlp),
+             int(wbuf.shape[0]), _stream(stream))

@@ -10,9 +10,13 @@
 //   iexcit [ndet][2][nex] holes (electron indices into refc), then particles (active orbitals)
 //   Twina  [nw][nelec][nchol][nact], R [nw][ndet][nex][nact], wgt [ndet][nw], S [nw][nelec][nact]
 //   EX, EJ, E [nw] (accumulated), KE [ndet][nw][nchol] (written)
+#include <cstring>
+#include <memory>
 #include <vector>
 
 #include "common.cuh"
+#include "detops.cuh"
+#include "zgemm.cuh"
 
 namespace afqmc {
 namespace {
@@ -176,6 +180,83 @@ __global__ void __launch_bounds__(PH_THREADS) ph_excited_1body_kernel(
   }
 }
 
+// TNN[w][i][:] = TMN[w][refc[i]][:]  (Log_OverlapForWoodbury's copy_select of the reference rows)
+__global__ void gather_ref_rows_kernel(const c128* __restrict__ TMN, const int* __restrict__ refc,
+                                       c128* __restrict__ TNN, int nact, int N) {
+  const int w = blockIdx.x;
+  for (int k = threadIdx.x; k < N * N; k += blockDim.x) {
+    const int i = k / N, j = k - i * N;
+    TNN[size_t(w) * N * N + k] = TMN[(size_t(w) * nact + refc[i]) * N + j];
+  }
+}
+
+// ov[w][u] = det(QQ0[w][particles_u][holes_u]) for every unique excitation u >= 1 (ov[w][0] = 1):
+// partial-pivoting LU of the nex x nex block in registers / local memory (nex <= PH_NEX_MAX).
+__global__ void excitation_det_kernel(const c128* __restrict__ QQ0, const int* __restrict__ uoff,
+                                      const int* __restrict__ unex, const int* __restrict__ uexc,
+                                      int nuniq, int W, int nact, int N, c128* __restrict__ ov) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(nuniq) * W) return;
+  const int w = int(t / nuniq), u = int(t - long(w) * nuniq);
+  if (u == 0) {
+    ov[t] = cmk(1.0, 0.0);
+    return;
+  }
+  const int n = unex[u];
+  const int* e = uexc + uoff[u];
+  const c128* Q = QQ0 + size_t(w) * nact * N;
+  c128 a[PH_NEX_MAX][PH_NEX_MAX];
+  for (int p = 0; p < n; ++p)
+    for (int q = 0; q < n; ++q) a[p][q] = Q[size_t(e[n + p]) * N + e[q]];
+  c128 det = cmk(1.0, 0.0);
+  for (int k = 0; k < n; ++k) {
+    int piv = k;
+    double best = cabs1(a[k][k]);
+    for (int i = k + 1; i < n; ++i) {
+      const double v = cabs1(a[i][k]);
+      if (v > best) {
+        best = v;
+        piv = i;
+      }
+    }
+    if (!(best > 0.0)) {
+      det = cmk(0.0, 0.0);
+      break;
+    }
+    if (piv != k) {
+      for (int j = 0; j < n; ++j) {
+        const c128 x = a[k][j];
+        a[k][j] = a[piv][j];
+        a[piv][j] = x;
+      }
+      det = cmk(-det.x, -det.y);
+    }
+    det = cmul(det, a[k][k]);
+    const c128 dinv = cdiv(cmk(1.0, 0.0), a[k][k]);
+    for (int i = k + 1; i < n; ++i) {
+      const c128 f = cmul(a[i][k], dinv);
+      for (int j = k + 1; j < n; ++j) a[i][j] = csub(a[i][j], cmul(f, a[k][j]));
+    }
+  }
+  ov[t] = det;
+}
+
+// ovlp[w] = log(sum_k c_k ov_up[w][det_up k] ov_dn[w][det_dn k]) + logov[w]  (PHMSD.cpp:884-896)
+__global__ void __launch_bounds__(PH_THREADS) phmsd_combine_kernel(
+    const c128* __restrict__ ov_up, const c128* __restrict__ ov_dn, int nu_up, int nu_dn,
+    const int* __restrict__ det_up, const int* __restrict__ det_dn, const c128* __restrict__ coef,
+    int ndet, const c128* __restrict__ logov, c128* __restrict__ ovlp) {
+  __shared__ double red[PH_THREADS / 32 * 6];
+  const int w = blockIdx.x;
+  const c128* ou = ov_up + size_t(w) * nu_up;
+  const c128* od = ov_dn + size_t(w) * nu_dn;
+  c128 s = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0);
+  for (int k = threadIdx.x; k < ndet; k += blockDim.x)
+    s = cadd(s, cmul(coef[k], cmul(ou[det_up[k]], od[det_dn[k]])));
+  block_sum3(s, z1, z2, red);
+  if (threadIdx.x == 0) ovlp[w] = cadd(clog(s), logov[w]);
+}
+
 int check_dims(const char* who, int nw, int ndet, int nex, int nact, int nelec) {
   if (nw < 0 || ndet < 0 || nex < 1 || nex > PH_NEX_MAX || nact < 1 || nelec < 1) {
     set_error_detail("%s: nw=%d ndet=%d nex=%d (1..%d) nact=%d nelec=%d", who, nw, ndet, nex,
@@ -264,4 +345,201 @@ extern "C" int afqmc_ph_excited_1body_energy(const int* iexcit, const int* refc,
       iexcit, refc, reinterpret_cast<const c128*>(S), reinterpret_cast<const c128*>(R),
       reinterpret_cast<const c128*>(wgt), nw, ndet, nex, nact, nelec, reinterpret_cast<c128*>(E));
   return launch_status("ph_excited_1body_kernel");
+}
+
+// ---------------------------------------------------------------------------------------------
+// PHMSD trial handle and its log overlap (PHMSD::Log_Overlap, Wavefunctions/PHMSD.cpp:804-900)
+// ---------------------------------------------------------------------------------------------
+struct afqmc_phmsd_s {
+  int device = 0, M = 0, nel[2] = {0, 0}, nact[2] = {0, 0}, nuniq[2] = {0, 0}, ndet = 0;
+  c128* orbmat[2] = {nullptr, nullptr};
+  int* refc[2] = {nullptr, nullptr};
+  int* uoff[2] = {nullptr, nullptr};
+  int* unex[2] = {nullptr, nullptr};
+  int* uexc[2] = {nullptr, nullptr};
+  int* det[2] = {nullptr, nullptr};
+  c128* coef = nullptr;
+  int capW = 0;
+  c128 *TMN = nullptr, *TNN = nullptr, *QQ0 = nullptr, *ov[2] = {nullptr, nullptr};
+  c128* logov = nullptr;
+  void free_scratch() {
+    for (c128** p : {&TMN, &TNN, &QQ0, &ov[0], &ov[1], &logov})
+      if (*p) {
+        cudaFree(*p);
+        *p = nullptr;
+      }
+    capW = 0;
+  }
+  ~afqmc_phmsd_s() {
+    free_scratch();
+    for (int s = 0; s < 2; ++s) {
+      cudaFree(orbmat[s]);
+      cudaFree(refc[s]);
+      cudaFree(uoff[s]);
+      cudaFree(unex[s]);
+      cudaFree(uexc[s]);
+      cudaFree(det[s]);
+    }
+    cudaFree(coef);
+  }
+};
+
+namespace {
+
+template <typename T>
+int to_device(T** dst, const T* src, size_t n) {
+  if (n == 0) n = 1;
+  AFQMC_CUDA_TRY(cudaMalloc(dst, n * sizeof(T)));
+  if (src) AFQMC_CUDA_TRY(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  return AFQMC_OK;
+}
+
+int phmsd_scratch(afqmc_phmsd h, int W) {
+  if (h->capW >= W) return AFQMC_OK;
+  AFQMC_CUDA_TRY(cudaDeviceSynchronize());
+  h->free_scratch();
+  const int na = h->nact[0] > h->nact[1] ? h->nact[0] : h->nact[1];
+  const int ne = h->nel[0] > h->nel[1] ? h->nel[0] : h->nel[1];
+  AFQMC_CUDA_TRY(cudaMalloc(&h->TMN, sizeof(c128) * size_t(W) * na * ne));
+  AFQMC_CUDA_TRY(cudaMalloc(&h->QQ0, sizeof(c128) * size_t(W) * na * ne));
+  AFQMC_CUDA_TRY(cudaMalloc(&h->TNN, sizeof(c128) * size_t(W) * ne * ne));
+  for (int s = 0; s < 2; ++s)
+    AFQMC_CUDA_TRY(cudaMalloc(&h->ov[s], sizeof(c128) * size_t(W) * h->nuniq[s]));
+  AFQMC_CUDA_TRY(cudaMalloc(&h->logov, sizeof(c128) * size_t(W)));
+  h->capW = W;
+  return AFQMC_OK;
+}
+
+}  // namespace
+
+extern "C" int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact_dn,
+                                  const afqmc_c128* orbmat_up, const afqmc_c128* orbmat_dn,
+                                  const int* refc_up, const int* refc_dn, int nuniq_up,
+                                  const int* nex_up, const int* exc_up, int nuniq_dn,
+                                  const int* nex_dn, const int* exc_dn, int ndet,
+                                  const int* det_up, const int* det_dn, const afqmc_c128* coef,
+                                  afqmc_phmsd* out) {
+  AFQMC_CHECK_ARG(out && orbmat_up && orbmat_dn && refc_up && refc_dn && det_up && det_dn && coef,
+                  "afqmc_phmsd_create: null argument");
+  *out = nullptr;
+  AFQMC_CHECK_ARG(M > 0 && nup > 0 && ndn > 0 && nact_up >= nup && nact_dn >= ndn &&
+                      nact_up <= M && nact_dn <= M && nuniq_up >= 1 && nuniq_dn >= 1 && ndet >= 1,
+                  "afqmc_phmsd_create: bad sizes (M=%d nup=%d ndn=%d nact=%d/%d nuniq=%d/%d "
+                  "ndet=%d)", M, nup, ndn, nact_up, nact_dn, nuniq_up, nuniq_dn, ndet);
+  const int nel[2] = {nup, ndn}, nact[2] = {nact_up, nact_dn}, nuniq[2] = {nuniq_up, nuniq_dn};
+  const int* refc[2] = {refc_up, refc_dn};
+  const int* nexs[2] = {nex_up, nex_dn};
+  const int* excs[2] = {exc_up, exc_dn};
+  // host validation of every index the kernels will read with
+  std::vector<int> off[2], nex[2];
+  for (int s = 0; s < 2; ++s) {
+    for (int i = 0; i < nel[s]; ++i)
+      AFQMC_CHECK_ARG(refc[s][i] >= 0 && refc[s][i] < nact[s],
+                      "afqmc_phmsd_create: refc[%d][%d] = %d outside [0, %d)", s, i, refc[s][i],
+                      nact[s]);
+    AFQMC_CHECK_ARG(nuniq[s] == 1 || (nexs[s] && excs[s]),
+                    "afqmc_phmsd_create: null excitation list");
+    off[s].assign(nuniq[s], 0);
+    nex[s].assign(nuniq[s], 0);
+    int pos = 0;
+    for (int u = 1; u < nuniq[s]; ++u) {
+      const int n = nexs[s][u - 1];
+      AFQMC_CHECK_ARG(n >= 1 && n <= PH_NEX_MAX && n <= nel[s],
+                      "afqmc_phmsd_create: excitation %d of spin %d has nex = %d (1..%d)", u, s,
+                      n, PH_NEX_MAX);
+      off[s][u] = pos;
+      nex[s][u] = n;
+      for (int q = 0; q < n; ++q) {
+        const int hole = excs[s][pos + q], part = excs[s][pos + n + q];
+        AFQMC_CHECK_ARG(hole >= 0 && hole < nel[s] && part >= 0 && part < nact[s],
+                        "afqmc_phmsd_create: excitation %d of spin %d: hole %d (< %d), particle "
+                        "%d (< %d)", u, s, hole, nel[s], part, nact[s]);
+      }
+      pos += 2 * n;
+    }
+  }
+  for (int k = 0; k < ndet; ++k)
+    AFQMC_CHECK_ARG(det_up[k] >= 0 && det_up[k] < nuniq_up && det_dn[k] >= 0 &&
+                        det_dn[k] < nuniq_dn,
+                    "afqmc_phmsd_create: determinant %d couples (%d, %d) outside (%d, %d)", k,
+                    det_up[k], det_dn[k], nuniq_up, nuniq_dn);
+  std::unique_ptr<afqmc_phmsd_s> h(new afqmc_phmsd_s);
+  cudaGetDevice(&h->device);
+  h->M = M;
+  h->ndet = ndet;
+  const afqmc_c128* orb[2] = {orbmat_up, orbmat_dn};
+  for (int s = 0; s < 2; ++s) {
+    h->nel[s] = nel[s];
+    h->nact[s] = nact[s];
+    h->nuniq[s] = nuniq[s];
+    AFQMC_TRY(to_device(&h->orbmat[s], reinterpret_cast<const c128*>(orb[s]),
+                        size_t(nact[s]) * M));
+    AFQMC_TRY(to_device(&h->refc[s], refc[s], size_t(nel[s])));
+    AFQMC_TRY(to_device(&h->uoff[s], off[s].data(), off[s].size()));
+    AFQMC_TRY(to_device(&h->unex[s], nex[s].data(), nex[s].size()));
+    size_t nexc = 0;
+    for (int u = 1; u < nuniq[s]; ++u) nexc += 2 * size_t(nex[s][u]);
+    AFQMC_TRY(to_device(&h->uexc[s], nuniq[s] > 1 ? excs[s] : nullptr, nexc));
+  }
+  AFQMC_TRY(to_device(&h->det[0], det_up, size_t(ndet)));
+  AFQMC_TRY(to_device(&h->det[1], det_dn, size_t(ndet)));
+  AFQMC_TRY(to_device(&h->coef, reinterpret_cast<const c128*>(coef), size_t(ndet)));
+  *out = h.release();
+  return AFQMC_OK;
+}
+
+extern "C" int afqmc_phmsd_destroy(afqmc_phmsd h) {
+  if (h) {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(h->device);
+    delete h;
+    cudaSetDevice(prev);
+  }
+  return AFQMC_OK;
+}
+
+extern "C" int afqmc_phmsd_log_overlap(afqmc_phmsd h, const afqmc_c128* wbuf, long ldS,
+                                       afqmc_c128* ovlp, int W, afqmc_stream stream) {
+  AFQMC_CHECK_ARG(h && wbuf && ovlp, "afqmc_phmsd_log_overlap: null argument");
+  AFQMC_CHECK_ARG(W >= 0 && ldS >= long(h->M) * (h->nel[0] + h->nel[1]),
+                  "afqmc_phmsd_log_overlap: W=%d, walker stride %ld < M (nup + ndn)", W, ldS);
+  if (W == 0) return AFQMC_OK;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  AFQMC_TRY(phmsd_scratch(h, W));
+  AFQMC_CUDA_TRY(cudaMemsetAsync(h->logov, 0, sizeof(c128) * W, s));
+  const c128* S = reinterpret_cast<const c128*>(wbuf);
+  for (int sp = 0; sp < 2; ++sp) {
+    const int N = h->nel[sp], na = h->nact[sp];
+    const c128* Ss = S + (sp == 0 ? 0 : long(h->M) * h->nel[0]);
+    // TMN = A S   (math::product(A,B,TMN), density_matrix.hpp:510)
+    GemmParams p{};
+    p.m = na; p.n = N; p.k = h->M;
+    p.A = h->orbmat[sp]; p.lda = h->M; p.strideA = 0;
+    p.B = Ss; p.ldb = N; p.strideB = ldS;
+    p.C = h->TMN; p.ldc = N; p.strideC = long(na) * N;
+    p.alpha = cmk(1, 0); p.beta = cmk(0, 0);
+    AFQMC_TRY(zgemm(s, W, GN, false, GN, false, p));
+    gather_ref_rows_kernel<<<W, 128, 0, s>>>(h->TMN, h->refc[sp], h->TNN, na, N);
+    AFQMC_TRY(launch_status("gather_ref_rows_kernel"));
+    // log det TNN accumulated, TNN <- TNN^{-1}
+    AFQMC_TRY(batched_logdet_inverse(s, h->TNN, long(N) * N, h->TNN, long(N) * N, h->logov, W, N,
+                                     true, cmk(1, 0), cmk(0, 0)));
+    // QQ0 = TMN TNN^{-1}
+    GemmParams q{};
+    q.m = na; q.n = N; q.k = N;
+    q.A = h->TMN; q.lda = N; q.strideA = long(na) * N;
+    q.B = h->TNN; q.ldb = N; q.strideB = long(N) * N;
+    q.C = h->QQ0; q.ldc = N; q.strideC = long(na) * N;
+    q.alpha = cmk(1, 0); q.beta = cmk(0, 0);
+    AFQMC_TRY(zgemm(s, W, GN, false, GN, false, q));
+    const long nt = long(h->nuniq[sp]) * W;
+    excitation_det_kernel<<<unsigned((nt + 127) / 128), 128, 0, s>>>(
+        h->QQ0, h->uoff[sp], h->unex[sp], h->uexc[sp], h->nuniq[sp], W, na, N, h->ov[sp]);
+    AFQMC_TRY(launch_status("excitation_det_kernel"));
+  }
+  phmsd_combine_kernel<<<W, PH_THREADS, 0, s>>>(h->ov[0], h->ov[1], h->nuniq[0], h->nuniq[1],
+                                                h->det[0], h->det[1], h->coef, h->ndet, h->logov,
+                                                reinterpret_cast<c128*>(ovlp));
+  return launch_status("phmsd_combine_kernel");
 }

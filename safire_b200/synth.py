@@ -69,3 +69,89 @@ def make_workload(name="cfg1", seed=0, W=None, M=None, N=None, Nc=None):
     PsiT = [np.ascontiguousarray(phi.conj().T).astype(np.complex128)]
     return Workload(name, M, nup, ndn, Nc, W, dt, CLOSED,
                     h1[None].astype(np.complex128), Likn[None], 0.0, PsiT)
+
+
+# --------------------------------------------------------------------------------------------
+# Particle-hole multi-determinant (PHMSD) trial
+# --------------------------------------------------------------------------------------------
+@dataclass
+class PHMSDTrial:
+    """A PHMSD trial in the layout afqmc_phmsd_create takes.
+
+    Per spin s: orbmat[s] [nact_s][M] (the active orbitals, conjugate-transposed), refc[s] [N_s]
+    (active orbital of each electron in the reference), exc[s] {nex: [nuniq][2 nex] int32} (the
+    unique excitations of that spin, holes as electron indices then particles as active
+    orbitals).  Unique index 0 is the reference; then the nex = 1 list, nex = 2, ... in order.
+    A determinant k couples unique alpha excitation det_up[k] with unique beta excitation
+    det_dn[k] and has coefficient coef[k]."""
+    M: int
+    nup: int
+    ndn: int
+    orbmat: list
+    refc: list
+    exc: list
+    det_up: np.ndarray
+    det_dn: np.ndarray
+    coef: np.ndarray
+
+    def unique_count(self, s):
+        return 1 + sum(len(v) for v in self.exc[s].values())
+
+
+def make_phmsd_trial(M, nup, ndn, orbitals, nocc=20, nvirt=40, ndet=4096, max_level=4, seed=0):
+    """Reference determinant plus ndet - 1 distinct excitations of levels 1..max_level, each a
+    (alpha, beta) pair of excitations confined to the top `nocc` occupied and the lowest `nvirt`
+    virtual orbitals of `orbitals` [M][M] (columns = orbitals, lowest first; the same orbitals for
+    both spins).  Level L = n_alpha + n_beta is drawn uniformly from 1..max_level and n_alpha
+    uniformly from max(0, L - nup_window)..min(L, window); holes and particles are drawn without
+    replacement.  Coefficients c = N(0,1) exp(-1.5 L) (the reference's L = 0), normalised."""
+    rng = np.random.default_rng(seed)
+    nact = max(nup, ndn) + nvirt
+    orbmat = np.ascontiguousarray(orbitals[:, :nact].conj().T).astype(np.complex128)
+    nel = (nup, ndn)
+    uniq = [dict(), dict()]   # spin -> {tuple: index}
+    lists = [dict(), dict()]  # spin -> {nex: [tuple]}
+    counts = [[1], [1]]
+
+    def key(s, holes, parts):
+        n = len(holes)
+        if n == 0:
+            return 0
+        t = tuple(sorted(holes)) + tuple(sorted(parts))
+        if t not in uniq[s]:
+            uniq[s][t] = None
+            lists[s].setdefault(n, []).append(t)
+        return t
+
+    dets = {(0, 0)}
+    order = [(0, 0)]
+    while len(order) < ndet:
+        L = int(rng.integers(1, max_level + 1))
+        na = int(rng.integers(max(0, L - min(nocc, ndn)), min(L, nocc, nup) + 1))
+        nb = L - na
+        ka = key(0, rng.choice(np.arange(nup - nocc, nup), na, replace=False).tolist(),
+                 rng.choice(np.arange(nup, nup + nvirt), na, replace=False).tolist())
+        kb = key(1, rng.choice(np.arange(ndn - nocc, ndn), nb, replace=False).tolist(),
+                 rng.choice(np.arange(ndn, ndn + nvirt), nb, replace=False).tolist())
+        if (ka, kb) in dets:
+            continue
+        dets.add((ka, kb))
+        order.append((ka, kb))
+    # unique indices: reference 0, then by excitation number in order of first appearance
+    index = [dict(), dict()]
+    exc = [dict(), dict()]
+    for s in (0, 1):
+        k = 1
+        for n in sorted(lists[s]):
+            exc[s][n] = np.array(lists[s][n], dtype=np.int32).reshape(-1, 2 * n)
+            for t in lists[s][n]:
+                index[s][t] = k
+                k += 1
+    det_up = np.array([0 if a == 0 else index[0][a] for a, _ in order], np.int32)
+    det_dn = np.array([0 if b == 0 else index[1][b] for _, b in order], np.int32)
+    level = np.array([(0 if a == 0 else len(a) // 2) + (0 if b == 0 else len(b) // 2)
+                      for a, b in order])
+    coef = rng.standard_normal(len(order)) * np.exp(-1.5 * level)
+    coef = (coef / np.linalg.norm(coef)).astype(np.complex128)
+    refc = [np.arange(nup, dtype=np.int32), np.arange(ndn, dtype=np.int32)]
+    return PHMSDTrial(M, nup, ndn, [orbmat, orbmat], refc, exc, det_up, det_dn, coef)

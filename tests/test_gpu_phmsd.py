@@ -82,3 +82,32 @@ def test_ph_excited_rejects_bad_index(cuda):
     iexcit[2, 0] = 5  # nelec = 5
     with pytest.raises(AfqmcError):
         _run2(cuda, iexcit, refc, T, R, wgt)
+
+
+def _trial(M, nup, ndn, nocc, nvirt, ndet, seed):
+    from safire_b200.synth import make_hamiltonian, make_phmsd_trial
+    h1, _ = make_hamiltonian(M, 2, 0.99, seed)
+    _, C = np.linalg.eigh(h1)
+    return make_phmsd_trial(M, nup, ndn, C, nocc=nocc, nvirt=nvirt, ndet=ndet, seed=seed)
+
+
+@pytest.mark.parametrize("M,nup,ndn,nocc,nvirt,ndet,W", [(24, 6, 5, 4, 8, 120, 3),
+                                                        (60, 15, 15, 8, 20, 700, 17)])
+def test_phmsd_log_overlap_vs_oracle(cuda, M, nup, ndn, nocc, nvirt, ndet, W):
+    """Woodbury log overlap of a multi-determinant trial (PHMSD.cpp:804-900) against the
+    oracle, walker rows in the walker-buffer layout with extra property columns."""
+    from safire_b200 import afqmc as A
+    t = _trial(M, nup, ndn, nocc, nvirt, ndet, seed=M)
+    rs = np.random.default_rng(M + 1)
+    Su = (rs.standard_normal((W, M, nup)) + 1j * rs.standard_normal((W, M, nup))) / np.sqrt(M)
+    Sd = (rs.standard_normal((W, M, ndn)) + 1j * rs.standard_normal((W, M, ndn))) / np.sqrt(M)
+    row = np.concatenate([Su.reshape(W, -1), Sd.reshape(W, -1), np.zeros((W, 11))], axis=1)
+    wbuf = to_dev(row)
+    ov = torch.zeros(W, dtype=torch.complex128, device=cuda)
+    A.PHMSD(t).Log_Overlap(wbuf, ov)
+    ref, _ = P.phmsd_log_overlap(t, Su, Sd)
+    got = to_host(ov)
+    # the log's imaginary part is a phase: compare modulo 2 pi
+    d = got - ref
+    d = d.real + 1j * ((d.imag + np.pi) % (2 * np.pi) - np.pi)
+    assert np.max(np.abs(d)) < 1e-10, (got, ref)
