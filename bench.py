@@ -41,6 +41,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--exchange-split", type=int, default=3, choices=[1, 3],
                     help="TF32 products per real product in the mixed exchange contraction")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch every kernel of a step eagerly instead of replaying the step's "
+                         "CUDA graph")
     ap.add_argument("--taylor-mode", type=int, default=1, choices=[0, 1, 2, 3],
                     help="mixed Taylor propagation: 0 per-term GEMMs, 1 fused (auto), 2 / 3 fused "
                          "with one / two walkers in flight per CTA")
@@ -255,6 +258,7 @@ def run_ours(args):
     wl = make_workload("cfg2")
     rp = RunParams(equilibration_steps=0, seed=0)
     sim = Simulation.from_workload(wl, W=W, precision=prec, rp=rp)
+    sim.use_graph = not args.no_graph
     if prec == A.PREC_MIXED and args.exchange_split != 3:
         sim.ham.set_exchange_split(args.exchange_split)
     if prec == A.PREC_MIXED and args.taylor_mode != 1:
@@ -274,6 +278,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     barrier()
     launches0 = capi.lib().afqmc_kernel_launches()
+    graph_k0 = sim.graph.kernels_replayed() if sim.graph is not None else 0
     clocks = ClockSampler(local)
     clocks.start()
     torch.cuda.synchronize()
@@ -287,6 +292,8 @@ def run_ours(args):
     barrier()
     clk = clocks.stop()
     launches = capi.lib().afqmc_kernel_launches() - launches0
+    if sim.graph is not None:  # kernels the step graph replayed inside the timed region
+        launches += sim.graph.kernels_replayed() - graph_k0
     t_ms = e0.elapsed_time(e1)
     if world > 1:
         t = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
@@ -406,6 +413,7 @@ def run_ours(args):
                        "precision": args.precision, "global_walkers": W * world,
                        "exchange_split": args.exchange_split if prec == A.PREC_MIXED else None,
                        "taylor_mode": args.taylor_mode if prec == A.PREC_MIXED else None,
+                       "step_graph": sim.graph is not None,
                        "parallelism": f"walker dp{world}",
                        "l2": "inputs larger than L2 (V 655 MB, Likn 512 MB per step)"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,

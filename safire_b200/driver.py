@@ -49,6 +49,42 @@ class RunParams:
     seed: int = 0
 
 
+class StepGraph:
+    """One propagation step (afqmc_prop_step_dev) captured in a CUDA graph.
+
+    Eshift is read from a one-element device buffer that replay() refreshes, so equilibration can
+    keep moving it; the fields come from the device Philox generator (its counter lives on the
+    device and advances inside the graph), or from a fixed device buffer `uniforms` [W, Nc] that
+    the caller refills before each replay.  Capture records without executing, so it is done
+    after the first eager step (every buffer allocated) and does not advance the run."""
+
+    def __init__(self, prop, wset, uniforms=None):
+        self.prop, self.wset, self.uniforms = prop, wset, uniforms
+        self.eshift = torch.zeros(1, dtype=torch.float64, device=wset.buffer.device)
+        self.graph = None
+
+    def capture(self):
+        stream = torch.cuda.Stream()
+        stream.wait_stream(torch.cuda.current_stream())
+        g = torch.cuda.CUDAGraph()
+        n0 = A.lib().afqmc_kernel_launches()
+        with torch.cuda.graph(g, stream=stream):
+            self.prop.Propagate_dev(self.wset, self.eshift, self.uniforms)
+        # kernels recorded in the graph (the library counts launches as it records them)
+        self.kernels = A.lib().afqmc_kernel_launches() - n0
+        torch.cuda.current_stream().wait_stream(stream)
+        self.graph = g
+        self.replays = 0
+
+    def replay(self, Eshift):
+        self.eshift.fill_(float(Eshift))
+        self.graph.replay()
+        self.replays += 1
+
+    def kernels_replayed(self):
+        return 0 if self.graph is None else self.kernels * self.replays
+
+
 @dataclass
 class Simulation:
     ham: A.HamiltonianOperations
@@ -63,6 +99,8 @@ class Simulation:
     precision: int = A.PREC_FP64
     step_index: int = 0
     energies: list = field(default_factory=list)
+    use_graph: bool = False
+    graph: StepGraph = None
 
     @staticmethod
     def from_workload(wl, W=None, precision=A.PREC_FP64, rp=None, **prop_kw):
@@ -107,7 +145,14 @@ class Simulation:
     def step(self, uniforms=None, measure=True):
         """One iteration of the run_afqmc loop.  Returns the measured energy or None."""
         step = self.step_index
-        self.prop.Propagate(self.wset, self.Eshift, uniforms)
+        if self.use_graph and uniforms is None and step > 0:
+            # device fields: replay the captured step (captured on first use, after step 0)
+            if self.graph is None:
+                self.graph = StepGraph(self.prop, self.wset)
+                self.graph.capture()
+            self.graph.replay(self.Eshift)
+        else:
+            self.prop.Propagate(self.wset, self.Eshift, uniforms)
         if step % self.rp.walker_ortho_interval == 0:
             self.prop.Orthogonalize(self.wset)
         if step % self.rp.population_control_interval == 0:

@@ -181,3 +181,26 @@ def test_nonfinite_walker_is_dropped(cuda):
     el = sim.wset.getProperty(O.PSEUDO_ELOC)
     assert w[3] == 0 and el[3] == old[3]
     assert np.all(w[[0, 1, 2, 4, 5, 6, 7]] != 0)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_graph_step_matches_eager(cuda, precision):
+    """The CUDA-graph replay of a step (device fields, Eshift from device memory) gives the same
+    walkers, weights and energies as launching the step eagerly, bit for bit."""
+    from safire_b200.driver import RunParams, Simulation
+    wl = make_workload("cfg1", W=24)
+    sims = []
+    for g in (False, True):
+        sim = Simulation.from_workload(wl, W=24, precision=precision,
+                                       rp=RunParams(equilibration_steps=6))
+        sim.use_graph = g
+        sims.append(sim)
+    for _ in range(14):
+        for sim in sims:
+            sim.step()
+    torch.cuda.synchronize()
+    assert sims[1].graph is not None and sims[1].graph.replays == 13
+    a, b = (to_host(s.wset.buffer) for s in sims)
+    assert np.array_equal(a, b)
+    assert sims[0].energies == sims[1].energies
+    assert sims[0].Eshift == sims[1].Eshift
