@@ -304,6 +304,7 @@ def run_ours(args):
     # per-phase timing of one step and of one energy measurement (untimed region)
     sim.prop.set_timing(True)
     sim.prop.Propagate(sim.wset, sim.Eshift)
+    sim._g_ready = False  # that step did not leave the density matrix for the next one
     phases = sim.prop.timings()
     sim.prop.set_timing(False)
     torch.cuda.synchronize()
@@ -358,16 +359,7 @@ def run_ours(args):
         def block_e2e():
             dev_u.copy_(host_u, non_blocking=True)
             for s in range(BLOCK):
-                st = sim.step_index
-                sim.prop.Propagate(sim.wset, sim.Eshift, dev_u[s])
-                if st % 5 == 0:
-                    sim.prop.Orthogonalize(sim.wset)
-                if st % 10 == 0:
-                    if world > 1:
-                        population_control_distributed(sim.wset, sim.walker_rng)
-                    else:
-                        A.population_control(sim.wset, sim.walker_rng)
-                sim.step_index += 1
+                sim.step(dev_u[s], measure=False)
             E, _ = sim.wfn.Energy(sim.wset, set_properties=False, precision=prec)
             sums = A.energy_sums(sim.wset, E)
             if world > 1:

@@ -257,6 +257,19 @@ int afqmc_prop_step(afqmc_prop prop, afqmc_wset ws, double Eshift, const double*
 /* Same as afqmc_prop_step but Eshift is read from device memory at run time (graph friendly). */
 int afqmc_prop_step_dev(afqmc_prop prop, afqmc_wset ws, const double* Eshift_dev,
                         const double* uniforms, afqmc_stream stream);
+/* Step with explicit reuse of the density matrix between steps (Eshift from device memory).
+ * AFQMC_STEP_KEEP_G: the new overlaps are computed together with the density matrix of the
+ *   propagated walkers (same product, LU and log det, plus the inverse and G), kept in the
+ *   propagator for the next step.
+ * AFQMC_STEP_G_READY: the propagator holds the density matrix of exactly these walkers (the last
+ *   step ran with KEEP_G on this walker set and nothing has changed its Slater matrices since:
+ *   no orthogonalisation, population control, row copy or direct write), so the step skips
+ *   recomputing it.  The caller owns this promise; results are identical to a step that
+ *   recomputes G when it holds. */
+#define AFQMC_STEP_G_READY 1
+#define AFQMC_STEP_KEEP_G 2
+int afqmc_prop_step_flags(afqmc_prop prop, afqmc_wset ws, const double* Eshift_dev,
+                          const double* uniforms, int flags, afqmc_stream stream);
 /* AFQMCBasePropagator::Orthogonalize (cpp:735-741): QR re-orthonormalisation then OVLP refresh. */
 int afqmc_prop_orthogonalize(afqmc_prop prop, afqmc_wset ws, afqmc_stream stream);
 /* Seeds / advances the device field generator (Philox4x32-10, counter = step). */

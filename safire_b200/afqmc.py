@@ -341,6 +341,11 @@ class Propagator:
         call("afqmc_prop_step_dev", self.handle, wset.handle, _ptr(Eshift_dev), _ptr(uniforms),
              _stream(stream))
 
+    def Propagate_flags(self, wset: WalkerSet, Eshift_dev, uniforms=None, flags=0, stream=None):
+        """One step with explicit density-matrix reuse (capi.STEP_G_READY / STEP_KEEP_G)."""
+        call("afqmc_prop_step_flags", self.handle, wset.handle, _ptr(Eshift_dev), _ptr(uniforms),
+             int(flags), _stream(stream))
+
     def Orthogonalize(self, wset: WalkerSet, stream=None):
         call("afqmc_prop_orthogonalize", self.handle, wset.handle, _stream(stream))
 

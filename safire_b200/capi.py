@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libsafire_afqmc.so")
 OK = 0
 CLOSED, COLLINEAR = 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
+STEP_G_READY, STEP_KEEP_G = 1, 2  # afqmc_prop_step_flags
 (WEIGHT, PHASE, PSEUDO_ELOC, E1, EXX, EJ, OVLP, LOGSCL_UP, LOGSCL_DN, IS_UNITARY,
  THETA) = range(11)
 NPROP = 11
@@ -58,6 +59,7 @@ _SIGS = {
     "afqmc_ham_device_error": (i32, [vp, C.POINTER(C.c_uint)]),
     "afqmc_ham_set_exchange_split": (i32, [vp, i32]),
     "afqmc_ham_set_taylor_fused": (i32, [vp, i32]),
+    "afqmc_prop_step_flags": (i32, [vp, vp, vp, vp, i32, vp]),
     "afqmc_ph_excited_2body_energy": (i32, [vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, i32,
                                             vp, vp, vp, vp]),
     "afqmc_ph_excited_1body_energy": (i32, [vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, vp, vp]),

@@ -1107,7 +1107,7 @@ extern "C" int afqmc_prop_set_field_seed(afqmc_prop pr, unsigned long long seed)
 namespace {
 
 int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* Eshift_dev,
-              const double* uniforms, cudaStream_t s) {
+              const double* uniforms, int flags, cudaStream_t s) {
   afqmc_ham_s* h = pr->ham;
   auto mark = [&](int i) -> int {
     if (pr->timing) AFQMC_CUDA_TRY(cudaEventRecord(pr->ev[i], s));
@@ -1118,8 +1118,10 @@ int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* E
   const double dt = pr->p.dt;
   const long ldG = long(h->nel_tot) * M;
   const bool mixed = pr->p.precision == AFQMC_PREC_MIXED;
-  // 1. vbias: G of the walkers (NOMSD::vbias, NOMSD.cpp:39-61)
-  AFQMC_TRY(wfn_density_matrix(h, ws, s, pr->G, ldG, pr->ovtmp, pr->T));
+  // 1. vbias: G of the walkers (NOMSD::vbias, NOMSD.cpp:39-61); with AFQMC_STEP_G_READY the
+  //    previous step left it for these walkers
+  if (!(flags & AFQMC_STEP_G_READY))
+    AFQMC_TRY(wfn_density_matrix(h, ws, s, pr->G, ldG, pr->ovtmp, pr->T));
   AFQMC_TRY(mark(1));
   if (mixed) {
     EnergyArgs a = energy_args(h, pr->G, ldG);
@@ -1158,8 +1160,12 @@ int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* E
     }
   }
   AFQMC_TRY(mark(5));
-  // 5. new overlaps
-  AFQMC_TRY(wfn_log_overlap(h, ws, s, pr->newov, pr->T));
+  // 5. new overlaps; with AFQMC_STEP_KEEP_G also the density matrix of the propagated walkers
+  //    for the next step (the same product, LU and log det, plus the inverse and G)
+  if (flags & AFQMC_STEP_KEEP_G)
+    AFQMC_TRY(wfn_density_matrix(h, ws, s, pr->G, ldG, pr->newov, pr->T));
+  else
+    AFQMC_TRY(wfn_log_overlap(h, ws, s, pr->newov, pr->T));
   AFQMC_TRY(mark(6));
   // 6-7. walker_update + bound_walker_weights
   const double max_weight = std::max(pr->p.weight_bound_floor, pr->p.weight_bound_fraction * W);
@@ -1178,7 +1184,7 @@ extern "C" int afqmc_prop_step(afqmc_prop pr, afqmc_wset ws, double Eshift, cons
   AFQMC_CHECK_ARG(ws->W <= pr->maxW, "afqmc_prop_step: %d walkers exceed the propagator's %d",
                   ws->W, pr->maxW);
   DeviceGuard g(pr->device);
-  return prop_step(pr, ws, Eshift, nullptr, u, reinterpret_cast<cudaStream_t>(stream));
+  return prop_step(pr, ws, Eshift, nullptr, u, 0, reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" int afqmc_prop_step_dev(afqmc_prop pr, afqmc_wset ws, const double* Eshift_dev,
@@ -1187,7 +1193,18 @@ extern "C" int afqmc_prop_step_dev(afqmc_prop pr, afqmc_wset ws, const double* E
   AFQMC_CHECK_ARG(wset_matches(pr->ham, ws), "afqmc_prop_step_dev: walker set / Hamiltonian mismatch");
   AFQMC_CHECK_ARG(ws->W <= pr->maxW, "afqmc_prop_step_dev: too many walkers");
   DeviceGuard g(pr->device);
-  return prop_step(pr, ws, 0.0, Eshift_dev, u, reinterpret_cast<cudaStream_t>(stream));
+  return prop_step(pr, ws, 0.0, Eshift_dev, u, 0, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int afqmc_prop_step_flags(afqmc_prop pr, afqmc_wset ws, const double* Eshift_dev,
+                                     const double* u, int flags, afqmc_stream stream) {
+  AFQMC_CHECK_ARG(pr && ws && Eshift_dev, "afqmc_prop_step_flags: null argument");
+  AFQMC_CHECK_ARG(wset_matches(pr->ham, ws), "afqmc_prop_step_flags: walker set / Hamiltonian mismatch");
+  AFQMC_CHECK_ARG(ws->W <= pr->maxW, "afqmc_prop_step_flags: too many walkers");
+  AFQMC_CHECK_ARG((flags & ~(AFQMC_STEP_G_READY | AFQMC_STEP_KEEP_G)) == 0,
+                  "afqmc_prop_step_flags: unknown flags %d", flags);
+  DeviceGuard g(pr->device);
+  return prop_step(pr, ws, 0.0, Eshift_dev, u, flags, reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" int afqmc_prop_orthogonalize(afqmc_prop pr, afqmc_wset ws, afqmc_stream stream) {

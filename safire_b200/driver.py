@@ -50,39 +50,40 @@ class RunParams:
 
 
 class StepGraph:
-    """One propagation step (afqmc_prop_step_dev) captured in a CUDA graph.
+    """The propagation step (afqmc_prop_step_flags) captured in CUDA graphs, one per flag set.
 
-    Eshift is read from a one-element device buffer that replay() refreshes, so equilibration can
-    keep moving it; the fields come from the device Philox generator (its counter lives on the
-    device and advances inside the graph), or from a fixed device buffer `uniforms` [W, Nc] that
-    the caller refills before each replay.  Capture records without executing, so it is done
-    after the first eager step (every buffer allocated) and does not advance the run."""
+    Eshift is read from a one-element device buffer (`eshift`, refreshed before each replay), so
+    equilibration can keep moving it; the fields come from the device Philox generator (its
+    counter lives on the device and advances inside the graph), or from a fixed device buffer
+    `uniforms` [W, Nc] that the caller refills before each replay.  Capture records without
+    executing, so it is done after the first eager step (every buffer allocated) and does not
+    advance the run."""
 
-    def __init__(self, prop, wset, uniforms=None):
-        self.prop, self.wset, self.uniforms = prop, wset, uniforms
-        self.eshift = torch.zeros(1, dtype=torch.float64, device=wset.buffer.device)
-        self.graph = None
+    def __init__(self, prop, wset, eshift, uniforms=None):
+        self.prop, self.wset, self.eshift, self.uniforms = prop, wset, eshift, uniforms
+        self.graphs, self.kernels = {}, {}
+        self.replayed = 0
 
-    def capture(self):
+    def _capture(self, flags):
         stream = torch.cuda.Stream()
         stream.wait_stream(torch.cuda.current_stream())
         g = torch.cuda.CUDAGraph()
         n0 = A.lib().afqmc_kernel_launches()
         with torch.cuda.graph(g, stream=stream):
-            self.prop.Propagate_dev(self.wset, self.eshift, self.uniforms)
+            self.prop.Propagate_flags(self.wset, self.eshift, self.uniforms, flags)
         # kernels recorded in the graph (the library counts launches as it records them)
-        self.kernels = A.lib().afqmc_kernel_launches() - n0
+        self.kernels[flags] = A.lib().afqmc_kernel_launches() - n0
         torch.cuda.current_stream().wait_stream(stream)
-        self.graph = g
-        self.replays = 0
+        self.graphs[flags] = g
 
-    def replay(self, Eshift):
-        self.eshift.fill_(float(Eshift))
-        self.graph.replay()
-        self.replays += 1
+    def replay(self, flags):
+        if flags not in self.graphs:
+            self._capture(flags)
+        self.graphs[flags].replay()
+        self.replayed += self.kernels[flags]
 
     def kernels_replayed(self):
-        return 0 if self.graph is None else self.kernels * self.replays
+        return self.replayed
 
 
 @dataclass
@@ -101,6 +102,11 @@ class Simulation:
     energies: list = field(default_factory=list)
     use_graph: bool = False
     graph: StepGraph = None
+    # the step leaves the density matrix of the propagated walkers for the next step, which
+    # skips recomputing it unless orthogonalisation or population control changed the walkers
+    reuse_density: bool = True
+    _g_ready: bool = False
+    _eshift_dev: torch.Tensor = None
 
     @staticmethod
     def from_workload(wl, W=None, precision=A.PREC_FP64, rp=None, **prop_kw):
@@ -145,17 +151,25 @@ class Simulation:
     def step(self, uniforms=None, measure=True):
         """One iteration of the run_afqmc loop.  Returns the measured energy or None."""
         step = self.step_index
+        if self._eshift_dev is None:
+            self._eshift_dev = torch.zeros(1, dtype=torch.float64, device=self.wset.buffer.device)
+        self._eshift_dev.fill_(float(self.Eshift))
+        flags = 0
+        if self.reuse_density:
+            flags = A.capi.STEP_KEEP_G | (A.capi.STEP_G_READY if self._g_ready else 0)
         if self.use_graph and uniforms is None and step > 0:
             # device fields: replay the captured step (captured on first use, after step 0)
             if self.graph is None:
-                self.graph = StepGraph(self.prop, self.wset)
-                self.graph.capture()
-            self.graph.replay(self.Eshift)
+                self.graph = StepGraph(self.prop, self.wset, self._eshift_dev)
+            self.graph.replay(flags)
         else:
-            self.prop.Propagate(self.wset, self.Eshift, uniforms)
+            self.prop.Propagate_flags(self.wset, self._eshift_dev, uniforms, flags)
+        self._g_ready = self.reuse_density
         if step % self.rp.walker_ortho_interval == 0:
             self.prop.Orthogonalize(self.wset)
+            self._g_ready = False
         if step % self.rp.population_control_interval == 0:
+            self._g_ready = False
             if _world() > 1:
                 from .population import population_control_distributed
                 population_control_distributed(self.wset, self.walker_rng)

@@ -199,8 +199,34 @@ def test_graph_step_matches_eager(cuda, precision):
         for sim in sims:
             sim.step()
     torch.cuda.synchronize()
-    assert sims[1].graph is not None and sims[1].graph.replays == 13
+    # steps 1..13 replay graphs: one per flag set (after orthogonalisation / comb the density
+    # matrix is recomputed, otherwise reused)
+    assert sims[1].graph is not None and len(sims[1].graph.graphs) == 2
+    assert sims[1].graph.kernels_replayed() > 0
     a, b = (to_host(s.wset.buffer) for s in sims)
     assert np.array_equal(a, b)
     assert sims[0].energies == sims[1].energies
     assert sims[0].Eshift == sims[1].Eshift
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_density_reuse_matches_recompute(cuda, precision):
+    """Steps that keep the propagated walkers' density matrix for the next step (skipped
+    recomputation between orthogonalisations / combs) give the same run as recomputing it at
+    every step."""
+    from safire_b200.driver import RunParams, Simulation
+    wl = make_workload("cfg1", W=24)
+    sims = []
+    for reuse in (False, True):
+        sim = Simulation.from_workload(wl, W=24, precision=precision,
+                                       rp=RunParams(equilibration_steps=6))
+        sim.reuse_density = reuse
+        sims.append(sim)
+    for _ in range(23):
+        for sim in sims:
+            sim.step()
+    torch.cuda.synchronize()
+    a, b = (to_host(s.wset.buffer) for s in sims)
+    assert rel_err(a, b) < 1e-13
+    assert np.allclose([e for _, e in sims[0].energies], [e for _, e in sims[1].energies],
+                       rtol=1e-13, atol=0)
