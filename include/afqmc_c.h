@@ -345,6 +345,18 @@ int afqmc_phmsd_destroy(afqmc_phmsd trial);
 int afqmc_phmsd_log_overlap(afqmc_phmsd trial, const afqmc_c128* wbuf, long ldS,
                             afqmc_c128* ovlp, int W, afqmc_stream stream);
 
+/* The Real3IndexFactorization tensors of a PHMSD trial: Likn [nspin_H2][M][M][Nc] (real) and
+ * hij [nspin_H1][M][M] on the host, half-rotated on the device with the active orbitals
+ * (the HamiltonianOperations a PHMSD wavefunction builds). */
+int afqmc_phmsd_set_hamiltonian(afqmc_phmsd trial, const double* Likn, int nspin_H2,
+                                const afqmc_c128* hij, int nspin_H1, int Nc, double E0);
+/* PHMSD::energy_alg1 (PHMSD.cpp:376-546), COLLINEAR walkers: E [W][3] (E1, EXX, EJ, device,
+ * written) and the log overlap [W] (device, written) of the multi-determinant trial, by the
+ * Woodbury evaluation of every excited determinant.  Walkers are processed in blocks of `block`
+ * (<= 0: 32); the excitation lists must be ordered by excitation number. */
+int afqmc_phmsd_energy(afqmc_phmsd trial, const afqmc_c128* wbuf, long ldS, afqmc_c128* E,
+                       afqmc_c128* ovlp, int W, int block, afqmc_stream stream);
+
 /* comb (population_control.hpp:34-65): host arrays; draws one uniform from rng. */
 int afqmc_comb(afqmc_host_rng rng, const double* weights, int n, int num_target, int* offspring);
 /* plan_walker_exchange (population_control.hpp:87-133): pure host logic. plan holds up to

@@ -121,3 +121,170 @@ def phmsd_log_overlap(trial, S_up, S_dn):
         ovs.append(np.array(ov))
     tot = np.einsum("k,kw,kw->w", trial.coef, ovs[0][trial.det_up], ovs[1][trial.det_dn])
     return np.log(tot) + log_ov, ovs
+
+
+# --------------------------------------------------------------------------------------------
+# PHMSD energy (Wavefunctions/PHMSD.cpp:376-546 energy_alg1, COLLINEAR) and its building blocks
+# --------------------------------------------------------------------------------------------
+class ActiveSpaceHamiltonian:
+    """Real3IndexFactorization tensors half-rotated with the active orbitals of a PHMSD trial
+    (the HamiltonianOperations built for a PHMSD wavefunction: its 'nup/ndown' rows are the
+    active orbitals, Real3IndexFactorization.hpp:598-602).  Lnak[s] [Nc][nact_s][M],
+    haj[s] [nact_s][M]."""
+
+    def __init__(self, trial, Likn, hij, E0):
+        Likn = np.asarray(Likn, dtype=np.float64)
+        hij = np.asarray(hij, dtype=np.complex128)
+        M = trial.M
+        self.E0 = float(E0)
+        self.nCV = Likn.shape[3]
+        self.Lnak, self.haj = [], []
+        for s in (0, 1):
+            A = trial.orbmat[s]
+            L = Likn[s % Likn.shape[0]]
+            PL = (A @ L.reshape(M, M * self.nCV)).reshape(A.shape[0], M, self.nCV)
+            self.Lnak.append(np.ascontiguousarray(PL.transpose(2, 0, 1)))
+            self.haj.append(A @ hij[s % hij.shape[0]])
+
+
+def mixed_density_matrix_for_woodbury(A, S, refc):
+    """det_ops::MixedDensityMatrixForWoodbury, compact (density_matrix.hpp:651-717):
+    TAB = A S, TNN = TAB[refc], log det (getrf conventions), inverse, QQ0 = TAB TNN^{-1},
+    G = TNN^{-T} S^T.  Returns (G [W,N,M], log_ov [W], QQ0 [W,nact,N])."""
+    from oracle.afqmc import _getrf_ref, _getri_or_zero_ref, log_det_from_getrf
+    W = S.shape[0]
+    TAB = np.einsum("am,wmn->wan", A, S)
+    G = np.empty((W, S.shape[2], S.shape[1]), complex)
+    QQ0 = np.empty_like(TAB)
+    logov = np.zeros(W, complex)
+    for w in range(W):
+        lu, piv1, info = _getrf_ref(TAB[w][refc, :])
+        logov[w] = log_det_from_getrf(lu, piv1, 0j)
+        inv = _getri_or_zero_ref(lu, piv1)
+        QQ0[w] = TAB[w] @ inv
+        G[w] = inv.T @ S[w].T
+    return G, logov, QQ0
+
+
+def excitation_overlaps(trial, s, QQ0):
+    """calculate_overlaps (phmsd_helpers.hpp:111-193): [nuniq, W], index 0 = reference."""
+    W = QQ0.shape[0]
+    ov = [np.ones(W, complex)]
+    for n in sorted(trial.exc[s]):
+        for e in trial.exc[s][n]:
+            ov.append(np.linalg.det(QQ0[:, e[n:]][:, :, e[:n]]))
+    return np.array(ov)
+
+
+def compact_R(iexcit, refc, QQ0):
+    """get_compact_ph_R_matrices (phmsd_helpers.hpp:311-398): R [W][ndet][nex][nact] from the
+    inverse Q of each nex x nex excitation block: R[p][orb_i] -= Q[p][q] QQ0[part_q][i] for every
+    electron i, R[p][orb(hole_q)] += Q[p][q], orb = the determinant's occupations."""
+    W, nact, nel = QQ0.shape
+    ndet, two_nex = iexcit.shape
+    nex = two_nex // 2
+    R = np.zeros((W, ndet, nex, nact), complex)
+    for d in range(ndet):
+        holes, parts = iexcit[d, :nex], iexcit[d, nex:]
+        orbs = np.array(refc).copy()
+        orbs[holes] = parts
+        for w in range(W):
+            Q = QQ0[w][np.ix_(parts, holes)]
+            if abs(np.linalg.det(Q)) == 0.0:
+                continue
+            Qi = np.linalg.inv(Q)
+            for p in range(nex):
+                for q in range(nex):
+                    R[w, d, p, orbs] -= Qi[p, q] * QQ0[w, parts[q], :]
+                    R[w, d, p, orbs[holes[q]]] += Qi[p, q]
+    return R
+
+
+def ph_reference_energy(H, s, G, refc, alpha):
+    """ph_reference_energy / ph_ref_energy_impl (Real3IndexFactorization.hpp:212-235, 598-696)
+    for COLLINEAR walkers: returns (E [W,3], Kl [W,Nc], Swia [W,N,nact], Twina [W,N,Nc,nact]).
+    E1 = (E0 if alpha) + sum_i Swia[i, refc_i]; EXX = -1/2 sum Twina[i,n,refc_j] Twina[j,n,refc_i];
+    EJ = 1/2 Kl.Kl with Kl[n] = sum_i Twina[i,n,refc_i]."""
+    W, N, M = G.shape
+    Swia = np.einsum("wik,ak->wia", G, H.haj[s])
+    Twina = np.einsum("wik,nak->wina", G, H.Lnak[s])
+    E = np.zeros((W, 3), complex)
+    if alpha:
+        E[:, 0] = H.E0
+    r = np.asarray(refc)
+    E[:, 0] += np.einsum("wii->w", Swia[:, :, r])
+    Tr = Twina[:, :, :, r]  # [W, i, n, j] with j over electrons
+    E[:, 1] += -0.5 * np.einsum("winj,wjni->w", Tr, Tr)
+    Kl = np.einsum("wini->wn", Tr)
+    E[:, 2] += 0.5 * np.einsum("wn,wn->w", Kl, Kl)
+    return E, Kl, Swia, Twina
+
+
+def _shells(trial, s):
+    """(first unique index, iexcit) per excitation number, in the unique-index order."""
+    out, k = [], 1
+    for n in sorted(trial.exc[s]):
+        e = trial.exc[s][n]
+        out.append((k, e))
+        k += e.shape[0]
+    return out
+
+
+def _couple(trial, s, vec_other):
+    """sum over determinants of spin s's unique index u: c_k vec_other[det_other[k]] (the
+    OpSpinDetCouplings CSR products of energy_alg1)."""
+    det_s = trial.det_up if s == 0 else trial.det_dn
+    det_o = trial.det_dn if s == 0 else trial.det_up
+    nu = trial.unique_count(s)
+    out = np.zeros((nu,) + vec_other.shape[1:], complex)
+    for k in range(trial.coef.size):
+        out[det_s[k]] += trial.coef[k] * vec_other[det_o[k]]
+    return out
+
+
+def phmsd_energy(trial, H, S_up, S_dn):
+    """PHMSD::energy_alg1 (PHMSD.cpp:376-546), COLLINEAR: returns (E [W,3], log overlap [W])."""
+    W = S_up.shape[0]
+    Gu, lu, Qu = mixed_density_matrix_for_woodbury(trial.orbmat[0], S_up, trial.refc[0])
+    Gd, ld, Qd = mixed_density_matrix_for_woodbury(trial.orbmat[1], S_dn, trial.refc[1])
+    log_ov = lu + ld
+    ovu = excitation_overlaps(trial, 0, Qu)
+    ovd = excitation_overlaps(trial, 1, Qd)
+    E = np.zeros((W, 3), complex)
+    # spin up: weights, Ov, reference energy, excited energies
+    wgt = _couple(trial, 0, ovd)                   # [nu_up, W]
+    Ov = np.sum(wgt * ovu, axis=0)
+    wgt = wgt * ovu
+    eloc, Kl_up, Swia, Twina = ph_reference_energy(H, 0, Gu, trial.refc[0], True)
+    E += eloc * Ov[:, None]
+    KEr = np.zeros((trial.unique_count(0), W, H.nCV), complex)
+    KEr[0] = Kl_up
+    el = np.zeros((W, 3), complex)
+    for k0, iex in _shells(trial, 0):
+        R = compact_R(iex, trial.refc[0], Qu)
+        w = wgt[k0:k0 + iex.shape[0]]
+        el[:, 0] = ph_excited_1body_energy(iex, trial.refc[0], Swia, R, w, el[:, 0])
+        EX, EJ, KE = ph_excited_2body_energy_dense_cholesky(iex, trial.refc[0], Twina, R, w,
+                                                            el[:, 1], el[:, 2])
+        el[:, 1], el[:, 2] = EX, EJ
+        KEr[k0:k0 + iex.shape[0]] = KE
+    E += el
+    KEr = KEr * ovu[:, :, None]
+    KEd = _couple(trial, 1, KEr) * ovd[:, :, None]  # [nu_dn, W, Nc]
+    # spin down
+    wgt = _couple(trial, 1, ovu) * ovd
+    eloc, Kl_dn, Swia, Twina = ph_reference_energy(H, 1, Gd, trial.refc[1], False)
+    E += eloc * Ov[:, None]
+    E[:, 2] += np.einsum("wn,wn->w", KEd[0], Kl_dn)
+    el = np.zeros((W, 3), complex)
+    for k0, iex in _shells(trial, 1):
+        R = compact_R(iex, trial.refc[1], Qd)
+        w = wgt[k0:k0 + iex.shape[0]]
+        el[:, 0] = ph_excited_1body_energy(iex, trial.refc[1], Swia, R, w, el[:, 0])
+        EX, EJ, KEl = ph_excited_2body_energy_dense_cholesky(iex, trial.refc[1], Twina, R, w,
+                                                             el[:, 1], el[:, 2])
+        el[:, 1], el[:, 2] = EX, EJ
+        el[:, 2] += np.einsum("dwn,dwn->w", KEd[k0:k0 + iex.shape[0]], KEl)
+    E += el
+    E = E / Ov[:, None]
+    return E, np.log(Ov) + log_ov

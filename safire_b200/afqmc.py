@@ -504,6 +504,18 @@ class PHMSD:
             capi._lib.afqmc_phmsd_destroy(h)
             self.handle = None
 
+    def set_hamiltonian(self, Likn, hij, E0):
+        """Likn real [nspin_H2, M, M, Nc], hij complex [nspin_H1, M, M] (host)."""
+        L = np.ascontiguousarray(Likn, dtype=np.float64)
+        h = np.ascontiguousarray(hij, dtype=np.complex128)
+        call("afqmc_phmsd_set_hamiltonian", self.handle, _host_ptr(L), L.shape[0], _host_ptr(h),
+             h.shape[0], L.shape[3], float(E0))
+
+    def Energy(self, wbuf, E, ovlp, block=0, stream=None):
+        """E [W, 3] (device) and ovlp [W] (device) of every walker row of wbuf [W][ldS]."""
+        call("afqmc_phmsd_energy", self.handle, _ptr(wbuf), int(wbuf.stride(0)), _ptr(E),
+             _ptr(ovlp), int(wbuf.shape[0]), int(block), _stream(stream))
+
     def Log_Overlap(self, wbuf, ovlp, stream=None):
         """ovlp [W] (device) <- log overlap of every walker row of wbuf [W][ldS] (device)."""
         call("afqmc_phmsd_log_overlap", self.handle, _ptr(wbuf), int(wbuf.stride(0)), _ptr(ovlp),

@@ -10,6 +10,7 @@
 //   iexcit [ndet][2][nex] holes (electron indices into refc), then particles (active orbitals)
 //   Twina  [nw][nelec][nchol][nact], R [nw][ndet][nex][nact], wgt [ndet][nw], S [nw][nelec][nact]
 //   EX, EJ, E [nw] (accumulated), KE [ndet][nw][nchol] (written)
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -257,6 +258,208 @@ __global__ void __launch_bounds__(PH_THREADS) phmsd_combine_kernel(
   if (threadIdx.x == 0) ovlp[w] = cadd(clog(s), logov[w]);
 }
 
+// Lnak[n][a][k] <- tmp[a][k][n]  (rows of OrbMat * L viewed as M x (M Nc))
+__global__ void lnak_act_reorder_kernel(const c128* __restrict__ in, c128* __restrict__ out,
+                                        int nact, int M, int Nc) {
+  const long e = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= long(nact) * M * Nc) return;
+  const int n = int(e % Nc);
+  const long r = e / Nc;
+  const int k = int(r % M), a = int(r / M);
+  out[(long(n) * nact + a) * M + k] = in[e];
+}
+
+// wgt[u][w] = scale_u(w) * sum over the determinants k of unique excitation u (CSR row u) of
+// c_k v_other[w][other_k]; scale = ov_self[w][u] when ov_self is given (energy_alg1's
+// "W *= ovlp_ratio" steps)
+__global__ void couple_kernel(const int* __restrict__ rowptr, const int* __restrict__ kidx,
+                              const int* __restrict__ det_other, const c128* __restrict__ coef,
+                              const c128* __restrict__ v_other, int nu_other,
+                              const c128* __restrict__ ov_self, int nu, int W,
+                              c128* __restrict__ wgt) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(nu) * W) return;
+  const int u = int(t / W), w = int(t - long(u) * W);
+  c128 acc = cmk(0, 0);
+  for (int j = rowptr[u]; j < rowptr[u + 1]; ++j) {
+    const int k = kidx[j];
+    acc = cadd(acc, cmul(coef[k], v_other[size_t(w) * nu_other + det_other[k]]));
+  }
+  if (ov_self) acc = cmul(acc, ov_self[size_t(w) * nu + u]);
+  wgt[t] = acc;
+}
+
+// Ov[w] = sum_u wgt[u][w] ov[w][u]   (before the weights are scaled by the overlaps)
+__global__ void __launch_bounds__(PH_THREADS) total_overlap_kernel(
+    const c128* __restrict__ wgt, const c128* __restrict__ ov, int nu, int W,
+    c128* __restrict__ Ov) {
+  __shared__ double red[PH_THREADS / 32 * 6];
+  const int w = blockIdx.x;
+  c128 s = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0);
+  for (int u = threadIdx.x; u < nu; u += blockDim.x)
+    s = cadd(s, cmul(wgt[size_t(u) * W + w], ov[size_t(w) * nu + u]));
+  block_sum3(s, z1, z2, red);
+  if (threadIdx.x == 0) Ov[w] = s;
+}
+
+// ph_reference_energy (Real3IndexFactorization.hpp:212-235, 612-690): per walker
+//   e1 = (E0) + sum_i Swia[i][refc_i],  ex = -1/2 sum_{i,j,n} T[i][n][refc_j] T[j][n][refc_i],
+//   Kl[n] = sum_i T[i][n][refc_i],  ej = 1/2 Kl.Kl;  E[w] += Ov[w] (e1, ex, ej)
+__global__ void __launch_bounds__(PH_THREADS) ph_reference_kernel(
+    const c128* __restrict__ Swia, const c128* __restrict__ Twina, const int* __restrict__ refc,
+    int nel, int nchol, int nact, double E0, const c128* __restrict__ Ov, c128* __restrict__ E,
+    c128* __restrict__ Kl) {
+  __shared__ double red[PH_THREADS / 32 * 6];
+  const int w = blockIdx.x;
+  const c128* T = Twina + size_t(w) * nel * nchol * nact;
+  c128 ex = cmk(0, 0), ej = cmk(0, 0), e1 = cmk(0, 0);
+  for (int n = threadIdx.x; n < nchol; n += blockDim.x) {
+    c128 kn = cmk(0, 0);
+    for (int i = 0; i < nel; ++i) {
+      const c128* ti = T + (size_t(i) * nchol + n) * nact;
+      kn = cadd(kn, ti[refc[i]]);
+      for (int j = 0; j < nel; ++j) {
+        const c128* tj = T + (size_t(j) * nchol + n) * nact;
+        ex = cadd(ex, cmul(ti[refc[j]], tj[refc[i]]));
+      }
+    }
+    Kl[size_t(w) * nchol + n] = kn;
+    ej = cadd(ej, cmul(kn, kn));
+  }
+  for (int i = threadIdx.x; i < nel; i += blockDim.x)
+    e1 = cadd(e1, Swia[(size_t(w) * nel + i) * nact + refc[i]]);
+  block_sum3(ex, ej, e1, red);
+  if (threadIdx.x == 0) {
+    const c128 o = Ov[w];
+    const c128 v1 = cmul(o, cmk(e1.x + E0, e1.y));
+    const c128 vx = cmul(o, cmul(cmk(-0.5, 0), ex));
+    const c128 vj = cmul(o, cmul(cmk(0.5, 0), ej));
+    E[w * 3 + 0] = cadd(E[w * 3 + 0], v1);
+    E[w * 3 + 1] = cadd(E[w * 3 + 1], vx);
+    E[w * 3 + 2] = cadd(E[w * 3 + 2], vj);
+  }
+}
+
+// get_compact_ph_R_matrices (phmsd_helpers.hpp:311-398): R[w][d][p][:] from the inverse Q of the
+// excitation block QQ0[particles][holes]; orbs = the determinant's occupied active orbitals:
+//   R[p][orbs_i] -= Q[p][q] QQ0[part_q][i]  (all electrons i),  R[p][orbs(hole_q)] += Q[p][q]
+// R must be zero on entry; a singular block leaves its rows zero (as the reference).
+__global__ void compact_R_kernel(const c128* __restrict__ QQ0, const int* __restrict__ iexcit,
+                                 const int* __restrict__ refc, int ndet, int nex, int W, int nact,
+                                 int nel, c128* __restrict__ R) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(W) * ndet) return;
+  const int w = int(t / ndet), d = int(t - long(w) * ndet);
+  const int* e = iexcit + size_t(d) * 2 * nex;
+  const c128* Q0 = QQ0 + size_t(w) * nact * nel;
+  c128 a[PH_NEX_MAX][PH_NEX_MAX], inv[PH_NEX_MAX][PH_NEX_MAX];
+  for (int p = 0; p < nex; ++p)
+    for (int q = 0; q < nex; ++q) {
+      a[p][q] = Q0[size_t(e[nex + p]) * nel + e[q]];
+      inv[p][q] = cmk(p == q ? 1.0 : 0.0, 0.0);
+    }
+  // Gauss-Jordan with partial pivoting on [a | I]
+  for (int k = 0; k < nex; ++k) {
+    int piv = k;
+    double best = cabs1(a[k][k]);
+    for (int i = k + 1; i < nex; ++i)
+      if (cabs1(a[i][k]) > best) {
+        best = cabs1(a[i][k]);
+        piv = i;
+      }
+    if (!(best > 0.0)) return;  // singular block: this determinant's R stays zero
+    if (piv != k)
+      for (int j = 0; j < nex; ++j) {
+        c128 x = a[k][j]; a[k][j] = a[piv][j]; a[piv][j] = x;
+        x = inv[k][j]; inv[k][j] = inv[piv][j]; inv[piv][j] = x;
+      }
+    const c128 dinv = cdiv(cmk(1.0, 0.0), a[k][k]);
+    for (int j = 0; j < nex; ++j) {
+      a[k][j] = cmul(a[k][j], dinv);
+      inv[k][j] = cmul(inv[k][j], dinv);
+    }
+    for (int i = 0; i < nex; ++i)
+      if (i != k) {
+        const c128 f = a[i][k];
+        for (int j = 0; j < nex; ++j) {
+          a[i][j] = csub(a[i][j], cmul(f, a[k][j]));
+          inv[i][j] = csub(inv[i][j], cmul(f, inv[k][j]));
+        }
+      }
+  }
+  c128* Rw = R + (size_t(w) * ndet + d) * nex * nact;
+  for (int p = 0; p < nex; ++p) {
+    c128* Rp = Rw + size_t(p) * nact;
+    for (int q = 0; q < nex; ++q) {
+      const c128 ipq = inv[p][q];
+      const c128* Tq = Q0 + size_t(e[nex + q]) * nel;
+      for (int i = 0; i < nel; ++i) {
+        int oi = refc[i];
+        for (int h = 0; h < nex; ++h)
+          if (e[h] == i) oi = e[nex + h];
+        Rp[oi] = csub(Rp[oi], cmul(ipq, Tq[i]));
+      }
+      int oh = e[nex + q];  // orbital of hole q's electron in this determinant
+      Rp[oh] = cadd(Rp[oh], ipq);
+    }
+  }
+}
+
+// KEd[d][w][n] = ov_dn[w][d] sum_{k in CSR row d} c_k ov_up[w][up_k] KEr[up_k][w][n]
+__global__ void couple_ke_kernel(const int* __restrict__ rowptr, const int* __restrict__ kidx,
+                                 const int* __restrict__ det_up, const c128* __restrict__ coef,
+                                 const c128* __restrict__ KEr, const c128* __restrict__ ov_up,
+                                 int nu_up, const c128* __restrict__ ov_dn, int nu_dn, int W,
+                                 int nchol, c128* __restrict__ KEd) {
+  const int d = blockIdx.x, w = blockIdx.y;
+  for (int n = threadIdx.x; n < nchol; n += blockDim.x) {
+    c128 acc = cmk(0, 0);
+    for (int j = rowptr[d]; j < rowptr[d + 1]; ++j) {
+      const int k = kidx[j], u = det_up[k];
+      const c128 f = cmul(coef[k], ov_up[size_t(w) * nu_up + u]);
+      acc = cadd(acc, cmul(f, KEr[(size_t(u) * W + w) * nchol + n]));
+    }
+    KEd[(size_t(d) * W + w) * nchol + n] = cmul(acc, ov_dn[size_t(w) * nu_dn + d]);
+  }
+}
+
+// E[w][2] += sum_{d, n} A[d][w][n] B[d][w][n]  (the cross-spin Coulomb products)
+__global__ void __launch_bounds__(PH_THREADS) cross_ej_kernel(const c128* __restrict__ A,
+                                                              const c128* __restrict__ B, int nd,
+                                                              int W, int nchol,
+                                                              c128* __restrict__ E) {
+  __shared__ double red[PH_THREADS / 32 * 6];
+  const int w = blockIdx.x;
+  c128 s = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0);
+  for (long k = threadIdx.x; k < long(nd) * nchol; k += blockDim.x) {
+    const int d = int(k / nchol), n = int(k - long(d) * nchol);
+    const size_t o = (size_t(d) * W + w) * nchol + n;
+    s = cadd(s, cmul(A[o], B[o]));
+  }
+  block_sum3(s, z1, z2, red);
+  if (threadIdx.x == 0) E[w * 3 + 2] = cadd(E[w * 3 + 2], s);
+}
+
+// E[w] += (e1[w], ex[w], ej[w])
+__global__ void add_components_kernel(const c128* __restrict__ e1, const c128* __restrict__ ex,
+                                      const c128* __restrict__ ej, int W, c128* __restrict__ E) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  E[w * 3 + 0] = cadd(E[w * 3 + 0], e1[w]);
+  E[w * 3 + 1] = cadd(E[w * 3 + 1], ex[w]);
+  E[w * 3 + 2] = cadd(E[w * 3 + 2], ej[w]);
+}
+
+// E[w] /= Ov[w];  ovlp[w] = log Ov[w] + logov[w]
+__global__ void finish_energy_kernel(const c128* __restrict__ Ov, const c128* __restrict__ logov,
+                                     int W, c128* __restrict__ E, c128* __restrict__ ovlp) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  const c128 r = cdiv(cmk(1.0, 0.0), Ov[w]);
+  for (int c = 0; c < 3; ++c) E[w * 3 + c] = cmul(E[w * 3 + c], r);
+  ovlp[w] = cadd(clog(Ov[w]), logov[w]);
+}
+
 int check_dims(const char* who, int nw, int ndet, int nex, int nact, int nelec) {
   if (nw < 0 || ndet < 0 || nex < 1 || nex > PH_NEX_MAX || nact < 1 || nelec < 1) {
     set_error_detail("%s: nw=%d ndet=%d nex=%d (1..%d) nact=%d nelec=%d", who, nw, ndet, nex,
@@ -362,6 +565,34 @@ struct afqmc_phmsd_s {
   int capW = 0;
   c128 *TMN = nullptr, *TNN = nullptr, *QQ0 = nullptr, *ov[2] = {nullptr, nullptr};
   c128* logov = nullptr;
+  // determinants grouped by unique excitation of each spin (CSR rows u, entries = determinant k)
+  int* rowptr[2] = {nullptr, nullptr};
+  int* kidx[2] = {nullptr, nullptr};
+  // excitation shells (equal nex, contiguous unique indices): first index, count, nex
+  std::vector<int> sh_k0[2], sh_nd[2], sh_nex[2];
+  std::vector<int> uoff_h[2];
+  // energy: the Hamiltonian half-rotated with the active orbitals
+  bool has_ham = false;
+  int Nc = 0;
+  double E0 = 0.0;
+  c128* lnak[2] = {nullptr, nullptr};  // [Nc][nact][M]
+  c128* haj[2] = {nullptr, nullptr};   // [nact][M]
+  // energy scratch for a block of walkers
+  int capWb = 0;
+  c128 *eG[2] = {nullptr, nullptr}, *eQ[2] = {nullptr, nullptr}, *eov[2] = {nullptr, nullptr};
+  c128 *eTMN = nullptr, *eTNN = nullptr, *elogov = nullptr, *eOv = nullptr;
+  c128 *wgt = nullptr, *Swia = nullptr, *Twina = nullptr, *KEr = nullptr, *KEd = nullptr;
+  c128 *KEl = nullptr, *Kdn = nullptr, *R = nullptr, *el = nullptr;
+  size_t R_elems = 0, KEl_elems = 0;
+  void free_energy_scratch() {
+    for (c128** q : {&eG[0], &eG[1], &eQ[0], &eQ[1], &eov[0], &eov[1], &eTMN, &eTNN, &elogov,
+                     &eOv, &wgt, &Swia, &Twina, &KEr, &KEd, &KEl, &Kdn, &R, &el})
+      if (*q) {
+        cudaFree(*q);
+        *q = nullptr;
+      }
+    capWb = 0;
+  }
   void free_scratch() {
     for (c128** p : {&TMN, &TNN, &QQ0, &ov[0], &ov[1], &logov})
       if (*p) {
@@ -372,7 +603,12 @@ struct afqmc_phmsd_s {
   }
   ~afqmc_phmsd_s() {
     free_scratch();
+    free_energy_scratch();
     for (int s = 0; s < 2; ++s) {
+      cudaFree(rowptr[s]);
+      cudaFree(kidx[s]);
+      cudaFree(lnak[s]);
+      cudaFree(haj[s]);
       cudaFree(orbmat[s]);
       cudaFree(refc[s]);
       cudaFree(uoff[s]);
@@ -458,6 +694,12 @@ extern "C" int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact
       pos += 2 * n;
     }
   }
+  for (int s = 0; s < 2; ++s)
+    for (int u = 2; u < nuniq[s]; ++u)
+      AFQMC_CHECK_ARG(nex[s][u] >= nex[s][u - 1],
+                      "afqmc_phmsd_create: unique excitations of spin %d must be ordered by "
+                      "excitation number (u = %d has %d after %d)", s, u, nex[s][u],
+                      nex[s][u - 1]);
   for (int k = 0; k < ndet; ++k)
     AFQMC_CHECK_ARG(det_up[k] >= 0 && det_up[k] < nuniq_up && det_dn[k] >= 0 &&
                         det_dn[k] < nuniq_dn,
@@ -484,6 +726,27 @@ extern "C" int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact
   AFQMC_TRY(to_device(&h->det[0], det_up, size_t(ndet)));
   AFQMC_TRY(to_device(&h->det[1], det_dn, size_t(ndet)));
   AFQMC_TRY(to_device(&h->coef, reinterpret_cast<const c128*>(coef), size_t(ndet)));
+  const int* dets[2] = {det_up, det_dn};
+  for (int s = 0; s < 2; ++s) {
+    // CSR of the determinants by this spin's unique excitation, in determinant order
+    std::vector<int> rp(nuniq[s] + 1, 0), ki(ndet);
+    for (int k = 0; k < ndet; ++k) ++rp[dets[s][k] + 1];
+    for (int u = 0; u < nuniq[s]; ++u) rp[u + 1] += rp[u];
+    std::vector<int> pos(rp.begin(), rp.end() - 1);
+    for (int k = 0; k < ndet; ++k) ki[pos[dets[s][k]]++] = k;
+    AFQMC_TRY(to_device(&h->rowptr[s], rp.data(), rp.size()));
+    AFQMC_TRY(to_device(&h->kidx[s], ki.data(), ki.size()));
+    // shells of equal excitation number
+    for (int u = 1; u < nuniq[s]; ++u) {
+      if (h->sh_nex[s].empty() || h->sh_nex[s].back() != nex[s][u]) {
+        h->sh_k0[s].push_back(u);
+        h->sh_nd[s].push_back(0);
+        h->sh_nex[s].push_back(nex[s][u]);
+      }
+      ++h->sh_nd[s].back();
+    }
+    h->uoff_h[s] = off[s];
+  }
   *out = h.release();
   return AFQMC_OK;
 }
@@ -542,4 +805,297 @@ extern "C" int afqmc_phmsd_log_overlap(afqmc_phmsd h, const afqmc_c128* wbuf, lo
                                                 h->det[0], h->det[1], h->coef, h->ndet, h->logov,
                                                 reinterpret_cast<c128*>(ovlp));
   return launch_status("phmsd_combine_kernel");
+}
+
+// ---------------------------------------------------------------------------------------------
+// PHMSD energy (PHMSD::energy_alg1, Wavefunctions/PHMSD.cpp:376-546, COLLINEAR walkers)
+// ---------------------------------------------------------------------------------------------
+extern "C" int afqmc_phmsd_set_hamiltonian(afqmc_phmsd h, const double* Likn, int nspin_H2,
+                                           const afqmc_c128* hij, int nspin_H1, int Nc,
+                                           double E0) {
+  AFQMC_CHECK_ARG(h && Likn && hij, "afqmc_phmsd_set_hamiltonian: null argument");
+  AFQMC_CHECK_ARG(Nc > 0 && (nspin_H2 == 1 || nspin_H2 == 2) && (nspin_H1 == 1 || nspin_H1 == 2),
+                  "afqmc_phmsd_set_hamiltonian: Nc=%d nspin_H2=%d nspin_H1=%d", Nc, nspin_H2,
+                  nspin_H1);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(h->device);
+  const long M = h->M, MM = M * M;
+  double* L = nullptr;
+  c128 *hd = nullptr, *tmp = nullptr;
+  int st = AFQMC_OK;
+  auto fail = [&](int code) {
+    cudaFree(L);
+    cudaFree(hd);
+    cudaFree(tmp);
+    cudaSetDevice(prev);
+    return code;
+  };
+  if (cudaMalloc(&L, sizeof(double) * nspin_H2 * MM * Nc) != cudaSuccess ||
+      cudaMalloc(&hd, sizeof(c128) * nspin_H1 * MM) != cudaSuccess) {
+    set_error_detail("afqmc_phmsd_set_hamiltonian: out of device memory");
+    return fail(AFQMC_ERR_ALLOC);
+  }
+  cudaMemcpy(L, Likn, sizeof(double) * nspin_H2 * MM * Nc, cudaMemcpyHostToDevice);
+  cudaMemcpy(hd, hij, sizeof(c128) * nspin_H1 * MM, cudaMemcpyHostToDevice);
+  for (int sp = 0; sp < 2; ++sp) {
+    const int na = h->nact[sp];
+    cudaFree(h->lnak[sp]);
+    cudaFree(h->haj[sp]);
+    h->lnak[sp] = h->haj[sp] = nullptr;
+    if (cudaMalloc(&h->lnak[sp], sizeof(c128) * size_t(Nc) * na * M) != cudaSuccess ||
+        cudaMalloc(&h->haj[sp], sizeof(c128) * size_t(na) * M) != cudaSuccess ||
+        cudaMalloc(&tmp, sizeof(c128) * size_t(na) * MM * Nc) != cudaSuccess) {
+      set_error_detail("afqmc_phmsd_set_hamiltonian: out of device memory");
+      return fail(AFQMC_ERR_ALLOC);
+    }
+    // tmp[a][(k, n)] = sum_i OrbMat[a][i] L[i][(k, n)]  -> Lnak[n][a][k]
+    GemmParams p{};
+    p.m = na; p.n = int(M * Nc); p.k = int(M);
+    p.A = h->orbmat[sp]; p.lda = M; p.strideA = 0;
+    p.B = L + size_t(sp % nspin_H2) * MM * Nc; p.ldb = M * Nc; p.strideB = 0;
+    p.C = tmp; p.ldc = M * Nc; p.strideC = 0;
+    p.alpha = cmk(1, 0); p.beta = cmk(0, 0);
+    if ((st = zgemm(nullptr, 1, GN, false, GN, true, p))) return fail(st);
+    const long tot = long(na) * M * Nc;
+    lnak_act_reorder_kernel<<<unsigned((tot + 255) / 256), 256>>>(tmp, h->lnak[sp], na, int(M),
+                                                                   Nc);
+    if ((st = launch_status("lnak_act_reorder_kernel"))) return fail(st);
+    // haj = OrbMat h1
+    GemmParams q{};
+    q.m = na; q.n = int(M); q.k = int(M);
+    q.A = h->orbmat[sp]; q.lda = M;
+    q.B = hd + size_t(sp % nspin_H1) * MM; q.ldb = M;
+    q.C = h->haj[sp]; q.ldc = M;
+    q.alpha = cmk(1, 0); q.beta = cmk(0, 0);
+    if ((st = zgemm(nullptr, 1, GN, false, GN, false, q))) return fail(st);
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+      set_error_detail("afqmc_phmsd_set_hamiltonian: %s", cudaGetErrorString(cudaGetLastError()));
+      return fail(AFQMC_ERR_CUDA);
+    }
+    cudaFree(tmp);
+    tmp = nullptr;
+  }
+  h->Nc = Nc;
+  h->E0 = E0;
+  h->has_ham = true;
+  return fail(AFQMC_OK);
+}
+
+namespace {
+
+int phmsd_energy_scratch(afqmc_phmsd h, int Wb) {
+  if (h->capWb >= Wb) return AFQMC_OK;
+  AFQMC_CUDA_TRY(cudaDeviceSynchronize());
+  h->free_energy_scratch();
+  const size_t na = std::max(h->nact[0], h->nact[1]), ne = std::max(h->nel[0], h->nel[1]);
+  const size_t M = h->M, Nc = h->Nc;
+  int maxnd = 1;
+  size_t maxR = 1;
+  for (int s = 0; s < 2; ++s)
+    for (size_t j = 0; j < h->sh_nd[s].size(); ++j) {
+      maxnd = std::max(maxnd, h->sh_nd[s][j]);
+      maxR = std::max(maxR, size_t(h->sh_nd[s][j]) * h->sh_nex[s][j] * h->nact[s]);
+    }
+  const size_t nu = std::max(h->nuniq[0], h->nuniq[1]);
+  auto al = [](c128** p, size_t n) -> int {
+    if (cudaMalloc(p, sizeof(c128) * (n ? n : 1)) != cudaSuccess) {
+      set_error_detail("afqmc_phmsd_energy: out of device memory (%zu bytes)", sizeof(c128) * n);
+      return AFQMC_ERR_ALLOC;
+    }
+    return AFQMC_OK;
+  };
+  for (int s = 0; s < 2; ++s) {
+    AFQMC_TRY(al(&h->eG[s], size_t(Wb) * ne * M));
+    AFQMC_TRY(al(&h->eQ[s], size_t(Wb) * na * ne));
+    AFQMC_TRY(al(&h->eov[s], size_t(Wb) * h->nuniq[s]));
+  }
+  AFQMC_TRY(al(&h->eTMN, size_t(Wb) * na * ne));
+  AFQMC_TRY(al(&h->eTNN, size_t(Wb) * ne * ne));
+  AFQMC_TRY(al(&h->elogov, Wb));
+  AFQMC_TRY(al(&h->eOv, Wb));
+  AFQMC_TRY(al(&h->wgt, nu * Wb));
+  AFQMC_TRY(al(&h->Swia, size_t(Wb) * ne * na));
+  AFQMC_TRY(al(&h->Twina, size_t(Wb) * ne * Nc * na));
+  AFQMC_TRY(al(&h->KEr, size_t(h->nuniq[0]) * Wb * Nc));
+  AFQMC_TRY(al(&h->KEd, size_t(h->nuniq[1]) * Wb * Nc));
+  AFQMC_TRY(al(&h->KEl, size_t(maxnd) * Wb * Nc));
+  AFQMC_TRY(al(&h->Kdn, size_t(Wb) * Nc));
+  AFQMC_TRY(al(&h->R, maxR * Wb));
+  AFQMC_TRY(al(&h->el, 3 * size_t(Wb)));
+  h->capWb = Wb;
+  return AFQMC_OK;
+}
+
+// density matrix, Woodbury factors and excitation overlaps of spin sp for walkers [w0, w0+nb)
+int phmsd_spin_factors(afqmc_phmsd h, cudaStream_t s, int sp, const c128* S, long ldS, int nb) {
+  const int N = h->nel[sp], na = h->nact[sp];
+  GemmParams p{};
+  p.m = na; p.n = N; p.k = h->M;
+  p.A = h->orbmat[sp]; p.lda = h->M; p.strideA = 0;
+  p.B = S; p.ldb = N; p.strideB = ldS;
+  p.C = h->eTMN; p.ldc = N; p.strideC = long(na) * N;
+  p.alpha = cmk(1, 0); p.beta = cmk(0, 0);
+  AFQMC_TRY(zgemm(s, nb, GN, false, GN, false, p));
+  gather_ref_rows_kernel<<<nb, 128, 0, s>>>(h->eTMN, h->refc[sp], h->eTNN, na, N);
+  AFQMC_TRY(launch_status("gather_ref_rows_kernel"));
+  AFQMC_TRY(batched_logdet_inverse(s, h->eTNN, long(N) * N, h->eTNN, long(N) * N, h->elogov, nb,
+                                   N, true, cmk(1, 0), cmk(0, 0)));
+  // QQ0 = TAB TNN^{-1};  G = TNN^{-T} S^T  (compact, density_matrix.hpp:696-703)
+  GemmParams q{};
+  q.m = na; q.n = N; q.k = N;
+  q.A = h->eTMN; q.lda = N; q.strideA = long(na) * N;
+  q.B = h->eTNN; q.ldb = N; q.strideB = long(N) * N;
+  q.C = h->eQ[sp]; q.ldc = N; q.strideC = long(na) * N;
+  q.alpha = cmk(1, 0); q.beta = cmk(0, 0);
+  AFQMC_TRY(zgemm(s, nb, GN, false, GN, false, q));
+  GemmParams g{};
+  g.m = N; g.n = h->M; g.k = N;
+  g.A = h->eTNN; g.lda = N; g.strideA = long(N) * N;
+  g.B = S; g.ldb = N; g.strideB = ldS;
+  g.C = h->eG[sp]; g.ldc = h->M; g.strideC = long(N) * h->M;
+  g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+  AFQMC_TRY(zgemm(s, nb, GT, false, GT, false, g));
+  const long nt = long(h->nuniq[sp]) * nb;
+  excitation_det_kernel<<<unsigned((nt + 127) / 128), 128, 0, s>>>(
+      h->eQ[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->nuniq[sp], nb, na, N, h->eov[sp]);
+  return launch_status("excitation_det_kernel");
+}
+
+// Swia = G haj^T, Twina = G Lnak^T for spin sp
+int phmsd_half_rotated(afqmc_phmsd h, cudaStream_t s, int sp, int nb) {
+  const int N = h->nel[sp], na = h->nact[sp];
+  GemmParams p{};
+  p.m = nb * N; p.n = na; p.k = h->M;
+  p.A = h->eG[sp]; p.lda = h->M;
+  p.B = h->haj[sp]; p.ldb = h->M;
+  p.C = h->Swia; p.ldc = na;
+  p.alpha = cmk(1, 0); p.beta = cmk(0, 0);
+  AFQMC_TRY(zgemm(s, 1, GN, false, GT, false, p));
+  GemmParams q{};
+  q.m = nb * N; q.n = h->Nc * na; q.k = h->M;
+  q.A = h->eG[sp]; q.lda = h->M;
+  q.B = h->lnak[sp]; q.ldb = h->M;
+  q.C = h->Twina; q.ldc = long(h->Nc) * na;
+  q.alpha = cmk(1, 0); q.beta = cmk(0, 0);
+  return zgemm(s, 1, GN, false, GT, false, q);
+}
+
+// the excited determinants of spin sp, shell by shell: 1-body into el[0], 2-body into el[1..2],
+// KE of each determinant written to KEout + k0 * nb * Nc (cross = nullptr) or to KEl and
+// contracted with cross at once (the second step)
+int phmsd_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, c128* KEout, const c128* cross,
+                  c128* E) {
+  const int N = h->nel[sp], na = h->nact[sp], Nc = h->Nc;
+  AFQMC_CUDA_TRY(cudaMemsetAsync(h->el, 0, sizeof(c128) * 3 * nb, s));
+  for (size_t j = 0; j < h->sh_k0[sp].size(); ++j) {
+    const int k0 = h->sh_k0[sp][j], nd = h->sh_nd[sp][j], nex = h->sh_nex[sp][j];
+    const int* iex = h->uexc[sp] + h->uoff_h[sp][k0];
+    const size_t Rn = size_t(nb) * nd * nex * na;
+    AFQMC_CUDA_TRY(cudaMemsetAsync(h->R, 0, sizeof(c128) * Rn, s));
+    const long nt = long(nb) * nd;
+    compact_R_kernel<<<unsigned((nt + 127) / 128), 128, 0, s>>>(h->eQ[sp], iex, h->refc[sp], nd,
+                                                                nex, nb, na, N, h->R);
+    AFQMC_TRY(launch_status("compact_R_kernel"));
+    const c128* w = h->wgt + size_t(k0) * nb;
+    dim3 grid(nd, nb);
+    ph_excited_1body_kernel<<<grid, PH_THREADS, 0, s>>>(iex, h->refc[sp], h->Swia, h->R, w, nb,
+                                                        nd, nex, na, N, h->el);
+    AFQMC_TRY(launch_status("ph_excited_1body_kernel"));
+    c128* KE = cross ? h->KEl : KEout + size_t(k0) * nb * Nc;
+    const size_t smem = size_t(nex) * na * sizeof(c128) + 2 * size_t(N) * sizeof(int);
+    AFQMC_CUDA_TRY(cudaFuncSetAttribute(ph_excited_2body_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    ph_excited_2body_kernel<<<grid, PH_THREADS, smem, s>>>(iex, h->refc[sp], h->Twina, h->R, w,
+                                                          nb, nd, nex, na, N, Nc, h->el + nb,
+                                                          h->el + 2 * nb, KE);
+    AFQMC_TRY(launch_status("ph_excited_2body_kernel"));
+    if (cross) {
+      cross_ej_kernel<<<nb, PH_THREADS, 0, s>>>(cross + size_t(k0) * nb * Nc, h->KEl, nd, nb, Nc,
+                                                E);
+      AFQMC_TRY(launch_status("cross_ej_kernel"));
+    }
+  }
+  add_components_kernel<<<(nb + 127) / 128, 128, 0, s>>>(h->el, h->el + nb, h->el + 2 * nb, nb,
+                                                          E);
+  return launch_status("add_components_kernel");
+}
+
+}  // namespace
+
+extern "C" int afqmc_phmsd_energy(afqmc_phmsd h, const afqmc_c128* wbuf, long ldS,
+                                  afqmc_c128* E_out, afqmc_c128* ovlp, int W, int block,
+                                  afqmc_stream stream) {
+  AFQMC_CHECK_ARG(h && wbuf && E_out && ovlp, "afqmc_phmsd_energy: null argument");
+  AFQMC_CHECK_ARG(h->has_ham, "afqmc_phmsd_energy: no Hamiltonian (afqmc_phmsd_set_hamiltonian)");
+  AFQMC_CHECK_ARG(W >= 0 && ldS >= long(h->M) * (h->nel[0] + h->nel[1]),
+                  "afqmc_phmsd_energy: W=%d, walker stride %ld < M (nup + ndn)", W, ldS);
+  if (W == 0) return AFQMC_OK;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(h->device);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int Wb = block > 0 ? (block < W ? block : W) : (W < 32 ? W : 32);
+  int st = phmsd_energy_scratch(h, Wb);
+  if (st) {
+    cudaSetDevice(prev);
+    return st;
+  }
+  const int Nc = h->Nc;
+  const c128* S = reinterpret_cast<const c128*>(wbuf);
+  c128* Eall = reinterpret_cast<c128*>(E_out);
+  c128* Oall = reinterpret_cast<c128*>(ovlp);
+  auto run = [&]() -> int {
+    for (int w0 = 0; w0 < W; w0 += Wb) {
+      const int nb = (W - w0 < Wb) ? W - w0 : Wb;
+      const c128* Sb = S + long(w0) * ldS;
+      c128* E = Eall + size_t(w0) * 3;
+      AFQMC_CUDA_TRY(cudaMemsetAsync(E, 0, sizeof(c128) * 3 * nb, s));
+      AFQMC_CUDA_TRY(cudaMemsetAsync(h->elogov, 0, sizeof(c128) * nb, s));
+      AFQMC_TRY(phmsd_spin_factors(h, s, 0, Sb, ldS, nb));
+      AFQMC_TRY(phmsd_spin_factors(h, s, 1, Sb + long(h->M) * h->nel[0], ldS, nb));
+      const int nu0 = h->nuniq[0], nu1 = h->nuniq[1];
+      auto couple = [&](int sp, const c128* v_other, int nu_other, const c128* ov_self) -> int {
+        const long nt = long(h->nuniq[sp]) * nb;
+        couple_kernel<<<unsigned((nt + 127) / 128), 128, 0, s>>>(
+            h->rowptr[sp], h->kidx[sp], h->det[1 - sp], h->coef, v_other, nu_other, ov_self,
+            h->nuniq[sp], nb, h->wgt);
+        return launch_status("couple_kernel");
+      };
+      // spin up: weights, total overlap, reference and excited energies (PHMSD.cpp:438-470)
+      AFQMC_TRY(couple(0, h->eov[1], nu1, nullptr));
+      total_overlap_kernel<<<nb, PH_THREADS, 0, s>>>(h->wgt, h->eov[0], nu0, nb, h->eOv);
+      AFQMC_TRY(launch_status("total_overlap_kernel"));
+      AFQMC_TRY(couple(0, h->eov[1], nu1, h->eov[0]));
+      AFQMC_TRY(phmsd_half_rotated(h, s, 0, nb));
+      ph_reference_kernel<<<nb, PH_THREADS, 0, s>>>(h->Swia, h->Twina, h->refc[0], h->nel[0], Nc,
+                                                    h->nact[0], h->E0, h->eOv, E, h->KEr);
+      AFQMC_TRY(launch_status("ph_reference_kernel"));
+      AFQMC_TRY(phmsd_excited(h, s, 0, nb, h->KEr, nullptr, E));
+      // K vectors coupled to the down-spin excitations (PHMSD.cpp:472-494)
+      {
+        dim3 grid(nu1, nb);
+        couple_ke_kernel<<<grid, 128, 0, s>>>(h->rowptr[1], h->kidx[1], h->det[0], h->coef,
+                                              h->KEr, h->eov[0], nu0, h->eov[1], nu1, nb, Nc,
+                                              h->KEd);
+        AFQMC_TRY(launch_status("couple_ke_kernel"));
+      }
+      // spin down (PHMSD.cpp:497-531)
+      AFQMC_TRY(couple(1, h->eov[0], nu0, h->eov[1]));
+      AFQMC_TRY(phmsd_half_rotated(h, s, 1, nb));
+      ph_reference_kernel<<<nb, PH_THREADS, 0, s>>>(h->Swia, h->Twina, h->refc[1], h->nel[1], Nc,
+                                                    h->nact[1], 0.0, h->eOv, E, h->Kdn);
+      AFQMC_TRY(launch_status("ph_reference_kernel"));
+      cross_ej_kernel<<<nb, PH_THREADS, 0, s>>>(h->KEd, h->Kdn, 1, nb, Nc, E);
+      AFQMC_TRY(launch_status("cross_ej_kernel"));
+      AFQMC_TRY(phmsd_excited(h, s, 1, nb, nullptr, h->KEd, E));
+      finish_energy_kernel<<<(nb + 127) / 128, 128, 0, s>>>(h->eOv, h->elogov, nb, E,
+                                                            Oall + w0);
+      AFQMC_TRY(launch_status("finish_energy_kernel"));
+    }
+    return AFQMC_OK;
+  };
+  st = run();
+  cudaSetDevice(prev);
+  return st;
 }

@@ -111,3 +111,31 @@ def test_phmsd_log_overlap_vs_oracle(cuda, M, nup, ndn, nocc, nvirt, ndet, W):
     d = got - ref
     d = d.real + 1j * ((d.imag + np.pi) % (2 * np.pi) - np.pi)
     assert np.max(np.abs(d)) < 1e-10, (got, ref)
+
+
+@pytest.mark.parametrize("M,nup,ndn,Nc,nocc,nvirt,ndet,W,block", [
+    (16, 4, 3, 6, 3, 5, 40, 3, 0), (40, 10, 9, 30, 6, 14, 300, 21, 8)])
+def test_phmsd_energy_vs_oracle(cuda, M, nup, ndn, Nc, nocc, nvirt, ndet, W, block):
+    """PHMSD energy_alg1 on the GPU (walker blocks, excitation shells, spin couplings) against
+    the oracle's restatement (itself pinned against single-determinant energies)."""
+    from safire_b200 import afqmc as A
+    from safire_b200.synth import make_hamiltonian, make_phmsd_trial
+    h1, Likn = make_hamiltonian(M, Nc, 0.9, seed=M)
+    _, C = np.linalg.eigh(h1)
+    t = make_phmsd_trial(M, nup, ndn, C, nocc=nocc, nvirt=nvirt, ndet=ndet, seed=M)
+    hij = h1[None].astype(complex)
+    rs = np.random.default_rng(M + 2)
+    Su = (rs.standard_normal((W, M, nup)) + 1j * rs.standard_normal((W, M, nup))) / np.sqrt(M)
+    Sd = (rs.standard_normal((W, M, ndn)) + 1j * rs.standard_normal((W, M, ndn))) / np.sqrt(M)
+    wbuf = to_dev(np.concatenate([Su.reshape(W, -1), Sd.reshape(W, -1), np.zeros((W, 11))], 1))
+    ph = A.PHMSD(t)
+    ph.set_hamiltonian(Likn[None], hij, 0.3)
+    E = torch.zeros((W, 3), dtype=torch.complex128, device=cuda)
+    ov = torch.zeros(W, dtype=torch.complex128, device=cuda)
+    ph.Energy(wbuf, E, ov, block=block)
+    H = P.ActiveSpaceHamiltonian(t, Likn[None], hij, 0.3)
+    Eo, ovo = P.phmsd_energy(t, H, Su, Sd)
+    assert rel_err(to_host(E), Eo) < 1e-10
+    d = to_host(ov) - ovo
+    d = d.real + 1j * ((d.imag + np.pi) % (2 * np.pi) - np.pi)
+    assert np.max(np.abs(d)) < 1e-10

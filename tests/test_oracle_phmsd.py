@@ -75,3 +75,47 @@ def test_phmsd_log_overlap_woodbury_vs_full_determinants():
             dd = np.linalg.det(t.orbmat[1][occ[1][t.det_dn[k]]] @ S_dn[w])
             tot += t.coef[k] * du * dd
         assert abs(np.exp(logov[w]) - tot) <= 1e-10 * abs(tot), (w, np.exp(logov[w]), tot)
+
+
+def test_phmsd_energy_woodbury_vs_single_determinants():
+    """energy_alg1's Woodbury evaluation against sum_k c_k ov_k E_k / sum_k c_k ov_k with every
+    determinant's local energy from the single-determinant (NOMSD, COLLINEAR) oracle."""
+    from oracle import afqmc as O
+    from safire_b200.synth import make_hamiltonian, make_phmsd_trial
+    M, nup, ndn, Nc = 16, 4, 3, 6
+    h1, Likn = make_hamiltonian(M, Nc, 0.9, seed=3)
+    _, C = np.linalg.eigh(h1)
+    t = make_phmsd_trial(M, nup, ndn, C, nocc=3, nvirt=5, ndet=40, seed=3)
+    hij = h1[None].astype(complex)
+    H = P.ActiveSpaceHamiltonian(t, Likn[None], hij, 0.7)
+    rs = np.random.default_rng(8)
+    W = 3
+    S_up = (rs.standard_normal((W, M, nup)) + 1j * rs.standard_normal((W, M, nup))) / 4
+    S_dn = (rs.standard_normal((W, M, ndn)) + 1j * rs.standard_normal((W, M, ndn))) / 4
+    E, logov = P.phmsd_energy(t, H, S_up, S_dn)
+    # brute force over determinants
+    occ = []
+    for s in (0, 1):
+        lst = [t.refc[s].copy()]
+        for n in sorted(t.exc[s]):
+            for e in t.exc[s][n]:
+                o = t.refc[s].copy()
+                o[e[:n]] = e[n:]
+                lst.append(o)
+        occ.append(lst)
+    num = np.zeros((W, 3), complex)
+    den = np.zeros(W, complex)
+    for k in range(t.coef.size):
+        Pu = t.orbmat[0][occ[0][t.det_up[k]]]
+        Pd = t.orbmat[1][occ[1][t.det_dn[k]]]
+        ham = O.Real3IndexFactorization(O.COLLINEAR, M, nup, ndn, Likn[None], hij, 0.7, [Pu, Pd])
+        for w in range(W):
+            Tu, Td = Pu @ S_up[w], Pd @ S_dn[w]
+            ov = np.linalg.det(Tu) * np.linalg.det(Td)
+            G = np.concatenate([np.linalg.inv(Tu).T @ S_up[w].T, np.linalg.inv(Td).T @ S_dn[w].T])
+            Ek = ham.energy(G[None])[0]
+            num[w] += t.coef[k] * ov * Ek
+            den[w] += t.coef[k] * ov
+    ref = num / den[:, None]
+    assert np.allclose(E, ref, rtol=1e-10, atol=1e-10), (E, ref)
+    assert np.allclose(np.exp(logov), den, rtol=1e-10)
