@@ -356,6 +356,20 @@ int afqmc_phmsd_set_hamiltonian(afqmc_phmsd trial, const double* Likn, int nspin
  * (<= 0: 32); the excitation lists must be ordered by excitation number. */
 int afqmc_phmsd_energy(afqmc_phmsd trial, const afqmc_c128* wbuf, long ldS, afqmc_c128* E,
                        afqmc_c128* ovlp, int W, int block, afqmc_stream stream);
+/* PHMSD::MixedDensityMatrix, compact COLLINEAR (PHMSD.cpp:684-795): G [W][nact_up +
+ * nact_dn][M] (device, written) = (R_s^T G_s^ref) / Ov per spin block, with R the coefficient-
+ * weighted Woodbury matrices of every excited determinant (calculate_R,
+ * phmsd_helpers.hpp:200-309); ovlp [W] (device, written) the log overlap.  Blocks of `block`
+ * walkers (<= 0: 32). */
+int afqmc_phmsd_density_matrix(afqmc_phmsd trial, const afqmc_c128* wbuf, long ldS,
+                               afqmc_c128* G, afqmc_c128* ovlp, int W, int block,
+                               afqmc_stream stream);
+/* PHMSD::vbias (PHMSD.cpp:54-72) over Real3IndexFactorization::vbias
+ * (Real3IndexFactorization.hpp:328-384): v [W][Nc] (device, written) = sqrt(dt) sum_s Lnak_s . G_s
+ * with G from afqmc_phmsd_density_matrix and the active-space Lnak of
+ * afqmc_phmsd_set_hamiltonian. */
+int afqmc_phmsd_vbias(afqmc_phmsd trial, const afqmc_c128* G, afqmc_c128* v, int W, double dt,
+                      afqmc_stream stream);
 
 /* comb (population_control.hpp:34-65): host arrays; draws one uniform from rng. */
 int afqmc_comb(afqmc_host_rng rng, const double* weights, int n, int num_target, int* offspring);

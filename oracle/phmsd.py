@@ -288,3 +288,57 @@ def phmsd_energy(trial, H, S_up, S_dn):
     E += el
     E = E / Ov[:, None]
     return E, np.log(Ov) + log_ov
+
+
+def calculate_R(trial, s, QQ0, wgt):
+    """calculate_R (phmsd_helpers.hpp:200-309): R [W][N][nact] = sum over unique excitations u
+    (index 0 the reference) of wgt[u][w] times the Woodbury R of u: identity on the determinant's
+    occupations plus, on the hole rows, -Q[p][q] QQ0[part_q][i] at orbs(i) and +Q[p][q] at
+    orbs(hole_q)."""
+    W, nact, nel = QQ0.shape
+    refc = np.asarray(trial.refc[s])
+    R = np.zeros((W, nel, nact), complex)
+    R[:, np.arange(nel), refc] += wgt[0][:, None]
+    u = 1
+    for n in sorted(trial.exc[s]):
+        for e in trial.exc[s][n]:
+            holes, parts = e[:n], e[n:]
+            orbs = refc.copy()
+            orbs[holes] = parts
+            for w in range(W):
+                Q = QQ0[w][np.ix_(parts, holes)]
+                if abs(np.linalg.det(Q)) == 0.0:
+                    continue
+                Qi = np.linalg.inv(Q)
+                wu = wgt[u][w]
+                R[w, np.arange(nel), orbs] += wu
+                for p in range(n):
+                    for q in range(n):
+                        R[w, holes[p], orbs] -= wu * Qi[p, q] * QQ0[w, parts[q], :]
+                        R[w, holes[p], orbs[holes[q]]] += wu * Qi[p, q]
+            u += 1
+    return R
+
+
+def phmsd_mixed_density_matrix(trial, S_up, S_dn):
+    """PHMSD::MixedDensityMatrix, compact, COLLINEAR (PHMSD.cpp:684-795): G [W][nact_up +
+    nact_dn][M] = (R_s^T G_s) / Ov per spin block, and the log overlap [W]."""
+    Gu, lu, Qu = mixed_density_matrix_for_woodbury(trial.orbmat[0], S_up, trial.refc[0])
+    Gd, ld, Qd = mixed_density_matrix_for_woodbury(trial.orbmat[1], S_dn, trial.refc[1])
+    ovu = excitation_overlaps(trial, 0, Qu)
+    ovd = excitation_overlaps(trial, 1, Qd)
+    wgt = _couple(trial, 0, ovd)
+    Ov = np.sum(wgt * ovu, axis=0)
+    Ru = calculate_R(trial, 0, Qu, wgt * ovu)
+    Rd = calculate_R(trial, 1, Qd, _couple(trial, 1, ovu) * ovd)
+    G = np.concatenate([np.einsum("wia,wik->wak", Ru, Gu), np.einsum("wia,wik->wak", Rd, Gd)],
+                       axis=1) / Ov[:, None, None]
+    return G, np.log(Ov) + lu + ld
+
+
+def phmsd_vbias(ham, G, dt, nact_up):
+    """PHMSD::vbias over Real3IndexFactorization::vbias (PHMSD.cpp:54-72,
+    Real3IndexFactorization.hpp:328-384), COLLINEAR: v [W][Nc] = sqrt(dt) sum_s Lnak_s . G_s
+    with G [W][nact_up + nact_dn][M] the compact PHMSD density matrix."""
+    Gs = (G[:, :nact_up, :], G[:, nact_up:, :])
+    return np.sqrt(dt) * sum(np.einsum("nak,wak->wn", ham.Lnak[s], Gs[s]) for s in (0, 1))

@@ -520,3 +520,13 @@ class PHMSD:
         """ovlp [W] (device) <- log overlap of every walker row of wbuf [W][ldS] (device)."""
         call("afqmc_phmsd_log_overlap", self.handle, _ptr(wbuf), int(wbuf.stride(0)), _ptr(ovlp),
              int(wbuf.shape[0]), _stream(stream))
+
+    def MixedDensityMatrix(self, wbuf, G, ovlp, block=0, stream=None):
+        """G [W, nact_up + nact_dn, M] (device) and ovlp [W] (device) of every walker row."""
+        call("afqmc_phmsd_density_matrix", self.handle, _ptr(wbuf), int(wbuf.stride(0)), _ptr(G),
+             _ptr(ovlp), int(wbuf.shape[0]), int(block), _stream(stream))
+
+    def vbias(self, G, v, dt, stream=None):
+        """v [W, Nc] (device) <- sqrt(dt) sum_s Lnak_s . G_s (G from MixedDensityMatrix)."""
+        call("afqmc_phmsd_vbias", self.handle, _ptr(G), _ptr(v), int(G.shape[0]), float(dt),
+             _stream(stream))

@@ -11,6 +11,7 @@
 //   Twina  [nw][nelec][nchol][nact], R [nw][ndet][nex][nact], wgt [ndet][nw], S [nw][nelec][nact]
 //   EX, EJ, E [nw] (accumulated), KE [ndet][nw][nchol] (written)
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -450,6 +451,13 @@ __global__ void add_components_kernel(const c128* __restrict__ e1, const c128* _
   E[w * 3 + 2] = cadd(E[w * 3 + 2], ej[w]);
 }
 
+// ovlp[w] = log Ov[w] + logov[w]
+__global__ void phmsd_combine_log_kernel(const c128* __restrict__ Ov, const c128* __restrict__ logov,
+                                         int W, c128* __restrict__ ovlp) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w < W) ovlp[w] = cadd(clog(Ov[w]), logov[w]);
+}
+
 // E[w] /= Ov[w];  ovlp[w] = log Ov[w] + logov[w]
 __global__ void finish_energy_kernel(const c128* __restrict__ Ov, const c128* __restrict__ logov,
                                      int W, c128* __restrict__ E, c128* __restrict__ ovlp) {
@@ -458,6 +466,64 @@ __global__ void finish_energy_kernel(const c128* __restrict__ Ov, const c128* __
   const c128 r = cdiv(cmk(1.0, 0.0), Ov[w]);
   for (int c = 0; c < 3; ++c) E[w * 3 + c] = cmul(E[w * 3 + c], r);
   ovlp[w] = cadd(clog(Ov[w]), logov[w]);
+}
+
+// R[w][i][refc_i] += sum_u wgt[u][w]  (the identity part of every determinant's R on its
+// reference rows; the excited rows are corrected in accumulate_R_kernel)
+__global__ void __launch_bounds__(PH_THREADS) r_identity_kernel(const c128* __restrict__ wgt,
+                                                               int nu, int W,
+                                                               const int* __restrict__ refc,
+                                                               int nel, int nact,
+                                                               c128* __restrict__ R) {
+  __shared__ double red[PH_THREADS / 32 * 6];
+  __shared__ c128 tot;
+  const int w = blockIdx.x;
+  c128 s = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0);
+  for (int u = threadIdx.x; u < nu; u += blockDim.x) s = cadd(s, wgt[size_t(u) * W + w]);
+  block_sum3(s, z1, z2, red);
+  if (threadIdx.x == 0) tot = s;
+  __syncthreads();
+  for (int i = threadIdx.x; i < nel; i += blockDim.x) {
+    c128* r = R + (size_t(w) * nel + i) * nact + refc[i];
+    *r = cadd(*r, tot);
+  }
+}
+
+// One excitation shell's contribution to the full R (calculate_R, phmsd_helpers.hpp:225-262):
+// for electron i and every (determinant d, row p) of the shell where i is hole p,
+//   R[w][i][:] += wgt_d Rc[w][d][p][:],  R[w][i][particle_p] += wgt_d,  R[w][i][refc_i] -= wgt_d
+// (Rc: the compact R of the shell).  One CTA per (walker, electron): no atomics.
+__global__ void accumulate_R_kernel(const c128* __restrict__ Rc, const c128* __restrict__ wgt,
+                                    const int* __restrict__ eptr, const int* __restrict__ eidx,
+                                    const int* __restrict__ iexcit, const int* __restrict__ refc,
+                                    int nd, int nex, int W, int nel, int nact,
+                                    c128* __restrict__ R) {
+  const int w = blockIdx.x, i = blockIdx.y;
+  const int j0 = eptr[i], j1 = eptr[i + 1];
+  if (j0 == j1) return;
+  c128* Ri = R + (size_t(w) * nel + i) * nact;
+  for (int a = threadIdx.x; a < nact; a += blockDim.x) {
+    c128 acc = cmk(0, 0);
+    for (int j = j0; j < j1; ++j) {
+      const int dp = eidx[j], d = dp / nex, p = dp - d * nex;
+      const c128 wd = wgt[size_t(d) * W + w];
+      acc = cadd(acc, cmul(wd, Rc[((size_t(w) * nd + d) * nex + p) * nact + a]));
+      if (iexcit[size_t(d) * 2 * nex + nex + p] == a) acc = cadd(acc, wd);
+      if (refc[i] == a) acc = csub(acc, wd);
+    }
+    Ri[a] = cadd(Ri[a], acc);
+  }
+}
+
+// x[w][...] *= 1 / Ov[w]
+__global__ void scale_by_overlap_kernel(c128* __restrict__ x, long per_w, long stride_w,
+                                        const c128* __restrict__ Ov, int W) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(W) * per_w) return;
+  const int w = int(t / per_w);
+  const long e = t - long(w) * per_w;
+  c128* v = x + long(w) * stride_w + e;
+  *v = cmul(*v, cdiv(cmk(1.0, 0.0), Ov[w]));
 }
 
 int check_dims(const char* who, int nw, int ndet, int nex, int nact, int nelec) {
@@ -571,6 +637,12 @@ struct afqmc_phmsd_s {
   // excitation shells (equal nex, contiguous unique indices): first index, count, nex
   std::vector<int> sh_k0[2], sh_nd[2], sh_nex[2];
   std::vector<int> uoff_h[2];
+  // per shell: for every electron, the (determinant, row) pairs where it is a hole
+  std::vector<int> sh_eoff[2];  // offset of the shell's eptr block ([nel+1]) in eptr
+  std::vector<int> sh_ioff[2];  // offset of the shell's entries in eidx
+  int* eptr[2] = {nullptr, nullptr};
+  int* eidx[2] = {nullptr, nullptr};
+  c128* Rfull = nullptr;
   // energy: the Hamiltonian half-rotated with the active orbitals
   bool has_ham = false;
   int Nc = 0;
@@ -586,7 +658,7 @@ struct afqmc_phmsd_s {
   size_t R_elems = 0, KEl_elems = 0;
   void free_energy_scratch() {
     for (c128** q : {&eG[0], &eG[1], &eQ[0], &eQ[1], &eov[0], &eov[1], &eTMN, &eTNN, &elogov,
-                     &eOv, &wgt, &Swia, &Twina, &KEr, &KEd, &KEl, &Kdn, &R, &el})
+                     &eOv, &wgt, &Swia, &Twina, &KEr, &KEd, &KEl, &Kdn, &R, &el, &Rfull})
       if (*q) {
         cudaFree(*q);
         *q = nullptr;
@@ -607,6 +679,8 @@ struct afqmc_phmsd_s {
     for (int s = 0; s < 2; ++s) {
       cudaFree(rowptr[s]);
       cudaFree(kidx[s]);
+      cudaFree(eptr[s]);
+      cudaFree(eidx[s]);
       cudaFree(lnak[s]);
       cudaFree(haj[s]);
       cudaFree(orbmat[s]);
@@ -746,6 +820,25 @@ extern "C" int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact
       ++h->sh_nd[s].back();
     }
     h->uoff_h[s] = off[s];
+    // electron -> (determinant, row) lists of every shell
+    std::vector<int> ep, ei;
+    for (size_t j = 0; j < h->sh_k0[s].size(); ++j) {
+      const int k0 = h->sh_k0[s][j], nd = h->sh_nd[s][j], n = h->sh_nex[s][j];
+      std::vector<std::vector<int>> lists(nel[s]);
+      for (int d = 0; d < nd; ++d)
+        for (int p = 0; p < n; ++p) lists[excs[s][off[s][k0 + d] + p]].push_back(d * n + p);
+      h->sh_eoff[s].push_back(int(ep.size()));
+      h->sh_ioff[s].push_back(int(ei.size()));
+      int cnt = 0;
+      ep.push_back(0);
+      for (int i = 0; i < nel[s]; ++i) {
+        for (int x : lists[i]) ei.push_back(x);
+        cnt += int(lists[i].size());
+        ep.push_back(cnt);
+      }
+    }
+    AFQMC_TRY(to_device(&h->eptr[s], ep.data(), ep.size()));
+    AFQMC_TRY(to_device(&h->eidx[s], ei.data(), ei.size()));
   }
   *out = h.release();
   return AFQMC_OK;
@@ -876,6 +969,7 @@ extern "C" int afqmc_phmsd_set_hamiltonian(afqmc_phmsd h, const double* Likn, in
     cudaFree(tmp);
     tmp = nullptr;
   }
+  h->free_energy_scratch();  // sized for the previous number of Cholesky vectors
   h->Nc = Nc;
   h->E0 = E0;
   h->has_ham = true;
@@ -923,6 +1017,7 @@ int phmsd_energy_scratch(afqmc_phmsd h, int Wb) {
   AFQMC_TRY(al(&h->Kdn, size_t(Wb) * Nc));
   AFQMC_TRY(al(&h->R, maxR * Wb));
   AFQMC_TRY(al(&h->el, 3 * size_t(Wb)));
+  AFQMC_TRY(al(&h->Rfull, size_t(Wb) * ne * na));
   h->capWb = Wb;
   return AFQMC_OK;
 }
@@ -1096,6 +1191,123 @@ extern "C" int afqmc_phmsd_energy(afqmc_phmsd h, const afqmc_c128* wbuf, long ld
     return AFQMC_OK;
   };
   st = run();
+  cudaSetDevice(prev);
+  return st;
+}
+
+// ---------------------------------------------------------------------------------------------
+// PHMSD mixed density matrix (PHMSD::MixedDensityMatrix, compact, PHMSD.cpp:684-795) and vbias
+// ---------------------------------------------------------------------------------------------
+extern "C" int afqmc_phmsd_density_matrix(afqmc_phmsd h, const afqmc_c128* wbuf, long ldS,
+                                          afqmc_c128* G_out, afqmc_c128* ovlp, int W, int block,
+                                          afqmc_stream stream) {
+  AFQMC_CHECK_ARG(h && wbuf && G_out && ovlp, "afqmc_phmsd_density_matrix: null argument");
+  AFQMC_CHECK_ARG(W >= 0 && ldS >= long(h->M) * (h->nel[0] + h->nel[1]),
+                  "afqmc_phmsd_density_matrix: W=%d, walker stride %ld < M (nup + ndn)", W, ldS);
+  if (W == 0) return AFQMC_OK;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(h->device);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int Wb = block > 0 ? (block < W ? block : W) : (W < 32 ? W : 32);
+  int st = phmsd_energy_scratch(h, Wb);
+  if (st) {
+    cudaSetDevice(prev);
+    return st;
+  }
+  const c128* S = reinterpret_cast<const c128*>(wbuf);
+  c128* Gall = reinterpret_cast<c128*>(G_out);
+  c128* Oall = reinterpret_cast<c128*>(ovlp);
+  const long rowsG = long(h->nact[0]) + h->nact[1];
+  auto run = [&]() -> int {
+    for (int w0 = 0; w0 < W; w0 += Wb) {
+      const int nb = (W - w0 < Wb) ? W - w0 : Wb;
+      const c128* Sb = S + long(w0) * ldS;
+      AFQMC_CUDA_TRY(cudaMemsetAsync(h->elogov, 0, sizeof(c128) * nb, s));
+      AFQMC_TRY(phmsd_spin_factors(h, s, 0, Sb, ldS, nb));
+      AFQMC_TRY(phmsd_spin_factors(h, s, 1, Sb + long(h->M) * h->nel[0], ldS, nb));
+      for (int sp = 0; sp < 2; ++sp) {
+        const int N = h->nel[sp], na = h->nact[sp], nu = h->nuniq[sp];
+        const long nt = long(nu) * nb;
+        // wgt[u][w] (PHMSD.cpp:717-724, 754-760)
+        if (sp == 0) {
+          couple_kernel<<<unsigned((nt + 127) / 128), 128, 0, s>>>(
+              h->rowptr[0], h->kidx[0], h->det[1], h->coef, h->eov[1], h->nuniq[1], nullptr, nu,
+              nb, h->wgt);
+          AFQMC_TRY(launch_status("couple_kernel"));
+          total_overlap_kernel<<<nb, PH_THREADS, 0, s>>>(h->wgt, h->eov[0], nu, nb, h->eOv);
+          AFQMC_TRY(launch_status("total_overlap_kernel"));
+        }
+        couple_kernel<<<unsigned((nt + 127) / 128), 128, 0, s>>>(
+            h->rowptr[sp], h->kidx[sp], h->det[1 - sp], h->coef, h->eov[1 - sp],
+            h->nuniq[1 - sp], h->eov[sp], nu, nb, h->wgt);
+        AFQMC_TRY(launch_status("couple_kernel"));
+        // full R (calculate_R): identity part, then each shell's Woodbury rows
+        AFQMC_CUDA_TRY(cudaMemsetAsync(h->Rfull, 0, sizeof(c128) * size_t(nb) * N * na, s));
+        r_identity_kernel<<<nb, PH_THREADS, 0, s>>>(h->wgt, nu, nb, h->refc[sp], N, na, h->Rfull);
+        AFQMC_TRY(launch_status("r_identity_kernel"));
+        for (size_t j = 0; j < h->sh_k0[sp].size(); ++j) {
+          const int k0 = h->sh_k0[sp][j], nd = h->sh_nd[sp][j], nex = h->sh_nex[sp][j];
+          const int* iex = h->uexc[sp] + h->uoff_h[sp][k0];
+          AFQMC_CUDA_TRY(cudaMemsetAsync(h->R, 0, sizeof(c128) * size_t(nb) * nd * nex * na, s));
+          const long nr = long(nb) * nd;
+          compact_R_kernel<<<unsigned((nr + 127) / 128), 128, 0, s>>>(h->eQ[sp], iex, h->refc[sp],
+                                                                      nd, nex, nb, na, N, h->R);
+          AFQMC_TRY(launch_status("compact_R_kernel"));
+          dim3 grid(nb, N);
+          accumulate_R_kernel<<<grid, 64, 0, s>>>(h->R, h->wgt + size_t(k0) * nb,
+                                                  h->eptr[sp] + h->sh_eoff[sp][j],
+                                                  h->eidx[sp] + h->sh_ioff[sp][j], iex,
+                                                  h->refc[sp], nd, nex, nb, N, na, h->Rfull);
+          AFQMC_TRY(launch_status("accumulate_R_kernel"));
+        }
+        // G_s = R^T G_ref  (rows of this spin's active orbitals)
+        GemmParams p{};
+        p.m = na; p.n = h->M; p.k = N;
+        p.A = h->Rfull; p.lda = na; p.strideA = long(N) * na;
+        p.B = h->eG[sp]; p.ldb = h->M; p.strideB = long(N) * h->M;
+        p.C = Gall + long(w0) * rowsG * h->M + (sp == 0 ? 0 : long(h->nact[0]) * h->M);
+        p.ldc = h->M; p.strideC = rowsG * h->M;
+        p.alpha = cmk(1, 0); p.beta = cmk(0, 0);
+        AFQMC_TRY(zgemm(s, nb, GT, false, GN, false, p));
+      }
+      const long per = rowsG * h->M;
+      scale_by_overlap_kernel<<<unsigned((per * nb + 255) / 256), 256, 0, s>>>(
+          Gall + long(w0) * per, per, per, h->eOv, nb);
+      AFQMC_TRY(launch_status("scale_by_overlap_kernel"));
+      phmsd_combine_log_kernel<<<(nb + 127) / 128, 128, 0, s>>>(h->eOv, h->elogov, nb,
+                                                                Oall + w0);
+      AFQMC_TRY(launch_status("phmsd_combine_log_kernel"));
+    }
+    return AFQMC_OK;
+  };
+  st = run();
+  cudaSetDevice(prev);
+  return st;
+}
+
+extern "C" int afqmc_phmsd_vbias(afqmc_phmsd h, const afqmc_c128* G, afqmc_c128* v, int W,
+                                 double dt, afqmc_stream stream) {
+  AFQMC_CHECK_ARG(h && G && v, "afqmc_phmsd_vbias: null argument");
+  AFQMC_CHECK_ARG(h->has_ham, "afqmc_phmsd_vbias: no Hamiltonian (afqmc_phmsd_set_hamiltonian)");
+  if (W <= 0) return AFQMC_OK;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(h->device);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const long rowsG = long(h->nact[0]) + h->nact[1];
+  int st = AFQMC_OK;
+  // v[w][n] = sqrt(dt) sum_s sum_{a,k} G_s[w][a][k] Lnak_s[n][a][k]  (Real3Index vbias, COLLINEAR)
+  for (int sp = 0; sp < 2 && !st; ++sp) {
+    GemmParams p{};
+    p.m = W; p.n = h->Nc; p.k = h->nact[sp] * h->M;
+    p.A = reinterpret_cast<const c128*>(G) + (sp == 0 ? 0 : long(h->nact[0]) * h->M);
+    p.lda = rowsG * h->M;
+    p.B = h->lnak[sp]; p.ldb = long(h->nact[sp]) * h->M;
+    p.C = reinterpret_cast<c128*>(v); p.ldc = h->Nc;
+    p.alpha = cmk(std::sqrt(dt), 0); p.beta = cmk(sp == 0 ? 0.0 : 1.0, 0);
+    st = zgemm(s, 1, GN, false, GT, false, p);
+  }
   cudaSetDevice(prev);
   return st;
 }

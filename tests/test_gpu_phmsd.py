@@ -139,3 +139,42 @@ def test_phmsd_energy_vs_oracle(cuda, M, nup, ndn, Nc, nocc, nvirt, ndet, W, blo
     d = to_host(ov) - ovo
     d = d.real + 1j * ((d.imag + np.pi) % (2 * np.pi) - np.pi)
     assert np.max(np.abs(d)) < 1e-10
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("M,nup,ndn,Nc,nocc,nvirt,ndet,W,block", [
+    (24, 5, 4, 30, 5, 8, 40, 5, 0),
+    (40, 9, 9, 64, 9, 14, 300, 7, 3),
+    (64, 12, 10, 48, 12, 20, 800, 33, 0),
+])
+def test_phmsd_density_matrix_and_vbias_vs_oracle(cuda, M, nup, ndn, Nc, nocc, nvirt, ndet, W,
+                                                   block):
+    """PHMSD MixedDensityMatrix (full Woodbury R per electron, then R^T G_ref / Ov) and the
+    active-space vbias on the GPU against the oracle (whose density matrix is pinned against the
+    determinant-by-determinant sum)."""
+    from safire_b200 import afqmc as A
+    from safire_b200.synth import make_hamiltonian, make_phmsd_trial
+    h1, Likn = make_hamiltonian(M, Nc, 0.9, seed=M + 5)
+    _, C = np.linalg.eigh(h1)
+    t = make_phmsd_trial(M, nup, ndn, C, nocc=nocc, nvirt=nvirt, ndet=ndet, seed=M + 1)
+    hij = h1[None].astype(complex)
+    rs = np.random.default_rng(M + 3)
+    Su = (rs.standard_normal((W, M, nup)) + 1j * rs.standard_normal((W, M, nup))) / np.sqrt(M)
+    Sd = (rs.standard_normal((W, M, ndn)) + 1j * rs.standard_normal((W, M, ndn))) / np.sqrt(M)
+    wbuf = to_dev(np.concatenate([Su.reshape(W, -1), Sd.reshape(W, -1), np.zeros((W, 7))], 1))
+    ph = A.PHMSD(t)
+    ph.set_hamiltonian(Likn[None], hij, 0.0)
+    na = t.orbmat[0].shape[0] + t.orbmat[1].shape[0]
+    G = torch.zeros((W, na, M), dtype=torch.complex128, device=cuda)
+    ov = torch.zeros(W, dtype=torch.complex128, device=cuda)
+    ph.MixedDensityMatrix(wbuf, G, ov, block=block)
+    Go, ovo = P.phmsd_mixed_density_matrix(t, Su, Sd)
+    assert rel_err(to_host(G), Go) < 1e-10
+    d = to_host(ov) - ovo
+    d = d.real + 1j * ((d.imag + np.pi) % (2 * np.pi) - np.pi)
+    assert np.max(np.abs(d)) < 1e-10
+    v = torch.zeros((W, Nc), dtype=torch.complex128, device=cuda)
+    ph.vbias(G, v, 0.005)
+    H = P.ActiveSpaceHamiltonian(t, Likn[None], hij, 0.0)
+    vo = P.phmsd_vbias(H, Go, 0.005, t.orbmat[0].shape[0])
+    assert rel_err(to_host(v), vo) < 1e-10

@@ -119,3 +119,51 @@ def test_phmsd_energy_woodbury_vs_single_determinants():
     ref = num / den[:, None]
     assert np.allclose(E, ref, rtol=1e-10, atol=1e-10), (E, ref)
     assert np.allclose(np.exp(logov), den, rtol=1e-10)
+
+
+def test_phmsd_density_matrix_vs_single_determinants():
+    """The Woodbury mixed density matrix against sum_k c_k ov_k G_k / sum_k c_k ov_k with G_k the
+    full-space density matrix of determinant k, both mapped to the active orbitals:
+    G_act[a][k] = sum over the trial's active rows, i.e. G_k^full = Phi_k (Phi_k^H S)^-1 ... ."""
+    from safire_b200.synth import make_hamiltonian, make_phmsd_trial
+    M, nup, ndn = 14, 4, 3
+    h1, _ = make_hamiltonian(M, 2, 0.9, seed=5)
+    _, C = np.linalg.eigh(h1)
+    t = make_phmsd_trial(M, nup, ndn, C, nocc=3, nvirt=5, ndet=35, seed=5)
+    rs = np.random.default_rng(9)
+    W = 2
+    S_up = (rs.standard_normal((W, M, nup)) + 1j * rs.standard_normal((W, M, nup))) / 4
+    S_dn = (rs.standard_normal((W, M, ndn)) + 1j * rs.standard_normal((W, M, ndn))) / 4
+    G, logov = P.phmsd_mixed_density_matrix(t, S_up, S_dn)
+    # brute force: full density matrix of each determinant rho_k = S (D^H S)^-1 D^H, weighted
+    occ = []
+    for s in (0, 1):
+        lst = [t.refc[s].copy()]
+        for n in sorted(t.exc[s]):
+            for e in t.exc[s][n]:
+                o = t.refc[s].copy()
+                o[e[:n]] = e[n:]
+                lst.append(o)
+        occ.append(lst)
+    for w in range(W):
+        num = [np.zeros((M, M), complex), np.zeros((M, M), complex)]
+        den = 0j
+        for k in range(t.coef.size):
+            ov, rho = 1.0 + 0j, []
+            for s, S in ((0, S_up[w]), (1, S_dn[w])):
+                D = t.orbmat[s][occ[s][t.det_up[k] if s == 0 else t.det_dn[k]]]  # [N][M] = Phi^H
+                T = D @ S
+                ov *= np.linalg.det(T)
+                rho.append(S @ np.linalg.inv(T) @ D)                        # [M][M]
+            for s in (0, 1):
+                num[s] += t.coef[k] * ov * rho[s]
+            den += t.coef[k] * ov
+        for s in (0, 1):
+            full = (num[s] / den).T                                         # G[i][j] = <c_i^+ c_j>
+            na = t.orbmat[s].shape[0]
+            off = 0 if s == 0 else t.orbmat[0].shape[0]
+            # compact (active-space) form: G_act = C_act^T-rotated rows, as the reference's
+            # csrmm<'T'>(OrbMats, Gtmp) recovers the full one: full = OrbMats^T G_act
+            Gact = G[w, off:off + na]
+            assert np.allclose(t.orbmat[s].T @ Gact, full, atol=1e-10), s
+        assert np.isclose(np.exp(logov[w]), den, rtol=1e-10)
