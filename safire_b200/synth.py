@@ -123,15 +123,20 @@ def make_phmsd_trial(M, nup, ndn, orbitals, nocc=20, nvirt=40, ndet=4096, max_le
             lists[s].setdefault(n, []).append(t)
         return t
 
+    # hole windows per spin (a spin with fewer electrons than nocc uses all of them)
+    oa, ob = min(nocc, nup), min(nocc, ndn)
+    if max_level > min(oa, nvirt) + min(ob, nvirt):
+        raise ValueError(f"make_phmsd_trial: level {max_level} needs more than {oa}+{ob} holes "
+                         f"or {nvirt} particles per spin")
     dets = {(0, 0)}
     order = [(0, 0)]
     while len(order) < ndet:
         L = int(rng.integers(1, max_level + 1))
-        na = int(rng.integers(max(0, L - min(nocc, ndn)), min(L, nocc, nup) + 1))
+        na = int(rng.integers(max(0, L - min(ob, nvirt)), min(L, oa, nvirt) + 1))
         nb = L - na
-        ka = key(0, rng.choice(np.arange(nup - nocc, nup), na, replace=False).tolist(),
+        ka = key(0, rng.choice(np.arange(nup - oa, nup), na, replace=False).tolist(),
                  rng.choice(np.arange(nup, nup + nvirt), na, replace=False).tolist())
-        kb = key(1, rng.choice(np.arange(ndn - nocc, ndn), nb, replace=False).tolist(),
+        kb = key(1, rng.choice(np.arange(ndn - ob, ndn), nb, replace=False).tolist(),
                  rng.choice(np.arange(ndn, ndn + nvirt), nb, replace=False).tolist())
         if (ka, kb) in dets:
             continue
