@@ -242,6 +242,15 @@ void afqmc_prop_params_default(afqmc_prop_params* p);
 int afqmc_prop_create(afqmc_ham ham, const afqmc_prop_params* params, int max_walkers,
                       afqmc_prop* out);
 int afqmc_prop_destroy(afqmc_prop prop);
+/* Runs the propagator's steps with a multi-determinant trial (AFQMCBasePropagator over a
+ * PHMSD wavefunction, Wavefunction.hpp's variant): vbias from afqmc_phmsd_density_matrix and
+ * afqmc_phmsd_vbias, overlaps (step and orthogonalisation) from afqmc_phmsd_log_overlap.  Needs
+ * COLLINEAR walkers, FP64 precision and a trial whose Hamiltonian has been set.  vMF (host [Nc],
+ * may be NULL) replaces the mean field and regenerates P1 (generateP1 with the trial's vMF,
+ * PHMSD.cpp:1329-1572, computed by the caller).  trial NULL detaches.  Synchronous.  The trial
+ * must outlive its use by the propagator. */
+typedef struct afqmc_phmsd_s* afqmc_phmsd;
+int afqmc_prop_set_phmsd(afqmc_prop prop, afqmc_phmsd trial, const afqmc_c128* vMF);
 /* host copies: P1 [nspin][M][M], vMF [Nc] (either may be NULL) */
 int afqmc_prop_get_p1(afqmc_prop prop, afqmc_c128* P1, afqmc_c128* vMF);
 
@@ -329,8 +338,8 @@ int afqmc_ph_excited_1body_energy(const int* iexcit, const int* refc, const afqm
  * active orbital of every electron in the reference; unique excitations u = 1..nuniq_s-1 of each
  * spin (u = 0 is the reference): nex_s[u-1] holes/particles each, their lists concatenated in
  * exc_s as [holes (electron indices), particles (active orbitals)]; determinant k couples unique
- * excitations det_up[k], det_dn[k] with coefficient coef[k].  Every index is validated. */
-typedef struct afqmc_phmsd_s* afqmc_phmsd;
+ * excitations det_up[k], det_dn[k] with coefficient coef[k].  Every index is validated.
+ * (afqmc_phmsd is declared with the propagator above.) */
 int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact_dn,
                        const afqmc_c128* orbmat_up, const afqmc_c128* orbmat_dn,
                        const int* refc_up, const int* refc_dn, int nuniq_up, const int* nex_up,
@@ -344,6 +353,9 @@ int afqmc_phmsd_destroy(afqmc_phmsd trial);
  * S_dn [M][ndn] at the start of each row (the walker-buffer layout). */
 int afqmc_phmsd_log_overlap(afqmc_phmsd trial, const afqmc_c128* wbuf, long ldS,
                             afqmc_c128* ovlp, int W, afqmc_stream stream);
+
+/* dims[6] = {M, nup, ndn, nact_up, nact_dn, Nc (0 before afqmc_phmsd_set_hamiltonian)} */
+int afqmc_phmsd_info(afqmc_phmsd trial, int* dims);
 
 /* The Real3IndexFactorization tensors of a PHMSD trial: Likn [nspin_H2][M][M][Nc] (real) and
  * hij [nspin_H1][M][M] on the host, half-rotated on the device with the active orbitals

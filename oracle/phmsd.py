@@ -342,3 +342,28 @@ def phmsd_vbias(ham, G, dt, nact_up):
     with G [W][nact_up + nact_dn][M] the compact PHMSD density matrix."""
     Gs = (G[:, :nact_up, :], G[:, nact_up:, :])
     return np.sqrt(dt) * sum(np.einsum("nak,wak->wn", ham.Lnak[s], Gs[s]) for s in (0, 1))
+
+
+class PHMSDWavefunction:
+    """The PHMSD wavefunction as AFQMCBasePropagator uses it: vbias (PHMSD.cpp:54-72) from the
+    multi-determinant density matrix and the active-space Lnak, Log_Overlap (804-900), vHS and the
+    one-body propagator from `ham` (a COLLINEAR oracle.afqmc.Real3IndexFactorization), and a given
+    mean field vMF [Nc] (PHMSD::vMF, PHMSD.cpp:1329-1572, is the caller's)."""
+
+    def __init__(self, trial, ham, Likn, hij, vMF):
+        from oracle.afqmc import COLLINEAR
+        self.trial = trial
+        self.ham = ham
+        self.walker_type = COLLINEAR
+        self.H = ActiveSpaceHamiltonian(trial, Likn, hij, ham.E0)
+        self._vMF = np.asarray(vMF, dtype=np.complex128)
+
+    def vbias(self, SA, SB, dt):
+        G, _ = phmsd_mixed_density_matrix(self.trial, SA, SB)
+        return phmsd_vbias(self.H, G, dt, self.trial.orbmat[0].shape[0])
+
+    def Log_Overlap(self, SA, SB):
+        return phmsd_log_overlap(self.trial, SA, SB)[0]
+
+    def vMF(self, dt):
+        return self._vMF.copy()

@@ -332,6 +332,14 @@ class Propagator:
     def set_field_seed(self, seed):
         call("afqmc_prop_set_field_seed", self.handle, int(seed))
 
+    def set_trial(self, trial, vMF=None):
+        """Steps with a PHMSD trial (vbias and overlaps from it); vMF host [Nc] or None keeps
+        the current mean field.  trial None detaches."""
+        v = None if vMF is None else np.ascontiguousarray(vMF, dtype=np.complex128)
+        call("afqmc_prop_set_phmsd", self.handle, None if trial is None else trial.handle,
+             None if v is None else _host_ptr(v))
+        self._trial = trial  # the trial must outlive the propagator's use of it
+
     def Propagate(self, wset: WalkerSet, Eshift, uniforms=None, stream=None):
         """One step.  uniforms: device float64 [W, Nc] or None (device Philox generator)."""
         call("afqmc_prop_step", self.handle, wset.handle, float(Eshift), _ptr(uniforms),
@@ -520,6 +528,12 @@ class PHMSD:
         """ovlp [W] (device) <- log overlap of every walker row of wbuf [W][ldS] (device)."""
         call("afqmc_phmsd_log_overlap", self.handle, _ptr(wbuf), int(wbuf.stride(0)), _ptr(ovlp),
              int(wbuf.shape[0]), _stream(stream))
+
+    def info(self):
+        """(M, nup, ndn, nact_up, nact_dn, Nc)"""
+        d = np.zeros(6, dtype=np.int32)
+        call("afqmc_phmsd_info", self.handle, _host_ptr(d))
+        return tuple(int(x) for x in d)
 
     def MixedDensityMatrix(self, wbuf, G, ovlp, block=0, stream=None):
         """G [W, nact_up + nact_dn, M] (device) and ovlp [W] (device) of every walker row."""

@@ -71,6 +71,8 @@ _SIGS = {
     "afqmc_phmsd_energy": (i32, [vp, vp, i64, vp, vp, i32, i32, vp]),
     "afqmc_phmsd_density_matrix": (i32, [vp, vp, i64, vp, vp, i32, i32, vp]),
     "afqmc_phmsd_vbias": (i32, [vp, vp, vp, i32, C.c_double, vp]),
+    "afqmc_phmsd_info": (i32, [vp, vp]),
+    "afqmc_prop_set_phmsd": (i32, [vp, vp, vp]),
     "afqmc_wset_create": (i32, [i32, i32, i32, i32, i32, C.POINTER(vp)]),
     "afqmc_wset_destroy": (i32, [vp]),
     "afqmc_wset_buffer": (i32, [vp, C.POINTER(vp), C.POINTER(i64), C.POINTER(i32)]),

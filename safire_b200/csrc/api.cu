@@ -145,6 +145,9 @@ struct afqmc_prop_s {
   unsigned long long* counter = nullptr;
   unsigned long long* stats = nullptr;
   unsigned long long seed = 0x5AF1E5EEDull;
+  // multi-determinant trial used in place of the Hamiltonian's single determinant
+  afqmc_phmsd ph = nullptr;
+  c128* Gph = nullptr;       // [maxW][nact_up + nact_dn][M]
   // per-phase CUDA events of the last timed step (AFQMCTimers analogue)
   bool timing = false;
   cudaEvent_t ev[AFQMC_NPHASE + 1] = {};
@@ -155,7 +158,7 @@ struct afqmc_prop_s {
     dfree(P1); dfree(P1r); dfree(vMF);
     dfree(G); dfree(vb); dfree(X); dfree(HW); dfree(mf); dfree(newov); dfree(ovtmp);
     dfree(T); dfree(V); dfree(w1); dfree(w2); dfree(w3); dfree(ortho_work);
-    dfree(Eshift_d); dfree(counter); dfree(stats);
+    dfree(Eshift_d); dfree(counter); dfree(stats); dfree(Gph);
   }
 };
 
@@ -971,27 +974,20 @@ int expm_device(const std::vector<c128>& A, int M, std::vector<c128>& out) {
 
 }  // namespace
 
-extern "C" int afqmc_prop_create(afqmc_ham h, const afqmc_prop_params* params, int max_walkers,
-                                 afqmc_prop* out) {
-  AFQMC_CHECK_ARG(h && params && out && max_walkers > 0, "afqmc_prop_create: bad argument");
-  *out = nullptr;
-  AFQMC_CHECK_ARG(params->dt > 0 && params->taylor_n >= 0, "afqmc_prop_create: bad dt / order");
-  AFQMC_CHECK_ARG(params->precision == AFQMC_PREC_FP64 || params->precision == AFQMC_PREC_MIXED,
-                  "afqmc_prop_create: unknown precision");
-  DeviceGuard g(h->device);
-  std::unique_ptr<afqmc_prop_s> pr(new (std::nothrow) afqmc_prop_s());
-  AFQMC_CHECK_ARG(pr, "afqmc_prop_create: out of host memory");
-  pr->device = h->device;
-  pr->ham = h;
-  pr->p = *params;
-  pr->maxW = max_walkers;
+// vMF (given on the host, or the trial's own), P1 and their device copies: the setup part of
+// AFQMCBasePropagator's constructor and generateP1 (AFQMCBasePropagator.cpp:85-214)
+static int prop_mean_field(afqmc_prop_s* pr, const c128* vMF_host) {
+  afqmc_ham_s* h = pr->ham;
+  const afqmc_prop_params* params = &pr->p;
   const int M = h->M, Nc = h->Nc;
   const long MM = long(M) * M;
   const double dt = params->dt;
-
   // vMF with the imaginary part zeroed (AFQMCBasePropagator.cpp:85-110)
   pr->vMF_h.resize(Nc);
-  AFQMC_TRY(afqmc_wfn_vmf(h, dt, (afqmc_c128*)pr->vMF_h.data()));
+  if (vMF_host)
+    std::copy(vMF_host, vMF_host + Nc, pr->vMF_h.begin());
+  else
+    AFQMC_TRY(afqmc_wfn_vmf(h, dt, (afqmc_c128*)pr->vMF_h.data()));
   double re2 = 0;
   for (auto& v : pr->vMF_h) {
     v.y = 0.0;
@@ -1043,6 +1039,9 @@ extern "C" int afqmc_prop_create(afqmc_ham h, const afqmc_prop_params* params, i
   pr->p1_real = real;
   pr->nspin_P1 = nspin;
   pr->nspin_V = h->walker_type == AFQMC_COLLINEAR ? h->nspin_H2 : 1;
+  dfree(pr->P1);
+  dfree(pr->P1r);
+  dfree(pr->vMF);
   AFQMC_TRY(dalloc(&pr->P1, size_t(nspin) * MM));
   AFQMC_CUDA_TRY(cudaMemcpy(pr->P1, pr->P1_h.data(), sizeof(c128) * nspin * MM,
                             cudaMemcpyHostToDevice));
@@ -1055,6 +1054,27 @@ extern "C" int afqmc_prop_create(afqmc_ham h, const afqmc_prop_params* params, i
   }
   AFQMC_TRY(dalloc(&pr->vMF, size_t(Nc)));
   AFQMC_CUDA_TRY(cudaMemcpy(pr->vMF, pr->vMF_h.data(), sizeof(c128) * Nc, cudaMemcpyHostToDevice));
+  return AFQMC_OK;
+}
+
+extern "C" int afqmc_prop_create(afqmc_ham h, const afqmc_prop_params* params, int max_walkers,
+                                 afqmc_prop* out) {
+  AFQMC_CHECK_ARG(h && params && out && max_walkers > 0, "afqmc_prop_create: bad argument");
+  *out = nullptr;
+  AFQMC_CHECK_ARG(params->dt > 0 && params->taylor_n >= 0, "afqmc_prop_create: bad dt / order");
+  AFQMC_CHECK_ARG(params->precision == AFQMC_PREC_FP64 || params->precision == AFQMC_PREC_MIXED,
+                  "afqmc_prop_create: unknown precision");
+  DeviceGuard g(h->device);
+  std::unique_ptr<afqmc_prop_s> pr(new (std::nothrow) afqmc_prop_s());
+  AFQMC_CHECK_ARG(pr, "afqmc_prop_create: out of host memory");
+  pr->device = h->device;
+  pr->ham = h;
+  pr->p = *params;
+  pr->maxW = max_walkers;
+  const int M = h->M, Nc = h->Nc;
+  const long MM = long(M) * M;
+
+  AFQMC_TRY(prop_mean_field(pr.get(), nullptr));
 
   // step workspace
   const int W = max_walkers;
@@ -1089,6 +1109,34 @@ extern "C" int afqmc_prop_destroy(afqmc_prop prop) {
   return AFQMC_OK;
 }
 
+extern "C" int afqmc_prop_set_phmsd(afqmc_prop pr, afqmc_phmsd trial, const afqmc_c128* vMF) {
+  AFQMC_CHECK_ARG(pr, "afqmc_prop_set_phmsd: null handle");
+  DeviceGuard g(pr->device);
+  if (!trial) {
+    pr->ph = nullptr;
+    dfree(pr->Gph);
+    return vMF ? prop_mean_field(pr, reinterpret_cast<const c128*>(vMF)) : AFQMC_OK;
+  }
+  afqmc_ham_s* h = pr->ham;
+  int d[6];
+  AFQMC_TRY(afqmc_phmsd_info(trial, d));
+  AFQMC_CHECK_ARG(h->walker_type == AFQMC_COLLINEAR,
+                  "afqmc_prop_set_phmsd: a PHMSD trial needs COLLINEAR walkers");
+  AFQMC_CHECK_ARG(d[0] == h->M && d[1] == h->nel[0] && d[2] == h->nel[1],
+                  "afqmc_prop_set_phmsd: trial (M=%d, %d+%d) does not match the Hamiltonian "
+                  "(M=%d, %d+%d)", d[0], d[1], d[2], h->M, h->nel[0], h->nel[1]);
+  AFQMC_CHECK_ARG(d[5] == h->Nc,
+                  "afqmc_prop_set_phmsd: trial Hamiltonian has %d Cholesky vectors, the "
+                  "propagator %d (afqmc_phmsd_set_hamiltonian first)", d[5], h->Nc);
+  AFQMC_CHECK_ARG(pr->p.precision == AFQMC_PREC_FP64,
+                  "afqmc_prop_set_phmsd: PHMSD steps run in FP64");
+  dfree(pr->Gph);
+  AFQMC_TRY(dalloc(&pr->Gph, size_t(pr->maxW) * (d[3] + d[4]) * h->M));
+  if (vMF) AFQMC_TRY(prop_mean_field(pr, reinterpret_cast<const c128*>(vMF)));
+  pr->ph = trial;
+  return AFQMC_OK;
+}
+
 extern "C" int afqmc_prop_get_p1(afqmc_prop pr, afqmc_c128* P1, afqmc_c128* vMF) {
   AFQMC_CHECK_ARG(pr, "afqmc_prop_get_p1: null handle");
   if (P1) std::memcpy(P1, pr->P1_h.data(), sizeof(c128) * pr->P1_h.size());
@@ -1120,10 +1168,22 @@ int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* E
   const bool mixed = pr->p.precision == AFQMC_PREC_MIXED;
   // 1. vbias: G of the walkers (NOMSD::vbias, NOMSD.cpp:39-61); with AFQMC_STEP_G_READY the
   //    previous step left it for these walkers
-  if (!(flags & AFQMC_STEP_G_READY))
-    AFQMC_TRY(wfn_density_matrix(h, ws, s, pr->G, ldG, pr->ovtmp, pr->T));
-  AFQMC_TRY(mark(1));
-  if (mixed) {
+  if (pr->ph) {
+    // PHMSD::vbias (PHMSD.cpp:54-72): the multi-determinant density matrix, then Lnak . G
+    AFQMC_TRY(afqmc_phmsd_density_matrix(pr->ph, (const afqmc_c128*)ws->buf, ws->walker_size,
+                                         (afqmc_c128*)pr->Gph, (afqmc_c128*)pr->ovtmp, W, 0,
+                                         (afqmc_stream)s));
+    AFQMC_TRY(mark(1));
+    AFQMC_TRY(afqmc_phmsd_vbias(pr->ph, (const afqmc_c128*)pr->Gph, (afqmc_c128*)pr->vb, W, dt,
+                                (afqmc_stream)s));
+  } else {
+    if (!(flags & AFQMC_STEP_G_READY))
+      AFQMC_TRY(wfn_density_matrix(h, ws, s, pr->G, ldG, pr->ovtmp, pr->T));
+    AFQMC_TRY(mark(1));
+  }
+  if (pr->ph) {
+    // vbias done above
+  } else if (mixed) {
     EnergyArgs a = energy_args(h, pr->G, ldG);
     if (!h->mixed) AFQMC_TRY(mixed_ham_create(&h->mixed, a, s));
     AFQMC_TRY(vbias_mixed(s, h->mixed, pr->G, ldG, pr->vb, W,
@@ -1162,7 +1222,10 @@ int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* E
   AFQMC_TRY(mark(5));
   // 5. new overlaps; with AFQMC_STEP_KEEP_G also the density matrix of the propagated walkers
   //    for the next step (the same product, LU and log det, plus the inverse and G)
-  if (flags & AFQMC_STEP_KEEP_G)
+  if (pr->ph)
+    AFQMC_TRY(afqmc_phmsd_log_overlap(pr->ph, (const afqmc_c128*)ws->buf, ws->walker_size,
+                                      (afqmc_c128*)pr->newov, W, (afqmc_stream)s));
+  else if (flags & AFQMC_STEP_KEEP_G)
     AFQMC_TRY(wfn_density_matrix(h, ws, s, pr->G, ldG, pr->newov, pr->T));
   else
     AFQMC_TRY(wfn_log_overlap(h, ws, s, pr->newov, pr->T));
@@ -1203,6 +1266,7 @@ extern "C" int afqmc_prop_step_flags(afqmc_prop pr, afqmc_wset ws, const double*
   AFQMC_CHECK_ARG(ws->W <= pr->maxW, "afqmc_prop_step_flags: too many walkers");
   AFQMC_CHECK_ARG((flags & ~(AFQMC_STEP_G_READY | AFQMC_STEP_KEEP_G)) == 0,
                   "afqmc_prop_step_flags: unknown flags %d", flags);
+  AFQMC_CHECK_ARG(!(pr->ph && flags), "afqmc_prop_step_flags: no density reuse with a PHMSD trial");
   DeviceGuard g(pr->device);
   return prop_step(pr, ws, 0.0, Eshift_dev, u, flags, reinterpret_cast<cudaStream_t>(stream));
 }
@@ -1219,7 +1283,11 @@ extern "C" int afqmc_prop_orthogonalize(afqmc_prop pr, afqmc_wset ws, afqmc_stre
     AFQMC_TRY(orthogonalize(s, ws->buf + ws->offS(sp), ws->walker_size, pr->ovtmp, ws->W, h->M,
                             h->nel[sp], pr->ortho_work));
   }
-  AFQMC_TRY(wfn_log_overlap(h, ws, s, pr->newov, pr->T));
+  if (pr->ph)
+    AFQMC_TRY(afqmc_phmsd_log_overlap(pr->ph, (const afqmc_c128*)ws->buf, ws->walker_size,
+                                      (afqmc_c128*)pr->newov, ws->W, (afqmc_stream)s));
+  else
+    AFQMC_TRY(wfn_log_overlap(h, ws, s, pr->newov, pr->T));
   return scatter_property(s, ws->buf, ws->walker_size, ws->prop0 + AFQMC_OVLP, ws->W, pr->newov);
 }
 

@@ -855,6 +855,17 @@ extern "C" int afqmc_phmsd_destroy(afqmc_phmsd h) {
   return AFQMC_OK;
 }
 
+extern "C" int afqmc_phmsd_info(afqmc_phmsd h, int* dims) {
+  AFQMC_CHECK_ARG(h && dims, "afqmc_phmsd_info: null argument");
+  dims[0] = h->M;
+  dims[1] = h->nel[0];
+  dims[2] = h->nel[1];
+  dims[3] = h->nact[0];
+  dims[4] = h->nact[1];
+  dims[5] = h->has_ham ? h->Nc : 0;
+  return AFQMC_OK;
+}
+
 extern "C" int afqmc_phmsd_log_overlap(afqmc_phmsd h, const afqmc_c128* wbuf, long ldS,
                                        afqmc_c128* ovlp, int W, afqmc_stream stream) {
   AFQMC_CHECK_ARG(h && wbuf && ovlp, "afqmc_phmsd_log_overlap: null argument");

@@ -178,3 +178,64 @@ def test_phmsd_density_matrix_and_vbias_vs_oracle(cuda, M, nup, ndn, Nc, nocc, n
     H = P.ActiveSpaceHamiltonian(t, Likn[None], hij, 0.0)
     vo = P.phmsd_vbias(H, Go, 0.005, t.orbmat[0].shape[0])
     assert rel_err(to_host(v), vo) < 1e-10
+
+
+@pytest.mark.parametrize("W,steps", [(6, 4)])
+def test_phmsd_propagation_steps_vs_oracle(cuda, W, steps):
+    """Walker steps with a PHMSD trial attached to the propagator (PHMSD vbias and overlaps,
+    COLLINEAR vHS and propagation, hybrid weight update, orthogonalisation) against the oracle's
+    propagator driving the same PHMSD restatement, with the same field uniforms."""
+    from oracle import afqmc as O
+    from safire_b200 import afqmc as A
+    from safire_b200 import capi
+    from safire_b200.synth import make_hamiltonian, make_phmsd_trial
+    M, nup, ndn, Nc, dt = 24, 5, 4, 40, 0.01
+    h1, Likn = make_hamiltonian(M, Nc, 0.9, seed=7)
+    _, C = np.linalg.eigh(h1)
+    t = make_phmsd_trial(M, nup, ndn, C, nocc=4, nvirt=8, ndet=60, seed=3)
+    hij = h1[None].astype(complex)
+    PsiT = [t.orbmat[0][t.refc[0]], t.orbmat[1][t.refc[1]]]
+    ham = A.HamiltonianOperations(A.COLLINEAR, M, nup, ndn, Likn[None], hij, 0.2, PsiT)
+    oham = O.Real3IndexFactorization(O.COLLINEAR, M, nup, ndn, Likn[None], hij, 0.2, PsiT)
+    vMF = O.NOMSD(oham, PsiT).vMF(dt) * 0.8  # any mean field: both sides take it as given
+    ph = A.PHMSD(t)
+    ph.set_hamiltonian(Likn[None], hij, 0.2)
+    prop = A.Propagator(ham, A.default_params(dt=dt), W)
+    prop.set_trial(ph, vMF)
+    wset = A.WalkerSet(A.COLLINEAR, M, nup, ndn, W)
+    wset.init_from_trial(ham)
+    ov = torch.zeros(W, dtype=torch.complex128, device=cuda)
+    ph.Log_Overlap(wset.buffer, ov)
+    wset.setProperty(capi.OVLP, to_host(ov))
+    torch.cuda.synchronize()
+
+    owfn = P.PHMSDWavefunction(t, oham, Likn[None], hij, vMF)
+    oprop = O.Propagator(owfn, O.PropagatorParams(dt=dt))
+    P1d, vMFd = prop.P1_vMF()
+    assert rel_err(P1d, oprop.P1) < 1e-12 and rel_err(vMFd, oprop.vMF) < 1e-14
+    ows = O.WalkerSet(to_host(wset.SlaterMatrices(0)).copy(), to_host(wset.SlaterMatrices(1)).copy(),
+                      to_host(wset.properties()).copy(), W, O.COLLINEAR)
+    assert np.max(np.abs(ows.props[:, O.OVLP] - owfn.Log_Overlap(ows.SA, ows.SB))) < 1e-10
+    Eshift = -1.3
+    rs = np.random.default_rng(5)
+    for step in range(steps):
+        u = rs.random((W, Nc))
+        prop.Propagate(wset, Eshift, to_dev(u, torch.float64))
+        last = prop.last_step(W)
+        oprop.propagate(ows, Eshift, u)
+        lo = oprop.last
+        assert rel_err(to_host(last.vbias), lo["vbias"]) < 1e-10, step
+        assert rel_err(to_host(last.X), lo["X"]) < 1e-10, step
+        d = to_host(last.new_ovlp) - lo["new_ov"]
+        assert np.max(np.abs(d.real + 1j * ((d.imag + np.pi) % (2 * np.pi) - np.pi))) < 1e-9, step
+        assert rel_err(to_host(wset.SlaterMatrices(0)), ows.SA) < 1e-10, step
+        assert rel_err(to_host(wset.SlaterMatrices(1)), ows.SB) < 1e-10, step
+        props = to_host(wset.properties())
+        assert rel_err(props[:, O.WEIGHT], ows.props[:, O.WEIGHT]) < 1e-10, step
+        if step == 1:
+            prop.Orthogonalize(wset)
+            oprop.orthogonalize(ows)
+            assert rel_err(to_host(wset.SlaterMatrices(1)), ows.SB) < 1e-10
+            d = to_host(wset.properties())[:, O.OVLP] - ows.props[:, O.OVLP]
+            assert np.max(np.abs(d.real + 1j * ((d.imag + np.pi) % (2 * np.pi) - np.pi))) < 1e-9
+    prop.set_trial(None)
