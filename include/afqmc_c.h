@@ -365,14 +365,14 @@ int afqmc_phmsd_set_hamiltonian(afqmc_phmsd trial, const double* Likn, int nspin
 /* PHMSD::energy_alg1 (PHMSD.cpp:376-546), COLLINEAR walkers: E [W][3] (E1, EXX, EJ, device,
  * written) and the log overlap [W] (device, written) of the multi-determinant trial, by the
  * Woodbury evaluation of every excited determinant.  Walkers are processed in blocks of `block`
- * (<= 0: 32); the excitation lists must be ordered by excitation number. */
+ * (<= 0: 64); the excitation lists must be ordered by excitation number. */
 int afqmc_phmsd_energy(afqmc_phmsd trial, const afqmc_c128* wbuf, long ldS, afqmc_c128* E,
                        afqmc_c128* ovlp, int W, int block, afqmc_stream stream);
 /* PHMSD::MixedDensityMatrix, compact COLLINEAR (PHMSD.cpp:684-795): G [W][nact_up +
  * nact_dn][M] (device, written) = (R_s^T G_s^ref) / Ov per spin block, with R the coefficient-
  * weighted Woodbury matrices of every excited determinant (calculate_R,
  * phmsd_helpers.hpp:200-309); ovlp [W] (device, written) the log overlap.  Blocks of `block`
- * walkers (<= 0: 32). */
+ * walkers (<= 0: 512). */
 int afqmc_phmsd_density_matrix(afqmc_phmsd trial, const afqmc_c128* wbuf, long ldS,
                                afqmc_c128* G, afqmc_c128* ovlp, int W, int block,
                                afqmc_stream stream);

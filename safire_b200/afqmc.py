@@ -122,9 +122,12 @@ class HamiltonianOperations:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h and capi._lib is not None:
-            capi._lib.afqmc_ham_destroy(h)
-            self.handle = None
+        try:
+            if h and capi._lib is not None:
+                capi._lib.afqmc_ham_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is gone
+            pass
+        self.handle = None
 
     def number_of_cholesky_vectors(self):
         return self.Nc
@@ -208,9 +211,12 @@ class WalkerSet:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h and capi._lib is not None:
-            capi._lib.afqmc_wset_destroy(h)
-            self.handle = None
+        try:
+            if h and capi._lib is not None:
+                capi._lib.afqmc_wset_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is gone
+            pass
+        self.handle = None
 
     def size(self):
         return self.W
@@ -297,6 +303,45 @@ class NOMSD:
         return v
 
 
+class PHMSDWavefunction:
+    """The walker-set facade of a PHMSD trial (Wavefunction.hpp's variant over PHMSD.hpp): the
+    same calls as NOMSD, evaluated by the multi-determinant kernels.  FP64 only."""
+
+    def __init__(self, trial: "PHMSD", block=0):
+        self.ph = trial
+        self.block = block
+        self.M, self.nup, self.ndn, na_up, na_dn, self.Nc = trial.info()
+        self.nact = na_up + na_dn
+
+    def MixedDensityMatrix(self, wset: WalkerSet, G=None, ovlp=None, stream=None):
+        dev = wset.buffer.device
+        G = G if G is not None else torch.empty((wset.W, self.nact, self.M),
+                                                dtype=torch.complex128, device=dev)
+        ovlp = ovlp if ovlp is not None else torch.empty(wset.W, dtype=torch.complex128,
+                                                         device=dev)
+        self.ph.MixedDensityMatrix(wset.buffer, G, ovlp, self.block, stream)
+        return G, ovlp
+
+    def Log_Overlap(self, wset: WalkerSet, ovlp=None, stream=None):
+        ovlp = ovlp if ovlp is not None else torch.empty(wset.W, dtype=torch.complex128,
+                                                         device=wset.buffer.device)
+        self.ph.Log_Overlap(wset.buffer, ovlp, stream)
+        return ovlp
+
+    def Energy(self, wset: WalkerSet, set_properties=True, precision=PREC_FP64, stream=None):
+        if precision != PREC_FP64:
+            raise ValueError("PHMSD energies run in FP64")
+        dev = wset.buffer.device
+        E = torch.empty((wset.W, 3), dtype=torch.complex128, device=dev)
+        ov = torch.empty(wset.W, dtype=torch.complex128, device=dev)
+        self.ph.Energy(wset.buffer, E, ov, self.block, stream)
+        if set_properties:  # PHMSD::Energy(wset) (PHMSD.cpp:75-87)
+            p = wset.properties()
+            p[:, capi.OVLP] = ov
+            p[:, capi.E1], p[:, capi.EXX], p[:, capi.EJ] = E[:, 0], E[:, 1], E[:, 2]
+        return E, ov
+
+
 # --------------------------------------------------------------------------------------------
 # Propagator
 # --------------------------------------------------------------------------------------------
@@ -318,9 +363,12 @@ class Propagator:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h and capi._lib is not None:
-            capi._lib.afqmc_prop_destroy(h)
-            self.handle = None
+        try:
+            if h and capi._lib is not None:
+                capi._lib.afqmc_prop_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is gone
+            pass
+        self.handle = None
 
     def P1_vMF(self):
         nspin = 2 if self.ham.walker_type == COLLINEAR else 1
@@ -399,9 +447,12 @@ class HostRandomGenerator:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h and capi._lib is not None:
-            capi._lib.afqmc_host_rng_destroy(h)
-            self.handle = None
+        try:
+            if h and capi._lib is not None:
+                capi._lib.afqmc_host_rng_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is gone
+            pass
+        self.handle = None
 
     def sample_uniform(self, n):
         out = np.empty(n, dtype=np.float64)
@@ -508,9 +559,12 @@ class PHMSD:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h and capi._lib is not None:
-            capi._lib.afqmc_phmsd_destroy(h)
-            self.handle = None
+        try:
+            if h and capi._lib is not None:
+                capi._lib.afqmc_phmsd_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is gone
+            pass
+        self.handle = None
 
     def set_hamiltonian(self, Likn, hij, E0):
         """Likn real [nspin_H2, M, M, Nc], hij complex [nspin_H1, M, M] (host)."""

@@ -341,25 +341,16 @@ __global__ void __launch_bounds__(PH_THREADS) ph_reference_kernel(
   }
 }
 
-// get_compact_ph_R_matrices (phmsd_helpers.hpp:311-398): R[w][d][p][:] from the inverse Q of the
-// excitation block QQ0[particles][holes]; orbs = the determinant's occupied active orbitals:
-//   R[p][orbs_i] -= Q[p][q] QQ0[part_q][i]  (all electrons i),  R[p][orbs(hole_q)] += Q[p][q]
-// R must be zero on entry; a singular block leaves its rows zero (as the reference).
-__global__ void compact_R_kernel(const c128* __restrict__ QQ0, const int* __restrict__ iexcit,
-                                 const int* __restrict__ refc, int ndet, int nex, int W, int nact,
-                                 int nel, c128* __restrict__ R) {
-  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= long(W) * ndet) return;
-  const int w = int(t / ndet), d = int(t - long(w) * ndet);
-  const int* e = iexcit + size_t(d) * 2 * nex;
-  const c128* Q0 = QQ0 + size_t(w) * nact * nel;
-  c128 a[PH_NEX_MAX][PH_NEX_MAX], inv[PH_NEX_MAX][PH_NEX_MAX];
+// Inverse of the excitation block a[p][q] = QQ0[particle_p][hole_q] (nex x nex, e = holes then
+// particles) by Gauss-Jordan with partial pivoting; false for a singular block.
+__device__ bool woodbury_block_inverse(const c128* __restrict__ Q0, const int* __restrict__ e,
+                                       int nex, int nel, c128 (&inv)[PH_NEX_MAX][PH_NEX_MAX]) {
+  c128 a[PH_NEX_MAX][PH_NEX_MAX];
   for (int p = 0; p < nex; ++p)
     for (int q = 0; q < nex; ++q) {
       a[p][q] = Q0[size_t(e[nex + p]) * nel + e[q]];
       inv[p][q] = cmk(p == q ? 1.0 : 0.0, 0.0);
     }
-  // Gauss-Jordan with partial pivoting on [a | I]
   for (int k = 0; k < nex; ++k) {
     int piv = k;
     double best = cabs1(a[k][k]);
@@ -368,7 +359,7 @@ __global__ void compact_R_kernel(const c128* __restrict__ QQ0, const int* __rest
         best = cabs1(a[i][k]);
         piv = i;
       }
-    if (!(best > 0.0)) return;  // singular block: this determinant's R stays zero
+    if (!(best > 0.0)) return false;
     if (piv != k)
       for (int j = 0; j < nex; ++j) {
         c128 x = a[k][j]; a[k][j] = a[piv][j]; a[piv][j] = x;
@@ -388,6 +379,24 @@ __global__ void compact_R_kernel(const c128* __restrict__ QQ0, const int* __rest
         }
       }
   }
+  return true;
+}
+
+// get_compact_ph_R_matrices (phmsd_helpers.hpp:311-398): R[w][d][p][:] from the inverse Q of the
+// excitation block QQ0[particles][holes]; orbs = the determinant's occupied active orbitals:
+//   R[p][orbs_i] -= Q[p][q] QQ0[part_q][i]  (all electrons i),  R[p][orbs(hole_q)] += Q[p][q]
+// R must be zero on entry; a singular block leaves its rows zero (as the reference).
+__global__ void compact_R_kernel(const c128* __restrict__ QQ0, const int* __restrict__ iexcit,
+                                 const int* __restrict__ refc, int ndet, int nex, int W, int nact,
+                                 int nel, c128* __restrict__ R) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(W) * ndet) return;
+  const int w = int(t / ndet), d = int(t - long(w) * ndet);
+  const int* e = iexcit + size_t(d) * 2 * nex;
+  const c128* Q0 = QQ0 + size_t(w) * nact * nel;
+  c128 inv[PH_NEX_MAX][PH_NEX_MAX];
+  // a singular block leaves this determinant's R zero (as the reference)
+  if (!woodbury_block_inverse(Q0, e, nex, nel, inv)) return;
   c128* Rw = R + (size_t(w) * ndet + d) * nex * nact;
   for (int p = 0; p < nex; ++p) {
     c128* Rp = Rw + size_t(p) * nact;
@@ -402,6 +411,219 @@ __global__ void compact_R_kernel(const c128* __restrict__ QQ0, const int* __rest
       }
       int oh = e[nex + q];  // orbital of hole q's electron in this determinant
       Rp[oh] = cadd(Rp[oh], ipq);
+    }
+  }
+}
+
+// INV[w][uinv[u] ...] = inverse of the excitation block of every unique excitation u >= 1
+// (row-major nex x nex), zeros for a singular block: the Q matrices of the Woodbury R.
+__global__ void woodbury_inverses_kernel(const c128* __restrict__ QQ0, const int* __restrict__ uoff,
+                                         const int* __restrict__ unex,
+                                         const int* __restrict__ uexc,
+                                         const int* __restrict__ uinv, int nuniq, int W, int nact,
+                                         int nel, int ninv, c128* __restrict__ INV) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(nuniq - 1) * W) return;
+  const int w = int(t / (nuniq - 1)), u = 1 + int(t - long(w) * (nuniq - 1));
+  const int nex = unex[u];
+  c128 inv[PH_NEX_MAX][PH_NEX_MAX];
+  const bool ok = woodbury_block_inverse(QQ0 + size_t(w) * nact * nel, uexc + uoff[u], nex, nel,
+                                         inv);
+  c128* o = INV + size_t(w) * ninv + uinv[u];
+  for (int p = 0; p < nex; ++p)
+    for (int q = 0; q < nex; ++q) o[p * nex + q] = ok ? inv[p][q] : cmk(0.0, 0.0);
+}
+
+// The 2-body energy terms of one excited determinant at one Cholesky index n, from per-walker
+// tables instead of its R rows.  With t_j = T[j][n][:] (rows of the half-rotated Twina), the
+// determinant's holes h, particles p, reference orbitals r = refc[h], Q = INV (the inverse of
+// QQ0[p][h]) and the compact R_b[x] = sum_q Q[b][q] (delta(x, p_q) - sum_i delta(x, occ_i)
+// QQ0[p_q][i]):
+//   F[a][b] = t_{h_a} . R_b = sum_q Q[b][q] (t_{h_a}[p_q] - Y[h_a][p_q]
+//                                           - sum_e (t_{h_a}[p_e] - t_{h_a}[r_e]) QQ0[p_q][h_e])
+//   D[a]    = U[h_a] . R_a   (the same with U and Z in place of t and Y)
+// where U[h][x] = sum_j t_h[r_j] t_j[x], Y[h][x] = sum_i t_h[r_i] QQ0[x][i], Z = (t[:, r]) Y.
+// ex and kn are then the terms of ph_excited_2body_energy_dense_cholesky
+// (detail/phmsd_impl.hpp:33-153) summed in closed form: every sum over electrons reduces to the
+// tables U and f0 = sum_i t_i[r_i] plus corrections over the nex holes.
+template <int NEX>
+__device__ __forceinline__ void excited_terms(const int* __restrict__ e, const c128* __restrict__ Qi,
+                                              const c128* Tn, const c128* Yn, const c128* Un,
+                                              const c128* Zn, const c128* Q0t,
+                                              const int* refs, int nact, c128 f0, c128& ex_out,
+                                              c128& kn_out) {
+  int h[NEX], p[NEX], r[NEX];
+#pragma unroll
+  for (int a = 0; a < NEX; ++a) {
+    h[a] = e[a];
+    p[a] = e[NEX + a];
+    r[a] = refs[h[a]];
+  }
+  c128 F[NEX][NEX], D[NEX];
+#pragma unroll
+  for (int a = 0; a < NEX; ++a) {
+    const c128* ta = Tn + h[a] * nact;
+    const c128* ua = Un + h[a] * nact;
+    c128 dt[NEX], du[NEX];
+#pragma unroll
+    for (int x = 0; x < NEX; ++x) {
+      dt[x] = csub(ta[p[x]], ta[r[x]]);
+      du[x] = csub(ua[p[x]], ua[r[x]]);
+    }
+    c128 g[NEX], gu[NEX];
+#pragma unroll
+    for (int q = 0; q < NEX; ++q) {
+      c128 ct = cmk(0, 0), cu = cmk(0, 0);
+#pragma unroll
+      for (int x = 0; x < NEX; ++x) {
+        const c128 qv = Q0t[h[x] * nact + p[q]];  // QQ0[p_q][h_x]
+        ct = cadd(ct, cmul(dt[x], qv));
+        cu = cadd(cu, cmul(du[x], qv));
+      }
+      g[q] = csub(csub(ta[p[q]], Yn[h[a] * nact + p[q]]), ct);
+      gu[q] = csub(csub(ua[p[q]], Zn[h[a] * nact + p[q]]), cu);
+    }
+#pragma unroll
+    for (int b = 0; b < NEX; ++b) {
+      c128 f = cmk(0, 0);
+#pragma unroll
+      for (int q = 0; q < NEX; ++q) f = cadd(f, cmul(Qi[b * NEX + q], g[q]));
+      F[a][b] = f;
+    }
+    c128 dd = cmk(0, 0);
+#pragma unroll
+    for (int q = 0; q < NEX; ++q) dd = cadd(dd, cmul(Qi[a * NEX + q], gu[q]));
+    D[a] = dd;
+  }
+  c128 ex = cmk(0, 0), kn = f0;
+#pragma unroll
+  for (int a = 0; a < NEX; ++a) {
+    const c128* ta = Tn + h[a] * nact;
+    const c128* ua = Un + h[a] * nact;
+    const c128 tpa = ta[p[a]], tra = ta[r[a]];
+    kn = cadd(kn, cadd(F[a][a], csub(tpa, tra)));
+    // f_a^2 and the changed electron's own diagonal term
+    ex = cadd(ex, cmul(F[a][a], F[a][a]));
+    ex = cadd(ex, csub(cmul(tpa, tpa), cmul(tra, tra)));
+    // B_a = sum_j t_{h_a}[occ_j] F(j, a);  C_a = sum over unchanged j of the pair term (i = h_a)
+    c128 B = D[a];
+    c128 C = csub(ua[p[a]], ua[r[a]]);
+#pragma unroll
+    for (int x = 0; x < NEX; ++x) {
+      const c128* tx = Tn + h[x] * nact;
+      B = cadd(B, cmul(csub(ta[p[x]], ta[r[x]]), F[x][a]));
+      C = csub(C, cmul(ta[r[x]], csub(tx[p[a]], tx[r[a]])));
+      if (x != a) ex = cadd(ex, csub(cmul(ta[p[x]], tx[p[a]]), cmul(ta[r[x]], tx[r[a]])));
+      if (x > a) ex = cadd(ex, cscale(cmul(F[x][a], F[a][x]), 2.0));
+    }
+    ex = cadd(ex, cscale(cadd(B, C), 2.0));
+  }
+  ex_out = ex;
+  kn_out = kn;
+}
+
+// nex > 4 is rare: out of line, so that its larger frame stays out of the common path
+template <int NEX>
+__device__ __noinline__ void excited_terms_rare(const int* e, const c128* Qi, const c128* Tn,
+                                                const c128* Yn, const c128* Un, const c128* Zn,
+                                                const c128* Q0t, const int* refs, int nact,
+                                                c128 f0, c128& ex, c128& kn) {
+  excited_terms<NEX>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn);
+}
+
+// Excited-determinant 2-body energies of one spin for walker blockIdx.y at Cholesky index
+// blockIdx.x, all unique excitations in one launch (the work of ph_excited_energies_first_step /
+// second_step, phmsd_helpers.hpp:401-527, for every shell): the per-(walker, n) tables T, U, Y, Z
+// in shared memory, then one thread per excited determinant.  EXacc[w] -= wgt ex / 2,
+// EJacc[w] += wgt (kn^2 - f0^2) / 2; KE[u][w][n] = kn, or with `cross` E[w].EJ += cross . kn.
+constexpr int PHX_THREADS = 256;
+__global__ void __launch_bounds__(PHX_THREADS, 1) excited_energy_tables_kernel(
+    const c128* __restrict__ Twina, const c128* __restrict__ QQ0, const int* __restrict__ refc,
+    const int* __restrict__ uoff, const int* __restrict__ unex, const int* __restrict__ uexc,
+    const int* __restrict__ uinv, const c128* __restrict__ INV, int ninv,
+    const c128* __restrict__ wgt, int nuniq, int W, int nel, int nact, int nchol,
+    c128* __restrict__ EXacc, c128* __restrict__ EJacc, c128* __restrict__ KE,
+    const c128* __restrict__ cross, c128* __restrict__ E) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int NA = nel * nact;
+  c128* Tn = reinterpret_cast<c128*>(smem_raw);  // [nel][nact]
+  c128* Un = Tn + NA;                             // [nel][nact]
+  c128* Yn = Un + NA;                             // [nel][nact]
+  c128* Zn = Yn + NA;                             // [nel][nact]
+  c128* Q0t = Zn + NA;                            // [nel][nact]: QQ0 transposed
+  int* refs = reinterpret_cast<int*>(Q0t + NA);   // [nel]
+  __shared__ double red[PHX_THREADS / 32 * 6];
+  const int n = blockIdx.x, w = blockIdx.y;
+  const c128* Tw = Twina + size_t(w) * nel * nchol * nact;
+  const c128* Qw = QQ0 + size_t(w) * nact * nel;
+  for (int k = threadIdx.x; k < NA; k += blockDim.x) {
+    const int j = k / nact, x = k - j * nact;
+    Tn[k] = Tw[(size_t(j) * nchol + n) * nact + x];
+    Q0t[k] = Qw[size_t(x) * nel + j];
+  }
+  for (int i = threadIdx.x; i < nel; i += blockDim.x) refs[i] = refc[i];
+  __syncthreads();
+  // U = t[:, r] t,  Y = t[:, r] QQ0^T
+  for (int k = threadIdx.x; k < NA; k += blockDim.x) {
+    const int hh = k / nact, x = k - hh * nact;
+    const c128* th = Tn + hh * nact;
+    c128 u = cmk(0, 0), y = cmk(0, 0);
+    for (int j = 0; j < nel; ++j) {
+      const c128 tr = th[refs[j]];
+      u = cadd(u, cmul(tr, Tn[j * nact + x]));
+      y = cadd(y, cmul(tr, Q0t[j * nact + x]));
+    }
+    Un[k] = u;
+    Yn[k] = y;
+  }
+  __syncthreads();
+  // Z = t[:, r] Y
+  for (int k = threadIdx.x; k < NA; k += blockDim.x) {
+    const int hh = k / nact, x = k - hh * nact;
+    const c128* th = Tn + hh * nact;
+    c128 z = cmk(0, 0);
+    for (int j = 0; j < nel; ++j) z = cadd(z, cmul(th[refs[j]], Yn[j * nact + x]));
+    Zn[k] = z;
+  }
+  c128 f0 = cmk(0, 0);
+  for (int i = 0; i < nel; ++i) f0 = cadd(f0, Tn[i * nact + refs[i]]);
+  const c128 f00 = cmul(f0, f0);
+  __syncthreads();
+  c128 exs = cmk(0, 0), ejs = cmk(0, 0), ejc = cmk(0, 0);
+  const c128* Iw = INV + size_t(w) * ninv;
+  for (int u = 1 + threadIdx.x; u < nuniq; u += blockDim.x) {
+    const int nex = unex[u];
+    const int* e = uexc + uoff[u];
+    const c128* Qi = Iw + uinv[u];
+    c128 ex, kn;
+    switch (nex) {
+      case 1: excited_terms<1>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
+      case 2: excited_terms<2>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
+      case 3: excited_terms<3>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
+      case 4: excited_terms<4>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
+      case 5: excited_terms_rare<5>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
+      case 6: excited_terms_rare<6>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
+      case 7: excited_terms_rare<7>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
+      default: excited_terms_rare<8>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
+    }
+    const c128 wu = wgt[size_t(u) * W + w];
+    exs = cadd(exs, cmul(wu, ex));
+    ejs = cadd(ejs, cmul(wu, csub(cmul(kn, kn), f00)));
+    const size_t o = (size_t(u) * W + w) * nchol + n;
+    if (cross)
+      ejc = cadd(ejc, cmul(cross[o], kn));
+    else
+      KE[o] = kn;
+  }
+  block_sum3(exs, ejs, ejc, red);
+  if (threadIdx.x == 0) {
+    atomicAdd(&EXacc[w].x, -0.5 * exs.x);
+    atomicAdd(&EXacc[w].y, -0.5 * exs.y);
+    atomicAdd(&EJacc[w].x, 0.5 * ejs.x);
+    atomicAdd(&EJacc[w].y, 0.5 * ejs.y);
+    if (cross) {
+      atomicAdd(&E[w * 3 + 2].x, ejc.x);
+      atomicAdd(&E[w * 3 + 2].y, ejc.y);
     }
   }
 }
@@ -468,51 +690,86 @@ __global__ void finish_energy_kernel(const c128* __restrict__ Ov, const c128* __
   ovlp[w] = cadd(clog(Ov[w]), logov[w]);
 }
 
-// R[w][i][refc_i] += sum_u wgt[u][w]  (the identity part of every determinant's R on its
-// reference rows; the excited rows are corrected in accumulate_R_kernel)
-__global__ void __launch_bounds__(PH_THREADS) r_identity_kernel(const c128* __restrict__ wgt,
-                                                               int nu, int W,
-                                                               const int* __restrict__ refc,
-                                                               int nel, int nact,
-                                                               c128* __restrict__ R) {
-  __shared__ double red[PH_THREADS / 32 * 6];
-  __shared__ c128 tot;
+// The full R of calculate_R (phmsd_helpers.hpp:200-309) for walker blockIdx.x, all unique
+// excitations at once, accumulated in shared memory.  Determinant u (weight wu, holes h, particles
+// p, reference orbitals r, Q = INV) adds to row h_a, with c[q] = wu Q[a][q]:
+//   + c[q] at p_q,  + wu at p_a,  - wu at r_a            (its compact R row and the identity shift)
+//   - sum_q c[q] QQ0[p_q][i] at occ_i for every electron i
+// The last term is summed as A QQ0 (A[h][b] = sum of c over (u, a, q) with h_a = h, p_q = b) onto
+// the reference orbitals r_i, and the hole electrons' share is moved from r_{h_e} to p_e per
+// determinant.  Every electron row also gets sum_u wu at r_i (the identity of every determinant).
+// Shared-memory atomics order the sums differently from run to run (the reference reduces R with
+// atomics too).
+constexpr int PHR_THREADS = 256;
+__global__ void __launch_bounds__(PHR_THREADS) phmsd_R_kernel(
+    const c128* __restrict__ QQ0, const int* __restrict__ refc, const int* __restrict__ uoff,
+    const int* __restrict__ unex, const int* __restrict__ uexc, const int* __restrict__ uinv,
+    const c128* __restrict__ INV, int ninv, const c128* __restrict__ wgt, int nuniq, int W,
+    int nel, int nact, c128* __restrict__ R) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int NA = nel * nact;
+  c128* Rs = reinterpret_cast<c128*>(smem_raw);  // [nel][nact]
+  c128* As = Rs + NA;                             // [nel][nact]
+  c128* Qs = As + NA;                             // [nact][nel]
+  __shared__ double red[PHR_THREADS / 32 * 6];
+  __shared__ c128 wsum;
   const int w = blockIdx.x;
-  c128 s = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0);
-  for (int u = threadIdx.x; u < nu; u += blockDim.x) s = cadd(s, wgt[size_t(u) * W + w]);
-  block_sum3(s, z1, z2, red);
-  if (threadIdx.x == 0) tot = s;
+  const c128* Qw = QQ0 + size_t(w) * nact * nel;
+  for (int k = threadIdx.x; k < NA; k += blockDim.x) {
+    Rs[k] = cmk(0, 0);
+    As[k] = cmk(0, 0);
+    Qs[k] = Qw[k];
+  }
+  c128 ws = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0);
+  for (int u = threadIdx.x; u < nuniq; u += blockDim.x) ws = cadd(ws, wgt[size_t(u) * W + w]);
+  block_sum3(ws, z1, z2, red);
+  if (threadIdx.x == 0) wsum = ws;
   __syncthreads();
-  for (int i = threadIdx.x; i < nel; i += blockDim.x) {
-    c128* r = R + (size_t(w) * nel + i) * nact + refc[i];
-    *r = cadd(*r, tot);
-  }
-}
-
-// One excitation shell's contribution to the full R (calculate_R, phmsd_helpers.hpp:225-262):
-// for electron i and every (determinant d, row p) of the shell where i is hole p,
-//   R[w][i][:] += wgt_d Rc[w][d][p][:],  R[w][i][particle_p] += wgt_d,  R[w][i][refc_i] -= wgt_d
-// (Rc: the compact R of the shell).  One CTA per (walker, electron): no atomics.
-__global__ void accumulate_R_kernel(const c128* __restrict__ Rc, const c128* __restrict__ wgt,
-                                    const int* __restrict__ eptr, const int* __restrict__ eidx,
-                                    const int* __restrict__ iexcit, const int* __restrict__ refc,
-                                    int nd, int nex, int W, int nel, int nact,
-                                    c128* __restrict__ R) {
-  const int w = blockIdx.x, i = blockIdx.y;
-  const int j0 = eptr[i], j1 = eptr[i + 1];
-  if (j0 == j1) return;
-  c128* Ri = R + (size_t(w) * nel + i) * nact;
-  for (int a = threadIdx.x; a < nact; a += blockDim.x) {
-    c128 acc = cmk(0, 0);
-    for (int j = j0; j < j1; ++j) {
-      const int dp = eidx[j], d = dp / nex, p = dp - d * nex;
-      const c128 wd = wgt[size_t(d) * W + w];
-      acc = cadd(acc, cmul(wd, Rc[((size_t(w) * nd + d) * nex + p) * nact + a]));
-      if (iexcit[size_t(d) * 2 * nex + nex + p] == a) acc = cadd(acc, wd);
-      if (refc[i] == a) acc = csub(acc, wd);
+  auto add = [](c128* x, c128 v) {
+    atomicAdd(&x->x, v.x);
+    atomicAdd(&x->y, v.y);
+  };
+  const c128* Iw = INV + size_t(w) * ninv;
+  for (int u = 1 + threadIdx.x; u < nuniq; u += blockDim.x) {
+    const c128 wu = wgt[size_t(u) * W + w];
+    if (wu.x == 0.0 && wu.y == 0.0) continue;
+    const int nex = unex[u];
+    const int* e = uexc + uoff[u];
+    const c128* Qi = Iw + uinv[u];
+    for (int a = 0; a < nex; ++a) {
+      const int ha = e[a], pa = e[nex + a];
+      c128* Ra = Rs + ha * nact;
+      c128* Aa = As + ha * nact;
+      add(Ra + pa, wu);
+      add(Ra + refc[ha], cmk(-wu.x, -wu.y));
+      for (int q = 0; q < nex; ++q) {
+        const c128 c = cmul(wu, Qi[a * nex + q]);
+        add(Ra + e[nex + q], c);
+        add(Aa + e[nex + q], c);
+      }
+      for (int x = 0; x < nex; ++x) {
+        const int hx = e[x];
+        c128 sx = cmk(0, 0);
+        for (int q = 0; q < nex; ++q)
+          sx = cadd(sx, cmul(cmul(wu, Qi[a * nex + q]), Qs[e[nex + q] * nel + hx]));
+        add(Ra + refc[hx], sx);
+        add(Ra + e[nex + x], cmk(-sx.x, -sx.y));
+      }
     }
-    Ri[a] = cadd(Ri[a], acc);
   }
+  __syncthreads();
+  // R[h][r_i] += delta(h, i) sum_u wu - (A QQ0)[h][i]  (each (h, r_i) once: refc is one-to-one)
+  for (int k = threadIdx.x; k < nel * nel; k += blockDim.x) {
+    const int hh = k / nel, i = k - hh * nel;
+    const c128* Ah = As + hh * nact;
+    c128 v = hh == i ? wsum : cmk(0, 0);
+    for (int b = 0; b < nact; ++b) v = csub(v, cmul(Ah[b], Qs[b * nel + i]));
+    c128* t = Rs + hh * nact + refc[i];
+    *t = cadd(*t, v);
+  }
+  __syncthreads();
+  c128* Rw = R + size_t(w) * NA;
+  for (int k = threadIdx.x; k < NA; k += blockDim.x) Rw[k] = Rs[k];
 }
 
 // x[w][...] *= 1 / Ov[w]
@@ -637,12 +894,11 @@ struct afqmc_phmsd_s {
   // excitation shells (equal nex, contiguous unique indices): first index, count, nex
   std::vector<int> sh_k0[2], sh_nd[2], sh_nex[2];
   std::vector<int> uoff_h[2];
-  // per shell: for every electron, the (determinant, row) pairs where it is a hole
-  std::vector<int> sh_eoff[2];  // offset of the shell's eptr block ([nel+1]) in eptr
-  std::vector<int> sh_ioff[2];  // offset of the shell's entries in eidx
-  int* eptr[2] = {nullptr, nullptr};
-  int* eidx[2] = {nullptr, nullptr};
   c128* Rfull = nullptr;
+  // offset of every unique excitation's inverse block (nex^2 entries) and the total per walker
+  int* uinv[2] = {nullptr, nullptr};
+  int ninv[2] = {0, 0};
+  c128* INV = nullptr;
   // energy: the Hamiltonian half-rotated with the active orbitals
   bool has_ham = false;
   int Nc = 0;
@@ -656,14 +912,23 @@ struct afqmc_phmsd_s {
   c128 *wgt = nullptr, *Swia = nullptr, *Twina = nullptr, *KEr = nullptr, *KEd = nullptr;
   c128 *KEl = nullptr, *Kdn = nullptr, *R = nullptr, *el = nullptr;
   size_t R_elems = 0, KEl_elems = 0;
+  int capCore = 0;  // walkers the Woodbury factors / density-matrix buffers hold
   void free_energy_scratch() {
-    for (c128** q : {&eG[0], &eG[1], &eQ[0], &eQ[1], &eov[0], &eov[1], &eTMN, &eTNN, &elogov,
-                     &eOv, &wgt, &Swia, &Twina, &KEr, &KEd, &KEl, &Kdn, &R, &el, &Rfull})
+    for (c128** q : {&Swia, &Twina, &KEr, &KEd, &KEl, &Kdn, &R, &el})
       if (*q) {
         cudaFree(*q);
         *q = nullptr;
       }
     capWb = 0;
+  }
+  void free_core_scratch() {
+    for (c128** q : {&eG[0], &eG[1], &eQ[0], &eQ[1], &eov[0], &eov[1], &eTMN, &eTNN, &elogov,
+                     &eOv, &wgt, &Rfull, &INV})
+      if (*q) {
+        cudaFree(*q);
+        *q = nullptr;
+      }
+    capCore = 0;
   }
   void free_scratch() {
     for (c128** p : {&TMN, &TNN, &QQ0, &ov[0], &ov[1], &logov})
@@ -676,11 +941,11 @@ struct afqmc_phmsd_s {
   ~afqmc_phmsd_s() {
     free_scratch();
     free_energy_scratch();
+    free_core_scratch();
     for (int s = 0; s < 2; ++s) {
       cudaFree(rowptr[s]);
       cudaFree(kidx[s]);
-      cudaFree(eptr[s]);
-      cudaFree(eidx[s]);
+      cudaFree(uinv[s]);
       cudaFree(lnak[s]);
       cudaFree(haj[s]);
       cudaFree(orbmat[s]);
@@ -820,25 +1085,12 @@ extern "C" int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact
       ++h->sh_nd[s].back();
     }
     h->uoff_h[s] = off[s];
-    // electron -> (determinant, row) lists of every shell
-    std::vector<int> ep, ei;
-    for (size_t j = 0; j < h->sh_k0[s].size(); ++j) {
-      const int k0 = h->sh_k0[s][j], nd = h->sh_nd[s][j], n = h->sh_nex[s][j];
-      std::vector<std::vector<int>> lists(nel[s]);
-      for (int d = 0; d < nd; ++d)
-        for (int p = 0; p < n; ++p) lists[excs[s][off[s][k0 + d] + p]].push_back(d * n + p);
-      h->sh_eoff[s].push_back(int(ep.size()));
-      h->sh_ioff[s].push_back(int(ei.size()));
-      int cnt = 0;
-      ep.push_back(0);
-      for (int i = 0; i < nel[s]; ++i) {
-        for (int x : lists[i]) ei.push_back(x);
-        cnt += int(lists[i].size());
-        ep.push_back(cnt);
-      }
+    std::vector<int> io(nuniq[s], 0);
+    for (int u = 1; u < nuniq[s]; ++u) {
+      io[u] = h->ninv[s];
+      h->ninv[s] += nex[s][u] * nex[s][u];
     }
-    AFQMC_TRY(to_device(&h->eptr[s], ep.data(), ep.size()));
-    AFQMC_TRY(to_device(&h->eidx[s], ei.data(), ei.size()));
+    AFQMC_TRY(to_device(&h->uinv[s], io.data(), io.size()));
   }
   *out = h.release();
   return AFQMC_OK;
@@ -989,12 +1241,46 @@ extern "C" int afqmc_phmsd_set_hamiltonian(afqmc_phmsd h, const double* Likn, in
 
 namespace {
 
+int scratch_alloc(c128** p, size_t n) {
+  if (cudaMalloc(p, sizeof(c128) * (n ? n : 1)) != cudaSuccess) {
+    set_error_detail("PHMSD scratch: out of device memory (%zu bytes)", sizeof(c128) * n);
+    return AFQMC_ERR_ALLOC;
+  }
+  return AFQMC_OK;
+}
+
+// per-block buffers of the Woodbury factors, excitation overlaps, weights and R (density matrix
+// and energy), for Wb walkers
+int phmsd_core_scratch(afqmc_phmsd h, int Wb) {
+  if (h->capCore >= Wb) return AFQMC_OK;
+  AFQMC_CUDA_TRY(cudaDeviceSynchronize());
+  h->free_core_scratch();
+  const size_t na = std::max(h->nact[0], h->nact[1]), ne = std::max(h->nel[0], h->nel[1]);
+  const size_t M = h->M, nu = std::max(h->nuniq[0], h->nuniq[1]);
+  for (int s = 0; s < 2; ++s) {
+    AFQMC_TRY(scratch_alloc(&h->eG[s], size_t(Wb) * ne * M));
+    AFQMC_TRY(scratch_alloc(&h->eQ[s], size_t(Wb) * na * ne));
+    AFQMC_TRY(scratch_alloc(&h->eov[s], size_t(Wb) * h->nuniq[s]));
+  }
+  AFQMC_TRY(scratch_alloc(&h->eTMN, size_t(Wb) * na * ne));
+  AFQMC_TRY(scratch_alloc(&h->eTNN, size_t(Wb) * ne * ne));
+  AFQMC_TRY(scratch_alloc(&h->elogov, Wb));
+  AFQMC_TRY(scratch_alloc(&h->eOv, Wb));
+  AFQMC_TRY(scratch_alloc(&h->wgt, nu * Wb));
+  AFQMC_TRY(scratch_alloc(&h->Rfull, size_t(Wb) * ne * na));
+  AFQMC_TRY(scratch_alloc(&h->INV, size_t(Wb) * std::max(h->ninv[0], h->ninv[1])));
+  h->capCore = Wb;
+  return AFQMC_OK;
+}
+
+// the energy's additional per-block buffers (half-rotated tensors, K vectors, R rows)
 int phmsd_energy_scratch(afqmc_phmsd h, int Wb) {
+  AFQMC_TRY(phmsd_core_scratch(h, Wb));
   if (h->capWb >= Wb) return AFQMC_OK;
   AFQMC_CUDA_TRY(cudaDeviceSynchronize());
   h->free_energy_scratch();
   const size_t na = std::max(h->nact[0], h->nact[1]), ne = std::max(h->nel[0], h->nel[1]);
-  const size_t M = h->M, Nc = h->Nc;
+  const size_t Nc = h->Nc;
   int maxnd = 1;
   size_t maxR = 1;
   for (int s = 0; s < 2; ++s)
@@ -1002,33 +1288,14 @@ int phmsd_energy_scratch(afqmc_phmsd h, int Wb) {
       maxnd = std::max(maxnd, h->sh_nd[s][j]);
       maxR = std::max(maxR, size_t(h->sh_nd[s][j]) * h->sh_nex[s][j] * h->nact[s]);
     }
-  const size_t nu = std::max(h->nuniq[0], h->nuniq[1]);
-  auto al = [](c128** p, size_t n) -> int {
-    if (cudaMalloc(p, sizeof(c128) * (n ? n : 1)) != cudaSuccess) {
-      set_error_detail("afqmc_phmsd_energy: out of device memory (%zu bytes)", sizeof(c128) * n);
-      return AFQMC_ERR_ALLOC;
-    }
-    return AFQMC_OK;
-  };
-  for (int s = 0; s < 2; ++s) {
-    AFQMC_TRY(al(&h->eG[s], size_t(Wb) * ne * M));
-    AFQMC_TRY(al(&h->eQ[s], size_t(Wb) * na * ne));
-    AFQMC_TRY(al(&h->eov[s], size_t(Wb) * h->nuniq[s]));
-  }
-  AFQMC_TRY(al(&h->eTMN, size_t(Wb) * na * ne));
-  AFQMC_TRY(al(&h->eTNN, size_t(Wb) * ne * ne));
-  AFQMC_TRY(al(&h->elogov, Wb));
-  AFQMC_TRY(al(&h->eOv, Wb));
-  AFQMC_TRY(al(&h->wgt, nu * Wb));
-  AFQMC_TRY(al(&h->Swia, size_t(Wb) * ne * na));
-  AFQMC_TRY(al(&h->Twina, size_t(Wb) * ne * Nc * na));
-  AFQMC_TRY(al(&h->KEr, size_t(h->nuniq[0]) * Wb * Nc));
-  AFQMC_TRY(al(&h->KEd, size_t(h->nuniq[1]) * Wb * Nc));
-  AFQMC_TRY(al(&h->KEl, size_t(maxnd) * Wb * Nc));
-  AFQMC_TRY(al(&h->Kdn, size_t(Wb) * Nc));
-  AFQMC_TRY(al(&h->R, maxR * Wb));
-  AFQMC_TRY(al(&h->el, 3 * size_t(Wb)));
-  AFQMC_TRY(al(&h->Rfull, size_t(Wb) * ne * na));
+  AFQMC_TRY(scratch_alloc(&h->Swia, size_t(Wb) * ne * na));
+  AFQMC_TRY(scratch_alloc(&h->Twina, size_t(Wb) * ne * Nc * na));
+  AFQMC_TRY(scratch_alloc(&h->KEr, size_t(h->nuniq[0]) * Wb * Nc));
+  AFQMC_TRY(scratch_alloc(&h->KEd, size_t(h->nuniq[1]) * Wb * Nc));
+  AFQMC_TRY(scratch_alloc(&h->KEl, size_t(maxnd) * Wb * Nc));
+  AFQMC_TRY(scratch_alloc(&h->Kdn, size_t(Wb) * Nc));
+  AFQMC_TRY(scratch_alloc(&h->R, maxR * Wb));
+  AFQMC_TRY(scratch_alloc(&h->el, 3 * size_t(Wb)));
   h->capWb = Wb;
   return AFQMC_OK;
 }
@@ -1090,9 +1357,17 @@ int phmsd_half_rotated(afqmc_phmsd h, cudaStream_t s, int sp, int nb) {
 // the excited determinants of spin sp, shell by shell: 1-body into el[0], 2-body into el[1..2],
 // KE of each determinant written to KEout + k0 * nb * Nc (cross = nullptr) or to KEl and
 // contracted with cross at once (the second step)
+size_t excited_tables_smem(afqmc_phmsd h, int sp) {
+  return 5 * size_t(h->nel[sp]) * h->nact[sp] * sizeof(c128) + size_t(h->nel[sp]) * sizeof(int);
+}
+
 int phmsd_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, c128* KEout, const c128* cross,
                   c128* E) {
   const int N = h->nel[sp], na = h->nact[sp], Nc = h->Nc;
+  // the 2-body terms from per-(walker, n) tables when they fit in shared memory, else per shell
+  // from the R rows (the reference kernel's formulation)
+  const size_t tsmem = excited_tables_smem(h, sp);
+  const bool tables = h->nuniq[sp] > 1 && tsmem <= 200 * 1024;
   AFQMC_CUDA_TRY(cudaMemsetAsync(h->el, 0, sizeof(c128) * 3 * nb, s));
   for (size_t j = 0; j < h->sh_k0[sp].size(); ++j) {
     const int k0 = h->sh_k0[sp][j], nd = h->sh_nd[sp][j], nex = h->sh_nex[sp][j];
@@ -1108,6 +1383,7 @@ int phmsd_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, c128* KEout, co
     ph_excited_1body_kernel<<<grid, PH_THREADS, 0, s>>>(iex, h->refc[sp], h->Swia, h->R, w, nb,
                                                         nd, nex, na, N, h->el);
     AFQMC_TRY(launch_status("ph_excited_1body_kernel"));
+    if (tables) continue;
     c128* KE = cross ? h->KEl : KEout + size_t(k0) * nb * Nc;
     const size_t smem = size_t(nex) * na * sizeof(c128) + 2 * size_t(N) * sizeof(int);
     AFQMC_CUDA_TRY(cudaFuncSetAttribute(ph_excited_2body_kernel,
@@ -1121,6 +1397,20 @@ int phmsd_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, c128* KEout, co
                                                 E);
       AFQMC_TRY(launch_status("cross_ej_kernel"));
     }
+  }
+  if (tables) {
+    const long nt = long(h->nuniq[sp] - 1) * nb;
+    woodbury_inverses_kernel<<<unsigned((nt + 127) / 128), 128, 0, s>>>(
+        h->eQ[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp], h->nuniq[sp], nb, na, N,
+        h->ninv[sp], h->INV);
+    AFQMC_TRY(launch_status("woodbury_inverses_kernel"));
+    AFQMC_CUDA_TRY(cudaFuncSetAttribute(excited_energy_tables_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(tsmem)));
+    excited_energy_tables_kernel<<<dim3(Nc, nb), PHX_THREADS, tsmem, s>>>(
+        h->Twina, h->eQ[sp], h->refc[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp],
+        h->INV, h->ninv[sp], h->wgt, h->nuniq[sp], nb, N, na, Nc, h->el + nb, h->el + 2 * nb,
+        cross ? nullptr : KEout, cross, E);
+    AFQMC_TRY(launch_status("excited_energy_tables_kernel"));
   }
   add_components_kernel<<<(nb + 127) / 128, 128, 0, s>>>(h->el, h->el + nb, h->el + 2 * nb, nb,
                                                           E);
@@ -1141,7 +1431,7 @@ extern "C" int afqmc_phmsd_energy(afqmc_phmsd h, const afqmc_c128* wbuf, long ld
   cudaGetDevice(&prev);
   cudaSetDevice(h->device);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const int Wb = block > 0 ? (block < W ? block : W) : (W < 32 ? W : 32);
+  const int Wb = block > 0 ? (block < W ? block : W) : (W < 64 ? W : 64);
   int st = phmsd_energy_scratch(h, Wb);
   if (st) {
     cudaSetDevice(prev);
@@ -1220,8 +1510,10 @@ extern "C" int afqmc_phmsd_density_matrix(afqmc_phmsd h, const afqmc_c128* wbuf,
   cudaGetDevice(&prev);
   cudaSetDevice(h->device);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const int Wb = block > 0 ? (block < W ? block : W) : (W < 32 ? W : 32);
-  int st = phmsd_energy_scratch(h, Wb);
+  // the density matrix needs only the per-walker Woodbury buffers (~0.5 MB per walker at
+  // nel = 30, nact = 70, 2000 excitations): blocks of up to 512 walkers
+  const int Wb = block > 0 ? (block < W ? block : W) : (W < 512 ? W : 512);
+  int st = phmsd_core_scratch(h, Wb);
   if (st) {
     cudaSetDevice(prev);
     return st;
@@ -1253,25 +1545,25 @@ extern "C" int afqmc_phmsd_density_matrix(afqmc_phmsd h, const afqmc_c128* wbuf,
             h->rowptr[sp], h->kidx[sp], h->det[1 - sp], h->coef, h->eov[1 - sp],
             h->nuniq[1 - sp], h->eov[sp], nu, nb, h->wgt);
         AFQMC_TRY(launch_status("couple_kernel"));
-        // full R (calculate_R): identity part, then each shell's Woodbury rows
-        AFQMC_CUDA_TRY(cudaMemsetAsync(h->Rfull, 0, sizeof(c128) * size_t(nb) * N * na, s));
-        r_identity_kernel<<<nb, PH_THREADS, 0, s>>>(h->wgt, nu, nb, h->refc[sp], N, na, h->Rfull);
-        AFQMC_TRY(launch_status("r_identity_kernel"));
-        for (size_t j = 0; j < h->sh_k0[sp].size(); ++j) {
-          const int k0 = h->sh_k0[sp][j], nd = h->sh_nd[sp][j], nex = h->sh_nex[sp][j];
-          const int* iex = h->uexc[sp] + h->uoff_h[sp][k0];
-          AFQMC_CUDA_TRY(cudaMemsetAsync(h->R, 0, sizeof(c128) * size_t(nb) * nd * nex * na, s));
-          const long nr = long(nb) * nd;
-          compact_R_kernel<<<unsigned((nr + 127) / 128), 128, 0, s>>>(h->eQ[sp], iex, h->refc[sp],
-                                                                      nd, nex, nb, na, N, h->R);
-          AFQMC_TRY(launch_status("compact_R_kernel"));
-          dim3 grid(nb, N);
-          accumulate_R_kernel<<<grid, 64, 0, s>>>(h->R, h->wgt + size_t(k0) * nb,
-                                                  h->eptr[sp] + h->sh_eoff[sp][j],
-                                                  h->eidx[sp] + h->sh_ioff[sp][j], iex,
-                                                  h->refc[sp], nd, nex, nb, N, na, h->Rfull);
-          AFQMC_TRY(launch_status("accumulate_R_kernel"));
+        // full R (calculate_R): the inverse of every excitation block, then all determinants'
+        // rows accumulated per walker
+        if (nu > 1) {
+          const long ni = long(nu - 1) * nb;
+          woodbury_inverses_kernel<<<unsigned((ni + 127) / 128), 128, 0, s>>>(
+              h->eQ[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp], nu, nb, na, N,
+              h->ninv[sp], h->INV);
+          AFQMC_TRY(launch_status("woodbury_inverses_kernel"));
         }
+        const size_t rsm = 3 * size_t(N) * na * sizeof(c128);
+        AFQMC_CHECK_ARG(rsm <= 200 * 1024,
+                        "afqmc_phmsd_density_matrix: nel x nact = %d x %d exceeds shared memory",
+                        N, na);
+        AFQMC_CUDA_TRY(cudaFuncSetAttribute(phmsd_R_kernel,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(rsm)));
+        phmsd_R_kernel<<<nb, PHR_THREADS, rsm, s>>>(h->eQ[sp], h->refc[sp], h->uoff[sp],
+                                                    h->unex[sp], h->uexc[sp], h->uinv[sp], h->INV,
+                                                    h->ninv[sp], h->wgt, nu, nb, N, na, h->Rfull);
+        AFQMC_TRY(launch_status("phmsd_R_kernel"));
         // G_s = R^T G_ref  (rows of this spin's active orbitals)
         GemmParams p{};
         p.m = na; p.n = h->M; p.k = N;

@@ -109,12 +109,22 @@ class Simulation:
     _eshift_dev: torch.Tensor = None
 
     @staticmethod
-    def from_workload(wl, W=None, precision=A.PREC_FP64, rp=None, **prop_kw):
+    def from_workload(wl, W=None, precision=A.PREC_FP64, rp=None, trial=None, vMF=None,
+                      **prop_kw):
+        """wl: a safire_b200.synth.Workload.  trial: an optional PHMSD trial
+        (safire_b200.synth.PHMSDTrial, COLLINEAR workload whose PsiT is its reference
+        determinant); vMF: its mean field [Nc] (host), default the reference determinant's."""
         rp = rp or RunParams()
         W = W or wl.W
         ham = A.HamiltonianOperations(wl.walker_type, wl.M, wl.nup, wl.ndn, wl.Likn, wl.hij,
                                       wl.E0, wl.PsiT)
-        wfn = A.NOMSD(ham)
+        ph = None
+        if trial is not None:
+            ph = A.PHMSD(trial)
+            ph.set_hamiltonian(wl.Likn, wl.hij, wl.E0)
+            wfn = A.PHMSDWavefunction(ph)
+        else:
+            wfn = A.NOMSD(ham)
         wset = A.WalkerSet(wl.walker_type, wl.M, wl.nup, wl.ndn, W)
         wset.init_from_trial(ham)
         # the comb's generator is the same on every rank (the reference's root draws it); the
@@ -133,9 +143,14 @@ class Simulation:
         params = A.default_params(dt=wl.dt, precision=precision, **prop_kw)
         prop = A.Propagator(ham, params, W)
         prop.set_field_seed(A.split_seed(rp.seed, _rank(), 1))
+        if ph is not None:
+            prop.set_trial(ph, vMF)
         n = rp.equilibration_steps
         relax = 1 - math.exp(-10.0 / n) if n > 1 else 1.0
-        return Simulation(ham, wfn, wset, prop, walker_rng, rp, wl.dt, Eshift, relax, precision)
+        sim = Simulation(ham, wfn, wset, prop, walker_rng, rp, wl.dt, Eshift, relax, precision)
+        if ph is not None:
+            sim.reuse_density = False  # the PHMSD step recomputes its density matrix
+        return sim
 
     def average_pseudo_energy(self):
         s = _sum_over_ranks(A.pseudo_energy_sums(self.wset, self.dt))

@@ -160,3 +160,18 @@ def make_phmsd_trial(M, nup, ndn, orbitals, nocc=20, nvirt=40, ndet=4096, max_le
     coef = (coef / np.linalg.norm(coef)).astype(np.complex128)
     refc = [np.arange(nup, dtype=np.int32), np.arange(ndn, dtype=np.int32)]
     return PHMSDTrial(M, nup, ndn, [orbmat, orbmat], refc, exc, det_up, det_dn, coef)
+
+
+def make_phmsd_workload(seed=0, W=512, M=120, N=30, Nc=960, decay=0.99, dt=0.005, ndet=4096,
+                        nocc=20, nvirt=40):
+    """The PHMSD benchmark system: COLLINEAR, M=120, N_up=N_dn=30, N_chol=960 (decay 0.99^n), a
+    trial of the reference determinant plus ndet - 1 singles-to-quadruples in a 20-occupied /
+    40-virtual window (make_phmsd_trial), 512 walkers starting at the reference determinant.
+    Returns (Workload, PHMSDTrial)."""
+    h1, Likn = make_hamiltonian(M, Nc, decay, seed)
+    _, evecs = np.linalg.eigh(h1)
+    trial = make_phmsd_trial(M, N, N, evecs, nocc=nocc, nvirt=nvirt, ndet=ndet, seed=seed)
+    PsiT = [np.ascontiguousarray(trial.orbmat[s][trial.refc[s]]) for s in (0, 1)]
+    wl = Workload("phmsd", M, N, N, Nc, W, dt, COLLINEAR, h1[None].astype(np.complex128),
+                  Likn[None], 0.0, PsiT)
+    return wl, trial

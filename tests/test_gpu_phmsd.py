@@ -114,7 +114,9 @@ def test_phmsd_log_overlap_vs_oracle(cuda, M, nup, ndn, nocc, nvirt, ndet, W):
 
 
 @pytest.mark.parametrize("M,nup,ndn,Nc,nocc,nvirt,ndet,W,block", [
-    (16, 4, 3, 6, 3, 5, 40, 3, 0), (40, 10, 9, 30, 6, 14, 300, 21, 8)])
+    (16, 4, 3, 6, 3, 5, 40, 3, 0), (40, 10, 9, 30, 6, 14, 300, 21, 8),
+    # N * nact too large for the shared-memory tables: the per-shell R-row kernels
+    (80, 40, 38, 8, 6, 30, 30, 3, 0)])
 def test_phmsd_energy_vs_oracle(cuda, M, nup, ndn, Nc, nocc, nvirt, ndet, W, block):
     """PHMSD energy_alg1 on the GPU (walker blocks, excitation shells, spin couplings) against
     the oracle's restatement (itself pinned against single-determinant energies)."""
