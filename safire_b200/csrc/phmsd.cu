@@ -446,24 +446,29 @@ __global__ void woodbury_inverses_kernel(const c128* __restrict__ QQ0, const int
 // ex and kn are then the terms of ph_excited_2body_energy_dense_cholesky
 // (detail/phmsd_impl.hpp:33-153) summed in closed form: every sum over electrons reduces to the
 // tables U and f0 = sum_i t_i[r_i] plus corrections over the nex holes.
+// Table layout: Tn [nel][nact]; Yv [nel][nv] and Qv [nel][nv] (QQ0 transposed) on the virtual
+// columns c; Uh [nh][nact] and Zh [nh][nv] on the hole rows k.  e4 = the determinant's holes,
+// particles, hole rows k and particle columns c.
 template <int NEX>
-__device__ __forceinline__ void excited_terms(const int* __restrict__ e, const c128* __restrict__ Qi,
-                                              const c128* Tn, const c128* Yn, const c128* Un,
-                                              const c128* Zn, const c128* Q0t,
-                                              const int* refs, int nact, c128 f0, c128& ex_out,
-                                              c128& kn_out) {
-  int h[NEX], p[NEX], r[NEX];
+__device__ __forceinline__ void excited_terms(const int* __restrict__ e4,
+                                              const c128* __restrict__ Qi, const c128* Tn,
+                                              const c128* Yv, const c128* Uh, const c128* Zh,
+                                              const c128* Qv, const int* refs, int nact, int nv,
+                                              c128 f0, c128& ex_out, c128& kn_out) {
+  int h[NEX], p[NEX], r[NEX], hr[NEX], pc[NEX];
 #pragma unroll
   for (int a = 0; a < NEX; ++a) {
-    h[a] = e[a];
-    p[a] = e[NEX + a];
+    h[a] = e4[a];
+    p[a] = e4[NEX + a];
+    hr[a] = e4[2 * NEX + a];
+    pc[a] = e4[3 * NEX + a];
     r[a] = refs[h[a]];
   }
   c128 F[NEX][NEX], D[NEX];
 #pragma unroll
   for (int a = 0; a < NEX; ++a) {
     const c128* ta = Tn + h[a] * nact;
-    const c128* ua = Un + h[a] * nact;
+    const c128* ua = Uh + hr[a] * nact;
     c128 dt[NEX], du[NEX];
 #pragma unroll
     for (int x = 0; x < NEX; ++x) {
@@ -476,12 +481,12 @@ __device__ __forceinline__ void excited_terms(const int* __restrict__ e, const c
       c128 ct = cmk(0, 0), cu = cmk(0, 0);
 #pragma unroll
       for (int x = 0; x < NEX; ++x) {
-        const c128 qv = Q0t[h[x] * nact + p[q]];  // QQ0[p_q][h_x]
+        const c128 qv = Qv[h[x] * nv + pc[q]];  // QQ0[p_q][h_x]
         ct = cadd(ct, cmul(dt[x], qv));
         cu = cadd(cu, cmul(du[x], qv));
       }
-      g[q] = csub(csub(ta[p[q]], Yn[h[a] * nact + p[q]]), ct);
-      gu[q] = csub(csub(ua[p[q]], Zn[h[a] * nact + p[q]]), cu);
+      g[q] = csub(csub(ta[p[q]], Yv[h[a] * nv + pc[q]]), ct);
+      gu[q] = csub(csub(ua[p[q]], Zh[hr[a] * nv + pc[q]]), cu);
     }
 #pragma unroll
     for (int b = 0; b < NEX; ++b) {
@@ -499,7 +504,7 @@ __device__ __forceinline__ void excited_terms(const int* __restrict__ e, const c
 #pragma unroll
   for (int a = 0; a < NEX; ++a) {
     const c128* ta = Tn + h[a] * nact;
-    const c128* ua = Un + h[a] * nact;
+    const c128* ua = Uh + hr[a] * nact;
     const c128 tpa = ta[p[a]], tra = ta[r[a]];
     kn = cadd(kn, cadd(F[a][a], csub(tpa, tra)));
     // f_a^2 and the changed electron's own diagonal term
@@ -524,87 +529,145 @@ __device__ __forceinline__ void excited_terms(const int* __restrict__ e, const c
 
 // nex > 4 is rare: out of line, so that its larger frame stays out of the common path
 template <int NEX>
-__device__ __noinline__ void excited_terms_rare(const int* e, const c128* Qi, const c128* Tn,
-                                                const c128* Yn, const c128* Un, const c128* Zn,
-                                                const c128* Q0t, const int* refs, int nact,
+__device__ __noinline__ void excited_terms_rare(const int* e4, const c128* Qi, const c128* Tn,
+                                                const c128* Yv, const c128* Uh, const c128* Zh,
+                                                const c128* Qv, const int* refs, int nact, int nv,
                                                 c128 f0, c128& ex, c128& kn) {
-  excited_terms<NEX>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn);
+  excited_terms<NEX>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn);
+}
+
+// One product of the tables: out[k][c] = sum_j a[k][sel_j] b[j][c] over the rows k of `rows`
+// (row index rows[k], or k when rows is null).
+struct TableProduct {
+  const c128* a;
+  int lda;
+  const int* rows;
+  int nrows;
+  const c128* b;
+  int ldb, ncol;
+  c128* out;
+  int ldo;
+};
+
+// Runs products side by side over the block: a thread owns the columns t and t + nt (nt =
+// ceil(ncol / 2)) of one row, so that each shared-memory read of a feeds two products and
+// neighbouring threads read neighbouring columns of b.
+template <int NP>
+__device__ __forceinline__ void table_products(const TableProduct (&P)[NP], const int* sel,
+                                               int nsum) {
+  int start[NP + 1];
+  start[0] = 0;
+#pragma unroll
+  for (int i = 0; i < NP; ++i) start[i + 1] = start[i] + P[i].nrows * ((P[i].ncol + 1) / 2);
+  for (int idx = threadIdx.x; idx < start[NP]; idx += blockDim.x) {
+    int i = 0;
+#pragma unroll
+    for (int q = 1; q < NP; ++q)
+      if (idx >= start[q]) i = q;
+    const TableProduct& T = P[i];
+    const int nt = (T.ncol + 1) / 2, loc = idx - start[i];
+    const int k = loc / nt, t = loc - k * nt;
+    const bool two = t + nt < T.ncol;
+    const c128* ak = T.a + (T.rows ? T.rows[k] : k) * T.lda;
+    c128 a0 = cmk(0, 0), a1 = cmk(0, 0);
+    for (int j = 0; j < nsum; ++j) {
+      const c128 x = ak[sel[j]];
+      const c128* bj = T.b + j * T.ldb + t;
+      a0 = cadd(a0, cmul(x, bj[0]));
+      if (two) a1 = cadd(a1, cmul(x, bj[nt]));
+    }
+    T.out[k * T.ldo + t] = a0;
+    if (two) T.out[k * T.ldo + t + nt] = a1;
+  }
 }
 
 // Excited-determinant 2-body energies of one spin for walker blockIdx.y at Cholesky index
 // blockIdx.x, all unique excitations in one launch (the work of ph_excited_energies_first_step /
-// second_step, phmsd_helpers.hpp:401-527, for every shell): the per-(walker, n) tables T, U, Y, Z
-// in shared memory, then one thread per excited determinant.  EXacc[w] -= wgt ex / 2,
+// second_step, phmsd_helpers.hpp:401-527, for every shell): the per-(walker, n) tables in shared
+// memory, then one thread per excited determinant.  EXacc[w] -= wgt ex / 2,
 // EJacc[w] += wgt (kn^2 - f0^2) / 2; KE[u][w][n] = kn, or with `cross` E[w].EJ += cross . kn.
+// The reference determinant's terms come from the same tables (ph_reference_energy,
+// Real3IndexFactorization.hpp:212-233, 598-696): Kref[w][n] = f0, REF[w] += (sum_ij t_i[r_j]
+// t_j[r_i], f0^2).
 constexpr int PHX_THREADS = 256;
 __global__ void __launch_bounds__(PHX_THREADS, 1) excited_energy_tables_kernel(
     const c128* __restrict__ Twina, const c128* __restrict__ QQ0, const int* __restrict__ refc,
-    const int* __restrict__ uoff, const int* __restrict__ unex, const int* __restrict__ uexc,
+    const int* __restrict__ hl, const int* __restrict__ vl, int nh, int nv,
+    const int* __restrict__ uoff4, const int* __restrict__ unex, const int* __restrict__ uexc4,
     const int* __restrict__ uinv, const c128* __restrict__ INV, int ninv,
     const c128* __restrict__ wgt, int nuniq, int W, int nel, int nact, int nchol,
     c128* __restrict__ EXacc, c128* __restrict__ EJacc, c128* __restrict__ KE,
-    const c128* __restrict__ cross, c128* __restrict__ E) {
+    const c128* __restrict__ cross, c128* __restrict__ E, c128* __restrict__ Kref,
+    c128* __restrict__ REF) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int NA = nel * nact;
-  c128* Tn = reinterpret_cast<c128*>(smem_raw);  // [nel][nact]
-  c128* Un = Tn + NA;                             // [nel][nact]
-  c128* Yn = Un + NA;                             // [nel][nact]
-  c128* Zn = Yn + NA;                             // [nel][nact]
-  c128* Q0t = Zn + NA;                            // [nel][nact]: QQ0 transposed
-  int* refs = reinterpret_cast<int*>(Q0t + NA);   // [nel]
+  c128* Tn = reinterpret_cast<c128*>(smem_raw);     // [nel][nact]
+  c128* Qv = Tn + nel * nact;                        // [nel][nv]
+  c128* Yv = Qv + nel * nv;                          // [nel][nv]
+  c128* Uh = Yv + nel * nv;                          // [nh][nact]
+  c128* Zh = Uh + nh * nact;                         // [nh][nv]
+  int* refs = reinterpret_cast<int*>(Zh + nh * nv);  // [nel]
+  int* hls = refs + nel;                             // [nh]
   __shared__ double red[PHX_THREADS / 32 * 6];
   const int n = blockIdx.x, w = blockIdx.y;
   const c128* Tw = Twina + size_t(w) * nel * nchol * nact;
   const c128* Qw = QQ0 + size_t(w) * nact * nel;
-  for (int k = threadIdx.x; k < NA; k += blockDim.x) {
+  for (int k = threadIdx.x; k < nel * nact; k += blockDim.x) {
     const int j = k / nact, x = k - j * nact;
     Tn[k] = Tw[(size_t(j) * nchol + n) * nact + x];
-    Q0t[k] = Qw[size_t(x) * nel + j];
+  }
+  for (int k = threadIdx.x; k < nel * nv; k += blockDim.x) {
+    const int i = k / nv, c = k - i * nv;
+    Qv[k] = Qw[size_t(vl[c]) * nel + i];
   }
   for (int i = threadIdx.x; i < nel; i += blockDim.x) refs[i] = refc[i];
+  for (int k = threadIdx.x; k < nh; k += blockDim.x) hls[k] = hl[k];
   __syncthreads();
-  // U = t[:, r] t,  Y = t[:, r] QQ0^T
-  for (int k = threadIdx.x; k < NA; k += blockDim.x) {
-    const int hh = k / nact, x = k - hh * nact;
-    const c128* th = Tn + hh * nact;
-    c128 u = cmk(0, 0), y = cmk(0, 0);
-    for (int j = 0; j < nel; ++j) {
-      const c128 tr = th[refs[j]];
-      u = cadd(u, cmul(tr, Tn[j * nact + x]));
-      y = cadd(y, cmul(tr, Q0t[j * nact + x]));
-    }
-    Un[k] = u;
-    Yn[k] = y;
+  // Y = t[:, r] Qv,  U = t[hole rows, r] t
+  {
+    const TableProduct P[2] = {{Tn, nact, nullptr, nel, Qv, nv, nv, Yv, nv},
+                               {Tn, nact, hls, nh, Tn, nact, nact, Uh, nact}};
+    table_products<2>(P, refs, nel);
+  }
+  // the reference determinant: f0 = sum_i t_i[r_i], ex0 = sum_ij t_i[r_j] t_j[r_i]
+  c128 ex0 = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0);
+  for (int k = threadIdx.x; k < nel * nel; k += blockDim.x) {
+    const int i = k / nel, j = k - i * nel;
+    ex0 = cadd(ex0, cmul(Tn[i * nact + refs[j]], Tn[j * nact + refs[i]]));
   }
   __syncthreads();
-  // Z = t[:, r] Y
-  for (int k = threadIdx.x; k < NA; k += blockDim.x) {
-    const int hh = k / nact, x = k - hh * nact;
-    const c128* th = Tn + hh * nact;
-    c128 z = cmk(0, 0);
-    for (int j = 0; j < nel; ++j) z = cadd(z, cmul(th[refs[j]], Yn[j * nact + x]));
-    Zn[k] = z;
+  // Z = t[hole rows, r] Y
+  {
+    const TableProduct P[1] = {{Tn, nact, hls, nh, Yv, nv, nv, Zh, nv}};
+    table_products<1>(P, refs, nel);
   }
   c128 f0 = cmk(0, 0);
   for (int i = 0; i < nel; ++i) f0 = cadd(f0, Tn[i * nact + refs[i]]);
   const c128 f00 = cmul(f0, f0);
+  block_sum3(ex0, z1, z2, red);  // ends with a barrier: Zh is complete after it
+  if (threadIdx.x == 0 && Kref) {
+    Kref[size_t(w) * nchol + n] = f0;
+    atomicAdd(&REF[2 * w].x, ex0.x);
+    atomicAdd(&REF[2 * w].y, ex0.y);
+    atomicAdd(&REF[2 * w + 1].x, f00.x);
+    atomicAdd(&REF[2 * w + 1].y, f00.y);
+  }
   __syncthreads();
   c128 exs = cmk(0, 0), ejs = cmk(0, 0), ejc = cmk(0, 0);
   const c128* Iw = INV + size_t(w) * ninv;
   for (int u = 1 + threadIdx.x; u < nuniq; u += blockDim.x) {
     const int nex = unex[u];
-    const int* e = uexc + uoff[u];
+    const int* e4 = uexc4 + uoff4[u];
     const c128* Qi = Iw + uinv[u];
     c128 ex, kn;
     switch (nex) {
-      case 1: excited_terms<1>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
-      case 2: excited_terms<2>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
-      case 3: excited_terms<3>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
-      case 4: excited_terms<4>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
-      case 5: excited_terms_rare<5>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
-      case 6: excited_terms_rare<6>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
-      case 7: excited_terms_rare<7>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
-      default: excited_terms_rare<8>(e, Qi, Tn, Yn, Un, Zn, Q0t, refs, nact, f0, ex, kn); break;
+      case 1: excited_terms<1>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
+      case 2: excited_terms<2>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
+      case 3: excited_terms<3>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
+      case 4: excited_terms<4>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
+      case 5: excited_terms_rare<5>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
+      case 6: excited_terms_rare<6>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
+      case 7: excited_terms_rare<7>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
+      default: excited_terms_rare<8>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
     }
     const c128 wu = wgt[size_t(u) * W + w];
     exs = cadd(exs, cmul(wu, ex));
@@ -628,21 +691,56 @@ __global__ void __launch_bounds__(PHX_THREADS, 1) excited_energy_tables_kernel(
   }
 }
 
+// The reference determinant's energy from the table sums (ph_reference_kernel's result):
+// E[w] += Ov (E0 + sum_i S[i][r_i], -ex0 / 2, f0^2 / 2)
+__global__ void reference_from_tables_kernel(const c128* __restrict__ Swia,
+                                             const int* __restrict__ refc, int nel, int nact,
+                                             double E0, const c128* __restrict__ Ov,
+                                             const c128* __restrict__ REF, int W,
+                                             c128* __restrict__ E) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  c128 e1 = cmk(E0, 0);
+  for (int i = 0; i < nel; ++i) e1 = cadd(e1, Swia[(size_t(w) * nel + i) * nact + refc[i]]);
+  const c128 o = Ov[w];
+  E[w * 3 + 0] = cadd(E[w * 3 + 0], cmul(o, e1));
+  E[w * 3 + 1] = cadd(E[w * 3 + 1], cmul(o, cscale(REF[2 * w], -0.5)));
+  E[w * 3 + 2] = cadd(E[w * 3 + 2], cmul(o, cscale(REF[2 * w + 1], 0.5)));
+}
+
 // KEd[d][w][n] = ov_dn[w][d] sum_{k in CSR row d} c_k ov_up[w][up_k] KEr[up_k][w][n]
-__global__ void couple_ke_kernel(const int* __restrict__ rowptr, const int* __restrict__ kidx,
+// The determinants of CSR row d are split into segments of at most KE_SEG (rows with many
+// determinants, such as the reference down-spin excitation, would otherwise serialise one CTA);
+// segment g = (d, j0, j1).  A row of one segment stores its result, longer rows add into KEd,
+// which is zeroed first.
+constexpr int KE_SEG = 16;
+__global__ void couple_ke_kernel(const int* __restrict__ seg, const int* __restrict__ kidx,
                                  const int* __restrict__ det_up, const c128* __restrict__ coef,
                                  const c128* __restrict__ KEr, const c128* __restrict__ ov_up,
                                  int nu_up, const c128* __restrict__ ov_dn, int nu_dn, int W,
                                  int nchol, c128* __restrict__ KEd) {
-  const int d = blockIdx.x, w = blockIdx.y;
+  __shared__ c128 f[KE_SEG];
+  __shared__ int uu[KE_SEG];
+  const int g = blockIdx.x, w = blockIdx.y;
+  const int d = seg[4 * g], j0 = seg[4 * g + 1], j1 = seg[4 * g + 2], single = seg[4 * g + 3];
+  const c128 od = ov_dn[size_t(w) * nu_dn + d];
+  for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+    const int k = kidx[j], u = det_up[k];
+    uu[j - j0] = u;
+    f[j - j0] = cmul(od, cmul(coef[k], ov_up[size_t(w) * nu_up + u]));
+  }
+  __syncthreads();
   for (int n = threadIdx.x; n < nchol; n += blockDim.x) {
     c128 acc = cmk(0, 0);
-    for (int j = rowptr[d]; j < rowptr[d + 1]; ++j) {
-      const int k = kidx[j], u = det_up[k];
-      const c128 f = cmul(coef[k], ov_up[size_t(w) * nu_up + u]);
-      acc = cadd(acc, cmul(f, KEr[(size_t(u) * W + w) * nchol + n]));
+    for (int j = 0; j < j1 - j0; ++j)
+      acc = cadd(acc, cmul(f[j], KEr[(size_t(uu[j]) * W + w) * nchol + n]));
+    c128* o = KEd + (size_t(d) * W + w) * nchol + n;
+    if (single) {
+      *o = acc;
+    } else {
+      atomicAdd(&o->x, acc.x);
+      atomicAdd(&o->y, acc.y);
     }
-    KEd[(size_t(d) * W + w) * nchol + n] = cmul(acc, ov_dn[size_t(w) * nu_dn + d]);
   }
 }
 
@@ -898,6 +996,19 @@ struct afqmc_phmsd_s {
   // offset of every unique excitation's inverse block (nex^2 entries) and the total per walker
   int* uinv[2] = {nullptr, nullptr};
   int ninv[2] = {0, 0};
+  // energy tables: hole rows (electrons that are a hole of some excitation) and virtual columns
+  // (active orbitals outside the reference); per excitation its holes, particles, hole rows and
+  // particle columns (uexc4 from uoff4)
+  int* hl[2] = {nullptr, nullptr};
+  int* vl[2] = {nullptr, nullptr};
+  int nh[2] = {0, 0}, nv[2] = {0, 0};
+  int* uexc4[2] = {nullptr, nullptr};
+  int* uoff4[2] = {nullptr, nullptr};
+  bool tables_ok[2] = {false, false};
+  // segments {d, j0, j1, single} of the down-spin CSR rows for couple_ke_kernel
+  int* kseg = nullptr;
+  int nkseg = 0;
+  bool kseg_split = false;
   c128* INV = nullptr;
   // energy: the Hamiltonian half-rotated with the active orbitals
   bool has_ham = false;
@@ -946,6 +1057,10 @@ struct afqmc_phmsd_s {
       cudaFree(rowptr[s]);
       cudaFree(kidx[s]);
       cudaFree(uinv[s]);
+      cudaFree(hl[s]);
+      cudaFree(vl[s]);
+      cudaFree(uexc4[s]);
+      cudaFree(uoff4[s]);
       cudaFree(lnak[s]);
       cudaFree(haj[s]);
       cudaFree(orbmat[s]);
@@ -956,6 +1071,7 @@ struct afqmc_phmsd_s {
       cudaFree(det[s]);
     }
     cudaFree(coef);
+    cudaFree(kseg);
   }
 };
 
@@ -1075,6 +1191,19 @@ extern "C" int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact
     for (int k = 0; k < ndet; ++k) ki[pos[dets[s][k]]++] = k;
     AFQMC_TRY(to_device(&h->rowptr[s], rp.data(), rp.size()));
     AFQMC_TRY(to_device(&h->kidx[s], ki.data(), ki.size()));
+    if (s == 1) {
+      std::vector<int> sg;
+      for (int u = 0; u < nuniq[1]; ++u) {
+        const bool single = rp[u + 1] - rp[u] <= KE_SEG;
+        h->kseg_split = h->kseg_split || !single;
+        for (int j = rp[u]; j < rp[u + 1] || j == rp[u]; j += KE_SEG) {
+          sg.insert(sg.end(), {u, j, std::min(j + KE_SEG, rp[u + 1]), single ? 1 : 0});
+          if (rp[u + 1] == rp[u]) break;
+        }
+      }
+      h->nkseg = int(sg.size() / 4);
+      AFQMC_TRY(to_device(&h->kseg, sg.data(), sg.size()));
+    }
     // shells of equal excitation number
     for (int u = 1; u < nuniq[s]; ++u) {
       if (h->sh_nex[s].empty() || h->sh_nex[s].back() != nex[s][u]) {
@@ -1091,6 +1220,41 @@ extern "C" int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact
       h->ninv[s] += nex[s][u] * nex[s][u];
     }
     AFQMC_TRY(to_device(&h->uinv[s], io.data(), io.size()));
+    // table indexing of the excitations
+    std::vector<int> hrow(nel[s], -1), vcol(nact[s], -1), hlv, vlv;
+    for (int u = 1; u < nuniq[s]; ++u)
+      for (int a = 0; a < nex[s][u]; ++a) hrow[excs[s][off[s][u] + a]] = 0;
+    for (int i = 0; i < nel[s]; ++i)
+      if (hrow[i] == 0) {
+        hrow[i] = int(hlv.size());
+        hlv.push_back(i);
+      }
+    std::vector<char> isref(nact[s], 0);
+    for (int i = 0; i < nel[s]; ++i) isref[refc[s][i]] = 1;
+    for (int x = 0; x < nact[s]; ++x)
+      if (!isref[x]) {
+        vcol[x] = int(vlv.size());
+        vlv.push_back(x);
+      }
+    std::vector<int> e4, o4(nuniq[s], 0);
+    bool ok = true;
+    for (int u = 1; u < nuniq[s]; ++u) {
+      const int n = nex[s][u], *e = excs[s] + off[s][u];
+      o4[u] = int(e4.size());
+      for (int a = 0; a < 2 * n; ++a) e4.push_back(e[a]);
+      for (int a = 0; a < n; ++a) e4.push_back(hrow[e[a]]);
+      for (int a = 0; a < n; ++a) {
+        e4.push_back(vcol[e[n + a]]);
+        ok = ok && vcol[e[n + a]] >= 0;  // a particle inside the reference: R-row kernels
+      }
+    }
+    h->nh[s] = int(hlv.size());
+    h->nv[s] = int(vlv.size());
+    h->tables_ok[s] = ok;
+    AFQMC_TRY(to_device(&h->hl[s], hlv.data(), hlv.size()));
+    AFQMC_TRY(to_device(&h->vl[s], vlv.data(), vlv.size()));
+    AFQMC_TRY(to_device(&h->uexc4[s], e4.data(), e4.size()));
+    AFQMC_TRY(to_device(&h->uoff4[s], o4.data(), o4.size()));
   }
   *out = h.release();
   return AFQMC_OK;
@@ -1295,7 +1459,7 @@ int phmsd_energy_scratch(afqmc_phmsd h, int Wb) {
   AFQMC_TRY(scratch_alloc(&h->KEl, size_t(maxnd) * Wb * Nc));
   AFQMC_TRY(scratch_alloc(&h->Kdn, size_t(Wb) * Nc));
   AFQMC_TRY(scratch_alloc(&h->R, maxR * Wb));
-  AFQMC_TRY(scratch_alloc(&h->el, 3 * size_t(Wb)));
+  AFQMC_TRY(scratch_alloc(&h->el, 5 * size_t(Wb)));
   h->capWb = Wb;
   return AFQMC_OK;
 }
@@ -1358,17 +1522,26 @@ int phmsd_half_rotated(afqmc_phmsd h, cudaStream_t s, int sp, int nb) {
 // KE of each determinant written to KEout + k0 * nb * Nc (cross = nullptr) or to KEl and
 // contracted with cross at once (the second step)
 size_t excited_tables_smem(afqmc_phmsd h, int sp) {
-  return 5 * size_t(h->nel[sp]) * h->nact[sp] * sizeof(c128) + size_t(h->nel[sp]) * sizeof(int);
+  const size_t N = h->nel[sp], na = h->nact[sp], nv = h->nv[sp], nh = h->nh[sp];
+  return (N * na + 2 * N * nv + nh * na + nh * nv) * sizeof(c128) + (N + nh) * sizeof(int);
 }
 
-int phmsd_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, c128* KEout, const c128* cross,
-                  c128* E) {
+// The reference determinant's and the excited determinants' energies of spin sp
+// (PHMSD.cpp:438-531): Kref [W][Nc] receives the reference K vector; KEout the excited ones
+// [u][W][Nc] (first spin), or `cross` [u][W][Nc] is contracted with them (second spin).
+int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, double E0,
+                                c128* Kref, c128* KEout, const c128* cross, c128* E) {
   const int N = h->nel[sp], na = h->nact[sp], Nc = h->Nc;
   // the 2-body terms from per-(walker, n) tables when they fit in shared memory, else per shell
   // from the R rows (the reference kernel's formulation)
   const size_t tsmem = excited_tables_smem(h, sp);
-  const bool tables = h->nuniq[sp] > 1 && tsmem <= 200 * 1024;
-  AFQMC_CUDA_TRY(cudaMemsetAsync(h->el, 0, sizeof(c128) * 3 * nb, s));
+  const bool tables = h->tables_ok[sp] && tsmem <= 200 * 1024;
+  if (!tables) {
+    ph_reference_kernel<<<nb, PH_THREADS, 0, s>>>(h->Swia, h->Twina, h->refc[sp], N, Nc, na, E0,
+                                                  h->eOv, E, Kref);
+    AFQMC_TRY(launch_status("ph_reference_kernel"));
+  }
+  AFQMC_CUDA_TRY(cudaMemsetAsync(h->el, 0, sizeof(c128) * 5 * nb, s));
   for (size_t j = 0; j < h->sh_k0[sp].size(); ++j) {
     const int k0 = h->sh_k0[sp][j], nd = h->sh_nd[sp][j], nex = h->sh_nex[sp][j];
     const int* iex = h->uexc[sp] + h->uoff_h[sp][k0];
@@ -1399,18 +1572,25 @@ int phmsd_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, c128* KEout, co
     }
   }
   if (tables) {
-    const long nt = long(h->nuniq[sp] - 1) * nb;
-    woodbury_inverses_kernel<<<unsigned((nt + 127) / 128), 128, 0, s>>>(
-        h->eQ[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp], h->nuniq[sp], nb, na, N,
-        h->ninv[sp], h->INV);
-    AFQMC_TRY(launch_status("woodbury_inverses_kernel"));
+    if (h->nuniq[sp] > 1) {
+      const long nt = long(h->nuniq[sp] - 1) * nb;
+      woodbury_inverses_kernel<<<unsigned((nt + 127) / 128), 128, 0, s>>>(
+          h->eQ[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp], h->nuniq[sp], nb, na, N,
+          h->ninv[sp], h->INV);
+      AFQMC_TRY(launch_status("woodbury_inverses_kernel"));
+    }
+    c128* REF = h->el + 3 * nb;  // [nb][2]: sum_n ex0, sum_n f0^2
     AFQMC_CUDA_TRY(cudaFuncSetAttribute(excited_energy_tables_kernel,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(tsmem)));
     excited_energy_tables_kernel<<<dim3(Nc, nb), PHX_THREADS, tsmem, s>>>(
-        h->Twina, h->eQ[sp], h->refc[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp],
-        h->INV, h->ninv[sp], h->wgt, h->nuniq[sp], nb, N, na, Nc, h->el + nb, h->el + 2 * nb,
-        cross ? nullptr : KEout, cross, E);
+        h->Twina, h->eQ[sp], h->refc[sp], h->hl[sp], h->vl[sp], h->nh[sp], h->nv[sp],
+        h->uoff4[sp], h->unex[sp], h->uexc4[sp], h->uinv[sp], h->INV, h->ninv[sp], h->wgt,
+        h->nuniq[sp], nb, N, na, Nc, h->el + nb, h->el + 2 * nb, cross ? nullptr : KEout, cross,
+        E, Kref, REF);
     AFQMC_TRY(launch_status("excited_energy_tables_kernel"));
+    reference_from_tables_kernel<<<(nb + 127) / 128, 128, 0, s>>>(h->Swia, h->refc[sp], N, na, E0,
+                                                                  h->eOv, REF, nb, E);
+    AFQMC_TRY(launch_status("reference_from_tables_kernel"));
   }
   add_components_kernel<<<(nb + 127) / 128, 128, 0, s>>>(h->el, h->el + nb, h->el + 2 * nb, nb,
                                                           E);
@@ -1464,27 +1644,22 @@ extern "C" int afqmc_phmsd_energy(afqmc_phmsd h, const afqmc_c128* wbuf, long ld
       AFQMC_TRY(launch_status("total_overlap_kernel"));
       AFQMC_TRY(couple(0, h->eov[1], nu1, h->eov[0]));
       AFQMC_TRY(phmsd_half_rotated(h, s, 0, nb));
-      ph_reference_kernel<<<nb, PH_THREADS, 0, s>>>(h->Swia, h->Twina, h->refc[0], h->nel[0], Nc,
-                                                    h->nact[0], h->E0, h->eOv, E, h->KEr);
-      AFQMC_TRY(launch_status("ph_reference_kernel"));
-      AFQMC_TRY(phmsd_excited(h, s, 0, nb, h->KEr, nullptr, E));
+      AFQMC_TRY(phmsd_reference_and_excited(h, s, 0, nb, h->E0, h->KEr, h->KEr, nullptr, E));
       // K vectors coupled to the down-spin excitations (PHMSD.cpp:472-494)
       {
-        dim3 grid(nu1, nb);
-        couple_ke_kernel<<<grid, 128, 0, s>>>(h->rowptr[1], h->kidx[1], h->det[0], h->coef,
-                                              h->KEr, h->eov[0], nu0, h->eov[1], nu1, nb, Nc,
-                                              h->KEd);
+        if (h->kseg_split)
+          AFQMC_CUDA_TRY(cudaMemsetAsync(h->KEd, 0, sizeof(c128) * size_t(nu1) * nb * Nc, s));
+        dim3 grid(h->nkseg, nb);
+        couple_ke_kernel<<<grid, 128, 0, s>>>(h->kseg, h->kidx[1], h->det[0], h->coef, h->KEr,
+                                              h->eov[0], nu0, h->eov[1], nu1, nb, Nc, h->KEd);
         AFQMC_TRY(launch_status("couple_ke_kernel"));
       }
       // spin down (PHMSD.cpp:497-531)
       AFQMC_TRY(couple(1, h->eov[0], nu0, h->eov[1]));
       AFQMC_TRY(phmsd_half_rotated(h, s, 1, nb));
-      ph_reference_kernel<<<nb, PH_THREADS, 0, s>>>(h->Swia, h->Twina, h->refc[1], h->nel[1], Nc,
-                                                    h->nact[1], 0.0, h->eOv, E, h->Kdn);
-      AFQMC_TRY(launch_status("ph_reference_kernel"));
+      AFQMC_TRY(phmsd_reference_and_excited(h, s, 1, nb, 0.0, h->Kdn, nullptr, h->KEd, E));
       cross_ej_kernel<<<nb, PH_THREADS, 0, s>>>(h->KEd, h->Kdn, 1, nb, Nc, E);
       AFQMC_TRY(launch_status("cross_ej_kernel"));
-      AFQMC_TRY(phmsd_excited(h, s, 1, nb, nullptr, h->KEd, E));
       finish_energy_kernel<<<(nb + 127) / 128, 128, 0, s>>>(h->eOv, h->elogov, nb, E,
                                                             Oall + w0);
       AFQMC_TRY(launch_status("finish_energy_kernel"));
