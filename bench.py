@@ -10,7 +10,14 @@ cadence: 10 propagation steps, QR re-orthogonalisation every 5, comb population 
 and one mixed-estimator energy measurement every 10.  value = walker-steps/s over all ranks
 (= W * 10 * K * N_gpus / max-over-ranks device time).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed] [--impl reference]
+The default run times the mixed-precision path (3xTF32 tensor-core contractions, FP64
+determinants, weights and energy sums) and then the complex128 path on the same inputs
+(`fp64` in the JSON line, with the mixed / FP64 ratio).  `--workload phmsd` times the
+particle-hole multi-determinant system instead (COLLINEAR M=120, N=30+30, N_chol=960, reference
++ 4095 determinants, 512 walkers, complex128).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+                  [--workload nomsd|phmsd] [--impl reference]
 """
 from __future__ import annotations
 
@@ -32,10 +39,15 @@ BLOCK = 10  # AFQMC steps per bench step
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=6)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="nomsd", choices=["nomsd", "phmsd"],
+                    help="nomsd: the single-determinant M=200 system (the metric's workload); "
+                         "phmsd: the particle-hole multi-determinant system")
+    ap.add_argument("--no-fp64-compare", action="store_true",
+                    help="skip timing the complex128 path beside the mixed one")
     ap.add_argument("--walkers", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -101,6 +113,11 @@ def host_cores():
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
+        return 0
+    if args.workload == "phmsd":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the oracle's PHMSD energy is a per-determinant Python loop; no CPU "
+                          "timing of the 4096-determinant system"}), flush=True)
         return 0
     cores = host_cores()
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
@@ -234,17 +251,119 @@ def tf32_peak_tflops(torch):
     return 2 * n ** 3 / best / 1e12
 
 
-def run_ours(args):
-    import numpy as np
+def _timed_blocks(sim, steps, warmup, world, local, clocks=None):
+    """Warm up, then time `steps` blocks of BLOCK steps with CUDA events on the current stream,
+    barriers on both sides; returns (max-over-ranks ms, our kernel launches, clock summary)."""
     import torch
     import torch.distributed as dist
-
-    from safire_b200 import afqmc as A
     from safire_b200 import capi
-    from safire_b200.driver import RunParams, Simulation
-    from safire_b200.population import population_control_distributed
-    from safire_b200.synth import make_workload
 
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def block():
+        for _ in range(BLOCK):
+            sim.step()
+
+    for _ in range(warmup):
+        block()
+    torch.cuda.synchronize()
+    barrier()
+    launches0 = capi.lib().afqmc_kernel_launches()
+    graph_k0 = sim.graph.kernels_replayed() if sim.graph is not None else 0
+    if clocks is not None:
+        clocks.start()
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        block()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop() if clocks is not None else None
+    launches = capi.lib().afqmc_kernel_launches() - launches0
+    if sim.graph is not None:  # kernels the step graph replayed inside the timed region
+        launches += sim.graph.kernels_replayed() - graph_k0
+    t_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+    return t_ms, int(launches), clk
+
+
+def _phases(sim):
+    """Per-phase device time of one step and of one energy measurement and orthogonalisation
+    (outside the timed region)."""
+    import torch
+    stream = torch.cuda.current_stream()
+    sim.prop.set_timing(True)
+    sim.prop.Propagate(sim.wset, sim.Eshift)
+    sim._g_ready = False  # that step did not leave the density matrix for the next one
+    phases = sim.prop.timings()
+    sim.prop.set_timing(False)
+    torch.cuda.synchronize()
+    for name, fn in (("energy_measurement", sim.measure),
+                     ("orthogonalize", lambda: sim.prop.Orthogonalize(sim.wset))):
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        fn()
+        m1.record(stream)
+        torch.cuda.synchronize()
+        phases[name] = m0.elapsed_time(m1)
+    return phases
+
+
+def _e2e(sim, W, Nc, steps, world, prec):
+    """The same blocks through the public API with host uniforms copied in from pinned memory
+    and the weights + energy estimate read back every block."""
+    import torch
+    import torch.distributed as dist
+    from safire_b200 import afqmc as A
+    stream = torch.cuda.current_stream()
+    host_u = torch.rand((BLOCK, W, Nc), dtype=torch.float64).pin_memory()
+    dev_u = torch.empty((BLOCK, W, Nc), dtype=torch.float64, device="cuda")
+    host_w = torch.empty((W,), dtype=torch.complex128).pin_memory()
+    host_e = torch.empty((4,), dtype=torch.complex128).pin_memory()
+
+    def block_e2e():
+        dev_u.copy_(host_u, non_blocking=True)
+        for s in range(BLOCK):
+            sim.step(dev_u[s], measure=False)
+        E, _ = sim.wfn.Energy(sim.wset, set_properties=False, precision=prec)
+        sums = A.energy_sums(sim.wset, E)
+        if world > 1:
+            dist.all_reduce(sums)
+        host_e.copy_(sums, non_blocking=True)
+        host_w.copy_(sim.wset.properties()[:, 0], non_blocking=True)
+
+    block_e2e()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0.record(stream)
+    for _ in range(steps):
+        block_e2e()
+    k1.record(stream)
+    torch.cuda.synchronize()
+    te = k0.elapsed_time(k1)
+    if world > 1:
+        t = torch.tensor([te], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        te = float(t.item())
+    return {"value": W * world * BLOCK * steps / (te / 1000), "unit": "walker-steps/s",
+            "h2d_bytes_per_step": int(host_u.numel() * 8),
+            "d2h_bytes_per_step": int((host_w.numel() + host_e.numel()) * 16)}
+
+
+def _init_dist():
+    import torch
+    import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -253,6 +372,20 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def run_ours(args):
+    if args.workload == "phmsd":
+        return run_phmsd(args)
+    import torch
+    import torch.distributed as dist
+
+    from safire_b200 import afqmc as A
+    from safire_b200.driver import RunParams, Simulation
+    from safire_b200.synth import make_workload
+
+    world, rank, local = _init_dist()
     prec = A.PREC_MIXED if args.precision == "mixed" else A.PREC_FP64
     W = args.walkers
     wl = make_workload("cfg2")
@@ -263,73 +396,23 @@ def run_ours(args):
         sim.ham.set_exchange_split(args.exchange_split)
     if prec == A.PREC_MIXED and args.taylor_mode != 1:
         sim.ham.set_taylor_fused(args.taylor_mode)
-    stream = torch.cuda.current_stream()
 
-    def block():
-        for _ in range(BLOCK):
-            sim.step()
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    for _ in range(args.warmup):
-        block()
-    torch.cuda.synchronize()
-    barrier()
-    launches0 = capi.lib().afqmc_kernel_launches()
-    graph_k0 = sim.graph.kernels_replayed() if sim.graph is not None else 0
-    clocks = ClockSampler(local)
-    clocks.start()
-    torch.cuda.synchronize()
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        block()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    clk = clocks.stop()
-    launches = capi.lib().afqmc_kernel_launches() - launches0
-    if sim.graph is not None:  # kernels the step graph replayed inside the timed region
-        launches += sim.graph.kernels_replayed() - graph_k0
-    t_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
+    t_ms, launches, clk = _timed_blocks(sim, args.steps, args.warmup, world, local,
+                                        ClockSampler(local))
     value = W * world * BLOCK * args.steps / (t_ms / 1000)
+    phases = _phases(sim)
 
-    # per-phase timing of one step and of one energy measurement (untimed region)
-    sim.prop.set_timing(True)
-    sim.prop.Propagate(sim.wset, sim.Eshift)
-    sim._g_ready = False  # that step did not leave the density matrix for the next one
-    phases = sim.prop.timings()
-    sim.prop.set_timing(False)
-    torch.cuda.synchronize()
-    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    m0.record(stream)
-    sim.measure()
-    m1.record(stream)
-    torch.cuda.synchronize()
-    phases["energy_measurement"] = m0.elapsed_time(m1)
-    o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    o0.record(stream)
-    sim.prop.Orthogonalize(sim.wset)
-    o1.record(stream)
-    torch.cuda.synchronize()
-    phases["orthogonalize"] = o0.elapsed_time(o1)
-
-    # roofline of the dominant kernel: the contraction with the largest share of a block
+    # roofline of the dominant contraction: the kernel with the largest share of a block
     M, N, Nc = wl.M, wl.nup, wl.Nc
+    peaks = measured_peaks()
     if prec == A.PREC_FP64:
         # flops the FP64 kernels execute (real trial: Lnak, L and P1 are real)
         flops = {"vHS": 4.0 * M * M * Nc * W, "vbias": 4.0 * N * M * Nc * W,
                  "propagate": W * (2 * 4.0 * M * M * N + 6 * 8.0 * M * M * N),
                  "energy_measurement": W * (4.0 * N * N * M * Nc + 8.0 * N * N * Nc)}
         peak = fp64_peak_tflops(torch)
-        peak_src = "cuBLAS DGEMM 8192^3 measured in this run (dense FP64)"
+        peak_src = "cuBLAS DGEMM 8192^3 measured in this run (dense FP64; no FP64 entry in " \
+                   "MEASURED_PEAKS.json)"
     else:
         # TF32 MMA flops of the split products (x3 for 3xTF32, unpadded tile extents)
         sp = 3.0
@@ -337,8 +420,13 @@ def run_ours(args):
         flops = {"vHS": sp * 4.0 * M * M * Nc * W, "vbias": sp * 4.0 * N * M * Nc * W,
                  "propagate": sp * W * (2 * 4.0 * M * M * N + 6 * 8.0 * M * M * N),
                  "energy_measurement": ex * W * 4.0 * N * N * M * Nc}
-        peak = tf32_peak_tflops(torch)
-        peak_src = "cuBLAS TF32 GEMM 8192^3 measured in this run (dense TF32 tensor cores)"
+        if peaks.get("bf16_tflops"):
+            peak = peaks["bf16_tflops"] / 2
+            peak_src = "of measured: MEASURED_PEAKS.json bf16_tflops / 2 (dense TF32 runs at " \
+                       "half the BF16 tensor rate)"
+        else:
+            peak = tf32_peak_tflops(torch)
+            peak_src = "cuBLAS TF32 GEMM 8192^3 measured in this run"
     block_share = {k: (phases[k] * (1 if k == "energy_measurement" else BLOCK)) for k in flops}
     top = max(block_share, key=block_share.get)
     achieved = flops[top] / (phases[top] / 1000) / 1e12
@@ -347,43 +435,22 @@ def run_ours(args):
                 "peak_source": peak_src, "flops_per_launch": flops[top],
                 "block_share_ms": block_share}
 
-    # e2e: the same loop through the public API with host uniforms copied in from pinned memory
-    # and the weights + energy estimate read back every block
-    e2e = None
-    if not args.no_e2e:
-        host_u = torch.rand((BLOCK, W, Nc), dtype=torch.float64).pin_memory()
-        dev_u = torch.empty((BLOCK, W, Nc), dtype=torch.float64, device="cuda")
-        host_w = torch.empty((W,), dtype=torch.complex128).pin_memory()
-        host_e = torch.empty((4,), dtype=torch.complex128).pin_memory()
+    e2e = None if args.no_e2e else _e2e(sim, W, Nc, args.steps, world, prec)
 
-        def block_e2e():
-            dev_u.copy_(host_u, non_blocking=True)
-            for s in range(BLOCK):
-                sim.step(dev_u[s], measure=False)
-            E, _ = sim.wfn.Energy(sim.wset, set_properties=False, precision=prec)
-            sums = A.energy_sums(sim.wset, E)
-            if world > 1:
-                dist.all_reduce(sums)
-            host_e.copy_(sums, non_blocking=True)
-            host_w.copy_(sim.wset.properties()[:, 0], non_blocking=True)
-
-        block_e2e()
-        torch.cuda.synchronize()
-        barrier()
-        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        k0.record(stream)
-        for _ in range(args.steps):
-            block_e2e()
-        k1.record(stream)
-        torch.cuda.synchronize()
-        te = k0.elapsed_time(k1)
-        if world > 1:
-            t = torch.tensor([te], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
-        e2e = {"value": W * world * BLOCK * args.steps / (te / 1000), "unit": "walker-steps/s",
-               "h2d_bytes_per_step": int(host_u.numel() * 8),
-               "d2h_bytes_per_step": int((host_w.numel() + host_e.numel()) * 16)}
+    # the plain complex128 path on the same inputs, timed the same way: the mixed-vs-FP64 ratio
+    fp64 = None
+    if prec == A.PREC_MIXED and not args.no_fp64_compare:
+        err_flag = int(sim.ham.device_error_flag())
+        del sim
+        torch.cuda.empty_cache()
+        ref = Simulation.from_workload(wl, W=W, precision=A.PREC_FP64, rp=rp)
+        ref.use_graph = not args.no_graph
+        t64, _, _ = _timed_blocks(ref, args.steps, args.warmup, world, local)
+        v64 = W * world * BLOCK * args.steps / (t64 / 1000)
+        fp64 = {"value": v64, "ms_per_step": t64 / args.steps, "mixed_over_fp64": value / v64}
+        sim = ref
+    else:
+        err_flag = int(sim.ham.device_error_flag())
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -405,12 +472,74 @@ def run_ours(args):
                        "precision": args.precision, "global_walkers": W * world,
                        "exchange_split": args.exchange_split if prec == A.PREC_MIXED else None,
                        "taylor_mode": args.taylor_mode if prec == A.PREC_MIXED else None,
-                       "step_graph": sim.graph is not None,
+                       "step_graph": not args.no_graph,
                        "parallelism": f"walker dp{world}",
                        "l2": "inputs larger than L2 (V 655 MB, Likn 512 MB per step)"},
+            "fp64": fp64,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": int(launches), "clocks": clk, "phases_ms": phases,
-            "device_error_flag": int(sim.ham.device_error_flag()),
+            "gpu_launches": launches, "clocks": clk, "phases_ms": phases,
+            "device_error_flag": err_flag,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_phmsd(args):
+    """The multi-determinant workload: COLLINEAR M=120, N=30+30, Nc=960, reference + 4095
+    particle-hole determinants, 512 walkers per GPU; FP64 (the PHMSD kernels run in complex128)."""
+    import torch
+    import torch.distributed as dist
+
+    from safire_b200 import afqmc as A
+    from safire_b200.driver import RunParams, Simulation
+    from safire_b200.synth import make_phmsd_workload
+
+    world, rank, local = _init_dist()
+    W = args.walkers if args.walkers != 1024 else 512
+    wl, trial = make_phmsd_workload(W=W)
+    rp = RunParams(equilibration_steps=0, seed=0)
+    sim = Simulation.from_workload(wl, W=W, rp=rp, trial=trial)
+    sim.use_graph = False
+    t_ms, launches, clk = _timed_blocks(sim, args.steps, args.warmup, world, local,
+                                        ClockSampler(local))
+    value = W * world * BLOCK * args.steps / (t_ms / 1000)
+    phases = _phases(sim)
+    # the excited-determinant energy tables, per (walker, Cholesky index) and spin: the table
+    # products Y = t[:, r] QQ0^T (nel x nv x nel), U = t[holes, r] t (nh x nact x nel),
+    # Z = t[holes, r] Y (nh x nv x nel), then 3 n^3 + 6 n^2 + 3 n complex MACs per n-hole
+    # determinant (the closed-form sums of excited_terms); 8 flops per complex MAC
+    macs = 0.0
+    for s in (0, 1):
+        nel = trial.nup if s == 0 else trial.ndn
+        nact = trial.orbmat[s].shape[0]
+        nv = nact - nel
+        nh = len({int(h) for n, e in trial.exc[s].items() for h in e[:, :n].ravel()})
+        macs += nel * nv * nel + nh * nact * nel + nh * nv * nel
+        macs += sum(len(e) * (3 * n ** 3 + 6 * n ** 2 + 3 * n) for n, e in trial.exc[s].items())
+    flops = 8.0 * W * wl.Nc * macs
+    fp64 = fp64_peak_tflops(torch)
+    achieved = flops / (phases["energy_measurement"] / 1000) / 1e12
+    roofline = {"kernel": "energy_measurement (excited_energy_tables_kernel ~80%)",
+                "bound": "fp64", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
+                "frac": achieved / fp64, "traffic": None, "flops_per_launch": flops,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"}
+    e2e = None if args.no_e2e else _e2e(sim, W, wl.Nc, args.steps, world, A.PREC_FP64)
+    if rank == 0:
+        line = {
+            "metric": "walker-steps/s, PHMSD trial (M=120, 30+30 electrons, 4096 determinants, "
+                      "512 walkers) on B200",
+            "value": value, "unit": "walker-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": f"PHMSD M=120 N=30+30 Nc=960 W={W}/GPU dt=0.005 taylor=6, "
+                                   "reference + 4095 determinants (20 occ / 40 virt window), "
+                                   "block of 10 steps (ortho/5, comb/10, energy/10)",
+                       "precision": "fp64", "global_walkers": W * world,
+                       "parallelism": f"walker dp{world}"},
+            "roofline": roofline, "cpu_baseline": None, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clk, "phases_ms": phases,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
