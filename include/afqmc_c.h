@@ -413,6 +413,39 @@ int afqmc_energy_sums(afqmc_wset ws, const afqmc_c128* E, afqmc_c128* out4, afqm
  * {sum w exp(dt*eloc), sum w} */
 int afqmc_pseudo_energy_sums(afqmc_wset ws, double dt, afqmc_c128* out2, afqmc_stream stream);
 
+/* =========================================================================================
+ * Learned exchange-energy control variate (no reference counterpart; the exact exchange of
+ * afqmc_ham_energy stays the judge).  An MLP features (D) -> H -> H -> 1 with GELU, trained and
+ * evaluated by BF16 tensor-core kernels with FP32 accumulation, FP32 master weights and Adam.
+ * Parameters are one FP32 block [W1 (H x D) | b1 (H) | W2 (H x H) | b2 (H) | w3 (H) | b3 (1)],
+ * row-major (out x in).  Features and targets are device FP32; targets in physical units, the
+ * network works on standardised features and targets (afqmc_mlp_set_normalization).
+ * ========================================================================================= */
+typedef struct afqmc_mlp_s* afqmc_mlp;
+/* D even, H a multiple of 8; uniform He initialisation from `seed` (host) */
+int afqmc_mlp_create(int D, int H, unsigned long long seed, afqmc_mlp* out);
+int afqmc_mlp_destroy(afqmc_mlp mlp);
+long afqmc_mlp_num_params(afqmc_mlp mlp);
+/* host arrays: mean, istd [D]; the target's mean and standard deviation */
+int afqmc_mlp_set_normalization(afqmc_mlp mlp, const float* mean, const float* istd,
+                                float y_mean, float y_std);
+/* which = 0: parameters (read or write), 1: gradients of the last afqmc_mlp_gradients /
+ * afqmc_mlp_train_step (read); host FP32 [afqmc_mlp_num_params].  Synchronous. */
+int afqmc_mlp_params(afqmc_mlp mlp, int which, float* host, int to_device);
+/* y [B] (device) = prediction for features X [B][D] (device) */
+int afqmc_mlp_predict(afqmc_mlp mlp, const float* X, int B, float* y, afqmc_stream stream);
+/* forward + backward of the loss mean((y - t)^2) / 2 in standardised units for X [B][D],
+ * t [B]; gradients kept in the handle; loss (device float, may be NULL) */
+int afqmc_mlp_gradients(afqmc_mlp mlp, const float* X, const float* t, int B, float* loss,
+                        afqmc_stream stream);
+/* afqmc_mlp_gradients followed by one Adam step (beta 0.9 / 0.999, eps 1e-8) */
+int afqmc_mlp_train_step(afqmc_mlp mlp, const float* X, const float* t, int B, float lr,
+                         float* loss, afqmc_stream stream);
+/* features of W walkers: X [W][2 Nc + 2 N] = [Re vbias, Im vbias, Re G[a][a], Im G[a][a] (a < N)]
+ * from vbias [W][ldv] and the compact density matrix G [W][ldG] ([N][M] per spin block) */
+int afqmc_exchange_features(const afqmc_c128* vbias, long ldv, const afqmc_c128* G, long ldG,
+                            int N, int M, int Nc, int W, float* X, afqmc_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -73,6 +73,15 @@ _SIGS = {
     "afqmc_phmsd_vbias": (i32, [vp, vp, vp, i32, C.c_double, vp]),
     "afqmc_phmsd_info": (i32, [vp, vp]),
     "afqmc_prop_set_phmsd": (i32, [vp, vp, vp]),
+    "afqmc_mlp_create": (i32, [i32, i32, u64, C.POINTER(vp)]),
+    "afqmc_mlp_destroy": (i32, [vp]),
+    "afqmc_mlp_num_params": (C.c_long, [vp]),
+    "afqmc_mlp_set_normalization": (i32, [vp, vp, vp, C.c_float, C.c_float]),
+    "afqmc_mlp_params": (i32, [vp, i32, vp, i32]),
+    "afqmc_mlp_predict": (i32, [vp, vp, i32, vp, vp]),
+    "afqmc_mlp_gradients": (i32, [vp, vp, vp, i32, vp, vp]),
+    "afqmc_mlp_train_step": (i32, [vp, vp, vp, i32, C.c_float, vp, vp]),
+    "afqmc_exchange_features": (i32, [vp, i64, vp, i64, i32, i32, i32, i32, vp, vp]),
     "afqmc_wset_create": (i32, [i32, i32, i32, i32, i32, C.POINTER(vp)]),
     "afqmc_wset_destroy": (i32, [vp]),
     "afqmc_wset_buffer": (i32, [vp, C.POINTER(vp), C.POINTER(i64), C.POINTER(i32)]),
