@@ -43,9 +43,14 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
-    ap.add_argument("--workload", default="nomsd", choices=["nomsd", "phmsd"],
+    ap.add_argument("--workload", default="nomsd", choices=["nomsd", "phmsd", "control-variate"],
                     help="nomsd: the single-determinant M=200 system (the metric's workload); "
-                         "phmsd: the particle-hole multi-determinant system")
+                         "phmsd: the particle-hole multi-determinant system; control-variate: "
+                         "the learned exchange estimator's cost at equal error bar")
+    ap.add_argument("--cv-epochs", type=int, default=30)
+    ap.add_argument("--cv-system", default="cfg2", choices=["cfg1", "cfg2"],
+                    help="control-variate workload: cfg2 = M=200 N=50+50 Nc=1600, cfg1 = M=32 "
+                         "N=8+8 Nc=128")
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="skip timing the complex128 path beside the mixed one")
     ap.add_argument("--walkers", type=int, default=1024)
@@ -113,6 +118,10 @@ def host_cores():
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
+        return 0
+    if args.workload == "control-variate":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the learned control variate has no reference counterpart"}), flush=True)
         return 0
     if args.workload == "phmsd":
         print(json.dumps({"impl": "reference", "unavailable":
@@ -378,6 +387,8 @@ def _init_dist():
 def run_ours(args):
     if args.workload == "phmsd":
         return run_phmsd(args)
+    if args.workload == "control-variate":
+        return run_control_variate(args)
     import torch
     import torch.distributed as dist
 
@@ -479,6 +490,103 @@ def run_ours(args):
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clk, "phases_ms": phases,
             "device_error_flag": err_flag,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_control_variate(args):
+    """The learned exchange control variate on the M=200 workload (mixed precision): pairs from
+    the exact kernel over 500 equilibration steps train the MLP; afterwards every measurement is
+    timed both ways (all-exact vs network on all walkers + exact exchange on a random 1/8), and the
+    cost ratio at equal statistical error bar is reported with the estimator's spread."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from safire_b200 import afqmc as A
+    from safire_b200.driver import RunParams, Simulation
+    from safire_b200.mlp import ExchangeControlVariate
+    from safire_b200.synth import make_workload
+
+    world, rank, local = _init_dist()
+    W = args.walkers
+    wl = make_workload(args.cv_system)
+    if args.cv_system == "cfg2":
+        # training pairs from the first 150 steps at a fixed Eshift (one set every step): on this
+        # synthetic system the reference algorithm's total weight collapses after
+        # a few hundred steps, so a 500-step equilibration cannot run
+        equil, every, eq_steps = 150, 1, 0
+    else:
+        # the M=32 system equilibrates: 500 steps with the Eshift update, a pair set every 10
+        equil, every, eq_steps = 500, 10, 500
+    sim = Simulation.from_workload(wl, W=W, precision=A.PREC_MIXED,
+                                   rp=RunParams(equilibration_steps=eq_steps, seed=0))
+    sim.use_graph = not args.no_graph
+    cv = ExchangeControlVariate(sim, hidden=512, fraction=1.0 / 8, seed=0)
+    for step in range(equil):
+        sim.step(measure=False)
+        if step % every == 0:
+            cv.collect()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = cv.fit(epochs=args.cv_epochs, batch=1024, lr=1e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r, e0.elapsed_time(e1)
+
+    exact_e, mf_e, t_ex, t_mf = [], [], [], []
+    for m in range(args.steps + args.warmup):
+        for _ in range(BLOCK):
+            sim.step(measure=False)
+        (e_exact, _, _), te = timed(sim.measure)
+        (e_mf, _), tm = timed(cv.measure)
+        if m >= args.warmup:
+            exact_e.append(e_exact)
+            mf_e.append(e_mf)
+            t_ex.append(te)
+            t_mf.append(tm)
+    exact_e, mf_e = np.array(exact_e), np.array(mf_e)
+    diff = mf_e - exact_e
+    s_qmc = float(np.std(exact_e, ddof=1))
+    s_sub = float(np.std(diff, ddof=1))
+    factor = (s_qmc ** 2 + s_sub ** 2) / s_qmc ** 2  # measurements needed for equal error bar
+    tex, tmf = float(np.median(t_ex)), float(np.median(t_mf))
+    value = tex / (tmf * factor)
+    if rank == 0:
+        line = {
+            "metric": "energy-measurement cost reduction at equal statistical error bar, "
+                      f"learned exchange control variate (M={wl.M}, {W} walkers, mixed)",
+            "value": value, "unit": "x (all-exact cost / control-variate cost)",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 MLP (fp32 accumulate) + c128/tf32x3 exact exchange",
+            "data": "synthetic",
+            "config": {"workload": f"M={wl.M} N={wl.nup}+{wl.ndn} Nc={wl.Nc} W={W} "
+                                   f"dt={wl.dt}; MLP {cv.mlp.D}-512-512-1 GELU trained on pairs "
+                                   f"from the first {equil} steps (one set per {every} steps"
+                                   f"{', fixed Eshift' if eq_steps == 0 else ''}); exact "
+                                   "exchange on 1/8 of the walkers per measurement; one "
+                                   "measurement per 10-step block",
+                       "training_samples": int(sum(x.shape[0] for x in cv.X)),
+                       "epochs": args.cv_epochs, "train_seconds": t_train,
+                       "loss_first_last": [hist[0], hist[-1]]},
+            "measurement_ms": {"all_exact": tex, "control_variate": tmf},
+            "sigma": {"qmc_between_measurements": s_qmc, "subsampling": s_sub,
+                      "measurements_factor_for_equal_error": factor},
+            "bias": {"mean_mf_minus_exact": float(diff.mean()),
+                     "standard_error": float(s_sub / np.sqrt(diff.size))},
         }
         print(json.dumps(line), flush=True)
     if world > 1:

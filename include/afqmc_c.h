@@ -441,10 +441,12 @@ int afqmc_mlp_gradients(afqmc_mlp mlp, const float* X, const float* t, int B, fl
 /* afqmc_mlp_gradients followed by one Adam step (beta 0.9 / 0.999, eps 1e-8) */
 int afqmc_mlp_train_step(afqmc_mlp mlp, const float* X, const float* t, int B, float lr,
                          float* loss, afqmc_stream stream);
-/* features of W walkers: X [W][2 Nc + 2 N] = [Re vbias, Im vbias, Re G[a][a], Im G[a][a] (a < N)]
- * from vbias [W][ldv] and the compact density matrix G [W][ldG] ([N][M] per spin block) */
+/* features of W walkers: X [W][D] = [Re vbias, Im vbias, Re G[a][a], Im G[a][a] (a < N)] from
+ * vbias [W][ldv] and the compact density matrix G [W][ldG] ([N][M] per spin block), D = 2 Nc +
+ * 2 N; with E [W][3] (E1, EXX, EJ; may be NULL) also Re E1, Im E1, Re EJ, Im EJ (D + 4) */
 int afqmc_exchange_features(const afqmc_c128* vbias, long ldv, const afqmc_c128* G, long ldG,
-                            int N, int M, int Nc, int W, float* X, afqmc_stream stream);
+                            int N, int M, int Nc, int W, const afqmc_c128* E, float* X,
+                            afqmc_stream stream);
 
 #ifdef __cplusplus
 }

@@ -81,7 +81,7 @@ _SIGS = {
     "afqmc_mlp_predict": (i32, [vp, vp, i32, vp, vp]),
     "afqmc_mlp_gradients": (i32, [vp, vp, vp, i32, vp, vp]),
     "afqmc_mlp_train_step": (i32, [vp, vp, vp, i32, C.c_float, vp, vp]),
-    "afqmc_exchange_features": (i32, [vp, i64, vp, i64, i32, i32, i32, i32, vp, vp]),
+    "afqmc_exchange_features": (i32, [vp, i64, vp, i64, i32, i32, i32, i32, vp, vp, vp]),
     "afqmc_wset_create": (i32, [i32, i32, i32, i32, i32, C.POINTER(vp)]),
     "afqmc_wset_destroy": (i32, [vp]),
     "afqmc_wset_buffer": (i32, [vp, C.POINTER(vp), C.POINTER(i64), C.POINTER(i32)]),

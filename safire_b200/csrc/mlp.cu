@@ -221,13 +221,21 @@ __global__ void to_bf16_kernel(const float* __restrict__ x, long n, bf16* __rest
   if (i < n) y[i] = __float2bfloat16(x[i]);
 }
 
-// X[w] = [Re vbias (Nc), Im vbias (Nc), Re G[a][a] (a < N), Im G[a][a]] for each walker
+// X[w] = [Re vbias (Nc), Im vbias (Nc), Re G[a][a] (a < N), Im G[a][a], and with E:
+// Re E1, Im E1, Re EJ, Im EJ] for each walker
 __global__ void exchange_features_kernel(const c128* __restrict__ vb, long ldv,
                                          const c128* __restrict__ G, long ldG, int N, int M,
-                                         int Nc, int W, float* __restrict__ X) {
+                                         int Nc, int W, const c128* __restrict__ E,
+                                         float* __restrict__ X) {
   const int w = blockIdx.x;
-  const int D = 2 * Nc + 2 * N;
+  const int D = 2 * Nc + 2 * N + (E ? 4 : 0);
   float* x = X + long(w) * D;
+  if (E && threadIdx.x == 0) {
+    x[2 * Nc + 2 * N + 0] = float(E[w * 3 + 0].x);
+    x[2 * Nc + 2 * N + 1] = float(E[w * 3 + 0].y);
+    x[2 * Nc + 2 * N + 2] = float(E[w * 3 + 2].x);
+    x[2 * Nc + 2 * N + 3] = float(E[w * 3 + 2].y);
+  }
   for (int i = threadIdx.x; i < Nc; i += blockDim.x) {
     const c128 v = vb[long(w) * ldv + i];
     x[i] = float(v.x);
@@ -505,13 +513,13 @@ extern "C" int afqmc_mlp_train_step(afqmc_mlp h, const float* X, const float* t,
 }
 
 extern "C" int afqmc_exchange_features(const afqmc_c128* vbias, long ldv, const afqmc_c128* G,
-                                       long ldG, int N, int M, int Nc, int W, float* X,
-                                       afqmc_stream stream) {
+                                       long ldG, int N, int M, int Nc, int W,
+                                       const afqmc_c128* E, float* X, afqmc_stream stream) {
   AFQMC_CHECK_ARG(vbias && G && X && N > 0 && M >= N && Nc > 0 && W >= 0,
                   "afqmc_exchange_features: bad argument");
   if (W == 0) return AFQMC_OK;
   exchange_features_kernel<<<W, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
       reinterpret_cast<const c128*>(vbias), ldv, reinterpret_cast<const c128*>(G), ldG, N, M, Nc,
-      W, X);
+      W, reinterpret_cast<const c128*>(E), X);
   return launch_status("exchange_features_kernel");
 }

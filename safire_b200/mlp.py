@@ -112,12 +112,14 @@ class ExchangeMLP:
         return hist
 
 
-def exchange_features(vbias, G, N, M, stream=None):
-    """X [W][2 Nc + 2 N] (FP32) from vbias [W][Nc] and the compact density matrix G [W][..]."""
+def exchange_features(vbias, G, N, M, E=None, stream=None):
+    """X [W][2 Nc + 2 N (+ 4 with E)] (FP32) from vbias [W][Nc], the compact density matrix
+    G [W][..] and optionally the walkers' E1 and EJ (E [W][3])."""
     W, Nc = vbias.shape
-    X = torch.empty((W, 2 * Nc + 2 * N), dtype=torch.float32, device=vbias.device)
+    D = 2 * Nc + 2 * N + (4 if E is not None else 0)
+    X = torch.empty((W, D), dtype=torch.float32, device=vbias.device)
     call("afqmc_exchange_features", _p(vbias), int(vbias.stride(0)), _p(G), int(G.stride(0)),
-         int(N), int(M), int(Nc), int(W), _p(X), _s(stream))
+         int(N), int(M), int(Nc), int(W), _p(E), _p(X), _s(stream))
     return X
 
 
@@ -125,12 +127,14 @@ class ExchangeControlVariate:
     """Multi-fidelity exchange energy for a Simulation (safire_b200.driver): collect pairs during
     equilibration, fit, then measure with the exact exchange on a random fraction of walkers."""
 
-    def __init__(self, sim, hidden=512, fraction=1.0 / 8, seed=0):
+    def __init__(self, sim, hidden=512, fraction=1.0 / 8, seed=0, scalars=False):
+        """scalars: also feed each walker's E1 and EJ to the network."""
         self.sim = sim
         ham = sim.ham
         self.N, self.M, self.Nc = ham.nup, ham.M, ham.Nc
         self.nel = ham.nel
-        self.mlp = ExchangeMLP(2 * self.Nc + 2 * self.N, hidden, seed)
+        self.scalars = scalars
+        self.mlp = ExchangeMLP(2 * self.Nc + 2 * self.N + (4 if scalars else 0), hidden, seed)
         self.fraction = fraction
         self.rng = np.random.default_rng(seed)
         self.X, self.y = [], []
@@ -138,15 +142,21 @@ class ExchangeControlVariate:
         self._v = torch.empty((sim.wset.W, self.Nc), dtype=torch.complex128, device=dev)
 
     def _features(self):
-        """G of the walkers, their vbias (FP64) and the features."""
+        """G of the walkers, their vbias, E1 and EJ (E [W][3], EXX left zero) and the features.
+        EJ comes from the Coulomb vector the force bias already holds (Kl = vbias / (sqrt(dt) a)
+        with a = 2 for CLOSED walkers and EJ = sclj / 2 sum_n Kl^2 with sclj = a^2): EJ =
+        sum_n vbias_n^2 / (2 dt) for either walker type."""
         sim = self.sim
         G, _ = sim.wfn.MixedDensityMatrix(sim.wset)
-        sim.ham.vbias(G, self._v, sim.dt)
-        return G, exchange_features(self._v, G, self.N, self.M)
+        sim.ham.vbias(G, self._v, sim.dt, precision=sim.precision)
+        E = torch.empty((sim.wset.W, 3), dtype=torch.complex128, device=G.device)
+        sim.ham.energy(E, G, addH1=True, addEJ=False, addEXX=False, precision=sim.precision)
+        E[:, 2] = (self._v * self._v).sum(1) / (2.0 * sim.dt)
+        return G, E, exchange_features(self._v, G, self.N, self.M, E if self.scalars else None)
 
     def collect(self):
         """One training sample per walker: features and the exact exchange energy."""
-        G, X = self._features()
+        G, _, X = self._features()
         E = torch.empty((self.sim.wset.W, 3), dtype=torch.complex128, device=G.device)
         self.sim.ham.energy(E, G, addH1=False, addEJ=False, addEXX=True,
                             precision=self.sim.precision)
@@ -164,14 +174,9 @@ class ExchangeControlVariate:
         exact exchange).  Returns (energy, {'exx_mf', 'exx_exact' (when computed)})."""
         sim = self.sim
         W = sim.wset.W
-        G, X = self._features()
+        # E1 and EJ exactly for every walker
+        G, E, X = self._features()
         dev = G.device
-        E = torch.empty((W, 3), dtype=torch.complex128, device=dev)
-        # E1 and EJ exactly for every walker: EJ from the Coulomb vector the force bias already
-        # holds (Kl = vbias / (sqrt(dt) a) with a = 2 for CLOSED walkers, EJ = sclj/2 sum Kl^2
-        # with sclj = a^2): EJ = sum_n vbias_n^2 / (2 dt) for either walker type
-        sim.ham.energy(E, G, addH1=True, addEJ=False, addEXX=False, precision=sim.precision)
-        E[:, 2] = (self._v * self._v).sum(1) / (2.0 * sim.dt)
         w = sim.wset.properties()[:, capi.WEIGHT]
         f = self.mlp.predict(X).double()
         k = max(1, int(round(self.fraction * W)))

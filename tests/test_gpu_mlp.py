@@ -73,6 +73,11 @@ def test_exchange_features(cuda):
     d = np.stack([Gh[:, a * M + a] for a in range(N)], 1)
     ref = np.concatenate([vh.real, vh.imag, d.real, d.imag], 1).astype(np.float32)
     assert np.array_equal(X, ref)
+    E = torch.as_tensor(rs.standard_normal((W, 3)) + 1j * rs.standard_normal((W, 3)), device=cuda)
+    XE = exchange_features(v, G, N, M, E).cpu().numpy()
+    Eh = E.cpu().numpy()
+    extra = np.stack([Eh[:, 0].real, Eh[:, 0].imag, Eh[:, 2].real, Eh[:, 2].imag], 1)
+    assert np.array_equal(XE, np.concatenate([ref, extra.astype(np.float32)], 1))
 
 
 def test_control_variate_on_a_run(cuda):
