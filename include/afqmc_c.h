@@ -354,6 +354,17 @@ int afqmc_phmsd_destroy(afqmc_phmsd trial);
 int afqmc_phmsd_log_overlap(afqmc_phmsd trial, const afqmc_c128* wbuf, long ldS,
                             afqmc_c128* ovlp, int W, afqmc_stream stream);
 
+/* The particle-hole structure of one spin of a determinant expansion given as occupation lists
+ * (the ph_excitations that PHMSD's factory builds, Excitations.hpp:207-554), host only:
+ * occ [ndet][nel] holds each determinant's occupied active orbitals in the column order its
+ * coefficient refers to; refc [nel] the reference (electron i in orbital refc[i]).  Outputs:
+ * det_index [ndet] (0 = the reference, else the unique excitation), sign [ndet] (+-1: multiply the
+ * coefficient by it for afqmc_phmsd_create, whose determinants replace hole h_e by particle p_e
+ * in place, holes and particles ascending), *nuniq, nex [ndet] (excitation number of unique
+ * excitations 1..nuniq-1) and exc [ndet * 2 * nel] (their holes then particles), ordered by
+ * excitation number and first appearance. */
+int afqmc_phmsd_excitations(int nact, int nel, const int* refc, int ndet, const int* occ,
+                            int* det_index, double* sign, int* nuniq, int* nex, int* exc);
 /* dims[6] = {M, nup, ndn, nact_up, nact_dn, Nc (0 before afqmc_phmsd_set_hamiltonian)} */
 int afqmc_phmsd_info(afqmc_phmsd trial, int* dims);
 

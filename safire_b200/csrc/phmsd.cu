@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -1789,3 +1790,92 @@ extern "C" int afqmc_phmsd_vbias(afqmc_phmsd h, const afqmc_c128* G, afqmc_c128*
   cudaSetDevice(prev);
   return st;
 }
+
+// ---------------------------------------------------------------------------------------------
+// Particle-hole structure of a determinant expansion given as occupation lists (what the
+// PHMSD factory builds into ph_excitations from the wavefunction file, Wavefunction.cpp:349-495,
+// Excitations.hpp:207-554): host logic.
+// ---------------------------------------------------------------------------------------------
+namespace {
+// parity of the permutation that sorts v (number of inversions mod 2)
+int parity(const std::vector<int>& v) {
+  int inv = 0;
+  for (size_t i = 0; i < v.size(); ++i)
+    for (size_t j = i + 1; j < v.size(); ++j) inv += v[i] > v[j];
+  return inv & 1;
+}
+}  // namespace
+
+extern "C" int afqmc_phmsd_excitations(int nact, int nel, const int* refc, int ndet,
+                                       const int* occ, int* det_index, double* sign, int* nuniq,
+                                       int* nex, int* exc) {
+  AFQMC_CHECK_ARG(nact > 0 && nel >= 0 && nel <= nact && ndet >= 0 && refc && nuniq && nex &&
+                      (ndet == 0 || (occ && det_index && sign && exc)),
+                  "afqmc_phmsd_excitations: bad argument");
+  std::vector<int> where(nact, -1);  // electron of each reference orbital
+  for (int i = 0; i < nel; ++i) {
+    AFQMC_CHECK_ARG(refc[i] >= 0 && refc[i] < nact && where[refc[i]] < 0,
+                    "afqmc_phmsd_excitations: reference orbital %d of electron %d invalid or "
+                    "repeated", refc[i], i);
+    where[refc[i]] = i;
+  }
+  std::vector<int> ref(refc, refc + nel);
+  // unique excitations per excitation number, in order of first appearance
+  std::vector<std::map<std::vector<int>, int>> seen;
+  std::vector<std::vector<std::vector<int>>> lists;
+  std::vector<std::pair<int, int>> key(ndet);  // (n, position in lists[n])
+  std::vector<char> mark(nact);
+  for (int k = 0; k < ndet; ++k) {
+    const int* o = occ + size_t(k) * nel;
+    std::fill(mark.begin(), mark.end(), 0);
+    for (int i = 0; i < nel; ++i) {
+      AFQMC_CHECK_ARG(o[i] >= 0 && o[i] < nact && !mark[o[i]],
+                      "afqmc_phmsd_excitations: determinant %d: orbital %d invalid or repeated",
+                      k, o[i]);
+      mark[o[i]] = 1;
+    }
+    std::vector<int> holes, parts;
+    for (int i = 0; i < nel; ++i)
+      if (!mark[refc[i]]) holes.push_back(i);
+    for (int x = 0; x < nact; ++x)
+      if (mark[x] && where[x] < 0) parts.push_back(x);
+    const int n = int(holes.size());
+    AFQMC_CHECK_ARG(n <= PH_NEX_MAX, "afqmc_phmsd_excitations: determinant %d is a %d-fold "
+                                      "excitation (at most %d)", k, n, PH_NEX_MAX);
+    // the Woodbury determinant: reference columns with hole h_e replaced by particle p_e (both
+    // ascending); its sign relative to the determinant in the given column order
+    std::vector<int> L = ref;
+    for (int e = 0; e < n; ++e) L[holes[e]] = parts[e];
+    std::vector<int> given(o, o + nel);
+    sign[k] = ((parity(L) + parity(given)) & 1) ? -1.0 : 1.0;
+    if (int(seen.size()) <= n) {
+      seen.resize(n + 1);
+      lists.resize(n + 1);
+    }
+    std::vector<int> e = holes;
+    e.insert(e.end(), parts.begin(), parts.end());
+    auto it = seen[n].find(e);
+    if (it == seen[n].end()) {
+      it = seen[n].emplace(e, int(lists[n].size())).first;
+      lists[n].push_back(e);
+    }
+    key[k] = {n, it->second};
+  }
+  // unique index: 0 the reference, then by excitation number
+  std::vector<int> first(lists.size() + 1, 1);
+  int u = 1, pos = 0;
+  for (size_t n = 1; n < lists.size(); ++n) {
+    first[n] = u;
+    for (const auto& e : lists[n]) {
+      nex[u - 1] = int(n);
+      std::copy(e.begin(), e.end(), exc + pos);
+      pos += int(e.size());
+      ++u;
+    }
+  }
+  *nuniq = u;
+  for (int k = 0; k < ndet; ++k)
+    det_index[k] = key[k].first == 0 ? 0 : first[key[k].first] + key[k].second;
+  return AFQMC_OK;
+}
+

@@ -175,3 +175,39 @@ def make_phmsd_workload(seed=0, W=512, M=120, N=30, Nc=960, decay=0.99, dt=0.005
     wl = Workload("phmsd", M, N, N, Nc, W, dt, COLLINEAR, h1[None].astype(np.complex128),
                   Likn[None], 0.0, PsiT)
     return wl, trial
+
+
+def phmsd_trial_from_occupations(M, orbmat, refc, occ_up, occ_dn, coef):
+    """A PHMSDTrial from a determinant expansion given as occupation lists: orbmat[s] [nact_s][M]
+    (active orbitals, conjugate-transposed), refc[s] [N_s] the reference, occ_up / occ_dn
+    [ndet][N_s] each determinant's occupied active orbitals in the column order of its coefficient
+    coef [ndet].  The particle-hole structure comes from afqmc_phmsd_excitations (the library's
+    host code); the permutation signs are folded into the coefficients."""
+    import ctypes as C
+
+    from . import capi
+    occ = [np.ascontiguousarray(occ_up, dtype=np.int32), np.ascontiguousarray(occ_dn, dtype=np.int32)]
+    ndet = occ[0].shape[0]
+    coef = np.asarray(coef, dtype=np.complex128).copy()
+    exc, dets = [dict(), dict()], []
+    for s in (0, 1):
+        nel = occ[s].shape[1]
+        rc = np.ascontiguousarray(refc[s], dtype=np.int32)
+        di = np.zeros(ndet, np.int32)
+        sg = np.zeros(ndet, np.float64)
+        nu = C.c_int()
+        nx = np.zeros(max(ndet, 1), np.int32)
+        ex = np.zeros(max(ndet * 2 * nel, 1), np.int32)
+        ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+        capi.call("afqmc_phmsd_excitations", int(orbmat[s].shape[0]), int(nel), ptr(rc),
+                  int(ndet), ptr(occ[s]), ptr(di), ptr(sg), C.byref(nu), ptr(nx), ptr(ex))
+        coef *= sg
+        pos = 0
+        for u in range(1, nu.value):
+            n = int(nx[u - 1])
+            exc[s].setdefault(n, []).append(ex[pos:pos + 2 * n].copy())
+            pos += 2 * n
+        exc[s] = {n: np.array(v, dtype=np.int32).reshape(-1, 2 * n) for n, v in exc[s].items()}
+        dets.append(di)
+    return PHMSDTrial(M, occ[0].shape[1], occ[1].shape[1], [np.asarray(o) for o in orbmat],
+                      [np.asarray(r, dtype=np.int32) for r in refc], exc, dets[0], dets[1], coef)

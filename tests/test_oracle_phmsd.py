@@ -167,3 +167,34 @@ def test_phmsd_density_matrix_vs_single_determinants():
             Gact = G[w, off:off + na]
             assert np.allclose(t.orbmat[s].T @ Gact, full, atol=1e-10), s
         assert np.isclose(np.exp(logov[w]), den, rtol=1e-10)
+
+
+def test_excitations_from_occupation_lists():
+    """afqmc_phmsd_excitations (host code of the library, no GPU) turns occupation lists in
+    arbitrary column order into the particle-hole structure: the Woodbury log overlap of the
+    resulting trial equals the sum over the determinants as given, sum_k c_k det(D_k^H S)."""
+    from safire_b200.synth import phmsd_trial_from_occupations
+    rs = np.random.default_rng(9)
+    M, nup, ndn, nact, ndet = 14, 4, 3, 10, 25
+    A = np.linalg.qr(rs.standard_normal((M, M)) + 1j * rs.standard_normal((M, M)))[0]
+    orb = [np.ascontiguousarray(A[:, :nact].conj().T)] * 2
+    refc = [np.arange(nup), np.arange(ndn)]
+    occ = []
+    for nel in (nup, ndn):
+        lst = [np.arange(nel)]
+        while len(lst) < ndet:
+            o = np.sort(rs.choice(nact, nel, replace=False))
+            if rs.random() < 0.5:
+                rs.shuffle(o)  # the coefficient refers to this column order
+            lst.append(o)
+        occ.append(np.array(lst))
+    coef = rs.standard_normal(ndet) + 1j * rs.standard_normal(ndet)
+    t = phmsd_trial_from_occupations(M, orb, refc, occ[0], occ[1], coef)
+    W = 3
+    Su = rs.standard_normal((W, M, nup)) + 1j * rs.standard_normal((W, M, nup))
+    Sd = rs.standard_normal((W, M, ndn)) + 1j * rs.standard_normal((W, M, ndn))
+    logov, _ = P.phmsd_log_overlap(t, Su, Sd)
+    for w in range(W):
+        tot = sum(coef[k] * np.linalg.det(orb[0][occ[0][k]] @ Su[w]) *
+                  np.linalg.det(orb[1][occ[1][k]] @ Sd[w]) for k in range(ndet))
+        assert abs(np.exp(logov[w]) - tot) <= 1e-10 * abs(tot)
