@@ -212,6 +212,13 @@ int afqmc_wfn_log_overlap(afqmc_ham ham, afqmc_wset ws, afqmc_c128* ovlp, afqmc_
  * set_properties != 0 also stores OVLP, E1, EXX, EJ on the walkers (NOMSD.cpp:67-79). */
 int afqmc_wfn_energy(afqmc_ham ham, afqmc_wset ws, afqmc_c128* E, afqmc_c128* ovlp,
                      int set_properties, int precision, afqmc_stream stream);
+/* The OneRDM observable of the MixedEstimator (Estimators/Observables/onerdm.hpp:39-64,
+ * MixedEstimator.hpp:42-108), single reference: rdm [nspin][M][M] (device, written) =
+ * sum_w w_w G_w with G_w[i][k] = sum_a PsiT[a][i] Gc_w[a][k] the full mixed density matrix built
+ * from the compact one G [W][ldG] of afqmc_wfn_density_matrix, w the walkers' weights; the caller
+ * divides by the weight sum (as the reference's Measurements do).  No RotationMatrix. */
+int afqmc_wfn_onerdm(afqmc_ham ham, afqmc_wset ws, const afqmc_c128* G, long ldG,
+                     afqmc_c128* rdm, afqmc_stream stream);
 /* NOMSD::vMF — NOMSD.cpp:437-465: vbias of the trial's own density matrix.  host [Nc]. */
 int afqmc_wfn_vmf(afqmc_ham ham, double dt, afqmc_c128* vMF_host);
 

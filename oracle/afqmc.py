@@ -824,3 +824,22 @@ def run_afqmc(wfn: NOMSD, prop: Propagator, ws: WalkerSet, rp: RunParams, field_
         if on_step is not None:
             on_step(step, ws, Eshift)
     return energies, Eshift
+
+
+def onerdm(wfn: NOMSD, ws: WalkerSet):
+    """The MixedEstimator's OneRDM, single reference (Estimators/Observables/onerdm.hpp:39-64,
+    MixedEstimator.hpp:42-108): sum_w w_w G_w per spin block with the full mixed density matrix
+    G_w = (S_w (PsiT S_w)^{-1} PsiT)^T (density_matrix.hpp:535-601, compact = false)."""
+    blocks = [ws.SA] if ws.walker_type != COLLINEAR else [ws.SA, ws.SB]
+    out = []
+    off = 0
+    for S in blocks:
+        N = S.shape[2]
+        PsiT = wfn.PsiT[0][off:off + N] if len(wfn.PsiT) == 1 else wfn.PsiT[len(out)]
+        acc = np.zeros((S.shape[1], S.shape[1]), complex)
+        for w in range(S.shape[0]):
+            Mf = S[w] @ np.linalg.inv(PsiT @ S[w]) @ PsiT
+            acc += ws.props[w, WEIGHT] * Mf.T
+        out.append(acc)
+        off += N
+    return np.stack(out)

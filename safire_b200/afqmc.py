@@ -297,6 +297,17 @@ class NOMSD:
              int(set_properties), precision, _stream(stream))
         return E, ov
 
+    def OneRDM(self, wset: WalkerSet, G=None, stream=None):
+        """sum_w w_w G_w (full mixed density matrices [nspin][M][M], device) and sum_w w_w."""
+        if G is None:
+            G, _ = self.MixedDensityMatrix(wset, stream=stream)
+        nspin = 2 if self.ham.walker_type == COLLINEAR else 1
+        rdm = torch.empty((nspin, self.ham.M, self.ham.M), dtype=torch.complex128,
+                          device=G.device)
+        call("afqmc_wfn_onerdm", self.ham.handle, wset.handle, _ptr(G), int(G.stride(0)),
+             _ptr(rdm), _stream(stream))
+        return rdm, wset.properties()[:, capi.WEIGHT].sum()
+
     def vMF(self, dt):
         v = np.zeros(self.ham.Nc, dtype=np.complex128)
         call("afqmc_wfn_vmf", self.ham.handle, float(dt), _host_ptr(v))

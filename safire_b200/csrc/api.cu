@@ -821,6 +821,44 @@ extern "C" int afqmc_wfn_density_matrix(afqmc_ham h, afqmc_wset ws, afqmc_c128* 
   return wfn_density_matrix(h, ws, s, (c128*)G, long(h->nel_tot) * h->M, (c128*)ovlp, (c128*)T.p);
 }
 
+extern "C" int afqmc_wfn_onerdm(afqmc_ham h, afqmc_wset ws, const afqmc_c128* G, long ldG,
+                                afqmc_c128* rdm, afqmc_stream stream) {
+  AFQMC_CHECK_ARG(h && ws && G && rdm, "afqmc_wfn_onerdm: null argument");
+  AFQMC_CHECK_ARG(wset_matches(h, ws), "afqmc_wfn_onerdm: walker set / Hamiltonian mismatch");
+  AFQMC_CHECK_ARG(ldG >= long(h->nel_tot) * h->M, "afqmc_wfn_onerdm: ldG %ld < nel M", ldG);
+  DeviceGuard g(h->device);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int M = h->M, W = ws->W;
+  int nmax = h->nel[0] > h->nel[1] ? h->nel[0] : h->nel[1];
+  Scratch Gs;
+  AFQMC_TRY(Gs.get(sizeof(c128) * size_t(nmax > 0 ? nmax : 1) * M, s));
+  for (int sp = 0; sp < h->nspin; ++sp) {
+    const int Ns = h->nel[sp];
+    c128* out = reinterpret_cast<c128*>(rdm) + size_t(sp) * M * M;
+    if (Ns == 0) {
+      AFQMC_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(c128) * M * M, s));
+      continue;
+    }
+    // Gsum [Ns][M] = sum_w w_w G_w (the weights are the walkers' WEIGHT column)
+    GemmParams a{};
+    a.m = 1; a.n = Ns * M; a.k = W;
+    a.A = ws->buf + ws->prop0 + AFQMC_WEIGHT; a.lda = ws->walker_size;
+    a.B = reinterpret_cast<const c128*>(G) + long(h->el_off[sp]) * M; a.ldb = ldG;
+    a.C = reinterpret_cast<c128*>(Gs.p); a.ldc = Ns * M;
+    a.alpha = cmk(1, 0); a.beta = cmk(0, 0);
+    AFQMC_TRY(zgemm(s, 1, GT, false, GN, false, a));
+    // full G [M][M] = PsiT^T Gsum  (G[i][k] = sum_a PsiT[a][i] Gc[a][k])
+    GemmParams b{};
+    b.m = M; b.n = M; b.k = Ns;
+    b.A = h->PsiT + long(h->el_off[sp]) * M; b.lda = M;
+    b.B = reinterpret_cast<const c128*>(Gs.p); b.ldb = M;
+    b.C = out; b.ldc = M;
+    b.alpha = cmk(1, 0); b.beta = cmk(0, 0);
+    AFQMC_TRY(zgemm(s, 1, GT, false, GN, false, b));
+  }
+  return AFQMC_OK;
+}
+
 extern "C" int afqmc_wfn_log_overlap(afqmc_ham h, afqmc_wset ws, afqmc_c128* ovlp,
                                      afqmc_stream stream) {
   AFQMC_CHECK_ARG(h && ws && ovlp, "afqmc_wfn_log_overlap: null argument");
