@@ -39,7 +39,7 @@ BLOCK = 10  # AFQMC steps per bench step
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
@@ -405,8 +405,13 @@ def run_ours(args):
     sim.use_graph = not args.no_graph
     if prec == A.PREC_MIXED and args.exchange_split != 3:
         sim.ham.set_exchange_split(args.exchange_split)
+    tuned = None
     if prec == A.PREC_MIXED and args.taylor_mode != 1:
         sim.ham.set_taylor_fused(args.taylor_mode)
+    elif prec == A.PREC_MIXED:
+        # the library's autotuner times each Taylor variant on these walkers (state restored)
+        best, ms = sim.autotune()
+        tuned = {"taylor_mode": best, "step_ms": ms}
 
     t_ms, launches, clk = _timed_blocks(sim, args.steps, args.warmup, world, local,
                                         ClockSampler(local))
@@ -446,6 +451,8 @@ def run_ours(args):
                 "peak_source": peak_src, "flops_per_launch": flops[top],
                 "block_share_ms": block_share}
 
+    # the synthetic system's total weight collapses after ~200 steps: restart from the trial
+    sim.restart()
     e2e = None if args.no_e2e else _e2e(sim, W, Nc, args.steps, world, prec)
 
     # the plain complex128 path on the same inputs, timed the same way: the mixed-vs-FP64 ratio
@@ -482,7 +489,9 @@ def run_ours(args):
                                    "block of 10 steps (ortho/5, comb/10, energy/10)",
                        "precision": args.precision, "global_walkers": W * world,
                        "exchange_split": args.exchange_split if prec == A.PREC_MIXED else None,
-                       "taylor_mode": args.taylor_mode if prec == A.PREC_MIXED else None,
+                       "taylor_mode": (tuned["taylor_mode"] if tuned else args.taylor_mode)
+                                      if prec == A.PREC_MIXED else None,
+                       "autotune": tuned,
                        "step_graph": not args.no_graph,
                        "parallelism": f"walker dp{world}",
                        "l2": "inputs larger than L2 (V 655 MB, Likn 512 MB per step)"},

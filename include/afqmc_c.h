@@ -286,6 +286,13 @@ int afqmc_prop_step_dev(afqmc_prop prop, afqmc_wset ws, const double* Eshift_dev
 #define AFQMC_STEP_KEEP_G 2
 int afqmc_prop_step_flags(afqmc_prop prop, afqmc_wset ws, const double* Eshift_dev,
                           const double* uniforms, int flags, afqmc_stream stream);
+/* Autotuner: times the mixed-precision step on these walkers with each Taylor propagation
+ * variant (0 per-term GEMMs, 2 fused with one walker per CTA in flight, 3 fused with two) and keeps
+ * the fastest for the Hamiltonian; walkers, field counter and bound statistics are restored, so
+ * the run continues as if it had not been called.  *best = chosen mode (-1: FP64 or PHMSD,
+ * nothing to tune); ms [3] (may be NULL) = the step time of each variant.  Synchronous. */
+int afqmc_prop_autotune(afqmc_prop prop, afqmc_wset ws, int* best, float* ms,
+                        afqmc_stream stream);
 /* AFQMCBasePropagator::Orthogonalize (cpp:735-741): QR re-orthonormalisation then OVLP refresh. */
 int afqmc_prop_orthogonalize(afqmc_prop prop, afqmc_wset ws, afqmc_stream stream);
 /* Seeds / advances the device field generator (Philox4x32-10, counter = step). */

@@ -391,6 +391,15 @@ class Propagator:
     def set_field_seed(self, seed):
         call("afqmc_prop_set_field_seed", self.handle, int(seed))
 
+    def autotune(self, wset: WalkerSet, stream=None):
+        """Picks the fastest Taylor propagation variant for these walkers (mixed precision);
+        returns (mode or -1, {mode: step ms}).  The walkers are left as they were."""
+        best = C.c_int()
+        ms = np.zeros(3, dtype=np.float32)
+        call("afqmc_prop_autotune", self.handle, wset.handle, C.byref(best), _host_ptr(ms),
+             _stream(stream))
+        return best.value, {m: float(t) for m, t in zip((0, 2, 3), ms)}
+
     def set_trial(self, trial, vMF=None):
         """Steps with a PHMSD trial (vbias and overlaps from it); vMF host [Nc] or None keeps
         the current mean field.  trial None detaches."""

@@ -1309,6 +1309,77 @@ extern "C" int afqmc_prop_step_flags(afqmc_prop pr, afqmc_wset ws, const double*
   return prop_step(pr, ws, 0.0, Eshift_dev, u, flags, reinterpret_cast<cudaStream_t>(stream));
 }
 
+extern "C" int afqmc_prop_autotune(afqmc_prop pr, afqmc_wset ws, int* best, float* ms,
+                                   afqmc_stream stream) {
+  AFQMC_CHECK_ARG(pr && ws && best, "afqmc_prop_autotune: null argument");
+  AFQMC_CHECK_ARG(wset_matches(pr->ham, ws), "afqmc_prop_autotune: walker set / Hamiltonian mismatch");
+  AFQMC_CHECK_ARG(ws->W <= pr->maxW, "afqmc_prop_autotune: too many walkers");
+  DeviceGuard g(pr->device);
+  afqmc_ham_s* h = pr->ham;
+  *best = -1;
+  if (pr->p.precision != AFQMC_PREC_MIXED || pr->ph) return AFQMC_OK;  // nothing to choose
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const size_t nbuf = size_t(ws->W) * ws->walker_size;
+  // the state a step changes: walkers (with their properties), the field counter, the bound
+  // statistics; saved here and restored after every trial, so that tuning leaves no trace
+  Scratch save, aux;
+  AFQMC_TRY(save.get(sizeof(c128) * nbuf, s));
+  AFQMC_TRY(aux.get(sizeof(unsigned long long) * 9, s));
+  unsigned long long* auxp = reinterpret_cast<unsigned long long*>(aux.p);
+  AFQMC_CUDA_TRY(cudaMemcpyAsync(save.p, ws->buf, sizeof(c128) * nbuf, cudaMemcpyDeviceToDevice, s));
+  AFQMC_CUDA_TRY(cudaMemcpyAsync(auxp, pr->counter, sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToDevice, s));
+  AFQMC_CUDA_TRY(cudaMemcpyAsync(auxp + 1, pr->stats, 8 * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToDevice, s));
+  auto restore = [&]() -> int {
+    AFQMC_CUDA_TRY(cudaMemcpyAsync(ws->buf, save.p, sizeof(c128) * nbuf, cudaMemcpyDeviceToDevice, s));
+    AFQMC_CUDA_TRY(cudaMemcpyAsync(pr->counter, auxp, sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToDevice, s));
+    AFQMC_CUDA_TRY(cudaMemcpyAsync(pr->stats, auxp + 1, 8 * sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToDevice, s));
+    return AFQMC_OK;
+  };
+  cudaEvent_t e0, e1;
+  AFQMC_CUDA_TRY(cudaEventCreate(&e0));
+  AFQMC_CUDA_TRY(cudaEventCreate(&e1));
+  // Taylor propagation variants: 0 per-term GEMMs, 2 fused with one walker per CTA in flight,
+  // 3 fused with two (the fused kernel's occupancy / L2 working-set trade-off depends on W)
+  const int modes[3] = {0, 2, 3};
+  float best_ms = 1e30f;
+  int st = AFQMC_OK;
+  for (int mi = 0; mi < 3 && !st; ++mi) {
+    if (!h->mixed) {
+      EnergyArgs a = energy_args(h, nullptr, 0);
+      if ((st = mixed_ham_create(&h->mixed, a, s))) break;
+    }
+    if ((st = mixed_set_taylor_mode(h->mixed, modes[mi]))) break;
+    float t = 0.f;
+    for (int rep = 0; rep < 3 && !st; ++rep) {  // the first repetition warms up
+      if ((st = restore())) break;
+      if (rep > 0 && cudaEventRecord(e0, s) != cudaSuccess) st = AFQMC_ERR_CUDA;
+      if (!st) st = prop_step(pr, ws, 0.0, nullptr, nullptr, 0, s);
+      if (!st && rep > 0) {
+        float x = 0.f;
+        if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&x, e0, e1) != cudaSuccess)
+          st = AFQMC_ERR_CUDA;
+        t += x;
+      }
+    }
+    if (ms) ms[mi] = t / 2;
+    if (!st && t / 2 < best_ms) {
+      best_ms = t / 2;
+      *best = modes[mi];
+    }
+  }
+  if (!st && *best >= 0) st = mixed_set_taylor_mode(h->mixed, *best);
+  const int st2 = restore();
+  if (cudaStreamSynchronize(s) != cudaSuccess && !st) st = AFQMC_ERR_CUDA;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st ? st : st2;
+}
+
 extern "C" int afqmc_prop_orthogonalize(afqmc_prop pr, afqmc_wset ws, afqmc_stream stream) {
   AFQMC_CHECK_ARG(pr && ws, "afqmc_prop_orthogonalize: null handle");
   AFQMC_CHECK_ARG(wset_matches(pr->ham, ws), "afqmc_prop_orthogonalize: mismatch");

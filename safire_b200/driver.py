@@ -86,6 +86,20 @@ class StepGraph:
         return self.replayed
 
 
+def _initial_state(wfn, wset, precision):
+    """Initial energies, overlaps and seeded pseudo energies of the walkers, and Eshift
+    (execute.cpp:171-184)."""
+    wfn.Energy(wset, set_properties=True, precision=precision)
+    torch.cuda.synchronize()
+    e1, exx, ej = (wset.getProperty(p) for p in (E1, EXX, EJ))
+    wset.setProperty(PSEUDO_ELOC, e1 + exx + ej)
+    w = wset.getProperty(0)
+    sums = torch.tensor([np.sum(w * (e1 + exx + ej)), np.sum(w)], dtype=torch.complex128,
+                        device=wset.buffer.device)
+    sums = _sum_over_ranks(sums).cpu().numpy()
+    return float((sums[0] / sums[1]).real)
+
+
 @dataclass
 class Simulation:
     ham: A.HamiltonianOperations
@@ -130,16 +144,7 @@ class Simulation:
         # the comb's generator is the same on every rank (the reference's root draws it); the
         # auxiliary fields of each rank's walkers come from that rank's own stream
         walker_rng = A.HostRandomGenerator(A.split_seed(rp.seed, 0, 0))
-        # initial energy, seeded pseudo energy and Eshift (execute.cpp:171-184)
-        wfn.Energy(wset, set_properties=True, precision=precision)
-        torch.cuda.synchronize()
-        e1, exx, ej = (wset.getProperty(p) for p in (E1, EXX, EJ))
-        wset.setProperty(PSEUDO_ELOC, e1 + exx + ej)
-        w = wset.getProperty(0)
-        sums = torch.tensor([np.sum(w * (e1 + exx + ej)), np.sum(w)], dtype=torch.complex128,
-                            device=wset.buffer.device)
-        sums = _sum_over_ranks(sums).cpu().numpy()
-        Eshift = float((sums[0] / sums[1]).real)
+        Eshift = _initial_state(wfn, wset, precision)
         params = A.default_params(dt=wl.dt, precision=precision, **prop_kw)
         prop = A.Propagator(ham, params, W)
         prop.set_field_seed(A.split_seed(rp.seed, _rank(), 1))
@@ -151,6 +156,22 @@ class Simulation:
         if ph is not None:
             sim.reuse_density = False  # the PHMSD step recomputes its density matrix
         return sim
+
+    def restart(self):
+        """Walkers back at the trial with unit weights, their energies and overlaps, a re-seeded
+        Eshift and step counter; the field and walker generators continue their streams."""
+        self.wset.init_from_trial(self.ham)
+        self.Eshift = _initial_state(self.wfn, self.wset, self.precision)
+        self.step_index = 0
+        self._g_ready = False
+
+    def autotune(self):
+        """Let the library pick the fastest step variant for these walkers (mixed precision);
+        the walkers are left as they were.  Returns (mode, {mode: step ms})."""
+        best, ms = self.prop.autotune(self.wset)
+        self._g_ready = False
+        self.graph = None  # a captured step holds the previous variant's kernels
+        return best, ms
 
     def average_pseudo_energy(self):
         s = _sum_over_ranks(A.pseudo_energy_sums(self.wset, self.dt))

@@ -172,3 +172,31 @@ def test_taylor_fused_vs_per_term(cuda, name, W, Nc, order, mode):
           f"ovlp {eO:.2e}")
     assert eS < 1e-5 and eO < 1e-5
     assert dham.device_error_flag() == 0
+
+
+def test_autotune_leaves_the_run_unchanged(cuda):
+    """The autotuner times every Taylor variant on the live walkers and restores them: a run that
+    autotunes and one that is set to the chosen variant by hand take bit-identical next steps."""
+    import torch
+    from safire_b200 import afqmc as A
+    from safire_b200.driver import RunParams, Simulation
+    from safire_b200.synth import make_workload
+    wl = make_workload("cfg2", W=64)
+    runs = []
+    for tune in (True, False):
+        sim = Simulation.from_workload(wl, W=64, precision=A.PREC_MIXED,
+                                       rp=RunParams(equilibration_steps=0, seed=3))
+        sim.step()
+        sim.step()
+        before = sim.wset.buffer.clone()
+        if tune:
+            best, ms = sim.autotune()
+            assert best in (0, 2, 3) and all(t > 0 for t in ms.values()), (best, ms)
+            assert torch.equal(sim.wset.buffer, before)
+            chosen = best
+        else:
+            sim.ham.set_taylor_fused(chosen)
+        sim._g_ready = False
+        sim.step()
+        runs.append(sim.wset.buffer.clone())
+    assert torch.equal(runs[0], runs[1])
