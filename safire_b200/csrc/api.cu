@@ -579,8 +579,9 @@ extern "C" int afqmc_ham_get_tensors(afqmc_ham h, afqmc_c128* Lnak, afqmc_c128* 
 
 extern "C" int afqmc_ham_vbias(afqmc_ham h, const afqmc_c128* G, afqmc_c128* v, int W, double dt,
                                int precision, afqmc_stream stream) {
-  AFQMC_CHECK_ARG(h && G && v && W >= 0, "afqmc_ham_vbias: bad argument");
-  if (W == 0) return AFQMC_OK;
+  AFQMC_CHECK_ARG(h && W >= 0, "afqmc_ham_vbias: bad argument");
+  if (W == 0) return AFQMC_OK;  // no walkers: nothing is read or written
+  AFQMC_CHECK_ARG(G && v, "afqmc_ham_vbias: null array");
   DeviceGuard g(h->device);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (precision == AFQMC_PREC_MIXED) {
@@ -594,8 +595,9 @@ extern "C" int afqmc_ham_vbias(afqmc_ham h, const afqmc_c128* G, afqmc_c128* v, 
 
 extern "C" int afqmc_ham_vhs(afqmc_ham h, const afqmc_c128* X, afqmc_c128* V, int W, double dt,
                              int precision, afqmc_stream stream) {
-  AFQMC_CHECK_ARG(h && X && V && W >= 0, "afqmc_ham_vhs: bad argument");
-  if (W == 0) return AFQMC_OK;
+  AFQMC_CHECK_ARG(h && W >= 0, "afqmc_ham_vhs: bad argument");
+  if (W == 0) return AFQMC_OK;  // no walkers: nothing is read or written
+  AFQMC_CHECK_ARG(X && V, "afqmc_ham_vhs: null array");
   DeviceGuard g(h->device);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (precision == AFQMC_PREC_MIXED) {
@@ -608,10 +610,11 @@ extern "C" int afqmc_ham_vhs(afqmc_ham h, const afqmc_c128* X, afqmc_c128* V, in
 
 extern "C" int afqmc_ham_energy(afqmc_ham h, const afqmc_c128* G, afqmc_c128* E, int W, int addH1,
                                 int addEJ, int addEXX, int precision, afqmc_stream stream) {
-  AFQMC_CHECK_ARG(h && G && E && W >= 0, "afqmc_ham_energy: bad argument");
+  AFQMC_CHECK_ARG(h && W >= 0, "afqmc_ham_energy: bad argument");
   AFQMC_CHECK_ARG(!addEJ || addEXX, "afqmc_ham_energy: addEJ without addEXX is not implemented "
                                     "(as in Real3IndexFactorization.hpp:589)");
-  if (W == 0) return AFQMC_OK;
+  if (W == 0) return AFQMC_OK;  // no walkers: nothing is read or written
+  AFQMC_CHECK_ARG(G && E, "afqmc_ham_energy: null array");
   DeviceGuard g(h->device);
   return ham_energy(h, reinterpret_cast<cudaStream_t>(stream), (const c128*)G,
                     long(h->nel_tot) * h->M, (c128*)E, W, addH1 != 0, addEJ != 0, addEXX != 0,
