@@ -1161,6 +1161,40 @@ extern "C" int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact
                         det_dn[k] < nuniq_dn,
                     "afqmc_phmsd_create: determinant %d couples (%d, %d) outside (%d, %d)", k,
                     det_up[k], det_dn[k], nuniq_up, nuniq_dn);
+  // Internal order of the unique excitations: by excitation number, then holes, then particles
+  // (a permutation that changes no result).  Neighbouring threads of the energy kernels then
+  // evaluate determinants with the same holes and nearby particles, whose table reads fall on
+  // neighbouring shared-memory words.
+  std::vector<int> exc_sorted[2], det_sorted[2];
+  const int* det_in[2] = {det_up, det_dn};
+  for (int s = 0; s < 2; ++s) {
+    std::vector<int> order(nuniq[s] > 1 ? nuniq[s] - 1 : 0);
+    for (size_t j = 0; j < order.size(); ++j) order[j] = int(j) + 1;
+    auto key_less = [&](int a, int b) {
+      if (nex[s][a] != nex[s][b]) return nex[s][a] < nex[s][b];
+      const int n = nex[s][a];
+      return std::lexicographical_compare(excs[s] + off[s][a], excs[s] + off[s][a] + 2 * n,
+                                          excs[s] + off[s][b], excs[s] + off[s][b] + 2 * n);
+    };
+    std::stable_sort(order.begin(), order.end(), key_less);
+    std::vector<int> newidx(nuniq[s], 0), noff(nuniq[s], 0), nnex(nuniq[s], 0);
+    int pos = 0;
+    for (size_t j = 0; j < order.size(); ++j) {
+      const int u = order[j], v = int(j) + 1, n = nex[s][u];
+      newidx[u] = v;
+      noff[v] = pos;
+      nnex[v] = n;
+      exc_sorted[s].insert(exc_sorted[s].end(), excs[s] + off[s][u], excs[s] + off[s][u] + 2 * n);
+      pos += 2 * n;
+    }
+    det_sorted[s].resize(ndet);
+    for (int k = 0; k < ndet; ++k) det_sorted[s][k] = newidx[det_in[s][k]];
+    off[s] = noff;
+    nex[s] = nnex;
+    excs[s] = exc_sorted[s].data();
+  }
+  det_up = det_sorted[0].data();
+  det_dn = det_sorted[1].data();
   std::unique_ptr<afqmc_phmsd_s> h(new afqmc_phmsd_s);
   cudaGetDevice(&h->device);
   h->M = M;
