@@ -170,6 +170,10 @@ int afqmc_ham_set_exchange_split(afqmc_ham ham, int nsplit);
  * two walkers in flight per CTA chosen by the walker count; 2 / 3 force one / two walkers in
  * flight; 0 launches one batched GEMM per product.  All compute the same sums. */
 int afqmc_ham_set_taylor_fused(afqmc_ham ham, int fused);
+/* Mixed-precision energy: 1 takes EJ's Coulomb vector Kl = sum_{a,k} G Lnak from a complex128
+ * GEMM (one DMMA GEMM per measurement, ~4% of a 10-step block at M=200), 0 (default) from the
+ * traces of the tensor-core exchange tiles. */
+int afqmc_ham_set_coulomb_fp64(afqmc_ham ham, int on);
 
 /* Error word of the tensor-core kernels' bounded device waits (bit 0: a wait on a TMA or MMA
  * completion gave up after about 2 s and the kernel returned without finishing).  0 = none, or

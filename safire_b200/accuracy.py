@@ -36,8 +36,8 @@ def blocked_error(x, nblocks=10):
     return float(m.std(ddof=1) / math.sqrt(nblocks))
 
 
-def run(precision, steps, walkers, equil, seed, exchange_split=3, workload="cfg2"):
-    wl = make_workload(workload)
+def run(precision, steps, walkers, equil, seed, exchange_split=3, workload="cfg2", lscale=0.5):
+    wl = make_workload(workload, lscale=lscale)
     rp = RunParams(equilibration_steps=equil, seed=seed)
     sim = Simulation.from_workload(wl, W=walkers, precision=precision, rp=rp)
     if precision == A.PREC_MIXED and exchange_split != 3:
@@ -49,6 +49,46 @@ def run(precision, steps, walkers, equil, seed, exchange_split=3, workload="cfg2
     return sim.energies, time.time() - t0
 
 
+def lockstep(steps, walkers, equil, seed, workload, lscale, exchange_split=3):
+    """Correlated sampling: the complex128 and the mixed run advance side by side with the same
+    fields, the same Eshift and the same population-control decisions (the comb of the complex128
+    run's weights applied to both walker sets), so the paired energies differ only through the
+    arithmetic of the mixed step.  Returns the two measurement series."""
+    from .population import WalkerRows, exchange_walkers
+    wl = make_workload(workload, lscale=lscale)
+    sims = []
+    for prec in (A.PREC_FP64, A.PREC_MIXED):
+        rp = RunParams(equilibration_steps=equil, seed=seed, population_control_interval=0)
+        sim = Simulation.from_workload(wl, W=walkers, precision=prec, rp=rp)
+        if prec == A.PREC_MIXED and exchange_split != 3:
+            sim.ham.set_exchange_split(exchange_split)
+        sims.append(sim)
+    s64, smx = sims
+    rng = A.HostRandomGenerator(A.split_seed(seed, 0, 0))
+    e64, emx, weights, comp = [], [], [], []
+    for step in range(steps):
+        smx.Eshift = s64.Eshift
+        for sim in sims:
+            sim.step(measure=False)  # propagation, orthogonalisation, Eshift update
+        if step % 10 == 0:
+            w = np.abs(s64.wset.getProperty(0))
+            weights.append(float(w.sum()))
+            off = A.comb(rng, w, walkers)
+            for sim in sims:
+                exchange_walkers(WalkerRows(sim.wset), off, [walkers], 0)
+                sim.wset.normalize_weights()
+                sim._g_ready = False
+        if step >= equil and step % 10 == 0:
+            a, sa, _ = s64.measure()
+            b, sb, _ = smx.measure()
+            e64.append(a)
+            emx.append(b)
+            # per-component difference of the weighted averages (E1, EXX, EJ)
+            comp.append([((sb[i] / sb[3]) - (sa[i] / sa[3])).real for i in range(3)])
+    torch.cuda.synchronize()
+    return np.array(e64), np.array(emx), weights, np.array(comp)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=2000)
@@ -58,14 +98,42 @@ def main(argv=None):
     ap.add_argument("--exchange-split", default="3",
                     help="comma-separated TF32 products per exchange product (3 and/or 1)")
     ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2"])
+    ap.add_argument("--lscale", type=float, default=0.5,
+                    help="Cholesky-vector scale of the synthetic Hamiltonian (0.5: benchmark)")
+    ap.add_argument("--lockstep", action="store_true",
+                    help="correlated sampling: shared fields, Eshift and comb decisions")
     args = ap.parse_args(argv)
+    if args.lockstep:
+        outs = []
+        for split in (int(x) for x in args.exchange_split.split(",")):
+            t0 = time.time()
+            e64, emx, wsum, comp = lockstep(args.steps, args.walkers, args.equil, args.seed,
+                                            args.workload, args.lscale, split)
+            d = emx - e64
+            out = {
+                "mode": "lockstep", "workload": args.workload, "lscale": args.lscale,
+                "steps": args.steps, "walkers": args.walkers, "equilibration_steps": args.equil,
+                "exchange_split": split, "measurements": int(d.size),
+                "E_fp64": float(e64.mean()), "E_fp64_err": blocked_error(e64),
+                "E_mixed": float(emx.mean()), "E_mixed_err": blocked_error(emx),
+                "dE_estimate_mHa": 1e3 * float(d.mean()),
+                "dE_estimate_err_mHa": 1e3 * blocked_error(d),
+                "dE_max_abs_mHa": 1e3 * float(np.abs(d).max()),
+                "dE_components_mHa": {k: 1e3 * float(comp[:, i].mean())
+                                      for i, k in enumerate(("E1", "EXX", "EJ"))},
+                "total_weight_min_max": [min(wsum), max(wsum)],
+                "wall_s": time.time() - t0,
+            }
+            print(json.dumps(out), flush=True)
+            outs.append(out)
+        return outs
     e64, t64 = run(A.PREC_FP64, args.steps, args.walkers, args.equil, args.seed,
-                   workload=args.workload)
+                   workload=args.workload, lscale=args.lscale)
     s64 = np.array([e for _, e in e64])
     outs = []
     for split in (int(x) for x in args.exchange_split.split(",")):
         emx, tmx = run(A.PREC_MIXED, args.steps, args.walkers, args.equil, args.seed, split,
-                       workload=args.workload)
+                       workload=args.workload, lscale=args.lscale)
         smx = np.array([e for _, e in emx])
         n = min(s64.size, smx.size)
         d = smx[:n] - s64[:n]

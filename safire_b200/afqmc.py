@@ -164,6 +164,11 @@ class HamiltonianOperations:
         """3: 3xTF32 exchange contraction (default); 1: plain TF32."""
         call("afqmc_ham_set_exchange_split", self.handle, int(nsplit))
 
+    def set_coulomb_fp64(self, on=True):
+        """Mixed precision: EJ's Coulomb vector from a complex128 GEMM, or (default) from the
+        tensor-core exchange traces."""
+        call("afqmc_ham_set_coulomb_fp64", self.handle, int(bool(on)))
+
     def set_taylor_fused(self, mode):
         """1/True: one persistent kernel for all Taylor products (default); 0/False: one GEMM
         each; 2 / 3: the persistent kernel with one / two walkers in flight per CTA."""

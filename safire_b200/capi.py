@@ -74,6 +74,7 @@ _SIGS = {
     "afqmc_phmsd_info": (i32, [vp, vp]),
     "afqmc_wfn_onerdm": (i32, [vp, vp, vp, i64, vp, vp]),
     "afqmc_prop_autotune": (i32, [vp, vp, vp, vp, vp]),
+    "afqmc_ham_set_coulomb_fp64": (i32, [vp, i32]),
     "afqmc_phmsd_excitations": (i32, [i32, i32, vp, i32, vp, vp, vp, vp, vp, vp]),
     "afqmc_prop_set_phmsd": (i32, [vp, vp, vp]),
     "afqmc_mlp_create": (i32, [i32, i32, u64, C.POINTER(vp)]),

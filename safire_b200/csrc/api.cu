@@ -89,6 +89,7 @@ struct afqmc_ham_s {
   int nel[2] = {0, 0}, el_off[2] = {0, 0}, nel_tot = 0;
   double E0 = 0;
   bool trial_real = false;
+  bool coulomb_fp64 = false;  // mixed precision: EJ's Coulomb vector from a complex128 GEMM
   double* Likn = nullptr;               // [nspin_H2][M][M][Nc]
   c128* Lnak[2] = {nullptr, nullptr};   // [Nc][nel_s][M]
   double* Lnak_r[2] = {nullptr, nullptr};
@@ -376,6 +377,7 @@ EnergyArgs energy_args(afqmc_ham_s* h, const c128* G, long ldG) {
   a.sclj = h->walker_type == AFQMC_CLOSED ? 4.0 : 1.0;
   a.Likn = h->Likn;
   a.nspin_H2 = h->nspin_H2;
+  a.coulomb_fp64 = h->coulomb_fp64;
   return a;
 }
 
@@ -619,6 +621,12 @@ extern "C" int afqmc_ham_energy(afqmc_ham h, const afqmc_c128* G, afqmc_c128* E,
   return ham_energy(h, reinterpret_cast<cudaStream_t>(stream), (const c128*)G,
                     long(h->nel_tot) * h->M, (c128*)E, W, addH1 != 0, addEJ != 0, addEXX != 0,
                     precision);
+}
+
+extern "C" int afqmc_ham_set_coulomb_fp64(afqmc_ham h, int on) {
+  AFQMC_CHECK_ARG(h, "afqmc_ham_set_coulomb_fp64: null handle");
+  h->coulomb_fp64 = on != 0;
+  return AFQMC_OK;
 }
 
 extern "C" int afqmc_ham_set_exchange_split(afqmc_ham h, int nsplit) {

@@ -180,6 +180,24 @@ int energy_fp64(cudaStream_t s, const EnergyArgs& a, c128* E, int W, bool addH1,
       AFQMC_TRY(launch_status("exchange_block_kernel"));
     }
   }
+  if (tc && addEJ && a.coulomb_fp64) {
+    // Kl[w][n] = sum_s sum_{a,k} G[w][a][k] Lnak_s[n][a][k] in complex128 (DMMA), in place of the
+    // traces of the TF32-split exchange tiles
+    bool first = true;
+    for (int sp = 0; sp < a.nspin; ++sp) {
+      const int Ns = a.nel[sp];
+      if (Ns == 0) continue;
+      GemmParams p{};
+      p.m = W; p.n = a.Nc; p.k = Ns * a.M;
+      p.A = a.G + long(a.el_off[sp]) * a.M; p.lda = a.ldG; p.strideA = 0;
+      p.B = a.Lnak_real[sp] ? (const void*)a.Lnak_real[sp] : (const void*)a.Lnak[sp];
+      p.ldb = long(Ns) * a.M; p.strideB = 0;
+      p.C = Kl; p.ldc = a.Nc; p.strideC = 0;
+      p.alpha = cmk(1, 0); p.beta = first ? cmk(0, 0) : cmk(1, 0);
+      AFQMC_TRY(zgemm(s, 1, GN, false, GT, a.Lnak_real[sp] != nullptr, p));
+      first = false;
+    }
+  }
   if (need_T) {
     finish_kernel<<<W, 256, 0, s>>>(exx_part, Kl, a.Nc, -0.5 * a.scl, 0.5 * a.sclj, addEXX ? 1 : 0,
                                     addEJ ? 1 : 0, E);

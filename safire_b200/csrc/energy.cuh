@@ -16,6 +16,9 @@ struct EnergyArgs {
   double E0, scl, sclj;
   const double* Likn;  // [nspin_H2][M*M][Nc] (mixed-precision set-up)
   int nspin_H2;
+  // mixed precision: take the Coulomb vector Kl = sum_{a,k} G Lnak of EJ from a complex128 GEMM
+  // instead of the traces of the tensor-core exchange tiles
+  bool coulomb_fp64 = false;
 };
 
 struct MixedHam;

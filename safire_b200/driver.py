@@ -43,7 +43,7 @@ def _sum_over_ranks(t):
 @dataclass
 class RunParams:
     walker_ortho_interval: int = 5
-    population_control_interval: int = 10
+    population_control_interval: int = 10  # 0: none inside step()
     measure_interval: int = 10
     equilibration_steps: int = 100
     seed: int = 0
@@ -204,7 +204,8 @@ class Simulation:
         if step % self.rp.walker_ortho_interval == 0:
             self.prop.Orthogonalize(self.wset)
             self._g_ready = False
-        if step % self.rp.population_control_interval == 0:
+        pci = self.rp.population_control_interval
+        if pci > 0 and step % pci == 0:  # 0: the caller controls the population itself
             self._g_ready = False
             if _world() > 1:
                 from .population import population_control_distributed

@@ -46,24 +46,27 @@ def _sym(a):
     return 0.5 * (a + a.T)
 
 
-def make_hamiltonian(M, Nc, decay, seed=0):
+def make_hamiltonian(M, Nc, decay, seed=0, lscale=0.5):
+    """h1 = diag(-2 + 4 i / M) + 0.1 sym(N(0,1)); L_n = lscale decay^n sym(N(0,1)) / sqrt(M)
+    (lscale 0.5 in the benchmark construction)."""
     rng = np.random.default_rng(seed)
     h1 = np.diag(-2.0 + 4.0 * np.arange(M) / M) + 0.1 * _sym(rng.standard_normal((M, M)))
     Likn = np.empty((M, M, Nc), dtype=np.float64)
     for n in range(Nc):
-        Likn[:, :, n] = 0.5 * decay ** n * _sym(rng.standard_normal((M, M))) / np.sqrt(M)
+        Likn[:, :, n] = lscale * decay ** n * _sym(rng.standard_normal((M, M))) / np.sqrt(M)
     return h1, Likn
 
 
-def make_workload(name="cfg1", seed=0, W=None, M=None, N=None, Nc=None):
-    """Build a named workload; W/M/N/Nc override the table (same construction, smaller sizes)."""
+def make_workload(name="cfg1", seed=0, W=None, M=None, N=None, Nc=None, lscale=0.5):
+    """Build a named workload; W/M/N/Nc override the table (same construction, smaller sizes);
+    lscale scales the Cholesky vectors (0.5 in the benchmark construction)."""
     M0, nup, ndn, Nc0, decay, W0, dt = CONFIGS[name]
     M = M or M0
     Nc = Nc or Nc0
     W = W or W0
     if N is not None:
         nup = ndn = N
-    h1, Likn = make_hamiltonian(M, Nc, decay, seed)
+    h1, Likn = make_hamiltonian(M, Nc, decay, seed, lscale)
     evals, evecs = np.linalg.eigh(h1)
     phi = evecs[:, :nup]
     PsiT = [np.ascontiguousarray(phi.conj().T).astype(np.complex128)]
