@@ -223,6 +223,29 @@ int afqmc_wfn_energy(afqmc_ham ham, afqmc_wset ws, afqmc_c128* E, afqmc_c128* ov
  * divides by the weight sum (as the reference's Measurements do).  No RotationMatrix. */
 int afqmc_wfn_onerdm(afqmc_ham ham, afqmc_wset ws, const afqmc_c128* G, long ldG,
                      afqmc_c128* rdm, afqmc_stream stream);
+/* NOMSD with several determinants (ci.size() > 1; NOMSD.cpp:93-333): one Hamiltonian handle per
+ * determinant (afqmc_ham_create with that determinant's PsiT: its half-rotated Lnak / haj; the
+ * handles must outlive the trial) and the coefficients ci [ndet] (host). */
+typedef struct afqmc_nomsd_s* afqmc_nomsd;
+int afqmc_nomsd_create(int ndet, const afqmc_ham* hams, const afqmc_c128* ci, afqmc_nomsd* out);
+int afqmc_nomsd_destroy(afqmc_nomsd trial);
+/* NOMSD::Log_Overlap (NOMSD.cpp:281-333): ovlp [W] (device) = log sum_d conj(c_d) ov_d,
+ * summed relative to the largest determinant */
+int afqmc_nomsd_log_overlap(afqmc_nomsd trial, afqmc_wset ws, afqmc_c128* ovlp,
+                            afqmc_stream stream);
+/* NOMSD::Energy (NOMSD.cpp:159-217): E [W][3] = sum_d conj(c_d) e^{ov_d} E_d / sum_d
+ * conj(c_d) e^{ov_d}, ovlp [W] its log.  Synchronous. */
+int afqmc_nomsd_energy(afqmc_nomsd trial, afqmc_wset ws, afqmc_c128* E, afqmc_c128* ovlp,
+                       int precision, afqmc_stream stream);
+/* NOMSD::MixedDensityMatrix, compact = false (NOMSD.cpp:220-279): G [W][nspin][M][M] (device) =
+ * sum_d w_d G_d / sum_d w_d with w_d = conj(c_d) exp(ov_d - OVLP) (the walkers' OVLP property);
+ * ovlp [W] = sum_d w_d + OVLP, as the reference returns it. */
+int afqmc_nomsd_density_matrix(afqmc_nomsd trial, afqmc_wset ws, afqmc_c128* G,
+                               afqmc_c128* ovlp, afqmc_stream stream);
+/* Real3IndexFactorization::vbias on a full G (the ndet > 1 branch, hpp:389-427):
+ * v [W][Nc] = sqrt(dt) (x2 CLOSED) sum_s sum_{ik} L_s[ik][n] G[w][s][ik] */
+int afqmc_nomsd_vbias(afqmc_nomsd trial, const afqmc_c128* G, afqmc_c128* v, int W, double dt,
+                      afqmc_stream stream);
 /* NOMSD::vMF — NOMSD.cpp:437-465: vbias of the trial's own density matrix.  host [Nc]. */
 int afqmc_wfn_vmf(afqmc_ham ham, double dt, afqmc_c128* vMF_host);
 
@@ -262,6 +285,11 @@ int afqmc_prop_destroy(afqmc_prop prop);
  * must outlive its use by the propagator. */
 typedef struct afqmc_phmsd_s* afqmc_phmsd;
 int afqmc_prop_set_phmsd(afqmc_prop prop, afqmc_phmsd trial, const afqmc_c128* vMF);
+/* The same for a NOMSD trial with several determinants (afqmc_nomsd_create): vbias from the
+ * combined full density matrix (afqmc_nomsd_density_matrix / afqmc_nomsd_vbias), overlaps from
+ * afqmc_nomsd_log_overlap; FP64; vMF (host [Nc], may be NULL) as for PHMSD (NOMSD::vMF for
+ * several determinants, NOMSD.cpp:466-520, is the caller's). */
+int afqmc_prop_set_nomsd(afqmc_prop prop, afqmc_nomsd trial, const afqmc_c128* vMF);
 /* host copies: P1 [nspin][M][M], vMF [Nc] (either may be NULL) */
 int afqmc_prop_get_p1(afqmc_prop prop, afqmc_c128* P1, afqmc_c128* vMF);
 

@@ -843,3 +843,84 @@ def onerdm(wfn: NOMSD, ws: WalkerSet):
         out.append(acc)
         off += N
     return np.stack(out)
+
+
+
+class NOMSDMulti:
+    """NOMSD with several determinants (NOMSD.cpp:93-333, 159-217; Real3IndexFactorization.hpp
+    :389-427): hams[d] built with determinant d's PsiT, coefficients ci.  vMF is given (the
+    pairwise several-determinant vMF, NOMSD.cpp:466-520, is the caller's)."""
+
+    def __init__(self, hams, PsiTs, ci, vMF=None):
+        self.hams = list(hams)
+        self.ham = self.hams[0]
+        self.PsiTs = [[np.asarray(p, np.complex128) for p in P] for P in PsiTs]
+        self.ci = np.asarray(ci, np.complex128)
+        self.walker_type = self.ham.walker_type
+        self.M, self.nup, self.ndn = self.ham.M, self.ham.nup, self.ham.ndn
+        self._vMF = None if vMF is None else np.asarray(vMF, np.complex128)
+
+    def _per_det(self, SA, SB, compact=True):
+        out = []
+        for d, P in enumerate(self.PsiTs):
+            out.append(NOMSD(self.hams[d], P).DensityMatrix(SA, SB, compact))
+        return out
+
+    def Log_Overlap(self, SA, SB):
+        lo = []
+        for d, P in enumerate(self.PsiTs):
+            ov = np.zeros(SA.shape[0], complex)
+            Log_Overlap(P[0], SA, ov)
+            if self.walker_type == CLOSED:
+                ov *= 2.0
+            else:
+                Log_Overlap(P[1], SB, ov)
+            c = self.ci[d]
+            lo.append(ov + np.log(complex(1e-12) if abs(c) < 1e-12 else np.conj(c)))
+        lo = np.array(lo)
+        m = lo[np.argmax(lo.real, axis=0), np.arange(lo.shape[1])]
+        return m + np.log(np.sum(np.exp(lo - m), axis=0))
+
+    def Energy(self, SA, SB):
+        Ed, ov = [], []
+        for d, P in enumerate(self.PsiTs):
+            G, o = NOMSD(self.hams[d], P).DensityMatrix(SA, SB)
+            Ed.append(self.hams[d].energy(G))
+            ov.append(o)
+        Ed, ov = np.array(Ed), np.array(ov)
+        m = ov[np.argmax(ov.real, axis=0), np.arange(ov.shape[1])]
+        f = np.conj(self.ci)[:, None] * np.exp(ov - m)
+        E = np.einsum("dw,dwq->wq", f, Ed) / f.sum(0)[:, None]
+        return E, np.log(f.sum(0)) + m
+
+    def MixedDensityMatrix(self, SA, SB, log_m):
+        """Full G [W, nspin, M, M] and the reference's Ov (linear sum + log_m)."""
+        W = SA.shape[0]
+        nspin = 2 if self.walker_type == COLLINEAR else 1
+        G = np.zeros((W, nspin, self.M, self.M), complex)
+        Ov = np.zeros(W, complex)
+        for d, P in enumerate(self.PsiTs):
+            ot = np.zeros(W, complex)
+            Gs = [MixedDensityMatrix(P[0], SA, ot, compact=False)]
+            if self.walker_type == CLOSED:
+                ot *= 2.0
+            else:
+                Gs.append(MixedDensityMatrix(P[1], SB, ot, compact=False))
+            wd = np.conj(self.ci[d]) * np.exp(ot - log_m)
+            G += wd[:, None, None, None] * np.stack(Gs, 1)
+            Ov += wd
+        return G / Ov[:, None, None, None], Ov + log_m
+
+    def vbias(self, SA, SB, dt):
+        """Full-G branch of Real3IndexFactorization::vbias (hpp:389-427); the weights' shift
+        cancels in G, so the walkers' own log overlap serves."""
+        G, _ = self.MixedDensityMatrix(SA, SB, self.Log_Overlap(SA, SB))
+        a = math.sqrt(dt) * (2.0 if self.walker_type == CLOSED else 1.0)
+        L = self.ham.Likn  # [nspin_H2][M][M][Nc]
+        v = np.zeros((SA.shape[0], L.shape[3]), complex)
+        for s in range(G.shape[1]):
+            v += a * np.einsum("ikn,wik->wn", L[s % L.shape[0]], G[:, s])
+        return v
+
+    def vMF(self, dt):
+        return self._vMF.copy()

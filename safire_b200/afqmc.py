@@ -319,6 +319,64 @@ class NOMSD:
         return v
 
 
+class NOMSDMulti:
+    """NOMSD with several determinants (NOMSD.cpp, ci.size() > 1): one HamiltonianOperations per
+    determinant (built with that determinant's PsiT) and the coefficients ci."""
+
+    def __init__(self, hams, ci):
+        self.hams = list(hams)
+        self.ham = self.hams[0]
+        c = np.ascontiguousarray(ci, dtype=np.complex128)
+        arr = (vp * len(self.hams))(*[h.handle for h in self.hams])
+        h = vp()
+        call("afqmc_nomsd_create", len(self.hams), C.cast(arr, vp), _host_ptr(c), C.byref(h))
+        self.handle = h
+        self.ci = c
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        try:
+            if h and capi._lib is not None:
+                capi._lib.afqmc_nomsd_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is gone
+            pass
+        self.handle = None
+
+    def Log_Overlap(self, wset: WalkerSet, ovlp=None, stream=None):
+        ovlp = ovlp if ovlp is not None else torch.empty(wset.W, dtype=torch.complex128,
+                                                         device=wset.buffer.device)
+        call("afqmc_nomsd_log_overlap", self.handle, wset.handle, _ptr(ovlp), _stream(stream))
+        return ovlp
+
+    def Energy(self, wset: WalkerSet, set_properties=True, precision=PREC_FP64, stream=None):
+        dev = wset.buffer.device
+        E = torch.empty((wset.W, 3), dtype=torch.complex128, device=dev)
+        ov = torch.empty(wset.W, dtype=torch.complex128, device=dev)
+        call("afqmc_nomsd_energy", self.handle, wset.handle, _ptr(E), _ptr(ov), precision,
+             _stream(stream))
+        if set_properties:
+            p = wset.properties()
+            p[:, capi.OVLP] = ov
+            p[:, capi.E1], p[:, capi.EXX], p[:, capi.EJ] = E[:, 0], E[:, 1], E[:, 2]
+        return E, ov
+
+    def MixedDensityMatrix(self, wset: WalkerSet, stream=None):
+        """(G [W, nspin, M, M] full, ovlp [W]) as NOMSD::MixedDensityMatrix returns them."""
+        nspin = 2 if self.ham.walker_type == COLLINEAR else 1
+        dev = wset.buffer.device
+        G = torch.empty((wset.W, nspin, self.ham.M, self.ham.M), dtype=torch.complex128,
+                        device=dev)
+        ov = torch.empty(wset.W, dtype=torch.complex128, device=dev)
+        call("afqmc_nomsd_density_matrix", self.handle, wset.handle, _ptr(G), _ptr(ov),
+             _stream(stream))
+        return G, ov
+
+    def vbias(self, G, v, dt, stream=None):
+        call("afqmc_nomsd_vbias", self.handle, _ptr(G), _ptr(v), int(G.shape[0]), float(dt),
+             _stream(stream))
+        return v
+
+
 class PHMSDWavefunction:
     """The walker-set facade of a PHMSD trial (Wavefunction.hpp's variant over PHMSD.hpp): the
     same calls as NOMSD, evaluated by the multi-determinant kernels.  FP64 only."""
@@ -406,11 +464,19 @@ class Propagator:
         return best.value, {m: float(t) for m, t in zip((0, 2, 3), ms)}
 
     def set_trial(self, trial, vMF=None):
-        """Steps with a PHMSD trial (vbias and overlaps from it); vMF host [Nc] or None keeps
-        the current mean field.  trial None detaches."""
+        """Steps with a multi-determinant trial (PHMSD or NOMSDMulti: vbias and overlaps from
+        it); vMF host [Nc] or None keeps the current mean field.  trial None detaches."""
         v = None if vMF is None else np.ascontiguousarray(vMF, dtype=np.complex128)
-        call("afqmc_prop_set_phmsd", self.handle, None if trial is None else trial.handle,
-             None if v is None else _host_ptr(v))
+        vp_ = None if v is None else _host_ptr(v)
+        if trial is None:
+            prev = getattr(self, "_trial", None)
+            name = "afqmc_prop_set_nomsd" if isinstance(prev, NOMSDMulti) else \
+                "afqmc_prop_set_phmsd"
+            call(name, self.handle, None, vp_)
+        elif isinstance(trial, NOMSDMulti):
+            call("afqmc_prop_set_nomsd", self.handle, trial.handle, vp_)
+        else:
+            call("afqmc_prop_set_phmsd", self.handle, trial.handle, vp_)
         self._trial = trial  # the trial must outlive the propagator's use of it
 
     def Propagate(self, wset: WalkerSet, Eshift, uniforms=None, stream=None):

@@ -75,6 +75,13 @@ _SIGS = {
     "afqmc_wfn_onerdm": (i32, [vp, vp, vp, i64, vp, vp]),
     "afqmc_prop_autotune": (i32, [vp, vp, vp, vp, vp]),
     "afqmc_ham_set_coulomb_fp64": (i32, [vp, i32]),
+    "afqmc_nomsd_create": (i32, [i32, vp, vp, C.POINTER(vp)]),
+    "afqmc_nomsd_destroy": (i32, [vp]),
+    "afqmc_nomsd_log_overlap": (i32, [vp, vp, vp, vp]),
+    "afqmc_nomsd_energy": (i32, [vp, vp, vp, vp, i32, vp]),
+    "afqmc_nomsd_density_matrix": (i32, [vp, vp, vp, vp, vp]),
+    "afqmc_nomsd_vbias": (i32, [vp, vp, vp, i32, C.c_double, vp]),
+    "afqmc_prop_set_nomsd": (i32, [vp, vp, vp]),
     "afqmc_phmsd_excitations": (i32, [i32, i32, vp, i32, vp, vp, vp, vp, vp, vp]),
     "afqmc_prop_set_phmsd": (i32, [vp, vp, vp]),
     "afqmc_mlp_create": (i32, [i32, i32, u64, C.POINTER(vp)]),

@@ -149,6 +149,8 @@ struct afqmc_prop_s {
   // multi-determinant trial used in place of the Hamiltonian's single determinant
   afqmc_phmsd ph = nullptr;
   c128* Gph = nullptr;       // [maxW][nact_up + nact_dn][M]
+  afqmc_nomsd md = nullptr;  // several-determinant NOMSD trial
+  c128* Gfull = nullptr;     // [maxW][nspin][M][M]
   // per-phase CUDA events of the last timed step (AFQMCTimers analogue)
   bool timing = false;
   cudaEvent_t ev[AFQMC_NPHASE + 1] = {};
@@ -159,12 +161,30 @@ struct afqmc_prop_s {
     dfree(P1); dfree(P1r); dfree(vMF);
     dfree(G); dfree(vb); dfree(X); dfree(HW); dfree(mf); dfree(newov); dfree(ovtmp);
     dfree(T); dfree(V); dfree(w1); dfree(w2); dfree(w3); dfree(ortho_work);
-    dfree(Eshift_d); dfree(counter); dfree(stats); dfree(Gph);
+    dfree(Eshift_d); dfree(counter); dfree(stats); dfree(Gph); dfree(Gfull);
   }
 };
 
 struct afqmc_host_rng_s {
   std::mt19937 rng;
+};
+
+// NOMSD with several determinants (NOMSD.hpp / NOMSD.cpp, ci.size() > 1): one Hamiltonian
+// handle per determinant (its half-rotated tensors), the coefficients ci
+struct afqmc_nomsd_s {
+  int device = 0;
+  std::vector<afqmc_ham_s*> hams;
+  std::vector<c128> ci;
+  c128 *Gd = nullptr, *Gc = nullptr, *ov = nullptr, *wd = nullptr, *T = nullptr, *Ed = nullptr;
+  int capW = 0;
+  void free_bufs() {
+    dfree(Gd); dfree(Gc); dfree(ov); dfree(wd); dfree(T); dfree(Ed);
+    capW = 0;
+  }
+  ~afqmc_nomsd_s() {
+    DeviceGuard g(device);
+    free_bufs();
+  }
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -703,6 +723,11 @@ __global__ void broadcast_row_kernel(c128* buf, long walker_size, int W, const c
   long total = long(W) * walker_size;
   if (e < total) buf[e] = row[e % walker_size];
 }
+// x[w] += c
+__global__ void add_scalar_kernel(c128* __restrict__ x, int W, c128 c) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w < W) x[w] = cadd(x[w], c);
+}
 }  // namespace api_kernels
 
 extern "C" int afqmc_wset_create(int walker_type, int M, int nup, int ndn, int W,
@@ -868,6 +893,255 @@ extern "C" int afqmc_wfn_onerdm(afqmc_ham h, afqmc_wset ws, const afqmc_c128* G,
     AFQMC_TRY(zgemm(s, 1, GT, false, GN, false, b));
   }
   return AFQMC_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// NOMSD with several determinants (NOMSD.cpp:93-333, 159-217; Real3IndexFactorization.hpp:389-427)
+// ---------------------------------------------------------------------------------------------
+namespace multidet {
+// out[w] = m + log sum_d exp(lo[d][w] - m), m = the largest real part (NOMSD.cpp:318-331)
+__global__ void logsumexp_kernel(const c128* __restrict__ lo, int ndet, int W,
+                                 c128* __restrict__ out) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  c128 m = lo[w];
+  for (int d = 1; d < ndet; ++d)
+    if (lo[size_t(d) * W + w].x > m.x) m = lo[size_t(d) * W + w];
+  c128 sum = cmk(0, 0);
+  for (int d = 0; d < ndet; ++d) sum = cadd(sum, cexp(csub(lo[size_t(d) * W + w], m)));
+  out[w] = cadd(m, clog(sum));
+}
+
+// E[w] = sum_d conj(c_d) E_d e^{ov_d - m} / sum_d conj(c_d) e^{ov_d - m}, Ov = log(den) + m
+// (NOMSD.cpp:195-211)
+__global__ void multidet_energy_kernel(const c128* __restrict__ Ed, const c128* __restrict__ ov,
+                                       const c128* __restrict__ cc, int ndet, int W,
+                                       c128* __restrict__ E, c128* __restrict__ Ov) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  c128 m = ov[w];
+  for (int d = 1; d < ndet; ++d)
+    if (ov[size_t(d) * W + w].x > m.x) m = ov[size_t(d) * W + w];
+  c128 den = cmk(0, 0), s[3] = {cmk(0, 0), cmk(0, 0), cmk(0, 0)};
+  for (int d = 0; d < ndet; ++d) {
+    const c128 f = cmul(cc[d], cexp(csub(ov[size_t(d) * W + w], m)));
+    den = cadd(den, f);
+    for (int q = 0; q < 3; ++q) s[q] = cadd(s[q], cmul(f, Ed[(size_t(d) * W + w) * 3 + q]));
+  }
+  for (int q = 0; q < 3; ++q) E[w * 3 + q] = cdiv(s[q], den);
+  Ov[w] = cadd(clog(den), m);
+}
+
+// wd[w] = conj(c_d) exp(Ot[w] - log_m[w]) with log_m the walkers' OVLP property; Ov[w] += wd
+__global__ void multidet_weight_kernel(const c128* __restrict__ Ot, const c128* __restrict__ wbuf,
+                                       long ldw, long prop_ovlp, c128 cc, int W,
+                                       c128* __restrict__ wd, c128* __restrict__ Ov) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  const c128 f = cmul(cc, cexp(csub(Ot[w], wbuf[long(w) * ldw + prop_ovlp])));
+  wd[w] = f;
+  Ov[w] = cadd(Ov[w], f);
+}
+
+// G[w][:] += wd[w] Gd[w][:]   (n elements per walker)
+__global__ void axpy_rows_kernel(const c128* __restrict__ Gd, const c128* __restrict__ wd,
+                                 long n, int W, c128* __restrict__ G) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= n * W) return;
+  const int w = int(t / n);
+  G[t] = cadd(G[t], cmul(wd[w], Gd[t]));
+}
+
+// G[w][:] /= Ov[w]; then (add_log_shift_kernel) Ov[w] += log_m[w]: the reference adds the log of
+// the shift to the linear sum (NOMSD.cpp:274-276)
+__global__ void multidet_finish_kernel(c128* __restrict__ G, long n, int W,
+                                       const c128* __restrict__ Ov) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t < n * W) {
+    const int w = int(t / n);
+    G[t] = cdiv(G[t], Ov[w]);
+  }
+}
+__global__ void add_log_shift_kernel(c128* __restrict__ Ov, const c128* __restrict__ wbuf,
+                                     long ldw, long prop_ovlp, int W) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w < W) Ov[w] = cadd(Ov[w], wbuf[long(w) * ldw + prop_ovlp]);
+}
+
+int nomsd_bufs(afqmc_nomsd md, int W) {
+  if (md->capW >= W) return AFQMC_OK;
+  AFQMC_CUDA_TRY(cudaDeviceSynchronize());
+  md->free_bufs();
+  afqmc_ham_s* h = md->hams[0];
+  const long M = h->M, ldG = long(h->nel_tot) * M;
+  const int nmax = std::max(h->nel[0], h->nel[1]);
+  const size_t nd = md->hams.size();
+  AFQMC_TRY(dalloc(&md->Gd, size_t(W) * h->nspin * M * M));
+  AFQMC_TRY(dalloc(&md->Gc, size_t(W) * (ldG > 0 ? ldG : 1)));
+  AFQMC_TRY(dalloc(&md->ov, nd * W));
+  AFQMC_TRY(dalloc(&md->wd, size_t(W)));
+  AFQMC_TRY(dalloc(&md->T, size_t(W) * (nmax > 0 ? nmax * nmax : 1)));
+  AFQMC_TRY(dalloc(&md->Ed, nd * W * 3));
+  md->capW = W;
+  return AFQMC_OK;
+}
+
+int nomsd_log_overlap(afqmc_nomsd md, afqmc_wset_s* ws, cudaStream_t s, c128* ovlp) {
+  const int W = ws->W, nd = int(md->hams.size());
+  AFQMC_TRY(nomsd_bufs(md, W));
+  for (int d = 0; d < nd; ++d) {
+    // log overlap of determinant d (CLOSED x2) + log(conj ci), NOMSD.cpp:303-316
+    AFQMC_TRY(wfn_log_overlap(md->hams[d], ws, s, md->ov + size_t(d) * W, md->T));
+    const c128 c = md->ci[d];
+    const c128 lc = cabs(c) < 1e-12 ? clog(cmk(1e-12, 0)) : clog(cconj(c));
+    api_kernels::add_scalar_kernel<<<ceil_div(W, 128), 128, 0, s>>>(md->ov + size_t(d) * W, W, lc);
+    AFQMC_TRY(launch_status("add_scalar_kernel"));
+  }
+  logsumexp_kernel<<<ceil_div(W, 128), 128, 0, s>>>(md->ov, nd, W, ovlp);
+  return launch_status("logsumexp_kernel");
+}
+
+// full mixed density matrices of every determinant combined (NOMSD.cpp:220-279, compact=false)
+int nomsd_density_matrix(afqmc_nomsd md, afqmc_wset_s* ws, cudaStream_t s, c128* G, c128* Ov) {
+  afqmc_ham_s* h0 = md->hams[0];
+  const int W = ws->W, nd = int(md->hams.size()), nspin = h0->nspin;
+  const long M = h0->M, MM = M * M, per = long(nspin) * MM, ldG = long(h0->nel_tot) * M;
+  AFQMC_TRY(nomsd_bufs(md, W));
+  AFQMC_CUDA_TRY(cudaMemsetAsync(G, 0, sizeof(c128) * size_t(W) * per, s));
+  AFQMC_CUDA_TRY(cudaMemsetAsync(Ov, 0, sizeof(c128) * W, s));
+  for (int d = 0; d < nd; ++d) {
+    afqmc_ham_s* h = md->hams[d];
+    c128* Ot = md->ov + size_t(d) * W;
+    AFQMC_TRY(wfn_density_matrix(h, ws, s, md->Gc, ldG, Ot, md->T));
+    // Gd[w][s] = PsiT_s^T Gc[w][s]  (full G[i][k] = sum_a PsiT[a][i] Gc[a][k])
+    for (int sp = 0; sp < nspin; ++sp) {
+      const int Ns = h->nel[sp];
+      if (Ns == 0) {
+        AFQMC_CUDA_TRY(cudaMemset2DAsync(md->Gd + sp * MM, per * sizeof(c128), 0,
+                                         MM * sizeof(c128), W, s));
+        continue;
+      }
+      GemmParams p{};
+      p.m = int(M); p.n = int(M); p.k = Ns;
+      p.A = h->PsiT + long(h->el_off[sp]) * M; p.lda = M; p.strideA = 0;
+      p.B = md->Gc + long(h->el_off[sp]) * M; p.ldb = M; p.strideB = ldG;
+      p.C = md->Gd + sp * MM; p.ldc = M; p.strideC = per;
+      p.alpha = cmk(1, 0); p.beta = cmk(0, 0);
+      AFQMC_TRY(zgemm(s, W, GT, false, GN, false, p));
+    }
+    multidet_weight_kernel<<<ceil_div(W, 128), 128, 0, s>>>(Ot, ws->buf, ws->walker_size,
+                                                            ws->prop0 + AFQMC_OVLP,
+                                                            cconj(md->ci[d]), W, md->wd, Ov);
+    AFQMC_TRY(launch_status("multidet_weight_kernel"));
+    axpy_rows_kernel<<<ceil_div(per * W, 256), 256, 0, s>>>(md->Gd, md->wd, per, W, G);
+    AFQMC_TRY(launch_status("axpy_rows_kernel"));
+  }
+  multidet_finish_kernel<<<ceil_div(per * W, 256), 256, 0, s>>>(G, per, W, Ov);
+  AFQMC_TRY(launch_status("multidet_finish_kernel"));
+  add_log_shift_kernel<<<ceil_div(W, 128), 128, 0, s>>>(Ov, ws->buf, ws->walker_size,
+                                                        ws->prop0 + AFQMC_OVLP, W);
+  return launch_status("add_log_shift_kernel");
+}
+
+// vbias from the full G (the ndet > 1 branch, Real3IndexFactorization.hpp:389-427):
+// v[w][n] = a sum_s sum_{ik} L_s[ik][n] G[w][s][ik], a = sqrt(dt) (x2 CLOSED)
+int nomsd_vbias(afqmc_ham_s* h, cudaStream_t s, const c128* G, c128* v, int W, double dt) {
+  const int nspin = h->nspin;
+  const long MM = long(h->M) * h->M;
+  const double a = std::sqrt(dt) * (h->walker_type == AFQMC_CLOSED ? 2.0 : 1.0);
+  for (int sp = 0; sp < nspin; ++sp) {
+    GemmParams p{};
+    p.m = W; p.n = h->Nc; p.k = int(MM);
+    p.A = G + sp * MM; p.lda = nspin * MM; p.strideA = 0;
+    p.B = h->Likn + size_t(sp % h->nspin_H2) * MM * h->Nc; p.ldb = h->Nc; p.strideB = 0;
+    p.C = v; p.ldc = h->Nc; p.strideC = 0;
+    p.alpha = cmk(a, 0); p.beta = sp == 0 ? cmk(0, 0) : cmk(1, 0);
+    AFQMC_TRY(zgemm(s, 1, GN, false, GN, true, p));
+  }
+  return AFQMC_OK;
+}
+}  // namespace multidet
+using namespace multidet;
+
+extern "C" int afqmc_nomsd_create(int ndet, const afqmc_ham* hams, const afqmc_c128* ci,
+                                  afqmc_nomsd* out) {
+  AFQMC_CHECK_ARG(out && hams && ci && ndet >= 1, "afqmc_nomsd_create: bad argument");
+  *out = nullptr;
+  afqmc_ham_s* h0 = hams[0];
+  AFQMC_CHECK_ARG(h0, "afqmc_nomsd_create: null Hamiltonian 0");
+  for (int d = 1; d < ndet; ++d) {
+    afqmc_ham_s* h = hams[d];
+    AFQMC_CHECK_ARG(h && h->device == h0->device && h->walker_type == h0->walker_type &&
+                        h->M == h0->M && h->Nc == h0->Nc && h->nel[0] == h0->nel[0] &&
+                        h->nel[1] == h0->nel[1],
+                    "afqmc_nomsd_create: determinant %d's Hamiltonian differs in shape", d);
+  }
+  std::unique_ptr<afqmc_nomsd_s> md(new (std::nothrow) afqmc_nomsd_s());
+  AFQMC_CHECK_ARG(md, "afqmc_nomsd_create: out of host memory");
+  md->device = h0->device;
+  md->hams.assign(hams, hams + ndet);
+  md->ci.assign(reinterpret_cast<const c128*>(ci), reinterpret_cast<const c128*>(ci) + ndet);
+  *out = md.release();
+  return AFQMC_OK;
+}
+
+extern "C" int afqmc_nomsd_destroy(afqmc_nomsd md) {
+  delete md;
+  return AFQMC_OK;
+}
+
+extern "C" int afqmc_nomsd_log_overlap(afqmc_nomsd md, afqmc_wset ws, afqmc_c128* ovlp,
+                                       afqmc_stream stream) {
+  AFQMC_CHECK_ARG(md && ws && ovlp, "afqmc_nomsd_log_overlap: null argument");
+  AFQMC_CHECK_ARG(wset_matches(md->hams[0], ws), "afqmc_nomsd_log_overlap: mismatch");
+  DeviceGuard g(md->device);
+  return nomsd_log_overlap(md, ws, reinterpret_cast<cudaStream_t>(stream),
+                           reinterpret_cast<c128*>(ovlp));
+}
+
+extern "C" int afqmc_nomsd_energy(afqmc_nomsd md, afqmc_wset ws, afqmc_c128* E, afqmc_c128* ovlp,
+                                  int precision, afqmc_stream stream) {
+  AFQMC_CHECK_ARG(md && ws && E && ovlp, "afqmc_nomsd_energy: null argument");
+  AFQMC_CHECK_ARG(wset_matches(md->hams[0], ws), "afqmc_nomsd_energy: mismatch");
+  DeviceGuard g(md->device);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int W = ws->W, nd = int(md->hams.size());
+  AFQMC_TRY(nomsd_bufs(md, W));
+  const long ldG = long(md->hams[0]->nel_tot) * md->hams[0]->M;
+  for (int d = 0; d < nd; ++d) {
+    afqmc_ham_s* h = md->hams[d];
+    AFQMC_TRY(wfn_density_matrix(h, ws, s, md->Gc, ldG, md->ov + size_t(d) * W, md->T));
+    AFQMC_TRY(ham_energy(h, s, md->Gc, ldG, md->Ed + size_t(d) * W * 3, W, true, true, true,
+                         precision));
+  }
+  std::vector<c128> cc(nd);
+  for (int d = 0; d < nd; ++d) cc[d] = cconj(md->ci[d]);
+  Scratch cd;
+  AFQMC_TRY(cd.get(sizeof(c128) * nd, s));
+  AFQMC_CUDA_TRY(cudaMemcpyAsync(cd.p, cc.data(), sizeof(c128) * nd, cudaMemcpyHostToDevice, s));
+  multidet_energy_kernel<<<ceil_div(W, 128), 128, 0, s>>>(md->Ed, md->ov, (const c128*)cd.p, nd,
+                                                          W, (c128*)E, (c128*)ovlp);
+  AFQMC_TRY(launch_status("multidet_energy_kernel"));
+  return cudaStreamSynchronize(s) == cudaSuccess ? AFQMC_OK : AFQMC_ERR_CUDA;
+}
+
+extern "C" int afqmc_nomsd_density_matrix(afqmc_nomsd md, afqmc_wset ws, afqmc_c128* G,
+                                          afqmc_c128* ovlp, afqmc_stream stream) {
+  AFQMC_CHECK_ARG(md && ws && G && ovlp, "afqmc_nomsd_density_matrix: null argument");
+  AFQMC_CHECK_ARG(wset_matches(md->hams[0], ws), "afqmc_nomsd_density_matrix: mismatch");
+  DeviceGuard g(md->device);
+  return nomsd_density_matrix(md, ws, reinterpret_cast<cudaStream_t>(stream),
+                              reinterpret_cast<c128*>(G), reinterpret_cast<c128*>(ovlp));
+}
+
+extern "C" int afqmc_nomsd_vbias(afqmc_nomsd md, const afqmc_c128* G, afqmc_c128* v, int W,
+                                 double dt, afqmc_stream stream) {
+  AFQMC_CHECK_ARG(md && W >= 0, "afqmc_nomsd_vbias: bad argument");
+  if (W == 0) return AFQMC_OK;
+  AFQMC_CHECK_ARG(G && v, "afqmc_nomsd_vbias: null array");
+  DeviceGuard g(md->device);
+  return nomsd_vbias(md->hams[0], reinterpret_cast<cudaStream_t>(stream),
+                     reinterpret_cast<const c128*>(G), reinterpret_cast<c128*>(v), W, dt);
 }
 
 extern "C" int afqmc_wfn_log_overlap(afqmc_ham h, afqmc_wset ws, afqmc_c128* ovlp,
@@ -1179,10 +1453,34 @@ extern "C" int afqmc_prop_set_phmsd(afqmc_prop pr, afqmc_phmsd trial, const afqm
                   "propagator %d (afqmc_phmsd_set_hamiltonian first)", d[5], h->Nc);
   AFQMC_CHECK_ARG(pr->p.precision == AFQMC_PREC_FP64,
                   "afqmc_prop_set_phmsd: PHMSD steps run in FP64");
+  AFQMC_CHECK_ARG(!pr->md, "afqmc_prop_set_phmsd: a multi-determinant NOMSD trial is attached");
   dfree(pr->Gph);
   AFQMC_TRY(dalloc(&pr->Gph, size_t(pr->maxW) * (d[3] + d[4]) * h->M));
   if (vMF) AFQMC_TRY(prop_mean_field(pr, reinterpret_cast<const c128*>(vMF)));
   pr->ph = trial;
+  return AFQMC_OK;
+}
+
+extern "C" int afqmc_prop_set_nomsd(afqmc_prop pr, afqmc_nomsd trial, const afqmc_c128* vMF) {
+  AFQMC_CHECK_ARG(pr, "afqmc_prop_set_nomsd: null handle");
+  DeviceGuard g(pr->device);
+  if (!trial) {
+    pr->md = nullptr;
+    dfree(pr->Gfull);
+    return vMF ? prop_mean_field(pr, reinterpret_cast<const c128*>(vMF)) : AFQMC_OK;
+  }
+  afqmc_ham_s* h = pr->ham;
+  afqmc_ham_s* t = trial->hams[0];
+  AFQMC_CHECK_ARG(t->walker_type == h->walker_type && t->M == h->M && t->Nc == h->Nc &&
+                      t->nel[0] == h->nel[0] && t->nel[1] == h->nel[1],
+                  "afqmc_prop_set_nomsd: trial and propagator Hamiltonians differ in shape");
+  AFQMC_CHECK_ARG(pr->p.precision == AFQMC_PREC_FP64,
+                  "afqmc_prop_set_nomsd: multi-determinant steps run in FP64");
+  AFQMC_CHECK_ARG(!pr->ph, "afqmc_prop_set_nomsd: a PHMSD trial is attached");
+  dfree(pr->Gfull);
+  AFQMC_TRY(dalloc(&pr->Gfull, size_t(pr->maxW) * h->nspin * h->M * h->M));
+  if (vMF) AFQMC_TRY(prop_mean_field(pr, reinterpret_cast<const c128*>(vMF)));
+  pr->md = trial;
   return AFQMC_OK;
 }
 
@@ -1217,7 +1515,12 @@ int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* E
   const bool mixed = pr->p.precision == AFQMC_PREC_MIXED;
   // 1. vbias: G of the walkers (NOMSD::vbias, NOMSD.cpp:39-61); with AFQMC_STEP_G_READY the
   //    previous step left it for these walkers
-  if (pr->ph) {
+  if (pr->md) {
+    // NOMSD::vbias with several determinants (NOMSD.cpp:39-61): the full G, then Likn . G
+    AFQMC_TRY(nomsd_density_matrix(pr->md, ws, s, pr->Gfull, pr->ovtmp));
+    AFQMC_TRY(mark(1));
+    AFQMC_TRY(nomsd_vbias(h, s, pr->Gfull, pr->vb, W, dt));
+  } else if (pr->ph) {
     // PHMSD::vbias (PHMSD.cpp:54-72): the multi-determinant density matrix, then Lnak . G
     AFQMC_TRY(afqmc_phmsd_density_matrix(pr->ph, (const afqmc_c128*)ws->buf, ws->walker_size,
                                          (afqmc_c128*)pr->Gph, (afqmc_c128*)pr->ovtmp, W, 0,
@@ -1230,7 +1533,7 @@ int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* E
       AFQMC_TRY(wfn_density_matrix(h, ws, s, pr->G, ldG, pr->ovtmp, pr->T));
     AFQMC_TRY(mark(1));
   }
-  if (pr->ph) {
+  if (pr->ph || pr->md) {
     // vbias done above
   } else if (mixed) {
     EnergyArgs a = energy_args(h, pr->G, ldG);
@@ -1271,7 +1574,9 @@ int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* E
   AFQMC_TRY(mark(5));
   // 5. new overlaps; with AFQMC_STEP_KEEP_G also the density matrix of the propagated walkers
   //    for the next step (the same product, LU and log det, plus the inverse and G)
-  if (pr->ph)
+  if (pr->md)
+    AFQMC_TRY(nomsd_log_overlap(pr->md, ws, s, pr->newov));
+  else if (pr->ph)
     AFQMC_TRY(afqmc_phmsd_log_overlap(pr->ph, (const afqmc_c128*)ws->buf, ws->walker_size,
                                       (afqmc_c128*)pr->newov, W, (afqmc_stream)s));
   else if (flags & AFQMC_STEP_KEEP_G)
@@ -1315,7 +1620,8 @@ extern "C" int afqmc_prop_step_flags(afqmc_prop pr, afqmc_wset ws, const double*
   AFQMC_CHECK_ARG(ws->W <= pr->maxW, "afqmc_prop_step_flags: too many walkers");
   AFQMC_CHECK_ARG((flags & ~(AFQMC_STEP_G_READY | AFQMC_STEP_KEEP_G)) == 0,
                   "afqmc_prop_step_flags: unknown flags %d", flags);
-  AFQMC_CHECK_ARG(!(pr->ph && flags), "afqmc_prop_step_flags: no density reuse with a PHMSD trial");
+  AFQMC_CHECK_ARG(!((pr->ph || pr->md) && flags),
+                  "afqmc_prop_step_flags: no density reuse with a multi-determinant trial");
   DeviceGuard g(pr->device);
   return prop_step(pr, ws, 0.0, Eshift_dev, u, flags, reinterpret_cast<cudaStream_t>(stream));
 }
@@ -1328,7 +1634,7 @@ extern "C" int afqmc_prop_autotune(afqmc_prop pr, afqmc_wset ws, int* best, floa
   DeviceGuard g(pr->device);
   afqmc_ham_s* h = pr->ham;
   *best = -1;
-  if (pr->p.precision != AFQMC_PREC_MIXED || pr->ph) return AFQMC_OK;  // nothing to choose
+  if (pr->p.precision != AFQMC_PREC_MIXED || pr->ph || pr->md) return AFQMC_OK;  // no choice
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const size_t nbuf = size_t(ws->W) * ws->walker_size;
   // the state a step changes: walkers (with their properties), the field counter, the bound
@@ -1403,7 +1709,9 @@ extern "C" int afqmc_prop_orthogonalize(afqmc_prop pr, afqmc_wset ws, afqmc_stre
     AFQMC_TRY(orthogonalize(s, ws->buf + ws->offS(sp), ws->walker_size, pr->ovtmp, ws->W, h->M,
                             h->nel[sp], pr->ortho_work));
   }
-  if (pr->ph)
+  if (pr->md)
+    AFQMC_TRY(nomsd_log_overlap(pr->md, ws, s, pr->newov));
+  else if (pr->ph)
     AFQMC_TRY(afqmc_phmsd_log_overlap(pr->ph, (const afqmc_c128*)ws->buf, ws->walker_size,
                                       (afqmc_c128*)pr->newov, ws->W, (afqmc_stream)s));
   else
