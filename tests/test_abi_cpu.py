@@ -93,3 +93,29 @@ def test_plan_rejects_non_conserving_offspring(capi_lib):
     from safire_b200.capi import AfqmcError
     with pytest.raises(AfqmcError):
         A.plan_walker_exchange([2, 0, 0], [3])
+
+
+def test_cpp_consumer(tmp_path):
+    """A C++ program built against include/afqmc_c.h and the shared library alone (what a SAFIRE
+    build links): its host-side results equal the oracle's."""
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("no C++ compiler")
+    lib = os.path.join(ROOT, "safire_b200", "_lib")
+    exe = tmp_path / "abi_consumer"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "abi_consumer.cpp"), "-L", lib,
+                    "-lsafire_afqmc", f"-Wl,-rpath,{lib}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    lines = dict(line.split(" ", 1) for line in out.strip().splitlines())
+    assert int(lines["seed"]) == O.split_seed(7, 1, 0)
+    w = np.array([0.5, 1.5, 0.25, 2.0, 0.75, 1.0])
+    off = O.comb(O.HostRandomGenerator(O.split_seed(3, 0, 0)), w, w.size)
+    assert [int(x) for x in lines["offspring"].split()] == list(off)
+    plan = O.plan_walker_exchange(off, [3, 3])
+    p = [int(x) for x in lines["plan"].split()]
+    assert p[0] == len(plan) and p[1:] == [int(v) for e in plan for v in e]
+    # reference {0,1,2}: {3,1,2} single, {0,2,4} single with an odd column order, {5,4,1} double
+    assert lines["excitations"].split() == ["4", "0:+1", "1:+1", "2:-1", "3:+1"]
+    assert lines["status"] == "invalid argument"
