@@ -170,6 +170,14 @@ int afqmc_ham_set_exchange_split(afqmc_ham ham, int nsplit);
  * two walkers in flight per CTA chosen by the walker count; 2 / 3 force one / two walkers in
  * flight; 0 launches one batched GEMM per product.  All compute the same sums. */
 int afqmc_ham_set_taylor_fused(afqmc_ham ham, int fused);
+/* Which operations a mixed-precision call runs on the TF32 tensor cores (the rest in complex128):
+ * AFQMC_MIXED_VBIAS the step's vbias, AFQMC_MIXED_PROPAGATION its vHS and Taylor propagation,
+ * AFQMC_MIXED_ENERGY the energy's exchange / Coulomb contraction.  Default AFQMC_MIXED_ALL. */
+#define AFQMC_MIXED_VBIAS 1
+#define AFQMC_MIXED_PROPAGATION 2
+#define AFQMC_MIXED_ENERGY 4
+#define AFQMC_MIXED_ALL 7
+int afqmc_ham_set_mixed_ops(afqmc_ham ham, int mask);
 /* Mixed-precision energy: 1 takes EJ's Coulomb vector Kl = sum_{a,k} G Lnak from a complex128
  * GEMM (one DMMA GEMM per measurement, ~4% of a 10-step block at M=200), 0 (default) from the
  * traces of the tensor-core exchange tiles. */

@@ -49,7 +49,7 @@ def run(precision, steps, walkers, equil, seed, exchange_split=3, workload="cfg2
     return sim.energies, time.time() - t0
 
 
-def lockstep(steps, walkers, equil, seed, workload, lscale, exchange_split=3):
+def lockstep(steps, walkers, equil, seed, workload, lscale, exchange_split=3, mixed_ops=7):
     """Correlated sampling: the complex128 and the mixed run advance side by side with the same
     fields, the same Eshift and the same population-control decisions (the comb of the complex128
     run's weights applied to both walker sets), so the paired energies differ only through the
@@ -62,6 +62,8 @@ def lockstep(steps, walkers, equil, seed, workload, lscale, exchange_split=3):
         sim = Simulation.from_workload(wl, W=walkers, precision=prec, rp=rp)
         if prec == A.PREC_MIXED and exchange_split != 3:
             sim.ham.set_exchange_split(exchange_split)
+        if prec == A.PREC_MIXED and mixed_ops != 7:
+            sim.ham.set_mixed_ops(mixed_ops)
         sims.append(sim)
     s64, smx = sims
     rng = A.HostRandomGenerator(A.split_seed(seed, 0, 0))
@@ -102,18 +104,23 @@ def main(argv=None):
                     help="Cholesky-vector scale of the synthetic Hamiltonian (0.5: benchmark)")
     ap.add_argument("--lockstep", action="store_true",
                     help="correlated sampling: shared fields, Eshift and comb decisions")
+    ap.add_argument("--mixed-ops", default="7",
+                    help="comma-separated masks of the operations run in mixed precision "
+                         "(1 vbias, 2 vHS + propagation, 4 energy)")
     args = ap.parse_args(argv)
     if args.lockstep:
         outs = []
-        for split in (int(x) for x in args.exchange_split.split(",")):
+        runs = [(int(x), int(m)) for x in args.exchange_split.split(",")
+                for m in args.mixed_ops.split(",")]
+        for split, mops in runs:
             t0 = time.time()
             e64, emx, wsum, comp = lockstep(args.steps, args.walkers, args.equil, args.seed,
-                                            args.workload, args.lscale, split)
+                                            args.workload, args.lscale, split, mops)
             d = emx - e64
             out = {
                 "mode": "lockstep", "workload": args.workload, "lscale": args.lscale,
                 "steps": args.steps, "walkers": args.walkers, "equilibration_steps": args.equil,
-                "exchange_split": split, "measurements": int(d.size),
+                "exchange_split": split, "mixed_ops": mops, "measurements": int(d.size),
                 "E_fp64": float(e64.mean()), "E_fp64_err": blocked_error(e64),
                 "E_mixed": float(emx.mean()), "E_mixed_err": blocked_error(emx),
                 "dE_estimate_mHa": 1e3 * float(d.mean()),

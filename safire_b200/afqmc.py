@@ -164,6 +164,10 @@ class HamiltonianOperations:
         """3: 3xTF32 exchange contraction (default); 1: plain TF32."""
         call("afqmc_ham_set_exchange_split", self.handle, int(nsplit))
 
+    def set_mixed_ops(self, mask):
+        """Mixed precision per operation: 1 vbias, 2 vHS + propagation, 4 energy (default 7)."""
+        call("afqmc_ham_set_mixed_ops", self.handle, int(mask))
+
     def set_coulomb_fp64(self, on=True):
         """Mixed precision: EJ's Coulomb vector from a complex128 GEMM, or (default) from the
         tensor-core exchange traces."""

@@ -75,6 +75,7 @@ _SIGS = {
     "afqmc_wfn_onerdm": (i32, [vp, vp, vp, i64, vp, vp]),
     "afqmc_prop_autotune": (i32, [vp, vp, vp, vp, vp]),
     "afqmc_ham_set_coulomb_fp64": (i32, [vp, i32]),
+    "afqmc_ham_set_mixed_ops": (i32, [vp, i32]),
     "afqmc_nomsd_create": (i32, [i32, vp, vp, C.POINTER(vp)]),
     "afqmc_nomsd_destroy": (i32, [vp]),
     "afqmc_nomsd_log_overlap": (i32, [vp, vp, vp, vp]),

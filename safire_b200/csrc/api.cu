@@ -90,6 +90,7 @@ struct afqmc_ham_s {
   double E0 = 0;
   bool trial_real = false;
   bool coulomb_fp64 = false;  // mixed precision: EJ's Coulomb vector from a complex128 GEMM
+  int mixed_ops = AFQMC_MIXED_ALL;  // which operations a mixed-precision call runs on TF32
   double* Likn = nullptr;               // [nspin_H2][M][M][Nc]
   c128* Lnak[2] = {nullptr, nullptr};   // [Nc][nel_s][M]
   double* Lnak_r[2] = {nullptr, nullptr};
@@ -416,7 +417,7 @@ int ham_energy(afqmc_ham_s* h, cudaStream_t s, const c128* G, long ldG, c128* E,
                bool addEJ, bool addEXX, int precision) {
   EnergyArgs a = energy_args(h, G, ldG);
   MixedHam* tc = nullptr;
-  if (precision == AFQMC_PREC_MIXED) {
+  if (precision == AFQMC_PREC_MIXED && (h->mixed_ops & AFQMC_MIXED_ENERGY)) {
     if (!h->mixed) AFQMC_TRY(mixed_ham_create(&h->mixed, a, s));
     tc = h->mixed;
     AFQMC_TRY(mixed_prepare_G(s, tc, G, ldG, W));
@@ -606,7 +607,7 @@ extern "C" int afqmc_ham_vbias(afqmc_ham h, const afqmc_c128* G, afqmc_c128* v, 
   AFQMC_CHECK_ARG(G && v, "afqmc_ham_vbias: null array");
   DeviceGuard g(h->device);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (precision == AFQMC_PREC_MIXED) {
+  if (precision == AFQMC_PREC_MIXED && (h->mixed_ops & AFQMC_MIXED_VBIAS)) {
     EnergyArgs a = energy_args(h, (const c128*)G, long(h->nel_tot) * h->M);
     if (!h->mixed) AFQMC_TRY(mixed_ham_create(&h->mixed, a, s));
     return vbias_mixed(s, h->mixed, (const c128*)G, long(h->nel_tot) * h->M, (c128*)v, W,
@@ -622,7 +623,7 @@ extern "C" int afqmc_ham_vhs(afqmc_ham h, const afqmc_c128* X, afqmc_c128* V, in
   AFQMC_CHECK_ARG(X && V, "afqmc_ham_vhs: null array");
   DeviceGuard g(h->device);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (precision == AFQMC_PREC_MIXED) {
+  if (precision == AFQMC_PREC_MIXED && (h->mixed_ops & AFQMC_MIXED_PROPAGATION)) {
     EnergyArgs a = energy_args(h, nullptr, 0);
     if (!h->mixed) AFQMC_TRY(mixed_ham_create(&h->mixed, a, s));
     return vhs_mixed(s, h->mixed, (const c128*)X, (c128*)V, W, std::sqrt(dt));
@@ -641,6 +642,12 @@ extern "C" int afqmc_ham_energy(afqmc_ham h, const afqmc_c128* G, afqmc_c128* E,
   return ham_energy(h, reinterpret_cast<cudaStream_t>(stream), (const c128*)G,
                     long(h->nel_tot) * h->M, (c128*)E, W, addH1 != 0, addEJ != 0, addEXX != 0,
                     precision);
+}
+
+extern "C" int afqmc_ham_set_mixed_ops(afqmc_ham h, int mask) {
+  AFQMC_CHECK_ARG(h && (mask & ~AFQMC_MIXED_ALL) == 0, "afqmc_ham_set_mixed_ops: bad mask");
+  h->mixed_ops = mask;
+  return AFQMC_OK;
 }
 
 extern "C" int afqmc_ham_set_coulomb_fp64(afqmc_ham h, int on) {
@@ -1512,7 +1519,9 @@ int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* E
   const int W = ws->W, M = h->M, Nc = h->Nc;
   const double dt = pr->p.dt;
   const long ldG = long(h->nel_tot) * M;
-  const bool mixed = pr->p.precision == AFQMC_PREC_MIXED;
+  const bool mixed_any = pr->p.precision == AFQMC_PREC_MIXED;
+  const bool mixed_v = mixed_any && (h->mixed_ops & AFQMC_MIXED_VBIAS);
+  const bool mixed = mixed_any && (h->mixed_ops & AFQMC_MIXED_PROPAGATION);
   // 1. vbias: G of the walkers (NOMSD::vbias, NOMSD.cpp:39-61); with AFQMC_STEP_G_READY the
   //    previous step left it for these walkers
   if (pr->md) {
@@ -1535,7 +1544,7 @@ int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* E
   }
   if (pr->ph || pr->md) {
     // vbias done above
-  } else if (mixed) {
+  } else if (mixed_v) {
     EnergyArgs a = energy_args(h, pr->G, ldG);
     if (!h->mixed) AFQMC_TRY(mixed_ham_create(&h->mixed, a, s));
     AFQMC_TRY(vbias_mixed(s, h->mixed, pr->G, ldG, pr->vb, W,

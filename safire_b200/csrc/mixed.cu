@@ -494,6 +494,8 @@ struct MixedHam {
   int taylor_slots = 0;   // 2 / 3: fused with one / two walkers in flight per CTA
   Planes G;         // [W][1][nel_tot*M]  (A of vbias);  exchange view [W*nel][M]
   Planes X;         // [1][W][Nc] (A of vHS)
+  c128* vpart = nullptr;  // split-K partial sums of vbias [S][W][Nc]
+  long vpart_elems = 0;
   unsigned* err = nullptr;
   // propagation buffers
   int capP = 0;
@@ -517,6 +519,7 @@ struct MixedHam {
     free_planes(Sst);
     for (auto& a : acc)
       if (a) cudaFree(a);
+    if (vpart) cudaFree(vpart);
     if (err) cudaFree(err);
   }
 };
@@ -584,6 +587,18 @@ int ensure_walker_buffers(MixedHam* m, int W) {
 
 }  // namespace
 
+namespace {
+// v[i] (+)= sum_s part[s][i] in FP64
+__global__ void sum_partials_kernel(const c128* __restrict__ part, int S, long n,
+                                    c128* __restrict__ v, int accumulate) {
+  const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  c128 acc = accumulate ? v[i] : cmk(0, 0);
+  for (int z = 0; z < S; ++z) acc = cadd(acc, part[long(z) * n + i]);
+  v[i] = acc;
+}
+}  // namespace
+
 // vbias = a * G Lnak^T (Real3IndexFactorization.hpp:384): A = G planes [W][nel*M], B = Lnak
 // [Nc][nel*M] (per spin block: the K range of the spin's rows of G).
 int vbias_mixed(cudaStream_t s, MixedHam* m, const c128* G, long ldG, c128* v, int W, double a) {
@@ -600,19 +615,64 @@ int vbias_mixed(cudaStream_t s, MixedHam* m, const c128* G, long ldG, c128* v, i
     if (Ns == 0) continue;
     const long K = long(Ns) * m->M;
     const long off = long(m->el_off[sp]) * m->M;
+    // Split K = N M into S equal ranges (a multiple of 4 floats each): every range is one batch
+    // of the GEMM, accumulated in FP32 on the tensor cores over K / S only, and the S partial
+    // sums are added in FP64.  The shorter FP32 sums cut the accumulation error, and S times as
+    // many output tiles fill the SMs (W / 128 x Nc / 128 tiles alone are fewer than 148).
+    int S = 1;
+    for (int c = 16; c >= 2; --c)
+      if (K % c == 0 && (K / c) % 4 == 0 && K / c >= 512) {
+        S = c;
+        break;
+      }
+    const int bn_rows = m->lnak_cplx ? 64 : 128;
     TcParams p{};
-    for (int q = 0; q < 4; ++q)
-      AFQMC_TRY(make_map(&p.a[q], m->G.p[q] + off, K, W, m->G.ld, 1, long(W) * m->G.ld, 128));
-    AFQMC_TRY(maps_for(m->Lnak[sp], p.b, m->lnak_cplx ? 64 : 128));
-    p.m = W; p.n = m->Nc; p.k = int(K);
-    p.order = 1;  // a G tile (128 walkers x K) stays in L2 while the Lnak tiles stream past it
-    p.alpha = cmk(a, 0);
-    p.out_c = v; p.outc_ld = m->Nc; p.outc_bs = 0;
-    p.err = m->err;
-    if (m->lnak_cplx)
-      AFQMC_TRY((launch_tc<true, true, 64, 2, EPI_C128>(s, p, 1)));
-    else
-      AFQMC_TRY((launch_tc<true, false, 128, 2, EPI_C128>(s, p, 1)));
+    bool split = false;
+    if (S > 1 && !m->lnak_cplx) {
+      const long Kc = K / S;
+      const long need = long(S) * W * m->Nc;
+      if (m->vpart_elems < need) {
+        if (m->vpart) cudaFree(m->vpart);
+        m->vpart = nullptr;
+        m->vpart_elems = 0;
+        AFQMC_CUDA_TRY(cudaMalloc(&m->vpart, sizeof(c128) * need));
+        m->vpart_elems = need;
+      }
+      // 3-D maps whose third coordinate steps through the K ranges (stride Kc floats)
+      split = true;
+      for (int q = 0; q < 4 && split; ++q)
+        split = make_map(&p.a[q], m->G.p[q] + off, Kc, W, m->G.ld, S, Kc, 128) == AFQMC_OK;
+      for (int q = 0; q < 2 && split; ++q)
+        split = make_map(&p.b[q], m->Lnak[sp].p[q], Kc, m->Nc, m->Lnak[sp].ld, S, Kc,
+                         bn_rows) == AFQMC_OK;
+      if (split) {
+        p.m = W; p.n = m->Nc; p.k = int(Kc);
+        p.a_batched = 1; p.b_batched = 1;
+        p.order = 1;
+        p.alpha = cmk(a, 0);
+        p.out_c = m->vpart; p.outc_ld = m->Nc; p.outc_bs = long(W) * m->Nc;
+        p.err = m->err;
+        AFQMC_TRY((launch_tc<true, false, 128, 2, EPI_C128>(s, p, S)));
+        const long n = long(W) * m->Nc;
+        sum_partials_kernel<<<ceil_div(n, 256), 256, 0, s>>>(m->vpart, S, n, v, first ? 0 : 1);
+        AFQMC_TRY(launch_status("sum_partials_kernel"));
+      }
+    }
+    if (!split) {
+      p = TcParams{};
+      for (int q = 0; q < 4; ++q)
+        AFQMC_TRY(make_map(&p.a[q], m->G.p[q] + off, K, W, m->G.ld, 1, long(W) * m->G.ld, 128));
+      AFQMC_TRY(maps_for(m->Lnak[sp], p.b, bn_rows));
+      p.m = W; p.n = m->Nc; p.k = int(K);
+      p.order = 1;  // a G tile (128 walkers x K) stays in L2 while the Lnak tiles stream past it
+      p.alpha = cmk(a, 0);
+      p.out_c = v; p.outc_ld = m->Nc; p.outc_bs = 0;
+      p.err = m->err;
+      if (m->lnak_cplx)
+        AFQMC_TRY((launch_tc<true, true, 64, 2, EPI_C128>(s, p, 1)));
+      else
+        AFQMC_TRY((launch_tc<true, false, 128, 2, EPI_C128>(s, p, 1)));
+    }
     first = false;
   }
   return AFQMC_OK;
