@@ -450,6 +450,31 @@ def run_ours(args):
                 "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                 "peak_source": peak_src, "flops_per_launch": flops[top],
                 "block_share_ms": block_share}
+    if top == "energy_measurement" and prec == A.PREC_MIXED:
+        # the dominant kernel on its own: the fused exchange contraction (with its G split and
+        # the final sums), timed with CUDA events on the launching stream
+        G, _ = sim.wfn.MixedDensityMatrix(sim.wset)
+        E = torch.empty((W, 3), dtype=torch.complex128, device=G.device)
+        sim.ham.energy(E, G, addH1=False, precision=prec)
+        stream = torch.cuda.current_stream()
+        x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 5
+        x0.record(stream)
+        for _ in range(reps):
+            sim.ham.energy(E, G, addH1=False, precision=prec)
+        x1.record(stream)
+        torch.cuda.synchronize()
+        t_x = x0.elapsed_time(x1) / reps
+        del G, E
+        # DRAM bytes per launch from the ncu capture at 128 walkers (155.7 MB read + 10.1 MB
+        # written = Lnak planes once + G planes and the per-(walker, vector) sums), scaled to W:
+        # 2 Lnak planes + W x (4 G planes + 2 complex outputs per Cholesky vector)
+        traffic = 2 * Nc * N * M * 4 + W * (4 * N * M * 4 + 2 * Nc * 16)
+        roofline.update({"kernel": "exchange_tc_kernel<3> (fused EXX/EJ contraction)",
+                         "achieved": flops[top] / (t_x / 1000) / 1e12,
+                         "frac": flops[top] / (t_x / 1000) / 1e12 / peak,
+                         "launch_ms": t_x, "traffic": traffic,
+                         "traffic_source": "ncu capture at 128 walkers, scaled by walkers"})
 
     # the synthetic system's total weight collapses after ~200 steps: restart from the trial
     sim.restart()
