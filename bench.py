@@ -48,6 +48,12 @@ def parse():
                          "phmsd: the particle-hole multi-determinant system; control-variate: "
                          "the learned exchange estimator's cost at equal error bar")
     ap.add_argument("--cv-epochs", type=int, default=30)
+    ap.add_argument("--cv-fraction", type=float, default=1.0 / 8,
+                    help="walkers (or draws) evaluated exactly per measurement")
+    ap.add_argument("--cv-sampling", default="weight", choices=["uniform", "weight"])
+    ap.add_argument("--cv-lowrank", type=int, default=-1,
+                    help="leading Cholesky vectors of the low-fidelity exchange base (0: none, "
+                         "-1: Nc / 16)")
     ap.add_argument("--cv-system", default="cfg2", choices=["cfg1", "cfg2"],
                     help="control-variate workload: cfg2 = M=200 N=50+50 Nc=1600, cfg1 = M=32 "
                          "N=8+8 Nc=128")
@@ -533,16 +539,17 @@ def run_ours(args):
 
 def run_control_variate(args):
     """The learned exchange control variate on the M=200 workload (mixed precision): pairs from
-    the exact kernel over 500 equilibration steps train the MLP; afterwards every measurement is
-    timed both ways (all-exact vs network on all walkers + exact exchange on a random 1/8), and the
-    cost ratio at equal statistical error bar is reported with the estimator's spread."""
+    the exact kernel over the first steps train the MLP on top of the exchange over the leading
+    Nc / 16 Cholesky vectors; afterwards every measurement is timed both ways (all-exact vs the
+    base + network on all walkers + exact exchange on 1/8 weight-proportional draws), and the cost
+    ratio at equal statistical error bar is reported with the estimator's spread."""
     import numpy as np
     import torch
     import torch.distributed as dist
 
     from safire_b200 import afqmc as A
     from safire_b200.driver import RunParams, Simulation
-    from safire_b200.mlp import ExchangeControlVariate
+    from safire_b200.mlp import ExchangeControlVariate, lowrank_hamiltonian
     from safire_b200.synth import make_workload
 
     world, rank, local = _init_dist()
@@ -559,7 +566,14 @@ def run_control_variate(args):
     sim = Simulation.from_workload(wl, W=W, precision=A.PREC_MIXED,
                                    rp=RunParams(equilibration_steps=eq_steps, seed=0))
     sim.use_graph = not args.no_graph
-    cv = ExchangeControlVariate(sim, hidden=512, fraction=1.0 / 8, seed=0)
+    lowrank = None
+    if args.cv_lowrank < 0:
+        args.cv_lowrank = wl.Nc // 16
+    if args.cv_lowrank:
+        lowrank = lowrank_hamiltonian((wl.walker_type, wl.M, wl.nup, wl.ndn, wl.Likn, wl.hij,
+                                       wl.E0, wl.PsiT), args.cv_lowrank)
+    cv = ExchangeControlVariate(sim, hidden=512, fraction=args.cv_fraction, seed=0,
+                                sampling=args.cv_sampling, lowrank=lowrank)
     for step in range(equil):
         sim.step(measure=False)
         if step % every == 0:
@@ -591,6 +605,9 @@ def run_control_variate(args):
             mf_e.append(e_mf)
             t_ex.append(te)
             t_mf.append(tm)
+    # the Coulomb term the estimator takes from the force bias against the energy kernel's
+    _, o = cv.measure(exact=True)
+    ej_gap = (o["ej_from_vbias"] - o["ej_exact"]).real
     exact_e, mf_e = np.array(exact_e), np.array(mf_e)
     diff = mf_e - exact_e
     s_qmc = float(np.std(exact_e, ddof=1))
@@ -611,8 +628,12 @@ def run_control_variate(args):
                                    f"dt={wl.dt}; MLP {cv.mlp.D}-512-512-1 GELU trained on pairs "
                                    f"from the first {equil} steps (one set per {every} steps"
                                    f"{', fixed Eshift' if eq_steps == 0 else ''}); exact "
-                                   "exchange on 1/8 of the walkers per measurement; one "
-                                   "measurement per 10-step block",
+                                   f"exchange on {args.cv_fraction:.3g} of the walkers "
+                                   f"({args.cv_sampling} draws) per measurement; "
+                                   + (f"network on top of the exchange over the leading "
+                                      f"{args.cv_lowrank} Cholesky vectors; "
+                                      if args.cv_lowrank else "")
+                                   + "one measurement per 10-step block",
                        "training_samples": int(sum(x.shape[0] for x in cv.X)),
                        "epochs": args.cv_epochs, "train_seconds": t_train,
                        "loss_first_last": [hist[0], hist[-1]]},
@@ -620,7 +641,8 @@ def run_control_variate(args):
             "sigma": {"qmc_between_measurements": s_qmc, "subsampling": s_sub,
                       "measurements_factor_for_equal_error": factor},
             "bias": {"mean_mf_minus_exact": float(diff.mean()),
-                     "standard_error": float(s_sub / np.sqrt(diff.size))},
+                     "standard_error": float(s_sub / np.sqrt(diff.size)),
+                     "ej_from_vbias_minus_energy_kernel": float(ej_gap)},
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -499,8 +499,9 @@ int afqmc_mlp_set_normalization(afqmc_mlp mlp, const float* mean, const float* i
 int afqmc_mlp_params(afqmc_mlp mlp, int which, float* host, int to_device);
 /* y [B] (device) = prediction for features X [B][D] (device) */
 int afqmc_mlp_predict(afqmc_mlp mlp, const float* X, int B, float* y, afqmc_stream stream);
-/* forward + backward of the loss mean((y - t)^2) / 2 in standardised units for X [B][D],
- * t [B]; gradients kept in the handle; loss (device float, may be NULL) */
+/* forward + backward of the Huber loss (threshold 2: r^2 / 2 inside, 2 (|r| - 1) outside, r =
+ * y - t) averaged over the batch in standardised units for X [B][D], t [B]; gradients kept in the
+ * handle; loss (device float, may be NULL) */
 int afqmc_mlp_gradients(afqmc_mlp mlp, const float* X, const float* t, int B, float* loss,
                         afqmc_stream stream);
 /* afqmc_mlp_gradients followed by one Adam step (beta 0.9 / 0.999, eps 1e-8) */

@@ -3,8 +3,9 @@ the multi-fidelity estimator, the checker for safire_b200/csrc/mlp.cu.
 
 Network (no reference counterpart): standardised features xn = (x - mean) * istd, then
 z1 = xn W1^T + b1, a1 = gelu(z1), z2 = a1 W2^T + b2, a2 = gelu(z2), y = a2 . w3 + b3 in
-standardised target units; prediction = y * y_std + y_mean.  Loss = mean((y - tn)^2) / 2 with
-tn = (t - y_mean) / y_std.  Parameters are one flat block [W1 | b1 | W2 | b2 | w3 | b3].
+standardised target units; prediction = y * y_std + y_mean.  Loss = mean Huber(y - tn) with
+tn = (t - y_mean) / y_std and threshold HUBER (r^2 / 2 inside, HUBER (|r| - HUBER / 2) outside).
+Parameters are one flat block [W1 | b1 | W2 | b2 | w3 | b3].
 
 Estimator: with exact values e_s on a uniform random subset S (|S| = k, without replacement) of
 the W walkers and predictions f_w on all of them, the weighted sum sum_w omega_w e_w is estimated
@@ -15,6 +16,14 @@ from __future__ import annotations
 import math
 
 import numpy as np
+
+HUBER = 2.0
+
+
+def _huber(r):
+    a = np.abs(r)
+    loss = np.where(a <= HUBER, 0.5 * r * r, HUBER * (a - 0.5 * HUBER))
+    return np.mean(loss), np.clip(r, -HUBER, HUBER) / r.size
 
 
 def split_params(p, D, H):
@@ -61,8 +70,7 @@ def loss_and_grad(p, X, t, D, H, mean, istd, y_mean, y_std):
     y, (xn, z1, a1, z2, a2) = forward(p, X, D, H, mean, istd)
     B = y.size
     r = y - (np.asarray(t, np.float64) - y_mean) / y_std
-    loss = 0.5 * np.mean(r * r)
-    dy = r / B
+    loss, dy = _huber(r)
     dw3 = a2.T @ dy
     db3 = np.array([dy.sum()])
     dz2 = np.outer(dy, w3) * gelu_grad(z2)
@@ -106,10 +114,18 @@ def loss_and_grad_bf16(p, X, t, D, H, mean, istd, y_mean, y_std):
     y = a2 @ w3 + b3[0]
     B = y.size
     r = y - (np.asarray(t, np.float64) - y_mean) / y_std
-    loss = 0.5 * np.mean(r * r)
-    dy = r / B
+    loss, dy = _huber(r)
     dz2 = bf16(np.outer(dy, w3) * gelu_grad(z2)).astype(np.float64)
     dz1 = bf16((dz2 @ W2b) * gelu_grad(z1)).astype(np.float64)
     g = np.concatenate([(dz1.T @ xn).ravel(), dz1.sum(0), (dz2.T @ a1).ravel(), dz2.sum(0),
                         a2.T @ dy, [dy.sum()]])
     return y, loss, g
+
+
+def multifidelity_sum_weighted(omega, f, exact, draws, prob):
+    """The Horvitz-Thompson form for k draws with replacement at probabilities prob:
+    sum_w omega_w f_w + sum_{draws j} omega_j (e_j - f_j) / (k prob_j); unbiased for any f."""
+    omega, f, exact, prob = (np.asarray(x) for x in (omega, f, exact, prob))
+    draws = np.asarray(draws)
+    k = draws.size
+    return np.sum(omega * f) + np.sum(omega[draws] * (exact[draws] - f[draws]) / (k * prob[draws]))

@@ -140,8 +140,11 @@ __global__ void standardize_kernel(const float* __restrict__ X, const float* __r
   Xn[i] = __float2bfloat16((X[i] - mean[d]) * istd[d]);
 }
 
-// y[b] = A[b] . w3 + b3 (one warp per row); with target: dy[b] = (y[b] - t[b]) / B and the
-// loss sum_b (y - t)^2 / (2 B) accumulated into loss[0]
+// y[b] = A[b] . w3 + b3 (one warp per row); with target: the Huber loss of r = y - t with
+// threshold HUBER (r^2 / 2 inside, HUBER (|r| - HUBER / 2) outside) averaged over the batch into
+// loss[0] and its derivative clamp(r, -HUBER, HUBER) / B into dy[b]: heavy-tailed exchange
+// energies then cannot blow up a step
+constexpr float HUBER = 2.0f;
 __global__ void head_kernel(const bf16* __restrict__ A, const float* __restrict__ w3,
                             const float* __restrict__ b3, int B, int H, float* __restrict__ y,
                             const float* __restrict__ target, float* __restrict__ dy,
@@ -157,8 +160,9 @@ __global__ void head_kernel(const bf16* __restrict__ A, const float* __restrict_
     if (y) y[b] = v;
     if (target) {
       const float r = v - target[b];
-      dy[b] = r / B;
-      atomicAdd(loss, 0.5f * r * r / B);
+      const float a = fabsf(r);
+      dy[b] = fminf(fmaxf(r, -HUBER), HUBER) / B;
+      atomicAdd(loss, (a <= HUBER ? 0.5f * r * r : HUBER * (a - 0.5f * HUBER)) / B);
     }
   }
 }

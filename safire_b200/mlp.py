@@ -123,18 +123,36 @@ def exchange_features(vbias, G, N, M, E=None, stream=None):
     return X
 
 
+def lowrank_hamiltonian(ham_args, k):
+    """A HamiltonianOperations over the first k Cholesky vectors: ham_args = (walker_type, M, nup,
+    ndn, Likn [nspin_H2][M][M][Nc], hij, E0, PsiT) as HamiltonianOperations takes them."""
+    walker_type, M, nup, ndn, Likn, hij, E0, PsiT = ham_args
+    return A.HamiltonianOperations(walker_type, M, nup, ndn,
+                                   np.ascontiguousarray(np.asarray(Likn)[..., :k]), hij, E0, PsiT)
+
+
 class ExchangeControlVariate:
     """Multi-fidelity exchange energy for a Simulation (safire_b200.driver): collect pairs during
     equilibration, fit, then measure with the exact exchange on a random fraction of walkers."""
 
-    def __init__(self, sim, hidden=512, fraction=1.0 / 8, seed=0, scalars=False):
-        """scalars: also feed each walker's E1 and EJ to the network."""
+    def __init__(self, sim, hidden=512, fraction=1.0 / 8, seed=0, scalars=False,
+                 sampling="uniform", lowrank=None):
+        """scalars: also feed each walker's E1 and EJ to the network.  sampling: "uniform" (k
+        distinct walkers) or "weight" (k draws with probability |w| / sum |w|, with replacement:
+        the correction is then a Horvitz-Thompson sum, still unbiased, and concentrates the exact
+        evaluations on the walkers that carry the estimate).  lowrank: an optional
+        HamiltonianOperations over the leading Cholesky vectors (lowrank_hamiltonian); its
+        exchange energy EXX_k of every walker (real and imaginary parts) is a further feature and
+        the network learns the remainder EXX - EXX_k, so the prediction is EXX_k + network."""
+        self.sampling = sampling
         self.sim = sim
         ham = sim.ham
         self.N, self.M, self.Nc = ham.nup, ham.M, ham.Nc
         self.nel = ham.nel
         self.scalars = scalars
-        self.mlp = ExchangeMLP(2 * self.Nc + 2 * self.N + (4 if scalars else 0), hidden, seed)
+        self.lowrank = lowrank
+        D = 2 * self.Nc + 2 * self.N + (4 if scalars else 0) + (2 if lowrank else 0)
+        self.mlp = ExchangeMLP(D, hidden, seed)
         self.fraction = fraction
         self.rng = np.random.default_rng(seed)
         self.X, self.y = [], []
@@ -152,16 +170,26 @@ class ExchangeControlVariate:
         E = torch.empty((sim.wset.W, 3), dtype=torch.complex128, device=G.device)
         sim.ham.energy(E, G, addH1=True, addEJ=False, addEXX=False, precision=sim.precision)
         E[:, 2] = (self._v * self._v).sum(1) / (2.0 * sim.dt)
-        return G, E, exchange_features(self._v, G, self.N, self.M, E if self.scalars else None)
+        X = exchange_features(self._v, G, self.N, self.M, E if self.scalars else None)
+        base = None
+        if self.lowrank is not None:
+            Ek = torch.empty_like(E)
+            self.lowrank.energy(Ek, G, addH1=False, addEJ=False, addEXX=True,
+                                precision=sim.precision)
+            base = Ek[:, 1]
+            X = torch.cat([X, torch.view_as_real(base).float()], 1)
+        return G, E, X, base
 
     def collect(self):
-        """One training sample per walker: features and the exact exchange energy."""
-        G, _, X = self._features()
+        """One training sample per walker: features and the exact exchange energy (less the
+        leading-vector exchange with lowrank)."""
+        G, _, X, base = self._features()
         E = torch.empty((self.sim.wset.W, 3), dtype=torch.complex128, device=G.device)
         self.sim.ham.energy(E, G, addH1=False, addEJ=False, addEXX=True,
                             precision=self.sim.precision)
         self.X.append(X)
-        self.y.append(E[:, 1].real.float())
+        y = E[:, 1] if base is None else E[:, 1] - base
+        self.y.append(y.real.float())
 
     def fit(self, epochs=30, batch=1024, lr=1e-3):
         X = torch.cat(self.X)
@@ -175,16 +203,28 @@ class ExchangeControlVariate:
         sim = self.sim
         W = sim.wset.W
         # E1 and EJ exactly for every walker
-        G, E, X = self._features()
+        G, E, X, base = self._features()
         dev = G.device
         w = sim.wset.properties()[:, capi.WEIGHT]
         f = self.mlp.predict(X).double()
+        if base is not None:
+            f = base + f
         k = max(1, int(round(self.fraction * W)))
-        S = torch.as_tensor(np.sort(self.rng.choice(W, size=k, replace=False)), device=dev)
-        Es = torch.empty((k, 3), dtype=torch.complex128, device=dev)
+        if self.sampling == "weight":
+            aw = w.abs().cpu().numpy()
+            prob = aw / aw.sum()
+            draws = self.rng.choice(W, size=k, replace=True, p=prob)
+            uniq, cnt = np.unique(draws, return_counts=True)
+            S = torch.as_tensor(uniq, device=dev)
+            # sum over draws of w_s (e_s - f_s) / (k p_s), evaluated once per distinct walker
+            scale = torch.as_tensor(cnt / (k * prob[uniq]), dtype=torch.float64, device=dev)
+        else:
+            S = torch.as_tensor(np.sort(self.rng.choice(W, size=k, replace=False)), device=dev)
+            scale = torch.full((k,), W / k, dtype=torch.float64, device=dev)
+        Es = torch.empty((S.numel(), 3), dtype=torch.complex128, device=dev)
         sim.ham.energy(Es, G[S].contiguous(), addH1=False, addEJ=False, addEXX=True,
                        precision=sim.precision)
-        ex_mf = (w * f).sum() + (W / k) * (w[S] * (Es[:, 1] - f[S])).sum()
+        ex_mf = (w * f).sum() + (scale * w[S] * (Es[:, 1] - f[S])).sum()
         wsum = w.sum()
         e_other = (w * (E[:, 0] + E[:, 2])).sum()
         out = {"exx_mf": complex((ex_mf / wsum).item())}

@@ -121,3 +121,46 @@ def test_control_variate_on_a_run(cuda):
     plain = [O.multifidelity_sum(w, np.zeros_like(e), e[S], S) / w.sum()
              for S in (np.sort(rs.choice(e.size, 32, replace=False)) for _ in range(64))]
     assert ests.std() < 0.5 * np.std(plain), (ests.std(), np.std(plain))
+
+
+def test_control_variate_leading_cholesky(cuda):
+    """The low-fidelity base EXX_k over the leading Cholesky vectors: with all Nc vectors it is the
+    exact exchange, and the estimate equals the exact one for any subset; with Nc / 8 vectors the
+    estimate stays unbiased over random subsets and beats subsampling on the remainder alone."""
+    from safire_b200 import capi
+    from safire_b200.driver import RunParams, Simulation
+    from safire_b200.mlp import ExchangeControlVariate, lowrank_hamiltonian
+    from safire_b200.synth import make_workload
+    wl = make_workload("cfg1", W=128)
+    args = (wl.walker_type, wl.M, wl.nup, wl.ndn, wl.Likn, wl.hij, wl.E0, wl.PsiT)
+    sim = Simulation.from_workload(wl, W=128, rp=RunParams(equilibration_steps=1000, seed=3))
+    for _ in range(20):
+        sim.step(measure=False)
+    for k, tol in ((wl.Nc, 1e-9), (wl.Nc // 8, None)):
+        cv = ExchangeControlVariate(sim, hidden=128, fraction=1 / 8, seed=0,
+                                    lowrank=lowrank_hamiltonian(args, k))
+        assert cv.mlp.D == 2 * wl.Nc + 2 * wl.nup + 2
+        for _ in range(6):
+            sim.step(measure=False)
+            cv.collect()
+        cv.fit(epochs=20, batch=256, lr=1e-3)
+        ests, exact = [], None
+        for _ in range(48):
+            _, o = cv.measure(exact=exact is None)
+            exact = o["exx_exact"] if exact is None else exact
+            ests.append(o["exx_mf"].real)
+        ests = np.array(ests)
+        if tol is not None:
+            assert np.all(np.abs(ests - exact.real) < tol * abs(exact.real)), (ests[:4], exact)
+            continue
+        se = ests.std(ddof=1) / np.sqrt(ests.size)
+        assert abs(ests.mean() - exact.real) < 4 * se + 1e-9 * abs(exact.real)
+        w = sim.wset.properties()[:, capi.WEIGHT].real.cpu().numpy()
+        G, _ = sim.wfn.MixedDensityMatrix(sim.wset)
+        E = torch.empty((sim.wset.W, 3), dtype=torch.complex128, device=G.device)
+        sim.ham.energy(E, G, addH1=False, addEJ=False, addEXX=True)
+        e = E[:, 1].real.cpu().numpy()
+        rs = np.random.default_rng(5)
+        plain = [O.multifidelity_sum(w, np.zeros_like(e), e[S], S) / w.sum()
+                 for S in (np.sort(rs.choice(e.size, 16, replace=False)) for _ in range(48))]
+        assert ests.std() < 0.5 * np.std(plain), (ests.std(), np.std(plain))

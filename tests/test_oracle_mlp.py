@@ -52,3 +52,18 @@ def test_multifidelity_estimator_is_unbiased():
     ests = [O.multifidelity_sum(omega, e, e[list(S)], list(S))
             for S in itertools.combinations(range(W), k)]
     assert np.max(np.abs(np.array(ests) - np.sum(omega * e))) < 1e-12
+
+
+def test_weighted_draw_estimator_is_unbiased():
+    """Expectation over the multinomial draws (enumerated exactly for k = 2) equals the exact
+    weighted sum for any f and any positive draw probabilities."""
+    rs = np.random.default_rng(4)
+    W = 6
+    omega = rs.random(W) + 0.1
+    e, f = rs.standard_normal(W), rs.standard_normal(W)
+    prob = omega / omega.sum()
+    exp = 0.0
+    for a in range(W):
+        for b in range(W):
+            exp += prob[a] * prob[b] * O.multifidelity_sum_weighted(omega, f, e, [a, b], prob)
+    assert abs(exp - np.sum(omega * e)) < 1e-12
