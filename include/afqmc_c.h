@@ -392,7 +392,10 @@ int afqmc_ph_excited_1body_energy(const int* iexcit, const int* refc, const afqm
  * active orbital of every electron in the reference; unique excitations u = 1..nuniq_s-1 of each
  * spin (u = 0 is the reference): nex_s[u-1] holes/particles each, their lists concatenated in
  * exc_s as [holes (electron indices), particles (active orbitals)]; determinant k couples unique
- * excitations det_up[k], det_dn[k] with coefficient coef[k].  Every index is validated.
+ * excitations det_up[k], det_dn[k] with coupling coef[k] = conj(c_k) for the trial
+ * sum_k c_k |D_k> (the reference's determinant couplings hold the conjugated CI coefficients,
+ * Wavefunction.cpp:458-464), so the overlap is sum_k coef[k] <D_k|phi>.  Every index is
+ * validated.
  * (afqmc_phmsd is declared with the propagator above.) */
 int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact_dn,
                        const afqmc_c128* orbmat_up, const afqmc_c128* orbmat_dn,

@@ -124,19 +124,28 @@ class Simulation:
 
     @staticmethod
     def from_workload(wl, W=None, precision=A.PREC_FP64, rp=None, trial=None, vMF=None,
-                      **prop_kw):
+                      multidet=None, **prop_kw):
         """wl: a safire_b200.synth.Workload.  trial: an optional PHMSD trial
         (safire_b200.synth.PHMSDTrial, COLLINEAR workload whose PsiT is its reference
-        determinant); vMF: its mean field [Nc] (host), default the reference determinant's."""
+        determinant); multidet: an optional several-determinant NOMSD trial (PsiTs, ci) with
+        PsiTs[d] the per-spin PsiT of determinant d (wl.PsiT is determinant 0's); vMF: the mean
+        field [Nc] (host) of either, default determinant 0's."""
         rp = rp or RunParams()
         W = W or wl.W
         ham = A.HamiltonianOperations(wl.walker_type, wl.M, wl.nup, wl.ndn, wl.Likn, wl.hij,
                                       wl.E0, wl.PsiT)
         ph = None
+        if trial is not None and multidet is not None:
+            raise ValueError("a PHMSD trial and a several-determinant NOMSD trial exclude each other")
         if trial is not None:
             ph = A.PHMSD(trial)
             ph.set_hamiltonian(wl.Likn, wl.hij, wl.E0)
             wfn = A.PHMSDWavefunction(ph)
+        elif multidet is not None:
+            PsiTs, ci = multidet
+            hams = [ham] + [A.HamiltonianOperations(wl.walker_type, wl.M, wl.nup, wl.ndn, wl.Likn,
+                                                    wl.hij, wl.E0, P) for P in PsiTs[1:]]
+            ph = wfn = A.NOMSDMulti(hams, ci)
         else:
             wfn = A.NOMSD(ham)
         wset = A.WalkerSet(wl.walker_type, wl.M, wl.nup, wl.ndn, W)
@@ -154,7 +163,7 @@ class Simulation:
         relax = 1 - math.exp(-10.0 / n) if n > 1 else 1.0
         sim = Simulation(ham, wfn, wset, prop, walker_rng, rp, wl.dt, Eshift, relax, precision)
         if ph is not None:
-            sim.reuse_density = False  # the PHMSD step recomputes its density matrix
+            sim.reuse_density = False  # the multi-determinant step recomputes its density matrix
         return sim
 
     def restart(self):

@@ -86,7 +86,9 @@ class PHMSDTrial:
     unique excitations of that spin, holes as electron indices then particles as active
     orbitals).  Unique index 0 is the reference; then the nex = 1 list, nex = 2, ... in order.
     A determinant k couples unique alpha excitation det_up[k] with unique beta excitation
-    det_dn[k] and has coefficient coef[k]."""
+    det_dn[k] and has coupling coefficient coef[k]: the conjugate of its coefficient c_k in
+    |Psi_T> = sum_k c_k |D_k>, as the reference stores the determinant couplings
+    (Wavefunction.cpp:458-464), so the overlap is sum_k coef_k <D_k|phi>."""
     M: int
     nup: int
     ndn: int
@@ -184,8 +186,9 @@ def phmsd_trial_from_occupations(M, orbmat, refc, occ_up, occ_dn, coef):
     """A PHMSDTrial from a determinant expansion given as occupation lists: orbmat[s] [nact_s][M]
     (active orbitals, conjugate-transposed), refc[s] [N_s] the reference, occ_up / occ_dn
     [ndet][N_s] each determinant's occupied active orbitals in the column order of its coefficient
-    coef [ndet].  The particle-hole structure comes from afqmc_phmsd_excitations (the library's
-    host code); the permutation signs are folded into the coefficients."""
+    coef [ndet] (the wavefunction's c_k).  The particle-hole structure comes from
+    afqmc_phmsd_excitations (the library's host code); the permutation signs are folded into the
+    coefficients and the result holds their conjugates, the couplings of PHMSDTrial."""
     import ctypes as C
 
     from . import capi
@@ -213,4 +216,5 @@ def phmsd_trial_from_occupations(M, orbmat, refc, occ_up, occ_dn, coef):
         exc[s] = {n: np.array(v, dtype=np.int32).reshape(-1, 2 * n) for n, v in exc[s].items()}
         dets.append(di)
     return PHMSDTrial(M, occ[0].shape[1], occ[1].shape[1], [np.asarray(o) for o in orbmat],
-                      [np.asarray(r, dtype=np.int32) for r in refc], exc, dets[0], dets[1], coef)
+                      [np.asarray(r, dtype=np.int32) for r in refc], exc, dets[0], dets[1],
+                      np.conj(coef))

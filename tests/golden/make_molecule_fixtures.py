@@ -1,0 +1,120 @@
+"""Extract the molecular inputs and statistical reference energies of the reference's functional
+tests into committed fixtures, read with safire_b200's own HDF5 reader.
+
+Writes tests/golden/molecules.npz (Hamiltonians and trial wavefunctions of BH and N2) and
+tests/golden/molecule_references.json (the mixed-estimator energies with their error bars, the
+run settings, and the BH RHF mixed-estimator one-body density matrix).  Run from the repository
+root with the reference checked out at REFERENCE (default /root/reference):
+
+    python tests/golden/make_molecule_fixtures.py [REFERENCE]
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", ".."))
+
+from safire_b200 import inputs as I  # noqa: E402
+from safire_b200.h5 import File  # noqa: E402
+
+REF = "/root/reference"
+INP = os.path.join(REF, "tests/functional/afqmc_inputs")
+STAT = os.path.join(REF, "tests/functional/statistical_references")
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+HAMS = {"bh": "BH/afqmc_H_rhf_closed.h5", "n2": "N2/cas_basis_hamil.h5"}
+WFNS = {
+    "bh_rhf_nomsd": "BH/afqmc_rhf_nomsd.h5",
+    "bh_uhf_nomsd": "BH/afqmc_uhf_nomsd.h5",
+    "bh_casci_rhf_nomsd": "BH/afqmc_casci_rhf_nomsd.h5",
+    "bh_casci_rhf_phmsd": "BH/afqmc_casci_rhf_phmsd.h5",
+    "bh_casci_uhf_phmsd": "BH/afqmc_casci_uhf_phmsd.h5",
+    "n2_cas_phmsd": "N2/cas_wfn.h5",
+}
+# (case, hamiltonian, wavefunction, walker type, results.h5 below statistical_references)
+CASES = [
+    ("bh_rhf_closed", "bh", "bh_rhf_nomsd", "closed", "BH/dense_rhf_basis_closed/rhf_nomsd/closed"),
+    ("bh_rhf_collinear", "bh", "bh_rhf_nomsd", "collinear",
+     "BH/dense_rhf_basis_closed/rhf_nomsd/collinear"),
+    ("bh_uhf_collinear", "bh", "bh_uhf_nomsd", "collinear",
+     "BH/dense_rhf_basis_closed/uhf_nomsd/collinear"),
+    ("bh_casci_rhf_nomsd_closed", "bh", "bh_casci_rhf_nomsd", "closed",
+     "BH/dense_rhf_basis_closed/rcasci_rhf_nomsd/closed"),
+    ("bh_casci_rhf_phmsd_collinear", "bh", "bh_casci_rhf_phmsd", "collinear",
+     "BH/dense_rhf_basis_closed/rcasci_rhf_phmsd/collinear"),
+    ("bh_casci_uhf_phmsd_collinear", "bh", "bh_casci_uhf_phmsd", "collinear",
+     "BH/dense_rhf_basis_closed/rcasci_uhf_phmsd/collinear"),
+    ("n2_cas_phmsd_collinear", "n2", "n2_cas_phmsd", "collinear",
+     "N2/cas_basis_hamil_closed/cas_wfn_collinear/collinear"),
+]
+
+
+def _scalar(f, path):
+    return complex(np.asarray(f[path]).ravel()[0])
+
+
+def main():
+    global INP, STAT
+    if len(sys.argv) > 1:
+        INP = os.path.join(sys.argv[1], "tests/functional/afqmc_inputs")
+        STAT = os.path.join(sys.argv[1], "tests/functional/statistical_references")
+    arrays = {}
+    for key, rel in HAMS.items():
+        h = I.read_hamiltonian(os.path.join(INP, rel))
+        arrays[f"{key}/hcore"] = h.hcore
+        arrays[f"{key}/Likn"] = h.Likn
+        arrays[f"{key}/energies"] = np.array([h.nuclear_energy, h.frozen_core_energy,
+                                              h.madelung_constant])
+    for key, rel in WFNS.items():
+        w = I.read_wavefunction(os.path.join(INP, rel))
+        arrays[f"{key}/meta"] = np.array([w.walker_type, w.M, w.nup, w.ndn])
+        arrays[f"{key}/ci"] = w.ci
+        if isinstance(w, I.NOMSDInput):
+            for d, per_spin in enumerate(w.PsiT):
+                for s, p in enumerate(per_spin):
+                    arrays[f"{key}/PsiT_{d}_{s}"] = p
+        else:
+            arrays[f"{key}/occa"] = w.occa
+            arrays[f"{key}/occb"] = w.occb
+            for r, p in enumerate(w.references):
+                arrays[f"{key}/ref_{r}"] = p
+    np.savez_compressed(os.path.join(OUT, "molecules.npz"), **arrays)
+
+    refs = {}
+    for case, ham, wfn, walker, rel in CASES:
+        f = File(os.path.join(STAT, rel, "results.h5"))
+        inp = json.loads(str(f["input_file"]))
+        ex = inp["execute"]
+        m = "measurements/Stage0"
+        entry = {
+            "hamiltonian": ham, "wavefunction": wfn, "walker_type": walker,
+            "energy": _scalar(f, f"{m}/Energy/mean").real,
+            "energy_error": _scalar(f, f"{m}/Energy/error").real,
+            "components": {k: _scalar(f, f"{m}/{k}/mean").real
+                           for k in ("OnebodyEnergy", "CoulombEnergy", "ExchangeEnergy")},
+            "walkers": int(np.asarray(f["num_ranks"])) * int(ex.get("n_walkers_per_mpi_task",
+                                                                    ex.get("num_walkers", 0))),
+            "ranks": int(np.asarray(f["num_ranks"])),
+            "steps": ex["steps"], "timestep": ex["timestep"],
+            "equilibration_steps": ex["equilibration_steps"],
+            "population_control_interval": ex["population_control_interval"],
+            "measure_interval": ex["measure_interval"],
+            "walker_ortho_interval": ex["walker_ortho_interval"],
+            "seed": inp["seed"],
+            "source": f"tests/functional/statistical_references/{rel}/results.h5",
+        }
+        if case == "bh_rhf_closed":
+            g = np.asarray(f[f"{m}/MixedEstimator/OneRDM/mean"])
+            ge = np.asarray(f[f"{m}/MixedEstimator/OneRDM/error"])
+            entry["onerdm_real"] = g.real.tolist()
+            entry["onerdm_error_real"] = ge.real.tolist()
+        refs[case] = entry
+    with open(os.path.join(OUT, "molecule_references.json"), "w") as fh:
+        json.dump(refs, fh, indent=1)
+    print("wrote", len(arrays), "arrays and", len(refs), "references")
+
+
+if __name__ == "__main__":
+    main()
