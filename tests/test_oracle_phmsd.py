@@ -172,7 +172,8 @@ def test_phmsd_density_matrix_vs_single_determinants():
 def test_excitations_from_occupation_lists():
     """afqmc_phmsd_excitations (host code of the library, no GPU) turns occupation lists in
     arbitrary column order into the particle-hole structure: the Woodbury log overlap of the
-    resulting trial equals the sum over the determinants as given, sum_k c_k det(D_k^H S)."""
+    resulting trial equals the sum over the determinants as given, sum_k conj(c_k) det(D_k^H S)
+    (the trial is sum_k c_k |D_k>; its couplings hold the conjugates)."""
     from safire_b200.synth import phmsd_trial_from_occupations
     rs = np.random.default_rng(9)
     M, nup, ndn, nact, ndet = 14, 4, 3, 10, 25
@@ -195,6 +196,6 @@ def test_excitations_from_occupation_lists():
     Sd = rs.standard_normal((W, M, ndn)) + 1j * rs.standard_normal((W, M, ndn))
     logov, _ = P.phmsd_log_overlap(t, Su, Sd)
     for w in range(W):
-        tot = sum(coef[k] * np.linalg.det(orb[0][occ[0][k]] @ Su[w]) *
+        tot = sum(np.conj(coef[k]) * np.linalg.det(orb[0][occ[0][k]] @ Su[w]) *
                   np.linalg.det(orb[1][occ[1][k]] @ Sd[w]) for k in range(ndet))
         assert abs(np.exp(logov[w]) - tot) <= 1e-10 * abs(tot)
