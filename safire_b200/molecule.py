@@ -2,8 +2,8 @@
 
 `simulation` builds a safire_b200.driver.Simulation from a DenseHamiltonian and a trial read by
 safire_b200.inputs: a single NOMSD determinant, several NOMSD determinants (with the
-reference's pairwise mean field, NOMSD.cpp:466-520) or a PHMSD expansion (with the reference
-determinant's mean field).  `run` drives it with the run_afqmc cadence and returns the
+reference's pairwise mean field, NOMSD.cpp:466-520) or a PHMSD expansion (with the reference's
+PHMSD mean field, PHMSD.cpp:1330-1572).  `run` drives it with the run_afqmc cadence and returns the
 mixed-estimator energies; `blocked_mean` gives their mean and a blocking error bar.
 
 The command line takes the reference's JSON input (the document run_functional.py writes:
@@ -75,6 +75,84 @@ def nomsd_mean_field_density(PsiTs, ci, walker_type):
     return Gsum / osum
 
 
+def phmsd_configurations(trial, s):
+    """Occupied active orbitals of every unique configuration of spin s, sorted (index 0 the
+    reference, then the excitation shells in order)."""
+    ref = np.asarray(trial.refc[s])
+    out = [np.sort(ref)]
+    for n in sorted(trial.exc[s]):
+        for e in trial.exc[s][n]:
+            c = ref.copy()
+            c[e[:n]] = e[n:]
+            out.append(np.sort(c))
+    return out
+
+
+def phmsd_mean_field(trial, Likn, dt):
+    """PHMSD::vMF (PHMSD.cpp:1330-1572), COLLINEAR, restated on the host: the trial's one-body
+    density in the active representation, then the force bias of it.
+    - ov_s[u]: det(A_u^H A_u) of each unique configuration's orbitals (A = Orbs[:, conf], Orbs =
+      orbmat^H), relative to the reference's (all 1 for orthonormal orbitals);
+    - diagonal: each configuration adds w (A^H A)^-T A^T to its rows, w = ov_s[u] sum over its
+      determinants of ov_other |coupling|^2;
+    - off-diagonal: determinants that share the other spin's configuration and differ by one
+      orbital (o1 -> o2) add coupling1 conj(coupling2) orbmat[o1] to row o2 and the conjugate
+      weight times orbmat[o2] to row o1, without the overlap factor or the excitation's sign (as
+      the reference does; it assumes orthogonal orbitals);
+    - divided by sum_k |coupling_k|^2 ov_up ov_dn; then v[n] = sqrt(dt) sum_s sum_{a,m}
+      G_s[a][m] Lnak_s[n][a][m] with Lnak built from the active orbitals (Real3Index vbias,
+      COLLINEAR).  Returns vMF [Nc] (complex; the propagator keeps its real part)."""
+    L = np.asarray(Likn, dtype=np.float64)
+    M = trial.M
+    orb = [np.asarray(trial.orbmat[s], dtype=np.complex128) for s in (0, 1)]
+    Orbs = [o.conj().T for o in orb]
+    conf = [phmsd_configurations(trial, s) for s in (0, 1)]
+    det = [np.asarray(trial.det_up), np.asarray(trial.det_dn)]
+    c2 = np.abs(np.asarray(trial.coef)) ** 2
+    coup = np.asarray(trial.coef, dtype=np.complex128)
+    ovl = []
+    for s in (0, 1):
+        lo = []
+        for c in conf[s]:
+            A = Orbs[s][:, c]
+            sign, la = np.linalg.slogdet(A.conj().T @ A)
+            lo.append(np.log(sign + 0j) + la)
+        lo = np.array(lo)
+        o = np.exp(lo - lo[0])
+        o[0] = 1.0
+        ovl.append(o)
+    ov = np.sum(c2 * ovl[0][det[0]] * ovl[1][det[1]])
+    G = [np.zeros((orb[s].shape[0], M), dtype=np.complex128) for s in (0, 1)]
+    for s in (0, 1):
+        o = 1 - s
+        for u, c in enumerate(conf[s]):
+            ks = np.nonzero(det[s] == u)[0]
+            if ks.size == 0:
+                continue
+            w = ovl[s][u] * np.sum(ovl[o][det[o][ks]] * c2[ks])
+            A = Orbs[s][:, c]
+            G[s][c] += w * (np.linalg.inv(A.conj().T @ A).T @ A.T)
+        for u in range(len(conf[o])):
+            ks = np.nonzero(det[o] == u)[0]
+            for i1 in range(ks.size):
+                c1 = set(conf[s][det[s][ks[i1]]].tolist())
+                for i2 in range(i1 + 1, ks.size):
+                    c2set = set(conf[s][det[s][ks[i2]]].tolist())
+                    d1, d2 = c1 - c2set, c2set - c1
+                    if len(d1) != 1:
+                        continue
+                    o1, o2 = d1.pop(), d2.pop()
+                    w = coup[ks[i1]] * np.conj(coup[ks[i2]])
+                    G[s][o2] += w * orb[s][o1]
+                    G[s][o1] += np.conj(w) * orb[s][o2]
+    v = np.zeros(L.shape[3], dtype=np.complex128)
+    for s in (0, 1):
+        Ls = L[s % L.shape[0]]
+        Lnak = np.einsum("ai,imn->amn", orb[s], Ls)
+        v += np.einsum("am,amn->n", G[s] / ov, Lnak)
+    return math.sqrt(dt) * v
+
+
 def _workload(ham, wfn, W, dt, walker_type):
     if isinstance(wfn, PHMSDInput):
         trial = phmsd_trial(wfn)
@@ -92,7 +170,8 @@ def simulation(ham, wfn, W, dt, walker_type=None, rp=None, use_graph=True):
     rp = rp or RunParams()
     wl, trial = _workload(ham, wfn, W, dt, walker_type)
     if trial is not None:
-        sim = Simulation.from_workload(wl, W=W, rp=rp, trial=trial)
+        sim = Simulation.from_workload(wl, W=W, rp=rp, trial=trial,
+                                       vMF=phmsd_mean_field(trial, wl.Likn, dt))
         sim.use_graph = False
         return sim
     if wfn.ci.size > 1:

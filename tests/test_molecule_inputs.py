@@ -162,3 +162,53 @@ def test_blocked_mean():
     m, e = Mo.blocked_mean(x)
     assert abs(m - x.mean()) < 1e-15
     assert 0.5 / 40 < e < 2.0 / 40  # ~ 1 / sqrt(1600) for independent samples
+
+
+def _random_orbitals(rs, M, complex_=True):
+    A = rs.standard_normal((M, M)) + (1j * rs.standard_normal((M, M)) if complex_ else 0)
+    Q = np.linalg.qr(A)[0]
+    return np.ascontiguousarray(Q.conj().T)  # rows: conjugated orbitals
+
+
+def test_phmsd_mean_field_single_determinant_is_nomsd():
+    """One determinant: the PHMSD mean field equals NOMSD::vMF of that determinant."""
+    from safire_b200.synth import phmsd_trial_from_occupations
+    rs = np.random.default_rng(4)
+    M, nup, ndn, Nc, dt = 9, 3, 2, 7, 0.01
+    orb = _random_orbitals(rs, M)
+    L = rs.standard_normal((1, M, M, Nc))
+    L = 0.5 * (L + L.transpose(0, 2, 1, 3))
+    refc = [np.arange(nup), np.arange(ndn)]
+    tr = phmsd_trial_from_occupations(M, [orb, orb], refc, refc[0][None], refc[1][None],
+                                      np.array([0.7 - 0.2j]))
+    v = Mo.phmsd_mean_field(tr, L, dt)
+    psi = [orb[:nup], orb[:ndn]]
+    hij = np.zeros((2, M, M), complex)
+    ham = O.Real3IndexFactorization(I.COLLINEAR, M, nup, ndn, L, hij, 0.0, psi)
+    assert np.allclose(v, O.NOMSD(ham, psi).vMF(dt), atol=1e-13)
+
+
+def test_phmsd_mean_field_single_excitation_is_exact():
+    """Two determinants one alpha excitation apart (0 1 -> 0 2, sign +1) with real orbitals: the
+    restated mean field equals the force bias of the exact one-body density of the expansion."""
+    from safire_b200.synth import phmsd_trial_from_occupations
+    rs = np.random.default_rng(5)
+    M, Nc, dt = 8, 6, 0.02
+    orb = _random_orbitals(rs, M, complex_=False).astype(np.complex128)
+    L = rs.standard_normal((1, M, M, Nc))
+    L = 0.5 * (L + L.transpose(0, 2, 1, 3))
+    occa = np.array([[0, 1], [0, 2]])
+    occb = np.array([[0, 1], [0, 1]])
+    c = np.array([0.9, -0.4])
+    tr = phmsd_trial_from_occupations(M, [orb, orb], [occa[0], occb[0]], occa, occb, c)
+    v = Mo.phmsd_mean_field(tr, L, dt)
+    norm = np.sum(c ** 2)
+    ga = np.zeros((M, M))
+    ga[[0, 1], [0, 1]] += c[0] ** 2 / norm
+    ga[[0, 2], [0, 2]] += c[1] ** 2 / norm
+    ga[1, 2] = ga[2, 1] = c[0] * c[1] / norm
+    gb = np.zeros((M, M))
+    gb[[0, 1], [0, 1]] = 1.0
+    R = orb.real
+    exact = sum(np.einsum("ik,ikn->n", R.T @ g @ R, L[0]) for g in (ga, gb)) * np.sqrt(dt)
+    assert np.allclose(v, exact, atol=1e-13)
