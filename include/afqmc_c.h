@@ -45,7 +45,7 @@ typedef struct CUstream_st* afqmc_stream; /* == cudaStream_t */
 #define AFQMC_ERR_NONFINITE 4   /* non-finite value where the reference would abort */
 #define AFQMC_ERR_TIMEOUT 5     /* a bounded device wait gave up */
 #define AFQMC_ERR_ALLOC 6       /* device allocation failed */
-#define AFQMC_ERR_UNSUPPORTED 7 /* configuration outside what this build implements */
+#define AFQMC_ERR_UNSUPPORTED 7 /* configuration outside what the library implements */
 #define AFQMC_ERR_COLLAPSE 8    /* total walker weight collapsed (population_control.hpp:39) */
 
 /* walker types (reference enum WALKER_TYPES, src/AFQMC/config.h:46-52) */
@@ -483,7 +483,7 @@ int afqmc_pseudo_energy_sums(afqmc_wset ws, double dt, afqmc_c128* out2, afqmc_s
 
 /* =========================================================================================
  * Learned exchange-energy control variate (no reference counterpart; the exact exchange of
- * afqmc_ham_energy stays the judge).  An MLP features (D) -> H -> H -> 1 with GELU, trained and
+ * afqmc_ham_energy stays the reference value).  An MLP features (D) -> H -> H -> 1 with GELU, trained and
  * evaluated by BF16 tensor-core kernels with FP32 accumulation, FP32 master weights and Adam.
  * Parameters are one FP32 block [W1 (H x D) | b1 (H) | W2 (H x H) | b2 (H) | w3 (H) | b3 (1)],
  * row-major (out x in).  Features and targets are device FP32; targets in physical units, the

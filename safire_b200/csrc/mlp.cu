@@ -4,7 +4,7 @@
 // enough and tcgen05's 128-row tiles would leave most SMs idle), FP32 master weights and Adam.
 //
 // It has no counterpart in the reference: the exact exchange energy (Real3IndexFactorization
-// energy_impl, Real3IndexFactorization.hpp:476-590) stays the judge.  The estimator that uses it
+// energy_impl, Real3IndexFactorization.hpp:476-590) stays the reference value.  The estimator that uses it
 // evaluates the exact exchange on a random subset of walkers and the network on all of them, so
 // its expectation over the subset is the exact weighted average whatever the network predicts.
 //

@@ -9,8 +9,8 @@ uniform random subset, combined as
 
     sum_w omega_w EX_w  ~  sum_w omega_w f_w + (W / k) sum_{s in S} omega_s (EX_s - f_s),
 
-which is unbiased over the subset whatever the network predicts: the exact kernel stays the judge
-and the network only reduces the variance of the subsampled estimate.
+which is unbiased over the subset whatever the network predicts: the exact kernel stays the reference
+value and the network only reduces the variance of the subsampled estimate.
 """
 from __future__ import annotations
 
