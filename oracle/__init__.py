@@ -2,8 +2,8 @@
 
 A CPU restatement of the reference's batched AFQMC walker step (bkesk/SAFIRE) used to check the
 CUDA product path.  Only ``tests/``, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` /
-``--impl reference`` legs of ``bench.py`` may import it, and only as the checker or as the timed
-CPU baseline.  The product package (``safire_b200``) never imports it.
+``--impl reference`` legs of ``bench.py`` may import it, and only as the comparison
+standard or as the timed CPU baseline.  The product package (``safire_b200``) never imports it.
 
 Parity pins: the determinant / density-matrix / inverse functions are checked against the golden
 values of the reference's tests/test_sdet_ops.cpp, the PHMSD two-body kernel against

@@ -1,5 +1,5 @@
 """Test infrastructure: a float64 numpy statement of the exchange control-variate network and of
-the multi-fidelity estimator, the checker for safire_b200/csrc/mlp.cu.
+the multi-fidelity estimator, the comparison standard for safire_b200/csrc/mlp.cu.
 
 Network (no reference counterpart): standardised features xn = (x - mean) * istd, then
 z1 = xn W1^T + b1, a1 = gelu(z1), z2 = a1 W2^T + b2, a2 = gelu(z2), y = a2 . w3 + b3 in
