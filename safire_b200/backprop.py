@@ -1,0 +1,179 @@
+"""Back-propagated one-body density matrix for a single-determinant run
+(Estimators/BackPropEstimator.hpp, Propagators/AFQMCBasePropagator.cpp:403-533).
+
+`BackPropagation` attaches to a safire_b200.driver.Simulation as an observer and keeps, as the
+reference's walker set does (WalkerSetBase.h:493-530, WalkerSetUpdate.hpp:128-187):
+- the auxiliary fields X [nback][W][Nc] of every step, read from the step's own field buffer;
+- the per-step path-restoration factor of every walker, w / |w| / max(0, cos dtheta) (zero where
+  the projection or a non-finite energy killed it), formed from the phase and the dtheta the
+  update kernel writes: the new phase over the old one is w / |w|;
+- the walkers at the start of the window (the anchor, SlaterMatrixN).
+The comb copies walkers into the slots of the ones it removes; the histories and anchors follow
+with the same slot map (a walker keeps its slot, extra copies fill the emptied slots in
+increasing order, as afqmc_population_control does).
+
+At the end of each window of `steps` steps (BackPropEstimator::measure) the trial, one copy per
+walker, is propagated backwards through the stored fields, newest first:
+S <- P1^H sum_n (-i V^H)^n / n! P1^H S with V = vHS(X) (the library's afqmc_propagate given P1^H
+and -V^H), re-orthogonalised with afqmc_orthogonalize every `ortho_interval` steps and at the
+end.  The estimate is sum_w w'_w G_w / sum_w w'_w, w' the weights times the factors of the
+window, G_w = (B T^-1 A^H)^T with A the back-propagated trial, B the anchor and T = A^H B (its
+inverse by afqmc_inverse_logdet; the two batched products go to cuBLAS).  Then the window
+restarts from the current walkers.  One reference determinant, one walker set on one GPU.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import afqmc as A
+from . import capi
+from .capi import COLLINEAR
+
+
+def slot_map(offspring):
+    """Source walker of every slot after the single-rank comb: a walker with offspring >= 1
+    keeps its slot, its extra copies fill the slots of the walkers without offspring in
+    increasing order (population_control.hpp:142-209)."""
+    off = np.asarray(offspring)
+    src = np.arange(off.size)
+    free = np.nonzero(off == 0)[0]
+    nxt = 0
+    for i in range(off.size):
+        for _ in range(1, int(off[i])):
+            src[free[nxt]] = i
+            nxt += 1
+    if nxt != free.size:
+        raise ValueError("offspring counts do not conserve the population")
+    return src
+
+
+class BackPropagation:
+    def __init__(self, sim, PsiT, steps=100, ortho_interval=None, path_restoration=True):
+        """sim: a single-determinant Simulation; PsiT: its trial, per spin [N_s][M] (host)."""
+        ham = sim.ham
+        if getattr(sim.wfn, "ham", None) is not ham or not isinstance(sim.wfn, A.NOMSD):
+            raise ValueError("back-propagation is implemented for one NOMSD determinant")
+        if steps <= 0:
+            raise ValueError("steps must be positive")
+        self.sim = sim
+        self.nback = int(steps)
+        self.ortho = int(ortho_interval or sim.rp.walker_ortho_interval)
+        self.path_restoration = path_restoration
+        self.collinear = ham.walker_type == COLLINEAR
+        self.nel = [ham.nup] + ([ham.ndn] if self.collinear else [])
+        W, M, Nc = sim.wset.W, ham.M, ham.Nc
+        dev = sim.wset.buffer.device
+        self.W, self.M, self.dev = W, M, dev
+        self.X = torch.zeros((self.nback, W, Nc), dtype=torch.complex128, device=dev)
+        self.F = torch.ones((self.nback, W), dtype=torch.complex128, device=dev)
+        self.pos = 0
+        P1, _ = sim.prop.P1_vMF()
+        self.P1h = [torch.as_tensor(np.ascontiguousarray(P1[s].conj().T), device=dev)
+                    for s in range(P1.shape[0])]
+        self.trial = [torch.as_tensor(np.ascontiguousarray(np.asarray(p).conj().T), device=dev)
+                      for p in PsiT[:len(self.nel)]]
+        self.order = int(getattr(sim.prop.params, "taylor_n", 6))
+        self.samples = []  # (step, [nspin][M][M] on the host)
+        self._phase0 = None
+        self._set_anchor(sim.step_index - 1)
+        sim.observers.append(self)
+
+    # ---------------------------------------------------------------- walker data
+    def _slater(self, s):
+        return self.sim.wset.SlaterMatrices(s)
+
+    def _set_anchor(self, step):
+        self.anchor = [self._slater(s).clone() for s in range(len(self.nel))]
+        self.bp_pos = step
+
+    # ---------------------------------------------------------------- observer hooks
+    def before_step(self, sim):
+        self._phase0 = sim.wset.properties()[:, capi.PHASE].clone()
+
+    def after_propagate(self, sim):
+        X = sim.prop.last_step(self.W).X
+        self.X[self.pos].copy_(X)
+        props = sim.wset.properties()
+        p1 = props[:, capi.PHASE]
+        scale = torch.clamp(torch.cos(props[:, capi.THETA].real), min=0.0)
+        ok = (scale > np.finfo(np.float64).tiny) & (self._phase0 != 0)
+        ratio = torch.where(ok, p1 / torch.where(ok, self._phase0, torch.ones_like(p1)),
+                            torch.zeros_like(p1))
+        self.F[self.pos] = torch.where(ok, ratio / torch.where(ok, scale, torch.ones_like(scale)),
+                                       torch.zeros_like(p1))
+        self.pos = (self.pos + 1) % self.nback
+
+    def after_population_control(self, sim, offspring):
+        src = slot_map(offspring)
+        moved = np.nonzero(src != np.arange(src.size))[0]
+        if moved.size == 0:
+            return
+        d = torch.as_tensor(moved, device=self.dev)
+        s = torch.as_tensor(src[moved], device=self.dev)
+        self.X[:, d] = self.X[:, s]
+        self.F[:, d] = self.F[:, s]
+        for a in self.anchor:
+            a[d] = a[s]
+
+    def equilibrated(self, sim, step):
+        self._set_anchor(step)
+
+    def measure(self, sim, step):
+        bp_step = step - self.bp_pos
+        if bp_step < 0:
+            raise RuntimeError("back-propagation window starts after the current step")
+        if bp_step == self.nback:
+            self.samples.append((step, self.estimate(bp_step).cpu().numpy()))
+        if bp_step >= self.nback:
+            self._set_anchor(step)
+
+    # ---------------------------------------------------------------- the estimate
+    def back_propagate(self, nbp):
+        """The trial propagated backwards through the last nbp stored fields (per spin
+        [W][M][N_s], device) and the accumulated log det of the re-orthogonalisations."""
+        sim = self.sim
+        refs = [t.unsqueeze(0).expand(self.W, -1, -1).contiguous() for t in self.trial]
+        logdetR = torch.zeros(self.W, dtype=torch.complex128, device=self.dev)
+        slot = self.pos
+        for ni in range(nbp - 1, -1, -1):
+            slot = (slot - 1) % self.nback
+            V = sim.ham.vHS(self.X[slot].contiguous(), sim.dt)
+            for s, S in enumerate(refs):
+                if S.shape[2] == 0:
+                    continue
+                Vh = (-V[s % V.shape[0]].conj().transpose(1, 2)).contiguous()
+                A.det_ops.Propagate(S, self.P1h[s % len(self.P1h)], Vh, self.order)
+            if ni == 0 or ni % self.ortho == 0:
+                for S in refs:
+                    if S.shape[2]:
+                        A.det_ops.orthogonalize(S, logdetR)
+        return refs, logdetR
+
+    def weights(self, nbp):
+        w = self.sim.wset.properties()[:, capi.WEIGHT].clone()
+        if self.path_restoration:
+            slot = self.pos
+            for _ in range(nbp):
+                slot = (slot - 1) % self.nback
+                w = w * self.F[slot]
+        return w
+
+    def estimate(self, nbp):
+        refs, _ = self.back_propagate(nbp)
+        w = self.weights(nbp)
+        out = []
+        for Aref, B in zip(refs, self.anchor):
+            N = B.shape[2]
+            if N == 0:
+                out.append(torch.zeros((self.M, self.M), dtype=torch.complex128,
+                                       device=self.dev))
+                continue
+            AH = Aref.conj().transpose(1, 2)
+            T = torch.matmul(AH, B).contiguous()
+            Tinv = torch.empty_like(T)
+            ld = torch.zeros(self.W, dtype=torch.complex128, device=self.dev)
+            A.det_ops.inverse_logdet(T, Tinv, ld)
+            G = torch.matmul(B, torch.matmul(Tinv, AH)).transpose(1, 2)
+            out.append(torch.einsum("w,wik->ik", w, G) / w.sum())
+        return torch.stack(out)

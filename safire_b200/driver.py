@@ -119,6 +119,10 @@ class Simulation:
     # the step leaves the density matrix of the propagated walkers for the next step, which
     # skips recomputing it unless orthogonalisation or population control changed the walkers
     reuse_density: bool = True
+    # estimators that follow the walkers between measurements (safire_b200.backprop): each has
+    # before_step, after_propagate, after_population_control(sim, offspring), equilibrated(sim,
+    # step) and measure(sim, step), called at the points of the run_afqmc loop they name
+    observers: list = field(default_factory=list)
     _g_ready: bool = False
     _eshift_dev: torch.Tensor = None
 
@@ -199,6 +203,8 @@ class Simulation:
         if self._eshift_dev is None:
             self._eshift_dev = torch.zeros(1, dtype=torch.float64, device=self.wset.buffer.device)
         self._eshift_dev.fill_(float(self.Eshift))
+        for o in self.observers:
+            o.before_step(self)
         flags = 0
         if self.reuse_density:
             flags = A.capi.STEP_KEEP_G | (A.capi.STEP_G_READY if self._g_ready else 0)
@@ -210,6 +216,8 @@ class Simulation:
         else:
             self.prop.Propagate_flags(self.wset, self._eshift_dev, uniforms, flags)
         self._g_ready = self.reuse_density
+        for o in self.observers:
+            o.after_propagate(self)
         if step % self.rp.walker_ortho_interval == 0:
             self.prop.Orthogonalize(self.wset)
             self._g_ready = False
@@ -217,16 +225,25 @@ class Simulation:
         if pci > 0 and step % pci == 0:  # 0: the caller controls the population itself
             self._g_ready = False
             if _world() > 1:
+                if self.observers:
+                    raise NotImplementedError("walker-following estimators run on one rank")
                 from .population import population_control_distributed
                 population_control_distributed(self.wset, self.walker_rng)
             else:
-                A.population_control(self.wset, self.walker_rng)
+                off = A.population_control(self.wset, self.walker_rng)
+                for o in self.observers:
+                    o.after_population_control(self, off)
         out = None
         if step >= self.rp.equilibration_steps:
             if measure and step % self.rp.measure_interval == 0:
                 out, _, _ = self.measure()
                 self.energies.append((step, out))
+            for o in self.observers:
+                o.measure(self, step)
         else:
             self.Eshift += self.relax * (self.average_pseudo_energy() - self.Eshift)
+            if step == self.rp.equilibration_steps - 1:
+                for o in self.observers:
+                    o.equilibrated(self, step)
         self.step_index += 1
         return out

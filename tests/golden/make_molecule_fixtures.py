@@ -3,7 +3,7 @@ tests into committed fixtures, read with safire_b200's own HDF5 reader.
 
 Writes tests/golden/molecules.npz (Hamiltonians and trial wavefunctions of BH and N2) and
 tests/golden/molecule_references.json (the mixed-estimator energies with their error bars, the
-run settings, and the BH RHF mixed-estimator one-body density matrix).  Run from the repository
+run settings, and the BH RHF mixed-estimator and back-propagated one-body density matrices).  Run from the repository
 root with the reference checked out at REFERENCE (default /root/reference):
 
     python tests/golden/make_molecule_fixtures.py [REFERENCE]
@@ -110,6 +110,12 @@ def main():
             ge = np.asarray(f[f"{m}/MixedEstimator/OneRDM/error"])
             entry["onerdm_real"] = g.real.tolist()
             entry["onerdm_error_real"] = ge.real.tolist()
+            bp = f"{m}/BackPropEstimator/Steps=100/OneRDM"
+            entry["bp_steps"] = 100
+            entry["bp_onerdm_real"] = np.asarray(f[f"{bp}/mean"]).real.tolist()
+            entry["bp_onerdm_error_real"] = np.asarray(f[f"{bp}/error"]).real.tolist()
+            est = inp["execute"]["estimators"]["backprop"]
+            entry["bp_path_restoration"] = bool(est.get("path_restoration", True))
         refs[case] = entry
     with open(os.path.join(OUT, "molecule_references.json"), "w") as fh:
         json.dump(refs, fh, indent=1)
