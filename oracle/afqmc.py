@@ -826,6 +826,15 @@ def run_afqmc(wfn: NOMSD, prop: Propagator, ws: WalkerSet, rp: RunParams, field_
     return energies, Eshift
 
 
+def full_g_vbias(Likn, G, dt, walker_type):
+    """Real3IndexFactorization::vbias on a full density matrix G [nspin][M][M]
+    (Real3IndexFactorization.hpp:389-427): a sum_s sum_{ik} L_s[i][k][n] G_s[i][k], with
+    a = sqrt(dt) (2 sqrt(dt) for CLOSED)."""
+    L = np.asarray(Likn)
+    a = math.sqrt(dt) * (2.0 if walker_type == CLOSED else 1.0)
+    return a * sum(np.einsum("ikn,ik->n", L[s % L.shape[0]], G[s]) for s in range(G.shape[0]))
+
+
 def onerdm(wfn: NOMSD, ws: WalkerSet):
     """The MixedEstimator's OneRDM, single reference (Estimators/Observables/onerdm.hpp:39-64,
     MixedEstimator.hpp:42-108): sum_w w_w G_w per spin block with the full mixed density matrix
@@ -892,6 +901,13 @@ class NOMSDMulti:
         f = np.conj(self.ci)[:, None] * np.exp(ov - m)
         E = np.einsum("dw,dwq->wq", f, Ed) / f.sum(0)[:, None]
         return E, np.log(f.sum(0)) + m
+
+    def initial_walker(self):
+        """NOMSD::initial_guess (NOMSD.cpp:132-153): the determinant with the largest |c|."""
+        d = int(np.argmax(np.abs(self.ci)))
+        P = self.PsiTs[d]
+        return P[0].conj().T.copy(), (P[1].conj().T.copy() if self.walker_type == COLLINEAR
+                                      else None)
 
     def MixedDensityMatrix(self, SA, SB, log_m):
         """Full G [W, nspin, M, M] and the reference's Ov (linear sum + log_m)."""

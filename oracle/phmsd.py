@@ -365,5 +365,30 @@ class PHMSDWavefunction:
     def Log_Overlap(self, SA, SB):
         return phmsd_log_overlap(self.trial, SA, SB)[0]
 
+    def Energy(self, SA, SB):
+        """(E [W,3], log overlap [W]) by energy_alg1."""
+        return phmsd_energy(self.trial, self.H, SA, SB)
+
+    def initial_walker(self):
+        """PHMSD::initial_guess (PHMSD.hpp:284-302): the configuration of the determinant with
+        the largest coefficient, its orbitals' conjugates as columns (configuration_orbitals,
+        PHMSD.hpp:364-375), in the excitation order of the configuration."""
+        t = self.trial
+        k = int(np.argmax(np.abs(np.asarray(t.coef))))
+        out = []
+        for s, u in ((0, int(t.det_up[k])), (1, int(t.det_dn[k]))):
+            conf = np.asarray(t.refc[s]).copy()
+            if u > 0:
+                pos = 1
+                for n in sorted(t.exc[s]):
+                    e = t.exc[s][n]
+                    if u < pos + len(e):
+                        ex = e[u - pos]
+                        conf[ex[:n]] = ex[n:]
+                        break
+                    pos += len(e)
+            out.append(np.conj(np.asarray(t.orbmat[s])[conf]).T.copy())
+        return out[0], out[1]
+
     def vMF(self, dt):
         return self._vMF.copy()

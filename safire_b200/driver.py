@@ -123,6 +123,8 @@ class Simulation:
     # before_step, after_propagate, after_population_control(sim, offspring), equilibrated(sim,
     # step) and measure(sim, step), called at the points of the run_afqmc loop they name
     observers: list = field(default_factory=list)
+    # host field stream (use_host_fields); None: the device generator
+    field_rng: A.HostRandomGenerator = None
     _g_ready: bool = False
     _eshift_dev: torch.Tensor = None
 
@@ -178,6 +180,14 @@ class Simulation:
         self.step_index = 0
         self._g_ready = False
 
+    def use_host_fields(self):
+        """Draw every step's field uniforms on the host from std::mt19937 seeded with
+        split_seed(seed, rank, 1) and uniform_real_distribution<double>, W x Nc per step in
+        walker-major order: the field stream of the reference's host build (execute.cpp:124-125,
+        Random.hpp:37-51, AFQMCBasePropagator.cpp:706-716), so a seeded run reproduces the
+        reference's own.  Steps with host fields are launched eagerly, not from a graph."""
+        self.field_rng = A.HostRandomGenerator(A.split_seed(self.rp.seed, _rank(), 1))
+
     def autotune(self):
         """Let the library pick the fastest step variant for these walkers (mixed precision);
         the walkers are left as they were.  Returns (mode, {mode: step ms})."""
@@ -205,6 +215,10 @@ class Simulation:
         self._eshift_dev.fill_(float(self.Eshift))
         for o in self.observers:
             o.before_step(self)
+        if uniforms is None and self.field_rng is not None:
+            W, Nc = self.wset.W, self.ham.Nc
+            u = self.field_rng.sample_uniform(W * Nc).reshape(W, Nc)
+            uniforms = torch.as_tensor(u, device=self.wset.buffer.device)
         flags = 0
         if self.reuse_density:
             flags = A.capi.STEP_KEEP_G | (A.capi.STEP_G_READY if self._g_ready else 0)

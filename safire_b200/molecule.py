@@ -165,9 +165,28 @@ def _workload(ham, wfn, W, dt, walker_type):
     return molecule_workload(ham, first, W, dt, walker_type), None
 
 
-def simulation(ham, wfn, W, dt, walker_type=None, rp=None, use_graph=True):
-    """A Simulation of W walkers (FP64) for a trial read by safire_b200.inputs."""
+def simulation(ham, wfn, W, dt, walker_type=None, rp=None, use_graph=True, host_fields=False):
+    """A Simulation of W walkers (FP64) for a trial read by safire_b200.inputs.  The walkers
+    start from the determinant with the largest coefficient (NOMSD.cpp:132-153).  A PHMSD run
+    starts from the expansion's reference determinant; the reference starts from the
+    largest-coefficient configuration (PHMSD.hpp:284-302), the same one when the expansion is
+    led by its largest determinant, as the reference's own files are.
+    host_fields: draw the fields from the reference's host random stream
+    (Simulation.use_host_fields), so that a seeded run reproduces the reference's."""
     rp = rp or RunParams()
+    if isinstance(wfn, NOMSDInput) and wfn.ci.size > 1:
+        first = int(np.argmax(np.abs(wfn.ci)))
+        if first:
+            order = [first] + [d for d in range(wfn.ci.size) if d != first]
+            wfn = NOMSDInput(wfn.walker_type, wfn.M, wfn.nup, wfn.ndn, wfn.ci[order],
+                             [wfn.PsiT[d] for d in order])
+    sim = _simulation(ham, wfn, W, dt, walker_type, rp, use_graph)
+    if host_fields:
+        sim.use_host_fields()
+    return sim
+
+
+def _simulation(ham, wfn, W, dt, walker_type, rp, use_graph):
     wl, trial = _workload(ham, wfn, W, dt, walker_type)
     if trial is not None:
         sim = Simulation.from_workload(wl, W=W, rp=rp, trial=trial,

@@ -1,9 +1,12 @@
 """Extract the molecular inputs and statistical reference energies of the reference's functional
 tests into committed fixtures, read with safire_b200's own HDF5 reader.
 
-Writes tests/golden/molecules.npz (Hamiltonians and trial wavefunctions of BH and N2) and
-tests/golden/molecule_references.json (the mixed-estimator energies with their error bars, the
-run settings, and the BH RHF mixed-estimator and back-propagated one-body density matrices).  Run from the repository
+Writes tests/golden/molecules.npz (Hamiltonians and trial wavefunctions of BH and N2),
+tests/golden/molecule_references.json (the statistical references: mixed-estimator energies with
+their error bars, the run settings, and the BH RHF mixed-estimator and back-propagated one-body
+density matrices) and tests/golden/molecule_snapshots.json (the seeded single-rank snapshots:
+energies and density matrices of short runs that a restatement with the same random streams
+reproduces to rounding).  Run from the repository
 root with the reference checked out at REFERENCE (default /root/reference):
 
     python tests/golden/make_molecule_fixtures.py [REFERENCE]
@@ -32,7 +35,33 @@ WFNS = {
     "bh_casci_rhf_phmsd": "BH/afqmc_casci_rhf_phmsd.h5",
     "bh_casci_uhf_phmsd": "BH/afqmc_casci_uhf_phmsd.h5",
     "n2_cas_phmsd": "N2/cas_wfn.h5",
+    "bh_casci_rhf_1phmsd": "BH/afqmc_casci_rhf_1phmsd.h5",
+    "bh_casci_uhf_1phmsd": "BH/afqmc_casci_uhf_1phmsd.h5",
 }
+SNAP = "tests/functional/snapshot_references"
+# seeded single-rank snapshots (50 walkers, 20 steps, comb and measurement every step, a 2-step
+# back-propagation window where the case has one): (case, hamiltonian, wavefunction, walkers)
+SNAPSHOTS = [
+    ("bh_rhf_closed", "bh", "bh_rhf_nomsd", "closed", "BH/dense_rhf_basis_closed/rhf_nomsd/closed"),
+    ("bh_rhf_collinear", "bh", "bh_rhf_nomsd", "collinear",
+     "BH/dense_rhf_basis_closed/rhf_nomsd/collinear"),
+    ("bh_uhf_collinear", "bh", "bh_uhf_nomsd", "collinear",
+     "BH/dense_rhf_basis_closed/uhf_nomsd/collinear"),
+    ("bh_casci_rhf_nomsd_closed", "bh", "bh_casci_rhf_nomsd", "closed",
+     "BH/dense_rhf_basis_closed/rcasci_rhf_nomsd/closed"),
+    ("bh_casci_rhf_nomsd_collinear", "bh", "bh_casci_rhf_nomsd", "collinear",
+     "BH/dense_rhf_basis_closed/rcasci_rhf_nomsd/collinear"),
+    ("bh_casci_rhf_phmsd_collinear", "bh", "bh_casci_rhf_phmsd", "collinear",
+     "BH/dense_rhf_basis_closed/rcasci_rhf_phmsd/collinear"),
+    ("bh_casci_uhf_phmsd_collinear", "bh", "bh_casci_uhf_phmsd", "collinear",
+     "BH/dense_rhf_basis_closed/rcasci_uhf_phmsd/collinear"),
+    ("bh_casci_rhf_1phmsd_collinear", "bh", "bh_casci_rhf_1phmsd", "collinear",
+     "BH/dense_rhf_basis_closed/rcasci_rhf_1phmsd/collinear"),
+    ("bh_casci_uhf_1phmsd_collinear", "bh", "bh_casci_uhf_1phmsd", "collinear",
+     "BH/dense_rhf_basis_closed/rcasci_uhf_1phmsd/collinear"),
+    ("n2_cas_phmsd_collinear", "n2", "n2_cas_phmsd", "collinear",
+     "N2/cas_basis_hamil_closed/cas_wfn_collinear/collinear"),
+]
 # (case, hamiltonian, wavefunction, walker type, results.h5 below statistical_references)
 CASES = [
     ("bh_rhf_closed", "bh", "bh_rhf_nomsd", "closed", "BH/dense_rhf_basis_closed/rhf_nomsd/closed"),
@@ -55,9 +84,13 @@ def _scalar(f, path):
     return complex(np.asarray(f[path]).ravel()[0])
 
 
+REF_ROOT = [REF]
+
+
 def main():
     global INP, STAT
     if len(sys.argv) > 1:
+        REF_ROOT[0] = sys.argv[1]
         INP = os.path.join(sys.argv[1], "tests/functional/afqmc_inputs")
         STAT = os.path.join(sys.argv[1], "tests/functional/statistical_references")
     arrays = {}
@@ -119,7 +152,41 @@ def main():
         refs[case] = entry
     with open(os.path.join(OUT, "molecule_references.json"), "w") as fh:
         json.dump(refs, fh, indent=1)
-    print("wrote", len(arrays), "arrays and", len(refs), "references")
+
+    snaps = {}
+    for case, ham, wfn, walker, rel in SNAPSHOTS:
+        f = File(os.path.join(REF_ROOT[0], SNAP, rel, "results.h5"))
+        inp = json.loads(str(f["input_file"]))
+        ex = inp["execute"]
+        m = "measurements/Stage0"
+        est = ex.get("estimators", {})
+        entry = {
+            "hamiltonian": ham, "wavefunction": wfn, "walker_type": walker,
+            "ranks": int(np.asarray(f["num_ranks"])), "walkers": ex["num_walkers"],
+            "steps": ex["steps"], "timestep": ex["timestep"], "seed": inp["seed"],
+            "equilibration_steps": ex["equilibration_steps"],
+            "population_control_interval": ex["population_control_interval"],
+            "measure_interval": ex["measure_interval"],
+            "walker_ortho_interval": ex["walker_ortho_interval"],
+            "source": f"{SNAP}/{rel}/results.h5",
+        }
+        for k in ("Energy", "OnebodyEnergy", "CoulombEnergy", "ExchangeEnergy"):
+            z = _scalar(f, f"{m}/{k}/mean")
+            entry[k] = [z.real, z.imag]
+        if f"{m}/MixedEstimator/OneRDM/mean" in f:
+            g = np.asarray(f[f"{m}/MixedEstimator/OneRDM/mean"])
+            entry["mixed_interval"] = est["mixed"]["measure_interval"]
+            entry["onerdm"] = [g.real.tolist(), g.imag.tolist()]
+        if "backprop" in est:
+            n = est["backprop"]["propagation_steps"][0]
+            g = np.asarray(f[f"{m}/BackPropEstimator/Steps={n}/OneRDM/mean"])
+            entry["bp_steps"] = n
+            entry["bp_path_restoration"] = bool(est["backprop"].get("path_restoration", True))
+            entry["bp_onerdm"] = [g.real.tolist(), g.imag.tolist()]
+        snaps[case] = entry
+    with open(os.path.join(OUT, "molecule_snapshots.json"), "w") as fh:
+        json.dump(snaps, fh, indent=1)
+    print("wrote", len(arrays), "arrays,", len(refs), "references and", len(snaps), "snapshots")
 
 
 if __name__ == "__main__":

@@ -1,0 +1,42 @@
+"""The oracle against the reference's own seeded runs: each snapshot of its functional tests (one
+rank, 50 walkers, 20 steps, comb and measurement every step; BH and N2 with single-determinant,
+34-determinant NOMSD and PHMSD trials) is a full run whose field and comb draws come from the
+reference's host random streams.  Restated with the same streams, the oracle reproduces its
+mixed-estimator energy to rounding: this pins the restatement of the whole step (force bias,
+fields, propagation, phaseless update, bounds, re-orthogonalisation, comb, energy) and of the
+several-determinant and PHMSD mean fields to the reference's actual output.
+
+The reference's tools average an observable over a whole number of bins of a size chosen from
+the series (safiretools results/stats.py optimal_rebinsize, rebinning_analysis), so a reported
+mean covers the first (steps // B) * B measurements for some bin size B; the 34-determinant
+cases report the mean of the first 18 of their 20.  `reported_mean` accepts a series whose mean
+over one of those admissible lengths matches."""
+import numpy as np
+import pytest
+
+from tests import molecule_fixtures as F
+
+CASES = ["bh_rhf_closed", "bh_rhf_collinear", "bh_uhf_collinear", "bh_casci_rhf_nomsd_closed",
+         "bh_casci_rhf_nomsd_collinear", "bh_casci_rhf_phmsd_collinear",
+         "bh_casci_uhf_phmsd_collinear", "bh_casci_rhf_1phmsd_collinear",
+         "bh_casci_uhf_1phmsd_collinear", "n2_cas_phmsd_collinear"]
+
+
+def reported_mean(series, value, tol=1e-9):
+    """The admissible truncation length whose mean matches value, or None."""
+    x = np.asarray(series)
+    for B in range(1, x.size // 2 + 1):
+        n = (x.size // B) * B
+        if abs(x[:n].mean() - value) < tol:
+            return n
+    return None
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_reproduces_snapshot_energy(name):
+    e, r = F.oracle_snapshot_run(name)
+    assert len(e) == r["steps"]
+    n = reported_mean(e, r["Energy"][0])
+    assert n is not None, (np.mean(e), r["Energy"][0])
+    if "casci_rhf_nomsd" not in name:
+        assert n == r["steps"]
