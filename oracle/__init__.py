@@ -9,6 +9,9 @@ Parity pins: the determinant / density-matrix / inverse functions are checked ag
 values of the reference's tests/test_sdet_ops.cpp, the PHMSD two-body kernel against
 tests/test_phmsd_components.cpp, and the RNG against libstdc++ (oracle/stdrng_ref.cpp).  The
 Real3Index vbias / vHS / energy numbers have no stored golden values in the reference (its
-molecular HDF5 fixtures carry no TEST_RESULTS group); those parts are pinned by restating the
-formulas plus the internal-consistency tests in tests/test_oracle_*.py.
+molecular HDF5 fixtures carry no TEST_RESULTS group); the whole step is instead pinned by the
+reference's seeded snapshot runs (tests/functional/snapshot_references of BH and N2): fed the
+same host random streams, the oracle reproduces their reported energies to 1e-9
+(tests/test_molecule_snapshots.py), on top of the internal-consistency tests in
+tests/test_oracle_*.py.
 """
