@@ -27,7 +27,8 @@ INP = os.path.join(REF, "tests/functional/afqmc_inputs")
 STAT = os.path.join(REF, "tests/functional/statistical_references")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
-HAMS = {"bh": "BH/afqmc_H_rhf_closed.h5", "n2": "N2/cas_basis_hamil.h5"}
+HAMS = {"bh": "BH/afqmc_H_rhf_closed.h5", "n2": "N2/cas_basis_hamil.h5",
+        "bh_spin": "BH/afqmc_H_rhf_collinear.h5", "li": "Li/hamil_closed.h5"}
 WFNS = {
     "bh_rhf_nomsd": "BH/afqmc_rhf_nomsd.h5",
     "bh_uhf_nomsd": "BH/afqmc_uhf_nomsd.h5",
@@ -37,6 +38,7 @@ WFNS = {
     "n2_cas_phmsd": "N2/cas_wfn.h5",
     "bh_casci_rhf_1phmsd": "BH/afqmc_casci_rhf_1phmsd.h5",
     "bh_casci_uhf_1phmsd": "BH/afqmc_casci_uhf_1phmsd.h5",
+    "li_rohf_nomsd": "Li/rohf_nomsd_polarized.h5",
 }
 SNAP = "tests/functional/snapshot_references"
 # seeded single-rank snapshots (50 walkers, 20 steps, comb and measurement every step, a 2-step
@@ -61,6 +63,18 @@ SNAPSHOTS = [
      "BH/dense_rhf_basis_closed/rcasci_uhf_1phmsd/collinear"),
     ("n2_cas_phmsd_collinear", "n2", "n2_cas_phmsd", "collinear",
      "N2/cas_basis_hamil_closed/cas_wfn_collinear/collinear"),
+    # the same BH Hamiltonian written with a spin-resolved hcore [2][1][M][1][M]
+    ("bh_spinham_rhf_collinear", "bh_spin", "bh_rhf_nomsd", "collinear",
+     "BH/dense_rhf_basis_collinear/rhf_nomsd/collinear"),
+    ("bh_spinham_uhf_collinear", "bh_spin", "bh_uhf_nomsd", "collinear",
+     "BH/dense_rhf_basis_collinear/uhf_nomsd/collinear"),
+    ("bh_spinham_casci_rhf_nomsd_collinear", "bh_spin", "bh_casci_rhf_nomsd", "collinear",
+     "BH/dense_rhf_basis_collinear/rcasci_rhf_nomsd/collinear"),
+    ("bh_spinham_casci_rhf_phmsd_collinear", "bh_spin", "bh_casci_rhf_phmsd", "collinear",
+     "BH/dense_rhf_basis_collinear/rcasci_rhf_phmsd/collinear"),
+    # Li: a fully polarised ROHF trial, three alpha electrons and an empty beta sector
+    ("li_rohf_collinear", "li", "li_rohf_nomsd", "collinear",
+     "Li/hamil_closed/rohf_wfn_polarized/collinear"),
 ]
 # (case, hamiltonian, wavefunction, walker type, results.h5 below statistical_references)
 CASES = [
@@ -77,6 +91,18 @@ CASES = [
      "BH/dense_rhf_basis_closed/rcasci_uhf_phmsd/collinear"),
     ("n2_cas_phmsd_collinear", "n2", "n2_cas_phmsd", "collinear",
      "N2/cas_basis_hamil_closed/cas_wfn_collinear/collinear"),
+    # the same BH Hamiltonian written with a spin-resolved hcore [2][1][M][1][M]
+    ("bh_spinham_rhf_collinear", "bh_spin", "bh_rhf_nomsd", "collinear",
+     "BH/dense_rhf_basis_collinear/rhf_nomsd/collinear"),
+    ("bh_spinham_uhf_collinear", "bh_spin", "bh_uhf_nomsd", "collinear",
+     "BH/dense_rhf_basis_collinear/uhf_nomsd/collinear"),
+    ("bh_spinham_casci_rhf_nomsd_collinear", "bh_spin", "bh_casci_rhf_nomsd", "collinear",
+     "BH/dense_rhf_basis_collinear/rcasci_rhf_nomsd/collinear"),
+    ("bh_spinham_casci_rhf_phmsd_collinear", "bh_spin", "bh_casci_rhf_phmsd", "collinear",
+     "BH/dense_rhf_basis_collinear/rcasci_rhf_phmsd/collinear"),
+    # Li: a fully polarised ROHF trial, three alpha electrons and an empty beta sector
+    ("li_rohf_collinear", "li", "li_rohf_nomsd", "collinear",
+     "Li/hamil_closed/rohf_wfn_polarized/collinear"),
 ]
 
 

@@ -1,6 +1,7 @@
 """The CUDA path against the reference's own seeded runs: every snapshot of its functional tests
-that this library covers (BH and N2; one NOMSD determinant, 34 NOMSD determinants, PHMSD over
-its reference orbitals and over a rotated complex reference; CLOSED and COLLINEAR walkers) is
+that this library covers (BH, N2 and Li; one NOMSD determinant, 34 NOMSD determinants, PHMSD
+over its reference orbitals and over a rotated complex reference; CLOSED and COLLINEAR walkers,
+a spin-resolved one-body Hamiltonian, an empty beta sector) is
 rerun through the C ABI with the reference's host random streams (Simulation.use_host_fields and
 the comb's own stream).  The mixed-estimator energy, and for the single-determinant cases the
 mixed and back-propagated one-body density matrices, match the reference's reported means
@@ -56,7 +57,7 @@ def _matches_some_length(samples, want, tol=1e-8):
     return False
 
 
-@pytest.mark.parametrize("name", ["bh_rhf_closed", "bh_uhf_collinear"])
+@pytest.mark.parametrize("name", ["bh_rhf_closed", "bh_uhf_collinear", "li_rohf_collinear"])
 def test_cuda_path_reproduces_snapshot_density_matrices(cuda, name):
     e, mixed, bp, r = _run(name, with_rdms=True)
     want = np.array(r["onerdm"][0]) + 1j * np.array(r["onerdm"][1])

@@ -58,7 +58,7 @@ def test_fixture_contents():
     assert (w.walker_type, w.M, w.nup, w.ndn, w.ci.size) == (I.CLOSED, 19, 3, 3, 1)
     assert np.allclose(w.PsiT[0][0] @ w.PsiT[0][0].conj().T, np.eye(3))
     refs = F.references()
-    assert len(refs) == 7
+    assert len(refs) == 12
     for r in refs.values():
         assert r["walkers"] == 1536 and r["timestep"] == 0.01 and r["energy_error"] > 0
 
