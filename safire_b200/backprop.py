@@ -1,5 +1,5 @@
-"""Back-propagated one-body density matrix for a single-determinant run
-(Estimators/BackPropEstimator.hpp, Propagators/AFQMCBasePropagator.cpp:403-533).
+"""Back-propagated one-body density matrix (Estimators/BackPropEstimator.hpp,
+Propagators/AFQMCBasePropagator.cpp:403-533).
 
 `BackPropagation` attaches to a safire_b200.driver.Simulation as an observer and keeps, as the
 reference's walker set does (WalkerSetBase.h:493-530, WalkerSetUpdate.hpp:128-187):
@@ -19,7 +19,9 @@ and -V^H), re-orthogonalised with afqmc_orthogonalize every `ortho_interval` ste
 end.  The estimate is sum_w w'_w G_w / sum_w w'_w, w' the weights times the factors of the
 window, G_w = (B T^-1 A^H)^T with A the back-propagated trial, B the anchor and T = A^H B (its
 inverse by afqmc_inverse_logdet; the two batched products go to cuBLAS).  Then the window
-restarts from the current walkers.  One reference determinant, one walker set on one GPU.
+restarts from the current walkers.  A trial of several determinants back-propagates each of its
+references (NOMSD: its determinants; PHMSD: its configurations, phmsd_references) and weights
+their density matrices by their shares of each walker's overlap.  One walker set on one GPU.
 """
 from __future__ import annotations
 
@@ -48,12 +50,41 @@ def slot_map(offspring):
     return src
 
 
+def phmsd_references(trial):
+    """The references of a PHMSD trial for back propagation (PHMSD.hpp:232-279): one per
+    determinant, its configuration's orbitals in excitation order (the rows of orbmat it
+    occupies, per spin [N_s][M]), weighted by its coefficient with the permutation sign, c_k =
+    conj(coupling k)."""
+    refs = []
+    confs = []
+    for s in (0, 1):
+        ref = np.asarray(trial.refc[s])
+        cs = [ref.copy()]
+        for n in sorted(trial.exc[s]):
+            for e in trial.exc[s][n]:
+                c = ref.copy()
+                c[e[:n]] = e[n:]
+                cs.append(c)
+        confs.append(cs)
+    for k in range(len(trial.coef)):
+        psi = [np.asarray(trial.orbmat[s])[confs[s][int((trial.det_up, trial.det_dn)[s][k])]]
+               for s in (0, 1)]
+        refs.append((complex(np.conj(trial.coef[k])), psi))
+    return refs
+
+
 class BackPropagation:
-    def __init__(self, sim, PsiT, steps=100, ortho_interval=None, path_restoration=True):
-        """sim: a single-determinant Simulation; PsiT: its trial, per spin [N_s][M] (host)."""
+    def __init__(self, sim, PsiT=None, steps=100, ortho_interval=None, path_restoration=True,
+                 references=None):
+        """sim: a Simulation; PsiT: its single-determinant trial, per spin [N_s][M] (host); or
+        references: the trial's determinants [(c_d, per-spin PsiT_d)] as the reference's
+        getReferences / getReferenceWeight give them (NOMSD: its determinants and ci;
+        PHMSD: phmsd_references)."""
         ham = sim.ham
-        if getattr(sim.wfn, "ham", None) is not ham or not isinstance(sim.wfn, A.NOMSD):
-            raise ValueError("back-propagation is implemented for one NOMSD determinant")
+        if references is None:
+            if PsiT is None:
+                raise ValueError("give the trial's PsiT or its references")
+            references = [(1.0 + 0j, PsiT)]
         if steps <= 0:
             raise ValueError("steps must be positive")
         self.sim = sim
@@ -71,8 +102,13 @@ class BackPropagation:
         P1, _ = sim.prop.P1_vMF()
         self.P1h = [torch.as_tensor(np.ascontiguousarray(P1[s].conj().T), device=dev)
                     for s in range(P1.shape[0])]
-        self.trial = [torch.as_tensor(np.ascontiguousarray(np.asarray(p).conj().T), device=dev)
-                      for p in PsiT[:len(self.nel)]]
+        nsp = len(self.nel)
+        self.ref_w = np.array([complex(c) for c, _ in references])
+        # per spin, the references' Slater matrices PsiT_d^H stacked [nref][M][N_s]
+        self.trial = [torch.as_tensor(np.ascontiguousarray(np.stack(
+            [np.asarray(P[s]).conj().T for _, P in references])), device=dev)
+            for s in range(nsp)]
+        self.nref = len(references)
         self.order = int(getattr(sim.prop.params, "taylor_n", 6))
         self.samples = []  # (step, [nspin][M][M] on the host)
         self._phase0 = None
@@ -130,11 +166,14 @@ class BackPropagation:
 
     # ---------------------------------------------------------------- the estimate
     def back_propagate(self, nbp):
-        """The trial propagated backwards through the last nbp stored fields (per spin
-        [W][M][N_s], device) and the accumulated log det of the re-orthogonalisations."""
+        """The references propagated backwards through the last nbp stored fields, one copy per
+        walker (per spin [nref * W][M][N_s], reference-major, device), and the accumulated log
+        det of the re-orthogonalisations [nref * W]."""
         sim = self.sim
-        refs = [t.unsqueeze(0).expand(self.W, -1, -1).contiguous() for t in self.trial]
-        logdetR = torch.zeros(self.W, dtype=torch.complex128, device=self.dev)
+        nr, W = self.nref, self.W
+        refs = [t.unsqueeze(1).expand(-1, W, -1, -1).reshape(nr * W, self.M, t.shape[2])
+                .contiguous() for t in self.trial]
+        logdetR = torch.zeros(nr * W, dtype=torch.complex128, device=self.dev)
         slot = self.pos
         for ni in range(nbp - 1, -1, -1):
             slot = (slot - 1) % self.nback
@@ -142,7 +181,8 @@ class BackPropagation:
             for s, S in enumerate(refs):
                 if S.shape[2] == 0:
                     continue
-                Vh = (-V[s % V.shape[0]].conj().transpose(1, 2)).contiguous()
+                Vh = (-V[s % V.shape[0]].conj().transpose(1, 2))
+                Vh = (Vh.repeat(nr, 1, 1) if nr > 1 else Vh).contiguous()
                 A.det_ops.Propagate(S, self.P1h[s % len(self.P1h)], Vh, self.order)
             if ni == 0 or ni % self.ortho == 0:
                 for S in refs:
@@ -160,20 +200,46 @@ class BackPropagation:
         return w
 
     def estimate(self, nbp):
-        refs, _ = self.back_propagate(nbp)
+        """BackPropEstimator.hpp:36-120 and onerdm.hpp: per reference d and walker, the log
+        overlap of the back-propagated reference with the anchored walker (both spins; twice the
+        one block for CLOSED) plus conj(logdetR_d) after removing its mean over the references
+        (doubled for CLOSED), the overlap conj(c_d) e^{that}, each reference's share of the
+        walker's total, and sum_w w'_w sum_d share_{w,d} G_{w,d} / sum_w w'_w."""
+        refs, logdetR = self.back_propagate(nbp)
+        nr, W = self.nref, self.W
         w = self.weights(nbp)
-        out = []
-        for Aref, B in zip(refs, self.anchor):
+        closed = not self.collinear
+        L = logdetR.view(nr, W)
+        L = L - L.mean(0, keepdim=True)
+        if closed:
+            L = 2.0 * L
+        lo = torch.conj(L).clone()
+        Gs = []
+        for s, (Aref, B) in enumerate(zip(refs, self.anchor)):
             N = B.shape[2]
             if N == 0:
+                Gs.append(None)
+                continue
+            Bd = B.unsqueeze(0).expand(nr, -1, -1, -1).reshape(nr * W, self.M, N)
+            AH = Aref.conj().transpose(1, 2)
+            T = torch.matmul(AH, Bd).contiguous()
+            Tinv = torch.empty_like(T)
+            ld = torch.zeros(nr * W, dtype=torch.complex128, device=self.dev)
+            A.det_ops.inverse_logdet(T, Tinv, ld)
+            lo = lo + (2.0 if closed else 1.0) * ld.view(nr, W)
+            Gs.append(torch.matmul(Bd, torch.matmul(Tinv, AH)).transpose(1, 2)
+                      .reshape(nr, W, self.M, self.M))
+        cw = torch.as_tensor(np.conj(self.ref_w), device=self.dev)[:, None]
+        # shares ov_d / sum_d ov_d with ov_d = conj(c_d) e^{lo_d}; a common factor per walker
+        # cancels, so the largest real part comes off before the exponential
+        lo = lo - lo.real.max(0, keepdim=True).values
+        ov = cw * torch.exp(lo)
+        share = ov / ov.sum(0, keepdim=True)
+        out = []
+        for G in Gs:
+            if G is None:
                 out.append(torch.zeros((self.M, self.M), dtype=torch.complex128,
                                        device=self.dev))
                 continue
-            AH = Aref.conj().transpose(1, 2)
-            T = torch.matmul(AH, B).contiguous()
-            Tinv = torch.empty_like(T)
-            ld = torch.zeros(self.W, dtype=torch.complex128, device=self.dev)
-            A.det_ops.inverse_logdet(T, Tinv, ld)
-            G = torch.matmul(B, torch.matmul(Tinv, AH)).transpose(1, 2)
-            out.append(torch.einsum("w,wik->ik", w, G) / w.sum())
+            out.append(torch.einsum("w,dw,dwik->ik", w, share, G) / w.sum())
         return torch.stack(out)

@@ -39,6 +39,7 @@ WFNS = {
     "bh_casci_rhf_1phmsd": "BH/afqmc_casci_rhf_1phmsd.h5",
     "bh_casci_uhf_1phmsd": "BH/afqmc_casci_uhf_1phmsd.h5",
     "li_rohf_nomsd": "Li/rohf_nomsd_polarized.h5",
+    "bh_casci_uhf_nomsd": "BH/afqmc_casci_uhf_nomsd.h5",
 }
 SNAP = "tests/functional/snapshot_references"
 # seeded single-rank snapshots (50 walkers, 20 steps, comb and measurement every step, a 2-step
@@ -75,6 +76,9 @@ SNAPSHOTS = [
     # Li: a fully polarised ROHF trial, three alpha electrons and an empty beta sector
     ("li_rohf_collinear", "li", "li_rohf_nomsd", "collinear",
      "Li/hamil_closed/rohf_wfn_polarized/collinear"),
+    # the UHF-orbital CASCI expansion as COLLINEAR NOMSD determinants
+    ("bh_casci_uhf_nomsd_collinear", "bh", "bh_casci_uhf_nomsd", "collinear",
+     "BH/dense_rhf_basis_closed/rcasci_uhf_nomsd/collinear"),
 ]
 # (case, hamiltonian, wavefunction, walker type, results.h5 below statistical_references)
 CASES = [

@@ -35,7 +35,7 @@ class _Checked(BackPropagation):
         slots = [(self.pos - nbp + j) % self.nback for j in range(nbp)]  # oldest first
         V_hist = [self.oham.vHS(self.X[s].cpu().numpy(), sim.dt) for s in slots]
         P1, _ = sim.prop.P1_vMF()
-        refs = [np.repeat(t.cpu().numpy()[None], self.W, axis=0) for t in self.trial]
+        refs = [np.repeat(t.cpu().numpy()[0][None], self.W, axis=0) for t in self.trial]
         OB.back_propagate(refs, list(P1), V_hist, self.order, self.ortho)
         w0 = sim.wset.properties()[:, capi.WEIGHT].cpu().numpy()
         w = OB.path_restored_weights(w0, self.F[slots].cpu().numpy())

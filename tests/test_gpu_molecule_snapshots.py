@@ -66,3 +66,32 @@ def test_cuda_path_reproduces_snapshot_density_matrices(cuda, name):
     want_bp = np.array(r["bp_onerdm"][0]) + 1j * np.array(r["bp_onerdm"][1])
     assert len(bp.samples) == r["steps"] // r["bp_steps"]
     assert _matches_some_length([s[1] for s in bp.samples], want_bp)
+
+
+@pytest.mark.parametrize("name", ["bh_casci_rhf_phmsd_collinear", "bh_casci_uhf_phmsd_collinear",
+                                  "bh_casci_uhf_nomsd_collinear"])
+def test_cuda_path_reproduces_snapshot_multireference_backprop(cuda, name):
+    """Back propagation over the trial's determinants (44 or 34 references: the PHMSD
+    configurations over the rotated complex reference or the orbitals, or the NOMSD
+    determinants), each weighted by its share of every walker's overlap."""
+    from safire_b200 import inputs as I
+    from safire_b200.backprop import phmsd_references
+    ham, wfn, wt, r = F.snapshot_case(name)
+    rp = RunParams(walker_ortho_interval=r["walker_ortho_interval"],
+                   population_control_interval=r["population_control_interval"],
+                   measure_interval=r["measure_interval"],
+                   equilibration_steps=r["equilibration_steps"], seed=r["seed"])
+    sim = Mo.simulation(ham, wfn, r["walkers"], r["timestep"], wt, rp, host_fields=True)
+    if isinstance(wfn, I.PHMSDInput):
+        refs = phmsd_references(I.phmsd_trial(wfn))
+    else:
+        refs = [(c, P) for c, P in zip(wfn.ci, wfn.PsiT)]
+    bp = BackPropagation(sim, steps=r["bp_steps"], path_restoration=r["bp_path_restoration"],
+                         references=refs)
+    for _ in range(r["steps"]):
+        sim.step()
+    torch.cuda.synchronize()
+    assert reported_mean([v for _, v in sim.energies], r["Energy"][0], tol=1e-8) is not None
+    want = np.array(r["bp_onerdm"][0]) + 1j * np.array(r["bp_onerdm"][1])
+    assert len(bp.samples) == r["steps"] // r["bp_steps"]
+    assert _matches_some_length([s[1] for s in bp.samples], want)
