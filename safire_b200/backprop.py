@@ -73,6 +73,73 @@ def phmsd_references(trial):
     return refs
 
 
+def reference_onerdm(refs, walkers, weights, ref_w, log_offset, closed_factor):
+    """sum_w weights_w sum_d share_{w,d} G_{w,d} / sum_w weights_w per spin [nspin][M][M]: the
+    reference loop of BackPropEstimator.hpp:36-120 / MixedEstimator.hpp:40-105 with onerdm.hpp.
+    refs: per spin the references, one copy per walker, [nref * W][M][N_s] (reference-major);
+    walkers: per spin [W][M][N_s]; log_offset [nref][W] added to the log overlaps (the BP
+    log det shift, or minus the walkers' OVLP); closed_factor multiplies the one block's log
+    overlap of CLOSED walkers (2 in back propagation, 1 in the mixed estimator).  The log overlap
+    of reference d with walker w is log det(A^H B) over the spins (afqmc_inverse_logdet), its
+    overlap conj(c_d) e^{log}, its share that over the walker's sum, G_{w,d} = (B T^-1 A^H)^T."""
+    nr = len(ref_w)
+    W, M = walkers[0].shape[0], walkers[0].shape[1]
+    dev = walkers[0].device
+    lo = log_offset.clone()
+    Gs = []
+    for Aref, B in zip(refs, walkers):
+        N = B.shape[2]
+        if N == 0:
+            Gs.append(None)
+            continue
+        Bd = B.unsqueeze(0).expand(nr, -1, -1, -1).reshape(nr * W, M, N)
+        AH = Aref.conj().transpose(1, 2)
+        T = torch.matmul(AH, Bd).contiguous()
+        Tinv = torch.empty_like(T)
+        ld = torch.zeros(nr * W, dtype=torch.complex128, device=dev)
+        A.det_ops.inverse_logdet(T, Tinv, ld)
+        lo = lo + closed_factor * ld.view(nr, W)
+        Gs.append(torch.matmul(Bd, torch.matmul(Tinv, AH)).transpose(1, 2)
+                  .reshape(nr, W, M, M))
+    cw = torch.as_tensor(np.conj(np.asarray(ref_w, dtype=np.complex128)), device=dev)[:, None]
+    # shares ov_d / sum_d ov_d with ov_d = conj(c_d) e^{lo_d}: a common factor per walker
+    # cancels, so the largest real part comes off before the exponential
+    lo = lo - lo.real.max(0, keepdim=True).values
+    ov = cw * torch.exp(lo)
+    share = ov / ov.sum(0, keepdim=True)
+    out = []
+    for G in Gs:
+        if G is None:
+            out.append(torch.zeros((M, M), dtype=torch.complex128, device=dev))
+            continue
+        out.append(torch.einsum("w,dw,dwik->ik", weights, share, G) / weights.sum())
+    return torch.stack(out)
+
+
+def mixed_onerdm(sim, references):
+    """The mixed estimator's one-body density matrix of the current walkers
+    (MixedEstimator.hpp:40-105, onerdm.hpp) over the trial's references [(c_d, per-spin
+    PsiT_d)]: reference_onerdm with the references unpropagated, the walkers' stored log
+    overlaps subtracted, and no doubling for CLOSED walkers (the reference loops over the spin
+    blocks it has).  Returns [nspin][M][M] (device)."""
+    ham = sim.ham
+    nsp = 2 if ham.walker_type == COLLINEAR else 1
+    W, M = sim.wset.W, ham.M
+    dev = sim.wset.buffer.device
+    nr = len(references)
+    refs = []
+    for s in range(nsp):
+        R = torch.as_tensor(np.ascontiguousarray(np.stack(
+            [np.asarray(P[s]).conj().T for _, P in references])), device=dev)
+        refs.append(R.unsqueeze(1).expand(-1, W, -1, -1).reshape(nr * W, M, R.shape[2])
+                    .contiguous())
+    walkers = [sim.wset.SlaterMatrices(s).contiguous() for s in range(nsp)]
+    props = sim.wset.properties()
+    shift = -props[:, capi.OVLP].unsqueeze(0).expand(nr, -1)
+    return reference_onerdm(refs, walkers, props[:, capi.WEIGHT].clone(),
+                            [c for c, _ in references], shift, 1.0)
+
+
 class BackPropagation:
     def __init__(self, sim, PsiT=None, steps=100, ortho_interval=None, path_restoration=True,
                  references=None):
@@ -207,39 +274,10 @@ class BackPropagation:
         walker's total, and sum_w w'_w sum_d share_{w,d} G_{w,d} / sum_w w'_w."""
         refs, logdetR = self.back_propagate(nbp)
         nr, W = self.nref, self.W
-        w = self.weights(nbp)
         closed = not self.collinear
         L = logdetR.view(nr, W)
         L = L - L.mean(0, keepdim=True)
         if closed:
             L = 2.0 * L
-        lo = torch.conj(L).clone()
-        Gs = []
-        for s, (Aref, B) in enumerate(zip(refs, self.anchor)):
-            N = B.shape[2]
-            if N == 0:
-                Gs.append(None)
-                continue
-            Bd = B.unsqueeze(0).expand(nr, -1, -1, -1).reshape(nr * W, self.M, N)
-            AH = Aref.conj().transpose(1, 2)
-            T = torch.matmul(AH, Bd).contiguous()
-            Tinv = torch.empty_like(T)
-            ld = torch.zeros(nr * W, dtype=torch.complex128, device=self.dev)
-            A.det_ops.inverse_logdet(T, Tinv, ld)
-            lo = lo + (2.0 if closed else 1.0) * ld.view(nr, W)
-            Gs.append(torch.matmul(Bd, torch.matmul(Tinv, AH)).transpose(1, 2)
-                      .reshape(nr, W, self.M, self.M))
-        cw = torch.as_tensor(np.conj(self.ref_w), device=self.dev)[:, None]
-        # shares ov_d / sum_d ov_d with ov_d = conj(c_d) e^{lo_d}; a common factor per walker
-        # cancels, so the largest real part comes off before the exponential
-        lo = lo - lo.real.max(0, keepdim=True).values
-        ov = cw * torch.exp(lo)
-        share = ov / ov.sum(0, keepdim=True)
-        out = []
-        for G in Gs:
-            if G is None:
-                out.append(torch.zeros((self.M, self.M), dtype=torch.complex128,
-                                       device=self.dev))
-                continue
-            out.append(torch.einsum("w,dw,dwik->ik", w, share, G) / w.sum())
-        return torch.stack(out)
+        return reference_onerdm(refs, self.anchor, self.weights(nbp), self.ref_w,
+                                torch.conj(L), 2.0 if closed else 1.0)

@@ -11,7 +11,7 @@ import pytest
 import torch
 
 from safire_b200 import molecule as Mo
-from safire_b200.backprop import BackPropagation
+from safire_b200.backprop import BackPropagation, mixed_onerdm
 from safire_b200.driver import RunParams
 from tests import molecule_fixtures as F
 from tests.test_molecule_snapshots import CASES, reported_mean
@@ -73,7 +73,8 @@ def test_cuda_path_reproduces_snapshot_density_matrices(cuda, name):
 def test_cuda_path_reproduces_snapshot_multireference_backprop(cuda, name):
     """Back propagation over the trial's determinants (44 or 34 references: the PHMSD
     configurations over the rotated complex reference or the orbitals, or the NOMSD
-    determinants), each weighted by its share of every walker's overlap."""
+    determinants), each weighted by its share of every walker's overlap; and the mixed
+    estimator's density matrix over the same references."""
     from safire_b200 import inputs as I
     from safire_b200.backprop import phmsd_references
     ham, wfn, wt, r = F.snapshot_case(name)
@@ -88,10 +89,28 @@ def test_cuda_path_reproduces_snapshot_multireference_backprop(cuda, name):
         refs = [(c, P) for c, P in zip(wfn.ci, wfn.PsiT)]
     bp = BackPropagation(sim, steps=r["bp_steps"], path_restoration=r["bp_path_restoration"],
                          references=refs)
-    for _ in range(r["steps"]):
+    mixed = []
+    for step in range(r["steps"]):
         sim.step()
+        if step % r["mixed_interval"] == 0:
+            mixed.append(mixed_onerdm(sim, refs).cpu().numpy())
     torch.cuda.synchronize()
     assert reported_mean([v for _, v in sim.energies], r["Energy"][0], tol=1e-8) is not None
     want = np.array(r["bp_onerdm"][0]) + 1j * np.array(r["bp_onerdm"][1])
     assert len(bp.samples) == r["steps"] // r["bp_steps"]
     assert _matches_some_length([s[1] for s in bp.samples], want)
+    want = np.array(r["onerdm"][0]) + 1j * np.array(r["onerdm"][1])
+    assert _matches_some_length(mixed, want)
+
+
+def test_mixed_onerdm_over_references_equals_the_library_kernel(cuda):
+    """For one determinant the reference loop gives the library's afqmc_wfn_onerdm."""
+    ham, wfn, wt, r = F.snapshot_case("bh_uhf_collinear")
+    rp = RunParams(walker_ortho_interval=10, population_control_interval=1, measure_interval=1,
+                   equilibration_steps=0, seed=7)
+    sim = Mo.simulation(ham, wfn, 24, 0.01, wt, rp, host_fields=True)
+    for _ in range(5):
+        sim.step()
+    g, ws = sim.wfn.OneRDM(sim.wset)
+    got = mixed_onerdm(sim, [(1.0, wfn.PsiT[0])])
+    assert torch.max(torch.abs(got - g / ws)).item() < 1e-12
