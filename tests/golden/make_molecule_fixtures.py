@@ -166,6 +166,8 @@ def main():
             "measure_interval": ex["measure_interval"],
             "walker_ortho_interval": ex["walker_ortho_interval"],
             "seed": inp["seed"],
+            "run_time_seconds": float(np.asarray(f["run_time_seconds"])),
+            "back_propagation": "backprop" in ex.get("estimators", {}),
             "source": f"tests/functional/statistical_references/{rel}/results.h5",
         }
         if case == "bh_rhf_closed":
