@@ -17,7 +17,6 @@ link-message groups, dense attribute storage, other filters) raises H5Unsupporte
 """
 from __future__ import annotations
 
-import struct
 import zlib
 
 import numpy as np
@@ -50,8 +49,10 @@ class File:
         with open(path, "rb") as fh:
             self.buf = fh.read()
         b = self.buf
-        sb = b.find(_SIG)
-        if sb not in (0, 512, 1024, 2048) and sb < 0:
+        # the superblock sits at byte 0 or at a power of two from 512 on (a user block before it)
+        sb = next((o for o in [0] + [512 << k for k in range(24)]
+                   if o < len(b) and b[o:o + 8] == _SIG), -1)
+        if sb < 0:
             raise ValueError(f"{path}: not an HDF5 file")
         ver = b[sb + 8]
         if ver not in (0, 1):
@@ -307,11 +308,11 @@ class File:
         return a.copy()
 
     def _chunked(self, btree, rank, chunk, esize, shape, filters):
-        out = bytearray(int(np.prod(shape)) * esize if shape else esize)
-        full = np.zeros(shape, dtype=f"V{esize}") if shape else None
+        if not shape:
+            raise H5Unsupported("chunked scalar dataset")
+        full = np.zeros(shape, dtype=f"V{esize}")
         self._walk_chunks(btree, rank, chunk, esize, shape, filters, full)
-        out[:] = full.tobytes()
-        return bytes(out)
+        return full.tobytes()
 
     def _walk_chunks(self, addr, rank, chunk, esize, shape, filters, full):
         p = self._a(addr)

@@ -212,3 +212,14 @@ def test_phmsd_mean_field_single_excitation_is_exact():
     R = orb.real
     exact = sum(np.einsum("ik,ikn->n", R.T @ g @ R, L[0]) for g in (ga, gb)) * np.sqrt(dt)
     assert np.allclose(v, exact, atol=1e-13)
+
+
+def test_h5_reader_rejects_other_files(tmp_path):
+    from safire_b200.h5 import File
+    p = tmp_path / "not.h5"
+    p.write_bytes(b"\x00" * 600 + b"\x89HDF\r\n\x1a\n" + b"\x00" * 100)  # signature off-grid
+    with pytest.raises(ValueError):
+        File(str(p))
+    p.write_bytes(b"plain text, no superblock")
+    with pytest.raises(ValueError):
+        File(str(p))
