@@ -10,6 +10,11 @@ cadence: 10 propagation steps, QR re-orthogonalisation every 5, comb population 
 and one mixed-estimator energy measurement every 10.  value = walker-steps/s over all ranks
 (= W * 10 * K * N_gpus / max-over-ranks device time).
 
+The synthetic system's total walker weight collapses some 130-200 steps after the walkers leave
+the trial (the reference algorithm does the same on it), so the K timed blocks run in segments
+of at most 8 blocks, each from walkers restarted at the trial outside the timed region; the
+device times of the segments are summed (see _segmented).
+
 The default run times the mixed-precision path (3xTF32 tensor-core contractions, FP64
 determinants, weights and energy sums) and then the complex128 path on the same inputs
 (`fp64` in the JSON line, with the mixed / FP64 ratio).  `--workload phmsd` times the
@@ -70,7 +75,54 @@ def parse():
     ap.add_argument("--taylor-mode", type=int, default=1, choices=[0, 1, 2, 3],
                     help="mixed Taylor propagation: 0 per-term GEMMs, 1 fused (auto), 2 / 3 fused "
                          "with one / two walkers in flight per CTA")
+    ap.add_argument("--profile-case", default=None,
+                    choices=["step", "taylor", "vhs", "exchange", "phmsd-energy"],
+                    help="run one small case for an ncu capture instead of the bench: the "
+                         "M=200 system with --walkers walkers in --precision, after one step "
+                         "(taylor: three steps) one more call of the named operation "
+                         "(step: a propagation step; vhs: HamiltonianOperations.vHS of the last "
+                         "step's fields; exchange: the energy measurement); phmsd-energy: the "
+                         "PHMSD system with --walkers walkers (default 64), one Propagate and one "
+                         "energy evaluation")
     return ap.parse_args()
+
+
+def run_profile_case(args):
+    """Small cases for ncu captures (one GPU); prints one line with what ran."""
+    import torch
+    from safire_b200 import afqmc as A
+    from safire_b200.driver import RunParams, Simulation
+    from safire_b200.synth import make_phmsd_workload, make_workload
+    torch.cuda.set_device(0)
+    prec = A.PREC_MIXED if args.precision == "mixed" else A.PREC_FP64
+    rp = RunParams(equilibration_steps=0, seed=0)
+    if args.profile_case == "phmsd-energy":
+        W = args.walkers if args.walkers != 1024 else 64
+        wl, trial = make_phmsd_workload(W=W)
+        sim = Simulation.from_workload(wl, W=W, rp=rp, trial=trial)
+        sim.prop.Propagate(sim.wset, sim.Eshift)
+        sim.wfn.Energy(sim.wset, set_properties=False)
+    else:
+        W = args.walkers
+        sim = Simulation.from_workload(make_workload("cfg2"), W=W, precision=prec, rp=rp)
+        if prec == A.PREC_MIXED and args.taylor_mode != 1:
+            sim.ham.set_taylor_fused(args.taylor_mode)
+        nsteps = 3 if args.profile_case == "taylor" else 1
+        for _ in range(nsteps):
+            sim.prop.Propagate(sim.wset, sim.Eshift)
+        if args.profile_case == "step":
+            sim.prop.Propagate(sim.wset, sim.Eshift)
+        elif args.profile_case == "vhs":
+            X = sim.prop.last_step(W).X
+            sim.ham.vHS(X, sim.dt, precision=prec)
+        elif args.profile_case == "exchange":
+            sim.wfn.Energy(sim.wset, set_properties=False, precision=prec)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": args.profile_case, "walkers": W,
+                      "precision": args.precision, "device_error_flag":
+                      int(sim.ham.device_error_flag()) if hasattr(sim.ham, "device_error_flag")
+                      else None}), flush=True)
+    return 0
 
 
 def metric_name():
@@ -266,9 +318,23 @@ def tf32_peak_tflops(torch):
     return 2 * n ** 3 / best / 1e12
 
 
-def _timed_blocks(sim, steps, warmup, world, local, clocks=None):
-    """Warm up, then time `steps` blocks of BLOCK steps with CUDA events on the current stream,
-    barriers on both sides; returns (max-over-ranks ms, our kernel launches, clock summary)."""
+SEGMENT_BLOCKS = 8  # blocks timed from one restart of the walkers at the trial
+
+
+def _segmented(sim, n_blocks, world, body, clocks=None):
+    """Run n_blocks calls of body() (one bench block each) and time them on the device.
+
+    The synthetic M=200 system's total walker weight collapses to zero some 130-200 steps after
+    the walkers leave the trial (the reference algorithm does the same on it: the RHF trial of
+    h1 alone is far from the interacting ground state), so the blocks run in segments of at most
+    SEGMENT_BLOCKS blocks, each from walkers restarted at the trial (Simulation.restart: trial
+    walkers, unit weights, their energies and a re-seeded Eshift), the restart outside the timed
+    region.  A segment that collapses all the same (AFQMC_ERR_COLLAPSE from the comb) is
+    discarded and run again from a restart with half as many blocks.  Every segment is bracketed
+    by synchronize + barrier, with CUDA events on the current stream.
+
+    Returns (device ms summed over the segments, each segment's time the max over ranks; kernels
+    launched inside the timed segments; number of segments; clock summary)."""
     import torch
     import torch.distributed as dist
     from safire_b200 import capi
@@ -277,38 +343,56 @@ def _timed_blocks(sim, steps, warmup, world, local, clocks=None):
         if world > 1:
             dist.barrier()
 
+    stream = torch.cuda.current_stream()
+    seg_ms, launches, left, seg, retries = [], 0, n_blocks, SEGMENT_BLOCKS, 0
+    if clocks is not None:
+        clocks.start()
+    while left > 0:
+        k = min(seg, left)
+        sim.restart()
+        torch.cuda.synchronize()
+        barrier()
+        n0 = capi.lib().afqmc_kernel_launches()
+        g0 = sim.graph.kernels_replayed() if sim.graph is not None else 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        try:
+            for _ in range(k):
+                body()
+        except capi.AfqmcError as err:
+            # every rank sees the same total weight, so every rank lands here together
+            if err.status != capi.ERR_COLLAPSE or retries >= 8:
+                raise
+            torch.cuda.synchronize()
+            retries += 1
+            seg = max(1, k // 2)
+            continue
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        seg_ms.append(e0.elapsed_time(e1))
+        launches += capi.lib().afqmc_kernel_launches() - n0
+        if sim.graph is not None:  # kernels the step graph replayed inside the timed region
+            launches += sim.graph.kernels_replayed() - g0
+        left -= k
+    clk = clocks.stop() if clocks is not None else None
+    if world > 1 and seg_ms:
+        t = torch.tensor(seg_ms, device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        seg_ms = [float(x) for x in t.cpu()]
+    return float(sum(seg_ms)), int(launches), len(seg_ms), clk
+
+
+def _timed_blocks(sim, steps, warmup, world, local, clocks=None):
+    """Warm up for `warmup` blocks of BLOCK steps, then time `steps` blocks (in restart-separated
+    segments, _segmented); returns (max-over-ranks ms, our kernel launches, segments, clock
+    summary)."""
     def block():
         for _ in range(BLOCK):
             sim.step()
 
-    for _ in range(warmup):
-        block()
-    torch.cuda.synchronize()
-    barrier()
-    launches0 = capi.lib().afqmc_kernel_launches()
-    graph_k0 = sim.graph.kernels_replayed() if sim.graph is not None else 0
-    if clocks is not None:
-        clocks.start()
-    stream = torch.cuda.current_stream()
-    torch.cuda.synchronize()
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(steps):
-        block()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    clk = clocks.stop() if clocks is not None else None
-    launches = capi.lib().afqmc_kernel_launches() - launches0
-    if sim.graph is not None:  # kernels the step graph replayed inside the timed region
-        launches += sim.graph.kernels_replayed() - graph_k0
-    t_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
-    return t_ms, int(launches), clk
+    _segmented(sim, warmup, world, block)
+    return _segmented(sim, steps, world, block, clocks)
 
 
 def _phases(sim):
@@ -333,13 +417,13 @@ def _phases(sim):
     return phases
 
 
-def _e2e(sim, W, Nc, steps, world, prec):
-    """The same blocks through the public API with host uniforms copied in from pinned memory
-    and the weights + energy estimate read back every block."""
+def _e2e(sim, W, Nc, steps, warmup, world, prec):
+    """The same blocks through the public API with every block's field uniforms copied in from
+    pinned host memory and the weights + energy estimate read back, timed like the resident
+    blocks (restart-separated segments, _segmented)."""
     import torch
     import torch.distributed as dist
     from safire_b200 import afqmc as A
-    stream = torch.cuda.current_stream()
     host_u = torch.rand((BLOCK, W, Nc), dtype=torch.float64).pin_memory()
     dev_u = torch.empty((BLOCK, W, Nc), dtype=torch.float64, device="cuda")
     host_w = torch.empty((W,), dtype=torch.complex128).pin_memory()
@@ -356,24 +440,105 @@ def _e2e(sim, W, Nc, steps, world, prec):
         host_e.copy_(sums, non_blocking=True)
         host_w.copy_(sim.wset.properties()[:, 0], non_blocking=True)
 
-    block_e2e()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    k0.record(stream)
-    for _ in range(steps):
-        block_e2e()
-    k1.record(stream)
-    torch.cuda.synchronize()
-    te = k0.elapsed_time(k1)
-    if world > 1:
-        t = torch.tensor([te], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        te = float(t.item())
+    _segmented(sim, max(1, warmup), world, block_e2e)
+    te, _, nseg, _ = _segmented(sim, steps, world, block_e2e)
     return {"value": W * world * BLOCK * steps / (te / 1000), "unit": "walker-steps/s",
             "h2d_bytes_per_step": int(host_u.numel() * 8),
-            "d2h_bytes_per_step": int((host_w.numel() + host_e.numel()) * 16)}
+            "d2h_bytes_per_step": int((host_w.numel() + host_e.numel()) * 16),
+            "ms_per_step": te / steps, "segments": nseg}
+
+
+def _roofline(sim, wl, W, prec, phases, args, torch, taylor_mode=1):
+    """Roofline of the phase with the largest share of a block.
+
+    achieved = the ALGORITHMIC flops of one launch (complex MAC = 8 flops, real x complex MAC =
+    4, counted on the complex operands whatever the kernel exploits) / its CUDA-event time:
+      vbias 8 Nc N M, vHS 4 M^2 Nc, propagation (2 + order) 8 M^2 N and exchange 8 N^2 M Nc +
+      8 N^2 Nc per walker (one spin block: CLOSED walkers).
+    peak = the dense rate of the MMA kind the kernel issues: the measured BF16 rate of
+    MEASURED_PEAKS.json for the FP16 split (kind::f16 runs FP16 and BF16 at one rate), cuBLAS TF32
+    at 8192^3 measured in this run for the TF32 split, cuBLAS DGEMM for complex128 (the file has
+    no TF32 or FP64 entry).  `mma_tflops` / `mma_frac` give the tensor work the kernels actually
+    issue (real Lnak, L and P1; three products per real product for the split), against the
+    same peak."""
+    from safire_b200 import afqmc as A
+    M, N, Nc = wl.M, wl.nup, wl.Nc
+    order = 6
+    algo = {"vHS": 4.0 * M * M * Nc * W, "vbias": 8.0 * Nc * N * M * W,
+            "propagate": W * (2 + order) * 8.0 * M * M * N,
+            "energy_measurement": W * (8.0 * N * N * M * Nc + 8.0 * N * N * Nc)}
+    if prec == A.PREC_FP64:
+        issued = {"vHS": 4.0 * M * M * Nc * W, "vbias": 4.0 * N * M * Nc * W,
+                  "propagate": W * (2 * 4.0 * M * M * N + order * 8.0 * M * M * N),
+                  "energy_measurement": W * (4.0 * N * N * M * Nc + 8.0 * N * N * Nc)}
+        peak = fp64_peak_tflops(torch)
+        peak_src = "cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry in the file of " \
+                   "measured peaks)"
+    else:
+        sp, ex = 3.0, float(args.exchange_split)
+        issued = {"vHS": sp * 4.0 * M * M * Nc * W, "vbias": sp * 4.0 * N * M * Nc * W,
+                  "propagate": sp * W * (2 * 4.0 * M * M * N + order * 8.0 * M * M * N),
+                  "energy_measurement": ex * W * 4.0 * N * N * M * Nc}
+    block_share = {k: (phases[k] * (1 if k == "energy_measurement" else BLOCK)) for k in algo}
+    top = max(block_share, key=block_share.get)
+    if prec != A.PREC_FP64:
+        # the FP16 split runs vbias, vHS, the exchange and (fused) the Taylor series when the
+        # shapes allow it (afqmc_ham_set_split_format)
+        f16 = sim.ham.set_split_format(0)
+        f16_top = f16 and (top != "propagate" or taylor_mode != 0)
+        peaks = measured_peaks()
+        if f16_top and peaks.get("bf16_tflops"):
+            peak = float(peaks["bf16_tflops"])
+            peak_src = "of measured: MEASURED_PEAKS.json bf16_tflops (dense kind::f16 rate)"
+        else:
+            peak = tf32_peak_tflops(torch)
+            peak_src = "cuBLAS TF32 GEMM 8192^3 measured in this run (no TF32 entry in the file " \
+                       "of measured peaks)"
+    t_launch = phases[top]
+    kernel = {"vHS": "vHS GEMM", "vbias": "vbias GEMM", "propagate": "Taylor propagation",
+              "energy_measurement": "energy measurement"}[top]
+    traffic, traffic_src = None, None
+    if top == "energy_measurement" and prec == A.PREC_MIXED:
+        # the dominant kernel on its own: the fused exchange contraction (with its G split and
+        # the final sums), timed with CUDA events on the launching stream
+        G, _ = sim.wfn.MixedDensityMatrix(sim.wset)
+        E = torch.empty((W, 3), dtype=torch.complex128, device=G.device)
+        sim.ham.energy(E, G, addH1=False, precision=prec)
+        stream = torch.cuda.current_stream()
+        x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 5
+        x0.record(stream)
+        for _ in range(reps):
+            sim.ham.energy(E, G, addH1=False, precision=prec)
+        x1.record(stream)
+        torch.cuda.synchronize()
+        t_launch = x0.elapsed_time(x1) / reps
+        del G, E
+        kernel = f"exchange_tc_kernel<{args.exchange_split}> (fused EXX/EJ contraction)"
+        traffic, traffic_src = _EXCHANGE_TRAFFIC(W, Nc, N, M)
+    achieved = algo[top] / (t_launch / 1000) / 1e12
+    mma = issued[top] / (t_launch / 1000) / 1e12
+    return {"kernel": kernel, "bound": "tensor", "achieved": achieved, "peak": peak,
+            "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+            "traffic_source": traffic_src, "peak_source": peak_src,
+            "flops_per_launch": algo[top], "flops": "algorithmic (complex-counted)",
+            "launch_ms": t_launch, "mma_tflops": mma, "mma_frac": mma / peak,
+            "mma_flops_per_launch": issued[top], "block_share_ms": block_share}
+
+
+def _EXCHANGE_TRAFFIC(W, Nc, N, M):
+    """DRAM bytes per launch of exchange_tc_kernel<3>: ncu (dram__bytes_read.sum +
+    dram__bytes_write.sum) at the bench's 1024 walkers read 2.316 GB and wrote 55.6 MB.  The
+    tile order keeps the Lnak planes of 64 vector pairs in L2 while every walker pair passes, so
+    the reads are the Lnak planes once plus every walker's G planes once per 64-pair block, and
+    the writes the two complex sums per (walker, vector); other walker counts scale by that."""
+    if (W, Nc, N, M) == (1024, 1600, 50, 200):
+        return 2315739136 + 55630080, "ncu dram__bytes_read.sum + dram__bytes_write.sum, " \
+                                      "one launch at 1024 walkers"
+    blocks = -(-((Nc + 1) // 2) // 64)
+    return (2 * Nc * N * M * 4 + W * (4 * N * M * 4) * blocks + W * Nc * 32,
+            "ncu dram__bytes_read.sum + dram__bytes_write.sum at 1024 walkers (2.371 GB per "
+            "launch), by the tile-order model at other walker counts")
 
 
 def _init_dist():
@@ -419,72 +584,15 @@ def run_ours(args):
         best, ms = sim.autotune()
         tuned = {"taylor_mode": best, "step_ms": ms}
 
-    t_ms, launches, clk = _timed_blocks(sim, args.steps, args.warmup, world, local,
-                                        ClockSampler(local))
+    t_ms, launches, nseg, clk = _timed_blocks(sim, args.steps, args.warmup, world, local,
+                                              ClockSampler(local))
     value = W * world * BLOCK * args.steps / (t_ms / 1000)
-    phases = _phases(sim)
-
-    # roofline of the dominant contraction: the kernel with the largest share of a block
-    M, N, Nc = wl.M, wl.nup, wl.Nc
-    peaks = measured_peaks()
-    if prec == A.PREC_FP64:
-        # flops the FP64 kernels execute (real trial: Lnak, L and P1 are real)
-        flops = {"vHS": 4.0 * M * M * Nc * W, "vbias": 4.0 * N * M * Nc * W,
-                 "propagate": W * (2 * 4.0 * M * M * N + 6 * 8.0 * M * M * N),
-                 "energy_measurement": W * (4.0 * N * N * M * Nc + 8.0 * N * N * Nc)}
-        peak = fp64_peak_tflops(torch)
-        peak_src = "cuBLAS DGEMM 8192^3 measured in this run (dense FP64; no FP64 entry in " \
-                   "MEASURED_PEAKS.json)"
-    else:
-        # TF32 MMA flops of the split products (x3 for 3xTF32, unpadded tile extents)
-        sp = 3.0
-        ex = float(args.exchange_split)
-        flops = {"vHS": sp * 4.0 * M * M * Nc * W, "vbias": sp * 4.0 * N * M * Nc * W,
-                 "propagate": sp * W * (2 * 4.0 * M * M * N + 6 * 8.0 * M * M * N),
-                 "energy_measurement": ex * W * 4.0 * N * N * M * Nc}
-        if peaks.get("bf16_tflops"):
-            peak = peaks["bf16_tflops"] / 2
-            peak_src = "of measured: MEASURED_PEAKS.json bf16_tflops / 2 (dense TF32 runs at " \
-                       "half the BF16 tensor rate)"
-        else:
-            peak = tf32_peak_tflops(torch)
-            peak_src = "cuBLAS TF32 GEMM 8192^3 measured in this run"
-    block_share = {k: (phases[k] * (1 if k == "energy_measurement" else BLOCK)) for k in flops}
-    top = max(block_share, key=block_share.get)
-    achieved = flops[top] / (phases[top] / 1000) / 1e12
-    roofline = {"kernel": top, "bound": "tensor", "achieved": achieved,
-                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-                "peak_source": peak_src, "flops_per_launch": flops[top],
-                "block_share_ms": block_share}
-    if top == "energy_measurement" and prec == A.PREC_MIXED:
-        # the dominant kernel on its own: the fused exchange contraction (with its G split and
-        # the final sums), timed with CUDA events on the launching stream
-        G, _ = sim.wfn.MixedDensityMatrix(sim.wset)
-        E = torch.empty((W, 3), dtype=torch.complex128, device=G.device)
-        sim.ham.energy(E, G, addH1=False, precision=prec)
-        stream = torch.cuda.current_stream()
-        x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        reps = 5
-        x0.record(stream)
-        for _ in range(reps):
-            sim.ham.energy(E, G, addH1=False, precision=prec)
-        x1.record(stream)
-        torch.cuda.synchronize()
-        t_x = x0.elapsed_time(x1) / reps
-        del G, E
-        # DRAM bytes per launch from the ncu capture at 128 walkers (155.7 MB read + 10.1 MB
-        # written = Lnak planes once + G planes and the per-(walker, vector) sums), scaled to W:
-        # 2 Lnak planes + W x (4 G planes + 2 complex outputs per Cholesky vector)
-        traffic = 2 * Nc * N * M * 4 + W * (4 * N * M * 4 + 2 * Nc * 16)
-        roofline.update({"kernel": "exchange_tc_kernel<3> (fused EXX/EJ contraction)",
-                         "achieved": flops[top] / (t_x / 1000) / 1e12,
-                         "frac": flops[top] / (t_x / 1000) / 1e12 / peak,
-                         "launch_ms": t_x, "traffic": traffic,
-                         "traffic_source": "ncu capture at 128 walkers, scaled by walkers"})
-
-    # the synthetic system's total weight collapses after ~200 steps: restart from the trial
     sim.restart()
-    e2e = None if args.no_e2e else _e2e(sim, W, Nc, args.steps, world, prec)
+    phases = _phases(sim)
+    roofline = _roofline(sim, wl, W, prec, phases, args, torch,
+                         tuned["taylor_mode"] if tuned else args.taylor_mode)
+
+    e2e = None if args.no_e2e else _e2e(sim, W, wl.Nc, args.steps, args.warmup, world, prec)
 
     # the plain complex128 path on the same inputs, timed the same way: the mixed-vs-FP64 ratio
     fp64 = None
@@ -494,9 +602,10 @@ def run_ours(args):
         torch.cuda.empty_cache()
         ref = Simulation.from_workload(wl, W=W, precision=A.PREC_FP64, rp=rp)
         ref.use_graph = not args.no_graph
-        t64, _, _ = _timed_blocks(ref, args.steps, args.warmup, world, local)
+        t64, _, nseg64, _ = _timed_blocks(ref, args.steps, args.warmup, world, local)
         v64 = W * world * BLOCK * args.steps / (t64 / 1000)
-        fp64 = {"value": v64, "ms_per_step": t64 / args.steps, "mixed_over_fp64": value / v64}
+        fp64 = {"value": v64, "ms_per_step": t64 / args.steps, "mixed_over_fp64": value / v64,
+                "segments": nseg64}
         sim = ref
     else:
         err_flag = int(sim.ham.device_error_flag())
@@ -525,6 +634,9 @@ def run_ours(args):
                        "autotune": tuned,
                        "step_graph": not args.no_graph,
                        "parallelism": f"walker dp{world}",
+                       "segments": f"{nseg} timed segments of at most {SEGMENT_BLOCKS} blocks, "
+                                   "each from walkers restarted at the trial outside the timed "
+                                   "region",
                        "l2": "inputs larger than L2 (V 655 MB, Likn 512 MB per step)"},
             "fp64": fp64,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
@@ -538,11 +650,21 @@ def run_ours(args):
 
 
 def run_control_variate(args):
-    """The learned exchange control variate on the M=200 workload (mixed precision): pairs from
-    the exact kernel over the first steps train the MLP on top of the exchange over the leading
-    Nc / 16 Cholesky vectors; afterwards every measurement is timed both ways (all-exact vs the
-    base + network on all walkers + exact exchange on 1/8 weight-proportional draws), and the cost
-    ratio at equal statistical error bar is reported with the estimator's spread."""
+    """The learned exchange control variate on the M=200 workload (mixed precision).
+
+    Training: (features, exact exchange) pairs from 500 equilibration steps (Eshift relaxing),
+    run as five windows of 100 steps from the trial (the synthetic system's total weight
+    collapses some 130-200 steps after the walkers leave the trial), one pair set every 2 steps;
+    the MLP learns the exchange on top of the exchange over the leading Nc / 16 vectors.
+    Measurement: windows of 100 steps from the trial, 20 steps of Eshift relaxation, then one
+    measurement every 10 steps, each timed both ways (all-exact vs the base + network on all
+    walkers + exact exchange on 1/8 weight-proportional draws).  The windows are independent runs,
+    so the QMC spread of a measurement (sigma_qmc) is the spread across windows at the same step
+    of a window (the per-step mean over windows removed: the energy relaxes from the trial's);
+    the control variate adds its subsampling spread sigma_sub (of estimator minus exact, on the
+    same walkers) to every measurement.  Equal error bar then takes 1 + sigma_sub^2 / sigma_qmc^2
+    times as many measurements, and the cost ratio is all-exact ms / (control-variate ms x that
+    factor)."""
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -555,16 +677,14 @@ def run_control_variate(args):
     world, rank, local = _init_dist()
     W = args.walkers
     wl = make_workload(args.cv_system)
+    window, eq_win, meas_every = 100, 20, 10
     if args.cv_system == "cfg2":
-        # training pairs from the first 150 steps at a fixed Eshift (one set every step): on this
-        # synthetic system the reference algorithm's total weight collapses after
-        # a few hundred steps, so a 500-step equilibration cannot run
-        equil, every, eq_steps = 150, 1, 0
-    else:
-        # the M=32 system equilibrates: 500 steps with the Eshift update, a pair set every 10
-        equil, every, eq_steps = 500, 10, 500
+        train_windows, train_every = 5, 2
+    else:  # the M=32 system is stable: one 500-step equilibration, a pair set every 10 steps
+        train_windows, train_every = 1, 10
+    train_len = 500 // train_windows
     sim = Simulation.from_workload(wl, W=W, precision=A.PREC_MIXED,
-                                   rp=RunParams(equilibration_steps=eq_steps, seed=0))
+                                   rp=RunParams(equilibration_steps=train_len, seed=0))
     sim.use_graph = not args.no_graph
     lowrank = None
     if args.cv_lowrank < 0:
@@ -574,10 +694,13 @@ def run_control_variate(args):
                                        wl.E0, wl.PsiT), args.cv_lowrank)
     cv = ExchangeControlVariate(sim, hidden=512, fraction=args.cv_fraction, seed=0,
                                 sampling=args.cv_sampling, lowrank=lowrank)
-    for step in range(equil):
-        sim.step(measure=False)
-        if step % every == 0:
-            cv.collect()
+    for win in range(train_windows):
+        if win:
+            sim.restart()
+        for step in range(train_len):
+            sim.step(measure=False)
+            if step % train_every == 0:
+                cv.collect()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     hist = cv.fit(epochs=args.cv_epochs, batch=1024, lr=1e-3)
@@ -594,55 +717,74 @@ def run_control_variate(args):
         torch.cuda.synchronize()
         return r, e0.elapsed_time(e1)
 
-    exact_e, mf_e, t_ex, t_mf = [], [], [], []
-    for m in range(args.steps + args.warmup):
-        for _ in range(BLOCK):
+    # measurement windows
+    sim.rp.equilibration_steps = eq_win
+    sim.relax = 1 - math.exp(-10.0 / eq_win)
+    per_win = len(range(eq_win, window, meas_every))
+    n_win = max(2, -(-(args.steps + args.warmup) // per_win))
+    exact_e, mf_e, t_ex, t_mf, pos = [], [], [], [], []
+    for win in range(n_win):
+        sim.restart()
+        for step in range(window):
             sim.step(measure=False)
-        (e_exact, _, _), te = timed(sim.measure)
-        (e_mf, _), tm = timed(cv.measure)
-        if m >= args.warmup:
-            exact_e.append(e_exact)
-            mf_e.append(e_mf)
-            t_ex.append(te)
-            t_mf.append(tm)
+            if step >= eq_win and (step - eq_win) % meas_every == 0:
+                (e_exact, _, _), te = timed(sim.measure)
+                (e_mf, _), tm = timed(cv.measure)
+                exact_e.append(e_exact)
+                mf_e.append(e_mf)
+                pos.append((step - eq_win) // meas_every)
+                t_ex.append(te)
+                t_mf.append(tm)
     # the Coulomb term the estimator takes from the force bias against the energy kernel's
     _, o = cv.measure(exact=True)
     ej_gap = (o["ej_from_vbias"] - o["ej_exact"]).real
-    exact_e, mf_e = np.array(exact_e), np.array(mf_e)
+    exact_e, mf_e, pos = np.array(exact_e), np.array(mf_e), np.array(pos)
     diff = mf_e - exact_e
-    s_qmc = float(np.std(exact_e, ddof=1))
+    resid = exact_e.copy()
+    for k in np.unique(pos):
+        resid[pos == k] -= exact_e[pos == k].mean()
+    dof = exact_e.size - np.unique(pos).size
+    s_qmc = float(np.sqrt((resid ** 2).sum() / max(dof, 1)))
     s_sub = float(np.std(diff, ddof=1))
     factor = (s_qmc ** 2 + s_sub ** 2) / s_qmc ** 2  # measurements needed for equal error bar
-    tex, tmf = float(np.median(t_ex)), float(np.median(t_mf))
+    # the first measurement of the run pays for one-time set-up: medians of the rest
+    tex, tmf = float(np.median(t_ex[1:])), float(np.median(t_mf[1:]))
     value = tex / (tmf * factor)
     if rank == 0:
         line = {
             "metric": "energy-measurement cost reduction at equal statistical error bar, "
                       f"learned exchange control variate (M={wl.M}, {W} walkers, mixed)",
             "value": value, "unit": "x (all-exact cost / control-variate cost)",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "n_gpus": world, "steps": int(exact_e.size), "warmup": 0,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "bf16 MLP (fp32 accumulate) + c128/tf32x3 exact exchange",
+            "dtype": "bf16 MLP (fp32 accumulate) + c128/split-precision exact exchange",
             "data": "synthetic",
             "config": {"workload": f"M={wl.M} N={wl.nup}+{wl.ndn} Nc={wl.Nc} W={W} "
                                    f"dt={wl.dt}; MLP {cv.mlp.D}-512-512-1 GELU trained on pairs "
-                                   f"from the first {equil} steps (one set per {every} steps"
-                                   f"{', fixed Eshift' if eq_steps == 0 else ''}); exact "
-                                   f"exchange on {args.cv_fraction:.3g} of the walkers "
-                                   f"({args.cv_sampling} draws) per measurement; "
+                                   f"from {train_windows * train_len} equilibration steps "
+                                   f"({train_windows} window(s) of {train_len} from the trial, a "
+                                   f"pair set every {train_every} steps); exact exchange on "
+                                   f"{args.cv_fraction:.3g} of the walkers ({args.cv_sampling} "
+                                   "draws) per measurement; "
                                    + (f"network on top of the exchange over the leading "
                                       f"{args.cv_lowrank} Cholesky vectors; "
                                       if args.cv_lowrank else "")
-                                   + "one measurement per 10-step block",
+                                   + f"{n_win} measurement windows of {window} steps from the "
+                                   f"trial, a measurement every {meas_every} steps after "
+                                   f"{eq_win}",
                        "training_samples": int(sum(x.shape[0] for x in cv.X)),
                        "epochs": args.cv_epochs, "train_seconds": t_train,
                        "loss_first_last": [hist[0], hist[-1]]},
             "measurement_ms": {"all_exact": tex, "control_variate": tmf},
-            "sigma": {"qmc_between_measurements": s_qmc, "subsampling": s_sub,
+            "sigma": {"qmc_across_windows": s_qmc,
+                      "qmc_series_spread (drift included, not used)":
+                          float(np.std(exact_e, ddof=1)),
+                      "subsampling": s_sub,
                       "measurements_factor_for_equal_error": factor},
             "bias": {"mean_mf_minus_exact": float(diff.mean()),
                      "standard_error": float(s_sub / np.sqrt(diff.size)),
                      "ej_from_vbias_minus_energy_kernel": float(ej_gap)},
+            "meets_3x": bool(value >= 3.0),
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -666,9 +808,10 @@ def run_phmsd(args):
     rp = RunParams(equilibration_steps=0, seed=0)
     sim = Simulation.from_workload(wl, W=W, rp=rp, trial=trial)
     sim.use_graph = False
-    t_ms, launches, clk = _timed_blocks(sim, args.steps, args.warmup, world, local,
-                                        ClockSampler(local))
+    t_ms, launches, nseg, clk = _timed_blocks(sim, args.steps, args.warmup, world, local,
+                                              ClockSampler(local))
     value = W * world * BLOCK * args.steps / (t_ms / 1000)
+    sim.restart()
     phases = _phases(sim)
     # the excited-determinant energy tables, per (walker, Cholesky index) and spin: the table
     # products Y = t[:, r] QQ0^T (nel x nv x nel), U = t[holes, r] t (nh x nact x nel),
@@ -689,7 +832,8 @@ def run_phmsd(args):
                 "bound": "fp64", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
                 "frac": achieved / fp64, "traffic": None, "flops_per_launch": flops,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"}
-    e2e = None if args.no_e2e else _e2e(sim, W, wl.Nc, args.steps, world, A.PREC_FP64)
+    e2e = None if args.no_e2e else _e2e(sim, W, wl.Nc, args.steps, args.warmup, world,
+                                        A.PREC_FP64)
     if rank == 0:
         line = {
             "metric": "walker-steps/s, PHMSD trial (M=120, 30+30 electrons, 4096 determinants, "
@@ -715,6 +859,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_case:
+        return run_profile_case(args)
     return run_ours(args)
 
 

@@ -107,6 +107,15 @@ int afqmc_mixed_density_matrix(const afqmc_c128* PsiT, const afqmc_c128* S, long
                                afqmc_c128* G, long ldG, afqmc_c128* ovlp, int W, int M, int N,
                                int compact, afqmc_stream stream);
 
+/* det_ops::MixedDensityMatrix with a bra per walker (A [W][M][N], walker stride ldA) —
+ * density_matrix.hpp:603-649, the overload BackPropEstimator and MixedEstimator call with the
+ * back-propagated references (Estimators/BackPropEstimator.hpp:105-107).  T_w = A_w^H S_w,
+ * ovlp[w] += log det T_w; compact != 0: G [W][N][M] = T_w^{-T} S_w^T; compact == 0:
+ * G [W][M][M] = (S_w T_w^{-1} A_w^H)^T.  A singular T_w gives a zero inverse. */
+int afqmc_mixed_density_matrix_batched(const afqmc_c128* A, long ldA, const afqmc_c128* S,
+                                       long ldS, afqmc_c128* G, long ldG, afqmc_c128* ovlp, int W,
+                                       int M, int N, int compact, afqmc_stream stream);
+
 /* det_ops::detail::inverse_logdet (batched) — density_matrix.hpp:80-111.
  * Ainv [W][N][N] = A^{-1} (zero if singular), logdet[w] += log det A_w. */
 int afqmc_inverse_logdet(const afqmc_c128* A, afqmc_c128* Ainv, afqmc_c128* logdet, int W, int N,
@@ -165,6 +174,32 @@ int afqmc_ham_energy(afqmc_ham ham, const afqmc_c128* G, afqmc_c128* E, int W, i
  * default) or 1 (plain TF32, for runs whose energy tolerance allows it). */
 int afqmc_ham_set_exchange_split(afqmc_ham ham, int nsplit);
 
+/* Mixed-precision vHS over symmetric Cholesky vectors.  When every L_n is symmetric (to 1e-10 of
+ * the largest |L|, checked once on the device; real orbitals make it so), V_w = sum_n X_n L_n is
+ * complex symmetric and the tensor-core vHS computes only the (i, k) pairs with i <= k, writing
+ * each value to V[w][i][k] and V[w][k][i].  enable = 1 (default) uses that form when the vectors
+ * qualify, 0 always computes all M^2 pairs (the reference's contraction,
+ * Real3IndexFactorization.hpp:282-326, computes all of them).  *active (optional) receives 1 when
+ * the symmetric form runs. */
+int afqmc_ham_set_vhs_symmetry(afqmc_ham ham, int enable, int* active);
+
+/* Operand format of the mixed-precision vbias, vHS and exchange contractions.  Both keep 22
+ * significant bits of each operand in two terms, x = hi + lo, and multiply with three products
+ * (hi*hi + hi*lo + lo*hi) accumulated in FP32:
+ *   AFQMC_SPLIT_TF32  TF32 terms (kind::tf32 MMAs, 4 bytes per term);
+ *   AFQMC_SPLIT_FP16  FP16 terms of operands scaled by powers of two (per walker row for G and
+ *                     X, one scale per static tensor), the scales undone exactly in the
+ *                     epilogue: twice the tensor rate and half the operand bytes of TF32;
+ *   AFQMC_SPLIT_AUTO  FP16 when the shapes allow it (M and N_chol multiples of 8, one spin block
+ *                     of Cholesky vectors, a real trial, CLOSED walkers with 1..50 electrons),
+ *                     else TF32 (the default).
+ * AFQMC_SPLIT_FP16 on shapes that do not allow it returns AFQMC_ERR_UNSUPPORTED.  *active_f16
+ * (optional) receives 1 when the FP16 split runs.  The Taylor propagation always uses TF32. */
+#define AFQMC_SPLIT_AUTO 0
+#define AFQMC_SPLIT_TF32 1
+#define AFQMC_SPLIT_FP16 2
+int afqmc_ham_set_split_format(afqmc_ham ham, int format, int* active_f16);
+
 /* Mixed-precision Taylor propagation: 1 (default) runs all order + 2 products of each walker in
  * one persistent tensor-core kernel (M <= 256 orbitals, N <= 64 electrons per spin), with one or
  * two walkers in flight per CTA chosen by the walker count; 2 / 3 force one / two walkers in
@@ -177,6 +212,9 @@ int afqmc_ham_set_taylor_fused(afqmc_ham ham, int fused);
 #define AFQMC_MIXED_PROPAGATION 2
 #define AFQMC_MIXED_ENERGY 4
 #define AFQMC_MIXED_ALL 7
+/* Attribution only: the step's vHS on the tensor cores with the Taylor propagation in complex128
+ * (without AFQMC_MIXED_PROPAGATION). */
+#define AFQMC_MIXED_VHS 8
 int afqmc_ham_set_mixed_ops(afqmc_ham ham, int mask);
 /* Mixed-precision energy: 1 takes EJ's Coulomb vector Kl = sum_{a,k} G Lnak from a complex128
  * GEMM (one DMMA GEMM per measurement, ~4% of a 10-step block at M=200), 0 (default) from the
@@ -187,6 +225,17 @@ int afqmc_ham_set_coulomb_fp64(afqmc_ham ham, int on);
  * completion gave up after about 2 s and the kernel returned without finishing).  0 = none, or
  * the mixed-precision path was never used.  Synchronous. */
 int afqmc_ham_device_error(afqmc_ham ham, unsigned* flag);
+
+/* Clears the error word of afqmc_ham_device_error.  Synchronous. */
+int afqmc_ham_clear_device_error(afqmc_ham ham);
+
+/* Self-test of the bounded device waits (no counterpart in the reference): one kernel waits on
+ * an mbarrier that nothing arrives at, with the wait routine of the tensor-core kernels and a
+ * budget of budget_cycles (at most the kernels' own, about 2 s; <= 0 selects that).  The wait
+ * gives up, sets bit 0 of the Hamiltonian's error word and the kernel returns, leaving the
+ * context usable.  Returns AFQMC_ERR_TIMEOUT when the wait gave up (the expected outcome).
+ * Synchronous. */
+int afqmc_ham_wait_selftest(afqmc_ham ham, long long budget_cycles, afqmc_stream stream);
 
 /* getOneBodyPropagatorMatrix — Real3IndexFactorization.hpp:99-124 with add_one_body_shifts
  * (detail/one_body.hpp:65-85).  vMF host [Nc]; H1 host [nspin][M][M] = dt (h + v0) + vHS(vMF).

@@ -49,11 +49,19 @@ def run(precision, steps, walkers, equil, seed, exchange_split=3, workload="cfg2
     return sim.energies, time.time() - t0
 
 
-def lockstep(steps, walkers, equil, seed, workload, lscale, exchange_split=3, mixed_ops=7):
+def lockstep(steps, walkers, equil, seed, workload, lscale, exchange_split=3, mixed_ops=7,
+             restart_every=0, measure_every=10, split_format=0):
     """Correlated sampling: the complex128 and the mixed run advance side by side with the same
     fields, the same Eshift and the same population-control decisions (the comb of the complex128
     run's weights applied to both walker sets), so the paired energies differ only through the
-    arithmetic of the mixed step.  Returns the two measurement series."""
+    arithmetic of the mixed step.
+
+    restart_every > 0 restarts both runs from the trial every that many steps (both walker sets
+    back at the trial, Eshift re-seeded, equilibration run again): the benchmark system's total
+    weight collapses some 130-200 steps after the walkers leave the trial, so its paired
+    comparison runs in windows shorter than that.  Measurements come every measure_every steps
+    once a window is past its equilibration.  Returns the two measurement series, the total
+    weights at the combs, the per-component differences and the window of every measurement."""
     from .population import WalkerRows, exchange_walkers
     wl = make_workload(workload, lscale=lscale)
     sims = []
@@ -62,17 +70,24 @@ def lockstep(steps, walkers, equil, seed, workload, lscale, exchange_split=3, mi
         sim = Simulation.from_workload(wl, W=walkers, precision=prec, rp=rp)
         if prec == A.PREC_MIXED and exchange_split != 3:
             sim.ham.set_exchange_split(exchange_split)
-        if prec == A.PREC_MIXED and mixed_ops != 7:
+        if prec == A.PREC_MIXED and mixed_ops != 7:  # 8 (vHS alone) only for attribution
             sim.ham.set_mixed_ops(mixed_ops)
+        if prec == A.PREC_MIXED and split_format:
+            sim.ham.set_split_format(split_format)
         sims.append(sim)
     s64, smx = sims
     rng = A.HostRandomGenerator(A.split_seed(seed, 0, 0))
-    e64, emx, weights, comp = [], [], [], []
-    for step in range(steps):
+    e64, emx, weights, comp, window = [], [], [], [], []
+    win, k = 0, 0  # window index, step within the window
+    for _ in range(steps):
+        if restart_every and k == restart_every:
+            for sim in sims:
+                sim.restart()
+            win, k = win + 1, 0
         smx.Eshift = s64.Eshift
         for sim in sims:
             sim.step(measure=False)  # propagation, orthogonalisation, Eshift update
-        if step % 10 == 0:
+        if k % 10 == 0:
             w = np.abs(s64.wset.getProperty(0))
             weights.append(float(w.sum()))
             off = A.comb(rng, w, walkers)
@@ -80,15 +95,28 @@ def lockstep(steps, walkers, equil, seed, workload, lscale, exchange_split=3, mi
                 exchange_walkers(WalkerRows(sim.wset), off, [walkers], 0)
                 sim.wset.normalize_weights()
                 sim._g_ready = False
-        if step >= equil and step % 10 == 0:
+        if k >= equil and k % measure_every == 0:
             a, sa, _ = s64.measure()
             b, sb, _ = smx.measure()
             e64.append(a)
             emx.append(b)
+            window.append(win)
             # per-component difference of the weighted averages (E1, EXX, EJ)
             comp.append([((sb[i] / sb[3]) - (sa[i] / sa[3])).real for i in range(3)])
+        k += 1
     torch.cuda.synchronize()
-    return np.array(e64), np.array(emx), weights, np.array(comp)
+    return np.array(e64), np.array(emx), weights, np.array(comp), np.array(window)
+
+
+def window_error(x, window):
+    """Standard error of the mean of x from its per-window means (restarted windows are
+    independent); falls back to blocking for a single window."""
+    x, window = np.asarray(x, dtype=np.float64), np.asarray(window)
+    ids = np.unique(window)
+    if ids.size < 2:
+        return blocked_error(x)
+    m = np.array([x[window == i].mean() for i in ids])
+    return float(m.std(ddof=1) / math.sqrt(ids.size))
 
 
 def main(argv=None):
@@ -104,9 +132,16 @@ def main(argv=None):
                     help="Cholesky-vector scale of the synthetic Hamiltonian (0.5: benchmark)")
     ap.add_argument("--lockstep", action="store_true",
                     help="correlated sampling: shared fields, Eshift and comb decisions")
+    ap.add_argument("--restart-every", type=int, default=0,
+                    help="lockstep: restart both runs from the trial every this many steps "
+                         "(0: never)")
+    ap.add_argument("--measure-every", type=int, default=10,
+                    help="lockstep: steps between measurements")
+    ap.add_argument("--split-format", type=int, default=0, choices=[0, 1, 2],
+                    help="lockstep: operand format of the mixed split (0 auto, 1 TF32, 2 FP16)")
     ap.add_argument("--mixed-ops", default="7",
                     help="comma-separated masks of the operations run in mixed precision "
-                         "(1 vbias, 2 vHS + propagation, 4 energy)")
+                         "(1 vbias, 2 vHS + propagation, 4 energy, 8 vHS alone)")
     args = ap.parse_args(argv)
     if args.lockstep:
         outs = []
@@ -114,20 +149,27 @@ def main(argv=None):
                 for m in args.mixed_ops.split(",")]
         for split, mops in runs:
             t0 = time.time()
-            e64, emx, wsum, comp = lockstep(args.steps, args.walkers, args.equil, args.seed,
-                                            args.workload, args.lscale, split, mops)
+            e64, emx, wsum, comp, win = lockstep(args.steps, args.walkers, args.equil,
+                                                 args.seed, args.workload, args.lscale, split,
+                                                 mops, args.restart_every, args.measure_every,
+                                                 args.split_format)
             d = emx - e64
             out = {
                 "mode": "lockstep", "workload": args.workload, "lscale": args.lscale,
                 "steps": args.steps, "walkers": args.walkers, "equilibration_steps": args.equil,
-                "exchange_split": split, "mixed_ops": mops, "measurements": int(d.size),
-                "E_fp64": float(e64.mean()), "E_fp64_err": blocked_error(e64),
-                "E_mixed": float(emx.mean()), "E_mixed_err": blocked_error(emx),
+                "restart_every": args.restart_every, "measure_every": args.measure_every,
+                "windows": int(np.unique(win).size) if win.size else 0,
+                "exchange_split": split, "mixed_ops": mops, "split_format": args.split_format,
+                "measurements": int(d.size),
+                "E_fp64": float(e64.mean()), "E_fp64_err": window_error(e64, win),
+                "E_mixed": float(emx.mean()), "E_mixed_err": window_error(emx, win),
                 "dE_estimate_mHa": 1e3 * float(d.mean()),
-                "dE_estimate_err_mHa": 1e3 * blocked_error(d),
+                "dE_estimate_err_mHa": 1e3 * window_error(d, win),
                 "dE_max_abs_mHa": 1e3 * float(np.abs(d).max()),
                 "dE_components_mHa": {k: 1e3 * float(comp[:, i].mean())
                                       for i, k in enumerate(("E1", "EXX", "EJ"))},
+                "dE_components_err_mHa": {k: 1e3 * window_error(comp[:, i], win)
+                                          for i, k in enumerate(("E1", "EXX", "EJ"))},
                 "total_weight_min_max": [min(wsum), max(wsum)],
                 "wall_s": time.time() - t0,
             }

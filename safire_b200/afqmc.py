@@ -82,6 +82,14 @@ class det_ops:  # noqa: N801 (reference namespace name)
              _ptr(ovlp), W, M, N, int(bool(compact)), _stream(stream))
 
     @staticmethod
+    def MixedDensityMatrixBatched(A, B, C_, ovlp, compact=True, stream=None):
+        """The overload with a bra per walker: A, B [W][M][N] (walker strides A.stride(0),
+        B.stride(0)), C_ [W][N][M] (compact) or [W][M][M]."""
+        W, M, N = B.shape
+        call("afqmc_mixed_density_matrix_batched", _ptr(A), A.stride(0), _ptr(B), B.stride(0),
+             _ptr(C_), C_.stride(0), _ptr(ovlp), W, M, N, int(bool(compact)), _stream(stream))
+
+    @staticmethod
     def inverse_logdet(A, Ainv, logdet, stream=None):
         W, N, _ = A.shape
         call("afqmc_inverse_logdet", _ptr(A), _ptr(Ainv), _ptr(logdet), W, N, _stream(stream))
@@ -173,10 +181,32 @@ class HamiltonianOperations:
         tensor-core exchange traces."""
         call("afqmc_ham_set_coulomb_fp64", self.handle, int(bool(on)))
 
+    def set_vhs_symmetry(self, enable=True):
+        """Symmetric mixed-precision vHS (i <= k pairs only) when every Cholesky vector is
+        symmetric; returns whether it is in use."""
+        active = C.c_int()
+        call("afqmc_ham_set_vhs_symmetry", self.handle, int(bool(enable)), C.byref(active))
+        return bool(active.value)
+
+    def set_split_format(self, fmt=capi.SPLIT_AUTO):
+        """Operand format of the mixed-precision vbias, vHS and exchange (capi.SPLIT_AUTO,
+        SPLIT_TF32 or SPLIT_FP16); returns whether the FP16 split runs."""
+        active = C.c_int()
+        call("afqmc_ham_set_split_format", self.handle, int(fmt), C.byref(active))
+        return bool(active.value)
+
     def set_taylor_fused(self, mode):
         """1/True: one persistent kernel for all Taylor products (default); 0/False: one GEMM
         each; 2 / 3: the persistent kernel with one / two walkers in flight per CTA."""
         call("afqmc_ham_set_taylor_fused", self.handle, int(mode))
+
+    def clear_device_error(self):
+        call("afqmc_ham_clear_device_error", self.handle)
+
+    def wait_selftest(self, budget_cycles, stream=None):
+        """One bounded device wait that nothing completes (afqmc_ham_wait_selftest); raises
+        AfqmcError with status ERR_TIMEOUT when the wait gave up, as it should."""
+        call("afqmc_ham_wait_selftest", self.handle, int(budget_cycles), _stream(stream))
 
     def device_error_flag(self):
         f = C.c_uint()

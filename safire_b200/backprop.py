@@ -17,8 +17,9 @@ walker, is propagated backwards through the stored fields, newest first:
 S <- P1^H sum_n (-i V^H)^n / n! P1^H S with V = vHS(X) (the library's afqmc_propagate given P1^H
 and -V^H), re-orthogonalised with afqmc_orthogonalize every `ortho_interval` steps and at the
 end.  The estimate is sum_w w'_w G_w / sum_w w'_w, w' the weights times the factors of the
-window, G_w = (B T^-1 A^H)^T with A the back-propagated trial, B the anchor and T = A^H B (its
-inverse by afqmc_inverse_logdet; the two batched products go to cuBLAS).  Then the window
+window, G_w = (B T^-1 A^H)^T with A the back-propagated trial, B the anchor and T = A^H B
+(afqmc_mixed_density_matrix_batched: DMMA products and the library's Gauss-Jordan inverse, the
+reference's batched-bra det_ops::MixedDensityMatrix).  Then the window
 restarts from the current walkers.  A trial of several determinants back-propagates each of its
 references (NOMSD: its determinants; PHMSD: its configurations, phmsd_references) and weights
 their density matrices by their shares of each walker's overlap.  One walker set on one GPU.
@@ -80,7 +81,7 @@ def reference_onerdm(refs, walkers, weights, ref_w, log_offset, closed_factor):
     walkers: per spin [W][M][N_s]; log_offset [nref][W] added to the log overlaps (the BP
     log det shift, or minus the walkers' OVLP); closed_factor multiplies the one block's log
     overlap of CLOSED walkers (2 in back propagation, 1 in the mixed estimator).  The log overlap
-    of reference d with walker w is log det(A^H B) over the spins (afqmc_inverse_logdet), its
+    of reference d with walker w is log det(A^H B) over the spins, its
     overlap conj(c_d) e^{log}, its share that over the walker's sum, G_{w,d} = (B T^-1 A^H)^T."""
     nr = len(ref_w)
     W, M = walkers[0].shape[0], walkers[0].shape[1]
@@ -92,15 +93,12 @@ def reference_onerdm(refs, walkers, weights, ref_w, log_offset, closed_factor):
         if N == 0:
             Gs.append(None)
             continue
-        Bd = B.unsqueeze(0).expand(nr, -1, -1, -1).reshape(nr * W, M, N)
-        AH = Aref.conj().transpose(1, 2)
-        T = torch.matmul(AH, Bd).contiguous()
-        Tinv = torch.empty_like(T)
+        Bd = B.unsqueeze(0).expand(nr, -1, -1, -1).reshape(nr * W, M, N).contiguous()
+        G = torch.empty((nr * W, M, M), dtype=torch.complex128, device=dev)
         ld = torch.zeros(nr * W, dtype=torch.complex128, device=dev)
-        A.det_ops.inverse_logdet(T, Tinv, ld)
+        A.det_ops.MixedDensityMatrixBatched(Aref.contiguous(), Bd, G, ld, compact=False)
         lo = lo + closed_factor * ld.view(nr, W)
-        Gs.append(torch.matmul(Bd, torch.matmul(Tinv, AH)).transpose(1, 2)
-                  .reshape(nr, W, M, M))
+        Gs.append(G.view(nr, W, M, M))
     cw = torch.as_tensor(np.conj(np.asarray(ref_w, dtype=np.complex128)), device=dev)[:, None]
     # shares ov_d / sum_d ov_d with ov_d = conj(c_d) e^{lo_d}: a common factor per walker
     # cancels, so the largest real part comes off before the exponential

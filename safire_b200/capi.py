@@ -12,9 +12,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libsafire_afqmc.so")
 
 OK = 0
+# status codes of include/afqmc_c.h
+(ERR_ARG, ERR_SHAPE, ERR_CUDA, ERR_NONFINITE, ERR_TIMEOUT, ERR_ALLOC, ERR_UNSUPPORTED,
+ ERR_COLLAPSE) = range(1, 9)
 CLOSED, COLLINEAR = 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 STEP_G_READY, STEP_KEEP_G = 1, 2  # afqmc_prop_step_flags
+SPLIT_AUTO, SPLIT_TF32, SPLIT_FP16 = 0, 1, 2  # afqmc_ham_set_split_format
 (WEIGHT, PHASE, PSEUDO_ELOC, E1, EXX, EJ, OVLP, LOGSCL_UP, LOGSCL_DN, IS_UNITARY,
  THETA) = range(11)
 NPROP = 11
@@ -44,6 +48,8 @@ _SIGS = {
     "afqmc_log_overlap": (i32, [vp, vp, i64, vp, i32, i32, i32, vp]),
     "afqmc_log_overlap_noalloc": (i32, [vp, vp, i64, vp, i32, i32, i32, vp]),
     "afqmc_mixed_density_matrix": (i32, [vp, vp, i64, vp, i64, vp, i32, i32, i32, i32, vp]),
+    "afqmc_mixed_density_matrix_batched": (i32, [vp, i64, vp, i64, vp, i64, vp, i32, i32, i32,
+                                                 i32, vp]),
     "afqmc_inverse_logdet": (i32, [vp, vp, vp, i32, i32, vp]),
     "afqmc_orthogonalize": (i32, [vp, i64, vp, i32, i32, i32, vp]),
     "afqmc_propagate": (i32, [vp, vp, vp, i64, i32, i32, i32, i32, vp]),
@@ -57,7 +63,11 @@ _SIGS = {
     "afqmc_ham_energy": (i32, [vp, vp, vp, i32, i32, i32, i32, i32, vp]),
     "afqmc_ham_one_body_propagator": (i32, [vp, f64, vp, vp]),
     "afqmc_ham_device_error": (i32, [vp, C.POINTER(C.c_uint)]),
+    "afqmc_ham_clear_device_error": (i32, [vp]),
+    "afqmc_ham_wait_selftest": (i32, [vp, C.c_longlong, vp]),
     "afqmc_ham_set_exchange_split": (i32, [vp, i32]),
+    "afqmc_ham_set_vhs_symmetry": (i32, [vp, i32, C.POINTER(i32)]),
+    "afqmc_ham_set_split_format": (i32, [vp, i32, C.POINTER(i32)]),
     "afqmc_ham_set_taylor_fused": (i32, [vp, i32]),
     "afqmc_prop_step_flags": (i32, [vp, vp, vp, vp, i32, vp]),
     "afqmc_ph_excited_2body_energy": (i32, [vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, i32,

@@ -288,6 +288,67 @@ extern "C" int afqmc_mixed_density_matrix(const afqmc_c128* PsiT, const afqmc_c1
                               cmk(1, 0), cmk(0, 0));
 }
 
+extern "C" int afqmc_mixed_density_matrix_batched(const afqmc_c128* A, long ldA,
+                                                  const afqmc_c128* S, long ldS, afqmc_c128* G,
+                                                  long ldG, afqmc_c128* ovlp, int W, int M, int N,
+                                                  int compact, afqmc_stream stream) {
+  AFQMC_CHECK_ARG(W >= 0 && M >= 0 && N >= 0, "afqmc_mixed_density_matrix_batched: negative size");
+  if (W == 0) return AFQMC_OK;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const long gsize = compact ? long(N) * M : long(M) * M;
+  AFQMC_CHECK_ARG(G && ovlp && (N == 0 || (A && S)),
+                  "afqmc_mixed_density_matrix_batched: null pointer");
+  AFQMC_CHECK_ARG(ldG >= gsize, "afqmc_mixed_density_matrix_batched: ldG too small");
+  if (N == 0) {
+    if (!compact && gsize > 0)
+      AFQMC_CUDA_TRY(cudaMemset2DAsync(G, ldG * sizeof(c128), 0, gsize * sizeof(c128), W, s));
+    return AFQMC_OK;
+  }
+  AFQMC_CHECK_ARG(ldA >= long(M) * N && ldS >= long(M) * N,
+                  "afqmc_mixed_density_matrix_batched: ldA or ldS < M*N");
+  const long NN = long(N) * N;
+  Scratch T, Ti, NMw;
+  AFQMC_TRY(T.get(sizeof(c128) * size_t(W) * NN, s));
+  AFQMC_TRY(Ti.get(sizeof(c128) * size_t(W) * NN, s));
+  if (!compact) AFQMC_TRY(NMw.get(sizeof(c128) * size_t(W) * N * M, s));
+  // T_w = A_w^H S_w  (N x N)
+  GemmParams p{};
+  p.m = N; p.n = N; p.k = M;
+  p.A = A; p.lda = N; p.strideA = ldA;
+  p.B = S; p.ldb = N; p.strideB = ldS;
+  p.C = (c128*)T.p; p.ldc = N; p.strideC = NN;
+  p.alpha = cmk(1, 0); p.beta = cmk(0, 0);
+  AFQMC_TRY(zgemm(s, W, GH, false, GN, false, p));
+  // T_w^{-1} and ovlp[w] += log det T_w
+  AFQMC_TRY(batched_logdet_inverse(s, (const c128*)T.p, NN, (c128*)Ti.p, NN, (c128*)ovlp, W, N,
+                                   true, cmk(1, 0), cmk(0, 0)));
+  if (compact) {
+    // G_w = T_w^{-T} S_w^T  (N x M)
+    p = GemmParams{};
+    p.m = N; p.n = M; p.k = N;
+    p.A = Ti.p; p.lda = N; p.strideA = NN;
+    p.B = S; p.ldb = N; p.strideB = ldS;
+    p.C = (c128*)G; p.ldc = M; p.strideC = ldG;
+    p.alpha = cmk(1, 0); p.beta = cmk(0, 0);
+    return zgemm(s, W, GT, false, GT, false, p);
+  }
+  // X_w = T_w^{-1} A_w^H (N x M); G_w = X_w^T S_w^T = (S_w T_w^{-1} A_w^H)^T  (M x M)
+  p = GemmParams{};
+  p.m = N; p.n = M; p.k = N;
+  p.A = Ti.p; p.lda = N; p.strideA = NN;
+  p.B = A; p.ldb = N; p.strideB = ldA;
+  p.C = (c128*)NMw.p; p.ldc = M; p.strideC = long(N) * M;
+  p.alpha = cmk(1, 0); p.beta = cmk(0, 0);
+  AFQMC_TRY(zgemm(s, W, GN, false, GH, false, p));
+  p = GemmParams{};
+  p.m = M; p.n = M; p.k = N;
+  p.A = NMw.p; p.lda = M; p.strideA = long(N) * M;
+  p.B = S; p.ldb = N; p.strideB = ldS;
+  p.C = (c128*)G; p.ldc = M; p.strideC = ldG;
+  p.alpha = cmk(1, 0); p.beta = cmk(0, 0);
+  return zgemm(s, W, GT, false, GT, false, p);
+}
+
 extern "C" int afqmc_inverse_logdet(const afqmc_c128* A, afqmc_c128* Ainv, afqmc_c128* logdet,
                                     int W, int N, afqmc_stream stream) {
   AFQMC_CHECK_ARG(W >= 0 && N >= 0, "afqmc_inverse_logdet: negative size");
@@ -645,7 +706,8 @@ extern "C" int afqmc_ham_energy(afqmc_ham h, const afqmc_c128* G, afqmc_c128* E,
 }
 
 extern "C" int afqmc_ham_set_mixed_ops(afqmc_ham h, int mask) {
-  AFQMC_CHECK_ARG(h && (mask & ~AFQMC_MIXED_ALL) == 0, "afqmc_ham_set_mixed_ops: bad mask");
+  AFQMC_CHECK_ARG(h && (mask & ~(AFQMC_MIXED_ALL | AFQMC_MIXED_VHS)) == 0,
+                  "afqmc_ham_set_mixed_ops: bad mask");
   h->mixed_ops = mask;
   return AFQMC_OK;
 }
@@ -667,6 +729,26 @@ extern "C" int afqmc_ham_set_exchange_split(afqmc_ham h, int nsplit) {
   return mixed_set_exchange_split(h->mixed, nsplit);
 }
 
+extern "C" int afqmc_ham_set_vhs_symmetry(afqmc_ham h, int enable, int* active) {
+  AFQMC_CHECK_ARG(h, "afqmc_ham_set_vhs_symmetry: null handle");
+  DeviceGuard g(h->device);
+  if (!h->mixed) {
+    EnergyArgs a = energy_args(h, nullptr, 0);
+    AFQMC_TRY(mixed_ham_create(&h->mixed, a, nullptr));
+  }
+  return mixed_set_vhs_symmetry(h->mixed, enable, active);
+}
+
+extern "C" int afqmc_ham_set_split_format(afqmc_ham h, int format, int* active_f16) {
+  AFQMC_CHECK_ARG(h, "afqmc_ham_set_split_format: null handle");
+  DeviceGuard g(h->device);
+  if (!h->mixed) {
+    EnergyArgs a = energy_args(h, nullptr, 0);
+    AFQMC_TRY(mixed_ham_create(&h->mixed, a, nullptr));
+  }
+  return mixed_set_split_format(h->mixed, format, active_f16);
+}
+
 extern "C" int afqmc_ham_set_taylor_fused(afqmc_ham h, int fused) {
   AFQMC_CHECK_ARG(h, "afqmc_ham_set_taylor_fused: null handle");
   AFQMC_CHECK_ARG(fused >= 0 && fused <= 3, "afqmc_ham_set_taylor_fused: mode must be 0..3");
@@ -684,6 +766,25 @@ extern "C" int afqmc_ham_device_error(afqmc_ham h, unsigned* flag) {
   *flag = 0;
   if (h->mixed) return mixed_error_flag(h->mixed, flag);
   return AFQMC_OK;
+}
+
+extern "C" int afqmc_ham_clear_device_error(afqmc_ham h) {
+  AFQMC_CHECK_ARG(h, "afqmc_ham_clear_device_error: null argument");
+  DeviceGuard g(h->device);
+  if (h->mixed) return mixed_clear_error(h->mixed);
+  return AFQMC_OK;
+}
+
+extern "C" int afqmc_ham_wait_selftest(afqmc_ham h, long long budget_cycles,
+                                       afqmc_stream stream) {
+  AFQMC_CHECK_ARG(h, "afqmc_ham_wait_selftest: null argument");
+  DeviceGuard g(h->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!h->mixed) {
+    EnergyArgs a = energy_args(h, nullptr, 0);
+    AFQMC_TRY(mixed_ham_create(&h->mixed, a, s));
+  }
+  return mixed_wait_selftest(s, h->mixed, budget_cycles);
 }
 
 extern "C" int afqmc_ham_one_body_propagator(afqmc_ham h, double dt, const afqmc_c128* vMF,
@@ -1522,6 +1623,8 @@ int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* E
   const bool mixed_any = pr->p.precision == AFQMC_PREC_MIXED;
   const bool mixed_v = mixed_any && (h->mixed_ops & AFQMC_MIXED_VBIAS);
   const bool mixed = mixed_any && (h->mixed_ops & AFQMC_MIXED_PROPAGATION);
+  const bool mixed_vhs_only = mixed_any && !mixed && (h->mixed_ops & AFQMC_MIXED_VHS) &&
+                              h->nspin_H2 == 1;
   // 1. vbias: G of the walkers (NOMSD::vbias, NOMSD.cpp:39-61); with AFQMC_STEP_G_READY the
   //    previous step left it for these walkers
   if (pr->md) {
@@ -1560,6 +1663,12 @@ int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* E
   // 3. vHS
   if (mixed) {
     AFQMC_TRY(vhs_mixed(s, h->mixed, pr->X, nullptr, W, std::sqrt(dt)));
+  } else if (mixed_vhs_only) {
+    if (!h->mixed) {
+      EnergyArgs a = energy_args(h, pr->G, ldG);
+      AFQMC_TRY(mixed_ham_create(&h->mixed, a, s));
+    }
+    AFQMC_TRY(vhs_mixed(s, h->mixed, pr->X, pr->V, W, std::sqrt(dt)));
   } else {
     AFQMC_TRY(ham_vhs(h, s, pr->X, pr->V, W, dt));
   }

@@ -33,6 +33,8 @@ struct XParams {
   int W, N, Nc, M;
   c128* exx;         // [W][Nc] += sum_{a,b} T[b][a] T[a][b]
   c128* kl;          // [W][Nc] += trace T
+  const float* ginv; // FP16 operands: per-walker inverse scale of G (null for TF32)
+  float linv;        // FP16 operands: inverse scale of Lnak
   unsigned* err;
 };
 
@@ -72,9 +74,12 @@ __device__ __forceinline__ void tile_coords(long t, int WP, int NP, int& wp, int
   np = nb * NBLK + int(within % width);
 }
 
-template <int NSPLIT>
+template <int NSPLIT, bool F16>
 __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid_constant__ XParams p) {
   using K = XCfg<NSPLIT>;
+  // 128 bytes of K per stage and operand row: 32 TF32 or 64 FP16 elements; 32 bytes per MMA
+  constexpr int XBKE = F16 ? 2 * XBK : XBK;
+  constexpr int KSTEP = F16 ? 16 : 8;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -115,7 +120,7 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t taddr = *tmem_slot;
-  const int nk = (p.M + XBK - 1) / XBK;
+  const int nk = (p.M + XBKE - 1) / XBKE;
 
   if (warp == 0) {
     if (lane == 0) {
@@ -137,10 +142,10 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
           // A planes: re_hi, (re_lo), im_hi, (im_lo) -> plane order in smem 0..NA-1
 #pragma unroll
           for (int q = 0; q < K::NA; ++q)
-            tc::tma_load_3d(st + q * K::A_TILE, &p.a[q], &full[s], kc * XBK, 0, 2 * wp);
+            tc::tma_load_3d(st + q * K::A_TILE, &p.a[q], &full[s], kc * XBKE, 0, 2 * wp);
 #pragma unroll
           for (int q = 0; q < K::NB; ++q)
-            tc::tma_load_3d(st + K::NA * K::A_TILE + q * K::B_TILE, &p.b[q], &full[s], kc * XBK,
+            tc::tma_load_3d(st + K::NA * K::A_TILE + q * K::B_TILE, &p.b[q], &full[s], kc * XBKE,
                             0, 2 * np);
         }
         if (!ok) break;
@@ -148,7 +153,7 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      constexpr uint32_t ID = tc::idesc_tf32(128, XBN, false);
+      constexpr uint32_t ID = tc::idesc_split<F16>(128, XBN, false);
       long it = 0;
       long ti = 0;
       bool ok = true;
@@ -175,22 +180,22 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
           const uint32_t sa = tc::smem_u32(st);
           const uint32_t sb = tc::smem_u32(st + K::NA * K::A_TILE);
 #pragma unroll
-          for (int kk = 0; kk < XBK / 8; ++kk) {
-            if (kc * XBK + kk * 8 >= p.M) break;  // zero fill past K
+          for (int kk = 0; kk < 4; ++kk) {
+            if (kc * XBKE + kk * KSTEP >= p.M) break;  // zero fill past K
             auto A = [&](int q) { return tc::sdesc_sw128(sa + q * K::A_TILE) + uint64_t(2 * kk); };
             auto B = [&](int q) { return tc::sdesc_sw128(sb + q * K::B_TILE) + uint64_t(2 * kk); };
             const uint32_t acc0 = (kc > 0 || kk > 0) ? 1u : 0u;
             if constexpr (NSPLIT == 3) {
               // Dr = Gr L, Di = Gi L (real trial): hi*hi + hi*lo + lo*hi
-              tc::mma_tf32(dr, A(0), B(0), ID, acc0);
-              tc::mma_tf32(dr, A(0), B(1), ID, 1);
-              tc::mma_tf32(dr, A(1), B(0), ID, 1);
-              tc::mma_tf32(di, A(2), B(0), ID, acc0);
-              tc::mma_tf32(di, A(2), B(1), ID, 1);
-              tc::mma_tf32(di, A(3), B(0), ID, 1);
+              tc::mma_split<F16>(dr, A(0), B(0), ID, acc0);
+              tc::mma_split<F16>(dr, A(0), B(1), ID, 1);
+              tc::mma_split<F16>(dr, A(1), B(0), ID, 1);
+              tc::mma_split<F16>(di, A(2), B(0), ID, acc0);
+              tc::mma_split<F16>(di, A(2), B(1), ID, 1);
+              tc::mma_split<F16>(di, A(3), B(0), ID, 1);
             } else {
-              tc::mma_tf32(dr, A(0), B(0), ID, acc0);
-              tc::mma_tf32(di, A(1), B(0), ID, acc0);
+              tc::mma_split<F16>(dr, A(0), B(0), ID, acc0);
+              tc::mma_split<F16>(di, A(1), B(0), ID, acc0);
             }
           }
           tc::mma_commit(&empty[s]);
@@ -235,6 +240,14 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
         if (nl == 1) {
           tc::tc_fence_before();
           tc::mbar_arrive(&acc_empty[buf]);  // accumulator free for tile ti+2
+        }
+        if (F16 && valid) {  // undo the power-of-two operand scales (exact)
+          const float f = p.ginv[w] * p.linv;
+#pragma unroll
+          for (int a = 0; a < XSLOT_B; ++a) {
+            vr[a] *= f;
+            vi[a] *= f;
+          }
         }
         if (valid) {
 #pragma unroll
@@ -302,14 +315,28 @@ int g_num_sms = 0;
 
 }  // namespace
 
-int make_plane_map_3d(CUtensorMap* map, const float* base, long k, long rows, long row_stride,
-                      long batch, long batch_stride, int box_rows, int box_batch);
+int make_plane_map_3d_es(CUtensorMap* map, const void* base, int esize, long k, long rows,
+                         long row_stride, long batch, long batch_stride, int box_rows,
+                         int box_batch);
+
+namespace {
+template <int NSPLIT, bool F16>
+int launch_exchange(cudaStream_t s, const XParams& p, int grid) {
+  using K = XCfg<NSPLIT>;
+  AFQMC_CUDA_TRY(cudaFuncSetAttribute(exchange_tc_kernel<NSPLIT, F16>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM)));
+  exchange_tc_kernel<NSPLIT, F16><<<grid, XT_THREADS, K::SMEM, s>>>(p);
+  return launch_status("exchange_tc_kernel");
+}
+}  // namespace
 
 // T-free exchange: exx[w][n] += sum_{a,b} T[b][a]T[a][b], kl[w][n] += trace T for spin block sp.
-// G planes: [W][ldG] with the spin block at element offset `off` (rows of M); Lnak planes [Nc][N][M].
-int exchange_fused_tc(cudaStream_t s, const float* const Gp[4], long ldG, long off,
-                      const float* const Lp[2], int W, int N, int Nc, int M, int nsplit,
-                      c128* exx, c128* kl, unsigned* err) {
+// G planes: [W][ldG] with the spin block at element offset `off` (rows of M); Lnak planes
+// [Nc][N][M]; FP32 (esize 4, TF32 split) or FP16 (esize 2, FP16 split: G rows scaled per walker,
+// g_inv[w] and l_inv the inverse scales).
+int exchange_fused_tc(cudaStream_t s, const void* const Gp[4], int esize, long ldG, long off,
+                      const void* const Lp[2], int W, int N, int Nc, int M, int nsplit,
+                      const float* g_inv, float l_inv, c128* exx, c128* kl, unsigned* err) {
   if (N > 50 || N < 1) {
     set_error_detail("exchange_fused_tc: N = %d outside 1..50", N);
     return AFQMC_ERR_UNSUPPORTED;
@@ -321,17 +348,20 @@ int exchange_fused_tc(cudaStream_t s, const float* const Gp[4], long ldG, long o
   const int na = nsplit == 3 ? 4 : 2;
   for (int q = 0; q < na; ++q) {
     const int src = nsplit == 3 ? amap3[q] : amap1[q];
-    AFQMC_TRY(make_plane_map_3d(&p.a[q], Gp[src] + off, M, N, M, W, ldG, XSLOT_A, 2));
+    AFQMC_TRY(make_plane_map_3d_es(&p.a[q], static_cast<const char*>(Gp[src]) + off * esize,
+                                   esize, M, N, M, W, ldG, XSLOT_A, 2));
   }
   const int nb = nsplit == 3 ? 2 : 1;
   for (int q = 0; q < nb; ++q)
-    AFQMC_TRY(make_plane_map_3d(&p.b[q], Lp[q], M, N, M, Nc, long(N) * M, XSLOT_B, 2));
+    AFQMC_TRY(make_plane_map_3d_es(&p.b[q], Lp[q], esize, M, N, M, Nc, long(N) * M, XSLOT_B, 2));
   p.W = W;
   p.N = N;
   p.Nc = Nc;
   p.M = M;
   p.exx = exx;
   p.kl = kl;
+  p.ginv = g_inv;
+  p.linv = l_inv;
   p.err = err;
   if (g_num_sms == 0) {
     int dev = 0;
@@ -340,18 +370,13 @@ int exchange_fused_tc(cudaStream_t s, const float* const Gp[4], long ldG, long o
   }
   const long ntiles = long((W + 1) / 2) * ((Nc + 1) / 2);
   const int grid = int(ntiles < g_num_sms ? ntiles : g_num_sms);
-  if (nsplit == 3) {
-    using K = XCfg<3>;
-    AFQMC_CUDA_TRY(cudaFuncSetAttribute(exchange_tc_kernel<3>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM)));
-    exchange_tc_kernel<3><<<grid, XT_THREADS, K::SMEM, s>>>(p);
-  } else {
-    using K = XCfg<1>;
-    AFQMC_CUDA_TRY(cudaFuncSetAttribute(exchange_tc_kernel<1>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM)));
-    exchange_tc_kernel<1><<<grid, XT_THREADS, K::SMEM, s>>>(p);
+  const bool f16 = esize == 2;
+  if (f16 && !g_inv) {
+    set_error_detail("exchange_fused_tc: FP16 planes without their scales");
+    return AFQMC_ERR_ARG;
   }
-  return launch_status("exchange_tc_kernel");
+  if (nsplit == 3) return f16 ? launch_exchange<3, true>(s, p, grid) : launch_exchange<3, false>(s, p, grid);
+  return f16 ? launch_exchange<1, true>(s, p, grid) : launch_exchange<1, false>(s, p, grid);
 }
 
 }  // namespace afqmc

@@ -29,8 +29,19 @@ int exchange_T_tc(cudaStream_t s, MixedHam* m, int sp, int w0, int wc, c128* wor
 // fused T-free exchange for spin block sp (real trial, N <= 50): exx/kl [W][Nc] +=
 bool exchange_fused_ok(MixedHam* m, int sp);
 int exchange_fused(cudaStream_t s, MixedHam* m, int sp, int W, c128* exx, c128* kl);
+// vHS over the i <= k pairs only when every Cholesky vector is symmetric (enable = 1, the
+// default) or over all pairs (0); *active tells whether the symmetric form runs
+int mixed_set_vhs_symmetry(MixedHam* m, int enable, int* active);
+// operand format of vbias, vHS and the exchange contraction: 0 auto (FP16 split when the shapes
+// allow it), 1 TF32 split, 2 FP16 split (an error when the shapes do not allow it);
+// *active_f16 tells whether the FP16 split runs
+int mixed_set_split_format(MixedHam* m, int format, int* active_f16);
 // 3: 3xTF32 (default), 1: single TF32 product in the exchange contraction
 int mixed_set_exchange_split(MixedHam* m, int nsplit);
+// one bounded device wait that nothing completes, with a budget of `budget` cycles (at most the
+// kernels' own): AFQMC_ERR_TIMEOUT and bit 0 of the error word when it gave up
+int mixed_wait_selftest(cudaStream_t s, MixedHam* m, long long budget);
+int mixed_clear_error(MixedHam* m);
 // first device-side wait timeout reported by the tensor-core kernels (0 = none)
 int mixed_error_flag(MixedHam* m, unsigned* flag);
 

@@ -1,7 +1,7 @@
 // Learned exchange-energy control variate: a small MLP (features -> H -> H -> 1, GELU) trained
-// and evaluated by this library's own BF16 tensor-core kernels (mma.sync m16n8k16, FP32
-// accumulation; the layers are a few hundred wide, so one CTA tile per 64 x 64 output block is
-// enough and tcgen05's 128-row tiles would leave most SMs idle), FP32 master weights and Adam.
+// and evaluated by this library's own BF16 tensor-core kernels (tcgen05.mma kind::f16 with BF16
+// operands and an FP32 accumulator in tensor memory, one 128 x 64 output tile per CTA), FP32
+// master weights and Adam.
 //
 // It has no counterpart in the reference: the exact exchange energy (Real3IndexFactorization
 // energy_impl, Real3IndexFactorization.hpp:476-590) stays the reference value.  The estimator that uses it
@@ -20,13 +20,18 @@
 #include <vector>
 
 #include "common.cuh"
+#include "tc.cuh"
 
 namespace afqmc {
 namespace {
 
 using bf16 = __nv_bfloat16;
 
-constexpr int MB = 64, NB = 64, KB = 32, MLP_THREADS = 128;
+// GEMM tiles: 128 output rows (the tcgen05 M) x 64 columns, K in chunks of 64 BF16 (one 128-byte
+// swizzle row per operand row), two chunks in flight
+constexpr int TMB = 128, TNB = 64, TKB = 64, MLP_THREADS = 128;
+constexpr int MA_TILE = TMB * 128, MB_TILE = TNB * 128, M_STAGE = MA_TILE + MB_TILE;
+constexpr size_t MLP_SMEM = 2 * size_t(M_STAGE) + 1024 + 64;
 
 __device__ __forceinline__ float gelu(float z) {
   return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
@@ -38,96 +43,148 @@ __device__ __forceinline__ float gelu_grad(float z) {
 }
 
 __device__ __forceinline__ float to_f(bf16 x) { return __bfloat162float(x); }
+__device__ __forceinline__ float to_f(float x) { return x; }
 
 enum Epi { EPI_STORE = 0, EPI_BIAS_GELU = 1, EPI_GELU_GRAD = 2 };
 
+// Instruction descriptor: kind::f16 with BF16 A and B, F32 D, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                         uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// byte offset of BF16 element (r, k) of a K-major tile in the 128-byte swizzle layout the UMMA
+// descriptor expects (the layout TMA writes): 16-byte unit k/8 of row r sits at unit (k/8) ^ (r%8)
+__device__ __forceinline__ uint32_t sw128_off(int r, int k) {
+  return uint32_t(r) * 128u + ((uint32_t(k >> 3) ^ uint32_t(r & 7)) << 4) + uint32_t(k & 7) * 2u;
+}
+
+// rows x TKB of op(element) into a swizzled tile; elem(r, k) = P[r sr + k sk]; the thread walk
+// follows the contiguous index for coalesced reads
+template <typename T>
+__device__ __forceinline__ void fill_tile(unsigned char* tile, int rows, int r0, int R, int k0,
+                                          int K, const T* __restrict__ P, long sr, long sk) {
+  const bool k_fast = (sk == 1);
+  for (int idx = threadIdx.x; idx < rows * TKB; idx += MLP_THREADS) {
+    int r, k;
+    if (k_fast) {
+      r = idx / TKB;
+      k = idx - r * TKB;
+    } else {
+      k = idx / rows;
+      r = idx - k * rows;
+    }
+    const int gr = r0 + r, gk = k0 + k;
+    const float v = (gr < R && gk < K) ? to_f(P[gr * sr + gk * sk]) : 0.f;
+    *reinterpret_cast<bf16*>(tile + sw128_off(r, k)) = __float2bfloat16(v);
+  }
+}
+
 // C[m][n] = sum_k A(m, k) B(k, n), A(m, k) = A[m sam + k sak], B(k, n) = B[k sbk + n sbn],
-// operands rounded to BF16 in shared memory, FP32 accumulation by mma.sync m16n8k16.
+// operands rounded to BF16 in shared memory, FP32 accumulation in tensor memory:
 //   EPI_STORE:     Cf[m][n] = acc                                   (FP32, ldc)
 //   EPI_BIAS_GELU: Z = acc + bias[n]; Cf = Z (FP32); Cb = gelu(Z) (BF16)
 //   EPI_GELU_GRAD: Cb = acc * gelu'(Zin[m][n])                      (BF16)
+// All 128 threads convert the next K chunk into the free stage while one thread's MMAs run on
+// the other (an mbarrier per stage tells when those MMAs have read it); the four warps then
+// read their 32 accumulator rows from tensor memory.  Waits are bounded (error word err).
 template <typename TA, typename TB, int EPI>
-__global__ void __launch_bounds__(MLP_THREADS) mlp_gemm_kernel(
+__global__ void __launch_bounds__(MLP_THREADS, 1) mlp_gemm_kernel(
     int M, int N, int K, const TA* __restrict__ A, long sam, long sak, const TB* __restrict__ B,
     long sbk, long sbn, float* __restrict__ Cf, bf16* __restrict__ Cb, long ldc,
-    const float* __restrict__ bias, const float* __restrict__ Zin) {
-  __shared__ __align__(16) bf16 As[MB][KB + 8];  // [m][k]
-  __shared__ __align__(16) bf16 Bs[NB][KB + 8];  // [n][k]
-  const int m0 = blockIdx.y * MB, n0 = blockIdx.x * NB;
+    const float* __restrict__ bias, const float* __restrict__ Zin, unsigned* err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* done = reinterpret_cast<uint64_t*>(base + 2 * M_STAGE);  // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 2);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int m0 = blockIdx.y * TMB, n0 = blockIdx.x * TNB;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  const int g = lane >> 2, t = lane & 3;
-  float acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
-
-  for (int k0 = 0; k0 < K; k0 += KB) {
-    for (int idx = threadIdx.x; idx < MB * KB; idx += blockDim.x) {
-      const int m = idx / KB, k = idx - m * KB;
-      const int gm = m0 + m, gk = k0 + k;
-      As[m][k] = __float2bfloat16(gm < M && gk < K ? to_f(A[gm * sam + gk * sak]) : 0.f);
-    }
-    for (int idx = threadIdx.x; idx < NB * KB; idx += blockDim.x) {
-      const int n = idx / KB, k = idx - n * KB;
-      const int gn = n0 + n, gk = k0 + k;
-      Bs[n][k] = __float2bfloat16(gn < N && gk < K ? to_f(B[gk * sbk + gn * sbn]) : 0.f);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < KB; kk += 16) {
-      uint32_t af[2][4], bfr[4][2];
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int r = wm + 16 * i + g;
-        af[i][0] = *reinterpret_cast<const uint32_t*>(&As[r][kk + 2 * t]);
-        af[i][1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][kk + 2 * t]);
-        af[i][2] = *reinterpret_cast<const uint32_t*>(&As[r][kk + 2 * t + 8]);
-        af[i][3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][kk + 2 * t + 8]);
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int c = wn + 8 * j + g;
-        bfr[j][0] = *reinterpret_cast<const uint32_t*>(&Bs[c][kk + 2 * t]);
-        bfr[j][1] = *reinterpret_cast<const uint32_t*>(&Bs[c][kk + 2 * t + 8]);
-      }
-#pragma unroll
-      for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          asm volatile(
-              "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-              "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
-              : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
-              : "r"(af[i][0]), "r"(af[i][1]), "r"(af[i][2]), "r"(af[i][3]), "r"(bfr[j][0]),
-                "r"(bfr[j][1]));
-    }
-    __syncthreads();
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&done[0], 1);
+    tc::mbar_init(&done[1], 1);
+    *abort_flag = 0;
+    tc::fence_mbar_init();
   }
+  if (warp == 0) {
+    tc::tmem_alloc(tmem_slot, TNB);
+    tc::tmem_relinquish();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t taddr = *tmem_slot;
+  constexpr uint32_t ID = idesc_bf16(TMB, TNB);
+  const int nk = (K + TKB - 1) / TKB;
+  for (int kc = 0; kc < nk; ++kc) {
+    const int s = kc & 1;
+    unsigned char* st = base + s * M_STAGE;
+    // the MMAs of chunk kc - 2 read this stage
+    if (kc >= 2) tc::mbar_wait(&done[s], unsigned((kc - 2) >> 1) & 1u, err, abort_flag);
+    fill_tile(st, TMB, m0, M, kc * TKB, K, A, sam, sak);
+    fill_tile(st + MA_TILE, TNB, n0, N, kc * TKB, K, B, sbn, sbk);
+    // the generic-proxy stores above become visible to the tensor core (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0 && !*abort_flag) {
+      tc::tc_fence_after();
+      const uint32_t sa = tc::smem_u32(st), sb = tc::smem_u32(st + MA_TILE);
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+      for (int kk = 0; kk < 4; ++kk) {
+        if (kc * TKB + kk * 16 >= K) break;
+        mma_bf16(taddr, tc::sdesc_sw128(sa) + uint64_t(2 * kk), tc::sdesc_sw128(sb) + uint64_t(2 * kk),
+                 ID, (kc > 0 || kk > 0) ? 1u : 0u);
+      }
+      tc::mma_commit(&done[s]);
+    }
+  }
+  // the last commit completes after every earlier MMA of this thread
+  const int last = nk - 1;
+  const bool mine = nk > 0 && !*abort_flag &&
+                    tc::mbar_wait(&done[last & 1], unsigned(last >> 1) & 1u, err, abort_flag);
+  // every thread takes the same branch: the tensor-memory loads below are warp-collective
+  const bool ok = __syncthreads_and(mine) != 0;
+  tc::tc_fence_after();
+  if (ok) {
+    const int m = m0 + warp * 32 + lane;
+    const uint32_t trow = taddr + (uint32_t(warp * 32) << 16);
+#pragma unroll 1
+    for (int c0 = 0; c0 < TNB; c0 += 16) {
+      float v[16];
+      tc::tmem_ld16(trow + c0, v);
+      tc::tmem_ld_wait();
+      if (m >= M) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int m = m0 + wm + 16 * i + g + (q >= 2 ? 8 : 0);
-        const int n = n0 + wn + 8 * j + 2 * t + (q & 1);
-        if (m >= M || n >= N) continue;
-        const long o = m * ldc + n;
-        float v = acc[i][j][q];
+      for (int j = 0; j < 16; ++j) {
+        const int n = n0 + c0 + j;
+        if (n >= N) break;
+        const long o = long(m) * ldc + n;
+        float x = v[j];
         if (EPI == EPI_STORE) {
-          Cf[o] = v;
+          Cf[o] = x;
         } else if (EPI == EPI_BIAS_GELU) {
-          v += bias[n];
-          Cf[o] = v;
-          Cb[o] = __float2bfloat16(gelu(v));
+          x += bias[n];
+          Cf[o] = x;
+          Cb[o] = __float2bfloat16(gelu(x));
         } else {
-          Cb[o] = __float2bfloat16(v * gelu_grad(Zin[o]));
+          Cb[o] = __float2bfloat16(x * gelu_grad(Zin[o]));
         }
       }
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(taddr, TNB);
 }
 
 // Xn[b][d] = bf16((X[b][d] - mean[d]) * istd[d])
@@ -285,6 +342,7 @@ struct afqmc_mlp_s {
   // batch workspace (cap rows)
   bf16 *Xn = nullptr, *A1 = nullptr, *A2 = nullptr, *dZ2 = nullptr, *dZ1 = nullptr;
   float *Z1 = nullptr, *Z2 = nullptr, *y = nullptr, *dy = nullptr, *loss = nullptr;
+  unsigned* err = nullptr;  // bounded-wait error word of the GEMM kernels (bit 0: timeout)
   long nparam() const { return long(H) * D + H + long(H) * H + H + H + 1; }
   long oW1() const { return 0; }
   long ob1() const { return long(H) * D; }
@@ -306,7 +364,7 @@ struct afqmc_mlp_s {
     cudaSetDevice(device);
     free_batch();
     for (void* p : {(void*)P, (void*)Gr, (void*)Mo, (void*)Vo, (void*)Pb, (void*)mean,
-                    (void*)istd, (void*)loss})
+                    (void*)istd, (void*)loss, (void*)err})
       if (p) cudaFree(p);
     cudaSetDevice(prev);
   }
@@ -333,12 +391,16 @@ int mlp_batch(afqmc_mlp h, int B) {
 }
 
 template <typename TA, typename TB, int EPI>
-int gemm(cudaStream_t s, int M, int N, int K, const TA* A, long sam, long sak, const TB* B,
-         long sbk, long sbn, float* Cf, bf16* Cb, long ldc, const float* bias = nullptr,
-         const float* Zin = nullptr) {
-  dim3 grid((N + NB - 1) / NB, (M + MB - 1) / MB);
-  mlp_gemm_kernel<TA, TB, EPI><<<grid, MLP_THREADS, 0, s>>>(M, N, K, A, sam, sak, B, sbk, sbn, Cf,
-                                                            Cb, ldc, bias, Zin);
+int gemm(cudaStream_t s, unsigned* err, int M, int N, int K, const TA* A, long sam, long sak,
+         const TB* B, long sbk, long sbn, float* Cf, bf16* Cb, long ldc,
+         const float* bias = nullptr, const float* Zin = nullptr) {
+  if (M <= 0 || N <= 0) return AFQMC_OK;
+  auto kern = mlp_gemm_kernel<TA, TB, EPI>;
+  AFQMC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(MLP_SMEM)));
+  dim3 grid((N + TNB - 1) / TNB, (M + TMB - 1) / TMB);
+  kern<<<grid, MLP_THREADS, MLP_SMEM, s>>>(M, N, K, A, sam, sak, B, sbk, sbn, Cf, Cb, ldc, bias,
+                                           Zin, err);
   return launch_status("mlp_gemm_kernel");
 }
 
@@ -348,10 +410,10 @@ int mlp_forward(afqmc_mlp h, const float* X, int B, cudaStream_t s) {
   standardize_kernel<<<grid1(long(B) * D, 256), 256, 0, s>>>(X, h->mean, h->istd, B, D, h->Xn);
   AFQMC_TRY(launch_status("standardize_kernel"));
   // Z1 = Xn W1^T + b1
-  AFQMC_TRY((gemm<bf16, bf16, EPI_BIAS_GELU>(s, B, H, D, h->Xn, D, 1, h->Pb + h->oW1(), 1, D,
+  AFQMC_TRY((gemm<bf16, bf16, EPI_BIAS_GELU>(s, h->err, B, H, D, h->Xn, D, 1, h->Pb + h->oW1(), 1, D,
                                              h->Z1, h->A1, H, h->P + h->ob1())));
   // Z2 = A1 W2^T + b2
-  AFQMC_TRY((gemm<bf16, bf16, EPI_BIAS_GELU>(s, B, H, H, h->A1, H, 1, h->Pb + h->oW2(), 1, H,
+  AFQMC_TRY((gemm<bf16, bf16, EPI_BIAS_GELU>(s, h->err, B, H, H, h->A1, H, 1, h->Pb + h->oW2(), 1, H,
                                              h->Z2, h->A2, H, h->P + h->ob2())));
   return AFQMC_OK;
 }
@@ -369,15 +431,15 @@ int mlp_backward(afqmc_mlp h, int B, cudaStream_t s) {
                                                                H, h->dZ2);
   AFQMC_TRY(launch_status("head_backward_kernel"));
   // dW2 = dZ2^T A1, db2 = column sums of dZ2
-  AFQMC_TRY((gemm<bf16, bf16, EPI_STORE>(s, H, H, B, h->dZ2, 1, H, h->A1, H, 1, g + h->oW2(),
+  AFQMC_TRY((gemm<bf16, bf16, EPI_STORE>(s, h->err, H, H, B, h->dZ2, 1, H, h->A1, H, 1, g + h->oW2(),
                                          nullptr, H)));
   column_sum_kernel<bf16><<<grid1(H, 128), 128, 0, s>>>(h->dZ2, nullptr, B, H, g + h->ob2());
   AFQMC_TRY(launch_status("column_sum_kernel"));
   // dZ1 = (dZ2 W2) gelu'(Z1)
-  AFQMC_TRY((gemm<bf16, bf16, EPI_GELU_GRAD>(s, B, H, H, h->dZ2, H, 1, h->Pb + h->oW2(), H, 1,
+  AFQMC_TRY((gemm<bf16, bf16, EPI_GELU_GRAD>(s, h->err, B, H, H, h->dZ2, H, 1, h->Pb + h->oW2(), H, 1,
                                              nullptr, h->dZ1, H, nullptr, h->Z1)));
   // dW1 = dZ1^T Xn, db1 = column sums of dZ1
-  AFQMC_TRY((gemm<bf16, bf16, EPI_STORE>(s, H, D, B, h->dZ1, 1, H, h->Xn, D, 1, g + h->oW1(),
+  AFQMC_TRY((gemm<bf16, bf16, EPI_STORE>(s, h->err, H, D, B, h->dZ1, 1, H, h->Xn, D, 1, g + h->oW1(),
                                          nullptr, D)));
   column_sum_kernel<bf16><<<grid1(H, 128), 128, 0, s>>>(h->dZ1, nullptr, B, H, g + h->ob1());
   return launch_status("column_sum_kernel");
@@ -413,6 +475,8 @@ extern "C" int afqmc_mlp_create(int D, int H, unsigned long long seed, afqmc_mlp
   AFQMC_CUDA_TRY(cudaMalloc(&h->mean, sizeof(float) * D));
   AFQMC_CUDA_TRY(cudaMalloc(&h->istd, sizeof(float) * D));
   AFQMC_CUDA_TRY(cudaMalloc(&h->loss, sizeof(float)));
+  AFQMC_CUDA_TRY(cudaMalloc(&h->err, sizeof(unsigned)));
+  AFQMC_CUDA_TRY(cudaMemset(h->err, 0, sizeof(unsigned)));
   AFQMC_CUDA_TRY(cudaMemcpy(h->P, p.data(), sizeof(float) * np, cudaMemcpyHostToDevice));
   AFQMC_CUDA_TRY(cudaMemset(h->Gr, 0, sizeof(float) * np));
   AFQMC_CUDA_TRY(cudaMemset(h->Mo, 0, sizeof(float) * np));

@@ -17,7 +17,13 @@
 //     stream are ordered and safe.  Each call overwrites the whole scratch region it uses before
 //     reading it, so nothing in it needs to start at zero;
 //   - the first call on a device looks the array's device address up (cudaGetSymbolAddress) with
-//     that device current; make that first call before any stream capture on that device.
+//     that device current; make that first call before any stream capture on that device.  The
+//     address is kept with the unique ID of the context it belongs to (cuCtxGetId); a call in a
+//     different context of the device (after cudaDeviceReset, which reloads the module) looks it
+//     up again, so no call uses an address of a context that no longer exists.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <mutex>
 
 #include "detops.cuh"
@@ -32,8 +38,32 @@ static __device__ __align__(256) c128 g_noalloc_scratch[kNoAllocScratchElems];
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
 c128* g_scratch_ptr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};  // cuCtxGetId of the context of the address
 
-// Device address of the scratch array on the current device (looked up once per device).
+// unique ID of the current context (0 if the driver entry points are unavailable)
+unsigned long long current_context_id() {
+  static PFN_cuCtxGetCurrent_v4000 get_cur = nullptr;
+  static PFN_cuCtxGetId_v12000 get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_cur = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(p);
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_cur && get_id && get_cur(&ctx) == CUDA_SUCCESS && ctx) get_id(ctx, &id);
+  return id;
+}
+
+// Device address of the scratch array on the current device, looked up once per device and
+// context.
 int noalloc_scratch(c128** out) {
   int dev = -1;
   AFQMC_CUDA_TRY(cudaGetDevice(&dev));
@@ -41,8 +71,11 @@ int noalloc_scratch(c128** out) {
     set_error_detail("afqmc_log_overlap_noalloc: device %d out of range", dev);
     return AFQMC_ERR_ARG;
   }
+  // 0 before the context is current on this thread: then the address is looked up (which makes
+  // it current) and again on the next call, when the ID is known
+  const unsigned long long ctx = current_context_id();
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
+  if (!g_scratch_ptr[dev] || ctx == 0 || g_scratch_ctx[dev] != ctx) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
@@ -51,6 +84,7 @@ int noalloc_scratch(c128** out) {
       return AFQMC_ERR_CUDA;
     }
     g_scratch_ptr[dev] = static_cast<c128*>(p);
+    g_scratch_ctx[dev] = ctx;
   }
   *out = g_scratch_ptr[dev];
   return AFQMC_OK;

@@ -17,6 +17,14 @@
 // an async-proxy fence; the running sum R = sum_n T_n is kept in FP32 in global memory (the
 // epilogue adds each term, in the order of the per-term GEMM path) and split once for the last
 // product.  K steps past M (zero fill of the last 32-wide chunk) are not issued.
+//
+// FP16 form (F16 = true): the operands are FP16 split planes of power-of-two-scaled values (P1
+// one scale; V and S one scale per walker), twice the tensor rate and half the bytes of TF32.
+// The epilogue turns each accumulator into the term's true values with the operands' inverse
+// scales, and stores each term T_n (and R) in planes of its own scale: a first pass over the
+// walker's accumulators (both 128-row tiles) finds the largest |value|, the four epilogue warps
+// agree on it through shared memory, and a second pass scales, splits and stores.  The running
+// sum stays FP32 in true values.
 #include "mixed.cuh"
 #include "tc.cuh"
 
@@ -38,14 +46,18 @@ struct TyParams {
   CUtensorMap s[4];      // S^T planes: {M, N, W}
   CUtensorMap t[2][4];   // T ping-pong planes: {M, N, W}
   CUtensorMap r[4];      // R^T planes: {M, N, W}
-  float* tp[2][4];       // T ping-pong planes (epilogue writes) [W][N][M]
-  float* rp[4];          // R planes [W][N][M]
+  void* tp[2][4];        // T ping-pong planes (epilogue writes) [W][N][M]
+  void* rp[4];           // R planes [W][N][M]
   float* sum[2];         // running sum re, im (FP32) [W][N][M]
   c128* S;               // walker Slater matrices (output), [W] x ldS, [M][N] each
   long ldS;
   long pl_ld, pl_bs;     // ld / batch stride of the [W][N][M] planes
   int W, M, N, order;
   int nslots;            // walkers in flight per CTA (1 or 2)
+  // FP16 form: inverse power-of-two scales of the operands (V and S per walker, P1 one)
+  const float* v_inv;
+  const float* s_inv;
+  float p1_inv;
   unsigned* err;
 };
 
@@ -54,9 +66,21 @@ __device__ __forceinline__ void fence_proxy_async_global() {
 }
 
 __device__ __forceinline__ void split_store(float v, float* hi, float* lo, long idx) {
-  const float h = tc::tf32_hi(v);
+  float h, l;
+  tc::tf32_split(v, h, l);
   hi[idx] = h;
-  lo[idx] = v - h;
+  lo[idx] = l;
+}
+
+__device__ __forceinline__ void split_store16(float v, void* hi, void* lo, long idx) {
+  __half h, l;
+  tc::f16_split(v, h, l);
+  static_cast<__half*>(hi)[idx] = h;
+  static_cast<__half*>(lo)[idx] = l;
+}
+
+__device__ __forceinline__ void named_bar_sync(int id, int n) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
 }
 
 // The order in which a CTA runs (slot, walker, phase): the two slots alternate; a slot whose
@@ -93,7 +117,177 @@ struct Schedule {
   }
 };
 
+// Epilogue of the FP16 form (warps 2-5).  Per (slot, walker, phase): pass 1 reads the walker's
+// accumulators (both 128-row tiles) and finds the largest |value| of what the phase stores (the
+// new term, or R = sum + T_order for the last term); the four warps exchange their maxima and
+// failure flags through shared memory between two named barriers, so that they agree on the
+// scale and on whether to go on (a bounded wait that gave up ends every warp's loop at the same
+// point); pass 2 reads the accumulators again, frees them, and stores.  Values are true values
+// (the accumulator times the operands' inverse scales); the planes hold them times 2^e.
+__device__ __forceinline__ void taylor_epilogue_f16(const TyParams& p, uint32_t taddr,
+                                                    uint64_t* acc_full, uint64_t* acc_empty,
+                                                    uint64_t* phase_done,
+                                                    volatile int* abort_flag, float* red,
+                                                    int warp, int lane) {
+  const int q = warp & 3;
+  const int N = p.N, M = p.M, nph = p.order + 2, MT = (M + 127) / 128;
+  const long pl_ld = p.pl_ld;
+  float* __restrict__ const sum_r = p.sum[0];
+  float* __restrict__ const sum_i = p.sum[1];
+  int* const redf = reinterpret_cast<int*>(red + 4);
+  Schedule sc(p.W, nph, blockIdx.x, gridDim.x, p.nslots);
+  long use0 = 0, use1 = 0;
+  float pinv0 = 1.f, pinv1 = 1.f;  // inverse scale of the planes each slot stored last
+  int sl;
+  while (sc.get(sl)) {
+    const int w = sc.w(sl), ph = sc.ph(sl);
+    const bool taylor = (ph > 0 && ph < nph - 1);
+    const bool last_phase = (ph == nph - 1);
+    const bool last_term = (ph == nph - 2);
+    const float ai = taylor ? 1.0f / float(ph) : 0.0f;
+    const float pin = sl ? pinv1 : pinv0;
+    // accumulator -> true values: inverse scales of the A (P1 or V_w) and B (S_w, T or R) planes
+    const float f_in = ph == 0 ? p.p1_inv * p.s_inv[w]
+                               : (last_phase ? p.p1_inv * pin : p.v_inv[w] * pin);
+    const unsigned par = unsigned(sl ? use1 : use0) & 1u;
+    const long wb = long(w) * p.pl_bs;
+    bool ok = true;
+
+    // the true values of accumulator chunk (mt, c0), with the running sum when `with_sum`
+    auto values = [&](uint32_t tacc, int c0, float* xr, float* xi) {
+      float vr[16], vi[16];
+      tc::tmem_ld16(tacc + c0, vr);
+      tc::tmem_ld16(tacc + TBN + c0, vi);
+      tc::tmem_ld_wait();
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        if (taylor) {
+          xr[j] = -ai * (vi[j] * f_in);
+          xi[j] = ai * (vr[j] * f_in);
+        } else {
+          xr[j] = vr[j] * f_in;
+          xi[j] = vi[j] * f_in;
+        }
+      }
+    };
+
+    float mx = 0.f;
+    if (!last_phase) {
+      for (int mt = 0; mt < MT; ++mt) {
+        if (ok && !tc::mbar_wait(&acc_full[sl * 2 + mt], par, p.err, abort_flag)) ok = false;
+        if (!ok) continue;
+        tc::tc_fence_after();
+        const int row = mt * 128 + q * 32 + lane;
+        const uint32_t tacc =
+            taddr + (uint32_t(q * 32) << 16) + uint32_t(sl * 256 + mt * 2 * TBN);
+        const long off = wb + row;
+#pragma unroll 1
+        for (int c0 = 0; c0 < TBN; c0 += 16) {
+          float xr[16], xi[16];
+          values(tacc, c0, xr, xi);
+          if (row >= M || c0 >= N) continue;
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (c0 + j < N) {
+              float ur = xr[j], ui = xi[j];
+              if (last_term && taylor) {
+                const long idx = off + long(c0 + j) * pl_ld;
+                ur += sum_r[idx];
+                ui += sum_i[idx];
+              }
+              mx = fmaxf(mx, fmaxf(fabsf(ur), fabsf(ui)));
+            }
+        }
+      }
+    }
+    // agree on the scale and on going on
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) {
+      red[q] = mx;
+      redf[q] = ok ? 0 : 1;
+    }
+    named_bar_sync(1, 128);
+    const float m4 = fmaxf(fmaxf(red[0], red[1]), fmaxf(red[2], red[3]));
+    const int fail = redf[0] | redf[1] | redf[2] | redf[3];
+    named_bar_sync(1, 128);  // red is rewritten only after every warp has read it
+    if (fail) break;
+    const int e = tc::f16_scale_exponent(m4);
+    const float osc = ldexpf(1.f, e);
+    void* const* dst = last_term ? p.rp : p.tp[ph & 1];
+
+    for (int mt = 0; mt < MT; ++mt) {
+      if (last_phase) {
+        if (ok && !tc::mbar_wait(&acc_full[sl * 2 + mt], par, p.err, abort_flag)) ok = false;
+        if (!ok) continue;
+        tc::tc_fence_after();
+      }
+      const int row = mt * 128 + q * 32 + lane;
+      const bool rok = row < M;
+      const uint32_t tacc = taddr + (uint32_t(q * 32) << 16) + uint32_t(sl * 256 + mt * 2 * TBN);
+      const long off = wb + row;
+      c128* Sw = p.S + long(w) * p.ldS + long(row) * N;
+#pragma unroll 1
+      for (int c0 = 0; c0 < TBN; c0 += 16) {
+        float xr[16], xi[16];
+        values(tacc, c0, xr, xi);
+        if (c0 + 16 >= TBN) {
+          // the accumulator is free for this slot's next phase
+          tc::tc_fence_before();
+          tc::mbar_arrive(&acc_empty[sl * 2 + mt]);
+        }
+        if (!rok || c0 >= N) continue;
+        if (last_phase) {
+          // S = P1 R  (complex128 walker matrix [M][N])
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (c0 + j < N) Sw[c0 + j] = cmk(xr[j], xi[j]);
+          continue;
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          if (c0 + j < N) {
+            const long idx = off + long(c0 + j) * pl_ld;
+            float ur = xr[j], ui = xi[j];
+            if (taylor) {
+              ur += sum_r[idx];
+              ui += sum_i[idx];
+            }
+            if (last_term) {
+              split_store16(ur * osc, dst[0], dst[1], idx);
+              split_store16(ui * osc, dst[2], dst[3], idx);
+            } else {
+              sum_r[idx] = ur;
+              sum_i[idx] = ui;
+              split_store16(xr[j] * osc, dst[0], dst[1], idx);
+              split_store16(xi[j] * osc, dst[2], dst[3], idx);
+            }
+          }
+      }
+    }
+    if (last_phase) {
+      // the last phase has no pass 1: agree here on going on
+      if (lane == 0) redf[q] = ok ? 0 : 1;
+      named_bar_sync(1, 128);
+      const int fail2 = redf[0] | redf[1] | redf[2] | redf[3];
+      named_bar_sync(1, 128);
+      if (fail2) break;
+    } else {
+      // make this phase's planes visible to the TMA loads of the next phase
+      fence_proxy_async_global();
+      tc::mbar_arrive(&phase_done[sl]);
+      (sl ? pinv1 : pinv0) = ldexpf(1.f, -e);
+    }
+    ++(sl ? use1 : use0);
+    sc.advance(sl);
+  }
+}
+
+template <bool F16>
 __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_constant__ TyParams p) {
+  // 128 bytes of K per stage and operand row: 32 TF32 or 64 FP16 elements; 32 bytes per MMA
+  constexpr int TBKE = F16 ? 2 * TBK : TBK;
+  constexpr int KSTEP = F16 ? 16 : 8;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -104,11 +298,12 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
   uint64_t* phase_done = acc_empty + 4;   // [slot] epilogue -> TMA: the phase's term is written
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(phase_done + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  float* red = reinterpret_cast<float*>(tmem_slot + 2);  // [4] per-warp maxima (FP16 form)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nph = p.order + 2;
   const int M = p.M;
-  const int nk = (M + TBK - 1) / TBK;
+  const int nk = (M + TBKE - 1) / TBKE;
   const int MT = (M + 127) / 128;
 
   if (threadIdx.x == 0) {
@@ -166,7 +361,7 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
             // once per Taylor term: kept in L2 until its last term.
             const uint64_t pol = (ph == nph - 2) ? pol_first : pol_last;
             for (int q = 0; q < na; ++q)
-              tc::tma_load_3d_hint(st + q * T_A_TILE, &amap[q], &full[s], kc * TBK, mt * 128,
+              tc::tma_load_3d_hint(st + q * T_A_TILE, &amap[q], &full[s], kc * TBKE, mt * 128,
                                    p1 ? 0 : w, pol);
             if (!b_ready) {
               // B is the previous phase's term of this walker, written by the epilogue warps
@@ -178,7 +373,7 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
               b_ready = true;
             }
             for (int q = 0; q < 4; ++q)
-              tc::tma_load_3d(st + 4 * T_A_TILE + q * T_B_TILE, &bmap[q], &full[s], kc * TBK, 0,
+              tc::tma_load_3d(st + 4 * T_A_TILE + q * T_B_TILE, &bmap[q], &full[s], kc * TBKE, 0,
                               w);
           }
         sc.advance(sl);
@@ -186,8 +381,8 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      constexpr uint32_t ID = tc::idesc_tf32(128, TBN, false);
-      constexpr uint32_t IDN = tc::idesc_tf32(128, TBN, true);
+      constexpr uint32_t ID = tc::idesc_split<F16>(128, TBN, false);
+      constexpr uint32_t IDN = tc::idesc_split<F16>(128, TBN, true);
       Schedule sc(p.W, nph, blockIdx.x, gridDim.x, p.nslots);
       long it = 0;
       long use0 = 0, use1 = 0;  // accumulator uses of each slot
@@ -218,32 +413,32 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
             const uint32_t sa = tc::smem_u32(st);
             const uint32_t sb = tc::smem_u32(st + 4 * T_A_TILE);
 #pragma unroll
-            for (int kk = 0; kk < TBK / 8; ++kk) {
-              if (kc * TBK + kk * 8 >= M) break;  // zero fill past M
+            for (int kk = 0; kk < 4; ++kk) {
+              if (kc * TBKE + kk * KSTEP >= M) break;  // zero fill past M
               auto A = [&](int q) { return tc::sdesc_sw128(sa + q * T_A_TILE) + uint64_t(2 * kk); };
               auto B = [&](int q) { return tc::sdesc_sw128(sb + q * T_B_TILE) + uint64_t(2 * kk); };
               const uint32_t acc0 = (kc > 0 || kk > 0) ? 1u : 0u;
               if (p1) {
                 // real A (P1 hi, lo) x complex B
-                tc::mma_tf32(dr, A(0), B(0), ID, acc0);
-                tc::mma_tf32(dr, A(0), B(1), ID, 1);
-                tc::mma_tf32(dr, A(1), B(0), ID, 1);
-                tc::mma_tf32(di, A(0), B(2), ID, acc0);
-                tc::mma_tf32(di, A(0), B(3), ID, 1);
-                tc::mma_tf32(di, A(1), B(2), ID, 1);
+                tc::mma_split<F16>(dr, A(0), B(0), ID, acc0);
+                tc::mma_split<F16>(dr, A(0), B(1), ID, 1);
+                tc::mma_split<F16>(dr, A(1), B(0), ID, 1);
+                tc::mma_split<F16>(di, A(0), B(2), ID, acc0);
+                tc::mma_split<F16>(di, A(0), B(3), ID, 1);
+                tc::mma_split<F16>(di, A(1), B(2), ID, 1);
               } else {
-                tc::mma_tf32(dr, A(0), B(0), ID, acc0);
-                tc::mma_tf32(dr, A(0), B(1), ID, 1);
-                tc::mma_tf32(dr, A(1), B(0), ID, 1);
-                tc::mma_tf32(dr, A(2), B(2), IDN, 1);
-                tc::mma_tf32(dr, A(2), B(3), IDN, 1);
-                tc::mma_tf32(dr, A(3), B(2), IDN, 1);
-                tc::mma_tf32(di, A(0), B(2), ID, acc0);
-                tc::mma_tf32(di, A(0), B(3), ID, 1);
-                tc::mma_tf32(di, A(1), B(2), ID, 1);
-                tc::mma_tf32(di, A(2), B(0), ID, 1);
-                tc::mma_tf32(di, A(2), B(1), ID, 1);
-                tc::mma_tf32(di, A(3), B(0), ID, 1);
+                tc::mma_split<F16>(dr, A(0), B(0), ID, acc0);
+                tc::mma_split<F16>(dr, A(0), B(1), ID, 1);
+                tc::mma_split<F16>(dr, A(1), B(0), ID, 1);
+                tc::mma_split<F16>(dr, A(2), B(2), IDN, 1);
+                tc::mma_split<F16>(dr, A(2), B(3), IDN, 1);
+                tc::mma_split<F16>(dr, A(3), B(2), IDN, 1);
+                tc::mma_split<F16>(di, A(0), B(2), ID, acc0);
+                tc::mma_split<F16>(di, A(0), B(3), ID, 1);
+                tc::mma_split<F16>(di, A(1), B(2), ID, 1);
+                tc::mma_split<F16>(di, A(2), B(0), ID, 1);
+                tc::mma_split<F16>(di, A(2), B(1), ID, 1);
+                tc::mma_split<F16>(di, A(3), B(0), ID, 1);
               }
             }
             tc::mma_commit(&empty[s]);
@@ -255,6 +450,8 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
         sc.advance(sl);
       }
     }
+  } else if constexpr (F16) {
+    taylor_epilogue_f16(p, taddr, acc_full, acc_empty, phase_done, abort_flag, red, warp, lane);
   } else {
     // epilogue warps: TMEM lane quarter q = warp % 4, one accumulator row per thread
     const int q = warp & 3;
@@ -273,14 +470,11 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
       const bool last_term = (ph == nph - 2);
       const float ai = taylor ? 1.0f / float(ph) : 0.0f;
       // destination planes of this phase: the next B operand (T_ph, or R after the last term)
-      float *__restrict__ d0, *__restrict__ d1, *__restrict__ d2, *__restrict__ d3;
-      if (last_term) {
-        d0 = p.rp[0]; d1 = p.rp[1]; d2 = p.rp[2]; d3 = p.rp[3];
-      } else if (ph & 1) {
-        d0 = p.tp[1][0]; d1 = p.tp[1][1]; d2 = p.tp[1][2]; d3 = p.tp[1][3];
-      } else {
-        d0 = p.tp[0][0]; d1 = p.tp[0][1]; d2 = p.tp[0][2]; d3 = p.tp[0][3];
-      }
+      void* const* dst = last_term ? p.rp : p.tp[ph & 1];
+      float* __restrict__ const d0 = static_cast<float*>(dst[0]);
+      float* __restrict__ const d1 = static_cast<float*>(dst[1]);
+      float* __restrict__ const d2 = static_cast<float*>(dst[2]);
+      float* __restrict__ const d3 = static_cast<float*>(dst[3]);
       const long wb = long(w) * p.pl_bs;
       for (int mt = 0; mt < MT; ++mt) {
         if (!tc::mbar_wait(&acc_full[sl * 2 + mt], unsigned(sl ? use1 : use0) & 1u, p.err,
@@ -378,16 +572,25 @@ int g_nsm = 0;
 
 }  // namespace
 
-int make_plane_map_3d(CUtensorMap* map, const float* base, long k, long rows, long row_stride,
-                      long batch, long batch_stride, int box_rows, int box_batch);
+int make_plane_map_3d_es(CUtensorMap* map, const void* base, int esize, long k, long rows,
+                         long row_stride, long batch, long batch_stride, int box_rows,
+                         int box_batch);
 
-int taylor_fused_tc(cudaStream_t s, const float* const P1p[2], const float* const Vp[4],
-                    long ldV, const float* const Sp[4], float* const Tp0[4], float* const Tp1[4],
-                    float* const Rp[4], float* const sum[2], long pl_ld, c128* S, long ldS, int W,
-                    int M, int N, int order, int nslots, unsigned* err) {
+// Planes: FP32 (esize 4, TF32 split) or FP16 (esize 2, FP16 split; then v_inv, s_inv [W] and
+// p1_inv give the operands' inverse scales).
+int taylor_fused_tc(cudaStream_t s, int esize, const void* const P1p[2], const void* const Vp[4],
+                    long ldV, const void* const Sp[4], void* const Tp0[4], void* const Tp1[4],
+                    void* const Rp[4], float* const sum[2], long pl_ld, c128* S, long ldS, int W,
+                    int M, int N, int order, int nslots, const float* v_inv, const float* s_inv,
+                    float p1_inv, unsigned* err) {
   if (M > 256 || N > TBN || order < 0) {
     set_error_detail("taylor_fused_tc: M = %d (<= 256), N = %d (<= 64), order = %d", M, N, order);
     return AFQMC_ERR_UNSUPPORTED;
+  }
+  const bool f16 = esize == 2;
+  if (f16 && (!v_inv || !s_inv)) {
+    set_error_detail("taylor_fused_tc: FP16 planes without their scales");
+    return AFQMC_ERR_ARG;
   }
   if (g_nsm == 0) {
     int dev = 0;
@@ -396,13 +599,18 @@ int taylor_fused_tc(cudaStream_t s, const float* const P1p[2], const float* cons
   }
   TyParams p{};
   for (int q = 0; q < 2; ++q)
-    AFQMC_TRY(make_plane_map_3d(&p.p1[q], P1p[q], M, M, pl_ld, 1, long(M) * pl_ld, 128, 1));
+    AFQMC_TRY(make_plane_map_3d_es(&p.p1[q], P1p[q], esize, M, M, pl_ld, 1, long(M) * pl_ld, 128,
+                                   1));
   for (int q = 0; q < 4; ++q) {
-    AFQMC_TRY(make_plane_map_3d(&p.v[q], Vp[q], M, M, ldV, W, long(M) * ldV, 128, 1));
-    AFQMC_TRY(make_plane_map_3d(&p.s[q], Sp[q], M, N, pl_ld, W, long(N) * pl_ld, TBN, 1));
-    AFQMC_TRY(make_plane_map_3d(&p.t[0][q], Tp0[q], M, N, pl_ld, W, long(N) * pl_ld, TBN, 1));
-    AFQMC_TRY(make_plane_map_3d(&p.t[1][q], Tp1[q], M, N, pl_ld, W, long(N) * pl_ld, TBN, 1));
-    AFQMC_TRY(make_plane_map_3d(&p.r[q], Rp[q], M, N, pl_ld, W, long(N) * pl_ld, TBN, 1));
+    AFQMC_TRY(make_plane_map_3d_es(&p.v[q], Vp[q], esize, M, M, ldV, W, long(M) * ldV, 128, 1));
+    AFQMC_TRY(make_plane_map_3d_es(&p.s[q], Sp[q], esize, M, N, pl_ld, W, long(N) * pl_ld, TBN,
+                                   1));
+    AFQMC_TRY(make_plane_map_3d_es(&p.t[0][q], Tp0[q], esize, M, N, pl_ld, W, long(N) * pl_ld,
+                                   TBN, 1));
+    AFQMC_TRY(make_plane_map_3d_es(&p.t[1][q], Tp1[q], esize, M, N, pl_ld, W, long(N) * pl_ld,
+                                   TBN, 1));
+    AFQMC_TRY(make_plane_map_3d_es(&p.r[q], Rp[q], esize, M, N, pl_ld, W, long(N) * pl_ld, TBN,
+                                   1));
     p.tp[0][q] = Tp0[q];
     p.tp[1][q] = Tp1[q];
     p.rp[q] = Rp[q];
@@ -417,14 +625,18 @@ int taylor_fused_tc(cudaStream_t s, const float* const P1p[2], const float* cons
   p.M = M;
   p.N = N;
   p.order = order;
+  p.v_inv = v_inv;
+  p.s_inv = s_inv;
+  p.p1_inv = p1_inv;
   p.err = err;
-  AFQMC_CUDA_TRY(cudaFuncSetAttribute(taylor_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  auto kern = f16 ? taylor_tc_kernel<true> : taylor_tc_kernel<false>;
+  AFQMC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(T_SMEM)));
   // nslots = 0: two walkers in flight per CTA once every CTA has two, else one
   if (nslots <= 0) nslots = (W >= 2 * g_nsm) ? 2 : 1;
   p.nslots = nslots > 1 ? 2 : 1;
   const int grid = W < g_nsm ? W : g_nsm;
-  taylor_tc_kernel<<<grid, TY_THREADS, T_SMEM, s>>>(p);
+  kern<<<grid, TY_THREADS, T_SMEM, s>>>(p);
   return launch_status("taylor_tc_kernel");
 }
 

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_fp16.h>
 #include <stdint.h>
 
 #include "common.cuh"
@@ -51,16 +52,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   return ok != 0;
 }
 
-// Wait for the phase with the given parity; gives up after kWaitCycles, sets *err and returns
-// false.  `abort` lets a role stop waiting once another role has reported a failure.
+// Wait for the phase with the given parity; gives up after `budget` cycles (kWaitCycles unless a
+// caller passes less), sets *err and returns false.  `abort` lets a role stop waiting once
+// another role has reported a failure.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned* err,
-                                          volatile int* abort) {
+                                          volatile int* abort, long long budget = kWaitCycles) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
     if (abort && *abort) return false;
-    if (clock64() - t0 > kWaitCycles) {
+    if (clock64() - t0 > budget) {
       if (err) atomicOr(err, kTimeoutFlag);
       if (abort) *abort = 1;
       return false;
@@ -158,6 +160,38 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t adesc, uint64
       : "memory");
 }
 
+// Instruction descriptor: kind::f16, D = F32, A = B = F16, K-major, M x N, optional A negate.
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N, bool neg_a) {
+  return (1u << 4) | (0u << 7) | (0u << 10) | (neg_a ? (1u << 13) : 0u) |
+         (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                        uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// one MMA of the split arithmetic in either operand format (same shapes, same descriptors: a
+// K step is 32 bytes of the 128-byte swizzle row in both, 8 TF32 or 16 FP16 elements)
+template <bool F16>
+__device__ __forceinline__ void mma_split(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+  if constexpr (F16)
+    mma_f16(d_tmem, adesc, bdesc, idesc, accumulate);
+  else
+    mma_tf32(d_tmem, adesc, bdesc, idesc, accumulate);
+}
+
+template <bool F16>
+__host__ __device__ constexpr uint32_t idesc_split(int M, int N, bool neg_a) {
+  return F16 ? idesc_f16(M, N, neg_a) : idesc_tf32(M, N, neg_a);
+}
+
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                    smem_u32(bar))
@@ -182,7 +216,10 @@ __device__ __forceinline__ void tmem_ld_wait() {
 }
 
 // TF32 split: x = hi + lo with hi = x rounded to TF32 (10-bit mantissa, round to nearest) and
-// lo = x - hi (exact in FP32); the tensor core reads the 19 most significant bits of each.
+// lo = (x - hi) rounded to TF32 as well.  The tensor core reads only the 19 most significant bits
+// of an FP32 operand, dropping the rest: an unrounded lo would be truncated toward zero there,
+// which biases every product toward smaller magnitudes.  Rounded, both terms carry unbiased
+// errors and hi + lo keeps 22 significant bits of x.
 __host__ __device__ __forceinline__ float tf32_hi(float x) {
   uint32_t u;
   memcpy(&u, &x, 4);
@@ -193,6 +230,27 @@ __host__ __device__ __forceinline__ float tf32_hi(float x) {
   float r;
   memcpy(&r, &u, 4);
   return r;
+}
+
+__host__ __device__ __forceinline__ void tf32_split(float x, float& hi, float& lo) {
+  hi = tf32_hi(x);
+  lo = tf32_hi(x - hi);
+}
+
+// FP16 split of a value already scaled into the FP16 range (|x| < 2^15): x = hi + lo with
+// hi = FP16(x) and lo = FP16(x - hi), 22 significant bits like the TF32 split; the tensor core
+// multiplies FP16 values exactly and accumulates in FP32.
+__device__ __forceinline__ void f16_split(float x, __half& hi, __half& lo) {
+  hi = __float2half_rn(x);
+  lo = __float2half_rn(x - __half2float(hi));
+}
+
+// 2^e with |x| * 2^e in [2^13, 2^14) for the largest |x| of a row or tensor (1 for zero)
+__host__ __device__ inline int f16_scale_exponent(float amax) {
+  if (!(amax > 0.f)) return 0;
+  int e;
+  frexpf(amax, &e);  // amax = f * 2^e, f in [0.5, 1)
+  return 14 - e;
 }
 
 }  // namespace tc

@@ -275,6 +275,7 @@ int zgemm(cudaStream_t s, int batch, GemmTrans ta, bool a_real, GemmTrans tb, bo
   AFQMC_GEMM_CASE(true, true, false, false, false, false)    // A^H * B
   AFQMC_GEMM_CASE(false, false, true, true, false, true)     // real A * real B^T
   AFQMC_GEMM_CASE(false, false, false, false, true, false)   // A * conj(B)
+  AFQMC_GEMM_CASE(false, false, false, true, true, false)    // A * B^H
 #undef AFQMC_GEMM_CASE
   set_error_detail("zgemm: operand combination (ta=%d a_real=%d tb=%d b_real=%d) not instantiated",
                    int(ta), int(a_real), int(tb), int(b_real));

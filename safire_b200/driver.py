@@ -222,8 +222,9 @@ class Simulation:
         flags = 0
         if self.reuse_density:
             flags = A.capi.STEP_KEEP_G | (A.capi.STEP_G_READY if self._g_ready else 0)
-        if self.use_graph and uniforms is None and step > 0:
-            # device fields: replay the captured step (captured on first use, after step 0)
+        if self.use_graph and uniforms is None and (step > 0 or self.graph is not None):
+            # device fields: replay the captured step (captured on first use, after the first
+            # eager step has allocated every buffer; a restart keeps the captured graphs)
             if self.graph is None:
                 self.graph = StepGraph(self.prop, self.wset, self._eshift_dev)
             self.graph.replay(flags)

@@ -76,14 +76,26 @@ class WalkerRows:
 
 
 def _p2p(ops):
-    """Posts point-to-point ops in order and waits for all of them."""
+    """Posts point-to-point ops in order and waits for all of them.  Under a backend without
+    device point-to-point (gloo) device tensors are staged through host memory: a send copies
+    the packed rows to the host, a receive lands in a host buffer copied to the device after."""
     if not ops:
         return
-    reqs = []
+    stage = dist.get_backend() != "nccl"
+    reqs, landed = [], []
     for op, t, peer in ops:
-        reqs.append((dist.isend if op == "send" else dist.irecv)(t, peer))
+        buf = t
+        if stage and t.is_cuda:
+            if op == "send":
+                buf = t.cpu()
+            else:
+                buf = torch.empty(t.shape, dtype=t.dtype)
+                landed.append((t, buf))
+        reqs.append((dist.isend if op == "send" else dist.irecv)(buf, peer))
     for r in reqs:
         r.wait()
+    for t, buf in landed:
+        t.copy_(buf)
 
 
 def exchange_walkers(rows, offspring, counts, rank):

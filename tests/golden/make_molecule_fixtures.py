@@ -7,7 +7,8 @@ their error bars, the run settings, and the BH RHF mixed-estimator and back-prop
 density matrices) and tests/golden/molecule_snapshots.json (the seeded single-rank snapshots:
 energies and density matrices of short runs that a restatement with the same random streams
 reproduces to rounding).  Run from the repository
-root with the reference checked out at REFERENCE (default /root/reference):
+root with the reference checked out at REFERENCE (the argument, else the SAFIRE_REFERENCE
+environment variable):
 
     python tests/golden/make_molecule_fixtures.py [REFERENCE]
 """
@@ -22,7 +23,7 @@ sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), ".."
 from safire_b200 import inputs as I  # noqa: E402
 from safire_b200.h5 import File  # noqa: E402
 
-REF = "/root/reference"
+REF = os.environ.get("SAFIRE_REFERENCE", "")
 INP = os.path.join(REF, "tests/functional/afqmc_inputs")
 STAT = os.path.join(REF, "tests/functional/statistical_references")
 OUT = os.path.dirname(os.path.abspath(__file__))
@@ -123,6 +124,8 @@ def main():
         REF_ROOT[0] = sys.argv[1]
         INP = os.path.join(sys.argv[1], "tests/functional/afqmc_inputs")
         STAT = os.path.join(sys.argv[1], "tests/functional/statistical_references")
+    if not REF_ROOT[0] or not os.path.isdir(INP):
+        sys.exit("give the reference checkout as the argument or in SAFIRE_REFERENCE")
     arrays = {}
     for key, rel in HAMS.items():
         h = I.read_hamiltonian(os.path.join(INP, rel))

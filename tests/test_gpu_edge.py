@@ -6,7 +6,7 @@ import pytest
 import torch
 
 from oracle import afqmc as O
-from safire_b200.synth import make_hamiltonian
+from safire_b200.synth import make_hamiltonian, make_workload
 from tests.gpu_helpers import rel_err, to_dev, to_host
 
 pytestmark = pytest.mark.gpu
@@ -72,3 +72,30 @@ def test_empty_spin_sector_steps_vs_oracle(cuda):
     prop.Orthogonalize(wset)
     oprop.orthogonalize(ows)
     assert rel_err(to_host(wset.SlaterMatrices(0)), ows.SA) < 1e-10
+
+
+def test_bounded_wait_times_out(cuda):
+    """A bounded device wait that nothing completes gives up after its budget (about 0.05 s
+    here), reports AFQMC_ERR_TIMEOUT and sets bit 0 of the Hamiltonian's error word, and the
+    context stays usable: a mixed-precision contraction right after it runs and matches the
+    oracle, and clearing the word leaves it at zero."""
+    from safire_b200 import afqmc as A
+    from safire_b200 import capi
+    from tests.gpu_helpers import make_pair, rand_c
+
+    wl = make_workload("cfg1", W=16)
+    dham, oham, _ = make_pair(wl)
+    dham.clear_device_error()
+    assert dham.device_error_flag() == 0
+    with pytest.raises(capi.AfqmcError) as ei:
+        dham.wait_selftest(100_000_000)
+    assert ei.value.status == capi.ERR_TIMEOUT
+    assert dham.device_error_flag() & 1
+    dham.clear_device_error()
+    assert dham.device_error_flag() == 0
+    rs = np.random.default_rng(9)
+    G = rand_c(rs, wl.W, wl.nup * wl.M, scale=0.3)
+    v = torch.zeros((wl.W, wl.Nc), dtype=torch.complex128, device="cuda")
+    dham.vbias(to_dev(G), v, wl.dt, precision=A.PREC_MIXED)
+    assert rel_err(to_host(v), oham.vbias(G, wl.dt)) < 2e-5
+    assert dham.device_error_flag() == 0

@@ -137,9 +137,10 @@ def test_exchange_single_tf32_error(cuda):
     dham.set_exchange_split(3)
 
 
-def _mixed_steps(wl, dham, fused, nsteps=2, order=None):
+def _mixed_steps(wl, dham, fused, nsteps=2, order=None, split_format=1):
     from safire_b200 import afqmc as A
     W = wl.W
+    dham.set_split_format(split_format)
     dham.set_taylor_fused(fused)
     ws = A.WalkerSet(wl.walker_type, wl.M, wl.nup, wl.ndn, W)
     ws.init_from_trial(dham)
@@ -151,6 +152,7 @@ def _mixed_steps(wl, dham, fused, nsteps=2, order=None):
         prop.Propagate(ws, -30.0, ud)
     torch.cuda.synchronize()
     dham.set_taylor_fused(1)
+    dham.set_split_format(0)
     return to_host(ws.SlaterMatrices(0)), to_host(ws.properties())
 
 
@@ -159,8 +161,10 @@ def _mixed_steps(wl, dham, fused, nsteps=2, order=None):
                                              ("cfg2", 6, 40, None), ("cfg1", 301, None, 3)])
 def test_taylor_fused_vs_per_term(cuda, name, W, Nc, order, mode):
     """The persistent Taylor kernel (all products of a walker in one CTA; mode 2 / 3: one / two
-    walkers in flight per CTA) against one GEMM launch per product: same split arithmetic,
-    different kernels; W = 300, 301 run several walkers per CTA (301: one slot ends early)."""
+    walkers in flight per CTA) against one GEMM launch per product: same split arithmetic (the
+    TF32 split, which both run), different kernels; W = 300, 301 run several walkers per CTA
+    (301: one slot ends early).  The FP16 split of the fused kernel is checked against complex128
+    in test_gpu_mixed_full.py and below."""
     kw = {"W": W} if Nc is None else {"W": W, "Nc": Nc}
     wl = make_workload(name, **kw)
     dham, _, _ = make_pair(wl)
@@ -200,3 +204,33 @@ def test_autotune_leaves_the_run_unchanged(cuda):
         sim.step()
         runs.append(sim.wset.buffer.clone())
     assert torch.equal(runs[0], runs[1])
+
+
+@pytest.mark.parametrize("mode", [2, 3])
+@pytest.mark.parametrize("name,W,Nc,order", [("cfg1", 300, None, None), ("cfg1", 20, None, 0),
+                                             ("cfg1", 301, None, 3)])
+def test_taylor_fused_fp16_vs_fp64(cuda, name, W, Nc, order, mode):
+    """The persistent Taylor kernel in the FP16 split (operands and every term scaled by powers of
+    two) against complex128 propagation on the same walkers and fields: walkers within the
+    one-step bound of the mixed path (1e-4), log-overlaps within 1e-3 (the log-det sums the
+    walkers' error over the electrons)."""
+    from safire_b200 import afqmc as A
+    kw = {"W": W} if Nc is None else {"W": W, "Nc": Nc}
+    wl = make_workload(name, **kw)
+    dham, _, _ = make_pair(wl)
+    Sf, pf = _mixed_steps(wl, dham, mode, order=order, split_format=2)
+    ws = A.WalkerSet(wl.walker_type, wl.M, wl.nup, wl.ndn, W)
+    ws.init_from_trial(dham)
+    kwp = {} if order is None else {"taylor_n": order}
+    prop = A.Propagator(dham, A.default_params(dt=wl.dt, **kwp), W)
+    u = O.HostRandomGenerator(O.split_seed(0, 0, 7)).sample_uniform(W * wl.Nc)
+    ud = to_dev(u.reshape(W, wl.Nc), torch.float64)
+    for _ in range(2):
+        prop.Propagate(ws, -30.0, ud)
+    S64, p64 = to_host(ws.SlaterMatrices(0)), to_host(ws.properties())
+    eS = rel_err(Sf, S64)
+    eO = float(np.max(np.abs(pf[:, O.OVLP] - p64[:, O.OVLP])))
+    print(f"fused FP16 ({mode}) vs complex128 ({name}, W={W}, order={order}): S {eS:.2e} "
+          f"log-ovlp {eO:.2e}")
+    assert eS < TOL_STEP and eO < 1e-3
+    assert dham.device_error_flag() == 0
