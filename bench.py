@@ -72,9 +72,12 @@ def parse():
     ap.add_argument("--no-graph", action="store_true",
                     help="launch every kernel of a step eagerly instead of replaying the step's "
                          "CUDA graph")
-    ap.add_argument("--taylor-mode", type=int, default=1, choices=[0, 1, 2, 3],
-                    help="mixed Taylor propagation: 0 per-term GEMMs, 1 fused (auto), 2 / 3 fused "
-                         "with one / two walkers in flight per CTA")
+    ap.add_argument("--taylor-mode", type=int, default=1, choices=list(range(8)),
+                    help="mixed Taylor propagation (afqmc_ham_set_taylor_fused): 1 the library's "
+                         "autotuner picks between 2 and 4; 0 per-term GEMMs; fused: 2 / 3 TF32 "
+                         "split with one / two walkers in flight per CTA, 4 / 5 the same in the "
+                         "FP16 split, 6 / 7 one walker in flight with the running sum in tensor "
+                         "memory")
     ap.add_argument("--profile-case", default=None,
                     choices=["step", "taylor", "vhs", "exchange", "phmsd-energy"],
                     help="run one small case for an ncu capture instead of the bench: the "
@@ -485,7 +488,7 @@ def _roofline(sim, wl, W, prec, phases, args, torch, taylor_mode=1):
         # the FP16 split runs vbias, vHS, the exchange and (fused) the Taylor series when the
         # shapes allow it (afqmc_ham_set_split_format)
         f16 = sim.ham.set_split_format(0)
-        f16_top = f16 and (top != "propagate" or taylor_mode != 0)
+        f16_top = f16 and (top != "propagate" or taylor_mode in (4, 5, 7))
         peaks = measured_peaks()
         if f16_top and peaks.get("bf16_tflops"):
             peak = float(peaks["bf16_tflops"])
@@ -541,6 +544,15 @@ def _EXCHANGE_TRAFFIC(W, Nc, N, M):
             "launch), by the tile-order model at other walker counts")
 
 
+def _mixed_dtype(split_f16, taylor_mode, exchange_split):
+    """Arithmetic of the mixed line: complex128 plus 3-product split contractions (22-bit
+    operands, FP32 accumulation) in FP16 or TF32 terms."""
+    fmt = "fp16" if split_f16 else "tf32"
+    tay = "fp16" if (split_f16 and taylor_mode in (4, 5, 7)) else "tf32"
+    ex = fmt if exchange_split == 3 else fmt + " single product"
+    return f"c128 + split x3 (vbias/vHS {fmt}, taylor {tay}, exchange {ex})"
+
+
 def _init_dist():
     import torch
     import torch.distributed as dist
@@ -576,6 +588,7 @@ def run_ours(args):
     sim.use_graph = not args.no_graph
     if prec == A.PREC_MIXED and args.exchange_split != 3:
         sim.ham.set_exchange_split(args.exchange_split)
+    split_f16 = bool(sim.ham.set_split_format(0)) if prec == A.PREC_MIXED else False
     tuned = None
     if prec == A.PREC_MIXED and args.taylor_mode != 1:
         sim.ham.set_taylor_fused(args.taylor_mode)
@@ -622,8 +635,9 @@ def run_ours(args):
             "metric": metric_name(), "value": value, "unit": "walker-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "c128" if prec == A.PREC_FP64 else
-                     ("c128+tf32x3" if args.exchange_split == 3 else "c128+tf32x3 (exchange tf32)"),
+            "dtype": "c128" if prec == A.PREC_FP64 else _mixed_dtype(
+                split_f16, tuned["taylor_mode"] if tuned else args.taylor_mode,
+                args.exchange_split),
             "data": "synthetic",
             "config": {"workload": "M=200 N=50+50 Nc=1600 W=1024/GPU dt=0.005 taylor=6, "
                                    "block of 10 steps (ortho/5, comb/10, energy/10)",
@@ -794,7 +808,9 @@ def run_control_variate(args):
 
 def run_phmsd(args):
     """The multi-determinant workload: COLLINEAR M=120, N=30+30, Nc=960, reference + 4095
-    particle-hole determinants, 512 walkers per GPU; FP64 (the PHMSD kernels run in complex128)."""
+    particle-hole determinants, 512 walkers per GPU.  --precision mixed: vHS and the Taylor
+    series on the tensor cores (split precision) and the excited-determinant energy tables in
+    complex64; the trial's density matrix, vbias, overlaps and every sum stay complex128."""
     import torch
     import torch.distributed as dist
 
@@ -806,7 +822,8 @@ def run_phmsd(args):
     W = args.walkers if args.walkers != 1024 else 512
     wl, trial = make_phmsd_workload(W=W)
     rp = RunParams(equilibration_steps=0, seed=0)
-    sim = Simulation.from_workload(wl, W=W, rp=rp, trial=trial)
+    prec = A.PREC_MIXED if args.precision == "mixed" else A.PREC_FP64
+    sim = Simulation.from_workload(wl, W=W, rp=rp, trial=trial, precision=prec)
     sim.use_graph = False
     t_ms, launches, nseg, clk = _timed_blocks(sim, args.steps, args.warmup, world, local,
                                               ClockSampler(local))
@@ -832,19 +849,20 @@ def run_phmsd(args):
                 "bound": "fp64", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
                 "frac": achieved / fp64, "traffic": None, "flops_per_launch": flops,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"}
-    e2e = None if args.no_e2e else _e2e(sim, W, wl.Nc, args.steps, args.warmup, world,
-                                        A.PREC_FP64)
+    e2e = None if args.no_e2e else _e2e(sim, W, wl.Nc, args.steps, args.warmup, world, prec)
     if rank == 0:
         line = {
             "metric": "walker-steps/s, PHMSD trial (M=120, 30+30 electrons, 4096 determinants, "
                       "512 walkers) on B200",
             "value": value, "unit": "walker-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128" if prec == A.PREC_FP64 else
+                     "c128 + split x3 (vHS, taylor) + c64 energy tables", "data": "synthetic",
             "config": {"workload": f"PHMSD M=120 N=30+30 Nc=960 W={W}/GPU dt=0.005 taylor=6, "
                                    "reference + 4095 determinants (20 occ / 40 virt window), "
                                    "block of 10 steps (ortho/5, comb/10, energy/10)",
-                       "precision": "fp64", "global_walkers": W * world,
+                       "precision": args.precision, "global_walkers": W * world,
                        "parallelism": f"walker dp{world}"},
             "roofline": roofline, "cpu_baseline": None, "e2e": e2e,
             "gpu_launches": launches, "clocks": clk, "phases_ms": phases,

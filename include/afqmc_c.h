@@ -200,10 +200,16 @@ int afqmc_ham_set_vhs_symmetry(afqmc_ham ham, int enable, int* active);
 #define AFQMC_SPLIT_FP16 2
 int afqmc_ham_set_split_format(afqmc_ham ham, int format, int* active_f16);
 
-/* Mixed-precision Taylor propagation: 1 (default) runs all order + 2 products of each walker in
- * one persistent tensor-core kernel (M <= 256 orbitals, N <= 64 electrons per spin), with one or
- * two walkers in flight per CTA chosen by the walker count; 2 / 3 force one / two walkers in
- * flight; 0 launches one batched GEMM per product.  All compute the same sums. */
+/* Mixed-precision Taylor propagation.  0 launches one batched GEMM per product; the others run
+ * all order + 2 products of each walker in one persistent tensor-core kernel (M <= 256 orbitals,
+ * N <= 64 electrons per spin): 2 / 3 in the TF32 split with one / two walkers in flight per CTA,
+ * 4 / 5 the same in the FP16 split (afqmc_ham_set_split_format; every Taylor term stored with its
+ * own power-of-two scale), 6 / 7 (TF32 / FP16) one walker in flight with the running sum in
+ * tensor memory.  With one walker in flight (2, 4) the small split products (hi*lo, lo*hi) get
+ * their own FP32 accumulator, added to the main one (hi*hi) in the epilogue: the tensor core's
+ * FP32 accumulation truncates toward zero at every update, and a third of the updates in the
+ * main accumulator shrinks that bias threefold.  1 (and the default) is 2.  All compute the
+ * same sums. */
 int afqmc_ham_set_taylor_fused(afqmc_ham ham, int fused);
 /* Which operations a mixed-precision call runs on the TF32 tensor cores (the rest in complex128):
  * AFQMC_MIXED_VBIAS the step's vbias, AFQMC_MIXED_PROPAGATION its vHS and Taylor propagation,
@@ -336,7 +342,9 @@ int afqmc_prop_destroy(afqmc_prop prop);
 /* Runs the propagator's steps with a multi-determinant trial (AFQMCBasePropagator over a
  * PHMSD wavefunction, Wavefunction.hpp's variant): vbias from afqmc_phmsd_density_matrix and
  * afqmc_phmsd_vbias, overlaps (step and orthogonalisation) from afqmc_phmsd_log_overlap.  Needs
- * COLLINEAR walkers, FP64 precision and a trial whose Hamiltonian has been set.  vMF (host [Nc],
+ * COLLINEAR walkers and a trial whose Hamiltonian has been set.  With AFQMC_PREC_MIXED the vHS
+ * and the Taylor propagation of both spin blocks run on the tensor cores (split precision; the
+ * trial's vbias and overlaps stay complex128).  vMF (host [Nc],
  * may be NULL) replaces the mean field and regenerates P1 (generateP1 with the trial's vMF,
  * PHMSD.cpp:1329-1572, computed by the caller).  trial NULL detaches.  Synchronous.  The trial
  * must outlive its use by the propagator. */
@@ -376,10 +384,12 @@ int afqmc_prop_step_dev(afqmc_prop prop, afqmc_wset ws, const double* Eshift_dev
 int afqmc_prop_step_flags(afqmc_prop prop, afqmc_wset ws, const double* Eshift_dev,
                           const double* uniforms, int flags, afqmc_stream stream);
 /* Autotuner: times the mixed-precision step on these walkers with each Taylor propagation
- * variant (0 per-term GEMMs, 2 fused with one walker per CTA in flight, 3 fused with two) and keeps
- * the fastest for the Hamiltonian; walkers, field counter and bound statistics are restored, so
- * the run continues as if it had not been called.  *best = chosen mode (-1: FP64 or PHMSD,
- * nothing to tune); ms [3] (may be NULL) = the step time of each variant.  Synchronous. */
+ * variant of afqmc_ham_set_taylor_fused (0, 2, 3, 4, 5, 6, 7) and keeps for the Hamiltonian the
+ * faster of the two with separate accumulators for the small split products (2, 4); walkers,
+ * field counter and bound statistics are restored, so the run continues as if it had not been
+ * called.  *best = chosen mode (-1: FP64 or PHMSD,
+ * nothing to tune); ms [7] (may be NULL) = the step time of variants 0, 2, 3, 4, 5, 6, 7 (0 for
+ * a variant not tried: 4, 5 and 7 need the FP16 split).  Synchronous. */
 int afqmc_prop_autotune(afqmc_prop prop, afqmc_wset ws, int* best, float* ms,
                         afqmc_stream stream);
 /* AFQMCBasePropagator::Orthogonalize (cpp:735-741): QR re-orthonormalisation then OVLP refresh. */
@@ -473,6 +483,11 @@ int afqmc_phmsd_excitations(int nact, int nel, const int* refc, int ndet, const 
                             int* det_index, double* sign, int* nuniq, int* nex, int* exc);
 /* dims[6] = {M, nup, ndn, nact_up, nact_dn, Nc (0 before afqmc_phmsd_set_hamiltonian)} */
 int afqmc_phmsd_info(afqmc_phmsd trial, int* dims);
+/* Arithmetic of afqmc_phmsd_energy's excited-determinant 2-body terms: AFQMC_PREC_FP64 (default)
+ * complex128 per-(walker, Cholesky vector) tables and per-determinant sums; AFQMC_PREC_MIXED
+ * the same in complex64 (half the shared memory, the FP32 rate), the sums over determinants, the
+ * reference determinant's terms and every output in complex128. */
+int afqmc_phmsd_set_precision(afqmc_phmsd trial, int precision);
 
 /* The Real3IndexFactorization tensors of a PHMSD trial: Likn [nspin_H2][M][M][Nc] (real) and
  * hij [nspin_H1][M][M] on the host, half-rotated on the device with the active orbitals

@@ -50,7 +50,7 @@ def run(precision, steps, walkers, equil, seed, exchange_split=3, workload="cfg2
 
 
 def lockstep(steps, walkers, equil, seed, workload, lscale, exchange_split=3, mixed_ops=7,
-             restart_every=0, measure_every=10, split_format=0):
+             restart_every=0, measure_every=10, split_format=0, taylor_mode=1):
     """Correlated sampling: the complex128 and the mixed run advance side by side with the same
     fields, the same Eshift and the same population-control decisions (the comb of the complex128
     run's weights applied to both walker sets), so the paired energies differ only through the
@@ -74,6 +74,8 @@ def lockstep(steps, walkers, equil, seed, workload, lscale, exchange_split=3, mi
             sim.ham.set_mixed_ops(mixed_ops)
         if prec == A.PREC_MIXED and split_format:
             sim.ham.set_split_format(split_format)
+        if prec == A.PREC_MIXED and taylor_mode != 1:
+            sim.ham.set_taylor_fused(taylor_mode)
         sims.append(sim)
     s64, smx = sims
     rng = A.HostRandomGenerator(A.split_seed(seed, 0, 0))
@@ -139,20 +141,23 @@ def main(argv=None):
                     help="lockstep: steps between measurements")
     ap.add_argument("--split-format", type=int, default=0, choices=[0, 1, 2],
                     help="lockstep: operand format of the mixed split (0 auto, 1 TF32, 2 FP16)")
+    ap.add_argument("--taylor-mode", default="1",
+                    help="lockstep: comma-separated Taylor propagation modes of the mixed run "
+                         "(afqmc_ham_set_taylor_fused; 1 the default)")
     ap.add_argument("--mixed-ops", default="7",
                     help="comma-separated masks of the operations run in mixed precision "
                          "(1 vbias, 2 vHS + propagation, 4 energy, 8 vHS alone)")
     args = ap.parse_args(argv)
     if args.lockstep:
         outs = []
-        runs = [(int(x), int(m)) for x in args.exchange_split.split(",")
-                for m in args.mixed_ops.split(",")]
-        for split, mops in runs:
+        runs = [(int(x), int(m), int(t)) for x in args.exchange_split.split(",")
+                for m in args.mixed_ops.split(",") for t in args.taylor_mode.split(",")]
+        for split, mops, tmode in runs:
             t0 = time.time()
             e64, emx, wsum, comp, win = lockstep(args.steps, args.walkers, args.equil,
                                                  args.seed, args.workload, args.lscale, split,
                                                  mops, args.restart_every, args.measure_every,
-                                                 args.split_format)
+                                                 args.split_format, tmode)
             d = emx - e64
             out = {
                 "mode": "lockstep", "workload": args.workload, "lscale": args.lscale,
@@ -160,6 +165,7 @@ def main(argv=None):
                 "restart_every": args.restart_every, "measure_every": args.measure_every,
                 "windows": int(np.unique(win).size) if win.size else 0,
                 "exchange_split": split, "mixed_ops": mops, "split_format": args.split_format,
+                "taylor_mode": tmode,
                 "measurements": int(d.size),
                 "E_fp64": float(e64.mean()), "E_fp64_err": window_error(e64, win),
                 "E_mixed": float(emx.mean()), "E_mixed_err": window_error(emx, win),

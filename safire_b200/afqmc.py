@@ -413,7 +413,8 @@ class NOMSDMulti:
 
 class PHMSDWavefunction:
     """The walker-set facade of a PHMSD trial (Wavefunction.hpp's variant over PHMSD.hpp): the
-    same calls as NOMSD, evaluated by the multi-determinant kernels.  FP64 only."""
+    same calls as NOMSD, evaluated by the multi-determinant kernels.  Energy(precision=PREC_MIXED)
+    evaluates the excited determinants' 2-body terms in complex64 (afqmc_phmsd_set_precision)."""
 
     def __init__(self, trial: "PHMSD", block=0):
         self.ph = trial
@@ -437,11 +438,10 @@ class PHMSDWavefunction:
         return ovlp
 
     def Energy(self, wset: WalkerSet, set_properties=True, precision=PREC_FP64, stream=None):
-        if precision != PREC_FP64:
-            raise ValueError("PHMSD energies run in FP64")
         dev = wset.buffer.device
         E = torch.empty((wset.W, 3), dtype=torch.complex128, device=dev)
         ov = torch.empty(wset.W, dtype=torch.complex128, device=dev)
+        self.ph.set_precision(precision)
         self.ph.Energy(wset.buffer, E, ov, self.block, stream)
         if set_properties:  # PHMSD::Energy(wset) (PHMSD.cpp:75-87)
             p = wset.properties()
@@ -492,10 +492,10 @@ class Propagator:
         """Picks the fastest Taylor propagation variant for these walkers (mixed precision);
         returns (mode or -1, {mode: step ms}).  The walkers are left as they were."""
         best = C.c_int()
-        ms = np.zeros(3, dtype=np.float32)
+        ms = np.zeros(7, dtype=np.float32)
         call("afqmc_prop_autotune", self.handle, wset.handle, C.byref(best), _host_ptr(ms),
              _stream(stream))
-        return best.value, {m: float(t) for m, t in zip((0, 2, 3), ms)}
+        return best.value, {m: float(t) for m, t in zip((0, 2, 3, 4, 5, 6, 7), ms) if t > 0}
 
     def set_trial(self, trial, vMF=None):
         """Steps with a multi-determinant trial (PHMSD or NOMSDMulti: vbias and overlaps from
@@ -707,6 +707,10 @@ class PHMSD:
         """ovlp [W] (device) <- log overlap of every walker row of wbuf [W][ldS] (device)."""
         call("afqmc_phmsd_log_overlap", self.handle, _ptr(wbuf), int(wbuf.stride(0)), _ptr(ovlp),
              int(wbuf.shape[0]), _stream(stream))
+
+    def set_precision(self, precision):
+        """PREC_MIXED: the energy's excited-determinant tables in complex64 (afqmc_phmsd_set_precision)."""
+        call("afqmc_phmsd_set_precision", self.handle, int(precision))
 
     def info(self):
         """(M, nup, ndn, nact_up, nact_dn, Nc)"""

@@ -82,6 +82,7 @@ _SIGS = {
     "afqmc_phmsd_density_matrix": (i32, [vp, vp, i64, vp, vp, i32, i32, vp]),
     "afqmc_phmsd_vbias": (i32, [vp, vp, vp, i32, C.c_double, vp]),
     "afqmc_phmsd_info": (i32, [vp, vp]),
+    "afqmc_phmsd_set_precision": (i32, [vp, i32]),
     "afqmc_wfn_onerdm": (i32, [vp, vp, vp, i64, vp, vp]),
     "afqmc_prop_autotune": (i32, [vp, vp, vp, vp, vp]),
     "afqmc_ham_set_coulomb_fp64": (i32, [vp, i32]),

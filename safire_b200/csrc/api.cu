@@ -751,7 +751,7 @@ extern "C" int afqmc_ham_set_split_format(afqmc_ham h, int format, int* active_f
 
 extern "C" int afqmc_ham_set_taylor_fused(afqmc_ham h, int fused) {
   AFQMC_CHECK_ARG(h, "afqmc_ham_set_taylor_fused: null handle");
-  AFQMC_CHECK_ARG(fused >= 0 && fused <= 3, "afqmc_ham_set_taylor_fused: mode must be 0..3");
+  AFQMC_CHECK_ARG(fused >= 0 && fused <= 7, "afqmc_ham_set_taylor_fused: mode must be 0..7");
   DeviceGuard g(h->device);
   if (!h->mixed) {
     EnergyArgs a = energy_args(h, nullptr, 0);
@@ -1559,8 +1559,6 @@ extern "C" int afqmc_prop_set_phmsd(afqmc_prop pr, afqmc_phmsd trial, const afqm
   AFQMC_CHECK_ARG(d[5] == h->Nc,
                   "afqmc_prop_set_phmsd: trial Hamiltonian has %d Cholesky vectors, the "
                   "propagator %d (afqmc_phmsd_set_hamiltonian first)", d[5], h->Nc);
-  AFQMC_CHECK_ARG(pr->p.precision == AFQMC_PREC_FP64,
-                  "afqmc_prop_set_phmsd: PHMSD steps run in FP64");
   AFQMC_CHECK_ARG(!pr->md, "afqmc_prop_set_phmsd: a multi-determinant NOMSD trial is attached");
   dfree(pr->Gph);
   AFQMC_TRY(dalloc(&pr->Gph, size_t(pr->maxW) * (d[3] + d[4]) * h->M));
@@ -1662,6 +1660,12 @@ int prop_step(afqmc_prop_s* pr, afqmc_wset_s* ws, double Eshift, const double* E
   AFQMC_TRY(mark(3));
   // 3. vHS
   if (mixed) {
+    // (with a multi-determinant trial the vbias above ran through the trial, in complex128, and
+    // the mixed tensors may not exist yet)
+    if (!h->mixed) {
+      EnergyArgs a = energy_args(h, pr->G, ldG);
+      AFQMC_TRY(mixed_ham_create(&h->mixed, a, s));
+    }
     AFQMC_TRY(vhs_mixed(s, h->mixed, pr->X, nullptr, W, std::sqrt(dt)));
   } else if (mixed_vhs_only) {
     if (!h->mixed) {
@@ -1777,16 +1781,25 @@ extern "C" int afqmc_prop_autotune(afqmc_prop pr, afqmc_wset ws, int* best, floa
   cudaEvent_t e0, e1;
   AFQMC_CUDA_TRY(cudaEventCreate(&e0));
   AFQMC_CUDA_TRY(cudaEventCreate(&e1));
-  // Taylor propagation variants: 0 per-term GEMMs, 2 fused with one walker per CTA in flight,
-  // 3 fused with two (the fused kernel's occupancy / L2 working-set trade-off depends on W)
-  const int modes[3] = {0, 2, 3};
+  // Taylor propagation variants: 0 per-term GEMMs; fused: 2 / 3 TF32 split with one / two
+  // walkers in flight per CTA, 4 / 5 the same in the FP16 split (when the shapes allow it), 6 / 7
+  // one walker in flight with the running sum in tensor memory.  Every variant is timed; the
+  // choice is among 2 and 4, whose small split products have their own accumulator (the others
+  // accumulate three times as many updates in one FP32 accumulator, whose truncation toward zero
+  // shifts the mixed-estimator energy).
+  const int modes[7] = {0, 2, 3, 4, 5, 6, 7};
   float best_ms = 1e30f;
   int st = AFQMC_OK;
-  for (int mi = 0; mi < 3 && !st; ++mi) {
-    if (!h->mixed) {
-      EnergyArgs a = energy_args(h, nullptr, 0);
-      if ((st = mixed_ham_create(&h->mixed, a, s))) break;
-    }
+  if (!h->mixed) {
+    EnergyArgs a = energy_args(h, nullptr, 0);
+    st = mixed_ham_create(&h->mixed, a, s);
+  }
+  const bool f16 = !st && mixed_taylor_f16_ok(h->mixed);
+  for (int mi = 0; mi < 7; ++mi)
+    if (ms) ms[mi] = 0.f;
+  for (int mi = 0; mi < 7 && !st; ++mi) {
+    const int md = modes[mi];
+    if (!f16 && (md == 4 || md == 5 || md == 7)) continue;
     if ((st = mixed_set_taylor_mode(h->mixed, modes[mi]))) break;
     float t = 0.f;
     for (int rep = 0; rep < 3 && !st; ++rep) {  // the first repetition warms up
@@ -1802,9 +1815,9 @@ extern "C" int afqmc_prop_autotune(afqmc_prop pr, afqmc_wset ws, int* best, floa
       }
     }
     if (ms) ms[mi] = t / 2;
-    if (!st && t / 2 < best_ms) {
+    if (!st && (md == 2 || md == 4) && t / 2 < best_ms) {
       best_ms = t / 2;
-      *best = modes[mi];
+      *best = md;
     }
   }
   if (!st && *best >= 0) st = mixed_set_taylor_mode(h->mixed, *best);

@@ -216,7 +216,14 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
       int wp, np;
       tile_coords(t, WP, NP, wp, np);
       const int buf = int(ti & 1);
-      const bool ok = tc::mbar_wait(&acc_full[buf], unsigned(ti / 2) & 1u, p.err, abort_flag);
+      // the four epilogue warps meet at named barriers below: they leave the loop together, on
+      // the outcome of all four waits (a wait that gave up on one warp ends every warp's loop)
+      bool ok = tc::mbar_wait_warp(&acc_full[buf], unsigned(ti / 2) & 1u, p.err, abort_flag);
+      int* const agree = reinterpret_cast<int*>(red + 16);
+      if (lane == 0) agree[q] = ok ? 0 : 1;
+      named_bar(1, 128);
+      ok = (agree[0] | agree[1] | agree[2] | agree[3]) == 0;
+      named_bar(1, 128);
       tc::tc_fence_after();
       if (!ok) break;
       const int w = 2 * wp + wl;

@@ -389,7 +389,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_cgemm_kernel(const __grid_co
       int mt, nt, z;
       tc_tile(t, MT, NT, p.order, mt, nt, z);
       const int buf = int(ti & 1);
-      const bool ok = tc::mbar_wait(&acc_full[buf], unsigned(ti / 2) & 1u, p.err, abort_flag);
+      const bool ok =
+          tc::mbar_wait_warp(&acc_full[buf], unsigned(ti / 2) & 1u, p.err, abort_flag);
       tc::tc_fence_after();
       if (!ok) break;
       const int row = mt * 128 + q * 32 + lane;
@@ -884,8 +885,14 @@ struct MixedHam {
   const void* P1_16_src = nullptr;
   int capP16 = 0;
   bool v_is_f16 = false;   // format of the V planes the last vHS wrote
-  int taylor_mode = 1;    // 0: one GEMM launch per Taylor product; 1: fused, slots chosen by W;
-  int taylor_slots = 0;   // 2 / 3: fused with one / two walkers in flight per CTA
+  // Taylor propagation (mixed_set_taylor_mode): 0 one GEMM launch per product; 2 / 3 the fused
+  // kernel in the TF32 split with one / two walkers in flight per CTA; 4 / 5 the same in the FP16
+  // split; one walker in flight (2, 4) gives the small split products their own accumulator,
+  // 6 / 7 (TF32 / FP16) use that room for the running sum instead
+  int taylor_mode = 2;
+  int taylor_slots = 1;
+  bool taylor_f16 = false;
+  int taylor_one_slot = 0;  // 0 second accumulator, 1 running sum in tensor memory
   Planes G;         // [W][1][nel_tot*M]  (A of vbias);  exchange view [W*nel][M]
   Planes X;         // [1][W][Nc] (A of vHS)
   c128* vpart = nullptr;  // split-K partial sums of vbias [S][W][Nc]
@@ -1275,7 +1282,7 @@ int ensure_prop_buffers16(MixedHam* m, int W, int N) {
 // FP16 V planes and the FP16 Taylor kernel go together: the FP16 split, the fused Taylor
 // kernel, and shapes it takes (M <= 256, N <= 64)
 bool v16_ok(const MixedHam* m) {
-  return use_f16(m) && m->taylor_mode != 0 && m->M <= 256 && m->nel[0] <= 64;
+  return use_f16(m) && m->taylor_f16 && m->taylor_mode != 0 && m->M <= 256 && m->nel[0] <= 64;
 }
 
 int ensure_prop_buffers(MixedHam* m, int W, int N) {
@@ -1402,8 +1409,8 @@ int vhs_mixed(cudaStream_t s, MixedHam* m, const c128* X, c128* V, int W, double
 int taylor_fused_tc(cudaStream_t s, int esize, const void* const P1p[2], const void* const Vp[4],
                     long ldV, const void* const Sp[4], void* const Tp0[4], void* const Tp1[4],
                     void* const Rp[4], float* const sum[2], long pl_ld, c128* S, long ldS, int W,
-                    int M, int N, int order, int nslots, const float* v_inv, const float* s_inv,
-                    float p1_inv, unsigned* err);
+                    int M, int N, int order, int nslots, int one_slot_use, const float* v_inv,
+                    const float* s_inv, float p1_inv, unsigned* err);
 
 // Taylor propagation S <- P1 sum_n (iV)^n/n! P1 S (propagate.hpp:238-298) on the split planes.
 // V must have been produced by vhs_mixed (planes kept in MixedHam) for the same walkers.
@@ -1446,8 +1453,8 @@ int propagate_mixed(cudaStream_t s, MixedHam* m, const void* P1, bool p1_real, c
       return AFQMC_ERR_UNSUPPORTED;
     }
     return taylor_fused_tc(s, 2, p1p, vp, m->V16.ld, sp, t0, t1, rp, m->acc, m->T0_16.ld, S, ldS,
-                           W, M, N, order, m->taylor_slots, m->v_inv, m->s_inv, m->p1_inv,
-                           m->err);
+                           W, M, N, order, m->taylor_slots, m->taylor_one_slot, m->v_inv,
+                           m->s_inv, m->p1_inv, m->err);
   }
   if (m->P1_src != P1) {
     free_planes(m->P1);
@@ -1467,7 +1474,8 @@ int propagate_mixed(cudaStream_t s, MixedHam* m, const void* P1, bool p1_real, c
     void* rp[4] = {m->Tacc_split.p[0], m->Tacc_split.p[1], m->Tacc_split.p[2],
                    m->Tacc_split.p[3]};
     return taylor_fused_tc(s, 4, p1p, vp, m->V.ld, sp, t0, t1, rp, m->acc, m->T0.ld, S, ldS, W,
-                           M, N, order, m->taylor_slots, nullptr, nullptr, 1.f, m->err);
+                           M, N, order, m->taylor_slots, m->taylor_one_slot, nullptr, nullptr, 1.f,
+                           m->err);
   }
   Planes* Tin = &m->T0;
   Planes* Tout = &m->T1;
@@ -1516,10 +1524,19 @@ int propagate_mixed(cudaStream_t s, MixedHam* m, const void* P1, bool p1_real, c
 }
 
 int mixed_set_taylor_mode(MixedHam* m, int mode) {
+  if (mode < 0 || mode > 7) {
+    set_error_detail("Taylor mode must be 0..7");
+    return AFQMC_ERR_ARG;
+  }
+  if (mode == 1) mode = 2;  // the default: one walker in flight, two accumulators, TF32
   m->taylor_mode = mode;
-  m->taylor_slots = mode >= 2 ? mode - 1 : 0;
+  m->taylor_slots = (mode == 3 || mode == 5) ? 2 : (mode == 0 ? 0 : 1);
+  m->taylor_f16 = (mode == 4 || mode == 5 || mode == 7);
+  m->taylor_one_slot = mode >= 6 ? 1 : 0;
   return AFQMC_OK;
 }
+
+bool mixed_taylor_f16_ok(MixedHam* m) { return use_f16(m) && m->M <= 256 && m->nel[0] <= 64; }
 
 int mixed_prepare_G(cudaStream_t s, MixedHam* m, const c128* G, long ldG, int W) {
   if (use_f16(m)) {

@@ -19,8 +19,11 @@ int propagate_mixed(cudaStream_t s, MixedHam* m, const void* P1, bool p1_real, c
                     int W, int M, int N, int order);
 // 0: one batched GEMM launch per Taylor product; 1 (default): all products of a walker in one
 // persistent kernel (M <= 256, N <= 64), one or two walkers in flight per CTA chosen by the walker
-// count; 2 / 3: the persistent kernel with one / two walkers in flight
+// count; 2 / 3: the persistent kernel with one / two walkers in flight; 4 / 5: the same in the
+// FP16 split (vHS then writes FP16 V planes)
 int mixed_set_taylor_mode(MixedHam* m, int mode);
+// the FP16 Taylor variants (4, 5) are available for these shapes
+bool mixed_taylor_f16_ok(MixedHam* m);
 // split planes of G for the exchange-energy GEMMs
 int mixed_prepare_G(cudaStream_t s, MixedHam* m, const c128* G, long ldG, int W);
 // T [(w,b)][(n,a)] for walkers [w0, w0+wc) of spin block sp (complex128, the chunk layout of

@@ -27,6 +27,35 @@ namespace {
 constexpr int PH_THREADS = 256;
 constexpr int PH_NEX_MAX = 8;
 
+// complex arithmetic in single precision for the mixed-precision energy tables (the complex128
+// helpers of common.cuh, restated for float2)
+using c64 = float2;
+using afqmc::cadd;
+using afqmc::cmul;
+using afqmc::cscale;
+using afqmc::csub;
+__device__ __forceinline__ c64 cadd(c64 a, c64 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ c64 csub(c64 a, c64 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ c64 cmul(c64 a, c64 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ c64 cscale(c64 a, float s) { return make_float2(a.x * s, a.y * s); }
+template <typename R> struct CxOf;
+template <> struct CxOf<double> { using T = c128; };
+template <> struct CxOf<float> { using T = c64; };
+template <typename C> __device__ __forceinline__ C czero();
+template <> __device__ __forceinline__ c128 czero<c128>() { return cmk(0, 0); }
+template <> __device__ __forceinline__ c64 czero<c64>() { return make_float2(0.f, 0.f); }
+template <typename C> __device__ __forceinline__ C to_cx(c128 x);
+template <> __device__ __forceinline__ c128 to_cx<c128>(c128 x) { return x; }
+template <> __device__ __forceinline__ c64 to_cx<c64>(c128 x) {
+  return make_float2(float(x.x), float(x.y));
+}
+template <typename C> __device__ __forceinline__ C to_cx(c64 x);
+template <> __device__ __forceinline__ c128 to_cx<c128>(c64 x) {
+  return cmk(double(x.x), double(x.y));
+}
+
 __device__ __forceinline__ c128 dot_row(const c128* __restrict__ t, const c128* __restrict__ r,
                                         int nact) {
   double re = 0.0, im = 0.0;
@@ -450,12 +479,16 @@ __global__ void woodbury_inverses_kernel(const c128* __restrict__ QQ0, const int
 // Table layout: Tn [nel][nact]; Yv [nel][nv] and Qv [nel][nv] (QQ0 transposed) on the virtual
 // columns c; Uh [nh][nact] and Zh [nh][nv] on the hole rows k.  e4 = the determinant's holes,
 // particles, hole rows k and particle columns c.
-template <int NEX>
+template <int NEX, typename C>
 __device__ __forceinline__ void excited_terms(const int* __restrict__ e4,
-                                              const c128* __restrict__ Qi, const c128* Tn,
-                                              const c128* Yv, const c128* Uh, const c128* Zh,
-                                              const c128* Qv, const int* refs, int nact, int nv,
-                                              c128 f0, c128& ex_out, c128& kn_out) {
+                                              const c128* __restrict__ Qg, const C* Tn,
+                                              const C* Yv, const C* Uh, const C* Zh, const C* Qv,
+                                              const int* refs, int nact, int nv, C f0, C& ex_out,
+                                              C& kn_out) {
+  using R = decltype(f0.x);
+  C Qi[NEX * NEX];  // the determinant's Woodbury inverse, in the working precision
+#pragma unroll
+  for (int k = 0; k < NEX * NEX; ++k) Qi[k] = to_cx<C>(Qg[k]);
   int h[NEX], p[NEX], r[NEX], hr[NEX], pc[NEX];
 #pragma unroll
   for (int a = 0; a < NEX; ++a) {
@@ -465,24 +498,24 @@ __device__ __forceinline__ void excited_terms(const int* __restrict__ e4,
     pc[a] = e4[3 * NEX + a];
     r[a] = refs[h[a]];
   }
-  c128 F[NEX][NEX], D[NEX];
+  C F[NEX][NEX], D[NEX];
 #pragma unroll
   for (int a = 0; a < NEX; ++a) {
-    const c128* ta = Tn + h[a] * nact;
-    const c128* ua = Uh + hr[a] * nact;
-    c128 dt[NEX], du[NEX];
+    const C* ta = Tn + h[a] * nact;
+    const C* ua = Uh + hr[a] * nact;
+    C dt[NEX], du[NEX];
 #pragma unroll
     for (int x = 0; x < NEX; ++x) {
       dt[x] = csub(ta[p[x]], ta[r[x]]);
       du[x] = csub(ua[p[x]], ua[r[x]]);
     }
-    c128 g[NEX], gu[NEX];
+    C g[NEX], gu[NEX];
 #pragma unroll
     for (int q = 0; q < NEX; ++q) {
-      c128 ct = cmk(0, 0), cu = cmk(0, 0);
+      C ct = czero<C>(), cu = czero<C>();
 #pragma unroll
       for (int x = 0; x < NEX; ++x) {
-        const c128 qv = Qv[h[x] * nv + pc[q]];  // QQ0[p_q][h_x]
+        const C qv = Qv[h[x] * nv + pc[q]];  // QQ0[p_q][h_x]
         ct = cadd(ct, cmul(dt[x], qv));
         cu = cadd(cu, cmul(du[x], qv));
       }
@@ -491,70 +524,71 @@ __device__ __forceinline__ void excited_terms(const int* __restrict__ e4,
     }
 #pragma unroll
     for (int b = 0; b < NEX; ++b) {
-      c128 f = cmk(0, 0);
+      C f = czero<C>();
 #pragma unroll
       for (int q = 0; q < NEX; ++q) f = cadd(f, cmul(Qi[b * NEX + q], g[q]));
       F[a][b] = f;
     }
-    c128 dd = cmk(0, 0);
+    C dd = czero<C>();
 #pragma unroll
     for (int q = 0; q < NEX; ++q) dd = cadd(dd, cmul(Qi[a * NEX + q], gu[q]));
     D[a] = dd;
   }
-  c128 ex = cmk(0, 0), kn = f0;
+  C ex = czero<C>(), kn = f0;
 #pragma unroll
   for (int a = 0; a < NEX; ++a) {
-    const c128* ta = Tn + h[a] * nact;
-    const c128* ua = Uh + hr[a] * nact;
-    const c128 tpa = ta[p[a]], tra = ta[r[a]];
+    const C* ta = Tn + h[a] * nact;
+    const C* ua = Uh + hr[a] * nact;
+    const C tpa = ta[p[a]], tra = ta[r[a]];
     kn = cadd(kn, cadd(F[a][a], csub(tpa, tra)));
     // f_a^2 and the changed electron's own diagonal term
     ex = cadd(ex, cmul(F[a][a], F[a][a]));
     ex = cadd(ex, csub(cmul(tpa, tpa), cmul(tra, tra)));
     // B_a = sum_j t_{h_a}[occ_j] F(j, a);  C_a = sum over unchanged j of the pair term (i = h_a)
-    c128 B = D[a];
-    c128 C = csub(ua[p[a]], ua[r[a]]);
+    C B = D[a];
+    C Cc = csub(ua[p[a]], ua[r[a]]);
 #pragma unroll
     for (int x = 0; x < NEX; ++x) {
-      const c128* tx = Tn + h[x] * nact;
+      const C* tx = Tn + h[x] * nact;
       B = cadd(B, cmul(csub(ta[p[x]], ta[r[x]]), F[x][a]));
-      C = csub(C, cmul(ta[r[x]], csub(tx[p[a]], tx[r[a]])));
+      Cc = csub(Cc, cmul(ta[r[x]], csub(tx[p[a]], tx[r[a]])));
       if (x != a) ex = cadd(ex, csub(cmul(ta[p[x]], tx[p[a]]), cmul(ta[r[x]], tx[r[a]])));
-      if (x > a) ex = cadd(ex, cscale(cmul(F[x][a], F[a][x]), 2.0));
+      if (x > a) ex = cadd(ex, cscale(cmul(F[x][a], F[a][x]), R(2)));
     }
-    ex = cadd(ex, cscale(cadd(B, C), 2.0));
+    ex = cadd(ex, cscale(cadd(B, Cc), R(2)));
   }
   ex_out = ex;
   kn_out = kn;
 }
 
 // nex > 4 is rare: out of line, so that its larger frame stays out of the common path
-template <int NEX>
-__device__ __noinline__ void excited_terms_rare(const int* e4, const c128* Qi, const c128* Tn,
-                                                const c128* Yv, const c128* Uh, const c128* Zh,
-                                                const c128* Qv, const int* refs, int nact, int nv,
-                                                c128 f0, c128& ex, c128& kn) {
-  excited_terms<NEX>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn);
+template <int NEX, typename C>
+__device__ __noinline__ void excited_terms_rare(const int* e4, const c128* Qi, const C* Tn,
+                                                const C* Yv, const C* Uh, const C* Zh,
+                                                const C* Qv, const int* refs, int nact, int nv,
+                                                C f0, C& ex, C& kn) {
+  excited_terms<NEX, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn);
 }
 
 // One product of the tables: out[k][c] = sum_j a[k][sel_j] b[j][c] over the rows k of `rows`
 // (row index rows[k], or k when rows is null).
+template <typename C>
 struct TableProduct {
-  const c128* a;
+  const C* a;
   int lda;
   const int* rows;
   int nrows;
-  const c128* b;
+  const C* b;
   int ldb, ncol;
-  c128* out;
+  C* out;
   int ldo;
 };
 
 // Runs products side by side over the block: a thread owns the columns t and t + nt (nt =
 // ceil(ncol / 2)) of one row, so that each shared-memory read of a feeds two products and
 // neighbouring threads read neighbouring columns of b.
-template <int NP>
-__device__ __forceinline__ void table_products(const TableProduct (&P)[NP], const int* sel,
+template <int NP, typename C>
+__device__ __forceinline__ void table_products(const TableProduct<C> (&P)[NP], const int* sel,
                                                int nsum) {
   int start[NP + 1];
   start[0] = 0;
@@ -565,15 +599,15 @@ __device__ __forceinline__ void table_products(const TableProduct (&P)[NP], cons
 #pragma unroll
     for (int q = 1; q < NP; ++q)
       if (idx >= start[q]) i = q;
-    const TableProduct& T = P[i];
+    const TableProduct<C>& T = P[i];
     const int nt = (T.ncol + 1) / 2, loc = idx - start[i];
     const int k = loc / nt, t = loc - k * nt;
     const bool two = t + nt < T.ncol;
-    const c128* ak = T.a + (T.rows ? T.rows[k] : k) * T.lda;
-    c128 a0 = cmk(0, 0), a1 = cmk(0, 0);
+    const C* ak = T.a + (T.rows ? T.rows[k] : k) * T.lda;
+    C a0 = czero<C>(), a1 = czero<C>();
     for (int j = 0; j < nsum; ++j) {
-      const c128 x = ak[sel[j]];
-      const c128* bj = T.b + j * T.ldb + t;
+      const C x = ak[sel[j]];
+      const C* bj = T.b + j * T.ldb + t;
       a0 = cadd(a0, cmul(x, bj[0]));
       if (two) a1 = cadd(a1, cmul(x, bj[nt]));
     }
@@ -590,7 +624,12 @@ __device__ __forceinline__ void table_products(const TableProduct (&P)[NP], cons
 // The reference determinant's terms come from the same tables (ph_reference_energy,
 // Real3IndexFactorization.hpp:212-233, 598-696): Kref[w][n] = f0, REF[w] += (sum_ij t_i[r_j]
 // t_j[r_i], f0^2).
+// R = double: complex128 tables and per-determinant sums (the reference's arithmetic); R = float:
+// complex64 tables and per-determinant sums, for the mixed-precision energy (half the shared
+// memory, twice the FP32 rate); the sums over determinants, the reference determinant's terms
+// and every output stay FP64.
 constexpr int PHX_THREADS = 256;
+template <typename R>
 __global__ void __launch_bounds__(PHX_THREADS, 1) excited_energy_tables_kernel(
     const c128* __restrict__ Twina, const c128* __restrict__ QQ0, const int* __restrict__ refc,
     const int* __restrict__ hl, const int* __restrict__ vl, int nh, int nv,
@@ -600,12 +639,13 @@ __global__ void __launch_bounds__(PHX_THREADS, 1) excited_energy_tables_kernel(
     c128* __restrict__ EXacc, c128* __restrict__ EJacc, c128* __restrict__ KE,
     const c128* __restrict__ cross, c128* __restrict__ E, c128* __restrict__ Kref,
     c128* __restrict__ REF) {
+  using C = typename CxOf<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  c128* Tn = reinterpret_cast<c128*>(smem_raw);     // [nel][nact]
-  c128* Qv = Tn + nel * nact;                        // [nel][nv]
-  c128* Yv = Qv + nel * nv;                          // [nel][nv]
-  c128* Uh = Yv + nel * nv;                          // [nh][nact]
-  c128* Zh = Uh + nh * nact;                         // [nh][nv]
+  C* Tn = reinterpret_cast<C*>(smem_raw);            // [nel][nact]
+  C* Qv = Tn + nel * nact;                           // [nel][nv]
+  C* Yv = Qv + nel * nv;                             // [nel][nv]
+  C* Uh = Yv + nel * nv;                             // [nh][nact]
+  C* Zh = Uh + nh * nact;                            // [nh][nv]
   int* refs = reinterpret_cast<int*>(Zh + nh * nv);  // [nel]
   int* hls = refs + nel;                             // [nh]
   __shared__ double red[PHX_THREADS / 32 * 6];
@@ -614,35 +654,36 @@ __global__ void __launch_bounds__(PHX_THREADS, 1) excited_energy_tables_kernel(
   const c128* Qw = QQ0 + size_t(w) * nact * nel;
   for (int k = threadIdx.x; k < nel * nact; k += blockDim.x) {
     const int j = k / nact, x = k - j * nact;
-    Tn[k] = Tw[(size_t(j) * nchol + n) * nact + x];
+    Tn[k] = to_cx<C>(Tw[(size_t(j) * nchol + n) * nact + x]);
   }
   for (int k = threadIdx.x; k < nel * nv; k += blockDim.x) {
     const int i = k / nv, c = k - i * nv;
-    Qv[k] = Qw[size_t(vl[c]) * nel + i];
+    Qv[k] = to_cx<C>(Qw[size_t(vl[c]) * nel + i]);
   }
   for (int i = threadIdx.x; i < nel; i += blockDim.x) refs[i] = refc[i];
   for (int k = threadIdx.x; k < nh; k += blockDim.x) hls[k] = hl[k];
   __syncthreads();
   // Y = t[:, r] Qv,  U = t[hole rows, r] t
   {
-    const TableProduct P[2] = {{Tn, nact, nullptr, nel, Qv, nv, nv, Yv, nv},
-                               {Tn, nact, hls, nh, Tn, nact, nact, Uh, nact}};
-    table_products<2>(P, refs, nel);
+    const TableProduct<C> P[2] = {{Tn, nact, nullptr, nel, Qv, nv, nv, Yv, nv},
+                                  {Tn, nact, hls, nh, Tn, nact, nact, Uh, nact}};
+    table_products<2, C>(P, refs, nel);
   }
   // the reference determinant: f0 = sum_i t_i[r_i], ex0 = sum_ij t_i[r_j] t_j[r_i]
   c128 ex0 = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0);
   for (int k = threadIdx.x; k < nel * nel; k += blockDim.x) {
     const int i = k / nel, j = k - i * nel;
-    ex0 = cadd(ex0, cmul(Tn[i * nact + refs[j]], Tn[j * nact + refs[i]]));
+    ex0 = cadd(ex0, cmul(to_cx<c128>(Tn[i * nact + refs[j]]), to_cx<c128>(Tn[j * nact + refs[i]])));
   }
   __syncthreads();
   // Z = t[hole rows, r] Y
   {
-    const TableProduct P[1] = {{Tn, nact, hls, nh, Yv, nv, nv, Zh, nv}};
-    table_products<1>(P, refs, nel);
+    const TableProduct<C> P[1] = {{Tn, nact, hls, nh, Yv, nv, nv, Zh, nv}};
+    table_products<1, C>(P, refs, nel);
   }
   c128 f0 = cmk(0, 0);
-  for (int i = 0; i < nel; ++i) f0 = cadd(f0, Tn[i * nact + refs[i]]);
+  for (int i = 0; i < nel; ++i) f0 = cadd(f0, to_cx<c128>(Tn[i * nact + refs[i]]));
+  const C f0w = to_cx<C>(f0);
   const c128 f00 = cmul(f0, f0);
   block_sum3(ex0, z1, z2, red);  // ends with a barrier: Zh is complete after it
   if (threadIdx.x == 0 && Kref) {
@@ -659,17 +700,18 @@ __global__ void __launch_bounds__(PHX_THREADS, 1) excited_energy_tables_kernel(
     const int nex = unex[u];
     const int* e4 = uexc4 + uoff4[u];
     const c128* Qi = Iw + uinv[u];
-    c128 ex, kn;
+    C exw, knw;
     switch (nex) {
-      case 1: excited_terms<1>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
-      case 2: excited_terms<2>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
-      case 3: excited_terms<3>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
-      case 4: excited_terms<4>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
-      case 5: excited_terms_rare<5>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
-      case 6: excited_terms_rare<6>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
-      case 7: excited_terms_rare<7>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
-      default: excited_terms_rare<8>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn); break;
+      case 1: excited_terms<1, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
+      case 2: excited_terms<2, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
+      case 3: excited_terms<3, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
+      case 4: excited_terms<4, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
+      case 5: excited_terms_rare<5, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
+      case 6: excited_terms_rare<6, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
+      case 7: excited_terms_rare<7, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
+      default: excited_terms_rare<8, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
     }
+    const c128 ex = to_cx<c128>(exw), kn = to_cx<c128>(knw);
     const c128 wu = wgt[size_t(u) * W + w];
     exs = cadd(exs, cmul(wu, ex));
     ejs = cadd(ejs, cmul(wu, csub(cmul(kn, kn), f00)));
@@ -977,6 +1019,7 @@ extern "C" int afqmc_ph_excited_1body_energy(const int* iexcit, const int* refc,
 // ---------------------------------------------------------------------------------------------
 struct afqmc_phmsd_s {
   int device = 0, M = 0, nel[2] = {0, 0}, nact[2] = {0, 0}, nuniq[2] = {0, 0}, ndet = 0;
+  int precision = AFQMC_PREC_FP64;  // of the energy's per-(walker, vector) tables
   c128* orbmat[2] = {nullptr, nullptr};
   int* refc[2] = {nullptr, nullptr};
   int* uoff[2] = {nullptr, nullptr};
@@ -1306,6 +1349,13 @@ extern "C" int afqmc_phmsd_destroy(afqmc_phmsd h) {
   return AFQMC_OK;
 }
 
+extern "C" int afqmc_phmsd_set_precision(afqmc_phmsd h, int precision) {
+  AFQMC_CHECK_ARG(h && (precision == AFQMC_PREC_FP64 || precision == AFQMC_PREC_MIXED),
+                  "afqmc_phmsd_set_precision: precision must be FP64 or MIXED");
+  h->precision = precision;
+  return AFQMC_OK;
+}
+
 extern "C" int afqmc_phmsd_info(afqmc_phmsd h, int* dims) {
   AFQMC_CHECK_ARG(h && dims, "afqmc_phmsd_info: null argument");
   dims[0] = h->M;
@@ -1556,9 +1606,9 @@ int phmsd_half_rotated(afqmc_phmsd h, cudaStream_t s, int sp, int nb) {
 // the excited determinants of spin sp, shell by shell: 1-body into el[0], 2-body into el[1..2],
 // KE of each determinant written to KEout + k0 * nb * Nc (cross = nullptr) or to KEl and
 // contracted with cross at once (the second step)
-size_t excited_tables_smem(afqmc_phmsd h, int sp) {
+size_t excited_tables_smem(afqmc_phmsd h, int sp, size_t elem = sizeof(c128)) {
   const size_t N = h->nel[sp], na = h->nact[sp], nv = h->nv[sp], nh = h->nh[sp];
-  return (N * na + 2 * N * nv + nh * na + nh * nv) * sizeof(c128) + (N + nh) * sizeof(int);
+  return (N * na + 2 * N * nv + nh * na + nh * nv) * elem + (N + nh) * sizeof(int);
 }
 
 // The reference determinant's and the excited determinants' energies of spin sp
@@ -1569,7 +1619,8 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
   const int N = h->nel[sp], na = h->nact[sp], Nc = h->Nc;
   // the 2-body terms from per-(walker, n) tables when they fit in shared memory, else per shell
   // from the R rows (the reference kernel's formulation)
-  const size_t tsmem = excited_tables_smem(h, sp);
+  const bool mixed = h->precision == AFQMC_PREC_MIXED;
+  const size_t tsmem = excited_tables_smem(h, sp, mixed ? sizeof(c64) : sizeof(c128));
   const bool tables = h->tables_ok[sp] && tsmem <= 200 * 1024;
   if (!tables) {
     ph_reference_kernel<<<nb, PH_THREADS, 0, s>>>(h->Swia, h->Twina, h->refc[sp], N, Nc, na, E0,
@@ -1615,9 +1666,10 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
       AFQMC_TRY(launch_status("woodbury_inverses_kernel"));
     }
     c128* REF = h->el + 3 * nb;  // [nb][2]: sum_n ex0, sum_n f0^2
-    AFQMC_CUDA_TRY(cudaFuncSetAttribute(excited_energy_tables_kernel,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(tsmem)));
-    excited_energy_tables_kernel<<<dim3(Nc, nb), PHX_THREADS, tsmem, s>>>(
+    auto kern = mixed ? excited_energy_tables_kernel<float> : excited_energy_tables_kernel<double>;
+    AFQMC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(tsmem)));
+    kern<<<dim3(Nc, nb), PHX_THREADS, tsmem, s>>>(
         h->Twina, h->eQ[sp], h->refc[sp], h->hl[sp], h->vl[sp], h->nh[sp], h->nv[sp],
         h->uoff4[sp], h->unex[sp], h->uexc4[sp], h->uinv[sp], h->INV, h->ninv[sp], h->wgt,
         h->nuniq[sp], nb, N, na, Nc, h->el + nb, h->el + 2 * nb, cross ? nullptr : KEout, cross,

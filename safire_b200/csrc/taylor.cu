@@ -54,6 +54,12 @@ struct TyParams {
   long pl_ld, pl_bs;     // ld / batch stride of the [W][N][M] planes
   int W, M, N, order;
   int nslots;            // walkers in flight per CTA (1 or 2)
+  int sum_tmem;          // 1: the running sum lives in tensor memory (columns 256..511, one
+                         // walker in flight), not in `sum`
+  int dual;              // 1: the small split products (hi*lo, lo*hi) go to a second accumulator
+                         // (columns 256..511, one walker in flight), added to the main one
+                         // (hi*hi) in the epilogue: a third of the updates of the main
+                         // accumulator, whose FP32 accumulation truncates toward zero
   // FP16 form: inverse power-of-two scales of the operands (V and S per walker, P1 one)
   const float* v_inv;
   const float* s_inv;
@@ -158,6 +164,17 @@ __device__ __forceinline__ void taylor_epilogue_f16(const TyParams& p, uint32_t 
       float vr[16], vi[16];
       tc::tmem_ld16(tacc + c0, vr);
       tc::tmem_ld16(tacc + TBN + c0, vi);
+      if (p.dual) {  // + the small products' accumulator (FP32 add, rounded to nearest)
+        float wr[16], wi[16];
+        tc::tmem_ld16(tacc + 256 + c0, wr);
+        tc::tmem_ld16(tacc + 256 + TBN + c0, wi);
+        tc::tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          vr[j] += wr[j];
+          vi[j] += wi[j];
+        }
+      }
       tc::tmem_ld_wait();
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
@@ -174,26 +191,41 @@ __device__ __forceinline__ void taylor_epilogue_f16(const TyParams& p, uint32_t 
     float mx = 0.f;
     if (!last_phase) {
       for (int mt = 0; mt < MT; ++mt) {
-        if (ok && !tc::mbar_wait(&acc_full[sl * 2 + mt], par, p.err, abort_flag)) ok = false;
+        if (ok && !tc::mbar_wait_warp(&acc_full[sl * 2 + mt], par, p.err, abort_flag))
+          ok = false;
         if (!ok) continue;
         tc::tc_fence_after();
         const int row = mt * 128 + q * 32 + lane;
         const uint32_t tacc =
             taddr + (uint32_t(q * 32) << 16) + uint32_t(sl * 256 + mt * 2 * TBN);
+        const uint32_t tsum = taddr + (uint32_t(q * 32) << 16) + uint32_t(256 + mt * 2 * TBN);
         const long off = wb + row;
 #pragma unroll 1
         for (int c0 = 0; c0 < TBN; c0 += 16) {
+          if (c0 >= N) continue;
           float xr[16], xi[16];
           values(tacc, c0, xr, xi);
-          if (row >= M || c0 >= N) continue;
+          float sr[16], si[16];
+          const bool add_sum = last_term && taylor;
+          if (add_sum && p.sum_tmem) {  // warp-collective: before any per-row branch
+            tc::tmem_ld16(tsum + c0, sr);
+            tc::tmem_ld16(tsum + TBN + c0, si);
+            tc::tmem_ld_wait();
+          }
+          if (row >= M) continue;
 #pragma unroll
           for (int j = 0; j < 16; ++j)
             if (c0 + j < N) {
               float ur = xr[j], ui = xi[j];
-              if (last_term && taylor) {
-                const long idx = off + long(c0 + j) * pl_ld;
-                ur += sum_r[idx];
-                ui += sum_i[idx];
+              if (add_sum) {
+                if (p.sum_tmem) {
+                  ur += sr[j];
+                  ui += si[j];
+                } else {
+                  const long idx = off + long(c0 + j) * pl_ld;
+                  ur += sum_r[idx];
+                  ui += sum_i[idx];
+                }
               }
               mx = fmaxf(mx, fmaxf(fabsf(ur), fabsf(ui)));
             }
@@ -218,47 +250,82 @@ __device__ __forceinline__ void taylor_epilogue_f16(const TyParams& p, uint32_t 
 
     for (int mt = 0; mt < MT; ++mt) {
       if (last_phase) {
-        if (ok && !tc::mbar_wait(&acc_full[sl * 2 + mt], par, p.err, abort_flag)) ok = false;
+        if (ok && !tc::mbar_wait_warp(&acc_full[sl * 2 + mt], par, p.err, abort_flag))
+          ok = false;
         if (!ok) continue;
         tc::tc_fence_after();
       }
       const int row = mt * 128 + q * 32 + lane;
       const bool rok = row < M;
       const uint32_t tacc = taddr + (uint32_t(q * 32) << 16) + uint32_t(sl * 256 + mt * 2 * TBN);
+      const uint32_t tsum = taddr + (uint32_t(q * 32) << 16) + uint32_t(256 + mt * 2 * TBN);
       const long off = wb + row;
       c128* Sw = p.S + long(w) * p.ldS + long(row) * N;
 #pragma unroll 1
       for (int c0 = 0; c0 < TBN; c0 += 16) {
+        if (c0 >= N) {
+          // no electron column in this chunk: only free the accumulator
+          if (c0 + 16 >= TBN) {
+            tc::tc_fence_before();
+            tc::mbar_arrive(&acc_empty[sl * 2 + mt]);
+          }
+          continue;
+        }
         float xr[16], xi[16];
         values(tacc, c0, xr, xi);
+        // the running sum of this chunk (taylor phases), warp-collective in tensor memory
+        float sr[16], si[16];
+        if (taylor && p.sum_tmem) {
+          tc::tmem_ld16(tsum + c0, sr);
+          tc::tmem_ld16(tsum + TBN + c0, si);
+          tc::tmem_ld_wait();
+        }
         if (c0 + 16 >= TBN) {
           // the accumulator is free for this slot's next phase
           tc::tc_fence_before();
           tc::mbar_arrive(&acc_empty[sl * 2 + mt]);
         }
-        if (!rok || c0 >= N) continue;
         if (last_phase) {
           // S = P1 R  (complex128 walker matrix [M][N])
+          if (!rok) continue;
 #pragma unroll
           for (int j = 0; j < 16; ++j)
             if (c0 + j < N) Sw[c0 + j] = cmk(xr[j], xi[j]);
           continue;
         }
+        if (!p.sum_tmem && taylor && rok) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (c0 + j < N) {
+              const long idx = off + long(c0 + j) * pl_ld;
+              sr[j] = sum_r[idx];
+              si[j] = sum_i[idx];
+            }
+        }
+        float ur[16], ui[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          ur[j] = taylor ? xr[j] + sr[j] : xr[j];
+          ui[j] = taylor ? xi[j] + si[j] : xi[j];
+        }
+        if (p.sum_tmem && !last_term) {  // the new running sum, warp-collective
+          tc::tmem_st16(tsum + c0, ur);
+          tc::tmem_st16(tsum + TBN + c0, ui);
+          tc::tmem_st_wait();
+        }
+        if (!rok) continue;
 #pragma unroll
         for (int j = 0; j < 16; ++j)
           if (c0 + j < N) {
             const long idx = off + long(c0 + j) * pl_ld;
-            float ur = xr[j], ui = xi[j];
-            if (taylor) {
-              ur += sum_r[idx];
-              ui += sum_i[idx];
-            }
             if (last_term) {
-              split_store16(ur * osc, dst[0], dst[1], idx);
-              split_store16(ui * osc, dst[2], dst[3], idx);
+              split_store16(ur[j] * osc, dst[0], dst[1], idx);
+              split_store16(ui[j] * osc, dst[2], dst[3], idx);
             } else {
-              sum_r[idx] = ur;
-              sum_i[idx] = ui;
+              if (!p.sum_tmem) {
+                sum_r[idx] = ur[j];
+                sum_i[idx] = ui[j];
+              }
               split_store16(xr[j] * osc, dst[0], dst[1], idx);
               split_store16(xi[j] * osc, dst[2], dst[3], idx);
             }
@@ -402,6 +469,8 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
           }
           tc::tc_fence_after();
           const uint32_t dr = taddr + uint32_t(sl * 256 + mt * 2 * TBN), di = dr + TBN;
+          // the small products' accumulators (dual), else the main ones
+          const uint32_t er = p.dual ? dr + 256u : dr, ei = er + TBN;
           for (int kc = 0; kc < nk; ++kc, ++it) {
             const int s = int(it % T_STAGES);
             if (!tc::mbar_wait(&full[s], unsigned(it / T_STAGES) & 1u, p.err, abort_flag)) {
@@ -418,27 +487,30 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
               auto A = [&](int q) { return tc::sdesc_sw128(sa + q * T_A_TILE) + uint64_t(2 * kk); };
               auto B = [&](int q) { return tc::sdesc_sw128(sb + q * T_B_TILE) + uint64_t(2 * kk); };
               const uint32_t acc0 = (kc > 0 || kk > 0) ? 1u : 0u;
+              // hi*hi products into (dr, di); hi*lo and lo*hi into (er, ei), which are (dr, di)
+              // themselves unless dual (the first product into each accumulator starts it)
+              const uint32_t accs = p.dual ? acc0 : 1u;
               if (p1) {
                 // real A (P1 hi, lo) x complex B
                 tc::mma_split<F16>(dr, A(0), B(0), ID, acc0);
-                tc::mma_split<F16>(dr, A(0), B(1), ID, 1);
-                tc::mma_split<F16>(dr, A(1), B(0), ID, 1);
+                tc::mma_split<F16>(er, A(0), B(1), ID, accs);
+                tc::mma_split<F16>(er, A(1), B(0), ID, 1);
                 tc::mma_split<F16>(di, A(0), B(2), ID, acc0);
-                tc::mma_split<F16>(di, A(0), B(3), ID, 1);
-                tc::mma_split<F16>(di, A(1), B(2), ID, 1);
+                tc::mma_split<F16>(ei, A(0), B(3), ID, accs);
+                tc::mma_split<F16>(ei, A(1), B(2), ID, 1);
               } else {
                 tc::mma_split<F16>(dr, A(0), B(0), ID, acc0);
-                tc::mma_split<F16>(dr, A(0), B(1), ID, 1);
-                tc::mma_split<F16>(dr, A(1), B(0), ID, 1);
                 tc::mma_split<F16>(dr, A(2), B(2), IDN, 1);
-                tc::mma_split<F16>(dr, A(2), B(3), IDN, 1);
-                tc::mma_split<F16>(dr, A(3), B(2), IDN, 1);
+                tc::mma_split<F16>(er, A(0), B(1), ID, accs);
+                tc::mma_split<F16>(er, A(1), B(0), ID, 1);
+                tc::mma_split<F16>(er, A(2), B(3), IDN, 1);
+                tc::mma_split<F16>(er, A(3), B(2), IDN, 1);
                 tc::mma_split<F16>(di, A(0), B(2), ID, acc0);
-                tc::mma_split<F16>(di, A(0), B(3), ID, 1);
-                tc::mma_split<F16>(di, A(1), B(2), ID, 1);
                 tc::mma_split<F16>(di, A(2), B(0), ID, 1);
-                tc::mma_split<F16>(di, A(2), B(1), ID, 1);
-                tc::mma_split<F16>(di, A(3), B(0), ID, 1);
+                tc::mma_split<F16>(ei, A(0), B(3), ID, accs);
+                tc::mma_split<F16>(ei, A(1), B(2), ID, 1);
+                tc::mma_split<F16>(ei, A(2), B(1), ID, 1);
+                tc::mma_split<F16>(ei, A(3), B(0), ID, 1);
               }
             }
             tc::mma_commit(&empty[s]);
@@ -477,8 +549,8 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
       float* __restrict__ const d3 = static_cast<float*>(dst[3]);
       const long wb = long(w) * p.pl_bs;
       for (int mt = 0; mt < MT; ++mt) {
-        if (!tc::mbar_wait(&acc_full[sl * 2 + mt], unsigned(sl ? use1 : use0) & 1u, p.err,
-                           abort_flag)) {
+        if (!tc::mbar_wait_warp(&acc_full[sl * 2 + mt], unsigned(sl ? use1 : use0) & 1u, p.err,
+                                abort_flag)) {
           ok = false;
           break;
         }
@@ -490,11 +562,26 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
         // element (n, i) of the [w][n][i] planes: off + n * pl_ld
         const long off = wb + row;
         c128* Sw = p.S + long(w) * p.ldS + long(row) * N;
+        // the running sum's columns in tensor memory (sum_tmem): this lane quarter's rows
+        const uint32_t tsum = taddr + (uint32_t(q * 32) << 16) + uint32_t(256 + mt * 2 * TBN);
 #pragma unroll 1
         for (int c0 = 0; c0 < TBN; c0 += 16) {
+          if (c0 >= N) {
+            // no electron column in this chunk: only free the accumulator
+            if (c0 + 16 >= TBN) {
+              tc::tc_fence_before();
+              tc::mbar_arrive(&acc_empty[sl * 2 + mt]);
+            }
+            continue;
+          }
           // running-sum loads of this chunk first, then the accumulator columns
           float sr[16], si[16];
-          if (rok && taylor) {
+          if (p.sum_tmem) {
+            if (taylor) {  // tensor-memory loads are warp-collective: every lane takes part
+              tc::tmem_ld16(tsum + c0, sr);
+              tc::tmem_ld16(tsum + TBN + c0, si);
+            }
+          } else if (rok && taylor) {
 #pragma unroll
             for (int j = 0; j < 16; ++j)
               if (c0 + j < N) {
@@ -505,13 +592,23 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
           float vr[16], vi[16];
           tc::tmem_ld16(tacc + c0, vr);
           tc::tmem_ld16(tacc + TBN + c0, vi);
+          if (p.dual) {  // + the small products' accumulator (FP32 add, rounded to nearest)
+            float wr[16], wi[16];
+            tc::tmem_ld16(tacc + 256 + c0, wr);
+            tc::tmem_ld16(tacc + 256 + TBN + c0, wi);
+            tc::tmem_ld_wait();
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              vr[j] += wr[j];
+              vi[j] += wi[j];
+            }
+          }
           tc::tmem_ld_wait();
           if (c0 + 16 >= TBN) {
             // the accumulator is free for this slot's next phase
             tc::tc_fence_before();
             tc::mbar_arrive(&acc_empty[sl * 2 + mt]);
           }
-          if (!rok || c0 >= N) continue;
           if (taylor) {
             // x = (i/ph) * acc
 #pragma unroll
@@ -524,6 +621,7 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
           }
           if (last_phase) {
             // S = P1 R  (complex128 walker matrix [M][N])
+            if (!rok) continue;
 #pragma unroll
             for (int j = 0; j < 16; ++j)
               if (c0 + j < N) Sw[c0 + j] = cmk(vr[j], vi[j]);
@@ -536,17 +634,30 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
               si[j] = 0.f;
             }
           }
+          float ur[16], ui[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            ur[j] = sr[j] + vr[j];
+            ui[j] = si[j] + vi[j];
+          }
+          if (p.sum_tmem && !last_term) {
+            tc::tmem_st16(tsum + c0, ur);
+            tc::tmem_st16(tsum + TBN + c0, ui);
+            tc::tmem_st_wait();
+          }
+          if (!rok) continue;
 #pragma unroll
           for (int j = 0; j < 16; ++j)
             if (c0 + j < N) {
               const long idx = off + long(c0 + j) * pl_ld;
-              const float ur = sr[j] + vr[j], ui = si[j] + vi[j];
               if (last_term) {
-                split_store(ur, d0, d1, idx);
-                split_store(ui, d2, d3, idx);
+                split_store(ur[j], d0, d1, idx);
+                split_store(ui[j], d2, d3, idx);
               } else {
-                sum_r[idx] = ur;
-                sum_i[idx] = ui;
+                if (!p.sum_tmem) {
+                  sum_r[idx] = ur[j];
+                  sum_i[idx] = ui[j];
+                }
                 split_store(vr[j], d0, d1, idx);
                 split_store(vi[j], d2, d3, idx);
               }
@@ -581,8 +692,8 @@ int make_plane_map_3d_es(CUtensorMap* map, const void* base, int esize, long k, 
 int taylor_fused_tc(cudaStream_t s, int esize, const void* const P1p[2], const void* const Vp[4],
                     long ldV, const void* const Sp[4], void* const Tp0[4], void* const Tp1[4],
                     void* const Rp[4], float* const sum[2], long pl_ld, c128* S, long ldS, int W,
-                    int M, int N, int order, int nslots, const float* v_inv, const float* s_inv,
-                    float p1_inv, unsigned* err) {
+                    int M, int N, int order, int nslots, int one_slot_use,
+                    const float* v_inv, const float* s_inv, float p1_inv, unsigned* err) {
   if (M > 256 || N > TBN || order < 0) {
     set_error_detail("taylor_fused_tc: M = %d (<= 256), N = %d (<= 64), order = %d", M, N, order);
     return AFQMC_ERR_UNSUPPORTED;
@@ -635,6 +746,10 @@ int taylor_fused_tc(cudaStream_t s, int esize, const void* const P1p[2], const v
   // nslots = 0: two walkers in flight per CTA once every CTA has two, else one
   if (nslots <= 0) nslots = (W >= 2 * g_nsm) ? 2 : 1;
   p.nslots = nslots > 1 ? 2 : 1;
+  // with one walker in flight, columns 256..511 are free: for the small products' accumulator
+  // (one_slot_use 0) or for the running sum (1)
+  p.dual = (p.nslots == 1 && one_slot_use == 0) ? 1 : 0;
+  p.sum_tmem = (p.nslots == 1 && one_slot_use == 1) ? 1 : 0;
   const int grid = W < g_nsm ? W : g_nsm;
   kern<<<grid, TY_THREADS, T_SMEM, s>>>(p);
   return launch_status("taylor_tc_kernel");

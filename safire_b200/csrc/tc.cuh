@@ -70,6 +70,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsign
   }
 }
 
+// The same wait for a whole warp, with one outcome for all its lanes: the epilogue warps follow a
+// wait with warp-collective tensor-memory loads, which every lane must take part in.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, unsigned parity, unsigned* err,
+                                               volatile int* abort) {
+  const bool ok = mbar_wait(bar, parity, err, abort);
+  return __all_sync(0xffffffffu, ok) != 0;
+}
+
 // ---------------------------------------------------------------------------------------------
 // TMA
 // ---------------------------------------------------------------------------------------------
@@ -213,6 +221,23 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 }
 __device__ __forceinline__ void tmem_ld_wait() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// 32 lanes x 32 bits, 16 consecutive columns per thread (warp-collective)
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16};" ::"r"(taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+      "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+      "r"(__float_as_uint(v[15]))
+      : "memory");
+}
+__device__ __forceinline__ void tmem_st_wait() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
 // TF32 split: x = hi + lo with hi = x rounded to TF32 (10-bit mantissa, round to nearest) and

@@ -156,14 +156,15 @@ def _mixed_steps(wl, dham, fused, nsteps=2, order=None, split_format=1):
     return to_host(ws.SlaterMatrices(0)), to_host(ws.properties())
 
 
-@pytest.mark.parametrize("mode", [1, 2, 3])
+@pytest.mark.parametrize("mode", [2, 3, 6])
 @pytest.mark.parametrize("name,W,Nc,order", [("cfg1", 300, None, None), ("cfg1", 20, None, 0),
                                              ("cfg2", 6, 40, None), ("cfg1", 301, None, 3)])
 def test_taylor_fused_vs_per_term(cuda, name, W, Nc, order, mode):
     """The persistent Taylor kernel (all products of a walker in one CTA; mode 2 / 3: one / two
-    walkers in flight per CTA) against one GEMM launch per product: same split arithmetic (the
-    TF32 split, which both run), different kernels; W = 300, 301 run several walkers per CTA
-    (301: one slot ends early).  The FP16 split of the fused kernel is checked against complex128
+    walkers in flight per CTA; 2: the small products in a second accumulator; 6: the running sum
+    in tensor memory) against one GEMM launch per product: same split arithmetic (the TF32
+    split, which both run), different kernels and summation orders; W = 300, 301 run several
+    walkers per CTA (301: one slot ends early).  The FP16 split of the fused kernel is checked against complex128
     in test_gpu_mixed_full.py and below."""
     kw = {"W": W} if Nc is None else {"W": W, "Nc": Nc}
     wl = make_workload(name, **kw)
@@ -195,7 +196,8 @@ def test_autotune_leaves_the_run_unchanged(cuda):
         before = sim.wset.buffer.clone()
         if tune:
             best, ms = sim.autotune()
-            assert best in (0, 2, 3) and all(t > 0 for t in ms.values()), (best, ms)
+            assert best in (2, 4) and all(t > 0 for t in ms.values()), (best, ms)
+            assert set(ms) == {0, 2, 3, 4, 5, 6, 7}  # FP16 variants are tried on these shapes
             assert torch.equal(sim.wset.buffer, before)
             chosen = best
         else:
@@ -206,7 +208,7 @@ def test_autotune_leaves_the_run_unchanged(cuda):
     assert torch.equal(runs[0], runs[1])
 
 
-@pytest.mark.parametrize("mode", [2, 3])
+@pytest.mark.parametrize("mode", [4, 5, 7])
 @pytest.mark.parametrize("name,W,Nc,order", [("cfg1", 300, None, None), ("cfg1", 20, None, 0),
                                              ("cfg1", 301, None, 3)])
 def test_taylor_fused_fp16_vs_fp64(cuda, name, W, Nc, order, mode):

@@ -199,11 +199,12 @@ def _angle_err(a, b):
 
 
 @FORMATS
-@pytest.mark.parametrize("mode", [0, 2, 3])
+@pytest.mark.parametrize("mode", [0, 2, 3, 4, 5, 6, 7])
 def test_full_step(full, mode, fmt_set):
     """One propagation step from the same walkers with the same field uniforms: complex128 vs
-    mixed with the Taylor series as per-term GEMMs (0) or the persistent kernel with one (2) or
-    two (3) walkers in flight per CTA."""
+    mixed with the Taylor series as per-term GEMMs (0) or the persistent kernel with one (2, 4,
+    6, 7) or two (3, 5) walkers in flight per CTA, in the TF32 split (2, 3, 6) or the FP16 split
+    (4, 5, 7, which fall back to TF32 under the TF32 split format)."""
     from safire_b200 import afqmc as A
     wl, dham, owfn = full["wl"], full["dham"], full["owfn"]
     u = full["u"]
@@ -236,6 +237,7 @@ def test_full_step(full, mode, fmt_set):
     assert rel_err(r64["props"][:NO, O.WEIGHT], ows.props[:, O.WEIGHT]) < TOL_FP64
 
     e = {
+        "S_scale_bias": _scale_bias(rmx["S"], r64["S"]),
         "vbias": rel_err(rmx["vbias"], r64["vbias"]),
         "X": rel_err(rmx["X"], r64["X"]),
         "S": rel_err(rmx["S"], r64["S"]),
@@ -246,7 +248,8 @@ def test_full_step(full, mode, fmt_set):
         "phase": _angle_err(np.angle(rmx["props"][:, O.PHASE]),
                             np.angle(r64["props"][:, O.PHASE])),
     }
-    print(f"step W={W} taylor mode {mode} fmt {fmt_set}: " + ", ".join(f"{k} {v:.2e}" for k, v in e.items()))
+    print(f"step W={W} taylor mode {mode} fmt {fmt_set}: " +
+          ", ".join(f"{k} {v:.2e}" for k, v in e.items()))
     assert e["vbias"] < TOL_ONE and e["X"] < TOL_ONE
     assert e["S"] < TOL_STEP and e["S_oracle"] < TOL_STEP and e["weight"] < TOL_LOGOV
     assert e["log_ovlp_re"] < TOL_LOGOV and e["log_ovlp_im"] < TOL_STEP
