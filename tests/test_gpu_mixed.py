@@ -156,15 +156,16 @@ def _mixed_steps(wl, dham, fused, nsteps=2, order=None, split_format=1):
     return to_host(ws.SlaterMatrices(0)), to_host(ws.properties())
 
 
-@pytest.mark.parametrize("mode", [2, 3, 6])
+@pytest.mark.parametrize("mode", [3, 6])
 @pytest.mark.parametrize("name,W,Nc,order", [("cfg1", 300, None, None), ("cfg1", 20, None, 0),
                                              ("cfg2", 6, 40, None), ("cfg1", 301, None, 3)])
 def test_taylor_fused_vs_per_term(cuda, name, W, Nc, order, mode):
     """The persistent Taylor kernel (all products of a walker in one CTA; mode 2 / 3: one / two
-    walkers in flight per CTA; 2: the small products in a second accumulator; 6: the running sum
-    in tensor memory) against one GEMM launch per product: same split arithmetic (the TF32
-    split, which both run), different kernels and summation orders; W = 300, 301 run several
-    walkers per CTA (301: one slot ends early).  The FP16 split of the fused kernel is checked against complex128
+    walkers in flight per CTA; 6: one in flight with the running sum in tensor memory) against
+    one GEMM launch per product: the same split arithmetic (the TF32 split, one accumulator),
+    different kernels; W = 300, 301 run several walkers per CTA (301: one slot ends early).  The
+    modes with a second accumulator for the small products (2, 4) sum differently, more
+    accurately, and are checked against complex128 below.  The FP16 split of the fused kernel is checked against complex128
     in test_gpu_mixed_full.py and below."""
     kw = {"W": W} if Nc is None else {"W": W, "Nc": Nc}
     wl = make_workload(name, **kw)
@@ -208,19 +209,20 @@ def test_autotune_leaves_the_run_unchanged(cuda):
     assert torch.equal(runs[0], runs[1])
 
 
-@pytest.mark.parametrize("mode", [4, 5, 7])
+@pytest.mark.parametrize("mode", [2, 4, 5, 7])
 @pytest.mark.parametrize("name,W,Nc,order", [("cfg1", 300, None, None), ("cfg1", 20, None, 0),
                                              ("cfg1", 301, None, 3)])
 def test_taylor_fused_fp16_vs_fp64(cuda, name, W, Nc, order, mode):
-    """The persistent Taylor kernel in the FP16 split (operands and every term scaled by powers of
-    two) against complex128 propagation on the same walkers and fields: walkers within the
-    one-step bound of the mixed path (1e-4), log-overlaps within 1e-3 (the log-det sums the
+    """The persistent Taylor kernel with a second accumulator for the small split products (2:
+    TF32 split, 4: FP16 split) and in the FP16 split (4, 5, 7; operands and every term scaled by
+    powers of two) against complex128 propagation on the same walkers and fields: walkers within
+    the one-step bound of the mixed path (1e-4), log-overlaps within 1e-3 (the log-det sums the
     walkers' error over the electrons)."""
     from safire_b200 import afqmc as A
     kw = {"W": W} if Nc is None else {"W": W, "Nc": Nc}
     wl = make_workload(name, **kw)
     dham, _, _ = make_pair(wl)
-    Sf, pf = _mixed_steps(wl, dham, mode, order=order, split_format=2)
+    Sf, pf = _mixed_steps(wl, dham, mode, order=order, split_format=1 if mode == 2 else 2)
     ws = A.WalkerSet(wl.walker_type, wl.M, wl.nup, wl.ndn, W)
     ws.init_from_trial(dham)
     kwp = {} if order is None else {"taylor_n": order}
@@ -232,7 +234,7 @@ def test_taylor_fused_fp16_vs_fp64(cuda, name, W, Nc, order, mode):
     S64, p64 = to_host(ws.SlaterMatrices(0)), to_host(ws.properties())
     eS = rel_err(Sf, S64)
     eO = float(np.max(np.abs(pf[:, O.OVLP] - p64[:, O.OVLP])))
-    print(f"fused FP16 ({mode}) vs complex128 ({name}, W={W}, order={order}): S {eS:.2e} "
+    print(f"fused ({mode}) vs complex128 ({name}, W={W}, order={order}): S {eS:.2e} "
           f"log-ovlp {eO:.2e}")
     assert eS < TOL_STEP and eO < 1e-3
     assert dham.device_error_flag() == 0
