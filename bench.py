@@ -518,7 +518,9 @@ def _roofline(sim, wl, W, prec, phases, args, torch, taylor_mode=1):
         t_launch = x0.elapsed_time(x1) / reps
         del G, E
         kernel = f"exchange_tc_kernel<{args.exchange_split}> (fused EXX/EJ contraction)"
-        traffic, traffic_src = _EXCHANGE_TRAFFIC(W, Nc, N, M)
+        traffic, traffic_src = _EXCHANGE_TRAFFIC(W, Nc, N, M, 2 if f16 else 4)
+    if top == "propagate" and prec == A.PREC_MIXED:
+        traffic, traffic_src = _TAYLOR_TRAFFIC(W, M, N, taylor_mode)
     achieved = algo[top] / (t_launch / 1000) / 1e12
     mma = issued[top] / (t_launch / 1000) / 1e12
     return {"kernel": kernel, "bound": "tensor", "achieved": achieved, "peak": peak,
@@ -529,19 +531,33 @@ def _roofline(sim, wl, W, prec, phases, args, torch, taylor_mode=1):
             "mma_flops_per_launch": issued[top], "block_share_ms": block_share}
 
 
-def _EXCHANGE_TRAFFIC(W, Nc, N, M):
+def _EXCHANGE_TRAFFIC(W, Nc, N, M, esize=2):
     """DRAM bytes per launch of exchange_tc_kernel<3>: ncu (dram__bytes_read.sum +
-    dram__bytes_write.sum) at the bench's 1024 walkers read 2.316 GB and wrote 55.6 MB.  The
-    tile order keeps the Lnak planes of 64 vector pairs in L2 while every walker pair passes, so
-    the reads are the Lnak planes once plus every walker's G planes once per 64-pair block, and
-    the writes the two complex sums per (walker, vector); other walker counts scale by that."""
+    dram__bytes_write.sum) at the bench's 1024 walkers read 1.162 GB and wrote 53.9 MB with FP16
+    split planes (esize 2; 2.316 GB and 55.6 MB with TF32 planes).  The tile order keeps the Lnak
+    planes of 64 vector pairs in L2 while every walker pair passes, so the reads are the Lnak
+    planes once plus every walker's G planes once per 64-pair block, and the writes the two
+    complex sums per (walker, vector); other walker counts scale by that."""
+    src = "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch at 1024 walkers"
     if (W, Nc, N, M) == (1024, 1600, 50, 200):
-        return 2315739136 + 55630080, "ncu dram__bytes_read.sum + dram__bytes_write.sum, " \
-                                      "one launch at 1024 walkers"
+        return (1161931776 + 53940480 if esize == 2 else 2315739136 + 55630080), src
     blocks = -(-((Nc + 1) // 2) // 64)
-    return (2 * Nc * N * M * 4 + W * (4 * N * M * 4) * blocks + W * Nc * 32,
-            "ncu dram__bytes_read.sum + dram__bytes_write.sum at 1024 walkers (2.371 GB per "
-            "launch), by the tile-order model at other walker counts")
+    return (2 * Nc * N * M * esize + W * (4 * N * M * esize) * blocks + W * Nc * 32,
+            src + " scaled by the tile-order model to other walker counts")
+
+
+def _TAYLOR_TRAFFIC(W, M, N, taylor_mode):
+    """DRAM bytes per launch of taylor_tc_kernel: ncu (dram__bytes_read.sum +
+    dram__bytes_write.sum) of the second launch at the bench's 1024 walkers, FP16 split with the
+    second accumulator (mode 4): 571.4 MB read, 623.3 MB written, against 574 MB of compulsory
+    traffic (V planes 328 MB and S planes 82 MB read once, S 164 MB written).  The excess writes
+    are the terms' planes and the FP32 running sum leaving L2.  Other walker counts scale with
+    the walkers."""
+    if (M, N) != (200, 50) or taylor_mode != 4:
+        return None, None
+    return (571442944 + 623287040) * W // 1024, \
+        "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch at 1024 walkers " \
+        "(taylor mode 4), scaled by the walkers"
 
 
 def _mixed_dtype(split_f16, taylor_mode, exchange_split):

@@ -22,7 +22,7 @@
 // one scale; V and S one scale per walker), twice the tensor rate and half the bytes of TF32.
 // The epilogue turns each accumulator into the term's true values with the operands' inverse
 // scales, and stores each term T_n (and R) in planes of its own scale: a first pass over the
-// walker's accumulators (both 128-row tiles) finds the largest |value|, the four epilogue warps
+// walker's accumulators (both 128-row tiles) finds the largest |value|, the epilogue warps
 // agree on it through shared memory, and a second pass scales, splits and stores.  The running
 // sum stays FP32 in true values.
 #include "mixed.cuh"
@@ -31,7 +31,10 @@
 namespace afqmc {
 namespace {
 
-constexpr int TY_THREADS = 192;  // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+// warp 0 TMA, warp 1 MMA, then EPW epilogue warps: EPW / 4 per TMEM lane quarter, which split
+// the accumulator columns between them in chunks of 16 * 4 / EPW
+constexpr int TY_EPW = 8;
+__host__ __device__ constexpr int ty_threads(int epw) { return 64 + 32 * epw; }
 constexpr int TBK = 32;
 constexpr int TBN = 64;           // electrons per tile (N <= 64)
 constexpr int T_STAGES = 2;
@@ -123,24 +126,27 @@ struct Schedule {
   }
 };
 
-// Epilogue of the FP16 form (warps 2-5).  Per (slot, walker, phase): pass 1 reads the walker's
-// accumulators (both 128-row tiles) and finds the largest |value| of what the phase stores (the
-// new term, or R = sum + T_order for the last term); the four warps exchange their maxima and
+// Epilogue of the FP16 form (the EPW warps from warp 2).  Per (slot, walker, phase): pass 1 reads
+// the walker's accumulators (both 128-row tiles) and finds the largest |value| of what the phase
+// stores (the new term, or R = sum + T_order for the last term); the warps exchange their maxima and
 // failure flags through shared memory between two named barriers, so that they agree on the
 // scale and on whether to go on (a bounded wait that gave up ends every warp's loop at the same
 // point); pass 2 reads the accumulators again, frees them, and stores.  Values are true values
 // (the accumulator times the operands' inverse scales); the planes hold them times 2^e.
+template <int EPW>
 __device__ __forceinline__ void taylor_epilogue_f16(const TyParams& p, uint32_t taddr,
                                                     uint64_t* acc_full, uint64_t* acc_empty,
                                                     uint64_t* phase_done,
                                                     volatile int* abort_flag, float* red,
                                                     int warp, int lane) {
+  constexpr int NH = EPW / 4, CW = 16 / NH, NT = 32 * EPW;
   const int q = warp & 3;
+  const int h = (warp - 2) >> 2;  // which of the quarter's warps: columns c0 = CW * h + CW * NH * k
   const int N = p.N, M = p.M, nph = p.order + 2, MT = (M + 127) / 128;
   const long pl_ld = p.pl_ld;
   float* __restrict__ const sum_r = p.sum[0];
   float* __restrict__ const sum_i = p.sum[1];
-  int* const redf = reinterpret_cast<int*>(red + 4);
+  int* const redf = reinterpret_cast<int*>(red + EPW);
   Schedule sc(p.W, nph, blockIdx.x, gridDim.x, p.nslots);
   long use0 = 0, use1 = 0;
   float pinv0 = 1.f, pinv1 = 1.f;  // inverse scale of the planes each slot stored last
@@ -161,23 +167,23 @@ __device__ __forceinline__ void taylor_epilogue_f16(const TyParams& p, uint32_t 
 
     // the true values of accumulator chunk (mt, c0), with the running sum when `with_sum`
     auto values = [&](uint32_t tacc, int c0, float* xr, float* xi) {
-      float vr[16], vi[16];
-      tc::tmem_ld16(tacc + c0, vr);
-      tc::tmem_ld16(tacc + TBN + c0, vi);
+      float vr[CW], vi[CW];
+      tc::tmem_ld<CW>(tacc + c0, vr);
+      tc::tmem_ld<CW>(tacc + TBN + c0, vi);
       if (p.dual) {  // + the small products' accumulator (FP32 add, rounded to nearest)
-        float wr[16], wi[16];
-        tc::tmem_ld16(tacc + 256 + c0, wr);
-        tc::tmem_ld16(tacc + 256 + TBN + c0, wi);
+        float wr[CW], wi[CW];
+        tc::tmem_ld<CW>(tacc + 256 + c0, wr);
+        tc::tmem_ld<CW>(tacc + 256 + TBN + c0, wi);
         tc::tmem_ld_wait();
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
+        for (int j = 0; j < CW; ++j) {
           vr[j] += wr[j];
           vi[j] += wi[j];
         }
       }
       tc::tmem_ld_wait();
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
+      for (int j = 0; j < CW; ++j) {
         if (taylor) {
           xr[j] = -ai * (vi[j] * f_in);
           xi[j] = ai * (vr[j] * f_in);
@@ -201,31 +207,35 @@ __device__ __forceinline__ void taylor_epilogue_f16(const TyParams& p, uint32_t 
         const uint32_t tsum = taddr + (uint32_t(q * 32) << 16) + uint32_t(256 + mt * 2 * TBN);
         const long off = wb + row;
 #pragma unroll 1
-        for (int c0 = 0; c0 < TBN; c0 += 16) {
+        for (int c0 = CW * h; c0 < TBN; c0 += CW * NH) {
           if (c0 >= N) continue;
-          float xr[16], xi[16];
-          values(tacc, c0, xr, xi);
-          float sr[16], si[16];
           const bool add_sum = last_term && taylor;
+          float sr[CW], si[CW];
+          if (add_sum && !p.sum_tmem && row < M) {
+            // the running sum from global memory, in flight while the accumulator is read
+#pragma unroll
+            for (int j = 0; j < CW; ++j)
+              if (c0 + j < N) {
+                const long idx = off + long(c0 + j) * pl_ld;
+                sr[j] = sum_r[idx];
+                si[j] = sum_i[idx];
+              }
+          }
+          float xr[CW], xi[CW];
+          values(tacc, c0, xr, xi);
           if (add_sum && p.sum_tmem) {  // warp-collective: before any per-row branch
-            tc::tmem_ld16(tsum + c0, sr);
-            tc::tmem_ld16(tsum + TBN + c0, si);
+            tc::tmem_ld<CW>(tsum + c0, sr);
+            tc::tmem_ld<CW>(tsum + TBN + c0, si);
             tc::tmem_ld_wait();
           }
           if (row >= M) continue;
 #pragma unroll
-          for (int j = 0; j < 16; ++j)
+          for (int j = 0; j < CW; ++j)
             if (c0 + j < N) {
               float ur = xr[j], ui = xi[j];
               if (add_sum) {
-                if (p.sum_tmem) {
-                  ur += sr[j];
-                  ui += si[j];
-                } else {
-                  const long idx = off + long(c0 + j) * pl_ld;
-                  ur += sum_r[idx];
-                  ui += sum_i[idx];
-                }
+                ur += sr[j];
+                ui += si[j];
               }
               mx = fmaxf(mx, fmaxf(fabsf(ur), fabsf(ui)));
             }
@@ -236,13 +246,18 @@ __device__ __forceinline__ void taylor_epilogue_f16(const TyParams& p, uint32_t 
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     if (lane == 0) {
-      red[q] = mx;
-      redf[q] = ok ? 0 : 1;
+      red[warp - 2] = mx;
+      redf[warp - 2] = ok ? 0 : 1;
     }
-    named_bar_sync(1, 128);
-    const float m4 = fmaxf(fmaxf(red[0], red[1]), fmaxf(red[2], red[3]));
-    const int fail = redf[0] | redf[1] | redf[2] | redf[3];
-    named_bar_sync(1, 128);  // red is rewritten only after every warp has read it
+    named_bar_sync(1, NT);
+    float m4 = 0.f;
+    int fail = 0;
+#pragma unroll
+    for (int k = 0; k < EPW; ++k) {
+      m4 = fmaxf(m4, red[k]);
+      fail |= redf[k];
+    }
+    named_bar_sync(1, NT);  // red is rewritten only after every warp has read it
     if (fail) break;
     const int e = tc::f16_scale_exponent(m4);
     const float osc = ldexpf(1.f, e);
@@ -262,26 +277,37 @@ __device__ __forceinline__ void taylor_epilogue_f16(const TyParams& p, uint32_t 
       const long off = wb + row;
       c128* Sw = p.S + long(w) * p.ldS + long(row) * N;
 #pragma unroll 1
-      for (int c0 = 0; c0 < TBN; c0 += 16) {
+      for (int c0 = CW * h; c0 < TBN; c0 += CW * NH) {
+        // this warp's last chunk of the accumulator frees it for the slot's next phase
+        const bool last_chunk = c0 + CW * NH >= TBN;
         if (c0 >= N) {
           // no electron column in this chunk: only free the accumulator
-          if (c0 + 16 >= TBN) {
+          if (last_chunk) {
             tc::tc_fence_before();
             tc::mbar_arrive(&acc_empty[sl * 2 + mt]);
           }
           continue;
         }
-        float xr[16], xi[16];
+        float sr[CW], si[CW];
+        if (!p.sum_tmem && taylor && rok) {
+          // the running sum from global memory, in flight while the accumulator is read
+#pragma unroll
+          for (int j = 0; j < CW; ++j)
+            if (c0 + j < N) {
+              const long idx = off + long(c0 + j) * pl_ld;
+              sr[j] = sum_r[idx];
+              si[j] = sum_i[idx];
+            }
+        }
+        float xr[CW], xi[CW];
         values(tacc, c0, xr, xi);
         // the running sum of this chunk (taylor phases), warp-collective in tensor memory
-        float sr[16], si[16];
         if (taylor && p.sum_tmem) {
-          tc::tmem_ld16(tsum + c0, sr);
-          tc::tmem_ld16(tsum + TBN + c0, si);
+          tc::tmem_ld<CW>(tsum + c0, sr);
+          tc::tmem_ld<CW>(tsum + TBN + c0, si);
           tc::tmem_ld_wait();
         }
-        if (c0 + 16 >= TBN) {
-          // the accumulator is free for this slot's next phase
+        if (last_chunk) {
           tc::tc_fence_before();
           tc::mbar_arrive(&acc_empty[sl * 2 + mt]);
         }
@@ -289,33 +315,24 @@ __device__ __forceinline__ void taylor_epilogue_f16(const TyParams& p, uint32_t 
           // S = P1 R  (complex128 walker matrix [M][N])
           if (!rok) continue;
 #pragma unroll
-          for (int j = 0; j < 16; ++j)
+          for (int j = 0; j < CW; ++j)
             if (c0 + j < N) Sw[c0 + j] = cmk(xr[j], xi[j]);
           continue;
         }
-        if (!p.sum_tmem && taylor && rok) {
+        float ur[CW], ui[CW];
 #pragma unroll
-          for (int j = 0; j < 16; ++j)
-            if (c0 + j < N) {
-              const long idx = off + long(c0 + j) * pl_ld;
-              sr[j] = sum_r[idx];
-              si[j] = sum_i[idx];
-            }
-        }
-        float ur[16], ui[16];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
+        for (int j = 0; j < CW; ++j) {
           ur[j] = taylor ? xr[j] + sr[j] : xr[j];
           ui[j] = taylor ? xi[j] + si[j] : xi[j];
         }
         if (p.sum_tmem && !last_term) {  // the new running sum, warp-collective
-          tc::tmem_st16(tsum + c0, ur);
-          tc::tmem_st16(tsum + TBN + c0, ui);
+          tc::tmem_st<CW>(tsum + c0, ur);
+          tc::tmem_st<CW>(tsum + TBN + c0, ui);
           tc::tmem_st_wait();
         }
         if (!rok) continue;
 #pragma unroll
-        for (int j = 0; j < 16; ++j)
+        for (int j = 0; j < CW; ++j)
           if (c0 + j < N) {
             const long idx = off + long(c0 + j) * pl_ld;
             if (last_term) {
@@ -334,10 +351,12 @@ __device__ __forceinline__ void taylor_epilogue_f16(const TyParams& p, uint32_t 
     }
     if (last_phase) {
       // the last phase has no pass 1: agree here on going on
-      if (lane == 0) redf[q] = ok ? 0 : 1;
-      named_bar_sync(1, 128);
-      const int fail2 = redf[0] | redf[1] | redf[2] | redf[3];
-      named_bar_sync(1, 128);
+      if (lane == 0) redf[warp - 2] = ok ? 0 : 1;
+      named_bar_sync(1, NT);
+      int fail2 = 0;
+#pragma unroll
+      for (int k = 0; k < EPW; ++k) fail2 |= redf[k];
+      named_bar_sync(1, NT);
       if (fail2) break;
     } else {
       // make this phase's planes visible to the TMA loads of the next phase
@@ -350,8 +369,10 @@ __device__ __forceinline__ void taylor_epilogue_f16(const TyParams& p, uint32_t 
   }
 }
 
-template <bool F16>
-__global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_constant__ TyParams p) {
+template <bool F16, int EPW>
+__global__ void __launch_bounds__(ty_threads(EPW), 1)
+    taylor_tc_kernel(const __grid_constant__ TyParams p) {
+  static_assert(EPW == 4 || EPW == 8, "four or eight epilogue warps");
   // 128 bytes of K per stage and operand row: 32 TF32 or 64 FP16 elements; 32 bytes per MMA
   constexpr int TBKE = F16 ? 2 * TBK : TBK;
   constexpr int KSTEP = F16 ? 16 : 8;
@@ -365,7 +386,7 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
   uint64_t* phase_done = acc_empty + 4;   // [slot] epilogue -> TMA: the phase's term is written
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(phase_done + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-  float* red = reinterpret_cast<float*>(tmem_slot + 2);  // [4] per-warp maxima (FP16 form)
+  float* red = reinterpret_cast<float*>(tmem_slot + 2);  // [EPW] per-warp maxima, [EPW] flags
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nph = p.order + 2;
@@ -380,10 +401,10 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
     }
     for (int b = 0; b < 4; ++b) {
       tc::mbar_init(&acc_full[b], 1);
-      tc::mbar_init(&acc_empty[b], 128);
+      tc::mbar_init(&acc_empty[b], 32 * EPW);
     }
-    tc::mbar_init(&phase_done[0], 128);
-    tc::mbar_init(&phase_done[1], 128);
+    tc::mbar_init(&phase_done[0], 32 * EPW);
+    tc::mbar_init(&phase_done[1], 32 * EPW);
     *abort_flag = 0;
     tc::fence_mbar_init();
   }
@@ -523,10 +544,14 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
       }
     }
   } else if constexpr (F16) {
-    taylor_epilogue_f16(p, taddr, acc_full, acc_empty, phase_done, abort_flag, red, warp, lane);
+    taylor_epilogue_f16<EPW>(p, taddr, acc_full, acc_empty, phase_done, abort_flag, red, warp,
+                             lane);
   } else {
-    // epilogue warps: TMEM lane quarter q = warp % 4, one accumulator row per thread
+    // epilogue warps: TMEM lane quarter q = warp % 4, one accumulator row per thread; the
+    // quarter's NH warps take the column chunks c0 = CW * h + CW * NH * k
+    constexpr int NH = EPW / 4, CW = 16 / NH;
     const int q = warp & 3;
+    const int h = (warp - 2) >> 2;
     const int N = p.N;
     const long pl_ld = p.pl_ld;
     float* __restrict__ const sum_r = p.sum[0];
@@ -565,46 +590,47 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
         // the running sum's columns in tensor memory (sum_tmem): this lane quarter's rows
         const uint32_t tsum = taddr + (uint32_t(q * 32) << 16) + uint32_t(256 + mt * 2 * TBN);
 #pragma unroll 1
-        for (int c0 = 0; c0 < TBN; c0 += 16) {
+        for (int c0 = CW * h; c0 < TBN; c0 += CW * NH) {
+          const bool last_chunk = c0 + CW * NH >= TBN;
           if (c0 >= N) {
             // no electron column in this chunk: only free the accumulator
-            if (c0 + 16 >= TBN) {
+            if (last_chunk) {
               tc::tc_fence_before();
               tc::mbar_arrive(&acc_empty[sl * 2 + mt]);
             }
             continue;
           }
           // running-sum loads of this chunk first, then the accumulator columns
-          float sr[16], si[16];
+          float sr[CW], si[CW];
           if (p.sum_tmem) {
             if (taylor) {  // tensor-memory loads are warp-collective: every lane takes part
-              tc::tmem_ld16(tsum + c0, sr);
-              tc::tmem_ld16(tsum + TBN + c0, si);
+              tc::tmem_ld<CW>(tsum + c0, sr);
+              tc::tmem_ld<CW>(tsum + TBN + c0, si);
             }
           } else if (rok && taylor) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j)
+            for (int j = 0; j < CW; ++j)
               if (c0 + j < N) {
                 sr[j] = sum_r[off + long(c0 + j) * pl_ld];
                 si[j] = sum_i[off + long(c0 + j) * pl_ld];
               }
           }
-          float vr[16], vi[16];
-          tc::tmem_ld16(tacc + c0, vr);
-          tc::tmem_ld16(tacc + TBN + c0, vi);
+          float vr[CW], vi[CW];
+          tc::tmem_ld<CW>(tacc + c0, vr);
+          tc::tmem_ld<CW>(tacc + TBN + c0, vi);
           if (p.dual) {  // + the small products' accumulator (FP32 add, rounded to nearest)
-            float wr[16], wi[16];
-            tc::tmem_ld16(tacc + 256 + c0, wr);
-            tc::tmem_ld16(tacc + 256 + TBN + c0, wi);
+            float wr[CW], wi[CW];
+            tc::tmem_ld<CW>(tacc + 256 + c0, wr);
+            tc::tmem_ld<CW>(tacc + 256 + TBN + c0, wi);
             tc::tmem_ld_wait();
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
+            for (int j = 0; j < CW; ++j) {
               vr[j] += wr[j];
               vi[j] += wi[j];
             }
           }
           tc::tmem_ld_wait();
-          if (c0 + 16 >= TBN) {
+          if (last_chunk) {
             // the accumulator is free for this slot's next phase
             tc::tc_fence_before();
             tc::mbar_arrive(&acc_empty[sl * 2 + mt]);
@@ -612,7 +638,7 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
           if (taylor) {
             // x = (i/ph) * acc
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
+            for (int j = 0; j < CW; ++j) {
               const float xr = -ai * vi[j];
               const float xi = ai * vr[j];
               vr[j] = xr;
@@ -623,31 +649,31 @@ __global__ void __launch_bounds__(TY_THREADS, 1) taylor_tc_kernel(const __grid_c
             // S = P1 R  (complex128 walker matrix [M][N])
             if (!rok) continue;
 #pragma unroll
-            for (int j = 0; j < 16; ++j)
+            for (int j = 0; j < CW; ++j)
               if (c0 + j < N) Sw[c0 + j] = cmk(vr[j], vi[j]);
             continue;
           }
           if (!taylor) {  // phase 0: the sum starts at T_0
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
+            for (int j = 0; j < CW; ++j) {
               sr[j] = 0.f;
               si[j] = 0.f;
             }
           }
-          float ur[16], ui[16];
+          float ur[CW], ui[CW];
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
+          for (int j = 0; j < CW; ++j) {
             ur[j] = sr[j] + vr[j];
             ui[j] = si[j] + vi[j];
           }
           if (p.sum_tmem && !last_term) {
-            tc::tmem_st16(tsum + c0, ur);
-            tc::tmem_st16(tsum + TBN + c0, ui);
+            tc::tmem_st<CW>(tsum + c0, ur);
+            tc::tmem_st<CW>(tsum + TBN + c0, ui);
             tc::tmem_st_wait();
           }
           if (!rok) continue;
 #pragma unroll
-          for (int j = 0; j < 16; ++j)
+          for (int j = 0; j < CW; ++j)
             if (c0 + j < N) {
               const long idx = off + long(c0 + j) * pl_ld;
               if (last_term) {
@@ -740,7 +766,7 @@ int taylor_fused_tc(cudaStream_t s, int esize, const void* const P1p[2], const v
   p.s_inv = s_inv;
   p.p1_inv = p1_inv;
   p.err = err;
-  auto kern = f16 ? taylor_tc_kernel<true> : taylor_tc_kernel<false>;
+  auto kern = f16 ? taylor_tc_kernel<true, TY_EPW> : taylor_tc_kernel<false, TY_EPW>;
   AFQMC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(T_SMEM)));
   // nslots = 0: two walkers in flight per CTA once every CTA has two, else one
@@ -751,7 +777,7 @@ int taylor_fused_tc(cudaStream_t s, int esize, const void* const P1p[2], const v
   p.dual = (p.nslots == 1 && one_slot_use == 0) ? 1 : 0;
   p.sum_tmem = (p.nslots == 1 && one_slot_use == 1) ? 1 : 0;
   const int grid = W < g_nsm ? W : g_nsm;
-  kern<<<grid, TY_THREADS, T_SMEM, s>>>(p);
+  kern<<<grid, ty_threads(TY_EPW), T_SMEM, s>>>(p);
   return launch_status("taylor_tc_kernel");
 }
 
