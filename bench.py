@@ -85,8 +85,8 @@ def parse():
                          "(taylor: three steps) one more call of the named operation "
                          "(step: a propagation step; vhs: HamiltonianOperations.vHS of the last "
                          "step's fields; exchange: the energy measurement); phmsd-energy: the "
-                         "PHMSD system with --walkers walkers (default 64), one Propagate and one "
-                         "energy evaluation")
+                         "PHMSD system with --walkers walkers (default 64) in --precision, one Propagate "
+                         "and one energy evaluation")
     return ap.parse_args()
 
 
@@ -102,7 +102,7 @@ def run_profile_case(args):
     if args.profile_case == "phmsd-energy":
         W = args.walkers if args.walkers != 1024 else 64
         wl, trial = make_phmsd_workload(W=W)
-        sim = Simulation.from_workload(wl, W=W, rp=rp, trial=trial)
+        sim = Simulation.from_workload(wl, W=W, rp=rp, trial=trial, precision=prec)
         sim.prop.Propagate(sim.wset, sim.Eshift)
         sim.wfn.Energy(sim.wset, set_properties=False)
     else:
@@ -549,13 +549,13 @@ def _EXCHANGE_TRAFFIC(W, Nc, N, M, esize=2):
 def _TAYLOR_TRAFFIC(W, M, N, taylor_mode):
     """DRAM bytes per launch of taylor_tc_kernel: ncu (dram__bytes_read.sum +
     dram__bytes_write.sum) of the second launch at the bench's 1024 walkers, FP16 split with the
-    second accumulator (mode 4): 571.4 MB read, 623.3 MB written, against 574 MB of compulsory
+    second accumulator (mode 4): 578.4 MB read, 626.5 MB written, against 574 MB of compulsory
     traffic (V planes 328 MB and S planes 82 MB read once, S 164 MB written).  The excess writes
     are the terms' planes and the FP32 running sum leaving L2.  Other walker counts scale with
     the walkers."""
     if (M, N) != (200, 50) or taylor_mode != 4:
         return None, None
-    return (571442944 + 623287040) * W // 1024, \
+    return (578384640 + 626533888) * W // 1024, \
         "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch at 1024 walkers " \
         "(taylor mode 4), scaled by the walkers"
 

@@ -154,7 +154,8 @@ class ExchangeControlVariate:
         D = 2 * self.Nc + 2 * self.N + (4 if scalars else 0) + (2 if lowrank else 0)
         self.mlp = ExchangeMLP(D, hidden, seed)
         self.fraction = fraction
-        self.rng = np.random.default_rng(seed)
+        self._seed = seed
+        self._gen = None  # device generator of the exact-evaluation draws
         self.X, self.y = [], []
         dev = sim.wset.buffer.device
         self._v = torch.empty((sim.wset.W, self.Nc), dtype=torch.complex128, device=dev)
@@ -210,16 +211,19 @@ class ExchangeControlVariate:
         if base is not None:
             f = base + f
         k = max(1, int(round(self.fraction * W)))
+        # the draws stay on the device (no host round trip between the launches)
+        if self._gen is None or self._gen.device != dev:
+            self._gen = torch.Generator(device=dev)
+            self._gen.manual_seed(self._seed)
         if self.sampling == "weight":
-            aw = w.abs().cpu().numpy()
+            aw = w.abs()
             prob = aw / aw.sum()
-            draws = self.rng.choice(W, size=k, replace=True, p=prob)
-            uniq, cnt = np.unique(draws, return_counts=True)
-            S = torch.as_tensor(uniq, device=dev)
-            # sum over draws of w_s (e_s - f_s) / (k p_s), evaluated once per distinct walker
-            scale = torch.as_tensor(cnt / (k * prob[uniq]), dtype=torch.float64, device=dev)
+            S = torch.multinomial(prob, k, replacement=True, generator=self._gen)
+            # sum over the draws of w_s (e_s - f_s) / (k p_s); a walker drawn twice is evaluated
+            # twice
+            scale = 1.0 / (k * prob[S])
         else:
-            S = torch.as_tensor(np.sort(self.rng.choice(W, size=k, replace=False)), device=dev)
+            S = torch.randperm(W, device=dev, generator=self._gen)[:k]
             scale = torch.full((k,), W / k, dtype=torch.float64, device=dev)
         Es = torch.empty((S.numel(), 3), dtype=torch.complex128, device=dev)
         sim.ham.energy(Es, G[S].contiguous(), addH1=False, addEJ=False, addEXX=True,
@@ -227,11 +231,12 @@ class ExchangeControlVariate:
         ex_mf = (w * f).sum() + (scale * w[S] * (Es[:, 1] - f[S])).sum()
         wsum = w.sum()
         e_other = (w * (E[:, 0] + E[:, 2])).sum()
-        out = {"exx_mf": complex((ex_mf / wsum).item())}
+        energy = ((e_other + ex_mf) / wsum).real
+        out = {"exx_mf": complex((ex_mf / wsum).item())}  # the first host read: all is enqueued
         if exact:
             Ea = torch.empty((W, 3), dtype=torch.complex128, device=dev)
             sim.ham.energy(Ea, G, addH1=True, addEJ=True, addEXX=True, precision=sim.precision)
             out["exx_exact"] = complex(((w * Ea[:, 1]).sum() / wsum).item())
             out["ej_exact"] = complex(((w * Ea[:, 2]).sum() / wsum).item())
             out["ej_from_vbias"] = complex(((w * E[:, 2]).sum() / wsum).item())
-        return float(((e_other + ex_mf) / wsum).real.item()), out
+        return float(energy.item()), out
