@@ -13,6 +13,7 @@
 // Z (pre-GELU, FP32) and A (post-GELU, BF16) [B][H].
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -32,6 +33,7 @@ using bf16 = __nv_bfloat16;
 constexpr int TMB = 128, TNB = 64, TKB = 64, MLP_THREADS = 128;
 constexpr int MA_TILE = TMB * 128, MB_TILE = TNB * 128, M_STAGE = MA_TILE + MB_TILE;
 constexpr size_t MLP_SMEM = 2 * size_t(M_STAGE) + 1024 + 64;
+constexpr int MLP_MAX_SPLIT = 4;
 
 __device__ __forceinline__ float gelu(float z) {
   return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
@@ -97,11 +99,14 @@ __device__ __forceinline__ void fill_tile(unsigned char* tile, int rows, int r0,
 // All 128 threads convert the next K chunk into the free stage while one thread's MMAs run on
 // the other (an mbarrier per stage tells when those MMAs have read it); the four warps then
 // read their 32 accumulator rows from tensor memory.  Waits are bounded (error word err).
+// Split K (gridDim.z > 1): CTA z sums the chunks [z per, (z + 1) per) and stores its partial
+// sum (EPI_STORE) at Cf + z * split_stride; splitk_reduce_kernel adds them in order.
 template <typename TA, typename TB, int EPI>
 __global__ void __launch_bounds__(MLP_THREADS, 1) mlp_gemm_kernel(
     int M, int N, int K, const TA* __restrict__ A, long sam, long sak, const TB* __restrict__ B,
     long sbk, long sbn, float* __restrict__ Cf, bf16* __restrict__ Cb, long ldc,
-    const float* __restrict__ bias, const float* __restrict__ Zin, unsigned* err) {
+    const float* __restrict__ bias, const float* __restrict__ Zin, long split_stride,
+    unsigned* err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -125,12 +130,16 @@ __global__ void __launch_bounds__(MLP_THREADS, 1) mlp_gemm_kernel(
   tc::tc_fence_after();
   const uint32_t taddr = *tmem_slot;
   constexpr uint32_t ID = idesc_bf16(TMB, TNB);
-  const int nk = (K + TKB - 1) / TKB;
-  for (int kc = 0; kc < nk; ++kc) {
-    const int s = kc & 1;
+  const int nk_all = (K + TKB - 1) / TKB;
+  const int per = (nk_all + int(gridDim.z) - 1) / int(gridDim.z);
+  const int kbeg = int(blockIdx.z) * per;
+  const int nk = max(0, min(nk_all, kbeg + per) - kbeg);  // this CTA's chunks
+  if (gridDim.z > 1) Cf += long(blockIdx.z) * split_stride;
+  for (int j = 0; j < nk; ++j) {
+    const int s = j & 1, kc = kbeg + j;
     unsigned char* st = base + s * M_STAGE;
-    // the MMAs of chunk kc - 2 read this stage
-    if (kc >= 2) tc::mbar_wait(&done[s], unsigned((kc - 2) >> 1) & 1u, err, abort_flag);
+    // the MMAs of chunk j - 2 read this stage
+    if (j >= 2) tc::mbar_wait(&done[s], unsigned((j - 2) >> 1) & 1u, err, abort_flag);
     fill_tile(st, TMB, m0, M, kc * TKB, K, A, sam, sak);
     fill_tile(st + MA_TILE, TNB, n0, N, kc * TKB, K, B, sbn, sbk);
     // the generic-proxy stores above become visible to the tensor core (async proxy)
@@ -143,7 +152,7 @@ __global__ void __launch_bounds__(MLP_THREADS, 1) mlp_gemm_kernel(
       for (int kk = 0; kk < 4; ++kk) {
         if (kc * TKB + kk * 16 >= K) break;
         mma_bf16(taddr, tc::sdesc_sw128(sa) + uint64_t(2 * kk), tc::sdesc_sw128(sb) + uint64_t(2 * kk),
-                 ID, (kc > 0 || kk > 0) ? 1u : 0u);
+                 ID, (j > 0 || kk > 0) ? 1u : 0u);
       }
       tc::mma_commit(&done[s]);
     }
@@ -155,6 +164,12 @@ __global__ void __launch_bounds__(MLP_THREADS, 1) mlp_gemm_kernel(
   // every thread takes the same branch: the tensor-memory loads below are warp-collective
   const bool ok = __syncthreads_and(mine) != 0;
   tc::tc_fence_after();
+  if (nk == 0 && gridDim.z > 1) {
+    // a split without chunks (K shorter than the splits): its partial sum is zero
+    const int m = m0 + warp * 32 + lane;
+    if (m < M)
+      for (int n = n0; n < min(N, n0 + TNB); ++n) Cf[long(m) * ldc + n] = 0.f;
+  }
   if (ok) {
     const int m = m0 + warp * 32 + lane;
     const uint32_t trow = taddr + (uint32_t(warp * 32) << 16);
@@ -185,6 +200,29 @@ __global__ void __launch_bounds__(MLP_THREADS, 1) mlp_gemm_kernel(
   tc::tc_fence_before();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(taddr, TNB);
+}
+
+// the split-K partial sums P[z][m][n] (z < nsplit, ld N) added in order, then the epilogue
+template <int EPI>
+__global__ void splitk_reduce_kernel(const float* __restrict__ P, int nsplit, int M, int N,
+                                     float* __restrict__ Cf, bf16* __restrict__ Cb, long ldc,
+                                     const float* __restrict__ bias,
+                                     const float* __restrict__ Zin) {
+  const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= long(M) * N) return;
+  const int m = int(i / N), n = int(i - long(m) * N);
+  float x = 0.f;
+  for (int z = 0; z < nsplit; ++z) x += P[long(z) * M * N + i];
+  const long o = long(m) * ldc + n;
+  if (EPI == EPI_STORE) {
+    Cf[o] = x;
+  } else if (EPI == EPI_BIAS_GELU) {
+    x += bias[n];
+    Cf[o] = x;
+    Cb[o] = __float2bfloat16(gelu(x));
+  } else {
+    Cb[o] = __float2bfloat16(x * gelu_grad(Zin[o]));
+  }
 }
 
 // Xn[b][d] = bf16((X[b][d] - mean[d]) * istd[d])
@@ -342,6 +380,8 @@ struct afqmc_mlp_s {
   // batch workspace (cap rows)
   bf16 *Xn = nullptr, *A1 = nullptr, *A2 = nullptr, *dZ2 = nullptr, *dZ1 = nullptr;
   float *Z1 = nullptr, *Z2 = nullptr, *y = nullptr, *dy = nullptr, *loss = nullptr;
+  float* ws = nullptr;  // split-K partial sums (ws_cap floats)
+  long ws_cap = 0;
   unsigned* err = nullptr;  // bounded-wait error word of the GEMM kernels (bit 0: timeout)
   long nparam() const { return long(H) * D + H + long(H) * H + H + H + 1; }
   long oW1() const { return 0; }
@@ -352,11 +392,12 @@ struct afqmc_mlp_s {
   long ob3() const { return ow3() + H; }
   void free_batch() {
     for (void* p : {(void*)Xn, (void*)A1, (void*)A2, (void*)dZ2, (void*)dZ1, (void*)Z1,
-                    (void*)Z2, (void*)y, (void*)dy})
+                    (void*)Z2, (void*)y, (void*)dy, (void*)ws})
       if (p) cudaFree(p);
     Xn = A1 = A2 = dZ2 = dZ1 = nullptr;
-    Z1 = Z2 = y = dy = nullptr;
+    Z1 = Z2 = y = dy = ws = nullptr;
     cap = 0;
+    ws_cap = 0;
   }
   ~afqmc_mlp_s() {
     int prev = 0;
@@ -386,21 +427,54 @@ int mlp_batch(afqmc_mlp h, int B) {
   AFQMC_CUDA_TRY(cudaMalloc(&h->Z2, sizeof(float) * bh));
   AFQMC_CUDA_TRY(cudaMalloc(&h->y, sizeof(float) * B));
   AFQMC_CUDA_TRY(cudaMalloc(&h->dy, sizeof(float) * B));
+  // split-K partial sums of the GEMMs with few output tiles: up to MLP_MAX_SPLIT x (B or H) x H
+  h->ws_cap = long(MLP_MAX_SPLIT) * std::max(B, h->H) * h->H;
+  AFQMC_CUDA_TRY(cudaMalloc(&h->ws, sizeof(float) * size_t(h->ws_cap)));
   h->cap = B;
   return AFQMC_OK;
 }
 
+int g_mlp_sms = 0;
+
+// C = epilogue(A B).  With fewer output tiles than half the SMs and a long K, the K range is
+// split over up to MLP_MAX_SPLIT CTAs per tile whose partial sums (in the handle's workspace) a
+// second kernel adds in a fixed order: deterministic, and the SMs stay busy.
 template <typename TA, typename TB, int EPI>
-int gemm(cudaStream_t s, unsigned* err, int M, int N, int K, const TA* A, long sam, long sak,
+int gemm(afqmc_mlp h, cudaStream_t s, int M, int N, int K, const TA* A, long sam, long sak,
          const TB* B, long sbk, long sbn, float* Cf, bf16* Cb, long ldc,
          const float* bias = nullptr, const float* Zin = nullptr) {
   if (M <= 0 || N <= 0) return AFQMC_OK;
+  if (g_mlp_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_mlp_sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  dim3 grid((N + TNB - 1) / TNB, (M + TMB - 1) / TMB);
+  const long tiles = long(grid.x) * grid.y;
+  const int nk = (K + TKB - 1) / TKB;
+  int nsplit = 1;
+  if (2 * tiles < g_mlp_sms && nk >= 8) {
+    nsplit = int(std::min<long>(MLP_MAX_SPLIT, g_mlp_sms / tiles));
+    nsplit = std::min(nsplit, nk / 4);
+    if (long(nsplit) * M * N > h->ws_cap) nsplit = 1;
+  }
+  if (nsplit > 1) {
+    auto kern = mlp_gemm_kernel<TA, TB, EPI_STORE>;
+    AFQMC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(MLP_SMEM)));
+    grid.z = nsplit;
+    kern<<<grid, MLP_THREADS, MLP_SMEM, s>>>(M, N, K, A, sam, sak, B, sbk, sbn, h->ws, nullptr, N,
+                                             nullptr, nullptr, long(M) * N, h->err);
+    AFQMC_TRY(launch_status("mlp_gemm_kernel"));
+    splitk_reduce_kernel<EPI><<<grid1(long(M) * N, 256), 256, 0, s>>>(h->ws, nsplit, M, N, Cf,
+                                                                      Cb, ldc, bias, Zin);
+    return launch_status("splitk_reduce_kernel");
+  }
   auto kern = mlp_gemm_kernel<TA, TB, EPI>;
   AFQMC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(MLP_SMEM)));
-  dim3 grid((N + TNB - 1) / TNB, (M + TMB - 1) / TMB);
   kern<<<grid, MLP_THREADS, MLP_SMEM, s>>>(M, N, K, A, sam, sak, B, sbk, sbn, Cf, Cb, ldc, bias,
-                                           Zin, err);
+                                           Zin, 0, h->err);
   return launch_status("mlp_gemm_kernel");
 }
 
@@ -410,10 +484,10 @@ int mlp_forward(afqmc_mlp h, const float* X, int B, cudaStream_t s) {
   standardize_kernel<<<grid1(long(B) * D, 256), 256, 0, s>>>(X, h->mean, h->istd, B, D, h->Xn);
   AFQMC_TRY(launch_status("standardize_kernel"));
   // Z1 = Xn W1^T + b1
-  AFQMC_TRY((gemm<bf16, bf16, EPI_BIAS_GELU>(s, h->err, B, H, D, h->Xn, D, 1, h->Pb + h->oW1(), 1, D,
+  AFQMC_TRY((gemm<bf16, bf16, EPI_BIAS_GELU>(h, s, B, H, D, h->Xn, D, 1, h->Pb + h->oW1(), 1, D,
                                              h->Z1, h->A1, H, h->P + h->ob1())));
   // Z2 = A1 W2^T + b2
-  AFQMC_TRY((gemm<bf16, bf16, EPI_BIAS_GELU>(s, h->err, B, H, H, h->A1, H, 1, h->Pb + h->oW2(), 1, H,
+  AFQMC_TRY((gemm<bf16, bf16, EPI_BIAS_GELU>(h, s, B, H, H, h->A1, H, 1, h->Pb + h->oW2(), 1, H,
                                              h->Z2, h->A2, H, h->P + h->ob2())));
   return AFQMC_OK;
 }
@@ -431,15 +505,15 @@ int mlp_backward(afqmc_mlp h, int B, cudaStream_t s) {
                                                                H, h->dZ2);
   AFQMC_TRY(launch_status("head_backward_kernel"));
   // dW2 = dZ2^T A1, db2 = column sums of dZ2
-  AFQMC_TRY((gemm<bf16, bf16, EPI_STORE>(s, h->err, H, H, B, h->dZ2, 1, H, h->A1, H, 1, g + h->oW2(),
+  AFQMC_TRY((gemm<bf16, bf16, EPI_STORE>(h, s, H, H, B, h->dZ2, 1, H, h->A1, H, 1, g + h->oW2(),
                                          nullptr, H)));
   column_sum_kernel<bf16><<<grid1(H, 128), 128, 0, s>>>(h->dZ2, nullptr, B, H, g + h->ob2());
   AFQMC_TRY(launch_status("column_sum_kernel"));
   // dZ1 = (dZ2 W2) gelu'(Z1)
-  AFQMC_TRY((gemm<bf16, bf16, EPI_GELU_GRAD>(s, h->err, B, H, H, h->dZ2, H, 1, h->Pb + h->oW2(), H, 1,
+  AFQMC_TRY((gemm<bf16, bf16, EPI_GELU_GRAD>(h, s, B, H, H, h->dZ2, H, 1, h->Pb + h->oW2(), H, 1,
                                              nullptr, h->dZ1, H, nullptr, h->Z1)));
   // dW1 = dZ1^T Xn, db1 = column sums of dZ1
-  AFQMC_TRY((gemm<bf16, bf16, EPI_STORE>(s, h->err, H, D, B, h->dZ1, 1, H, h->Xn, D, 1, g + h->oW1(),
+  AFQMC_TRY((gemm<bf16, bf16, EPI_STORE>(h, s, H, D, B, h->dZ1, 1, H, h->Xn, D, 1, g + h->oW1(),
                                          nullptr, D)));
   column_sum_kernel<bf16><<<grid1(H, 128), 128, 0, s>>>(h->dZ1, nullptr, B, H, g + h->ob1());
   return launch_status("column_sum_kernel");

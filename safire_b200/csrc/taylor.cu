@@ -705,6 +705,383 @@ __global__ void __launch_bounds__(ty_threads(EPW), 1)
   if (warp == 1) tc::tmem_dealloc(taddr, 512);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Interleaved form (FP16 split, second accumulator).  Two walkers in flight per CTA, interleaved
+// at row-tile granularity: a slot owns 256 TMEM columns that hold ONE 128-row tile of its
+// walker's phase (hi*hi products in (dr, di), the small split products in (er, ei)), and the
+// tensor core alternates between the slots' tiles, so that one slot's epilogue (and its
+// phase-to-phase hand-off through global memory) overlaps the other slot's MMAs.
+// The epilogue makes one pass: the power-of-two scale of the planes it stores comes from a
+// bound known before the phase,
+//   T_0 = P1 S:            |T_0| <= M |P1|max |S|max
+//   T_n = (i/n) V T_{n-1}: |T_n| <= M |V|max |T_{n-1}|max / n   (|T_{n-1}|max measured)
+//   R = sum_n T_n:         |R|   <= sum_{n<order} |T_n|max + the bound of T_order
+// with |P1|max, |S|max, |V|max < 2^14 times their inverse scales.  A loose bound costs nothing:
+// FP16 keeps the 22-bit split for every element within 17 binades of the scaled maximum, and an
+// element further down has an absolute error (FP16 subnormal spacing) far below the largest
+// products'.
+constexpr int TI_EPW = 8;                  // epilogue warps: two per TMEM lane quarter
+constexpr int TI_NT = 32 * TI_EPW;
+constexpr int TI_THREADS = 64 + TI_NT;
+constexpr int TI_CW = 8;                   // accumulator columns per epilogue chunk
+
+// (slot, walker, phase, row tile) units in the order every warp role walks them: the slots take
+// turns tile by tile; a slot whose walker finished its last phase takes the CTA's next walker
+struct TileSchedule {
+  int w0, w1, ph0, ph1, mt0, mt1, wi0, wi1;
+  int next, cur, W, nph, MT, step;
+  __device__ TileSchedule(int W_, int nph_, int MT_, int first, int stride, int nslots)
+      : w0(first), w1(nslots > 1 ? first + stride : W_), ph0(0), ph1(0), mt0(0), mt1(0), wi0(0),
+        wi1(0), next(first + nslots * stride), cur(0), W(W_), nph(nph_), MT(MT_), step(stride) {}
+  __device__ int w(int s) const { return s ? w1 : w0; }
+  __device__ int ph(int s) const { return s ? ph1 : ph0; }
+  __device__ int mt(int s) const { return s ? mt1 : mt0; }
+  __device__ int wi(int s) const { return s ? wi1 : wi0; }
+  __device__ bool get(int& s) {
+    for (int k = 0; k < 2; ++k) {
+      const int c = cur;
+      cur ^= 1;
+      if (w(c) < W) {
+        s = c;
+        return true;
+      }
+    }
+    return false;
+  }
+  __device__ void advance(int s) {
+    int& mt_ = s ? mt1 : mt0;
+    if (++mt_ < MT) return;
+    mt_ = 0;
+    int& ph_ = s ? ph1 : ph0;
+    if (++ph_ < nph) return;
+    ph_ = 0;
+    ++(s ? wi1 : wi0);
+    (s ? w1 : w0) = next;
+    next += step;
+  }
+};
+
+__global__ void __launch_bounds__(TI_THREADS, 1)
+    taylor_il_kernel(const __grid_constant__ TyParams p) {
+  constexpr int TBKE = 2 * TBK;  // 64 FP16 elements per 128-byte stage row
+  constexpr int KSTEP = 16;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + T_STAGES * T_STAGE);
+  uint64_t* empty = full + T_STAGES;
+  uint64_t* acc_full = empty + T_STAGES;  // [slot]
+  uint64_t* acc_empty = acc_full + 2;     // [slot]
+  uint64_t* phase_done = acc_empty + 2;   // [slot] epilogue -> TMA: the phase's planes are written
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(phase_done + 2);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  // [slot][phase parity] maximum |stored value| of the phase (float bits, atomicMax)
+  unsigned* maxbits = reinterpret_cast<unsigned*>(tmem_slot + 2);
+  int* agree = reinterpret_cast<int*>(tmem_slot + 6);  // [TI_EPW]
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nph = p.order + 2;
+  const int M = p.M;
+  const int nk = (M + TBKE - 1) / TBKE;
+  const int MT = (M + 127) / 128;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < T_STAGES; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(&acc_full[b], 1);
+      tc::mbar_init(&acc_empty[b], TI_NT);
+      tc::mbar_init(&phase_done[b], TI_NT);
+      maxbits[2 * b] = maxbits[2 * b + 1] = 0u;
+    }
+    *abort_flag = 0;
+    tc::fence_mbar_init();
+  }
+  if (warp == 1) {
+    tc::tmem_alloc(tmem_slot, 512);
+    tc::tmem_relinquish();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t taddr = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      TileSchedule sc(p.W, nph, MT, blockIdx.x, gridDim.x, p.nslots);
+      const uint64_t pol_last = tc::make_policy_evict_last();
+      const uint64_t pol_first = tc::make_policy_evict_first();
+      long it = 0;
+      bool ok = true;
+      int sl;
+      while (ok && sc.get(sl)) {
+        const int w = sc.w(sl), ph = sc.ph(sl), mt = sc.mt(sl);
+        const bool p1 = (ph == 0 || ph == nph - 1);
+        const CUtensorMap* amap = p1 ? p.p1 : p.v;
+        const CUtensorMap* bmap = ph == 0 ? p.s : (ph == nph - 1 ? p.r : p.t[(ph - 1) & 1]);
+        const int na = p1 ? 2 : 4;
+        const unsigned bytes = unsigned(na * T_A_TILE + 4 * T_B_TILE);
+        // B is the previous phase's planes of this walker: ready once its hand-off arrived (the
+        // first row tile of the phase waits for it)
+        bool b_ready = (ph == 0) || (mt > 0);
+        for (int kc = 0; kc < nk; ++kc, ++it) {
+          const int s = int(it % T_STAGES);
+          if (it >= T_STAGES) {
+            if (!tc::mbar_wait(&empty[s], unsigned((it / T_STAGES) - 1) & 1u, p.err,
+                               abort_flag)) {
+              ok = false;
+              break;
+            }
+          }
+          unsigned char* st = base + size_t(s) * T_STAGE;
+          tc::mbar_arrive_expect_tx(&full[s], bytes);
+          // V_w is read once per Taylor term: kept in L2 until its last term
+          const uint64_t pol = (ph == nph - 2) ? pol_first : pol_last;
+          for (int q = 0; q < na; ++q)
+            tc::tma_load_3d_hint(st + q * T_A_TILE, &amap[q], &full[s], kc * TBKE, mt * 128,
+                                 p1 ? 0 : w, pol);
+          if (!b_ready) {
+            const long done = long(sc.wi(sl)) * (nph - 1) + (ph - 1);
+            if (!tc::mbar_wait(&phase_done[sl], unsigned(done) & 1u, p.err, abort_flag)) {
+              ok = false;
+              break;
+            }
+            b_ready = true;
+          }
+          for (int q = 0; q < 4; ++q)
+            tc::tma_load_3d(st + 4 * T_A_TILE + q * T_B_TILE, &bmap[q], &full[s], kc * TBKE, 0,
+                            w);
+        }
+        sc.advance(sl);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t ID = tc::idesc_split<true>(128, TBN, false);
+      constexpr uint32_t IDN = tc::idesc_split<true>(128, TBN, true);
+      TileSchedule sc(p.W, nph, MT, blockIdx.x, gridDim.x, p.nslots);
+      long it = 0;
+      long use0 = 0, use1 = 0;  // accumulator uses of each slot
+      bool ok = true;
+      int sl;
+      while (ok && sc.get(sl)) {
+        const int ph = sc.ph(sl);
+        const bool p1 = (ph == 0 || ph == nph - 1);
+        const long use = sl ? use1 : use0;
+        if (use >= 1) {
+          if (!tc::mbar_wait(&acc_empty[sl], unsigned(use - 1) & 1u, p.err, abort_flag)) break;
+        }
+        tc::tc_fence_after();
+        const uint32_t dr = taddr + uint32_t(sl * 256), di = dr + TBN;
+        const uint32_t er = dr + 2 * TBN, ei = dr + 3 * TBN;
+        for (int kc = 0; kc < nk; ++kc, ++it) {
+          const int s = int(it % T_STAGES);
+          if (!tc::mbar_wait(&full[s], unsigned(it / T_STAGES) & 1u, p.err, abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc::tc_fence_after();
+          unsigned char* st = base + size_t(s) * T_STAGE;
+          const uint32_t sa = tc::smem_u32(st);
+          const uint32_t sb = tc::smem_u32(st + 4 * T_A_TILE);
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {
+            if (kc * TBKE + kk * KSTEP >= M) break;  // zero fill past M
+            auto A = [&](int q) { return tc::sdesc_sw128(sa + q * T_A_TILE) + uint64_t(2 * kk); };
+            auto B = [&](int q) { return tc::sdesc_sw128(sb + q * T_B_TILE) + uint64_t(2 * kk); };
+            const uint32_t acc0 = (kc > 0 || kk > 0) ? 1u : 0u;
+            // hi*hi into (dr, di); hi*lo and lo*hi into (er, ei)
+            if (p1) {
+              tc::mma_split<true>(dr, A(0), B(0), ID, acc0);
+              tc::mma_split<true>(er, A(0), B(1), ID, acc0);
+              tc::mma_split<true>(er, A(1), B(0), ID, 1);
+              tc::mma_split<true>(di, A(0), B(2), ID, acc0);
+              tc::mma_split<true>(ei, A(0), B(3), ID, acc0);
+              tc::mma_split<true>(ei, A(1), B(2), ID, 1);
+            } else {
+              tc::mma_split<true>(dr, A(0), B(0), ID, acc0);
+              tc::mma_split<true>(dr, A(2), B(2), IDN, 1);
+              tc::mma_split<true>(er, A(0), B(1), ID, acc0);
+              tc::mma_split<true>(er, A(1), B(0), ID, 1);
+              tc::mma_split<true>(er, A(2), B(3), IDN, 1);
+              tc::mma_split<true>(er, A(3), B(2), IDN, 1);
+              tc::mma_split<true>(di, A(0), B(2), ID, acc0);
+              tc::mma_split<true>(di, A(2), B(0), ID, 1);
+              tc::mma_split<true>(ei, A(0), B(3), ID, acc0);
+              tc::mma_split<true>(ei, A(1), B(2), ID, 1);
+              tc::mma_split<true>(ei, A(2), B(1), ID, 1);
+              tc::mma_split<true>(ei, A(3), B(0), ID, 1);
+            }
+          }
+          tc::mma_commit(&empty[s]);
+        }
+        if (!ok) break;
+        tc::mma_commit(&acc_full[sl]);
+        ++(sl ? use1 : use0);
+        sc.advance(sl);
+      }
+    }
+  } else {
+    // epilogue: TMEM lane quarter q = warp % 4 (one accumulator row per thread), the quarter's two
+    // warps (h = 0, 1) take alternate 8-column chunks
+    const int q = warp & 3;
+    const int h = (warp - 2) >> 2;
+    const int N = p.N;
+    const long pl_ld = p.pl_ld;
+    float* __restrict__ const sum_r = p.sum[0];
+    float* __restrict__ const sum_i = p.sum[1];
+    const float two14 = 16384.f;
+    TileSchedule sc(p.W, nph, MT, blockIdx.x, gridDim.x, p.nslots);
+    long use0 = 0, use1 = 0;
+    // per slot: inverse scale of the planes it stored last, the output scale of its current
+    // phase, the measured maximum of its previous term and the sum of its terms' maxima
+    float pinv0 = 1.f, pinv1 = 1.f, osc0 = 1.f, osc1 = 1.f;
+    float mprev0 = 0.f, mprev1 = 0.f, msum0 = 0.f, msum1 = 0.f;
+    int eo0 = 0, eo1 = 0;
+    bool wok = true;  // this warp's waits (agreed on at every phase end)
+    int sl;
+    while (sc.get(sl)) {
+      const int w = sc.w(sl), ph = sc.ph(sl), mt = sc.mt(sl);
+      const bool taylor = (ph > 0 && ph < nph - 1);
+      const bool last_phase = (ph == nph - 1);
+      const bool last_term = (ph == nph - 2);
+      const float ai = taylor ? 1.0f / float(ph) : 0.0f;
+      const float pin = sl ? pinv1 : pinv0;
+      const float f_in = ph == 0 ? p.p1_inv * p.s_inv[w]
+                                 : (last_phase ? p.p1_inv * pin : p.v_inv[w] * pin);
+      if (mt == 0 && !last_phase) {
+        // the bound of what this phase stores, and its scale
+        const float mp = sl ? mprev1 : mprev0;
+        float b;
+        if (ph == 0) {
+          b = float(M) * (two14 * p.p1_inv) * (two14 * p.s_inv[w]);
+        } else {
+          b = float(M) * (two14 * p.v_inv[w]) * mp * ai;
+          if (last_term) b += sl ? msum1 : msum0;
+        }
+        const int e = tc::f16_scale_exponent(b);
+        (sl ? eo1 : eo0) = e;
+        (sl ? osc1 : osc0) = ldexpf(1.f, e);
+      }
+      const float osc = sl ? osc1 : osc0;
+      const unsigned par = unsigned(sl ? use1 : use0) & 1u;
+      if (wok) {
+        wok = tc::mbar_wait_warp(&acc_full[sl], par, p.err, abort_flag);
+        if (wok) tc::tc_fence_after();
+      }
+      const int row = mt * 128 + q * 32 + lane;
+      const bool rok = row < M;
+      const uint32_t tacc = taddr + (uint32_t(q * 32) << 16) + uint32_t(sl * 256);
+      const long off = long(w) * p.pl_bs + row;
+      void* const* dst = last_term ? p.rp : p.tp[ph & 1];
+      c128* Sw = p.S + long(w) * p.ldS + long(row) * N;
+      float lmax = 0.f;
+#pragma unroll 1
+      for (int c0 = TI_CW * h; c0 < TBN && wok; c0 += 2 * TI_CW) {
+        const bool last_chunk = c0 + 2 * TI_CW >= TBN;
+        if (c0 >= N) {
+          if (last_chunk) {  // no electron column here: only free the accumulator
+            tc::tc_fence_before();
+            tc::mbar_arrive(&acc_empty[sl]);
+          }
+          continue;
+        }
+        float sr[TI_CW], si[TI_CW];
+        if (taylor && rok) {
+          // the running sum from global memory, in flight while the accumulators are read
+#pragma unroll
+          for (int j = 0; j < TI_CW; ++j)
+            if (c0 + j < N) {
+              const long idx = off + long(c0 + j) * pl_ld;
+              sr[j] = sum_r[idx];
+              si[j] = sum_i[idx];
+            }
+        }
+        float vr[TI_CW], vi[TI_CW], wr[TI_CW], wi[TI_CW];
+        tc::tmem_ld<TI_CW>(tacc + c0, vr);
+        tc::tmem_ld<TI_CW>(tacc + TBN + c0, vi);
+        tc::tmem_ld<TI_CW>(tacc + 2 * TBN + c0, wr);
+        tc::tmem_ld<TI_CW>(tacc + 3 * TBN + c0, wi);
+        tc::tmem_ld_wait();
+        if (last_chunk) {  // the slot's accumulators are free for its next tile
+          tc::tc_fence_before();
+          tc::mbar_arrive(&acc_empty[sl]);
+        }
+        if (!rok) continue;
+        float xr[TI_CW], xi[TI_CW];
+#pragma unroll
+        for (int j = 0; j < TI_CW; ++j) {
+          // hi*hi plus the small products (FP32 add, rounded to nearest), in true values
+          const float ar = (vr[j] + wr[j]) * f_in, aim = (vi[j] + wi[j]) * f_in;
+          xr[j] = taylor ? -ai * aim : ar;
+          xi[j] = taylor ? ai * ar : aim;
+        }
+        if (last_phase) {
+          // S = P1 R  (complex128 walker matrix [M][N])
+#pragma unroll
+          for (int j = 0; j < TI_CW; ++j)
+            if (c0 + j < N) Sw[c0 + j] = cmk(xr[j], xi[j]);
+          continue;
+        }
+#pragma unroll
+        for (int j = 0; j < TI_CW; ++j)
+          if (c0 + j < N) {
+            const long idx = off + long(c0 + j) * pl_ld;
+            const float ur = taylor ? xr[j] + sr[j] : xr[j];
+            const float ui = taylor ? xi[j] + si[j] : xi[j];
+            // stored: T_ph (and the running sum), or R = sum + T_order after the last term
+            const float tr = last_term ? ur : xr[j];
+            const float ti = last_term ? ui : xi[j];
+            if (!last_term) {
+              sum_r[idx] = ur;
+              sum_i[idx] = ui;
+            }
+            lmax = fmaxf(lmax, fmaxf(fabsf(tr), fabsf(ti)));
+            split_store16(tr * osc, dst[0], dst[1], idx);
+            split_store16(ti * osc, dst[2], dst[3], idx);
+          }
+      }
+      // this warp's maximum of the tile, into the phase's maximum (non-negative floats order
+      // like their bits)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+      if (lane == 0 && !last_phase) atomicMax(&maxbits[2 * sl + (ph & 1)], __float_as_uint(lmax));
+      if (mt == MT - 1) {
+        // the phase is complete: agree on going on, and on the maximum of what it stored
+        if (lane == 0) agree[warp - 2] = wok ? 0 : 1;
+        named_bar_sync(1, TI_NT);
+        int fail = 0;
+#pragma unroll
+        for (int k = 0; k < TI_EPW; ++k) fail |= agree[k];
+        const float m = __uint_as_float(maxbits[2 * sl + (ph & 1)]);
+        // the slot's next phase accumulates into the other parity: cleared here, before the
+        // barrier that every warp passes before it works on that phase
+        if (threadIdx.x == 64) maxbits[2 * sl + (((ph + 1) % nph) & 1)] = 0u;
+        named_bar_sync(1, TI_NT);  // agree and maxbits are rewritten only after everyone read them
+        if (fail) break;
+        if (!last_phase) {
+          (sl ? mprev1 : mprev0) = m;
+          if (ph == 0)
+            (sl ? msum1 : msum0) = m;
+          else if (!last_term)
+            (sl ? msum1 : msum0) += m;
+          (sl ? pinv1 : pinv0) = ldexpf(1.f, -(sl ? eo1 : eo0));
+          // make this phase's planes visible to the TMA loads of the next phase
+          fence_proxy_async_global();
+          tc::mbar_arrive(&phase_done[sl]);
+        }
+      }
+      ++(sl ? use1 : use0);
+      sc.advance(sl);
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 1) tc::tmem_dealloc(taddr, 512);
+}
+
 int g_nsm = 0;
 
 }  // namespace
@@ -777,6 +1154,15 @@ int taylor_fused_tc(cudaStream_t s, int esize, const void* const P1p[2], const v
   p.dual = (p.nslots == 1 && one_slot_use == 0) ? 1 : 0;
   p.sum_tmem = (p.nslots == 1 && one_slot_use == 1) ? 1 : 0;
   const int grid = W < g_nsm ? W : g_nsm;
+  if (f16 && p.dual) {
+    // the FP16 split with the second accumulator runs interleaved: two walkers per CTA once
+    // every CTA has two, their row tiles taking turns on the tensor core
+    p.nslots = (W >= 2 * g_nsm) ? 2 : 1;
+    AFQMC_CUDA_TRY(cudaFuncSetAttribute(taylor_il_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(T_SMEM)));
+    taylor_il_kernel<<<grid, TI_THREADS, T_SMEM, s>>>(p);
+    return launch_status("taylor_il_kernel");
+  }
   kern<<<grid, ty_threads(TY_EPW), T_SMEM, s>>>(p);
   return launch_status("taylor_tc_kernel");
 }
