@@ -56,9 +56,10 @@ def parse():
     ap.add_argument("--cv-fraction", type=float, default=1.0 / 8,
                     help="walkers (or draws) evaluated exactly per measurement")
     ap.add_argument("--cv-sampling", default="weight", choices=["uniform", "weight"])
-    ap.add_argument("--cv-lowrank", type=int, default=-1,
-                    help="leading Cholesky vectors of the low-fidelity exchange base (0: none, "
-                         "-1: Nc / 16)")
+    ap.add_argument("--cv-lowrank", type=int, default=0,
+                    help="leading Cholesky vectors of an optional low-fidelity exchange base the "
+                         "network learns on top of (0: none, the network alone; -1: Nc / 16; a "
+                         "multiple of 4)")
     ap.add_argument("--cv-system", default="cfg2", choices=["cfg1", "cfg2"],
                     help="control-variate workload: cfg2 = M=200 N=50+50 Nc=1600, cfg1 = M=32 "
                          "N=8+8 Nc=128")
