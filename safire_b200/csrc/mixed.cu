@@ -13,6 +13,7 @@
 
 #include <cstring>
 #include <memory>
+#include <new>
 #include <mutex>
 
 #include "detops.cuh"
@@ -1656,6 +1657,136 @@ int mixed_clear_error(MixedHam* m) {
 int mixed_error_flag(MixedHam* m, unsigned* flag) {
   AFQMC_CUDA_TRY(cudaMemcpy(flag, m->err, sizeof(unsigned), cudaMemcpyDeviceToHost));
   return AFQMC_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// C = A B^T for a complex A and a real B held as complex128 with zero imaginary parts, in the
+// FP16 split on the tensor cores (the PHMSD energy's half rotation G Lnak^T in mixed precision)
+// ---------------------------------------------------------------------------------------------
+namespace {
+// largest |re| and |im| of a complex128 array (non-negative floats order like their bits)
+__global__ void amax_c128_kernel(const c128* __restrict__ x, long n, unsigned* __restrict__ out) {
+  float mr = 0.f, mi = 0.f;
+  for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n;
+       i += long(gridDim.x) * blockDim.x) {
+    mr = fmaxf(mr, fabsf(float(x[i].x)));
+    mi = fmaxf(mi, fabsf(float(x[i].y)));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mr = fmaxf(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+    mi = fmaxf(mi, __shfl_xor_sync(0xffffffffu, mi, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, __float_as_uint(mr));
+    atomicMax(out + 1, __float_as_uint(mi));
+  }
+}
+
+__global__ void split_real_part_f16_kernel(const c128* __restrict__ src, long rows, long cols,
+                                           long ld_src, __half* __restrict__ h,
+                                           __half* __restrict__ l, long ld_dst, float sc) {
+  const long e = blockIdx.x * long(blockDim.x) + threadIdx.x;
+  if (e >= rows * cols) return;
+  const long r = e / cols, c = e % cols;
+  __half hi, lo;
+  tc::f16_split(float(src[r * ld_src + c].x) * sc, hi, lo);
+  h[r * ld_dst + c] = hi;
+  l[r * ld_dst + c] = lo;
+}
+}  // namespace
+
+struct TcGemmRB {
+  Planes B;          // FP16 split of B (2 planes), one power-of-two scale
+  float b_inv = 1.f;
+  Planes A;          // FP16 split of A (4 planes), per-row scales a_inv
+  float* a_inv = nullptr;
+  long a_cap = 0;
+  unsigned* err = nullptr;
+  ~TcGemmRB() {
+    free_planes(B);
+    free_planes(A);
+    if (a_inv) cudaFree(a_inv);
+    if (err) cudaFree(err);
+  }
+};
+
+int tcgemm_rb_create(TcGemmRB** out, const c128* B, long rows_b, long K, long ldb) {
+  *out = nullptr;
+  if (K % 8 != 0 || rows_b < 1) {
+    set_error_detail("tcgemm_rb_create: K = %ld (a multiple of 8), rows = %ld", K, rows_b);
+    return AFQMC_ERR_UNSUPPORTED;
+  }
+  unsigned* d = nullptr;
+  AFQMC_CUDA_TRY(cudaMalloc(&d, 2 * sizeof(unsigned)));
+  cudaMemset(d, 0, 2 * sizeof(unsigned));
+  long n = rows_b * ldb;
+  amax_c128_kernel<<<1184, 256>>>(B, n, d);
+  unsigned bits[2] = {0, 0};
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(bits, d, sizeof(bits), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    set_error_detail("amax_c128_kernel: %s", cudaGetErrorString(e));
+    return AFQMC_ERR_CUDA;
+  }
+  float amax, imax;
+  memcpy(&amax, &bits[0], 4);
+  memcpy(&imax, &bits[1], 4);
+  if (imax != 0.f) {
+    set_error_detail("tcgemm_rb_create: B is not real (max |imag| %g)", double(imax));
+    return AFQMC_ERR_UNSUPPORTED;
+  }
+  std::unique_ptr<TcGemmRB> g(new (std::nothrow) TcGemmRB());
+  if (!g) return AFQMC_ERR_ALLOC;
+  AFQMC_TRY(alloc_planes(g->B, 2, 1, rows_b, K, 2));
+  const int ex = tc::f16_scale_exponent(amax);
+  g->b_inv = ldexpf(1.f, -ex);
+  const long tot = rows_b * K;
+  split_real_part_f16_kernel<<<ceil_div(tot, 256), 256>>>(B, rows_b, K, ldb, g->B.h(0), g->B.h(1),
+                                                         g->B.ld, ldexpf(1.f, ex));
+  AFQMC_TRY(launch_status("split_real_part_f16_kernel"));
+  AFQMC_CUDA_TRY(cudaMalloc(&g->err, sizeof(unsigned)));
+  AFQMC_CUDA_TRY(cudaMemset(g->err, 0, sizeof(unsigned)));
+  AFQMC_CUDA_TRY(cudaDeviceSynchronize());
+  *out = g.release();
+  return AFQMC_OK;
+}
+
+void tcgemm_rb_destroy(TcGemmRB* g) { delete g; }
+
+int tcgemm_rb_run(cudaStream_t s, TcGemmRB* g, const c128* A, long lda, int rows_a, c128* C,
+                  long ldc) {
+  if (rows_a <= 0) return AFQMC_OK;
+  const long K = g->B.k;
+  if (g->a_cap < rows_a) {
+    AFQMC_CUDA_TRY(cudaDeviceSynchronize());
+    free_planes(g->A);
+    if (g->a_inv) cudaFree(g->a_inv);
+    g->a_inv = nullptr;
+    g->a_cap = 0;
+    AFQMC_TRY(alloc_planes(g->A, 4, 1, rows_a, K, 2));
+    AFQMC_CUDA_TRY(cudaMalloc(&g->a_inv, sizeof(float) * rows_a));
+    g->a_cap = rows_a;
+  }
+  AFQMC_TRY(split_rows_f16(s, A, lda, rows_a, int(K), g->A, g->a_inv));
+  TcParams p{};
+  for (int q = 0; q < 4; ++q)
+    AFQMC_TRY(make_map_es(&p.a[q], g->A, q, 0, K, rows_a, g->A.ld, 1, long(rows_a) * g->A.ld,
+                          128));
+  for (int q = 0; q < 2; ++q)
+    AFQMC_TRY(make_map_es(&p.b[q], g->B, q, 0, K, g->B.rows, g->B.ld, 1, g->B.bstride(), 128));
+  p.m = rows_a;
+  p.n = int(g->B.rows);
+  p.k = int(K);
+  p.order = 1;  // an A tile stays in L2 while the B tiles stream past it
+  p.alpha = cmk(double(g->b_inv), 0);
+  p.row_inv = g->a_inv;
+  p.out_c = C;
+  p.outc_ld = ldc;
+  p.outc_bs = 0;
+  p.err = g->err;
+  return launch_tc<true, false, 128, 2, EPI_C128, true>(s, p, 1);
 }
 
 }  // namespace afqmc

@@ -48,4 +48,14 @@ int mixed_clear_error(MixedHam* m);
 // first device-side wait timeout reported by the tensor-core kernels (0 = none)
 int mixed_error_flag(MixedHam* m, unsigned* flag);
 
+// C [rows_a][cols of B] (complex128, ldc) = A B^T with A complex128 [rows_a][K] (lda) and B real,
+// given as complex128 [rows_b][K] (ldb) with zero imaginary parts: FP16 split products on the
+// tensor cores, FP32 accumulation (B split once at creation; AFQMC_ERR_UNSUPPORTED when B has an
+// imaginary part or K is not a multiple of 8)
+struct TcGemmRB;
+int tcgemm_rb_create(TcGemmRB** out, const c128* B, long rows_b, long K, long ldb);
+void tcgemm_rb_destroy(TcGemmRB* g);
+int tcgemm_rb_run(cudaStream_t s, TcGemmRB* g, const c128* A, long lda, int rows_a, c128* C,
+                  long ldc);
+
 }  // namespace afqmc

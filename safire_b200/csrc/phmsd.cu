@@ -19,6 +19,7 @@
 
 #include "common.cuh"
 #include "detops.cuh"
+#include "mixed.cuh"
 #include "zgemm.cuh"
 
 namespace afqmc {
@@ -464,6 +465,54 @@ __global__ void woodbury_inverses_kernel(const c128* __restrict__ QQ0, const int
     for (int q = 0; q < nex; ++q) o[p * nex + q] = ok ? inv[p][q] : cmk(0.0, 0.0);
 }
 
+// The 1-body energies of every unique excitation u >= 1 for walker blockIdx.x, from the
+// Woodbury inverses Qi (INV, uinv) instead of R rows (ph_excited_1body_kernel over compact_R's
+// rows, PHMSD.cpp:376-546): with R_u[p] = sum_q Qi[p][q] (e_{part_q} - sum_i QQ0[part_q][i]
+// e_{o_u(i)}), o_u(i) the orbital of electron i in determinant u (its particle for a hole, else
+// refc[i]),
+//   e1_u = sum_p (S[i_p] . R_u[p] + S[i_p][part_p] - S[i_p][refc[i_p]]),
+// and E[w] += sum_u wgt[u][w] e1_u.  A singular block has Qi = 0, so R_u = 0 (as the reference).
+__global__ void __launch_bounds__(PH_THREADS) excited_1body_all_kernel(
+    const c128* __restrict__ S, const c128* __restrict__ QQ0, const int* __restrict__ refc,
+    const int* __restrict__ uoff, const int* __restrict__ unex, const int* __restrict__ uexc,
+    const int* __restrict__ uinv, const c128* __restrict__ INV, int ninv,
+    const c128* __restrict__ wgt, int nuniq, int W, int nel, int nact, c128* __restrict__ E) {
+  __shared__ double red[PH_THREADS / 32 * 6];
+  const int w = blockIdx.x;
+  const c128* Sw = S + size_t(w) * nel * nact;
+  const c128* Q0 = QQ0 + size_t(w) * nact * nel;
+  const c128* Iw = INV + size_t(w) * ninv;
+  c128 acc = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0);
+  for (int u = 1 + threadIdx.x; u < nuniq; u += blockDim.x) {
+    const int n = unex[u];
+    const int* e = uexc + uoff[u];  // holes e[0..n), particles e[n..2n)
+    const c128* Qi = Iw + uinv[u];
+    c128 e1 = cmk(0, 0);
+    for (int p = 0; p < n; ++p) {
+      const c128* Sp = Sw + size_t(e[p]) * nact;
+      e1 = cadd(e1, csub(Sp[e[n + p]], Sp[refc[e[p]]]));
+      for (int q = 0; q < n; ++q) {
+        const c128* Tq = Q0 + size_t(e[n + q]) * nel;  // QQ0[part_q][:]
+        // S[i_p] . (e_{part_q} - sum_i QQ0[part_q][i] e_{o_u(i)})
+        c128 t = Sp[e[n + q]];
+        for (int i = 0; i < nel; ++i) {
+          int oi = refc[i];
+          for (int hh = 0; hh < n; ++hh)
+            if (e[hh] == i) oi = e[n + hh];
+          t = csub(t, cmul(Tq[i], Sp[oi]));
+        }
+        e1 = cadd(e1, cmul(Qi[p * n + q], t));
+      }
+    }
+    acc = cadd(acc, cmul(wgt[size_t(u) * W + w], e1));
+  }
+  block_sum3(acc, z1, z2, red);
+  if (threadIdx.x == 0) {
+    atomicAdd(&E[w].x, acc.x);
+    atomicAdd(&E[w].y, acc.y);
+  }
+}
+
 // The 2-body energy terms of one excited determinant at one Cholesky index n, from per-walker
 // tables instead of its R rows.  With t_j = T[j][n][:] (rows of the half-rotated Twina), the
 // determinant's holes h, particles p, reference orbitals r = refc[h], Q = INV (the inverse of
@@ -630,7 +679,7 @@ __device__ __forceinline__ void table_products(const TableProduct<C> (&P)[NP], c
 // and every output stay FP64.
 constexpr int PHX_THREADS = 256;
 template <typename R>
-__global__ void __launch_bounds__(PHX_THREADS, 1) excited_energy_tables_kernel(
+__global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_energy_tables_kernel(
     const c128* __restrict__ Twina, const c128* __restrict__ QQ0, const int* __restrict__ refc,
     const int* __restrict__ hl, const int* __restrict__ vl, int nh, int nv,
     const int* __restrict__ uoff4, const int* __restrict__ unex, const int* __restrict__ uexc4,
@@ -1060,6 +1109,17 @@ struct afqmc_phmsd_s {
   double E0 = 0.0;
   c128* lnak[2] = {nullptr, nullptr};  // [Nc][nact][M]
   c128* haj[2] = {nullptr, nullptr};   // [nact][M]
+  // mixed precision: Lnak in FP16 split planes for the tensor-core half rotation, made at the
+  // first mixed energy (state 0 untried, 1 ready, -1 Lnak complex: the complex128 GEMM runs)
+  TcGemmRB* tc_lnak[2] = {nullptr, nullptr};
+  int tc_lnak_state[2] = {0, 0};
+  void free_tc_lnak() {
+    for (int s = 0; s < 2; ++s) {
+      tcgemm_rb_destroy(tc_lnak[s]);
+      tc_lnak[s] = nullptr;
+      tc_lnak_state[s] = 0;
+    }
+  }
   // energy scratch for a block of walkers
   int capWb = 0;
   c128 *eG[2] = {nullptr, nullptr}, *eQ[2] = {nullptr, nullptr}, *eov[2] = {nullptr, nullptr};
@@ -1097,6 +1157,7 @@ struct afqmc_phmsd_s {
     free_scratch();
     free_energy_scratch();
     free_core_scratch();
+    free_tc_lnak();
     for (int s = 0; s < 2; ++s) {
       cudaFree(rowptr[s]);
       cudaFree(kidx[s]);
@@ -1443,6 +1504,7 @@ extern "C" int afqmc_phmsd_set_hamiltonian(afqmc_phmsd h, const double* Likn, in
   }
   cudaMemcpy(L, Likn, sizeof(double) * nspin_H2 * MM * Nc, cudaMemcpyHostToDevice);
   cudaMemcpy(hd, hij, sizeof(c128) * nspin_H1 * MM, cudaMemcpyHostToDevice);
+  h->free_tc_lnak();
   for (int sp = 0; sp < 2; ++sp) {
     const int na = h->nact[sp];
     cudaFree(h->lnak[sp]);
@@ -1594,6 +1656,19 @@ int phmsd_half_rotated(afqmc_phmsd h, cudaStream_t s, int sp, int nb) {
   p.C = h->Swia; p.ldc = na;
   p.alpha = cmk(1, 0); p.beta = cmk(0, 0);
   AFQMC_TRY(zgemm(s, 1, GN, false, GT, false, p));
+  if (h->precision == AFQMC_PREC_MIXED) {
+    // mixed precision: the FP16 split on the tensor cores when Lnak is real
+    if (h->tc_lnak_state[sp] == 0) {
+      AFQMC_CUDA_TRY(cudaStreamSynchronize(s));
+      const int st = tcgemm_rb_create(&h->tc_lnak[sp], h->lnak[sp], long(h->Nc) * na, h->M,
+                                      h->M);
+      if (st != AFQMC_OK && st != AFQMC_ERR_UNSUPPORTED) return st;
+      h->tc_lnak_state[sp] = st == AFQMC_OK ? 1 : -1;
+    }
+    if (h->tc_lnak_state[sp] == 1)
+      return tcgemm_rb_run(s, h->tc_lnak[sp], h->eG[sp], h->M, nb * N, h->Twina,
+                           long(h->Nc) * na);
+  }
   GemmParams q{};
   q.m = nb * N; q.n = h->Nc * na; q.k = h->M;
   q.A = h->eG[sp]; q.lda = h->M;
@@ -1628,7 +1703,9 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
     AFQMC_TRY(launch_status("ph_reference_kernel"));
   }
   AFQMC_CUDA_TRY(cudaMemsetAsync(h->el, 0, sizeof(c128) * 5 * nb, s));
-  for (size_t j = 0; j < h->sh_k0[sp].size(); ++j) {
+  // per shell (the R-row formulation) only without the tables; with them every unique
+  // excitation's 1-body term comes from its Woodbury inverse in one launch below
+  for (size_t j = 0; j < h->sh_k0[sp].size() && !tables; ++j) {
     const int k0 = h->sh_k0[sp][j], nd = h->sh_nd[sp][j], nex = h->sh_nex[sp][j];
     const int* iex = h->uexc[sp] + h->uoff_h[sp][k0];
     const size_t Rn = size_t(nb) * nd * nex * na;
@@ -1642,7 +1719,6 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
     ph_excited_1body_kernel<<<grid, PH_THREADS, 0, s>>>(iex, h->refc[sp], h->Swia, h->R, w, nb,
                                                         nd, nex, na, N, h->el);
     AFQMC_TRY(launch_status("ph_excited_1body_kernel"));
-    if (tables) continue;
     c128* KE = cross ? h->KEl : KEout + size_t(k0) * nb * Nc;
     const size_t smem = size_t(nex) * na * sizeof(c128) + 2 * size_t(N) * sizeof(int);
     AFQMC_CUDA_TRY(cudaFuncSetAttribute(ph_excited_2body_kernel,
@@ -1664,6 +1740,10 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
           h->eQ[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp], h->nuniq[sp], nb, na, N,
           h->ninv[sp], h->INV);
       AFQMC_TRY(launch_status("woodbury_inverses_kernel"));
+      excited_1body_all_kernel<<<nb, PH_THREADS, 0, s>>>(
+          h->Swia, h->eQ[sp], h->refc[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp],
+          h->INV, h->ninv[sp], h->wgt, h->nuniq[sp], nb, N, na, h->el);
+      AFQMC_TRY(launch_status("excited_1body_all_kernel"));
     }
     c128* REF = h->el + 3 * nb;  // [nb][2]: sum_n ex0, sum_n f0^2
     auto kern = mixed ? excited_energy_tables_kernel<float> : excited_energy_tables_kernel<double>;
