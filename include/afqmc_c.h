@@ -146,6 +146,22 @@ typedef struct afqmc_ham_s* afqmc_ham;
 int afqmc_ham_create(int walker_type, int M, int nup, int ndn, int Nc, const double* Likn,
                      int nspin_H2, const afqmc_c128* hij, int nspin_H1, double E0,
                      const afqmc_c128* PsiT, afqmc_ham* out);
+/* The tensor-hypercontraction factorisation behind the same handle — THCOps
+ * (HamiltonianOperations/THCOps.hpp:50-105, the constructor; vbias :571-615, vHS :462-569,
+ * energy :149-293).  The two-electron integrals are L_n[i][k] = sum_u X[i][u] X[k][u] L[u][n]:
+ *   X     host float64 [M][nu]   (Piu: the orbitals at the nu interpolation points)
+ *   L     host float64 [nu][nv]  (Luv; nv plays the part of N_chol: vbias [W][nv], X [W][nv])
+ *   Z     host float64 [nu][nu]  (rotMuv = L L^T; NULL: computed from L)
+ *   hij   host complex [nspin_H1][M][M];  v0 host float64 [M][M] (NULL: computed from X, Z)
+ *   PsiT  as afqmc_ham_create (the trial-rotated points Y = PsiT X are built from it)
+ * Every afqmc_ham_* operation and the propagator then use the THC contractions, in complex128
+ * only (a mixed-precision call returns AFQMC_ERR_UNSUPPORTED); one determinant (as THCOps). */
+int afqmc_ham_create_thc(int walker_type, int M, int nup, int ndn, int nu, int nv,
+                         const double* X, const double* L, const double* Z,
+                         const afqmc_c128* hij, int nspin_H1, const double* v0, double E0,
+                         const afqmc_c128* PsiT, afqmc_ham* out);
+/* nu and nv of a THC handle (0, 0 for a Cholesky one) */
+int afqmc_ham_thc_info(afqmc_ham ham, int* nu, int* nv);
 int afqmc_ham_destroy(afqmc_ham ham);
 /* number_of_cholesky_vectors / energy_offset / walker type (Real3IndexFactorization.hpp:432-438) */
 int afqmc_ham_info(afqmc_ham ham, int* walker_type, int* M, int* nup, int* ndn, int* Nc,

@@ -128,6 +128,34 @@ class HamiltonianOperations:
         self.handle = h
         self.nspin_H2 = Likn.shape[0]
 
+    @classmethod
+    def thc(cls, walker_type, M, nup, ndn, X, L, hij, E0, PsiT, Z=None, v0=None):
+        """THC Hamiltonian operations (THCOps, HamiltonianOperations/THCOps.hpp): X float64
+        [M, nu] (Piu), L float64 [nu, nv] (Luv), Z float64 [nu, nu] (rotMuv, default L L^T),
+        v0 float64 [M, M] (default from X and Z); the Cholesky vectors this factorisation
+        stands for are L_n = X diag(L[:, n]) X^T.  Same methods as the Cholesky form, complex128
+        only."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        L = np.ascontiguousarray(L, dtype=np.float64)
+        hij = np.ascontiguousarray(hij, dtype=np.complex128)
+        Zc = None if Z is None else np.ascontiguousarray(Z, dtype=np.float64)
+        v0c = None if v0 is None else np.ascontiguousarray(v0, dtype=np.float64)
+        psi = np.ascontiguousarray(np.concatenate([np.asarray(p) for p in PsiT], axis=0),
+                                   dtype=np.complex128)
+        self = cls.__new__(cls)
+        self.walker_type, self.M, self.nup, self.ndn = walker_type, M, nup, ndn
+        self.nu, self.Nc = L.shape
+        self.E0 = float(E0)
+        self.nel = nup + (ndn if walker_type == COLLINEAR else 0)
+        h = vp()
+        call("afqmc_ham_create_thc", walker_type, M, nup, ndn, self.nu, self.Nc, _host_ptr(X),
+             _host_ptr(L), _host_ptr(Zc) if Zc is not None else None, _host_ptr(hij),
+             hij.shape[0], _host_ptr(v0c) if v0c is not None else None, float(E0),
+             _host_ptr(psi), C.byref(h))
+        self.handle = h
+        self.nspin_H2 = 1
+        return self
+
     def __del__(self):
         h = getattr(self, "handle", None)
         try:

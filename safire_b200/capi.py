@@ -54,6 +54,9 @@ _SIGS = {
     "afqmc_orthogonalize": (i32, [vp, i64, vp, i32, i32, i32, vp]),
     "afqmc_propagate": (i32, [vp, vp, vp, i64, i32, i32, i32, i32, vp]),
     "afqmc_ham_create": (i32, [i32, i32, i32, i32, i32, vp, i32, vp, i32, f64, vp, C.POINTER(vp)]),
+    "afqmc_ham_create_thc": (i32, [i32, i32, i32, i32, i32, i32, vp, vp, vp, vp, i32, vp, f64,
+                                   vp, C.POINTER(vp)]),
+    "afqmc_ham_thc_info": (i32, [vp, C.POINTER(i32), C.POINTER(i32)]),
     "afqmc_ham_destroy": (i32, [vp]),
     "afqmc_ham_info": (i32, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), C.POINTER(i32),
                              C.POINTER(i32), C.POINTER(f64)]),

@@ -19,6 +19,7 @@
 #include "fields.cuh"
 #include "mixed.cuh"
 #include "update.cuh"
+#include "thc.cuh"
 #include "zgemm.cuh"
 
 namespace afqmc {
@@ -100,8 +101,10 @@ struct afqmc_ham_s {
   std::vector<c128> hij_h;              // [nspin_H1][M][M]
   std::vector<double> vexx_h;           // [nspin_H2][M][M]
   MixedHam* mixed = nullptr;            // tensor-core copies (built on first mixed call)
+  ThcData* thc = nullptr;               // THC factorisation instead of Likn (afqmc_ham_create_thc)
   ~afqmc_ham_s() {
     DeviceGuard g(device);
+    if (thc) thc_destroy(thc);
     dfree(Likn);
     for (int s = 0; s < 2; ++s) {
       dfree(Lnak[s]);
@@ -410,6 +413,7 @@ __global__ void lnak_reorder_kernel(const c128* __restrict__ in, c128* __restric
 namespace {
 
 int ham_vbias(afqmc_ham_s* h, cudaStream_t s, const c128* G, long ldG, c128* v, int W, double dt) {
+  if (h->thc) return thc_vbias(s, h->thc, G, ldG, v, W, dt, h->walker_type == AFQMC_CLOSED ? 2.0 : 1.0);
   const double a = std::sqrt(dt) * (h->walker_type == AFQMC_CLOSED ? 2.0 : 1.0);
   bool first = true;
   for (int sp = 0; sp < h->nspin; ++sp) {
@@ -430,6 +434,7 @@ int ham_vbias(afqmc_ham_s* h, cudaStream_t s, const c128* G, long ldG, c128* v, 
 }
 
 int ham_vhs(afqmc_ham_s* h, cudaStream_t s, const c128* X, c128* V, int W, double dt) {
+  if (h->thc) return thc_vhs(s, h->thc, X, V, W, dt);
   const int nst = h->walker_type == AFQMC_COLLINEAR ? h->nspin_H2 : 1;
   const long MM = long(h->M) * h->M;
   for (int is = 0; is < nst; ++is) {
@@ -476,6 +481,15 @@ long energy_chunk_elems(afqmc_ham_s* h, int W) {
 
 int ham_energy(afqmc_ham_s* h, cudaStream_t s, const c128* G, long ldG, c128* E, int W, bool addH1,
                bool addEJ, bool addEXX, int precision) {
+  if (h->thc) {
+    if (precision == AFQMC_PREC_MIXED) {
+      set_error_detail("THC Hamiltonian: complex128 only (no mixed-precision path)");
+      return AFQMC_ERR_UNSUPPORTED;
+    }
+    const double scl = h->walker_type == AFQMC_CLOSED ? 2.0 : 1.0;
+    return thc_energy(s, h->thc, G, ldG, h->haj, h->E0, scl, scl * scl, E, W, addH1, addEJ,
+                      addEXX);
+  }
   EnergyArgs a = energy_args(h, G, ldG);
   MixedHam* tc = nullptr;
   if (precision == AFQMC_PREC_MIXED && (h->mixed_ops & AFQMC_MIXED_ENERGY)) {
@@ -497,47 +511,16 @@ int ham_energy(afqmc_ham_s* h, cudaStream_t s, const c128* G, long ldG, c128* E,
 
 }  // namespace
 
-extern "C" int afqmc_ham_create(int walker_type, int M, int nup, int ndn, int Nc,
-                                const double* Likn, int nspin_H2, const afqmc_c128* hij,
-                                int nspin_H1, double E0, const afqmc_c128* PsiT,
-                                afqmc_ham* out) {
-  AFQMC_CHECK_ARG(out, "afqmc_ham_create: null out");
-  *out = nullptr;
-  AFQMC_CHECK_ARG(walker_type == AFQMC_CLOSED || walker_type == AFQMC_COLLINEAR,
-                  "afqmc_ham_create: walker_type must be CLOSED (1) or COLLINEAR (2)");
-  AFQMC_CHECK_ARG(M > 0 && Nc > 0 && nup >= 0 && ndn >= 0, "afqmc_ham_create: bad sizes");
-  AFQMC_CHECK_ARG(nup <= M && ndn <= M, "afqmc_ham_create: more electrons than orbitals");
-  AFQMC_CHECK_ARG(Likn && hij && PsiT, "afqmc_ham_create: null input");
-  AFQMC_CHECK_ARG(nspin_H2 == 1 || nspin_H2 == 2, "afqmc_ham_create: nspin_H2 must be 1 or 2");
-  AFQMC_CHECK_ARG(nspin_H1 == 1 || nspin_H1 == 2, "afqmc_ham_create: nspin_H1 must be 1 or 2");
-  if (walker_type == AFQMC_CLOSED) {
-    AFQMC_CHECK_ARG(nspin_H2 == 1 && nspin_H1 == 1,
-                    "afqmc_ham_create: CLOSED walkers take a spin-independent Hamiltonian");
-  }
-  std::unique_ptr<afqmc_ham_s> h(new (std::nothrow) afqmc_ham_s());
-  AFQMC_CHECK_ARG(h, "afqmc_ham_create: out of host memory");
-  cudaGetDevice(&h->device);
-  h->walker_type = walker_type;
-  h->M = M; h->nup = nup; h->ndn = ndn; h->Nc = Nc;
-  h->nspin = walker_type == AFQMC_COLLINEAR ? 2 : 1;
-  h->nspin_H2 = nspin_H2; h->nspin_H1 = nspin_H1;
-  h->nel[0] = nup;
-  h->nel[1] = walker_type == AFQMC_COLLINEAR ? ndn : 0;
-  h->el_off[0] = 0;
-  h->el_off[1] = nup;
-  h->nel_tot = h->nel[0] + h->nel[1];
-  h->E0 = E0;
+namespace {
+
+// the trial-dependent part of a Hamiltonian handle: PsiT, PsiH (the initial walker), haj
+int ham_trial_setup(afqmc_ham_s* h, const afqmc_c128* hij, int nspin_H1, const c128* psi) {
+  const int M = h->M;
   const long MM = long(M) * M;
-  h->hij_h.assign((const c128*)hij, (const c128*)hij + nspin_H1 * MM);
-  const c128* psi = (const c128*)PsiT;
   bool real = true;
   for (long e = 0; e < long(h->nel_tot) * M; ++e) real = real && psi[e].y == 0.0;
   h->trial_real = real;
-
   cudaStream_t s = nullptr;
-  AFQMC_TRY(dalloc(&h->Likn, size_t(nspin_H2) * MM * Nc));
-  AFQMC_CUDA_TRY(cudaMemcpy(h->Likn, Likn, sizeof(double) * nspin_H2 * MM * Nc,
-                            cudaMemcpyHostToDevice));
   AFQMC_TRY(dalloc(&h->PsiT, size_t(h->nel_tot) * M));
   if (h->nel_tot)
     AFQMC_CUDA_TRY(cudaMemcpy(h->PsiT, psi, sizeof(c128) * h->nel_tot * M, cudaMemcpyHostToDevice));
@@ -575,6 +558,50 @@ extern "C" int afqmc_ham_create(int walker_type, int M, int nup, int ndn, int Nc
     if (st) { dfree(hij_d); return st; }
   }
   dfree(hij_d);
+  return AFQMC_OK;
+}
+}  // namespace
+
+extern "C" int afqmc_ham_create(int walker_type, int M, int nup, int ndn, int Nc,
+                                const double* Likn, int nspin_H2, const afqmc_c128* hij,
+                                int nspin_H1, double E0, const afqmc_c128* PsiT,
+                                afqmc_ham* out) {
+  AFQMC_CHECK_ARG(out, "afqmc_ham_create: null out");
+  *out = nullptr;
+  AFQMC_CHECK_ARG(walker_type == AFQMC_CLOSED || walker_type == AFQMC_COLLINEAR,
+                  "afqmc_ham_create: walker_type must be CLOSED (1) or COLLINEAR (2)");
+  AFQMC_CHECK_ARG(M > 0 && Nc > 0 && nup >= 0 && ndn >= 0, "afqmc_ham_create: bad sizes");
+  AFQMC_CHECK_ARG(nup <= M && ndn <= M, "afqmc_ham_create: more electrons than orbitals");
+  AFQMC_CHECK_ARG(Likn && hij && PsiT, "afqmc_ham_create: null input");
+  AFQMC_CHECK_ARG(nspin_H2 == 1 || nspin_H2 == 2, "afqmc_ham_create: nspin_H2 must be 1 or 2");
+  AFQMC_CHECK_ARG(nspin_H1 == 1 || nspin_H1 == 2, "afqmc_ham_create: nspin_H1 must be 1 or 2");
+  if (walker_type == AFQMC_CLOSED) {
+    AFQMC_CHECK_ARG(nspin_H2 == 1 && nspin_H1 == 1,
+                    "afqmc_ham_create: CLOSED walkers take a spin-independent Hamiltonian");
+  }
+  std::unique_ptr<afqmc_ham_s> h(new (std::nothrow) afqmc_ham_s());
+  AFQMC_CHECK_ARG(h, "afqmc_ham_create: out of host memory");
+  cudaGetDevice(&h->device);
+  h->walker_type = walker_type;
+  h->M = M; h->nup = nup; h->ndn = ndn; h->Nc = Nc;
+  h->nspin = walker_type == AFQMC_COLLINEAR ? 2 : 1;
+  h->nspin_H2 = nspin_H2; h->nspin_H1 = nspin_H1;
+  h->nel[0] = nup;
+  h->nel[1] = walker_type == AFQMC_COLLINEAR ? ndn : 0;
+  h->el_off[0] = 0;
+  h->el_off[1] = nup;
+  h->nel_tot = h->nel[0] + h->nel[1];
+  h->E0 = E0;
+  const long MM = long(M) * M;
+  h->hij_h.assign((const c128*)hij, (const c128*)hij + nspin_H1 * MM);
+  const c128* psi = (const c128*)PsiT;
+
+  cudaStream_t s = nullptr;
+  AFQMC_TRY(dalloc(&h->Likn, size_t(nspin_H2) * MM * Nc));
+  AFQMC_CUDA_TRY(cudaMemcpy(h->Likn, Likn, sizeof(double) * nspin_H2 * MM * Nc,
+                            cudaMemcpyHostToDevice));
+  AFQMC_TRY(ham_trial_setup(h.get(), hij, nspin_H1, psi));
+  const bool real = h->trial_real;
   // Lnak_s[n][a][k] = sum_i PsiT_s[a][i] L_s[i][k][n]: one GEMM PsiT_s (N x M) * L_s (M x M*Nc)
   // into [a][k][n], then a reorder to [n][a][k]
   for (int sp = 0; sp < h->nspin; ++sp) {
@@ -625,6 +652,91 @@ extern "C" int afqmc_ham_create(int walker_type, int M, int nup, int ndn, int Nc
   return AFQMC_OK;
 }
 
+// THC Hamiltonian operations behind the same handle (THCOps, HamiltonianOperations/THCOps.hpp:
+// the constructor's factors Piu = X, Luv = L, rotMuv = Z, the half-rotated haj and v0)
+extern "C" int afqmc_ham_create_thc(int walker_type, int M, int nup, int ndn, int nu, int nv,
+                                    const double* X, const double* L, const double* Z,
+                                    const afqmc_c128* hij, int nspin_H1, const double* v0,
+                                    double E0, const afqmc_c128* PsiT, afqmc_ham* out) {
+  AFQMC_CHECK_ARG(out, "afqmc_ham_create_thc: null out");
+  *out = nullptr;
+  AFQMC_CHECK_ARG(walker_type == AFQMC_CLOSED || walker_type == AFQMC_COLLINEAR,
+                  "afqmc_ham_create_thc: walker_type must be CLOSED (1) or COLLINEAR (2)");
+  AFQMC_CHECK_ARG(M > 0 && nu > 0 && nv > 0 && nup >= 0 && ndn >= 0,
+                  "afqmc_ham_create_thc: bad sizes");
+  AFQMC_CHECK_ARG(nup <= M && ndn <= M, "afqmc_ham_create_thc: more electrons than orbitals");
+  AFQMC_CHECK_ARG(X && L && hij && PsiT, "afqmc_ham_create_thc: null input");
+  AFQMC_CHECK_ARG(nspin_H1 == 1 || nspin_H1 == 2, "afqmc_ham_create_thc: nspin_H1 must be 1 or 2");
+  if (walker_type == AFQMC_CLOSED)
+    AFQMC_CHECK_ARG(nspin_H1 == 1,
+                    "afqmc_ham_create_thc: CLOSED walkers take a spin-independent Hamiltonian");
+  std::unique_ptr<afqmc_ham_s> h(new (std::nothrow) afqmc_ham_s());
+  AFQMC_CHECK_ARG(h, "afqmc_ham_create_thc: out of host memory");
+  cudaGetDevice(&h->device);
+  h->walker_type = walker_type;
+  h->M = M; h->nup = nup; h->ndn = ndn; h->Nc = nv;
+  h->nspin = walker_type == AFQMC_COLLINEAR ? 2 : 1;
+  h->nspin_H2 = 1; h->nspin_H1 = nspin_H1;
+  h->nel[0] = nup;
+  h->nel[1] = walker_type == AFQMC_COLLINEAR ? ndn : 0;
+  h->el_off[0] = 0;
+  h->el_off[1] = nup;
+  h->nel_tot = h->nel[0] + h->nel[1];
+  h->E0 = E0;
+  const long MM = long(M) * M;
+  h->hij_h.assign((const c128*)hij, (const c128*)hij + nspin_H1 * MM);
+  AFQMC_TRY(ham_trial_setup(h.get(), hij, nspin_H1, (const c128*)PsiT));
+  AFQMC_TRY(thc_create(&h->thc, walker_type, M, nup, ndn, nu, nv, X, L, Z, h->PsiT));
+  h->vexx_h.assign(size_t(MM), 0.0);
+  if (v0) {
+    std::memcpy(h->vexx_h.data(), v0, sizeof(double) * MM);
+  } else {
+    // v0[i][l] = -1/2 sum_{j,n} L_n[i][j] L_n[l][j] = -1/2 sum_{u,v} X[i][u] Z[u][v] S[u][v]
+    // X[l][v], S[u][v] = sum_j X[j][u] X[j][v], Z = L L^T unless given (host set-up)
+    std::vector<double> Zh(size_t(nu) * nu, 0.0), S(size_t(nu) * nu, 0.0), A(size_t(M) * nu, 0.0);
+    for (int u = 0; u < nu; ++u)
+      for (int v = 0; v < nu; ++v) {
+        double z = 0.0, sv = 0.0;
+        if (Z) {
+          z = Z[size_t(u) * nu + v];
+        } else {
+          for (int n = 0; n < nv; ++n) z += L[size_t(u) * nv + n] * L[size_t(v) * nv + n];
+        }
+        for (int j = 0; j < M; ++j) sv += X[size_t(j) * nu + u] * X[size_t(j) * nu + v];
+        Zh[size_t(u) * nu + v] = z * sv;
+      }
+    for (int i = 0; i < M; ++i)
+      for (int v = 0; v < nu; ++v) {
+        double acc = 0.0;
+        for (int u = 0; u < nu; ++u) acc += X[size_t(i) * nu + u] * Zh[size_t(u) * nu + v];
+        A[size_t(i) * nu + v] = acc;
+      }
+    for (int i = 0; i < M; ++i)
+      for (int l = 0; l < M; ++l) {
+        double acc = 0.0;
+        for (int v = 0; v < nu; ++v) acc += A[size_t(i) * nu + v] * X[size_t(l) * nu + v];
+        h->vexx_h[size_t(i) * M + l] = -0.5 * acc;
+      }
+  }
+  AFQMC_CUDA_TRY(cudaDeviceSynchronize());
+  *out = h.release();
+  return AFQMC_OK;
+}
+
+extern "C" int afqmc_ham_thc_info(afqmc_ham h, int* nu, int* nv) {
+  AFQMC_CHECK_ARG(h, "afqmc_ham_thc_info: null handle");
+  if (!h->thc) {
+    if (nu) *nu = 0;
+    if (nv) *nv = 0;
+    return AFQMC_OK;
+  }
+  int a = 0, b = 0;
+  thc_sizes(h->thc, &a, &b);
+  if (nu) *nu = a;
+  if (nv) *nv = b;
+  return AFQMC_OK;
+}
+
 extern "C" int afqmc_ham_destroy(afqmc_ham ham) {
   delete ham;
   return AFQMC_OK;
@@ -645,6 +757,7 @@ extern "C" int afqmc_ham_info(afqmc_ham h, int* wt, int* M, int* nup, int* ndn, 
 extern "C" int afqmc_ham_get_tensors(afqmc_ham h, afqmc_c128* Lnak, afqmc_c128* haj,
                                      double* vexx) {
   AFQMC_CHECK_ARG(h, "afqmc_ham_get_tensors: null handle");
+  AFQMC_CHECK_ARG(!(Lnak && h->thc), "afqmc_ham_get_tensors: a THC Hamiltonian has no Lnak");
   DeviceGuard g(h->device);
   if (Lnak) {
     long off = 0;
@@ -1177,6 +1290,9 @@ extern "C" int afqmc_nomsd_create(int ndet, const afqmc_ham* hams, const afqmc_c
   *out = nullptr;
   afqmc_ham_s* h0 = hams[0];
   AFQMC_CHECK_ARG(h0, "afqmc_nomsd_create: null Hamiltonian 0");
+  for (int d = 0; d < ndet; ++d)
+    AFQMC_CHECK_ARG(!hams[d] || !hams[d]->thc,
+                    "afqmc_nomsd_create: THC Hamiltonians take one determinant (as THCOps)");
   for (int d = 1; d < ndet; ++d) {
     afqmc_ham_s* h = hams[d];
     AFQMC_CHECK_ARG(h && h->device == h0->device && h->walker_type == h0->walker_type &&
@@ -1542,6 +1658,8 @@ extern "C" int afqmc_prop_destroy(afqmc_prop prop) {
 
 extern "C" int afqmc_prop_set_phmsd(afqmc_prop pr, afqmc_phmsd trial, const afqmc_c128* vMF) {
   AFQMC_CHECK_ARG(pr, "afqmc_prop_set_phmsd: null handle");
+  AFQMC_CHECK_ARG(!trial || !pr->ham->thc,
+                  "afqmc_prop_set_phmsd: a THC Hamiltonian takes one determinant (as THCOps)");
   DeviceGuard g(pr->device);
   if (!trial) {
     pr->ph = nullptr;

@@ -988,8 +988,9 @@ int mixed_ham_create(MixedHam** out, const EnergyArgs& a, cudaStream_t s) {
     return AFQMC_ERR_UNSUPPORTED;
   }
   if (!a.Likn) {
-    set_error_detail("mixed_ham_create: missing Likn");
-    return AFQMC_ERR_ARG;
+    set_error_detail("mixed precision needs the Cholesky factorisation (a THC Hamiltonian runs "
+                     "in complex128)");
+    return AFQMC_ERR_UNSUPPORTED;
   }
   std::unique_ptr<MixedHam> m(new MixedHam());
   m->M = a.M;

@@ -130,16 +130,21 @@ class Simulation:
 
     @staticmethod
     def from_workload(wl, W=None, precision=A.PREC_FP64, rp=None, trial=None, vMF=None,
-                      multidet=None, **prop_kw):
+                      multidet=None, ham=None, **prop_kw):
         """wl: a safire_b200.synth.Workload.  trial: an optional PHMSD trial
         (safire_b200.synth.PHMSDTrial, COLLINEAR workload whose PsiT is its reference
         determinant); multidet: an optional several-determinant NOMSD trial (PsiTs, ci) with
         PsiTs[d] the per-spin PsiT of determinant d (wl.PsiT is determinant 0's); vMF: the mean
-        field [Nc] (host) of either, default determinant 0's."""
+        field [Nc] (host) of either, default determinant 0's.  ham: the Hamiltonian operations
+        to use instead of the workload's Cholesky ones (a THC HamiltonianOperations.thc over
+        the same system; one determinant)."""
         rp = rp or RunParams()
         W = W or wl.W
-        ham = A.HamiltonianOperations(wl.walker_type, wl.M, wl.nup, wl.ndn, wl.Likn, wl.hij,
-                                      wl.E0, wl.PsiT)
+        if ham is not None and (trial is not None or multidet is not None):
+            raise ValueError("a given Hamiltonian takes a single-determinant trial")
+        if ham is None:
+            ham = A.HamiltonianOperations(wl.walker_type, wl.M, wl.nup, wl.ndn, wl.Likn, wl.hij,
+                                          wl.E0, wl.PsiT)
         ph = None
         if trial is not None and multidet is not None:
             raise ValueError("a PHMSD trial and a several-determinant NOMSD trial exclude each other")

@@ -74,6 +74,31 @@ def make_workload(name="cfg1", seed=0, W=None, M=None, N=None, Nc=None, lscale=0
                     h1[None].astype(np.complex128), Likn[None], 0.0, PsiT)
 
 
+def make_thc_system(seed=0, M=32, N=8, nu=96, nv=64, W=64, dt=0.01, lscale=0.5,
+                    decay=0.97, walker_type=CLOSED):
+    """A THC-factorised system (THCOps): h1 as make_hamiltonian, X = Piu [M, nu] the orbitals
+    at nu points (N(0,1) / sqrt(M)), Luv [nu, nv] = lscale decay^n N(0,1) / sqrt(nu); the
+    Cholesky vectors they stand for are L_n = X diag(Luv[:, n]) X^T (real symmetric).  Returns
+    (Workload carrying that Likn, X, Luv); the trial is the N lowest eigenvectors of h1 per spin
+    (COLLINEAR: N up, N - 1 down)."""
+    rng = np.random.default_rng(seed)
+    h1 = np.diag(-2.0 + 4.0 * np.arange(M) / M) + 0.1 * _sym(rng.standard_normal((M, M)))
+    X = rng.standard_normal((M, nu)) / np.sqrt(M)
+    Luv = np.empty((nu, nv))
+    for n in range(nv):
+        Luv[:, n] = lscale * decay ** n * rng.standard_normal(nu) / np.sqrt(nu)
+    Likn = np.einsum("iu,ku,un->ikn", X, X, Luv)
+    _, evecs = np.linalg.eigh(h1)
+    nup = N
+    ndn = N if walker_type == CLOSED else N - 1
+    PsiT = [np.ascontiguousarray(evecs[:, :nup].conj().T).astype(np.complex128)]
+    if walker_type == COLLINEAR:
+        PsiT.append(np.ascontiguousarray(evecs[:, :ndn].conj().T).astype(np.complex128))
+    wl = Workload("thc", M, nup, ndn, nv, W, dt, walker_type, h1[None].astype(np.complex128),
+                  Likn[None], 0.0, PsiT)
+    return wl, X, Luv
+
+
 # --------------------------------------------------------------------------------------------
 # Particle-hole multi-determinant (PHMSD) trial
 # --------------------------------------------------------------------------------------------
