@@ -79,6 +79,10 @@ def parse():
                          "split with one / two walkers in flight per CTA, 4 / 5 the same in the "
                          "FP16 split, 6 / 7 one walker in flight with the running sum in tensor "
                          "memory")
+    ap.add_argument("--no-tile-tune", action="store_true",
+                    help="keep the default tile shapes (vbias 128-wide tiles, symmetric vHS, "
+                         "exchange L2 blocks of 64 vector pairs) instead of timing the "
+                         "alternatives")
     ap.add_argument("--profile-case", default=None,
                     choices=["step", "taylor", "vhs", "exchange", "phmsd-energy"],
                     help="run one small case for an ncu capture instead of the bench: the "
@@ -613,6 +617,11 @@ def run_ours(args):
         # the library's autotuner times each Taylor variant on these walkers (state restored)
         best, ms = sim.autotune()
         tuned = {"taylor_mode": best, "step_ms": ms}
+    if prec == A.PREC_MIXED and not args.no_tile_tune:
+        # tile shapes / orders with bit-identical results: vbias tile width, vHS form, the
+        # exchange kernel's L2 block
+        tiles, tile_ms = sim.autotune_tiles()
+        tuned = dict(tuned or {}, tiles=tiles, tile_ms=tile_ms)
 
     t_ms, launches, nseg, clk = _timed_blocks(sim, args.steps, args.warmup, world, local,
                                               ClockSampler(local))
@@ -620,7 +629,7 @@ def run_ours(args):
     sim.restart()
     phases = _phases(sim)
     roofline = _roofline(sim, wl, W, prec, phases, args, torch,
-                         tuned["taylor_mode"] if tuned else args.taylor_mode)
+                         (tuned or {}).get("taylor_mode", args.taylor_mode))
 
     e2e = None if args.no_e2e else _e2e(sim, W, wl.Nc, args.steps, args.warmup, world, prec)
 
@@ -653,14 +662,14 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "c128" if prec == A.PREC_FP64 else _mixed_dtype(
-                split_f16, tuned["taylor_mode"] if tuned else args.taylor_mode,
+                split_f16, (tuned or {}).get("taylor_mode", args.taylor_mode),
                 args.exchange_split),
             "data": "synthetic",
             "config": {"workload": "M=200 N=50+50 Nc=1600 W=1024/GPU dt=0.005 taylor=6, "
                                    "block of 10 steps (ortho/5, comb/10, energy/10)",
                        "precision": args.precision, "global_walkers": W * world,
                        "exchange_split": args.exchange_split if prec == A.PREC_MIXED else None,
-                       "taylor_mode": (tuned["taylor_mode"] if tuned else args.taylor_mode)
+                       "taylor_mode": ((tuned or {}).get("taylor_mode", args.taylor_mode))
                                       if prec == A.PREC_MIXED else None,
                        "autotune": tuned,
                        "step_graph": not args.no_graph,

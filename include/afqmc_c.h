@@ -408,6 +408,18 @@ int afqmc_prop_step_flags(afqmc_prop prop, afqmc_wset ws, const double* Eshift_d
  * a variant not tried: 4, 5 and 7 need the FP16 split).  Synchronous. */
 int afqmc_prop_autotune(afqmc_prop prop, afqmc_wset ws, int* best, float* ms,
                         afqmc_stream stream);
+/* Tile shapes and orders of the mixed-precision contractions that leave every result bit for
+ * bit the same, timed on the live walkers with their state restored (no reference counterpart:
+ * the reference's GEMMs are library calls): the vbias CTA tile width (128 / 64 Cholesky
+ * vectors), the vHS form (i <= k pairs mirrored / all pairs) and the exchange kernel's L2 block
+ * (16 / 32 / 64 / 128 vector pairs of its tile order).  choice [3] = the kept (width, symmetric,
+ * block), -1 where nothing was tuned (complex128 or multi-determinant propagators); ms [8] = the
+ * candidates' times in that order (ms per step, then ms per energy evaluation), may be NULL. */
+int afqmc_prop_autotune_tiles(afqmc_prop prop, afqmc_wset ws, int* choice, float* ms,
+                              afqmc_stream stream);
+/* the same choices by hand / as they stand (defaults 128 and 64) */
+int afqmc_ham_set_tiles(afqmc_ham ham, int vbias_bn, int exchange_block);
+int afqmc_ham_get_tiles(afqmc_ham ham, int* vbias_bn, int* exchange_block);
 /* AFQMCBasePropagator::Orthogonalize (cpp:735-741): QR re-orthonormalisation then OVLP refresh. */
 int afqmc_prop_orthogonalize(afqmc_prop prop, afqmc_wset ws, afqmc_stream stream);
 /* Seeds / advances the device field generator (Philox4x32-10, counter = step). */

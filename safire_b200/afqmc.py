@@ -196,6 +196,16 @@ class HamiltonianOperations:
         call("afqmc_ham_one_body_propagator", self.handle, float(dt), _host_ptr(vm), _host_ptr(H1))
         return H1
 
+    def set_tiles(self, vbias_bn=128, exchange_block=64):
+        """Tile width of the mixed vbias GEMM (128 / 64) and L2 block of the exchange kernel's
+        tile order: the results do not depend on them."""
+        call("afqmc_ham_set_tiles", self.handle, int(vbias_bn), int(exchange_block))
+
+    def get_tiles(self):
+        a, b = C.c_int(), C.c_int()
+        call("afqmc_ham_get_tiles", self.handle, C.byref(a), C.byref(b))
+        return a.value, b.value
+
     def set_exchange_split(self, nsplit):
         """3: 3xTF32 exchange contraction (default); 1: plain TF32."""
         call("afqmc_ham_set_exchange_split", self.handle, int(nsplit))
@@ -524,6 +534,21 @@ class Propagator:
         call("afqmc_prop_autotune", self.handle, wset.handle, C.byref(best), _host_ptr(ms),
              _stream(stream))
         return best.value, {m: float(t) for m, t in zip((0, 2, 3, 4, 5, 6, 7), ms) if t > 0}
+
+    def autotune_tiles(self, wset: WalkerSet, stream=None):
+        """Picks the tile shapes / orders that leave the results bit for bit the same (vbias
+        tile width, vHS form, exchange L2 block) on these walkers; returns ({'vbias_bn',
+        'vhs_symmetric', 'exchange_block'}, {candidate: ms}).  The walkers are left as they
+        were."""
+        ch = (C.c_int * 3)()
+        ms = np.zeros(8, dtype=np.float32)
+        call("afqmc_prop_autotune_tiles", self.handle, wset.handle, ch,
+             ms.ctypes.data_as(C.POINTER(C.c_float)), _stream(stream))
+        names = ["vbias_bn=128", "vbias_bn=64", "vhs_symmetric", "vhs_all_pairs",
+                 "exchange_block=16", "exchange_block=32", "exchange_block=64",
+                 "exchange_block=128"]
+        return ({"vbias_bn": ch[0], "vhs_symmetric": ch[1], "exchange_block": ch[2]},
+                {n: float(t) for n, t in zip(names, ms) if t > 0})
 
     def set_trial(self, trial, vMF=None):
         """Steps with a multi-determinant trial (PHMSD or NOMSDMulti: vbias and overlaps from

@@ -58,6 +58,9 @@ _SIGS = {
                                    vp, C.POINTER(vp)]),
     "afqmc_ham_thc_info": (i32, [vp, C.POINTER(i32), C.POINTER(i32)]),
     "afqmc_ham_destroy": (i32, [vp]),
+    "afqmc_prop_autotune_tiles": (i32, [vp, vp, C.POINTER(i32), C.POINTER(C.c_float), vp]),
+    "afqmc_ham_set_tiles": (i32, [vp, i32, i32]),
+    "afqmc_ham_get_tiles": (i32, [vp, C.POINTER(i32), C.POINTER(i32)]),
     "afqmc_ham_info": (i32, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), C.POINTER(i32),
                              C.POINTER(i32), C.POINTER(f64)]),
     "afqmc_ham_get_tensors": (i32, [vp, vp, vp, vp]),

@@ -1946,6 +1946,162 @@ extern "C" int afqmc_prop_autotune(afqmc_prop pr, afqmc_wset ws, int* best, floa
   return st ? st : st2;
 }
 
+// Tile shapes and orders of the mixed-precision contractions that leave every result bit for bit
+// the same, timed on the live walkers (state restored): the vbias CTA tile width (128 / 64
+// Cholesky vectors, one step each), the vHS form (i <= k pairs mirrored / all pairs, when the
+// Cholesky vectors are symmetric; one step each) and the exchange kernel's L2 block (16 / 32 / 64
+// / 128 vector pairs, one energy evaluation each).  choice [3] = the kept (bn, symmetric, block);
+// ms [8] = the times in that order (0 for a candidate not run).
+extern "C" int afqmc_prop_autotune_tiles(afqmc_prop pr, afqmc_wset ws, int* choice, float* ms,
+                                         afqmc_stream stream) {
+  AFQMC_CHECK_ARG(pr && ws && choice, "afqmc_prop_autotune_tiles: null argument");
+  AFQMC_CHECK_ARG(wset_matches(pr->ham, ws), "afqmc_prop_autotune_tiles: walker set / Hamiltonian mismatch");
+  AFQMC_CHECK_ARG(ws->W <= pr->maxW, "afqmc_prop_autotune_tiles: too many walkers");
+  DeviceGuard g(pr->device);
+  afqmc_ham_s* h = pr->ham;
+  for (int k = 0; k < 8; ++k)
+    if (ms) ms[k] = 0.f;
+  choice[0] = choice[1] = choice[2] = -1;
+  if (pr->p.precision != AFQMC_PREC_MIXED || pr->ph || pr->md) return AFQMC_OK;  // no choice
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (!h->mixed) {
+    EnergyArgs a = energy_args(h, nullptr, 0);
+    AFQMC_TRY(mixed_ham_create(&h->mixed, a, s));
+  }
+  MixedHam* m = h->mixed;
+  const size_t nbuf = size_t(ws->W) * ws->walker_size;
+  Scratch save, aux;
+  AFQMC_TRY(save.get(sizeof(c128) * nbuf, s));
+  AFQMC_TRY(aux.get(sizeof(unsigned long long) * 9, s));
+  unsigned long long* auxp = reinterpret_cast<unsigned long long*>(aux.p);
+  AFQMC_CUDA_TRY(cudaMemcpyAsync(save.p, ws->buf, sizeof(c128) * nbuf, cudaMemcpyDeviceToDevice, s));
+  AFQMC_CUDA_TRY(cudaMemcpyAsync(auxp, pr->counter, sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToDevice, s));
+  AFQMC_CUDA_TRY(cudaMemcpyAsync(auxp + 1, pr->stats, 8 * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToDevice, s));
+  auto restore = [&]() -> int {
+    AFQMC_CUDA_TRY(cudaMemcpyAsync(ws->buf, save.p, sizeof(c128) * nbuf, cudaMemcpyDeviceToDevice, s));
+    AFQMC_CUDA_TRY(cudaMemcpyAsync(pr->counter, auxp, sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToDevice, s));
+    AFQMC_CUDA_TRY(cudaMemcpyAsync(pr->stats, auxp + 1, 8 * sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToDevice, s));
+    return AFQMC_OK;
+  };
+  cudaEvent_t e0, e1;
+  AFQMC_CUDA_TRY(cudaEventCreate(&e0));
+  AFQMC_CUDA_TRY(cudaEventCreate(&e1));
+  // mean time of `body` over two runs after one warm-up run, each from the restored state
+  auto timed = [&](auto&& body, float* out) -> int {
+    float t = 0.f;
+    for (int rep = 0; rep < 3; ++rep) {
+      AFQMC_TRY(restore());
+      if (rep > 0 && cudaEventRecord(e0, s) != cudaSuccess) return AFQMC_ERR_CUDA;
+      AFQMC_TRY(body());
+      if (rep > 0) {
+        float x = 0.f;
+        if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&x, e0, e1) != cudaSuccess)
+          return AFQMC_ERR_CUDA;
+        t += x;
+      }
+    }
+    *out = t / 2;
+    return AFQMC_OK;
+  };
+  auto step = [&]() -> int { return prop_step(pr, ws, 0.0, nullptr, nullptr, 0, s); };
+  int st = AFQMC_OK;
+  int bn0 = 128, blk0 = 64;
+  mixed_get_tiles(m, &bn0, &blk0);
+  // vbias tile width
+  {
+    const int cand[2] = {128, 64};
+    float best = 1e30f;
+    for (int k = 0; k < 2 && !st; ++k) {
+      float t = 0.f;
+      if (!(st = mixed_set_tiles(m, cand[k], blk0)) && !(st = timed(step, &t))) {
+        if (ms) ms[k] = t;
+        if (t < best) {
+          best = t;
+          choice[0] = cand[k];
+        }
+      }
+    }
+    if (!st) st = mixed_set_tiles(m, choice[0], blk0);
+  }
+  // vHS form (only when the symmetric one is available)
+  if (!st) {
+    int active = 0;
+    st = mixed_set_vhs_symmetry(m, 1, &active);
+    if (!st && active) {
+      float t1 = 0.f, t0 = 0.f;
+      if (!(st = timed(step, &t1)) && !(st = mixed_set_vhs_symmetry(m, 0, &active)) &&
+          !(st = timed(step, &t0))) {
+        if (ms) {
+          ms[2] = t1;
+          ms[3] = t0;
+        }
+        choice[1] = t1 <= t0 ? 1 : 0;
+        st = mixed_set_vhs_symmetry(m, choice[1], &active);
+      }
+    } else if (!st) {
+      choice[1] = 0;
+    }
+  }
+  // exchange L2 block, on the walkers' own density matrix
+  if (!st) {
+    const int W = ws->W;
+    const long ldG = long(h->nel_tot) * h->M;
+    const int nmax = h->nel[0] > h->nel[1] ? h->nel[0] : h->nel[1];
+    Scratch Gb, Tb, ov, E;
+    if (!(st = Gb.get(sizeof(c128) * size_t(W) * ldG, s)) &&
+        !(st = Tb.get(sizeof(c128) * size_t(W) * nmax * nmax, s)) &&
+        !(st = ov.get(sizeof(c128) * size_t(W), s)) && !(st = E.get(sizeof(c128) * 3 * size_t(W), s)))
+      st = wfn_density_matrix(h, ws, s, (c128*)Gb.p, ldG, (c128*)ov.p, (c128*)Tb.p);
+    const int cand[4] = {16, 32, 64, 128};
+    float best = 1e30f;
+    for (int k = 0; k < 4 && !st; ++k) {
+      auto energy = [&]() -> int {
+        return ham_energy(h, s, (const c128*)Gb.p, ldG, (c128*)E.p, W, true, true, true,
+                          AFQMC_PREC_MIXED);
+      };
+      float t = 0.f;
+      if (!(st = mixed_set_tiles(m, choice[0], cand[k])) && !(st = timed(energy, &t))) {
+        if (ms) ms[4 + k] = t;
+        if (t < best) {
+          best = t;
+          choice[2] = cand[k];
+        }
+      }
+    }
+    if (!st) st = mixed_set_tiles(m, choice[0], choice[2]);
+  }
+  const int st2 = restore();
+  if (cudaStreamSynchronize(s) != cudaSuccess && !st) st = AFQMC_ERR_CUDA;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st ? st : st2;
+}
+
+// the current tile choices of the mixed-precision contractions (vbias tile width, exchange block)
+extern "C" int afqmc_ham_get_tiles(afqmc_ham h, int* vbias_bn, int* exchange_block) {
+  AFQMC_CHECK_ARG(h && vbias_bn && exchange_block, "afqmc_ham_get_tiles: null argument");
+  *vbias_bn = 128;
+  *exchange_block = 64;
+  if (h->mixed) mixed_get_tiles(h->mixed, vbias_bn, exchange_block);
+  return AFQMC_OK;
+}
+
+// set the tile choices by hand (bn 128 / 64, block >= 1; results are the same bit for bit)
+extern "C" int afqmc_ham_set_tiles(afqmc_ham h, int vbias_bn, int exchange_block) {
+  AFQMC_CHECK_ARG(h, "afqmc_ham_set_tiles: null argument");
+  DeviceGuard g(h->device);
+  if (!h->mixed) {
+    EnergyArgs a = energy_args(h, nullptr, 0);
+    AFQMC_TRY(mixed_ham_create(&h->mixed, a, nullptr));
+  }
+  return mixed_set_tiles(h->mixed, vbias_bn, exchange_block);
+}
+
 extern "C" int afqmc_prop_orthogonalize(afqmc_prop pr, afqmc_wset ws, afqmc_stream stream) {
   AFQMC_CHECK_ARG(pr && ws, "afqmc_prop_orthogonalize: null handle");
   AFQMC_CHECK_ARG(wset_matches(pr->ham, ws), "afqmc_prop_orthogonalize: mismatch");

@@ -25,7 +25,7 @@ constexpr int XBK = 32;
 constexpr int XSLOT_A = 64;      // rows per walker slot
 constexpr int XSLOT_B = 56;      // cols per Cholesky-vector slot (N <= 56)
 constexpr int XBN = 2 * XSLOT_B; // 112
-constexpr int NBLK = 64;         // n-pairs per L2 block of the tile order
+constexpr int NBLK_DEFAULT = 64; // n-pairs per L2 block of the tile order (autotuned: 16..128)
 
 struct XParams {
   CUtensorMap a[4];  // G planes as {M, N, W}: re_hi, re_lo, im_hi, im_lo
@@ -35,6 +35,7 @@ struct XParams {
   c128* kl;          // [W][Nc] += trace T
   const float* ginv; // FP16 operands: per-walker inverse scale of G (null for TF32)
   float linv;        // FP16 operands: inverse scale of Lnak
+  int nblk;          // vector pairs per L2 block of the tile order
   unsigned* err;
 };
 
@@ -65,13 +66,16 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
   for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void tile_coords(long t, int WP, int NP, int& wp, int& np) {
-  const long per_blk = long(WP) * NBLK;
+// tile t -> (walker pair, vector pair): blocks of nblk vector pairs, inside a block all walker
+// pairs for each vector pair in turn, so that a block's Lnak planes stay in L2 while every
+// walker pair passes
+__device__ __forceinline__ void tile_coords(long t, int WP, int NP, int nblk, int& wp, int& np) {
+  const long per_blk = long(WP) * nblk;
   const int nb = int(t / per_blk);
   const long within = t % per_blk;
-  const int width = min(NBLK, NP - nb * NBLK);
+  const int width = min(nblk, NP - nb * nblk);
   wp = int(within / width);
-  np = nb * NBLK + int(within % width);
+  np = nb * nblk + int(within % width);
 }
 
 template <int NSPLIT, bool F16>
@@ -127,7 +131,7 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
       long it = 0;  // global k-chunk counter (stage ring position)
       for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
         int wp, np;
-        tile_coords(t, WP, NP, wp, np);
+        tile_coords(t, WP, NP, p.nblk, wp, np);
         bool ok = true;
         for (int kc = 0; kc < nk; ++kc, ++it) {
           const int s = int(it % K::STAGES);
@@ -214,7 +218,7 @@ __global__ void __launch_bounds__(XT_THREADS, 1) exchange_tc_kernel(const __grid
     long ti = 0;
     for (long t = blockIdx.x; t < ntiles; t += gridDim.x, ++ti) {
       int wp, np;
-      tile_coords(t, WP, NP, wp, np);
+      tile_coords(t, WP, NP, p.nblk, wp, np);
       const int buf = int(ti & 1);
       // the four epilogue warps meet at named barriers below: they leave the loop together, on
       // the outcome of all four waits (a wait that gave up on one warp ends every warp's loop)
@@ -343,7 +347,8 @@ int launch_exchange(cudaStream_t s, const XParams& p, int grid) {
 // g_inv[w] and l_inv the inverse scales).
 int exchange_fused_tc(cudaStream_t s, const void* const Gp[4], int esize, long ldG, long off,
                       const void* const Lp[2], int W, int N, int Nc, int M, int nsplit,
-                      const float* g_inv, float l_inv, c128* exx, c128* kl, unsigned* err) {
+                      const float* g_inv, float l_inv, c128* exx, c128* kl, unsigned* err,
+                      int nblk) {
   if (N > 50 || N < 1) {
     set_error_detail("exchange_fused_tc: N = %d outside 1..50", N);
     return AFQMC_ERR_UNSUPPORTED;
@@ -369,6 +374,7 @@ int exchange_fused_tc(cudaStream_t s, const void* const Gp[4], int esize, long l
   p.kl = kl;
   p.ginv = g_inv;
   p.linv = l_inv;
+  p.nblk = nblk > 0 ? nblk : NBLK_DEFAULT;
   p.err = err;
   if (g_num_sms == 0) {
     int dev = 0;

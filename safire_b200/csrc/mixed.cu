@@ -863,6 +863,9 @@ struct MixedHam {
   // dynamic operands, sized on demand
   int capW = 0;
   int exchange_split = 3;  // TF32 products per real product in the exchange contraction
+  // tile shapes / orders with bit-identical results, chosen by afqmc_prop_autotune_tiles
+  int vbias_bn = 128;      // columns (Cholesky vectors) per vbias CTA tile: 128 or 64
+  int exch_nblk = 64;      // vector pairs per L2 block of the exchange tile order
   bool likn_sym = false;   // every L_n symmetric (to 1e-10 of max |L|): vHS computes i <= k only
   bool vhs_sym = true;     // use the symmetric vHS when likn_sym
   // Operand format of vbias, vHS and the exchange: FP16 split with power-of-two scales when the
@@ -1122,8 +1125,9 @@ int vbias_mixed_f16(cudaStream_t s, MixedHam* m, const c128* G, long ldG, c128* 
   }
   for (int q = 0; q < 4; ++q)
     AFQMC_TRY(make_map_es(&p.a[q], m->G16, q, 0, Kc, W, m->G16.ld, S, Kc, 128));
+  const int bn = m->vbias_bn == 64 ? 64 : 128;
   for (int q = 0; q < 2; ++q)
-    AFQMC_TRY(make_map_es(&p.b[q], m->Lnak16, q, 0, Kc, m->Nc, m->Lnak16.ld, S, Kc, 128));
+    AFQMC_TRY(make_map_es(&p.b[q], m->Lnak16, q, 0, Kc, m->Nc, m->Lnak16.ld, S, Kc, bn));
   p.m = W; p.n = m->Nc; p.k = int(Kc);
   p.a_batched = 1; p.b_batched = 1;
   p.order = 1;
@@ -1131,7 +1135,10 @@ int vbias_mixed_f16(cudaStream_t s, MixedHam* m, const c128* G, long ldG, c128* 
   p.row_inv = m->g_inv;
   p.out_c = out; p.outc_ld = m->Nc; p.outc_bs = long(W) * m->Nc;
   p.err = m->err;
-  AFQMC_TRY((launch_tc<true, false, 128, 2, EPI_C128, true>(s, p, S)));
+  if (bn == 64)
+    AFQMC_TRY((launch_tc<true, false, 64, 2, EPI_C128, true>(s, p, S)));
+  else
+    AFQMC_TRY((launch_tc<true, false, 128, 2, EPI_C128, true>(s, p, S)));
   if (S > 1) {
     const long n = long(W) * m->Nc;
     sum_partials_kernel<<<ceil_div(n, 256), 256, 0, s>>>(m->vpart, S, n, v, 0);
@@ -1573,7 +1580,8 @@ int exchange_T_tc(cudaStream_t s, MixedHam* m, int sp, int w0, int wc, c128* wor
 
 int exchange_fused_tc(cudaStream_t s, const void* const Gp[4], int esize, long ldG, long off,
                       const void* const Lp[2], int W, int N, int Nc, int M, int nsplit,
-                      const float* g_inv, float l_inv, c128* exx, c128* kl, unsigned* err);
+                      const float* g_inv, float l_inv, c128* exx, c128* kl, unsigned* err,
+                      int nblk);
 
 bool exchange_fused_ok(MixedHam* m, int sp) {
   return !m->lnak_cplx && m->nel[sp] >= 1 && m->nel[sp] <= 50;
@@ -1584,12 +1592,14 @@ int exchange_fused(cudaStream_t s, MixedHam* m, int sp, int W, c128* exx, c128* 
     const void* Gp[4] = {m->G16.p[0], m->G16.p[1], m->G16.p[2], m->G16.p[3]};
     const void* Lp[2] = {m->Lnak16.p[0], m->Lnak16.p[1]};
     return exchange_fused_tc(s, Gp, 2, m->G16.ld, 0, Lp, W, m->nel[0], m->Nc, m->M,
-                             m->exchange_split, m->g_inv, m->lnak_inv, exx, kl, m->err);
+                             m->exchange_split, m->g_inv, m->lnak_inv, exx, kl, m->err,
+                             m->exch_nblk);
   }
   const void* Gp[4] = {m->G.p[0], m->G.p[1], m->G.p[2], m->G.p[3]};
   const void* Lp[2] = {m->Lnak[sp].p[0], m->Lnak[sp].p[1]};
   return exchange_fused_tc(s, Gp, 4, m->G.ld, long(m->el_off[sp]) * m->M, Lp, W, m->nel[sp],
-                           m->Nc, m->M, m->exchange_split, nullptr, 1.f, exx, kl, m->err);
+                           m->Nc, m->M, m->exchange_split, nullptr, 1.f, exx, kl, m->err,
+                           m->exch_nblk);
 }
 
 int mixed_set_split_format(MixedHam* m, int format, int* active_f16) {
@@ -1657,6 +1667,26 @@ int mixed_clear_error(MixedHam* m) {
 
 int mixed_error_flag(MixedHam* m, unsigned* flag) {
   AFQMC_CUDA_TRY(cudaMemcpy(flag, m->err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  return AFQMC_OK;
+}
+
+int mixed_set_tiles(MixedHam* m, int vbias_bn, int exch_nblk) {
+  if (vbias_bn != 64 && vbias_bn != 128) {
+    set_error_detail("vbias tile width must be 64 or 128 (got %d)", vbias_bn);
+    return AFQMC_ERR_ARG;
+  }
+  if (exch_nblk < 1 || exch_nblk > 1024) {
+    set_error_detail("exchange block must be 1..1024 vector pairs (got %d)", exch_nblk);
+    return AFQMC_ERR_ARG;
+  }
+  m->vbias_bn = vbias_bn;
+  m->exch_nblk = exch_nblk;
+  return AFQMC_OK;
+}
+
+int mixed_get_tiles(MixedHam* m, int* vbias_bn, int* exch_nblk) {
+  *vbias_bn = m->vbias_bn;
+  *exch_nblk = m->exch_nblk;
   return AFQMC_OK;
 }
 

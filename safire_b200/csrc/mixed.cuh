@@ -41,6 +41,11 @@ int mixed_set_vhs_symmetry(MixedHam* m, int enable, int* active);
 int mixed_set_split_format(MixedHam* m, int format, int* active_f16);
 // 3: 3xTF32 (default), 1: single TF32 product in the exchange contraction
 int mixed_set_exchange_split(MixedHam* m, int nsplit);
+// tile shapes and orders that leave every result bit for bit the same: the vbias CTA tile width
+// (128 or 64 Cholesky vectors) and the exchange kernel's L2 block (vector pairs per block of its
+// tile order)
+int mixed_set_tiles(MixedHam* m, int vbias_bn, int exch_nblk);
+int mixed_get_tiles(MixedHam* m, int* vbias_bn, int* exch_nblk);
 // one bounded device wait that nothing completes, with a budget of `budget` cycles (at most the
 // kernels' own): AFQMC_ERR_TIMEOUT and bit 0 of the error word when it gave up
 int mixed_wait_selftest(cudaStream_t s, MixedHam* m, long long budget);

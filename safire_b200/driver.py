@@ -201,6 +201,15 @@ class Simulation:
         self.graph = None  # a captured step holds the previous variant's kernels
         return best, ms
 
+    def autotune_tiles(self):
+        """Let the library pick the tile shapes / orders with bit-identical results (vbias tile
+        width, vHS form, exchange L2 block) for these walkers; the walkers are left as they
+        were.  Returns ({choice: value}, {candidate: ms})."""
+        out = self.prop.autotune_tiles(self.wset)
+        self._g_ready = False
+        self.graph = None  # a captured step holds the previous tiles' kernels
+        return out
+
     def average_pseudo_energy(self):
         s = _sum_over_ranks(A.pseudo_energy_sums(self.wset, self.dt))
         s = s.cpu().numpy()

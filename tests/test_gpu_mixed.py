@@ -209,6 +209,40 @@ def test_autotune_leaves_the_run_unchanged(cuda):
     assert torch.equal(runs[0], runs[1])
 
 
+def test_tile_candidates_are_bit_identical(cuda):
+    """Every tile choice the tile autotuner picks among gives the same results bit for bit:
+    vbias with 128- and 64-wide tiles, the exchange energy with every L2 block size; and the
+    autotuner leaves the walkers as they were."""
+    import torch
+    from safire_b200 import afqmc as A
+    from safire_b200.driver import RunParams, Simulation
+    from safire_b200.synth import make_workload
+    wl = make_workload("cfg2", W=160, Nc=400)
+    sim = Simulation.from_workload(wl, W=160, precision=A.PREC_MIXED,
+                                   rp=RunParams(equilibration_steps=0, seed=5))
+    sim.step()
+    G, _ = sim.wfn.MixedDensityMatrix(sim.wset)
+    outs_v, outs_e = [], []
+    for bn, blk in [(128, 64), (64, 16), (128, 32), (64, 128)]:
+        sim.ham.set_tiles(bn, blk)
+        v = torch.zeros((160, wl.Nc), dtype=torch.complex128, device="cuda")
+        sim.ham.vbias(G, v, wl.dt, precision=A.PREC_MIXED)
+        E = torch.zeros((160, 3), dtype=torch.complex128, device="cuda")
+        sim.ham.energy(E, G, precision=A.PREC_MIXED)
+        outs_v.append(v)
+        outs_e.append(E)
+    for v, E in zip(outs_v[1:], outs_e[1:]):
+        assert torch.equal(v, outs_v[0])
+        assert torch.equal(E, outs_e[0])
+    before = sim.wset.buffer.clone()
+    tiles, ms = sim.autotune_tiles()
+    print("tile autotuner:", tiles, {k: round(t, 3) for k, t in ms.items()})
+    assert tiles["vbias_bn"] in (64, 128) and tiles["exchange_block"] in (16, 32, 64, 128)
+    assert tiles["vhs_symmetric"] in (0, 1)
+    assert torch.equal(sim.wset.buffer, before)
+    assert sim.ham.get_tiles() == (tiles["vbias_bn"], tiles["exchange_block"])
+
+
 @pytest.mark.parametrize("mode", [2, 4, 5, 7])
 @pytest.mark.parametrize("name,W,Nc,order", [("cfg1", 300, None, None), ("cfg1", 20, None, 0),
                                              ("cfg1", 301, None, 3)])
