@@ -426,9 +426,10 @@ def _phases(sim):
 
 
 def _e2e(sim, W, Nc, steps, warmup, world, prec):
-    """The same blocks through the public API with every block's field uniforms copied in from
-    pinned host memory and the weights + energy estimate read back, timed like the resident
-    blocks (restart-separated segments, _segmented)."""
+    """The same blocks through the public API with every step's field uniforms copied in from
+    pinned host memory (on a copy stream, overlapping the steps before it) and the weights +
+    energy estimate read back, timed like the resident blocks (restart-separated segments,
+    _segmented); the step replays its captured graph, refilling the graph's field buffer."""
     import torch
     import torch.distributed as dist
     from safire_b200 import afqmc as A
@@ -436,10 +437,20 @@ def _e2e(sim, W, Nc, steps, warmup, world, prec):
     dev_u = torch.empty((BLOCK, W, Nc), dtype=torch.float64, device="cuda")
     host_w = torch.empty((W,), dtype=torch.complex128).pin_memory()
     host_e = torch.empty((4,), dtype=torch.complex128).pin_memory()
+    copy_stream = torch.cuda.Stream()
+    copied = [torch.cuda.Event() for _ in range(BLOCK)]
 
     def block_e2e():
-        dev_u.copy_(host_u, non_blocking=True)
+        # every step's uniforms cross PCIe on a copy stream, step s waiting for its own copy
+        # only: the transfers of later steps overlap the computation of earlier ones
+        compute = torch.cuda.current_stream()
+        copy_stream.wait_stream(compute)  # the previous block's steps are done with dev_u
+        with torch.cuda.stream(copy_stream):
+            for s in range(BLOCK):
+                dev_u[s].copy_(host_u[s], non_blocking=True)
+                copied[s].record(copy_stream)
         for s in range(BLOCK):
+            compute.wait_event(copied[s])
             sim.step(dev_u[s], measure=False)
         E, _ = sim.wfn.Energy(sim.wset, set_properties=False, precision=prec)
         sums = A.energy_sums(sim.wset, E)

@@ -116,6 +116,8 @@ class Simulation:
     energies: list = field(default_factory=list)
     use_graph: bool = False
     graph: StepGraph = None
+    graph_u: StepGraph = None  # the captured step for fields given on the device
+    _u_buf: torch.Tensor = None
     # the step leaves the density matrix of the propagated walkers for the next step, which
     # skips recomputing it unless orthogonalisation or population control changed the walkers
     reuse_density: bool = True
@@ -198,7 +200,7 @@ class Simulation:
         the walkers are left as they were.  Returns (mode, {mode: step ms})."""
         best, ms = self.prop.autotune(self.wset)
         self._g_ready = False
-        self.graph = None  # a captured step holds the previous variant's kernels
+        self.graph = self.graph_u = None  # a captured step holds the previous variant's kernels
         return best, ms
 
     def autotune_tiles(self):
@@ -207,7 +209,7 @@ class Simulation:
         were.  Returns ({choice: value}, {candidate: ms})."""
         out = self.prop.autotune_tiles(self.wset)
         self._g_ready = False
-        self.graph = None  # a captured step holds the previous tiles' kernels
+        self.graph = self.graph_u = None  # a captured step holds the previous tiles' kernels
         return out
 
     def average_pseudo_energy(self):
@@ -242,6 +244,15 @@ class Simulation:
             if self.graph is None:
                 self.graph = StepGraph(self.prop, self.wset, self._eshift_dev)
             self.graph.replay(flags)
+        elif (self.use_graph and uniforms is not None and uniforms.is_cuda
+              and (step > 0 or self.graph_u is not None)):
+            # fields given on the device: a second captured step reads them from a fixed buffer,
+            # refilled here (a device copy on the step's stream)
+            if self.graph_u is None:
+                self._u_buf = torch.empty_like(uniforms)
+                self.graph_u = StepGraph(self.prop, self.wset, self._eshift_dev, self._u_buf)
+            self._u_buf.copy_(uniforms)
+            self.graph_u.replay(flags)
         else:
             self.prop.Propagate_flags(self.wset, self._eshift_dev, uniforms, flags)
         self._g_ready = self.reuse_density

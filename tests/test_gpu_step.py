@@ -210,6 +210,30 @@ def test_graph_step_matches_eager(cuda, precision):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
+def test_graph_step_with_given_fields_matches_eager(cuda, precision):
+    """Fields given on the device: the replayed step (its field buffer refilled before each
+    replay) equals the eager step, bit for bit."""
+    from safire_b200.driver import RunParams, Simulation
+    wl = make_workload("cfg1", W=24)
+    rs = np.random.default_rng(4)
+    U = torch.as_tensor(rs.random((14, 24, wl.Nc)), device="cuda")
+    sims = []
+    for g in (False, True):
+        sim = Simulation.from_workload(wl, W=24, precision=precision,
+                                       rp=RunParams(equilibration_steps=6))
+        sim.use_graph = g
+        sims.append(sim)
+    for k in range(14):
+        for sim in sims:
+            sim.step(U[k])
+    torch.cuda.synchronize()
+    assert sims[1].graph_u is not None and sims[1].graph_u.kernels_replayed() > 0
+    a, b = (to_host(s.wset.buffer) for s in sims)
+    assert np.array_equal(a, b)
+    assert sims[0].energies == sims[1].energies
+
+
+@pytest.mark.parametrize("precision", [0, 1])
 def test_density_reuse_matches_recompute(cuda, precision):
     """Steps that keep the propagated walkers' density matrix for the next step (skipped
     recomputation between orthogonalisations / combs) give the same run as recomputing it at
