@@ -174,20 +174,31 @@ struct afqmc_host_rng_s {
 };
 
 // NOMSD with several determinants (NOMSD.hpp / NOMSD.cpp, ci.size() > 1): one Hamiltonian
-// handle per determinant (its half-rotated tensors), the coefficients ci
+// handle per determinant (its half-rotated tensors), the coefficients ci.
+// The propagation step batches over the determinants: PsiTall holds every determinant's
+// PsiT stacked per spin ([nd][N_s][M] at nd * el_off[s] * M), so one GEMM per walker forms the
+// overlap matrices of all determinants, one Gauss-Jordan launch inverts them, and one GEMM
+// with K = nd * N_s sums the weighted full density matrices.  Walkers go in chunks of wchunk
+// (the batched GEMM's grid limit and a bounded workspace): Tb [wchunk][nd][N_s][N_s] and
+// Gcb [wchunk][nd][N_s][M] per spin, ovd / wdd [wchunk][nd].
 struct afqmc_nomsd_s {
   int device = 0;
   std::vector<afqmc_ham_s*> hams;
   std::vector<c128> ci;
-  c128 *Gd = nullptr, *Gc = nullptr, *ov = nullptr, *wd = nullptr, *T = nullptr, *Ed = nullptr;
-  int capW = 0;
+  c128 *PsiTall = nullptr, *dcc = nullptr, *dlc = nullptr;  // conj(ci), log conj(ci)
+  c128 *Gc = nullptr, *ov = nullptr, *T = nullptr, *Ed = nullptr;  // energy (per determinant)
+  c128 *Tb = nullptr, *Gcb = nullptr, *ovd = nullptr, *wdd = nullptr;
+  int capW = 0, wchunk = 0;
   void free_bufs() {
-    dfree(Gd); dfree(Gc); dfree(ov); dfree(wd); dfree(T); dfree(Ed);
+    dfree(Gc); dfree(ov); dfree(T); dfree(Ed);
+    dfree(Tb); dfree(Gcb); dfree(ovd); dfree(wdd);
     capW = 0;
+    wchunk = 0;
   }
   ~afqmc_nomsd_s() {
     DeviceGuard g(device);
     free_bufs();
+    dfree(PsiTall); dfree(dcc); dfree(dlc);
   }
 };
 
@@ -944,11 +955,6 @@ __global__ void broadcast_row_kernel(c128* buf, long walker_size, int W, const c
   long total = long(W) * walker_size;
   if (e < total) buf[e] = row[e % walker_size];
 }
-// x[w] += c
-__global__ void add_scalar_kernel(c128* __restrict__ x, int W, c128 c) {
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w < W) x[w] = cadd(x[w], c);
-}
 }  // namespace api_kernels
 
 extern "C" int afqmc_wset_create(int walker_type, int M, int nup, int ndn, int W,
@@ -1120,19 +1126,6 @@ extern "C" int afqmc_wfn_onerdm(afqmc_ham h, afqmc_wset ws, const afqmc_c128* G,
 // NOMSD with several determinants (NOMSD.cpp:93-333, 159-217; Real3IndexFactorization.hpp:389-427)
 // ---------------------------------------------------------------------------------------------
 namespace multidet {
-// out[w] = m + log sum_d exp(lo[d][w] - m), m = the largest real part (NOMSD.cpp:318-331)
-__global__ void logsumexp_kernel(const c128* __restrict__ lo, int ndet, int W,
-                                 c128* __restrict__ out) {
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= W) return;
-  c128 m = lo[w];
-  for (int d = 1; d < ndet; ++d)
-    if (lo[size_t(d) * W + w].x > m.x) m = lo[size_t(d) * W + w];
-  c128 sum = cmk(0, 0);
-  for (int d = 0; d < ndet; ++d) sum = cadd(sum, cexp(csub(lo[size_t(d) * W + w], m)));
-  out[w] = cadd(m, clog(sum));
-}
-
 // E[w] = sum_d conj(c_d) E_d e^{ov_d - m} / sum_d conj(c_d) e^{ov_d - m}, Ov = log(den) + m
 // (NOMSD.cpp:195-211)
 __global__ void multidet_energy_kernel(const c128* __restrict__ Ed, const c128* __restrict__ ov,
@@ -1153,41 +1146,8 @@ __global__ void multidet_energy_kernel(const c128* __restrict__ Ed, const c128* 
   Ov[w] = cadd(clog(den), m);
 }
 
-// wd[w] = conj(c_d) exp(Ot[w] - log_m[w]) with log_m the walkers' OVLP property; Ov[w] += wd
-__global__ void multidet_weight_kernel(const c128* __restrict__ Ot, const c128* __restrict__ wbuf,
-                                       long ldw, long prop_ovlp, c128 cc, int W,
-                                       c128* __restrict__ wd, c128* __restrict__ Ov) {
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= W) return;
-  const c128 f = cmul(cc, cexp(csub(Ot[w], wbuf[long(w) * ldw + prop_ovlp])));
-  wd[w] = f;
-  Ov[w] = cadd(Ov[w], f);
-}
-
-// G[w][:] += wd[w] Gd[w][:]   (n elements per walker)
-__global__ void axpy_rows_kernel(const c128* __restrict__ Gd, const c128* __restrict__ wd,
-                                 long n, int W, c128* __restrict__ G) {
-  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= n * W) return;
-  const int w = int(t / n);
-  G[t] = cadd(G[t], cmul(wd[w], Gd[t]));
-}
-
-// G[w][:] /= Ov[w]; then (add_log_shift_kernel) Ov[w] += log_m[w]: the reference adds the log of
-// the shift to the linear sum (NOMSD.cpp:274-276)
-__global__ void multidet_finish_kernel(c128* __restrict__ G, long n, int W,
-                                       const c128* __restrict__ Ov) {
-  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t < n * W) {
-    const int w = int(t / n);
-    G[t] = cdiv(G[t], Ov[w]);
-  }
-}
-__global__ void add_log_shift_kernel(c128* __restrict__ Ov, const c128* __restrict__ wbuf,
-                                     long ldw, long prop_ovlp, int W) {
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w < W) Ov[w] = cadd(Ov[w], wbuf[long(w) * ldw + prop_ovlp]);
-}
+// Workspace bound of one walker chunk of the batched several-determinant step
+constexpr size_t NOMSD_CHUNK_BYTES = size_t(1) << 30;
 
 int nomsd_bufs(afqmc_nomsd md, int W) {
   if (md->capW >= W) return AFQMC_OK;
@@ -1197,71 +1157,163 @@ int nomsd_bufs(afqmc_nomsd md, int W) {
   const long M = h->M, ldG = long(h->nel_tot) * M;
   const int nmax = std::max(h->nel[0], h->nel[1]);
   const size_t nd = md->hams.size();
-  AFQMC_TRY(dalloc(&md->Gd, size_t(W) * h->nspin * M * M));
   AFQMC_TRY(dalloc(&md->Gc, size_t(W) * (ldG > 0 ? ldG : 1)));
   AFQMC_TRY(dalloc(&md->ov, nd * W));
-  AFQMC_TRY(dalloc(&md->wd, size_t(W)));
   AFQMC_TRY(dalloc(&md->T, size_t(W) * (nmax > 0 ? nmax * nmax : 1)));
   AFQMC_TRY(dalloc(&md->Ed, nd * W * 3));
+  // batched step: chunk of walkers
+  const size_t nsq = size_t(h->nel[0]) * h->nel[0] + size_t(h->nel[1]) * h->nel[1];
+  const size_t per_walker = nd * (size_t(ldG) + nsq + 2) * sizeof(c128);
+  size_t wc = std::min<size_t>(size_t(W), 65535 / nd);
+  wc = std::min(wc, std::max<size_t>(1, NOMSD_CHUNK_BYTES / per_walker));
+  AFQMC_TRY(dalloc(&md->Tb, wc * nd * (nsq > 0 ? nsq : 1)));
+  AFQMC_TRY(dalloc(&md->Gcb, wc * nd * size_t(ldG > 0 ? ldG : 1)));
+  AFQMC_TRY(dalloc(&md->ovd, wc * nd));
+  AFQMC_TRY(dalloc(&md->wdd, wc * nd));
+  md->wchunk = int(wc);
   md->capW = W;
+  return AFQMC_OK;
+}
+
+// out[w] = m + log sum_d exp(ovd[w][d] + lc[d] - m), m = the largest real part of the
+// ovd[w][d] + lc[d] (NOMSD.cpp:303-331: per-determinant log overlap + log conj(ci))
+__global__ void logsumexp_wd_kernel(const c128* __restrict__ ovd, const c128* __restrict__ lc,
+                                    int ndet, int W, c128* __restrict__ out) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  const c128* o = ovd + size_t(w) * ndet;
+  c128 m = cadd(o[0], lc[0]);
+  for (int d = 1; d < ndet; ++d) {
+    const c128 x = cadd(o[d], lc[d]);
+    if (x.x > m.x) m = x;
+  }
+  c128 sum = cmk(0, 0);
+  for (int d = 0; d < ndet; ++d) sum = cadd(sum, cexp(csub(cadd(o[d], lc[d]), m)));
+  out[w] = cadd(m, clog(sum));
+}
+
+// f_d = conj(c_d) exp(ovd[w][d] - ovlp_w) with ovlp_w the walker's stored log overlap;
+// wdd[w][d] = f_d / sum_d f_d, Ov[w] = sum_d f_d + ovlp_w (NOMSD.cpp:220-279: the reference
+// divides the summed G by the linear sum and then adds the log of the shift to it)
+__global__ void multidet_weights_kernel(const c128* __restrict__ ovd, const c128* __restrict__ cc,
+                                        int ndet, int W, const c128* __restrict__ wbuf, long ldw,
+                                        long prop_ovlp, c128* __restrict__ wdd,
+                                        c128* __restrict__ Ov) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  const c128 shift = wbuf[long(w) * ldw + prop_ovlp];
+  const c128* o = ovd + size_t(w) * ndet;
+  c128* f = wdd + size_t(w) * ndet;
+  c128 sum = cmk(0, 0);
+  for (int d = 0; d < ndet; ++d) {
+    f[d] = cmul(cc[d], cexp(csub(o[d], shift)));
+    sum = cadd(sum, f[d]);
+  }
+  const c128 inv = cdiv(cmk(1, 0), sum);
+  for (int d = 0; d < ndet; ++d) f[d] = cmul(f[d], inv);
+  Ov[w] = cadd(sum, shift);
+}
+
+// T[b][:] *= wdd[b] for blocks of n elements
+__global__ void scale_blocks_kernel(c128* __restrict__ T, long n, long nb,
+                                    const c128* __restrict__ wdd) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t < n * nb) T[t] = cmul(T[t], wdd[t / n]);
+}
+
+// Overlap matrices T[w][d] = PsiT_d S_w of every determinant for walkers w0 .. w0+wc-1 (one
+// GEMM per spin), their log determinants summed over spins into ovd[w][d] (CLOSED x2) and,
+// with invert, T[w][d] <- T[w][d]^{-1} (one Gauss-Jordan launch per spin)
+int nomsd_overlaps(afqmc_nomsd md, afqmc_wset_s* ws, cudaStream_t s, int w0, int wc,
+                   bool invert) {
+  afqmc_ham_s* h0 = md->hams[0];
+  const int nd = int(md->hams.size());
+  const long M = h0->M, nb = long(wc) * nd;
+  const c128* S0 = ws->buf + long(w0) * ws->walker_size;
+  const c128 scale = (h0->walker_type == AFQMC_CLOSED) ? cmk(2, 0) : cmk(1, 0);
+  AFQMC_CUDA_TRY(cudaMemsetAsync(md->ovd, 0, sizeof(c128) * nb, s));
+  long toff = 0;
+  for (int sp = 0; sp < h0->nspin; ++sp) {
+    const int Ns = h0->nel[sp];
+    if (Ns == 0) continue;
+    const long nsq = long(Ns) * Ns;
+    c128* Tsp = md->Tb + toff;
+    toff += long(md->wchunk) * nd * nsq;
+    GemmParams p{};
+    p.m = nd * Ns; p.n = Ns; p.k = int(M);
+    p.A = md->PsiTall + long(nd) * h0->el_off[sp] * M; p.lda = M; p.strideA = 0;
+    p.B = S0 + ws->offS(sp); p.ldb = Ns; p.strideB = ws->walker_size;
+    p.C = Tsp; p.ldc = Ns; p.strideC = long(nd) * nsq;
+    p.alpha = cmk(1, 0); p.beta = cmk(0, 0);
+    AFQMC_TRY(zgemm(s, wc, GN, false, GN, false, p));
+    AFQMC_TRY(batched_logdet_inverse(s, Tsp, nsq, invert ? Tsp : nullptr, nsq, md->ovd, int(nb),
+                                     Ns, invert, scale, cmk(0, 0)));
+  }
   return AFQMC_OK;
 }
 
 int nomsd_log_overlap(afqmc_nomsd md, afqmc_wset_s* ws, cudaStream_t s, c128* ovlp) {
   const int W = ws->W, nd = int(md->hams.size());
   AFQMC_TRY(nomsd_bufs(md, W));
-  for (int d = 0; d < nd; ++d) {
-    // log overlap of determinant d (CLOSED x2) + log(conj ci), NOMSD.cpp:303-316
-    AFQMC_TRY(wfn_log_overlap(md->hams[d], ws, s, md->ov + size_t(d) * W, md->T));
-    const c128 c = md->ci[d];
-    const c128 lc = cabs(c) < 1e-12 ? clog(cmk(1e-12, 0)) : clog(cconj(c));
-    api_kernels::add_scalar_kernel<<<ceil_div(W, 128), 128, 0, s>>>(md->ov + size_t(d) * W, W, lc);
-    AFQMC_TRY(launch_status("add_scalar_kernel"));
+  for (int w0 = 0; w0 < W; w0 += md->wchunk) {
+    const int wc = std::min(md->wchunk, W - w0);
+    AFQMC_TRY(nomsd_overlaps(md, ws, s, w0, wc, false));
+    logsumexp_wd_kernel<<<ceil_div(wc, 128), 128, 0, s>>>(md->ovd, md->dlc, nd, wc, ovlp + w0);
+    AFQMC_TRY(launch_status("logsumexp_wd_kernel"));
   }
-  logsumexp_kernel<<<ceil_div(W, 128), 128, 0, s>>>(md->ov, nd, W, ovlp);
-  return launch_status("logsumexp_kernel");
+  return AFQMC_OK;
 }
 
-// full mixed density matrices of every determinant combined (NOMSD.cpp:220-279, compact=false)
+// full mixed density matrices of every determinant combined (NOMSD.cpp:220-279, compact=false):
+// G[w][s] = sum_d wdd[w][d] PsiT_d^T (T[w][d]^{-1})^T S_w^T, the weight folded into the inverse
+// before the compact product and the sum over determinants done by one GEMM with K = nd * N_s
 int nomsd_density_matrix(afqmc_nomsd md, afqmc_wset_s* ws, cudaStream_t s, c128* G, c128* Ov) {
   afqmc_ham_s* h0 = md->hams[0];
   const int W = ws->W, nd = int(md->hams.size()), nspin = h0->nspin;
-  const long M = h0->M, MM = M * M, per = long(nspin) * MM, ldG = long(h0->nel_tot) * M;
+  const long M = h0->M, MM = M * M, per = long(nspin) * MM;
   AFQMC_TRY(nomsd_bufs(md, W));
-  AFQMC_CUDA_TRY(cudaMemsetAsync(G, 0, sizeof(c128) * size_t(W) * per, s));
-  AFQMC_CUDA_TRY(cudaMemsetAsync(Ov, 0, sizeof(c128) * W, s));
-  for (int d = 0; d < nd; ++d) {
-    afqmc_ham_s* h = md->hams[d];
-    c128* Ot = md->ov + size_t(d) * W;
-    AFQMC_TRY(wfn_density_matrix(h, ws, s, md->Gc, ldG, Ot, md->T));
-    // Gd[w][s] = PsiT_s^T Gc[w][s]  (full G[i][k] = sum_a PsiT[a][i] Gc[a][k])
+  for (int w0 = 0; w0 < W; w0 += md->wchunk) {
+    const int wc = std::min(md->wchunk, W - w0);
+    const long nb = long(wc) * nd;
+    const c128* S0 = ws->buf + long(w0) * ws->walker_size;
+    c128* Gw = G + long(w0) * per;
+    AFQMC_TRY(nomsd_overlaps(md, ws, s, w0, wc, true));
+    multidet_weights_kernel<<<ceil_div(wc, 128), 128, 0, s>>>(
+        md->ovd, md->dcc, nd, wc, S0, ws->walker_size, ws->prop0 + AFQMC_OVLP, md->wdd, Ov + w0);
+    AFQMC_TRY(launch_status("multidet_weights_kernel"));
+    long toff = 0;
     for (int sp = 0; sp < nspin; ++sp) {
-      const int Ns = h->nel[sp];
+      const int Ns = h0->nel[sp];
       if (Ns == 0) {
-        AFQMC_CUDA_TRY(cudaMemset2DAsync(md->Gd + sp * MM, per * sizeof(c128), 0,
-                                         MM * sizeof(c128), W, s));
+        AFQMC_CUDA_TRY(cudaMemset2DAsync(Gw + sp * MM, per * sizeof(c128), 0, MM * sizeof(c128),
+                                         wc, s));
         continue;
       }
+      const long nsq = long(Ns) * Ns;
+      c128* Tsp = md->Tb + toff;
+      toff += long(md->wchunk) * nd * nsq;
+      c128* Gcsp = md->Gcb + long(md->wchunk) * nd * h0->el_off[sp] * M;
+      scale_blocks_kernel<<<ceil_div(nsq * nb, 256), 256, 0, s>>>(Tsp, nsq, nb, md->wdd);
+      AFQMC_TRY(launch_status("scale_blocks_kernel"));
+      // Gc[w][d] = (wdd T^{-1})^T S_w^T  [N_s x M]  (the determinant's compact G, weighted)
       GemmParams p{};
-      p.m = int(M); p.n = int(M); p.k = Ns;
-      p.A = h->PsiT + long(h->el_off[sp]) * M; p.lda = M; p.strideA = 0;
-      p.B = md->Gc + long(h->el_off[sp]) * M; p.ldb = M; p.strideB = ldG;
-      p.C = md->Gd + sp * MM; p.ldc = M; p.strideC = per;
+      p.m = Ns; p.n = int(M); p.k = Ns;
+      p.A = Tsp; p.lda = Ns; p.strideA = nsq;
+      p.B = S0 + ws->offS(sp); p.ldb = Ns; p.strideB = ws->walker_size; p.bdiv = nd;
+      p.C = Gcsp; p.ldc = M; p.strideC = long(Ns) * M;
       p.alpha = cmk(1, 0); p.beta = cmk(0, 0);
-      AFQMC_TRY(zgemm(s, W, GT, false, GN, false, p));
+      AFQMC_TRY(zgemm(s, int(nb), GT, false, GT, false, p));
+      // G[w][s] = PsiTall_s^T Gc[w]  (K = nd * N_s: the sum over determinants)
+      GemmParams q{};
+      q.m = int(M); q.n = int(M); q.k = nd * Ns;
+      q.A = md->PsiTall + long(nd) * h0->el_off[sp] * M; q.lda = M; q.strideA = 0;
+      q.B = Gcsp; q.ldb = M; q.strideB = long(nd) * Ns * M;
+      q.C = Gw + sp * MM; q.ldc = M; q.strideC = per;
+      q.alpha = cmk(1, 0); q.beta = cmk(0, 0);
+      AFQMC_TRY(zgemm(s, wc, GT, false, GN, false, q));
     }
-    multidet_weight_kernel<<<ceil_div(W, 128), 128, 0, s>>>(Ot, ws->buf, ws->walker_size,
-                                                            ws->prop0 + AFQMC_OVLP,
-                                                            cconj(md->ci[d]), W, md->wd, Ov);
-    AFQMC_TRY(launch_status("multidet_weight_kernel"));
-    axpy_rows_kernel<<<ceil_div(per * W, 256), 256, 0, s>>>(md->Gd, md->wd, per, W, G);
-    AFQMC_TRY(launch_status("axpy_rows_kernel"));
   }
-  multidet_finish_kernel<<<ceil_div(per * W, 256), 256, 0, s>>>(G, per, W, Ov);
-  AFQMC_TRY(launch_status("multidet_finish_kernel"));
-  add_log_shift_kernel<<<ceil_div(W, 128), 128, 0, s>>>(Ov, ws->buf, ws->walker_size,
-                                                        ws->prop0 + AFQMC_OVLP, W);
-  return launch_status("add_log_shift_kernel");
+  return AFQMC_OK;
 }
 
 // vbias from the full G (the ndet > 1 branch, Real3IndexFactorization.hpp:389-427):
@@ -1286,7 +1338,8 @@ using namespace multidet;
 
 extern "C" int afqmc_nomsd_create(int ndet, const afqmc_ham* hams, const afqmc_c128* ci,
                                   afqmc_nomsd* out) {
-  AFQMC_CHECK_ARG(out && hams && ci && ndet >= 1, "afqmc_nomsd_create: bad argument");
+  AFQMC_CHECK_ARG(out && hams && ci && ndet >= 1 && ndet <= 65535,
+                  "afqmc_nomsd_create: bad argument");
   *out = nullptr;
   afqmc_ham_s* h0 = hams[0];
   AFQMC_CHECK_ARG(h0, "afqmc_nomsd_create: null Hamiltonian 0");
@@ -1305,6 +1358,27 @@ extern "C" int afqmc_nomsd_create(int ndet, const afqmc_ham* hams, const afqmc_c
   md->device = h0->device;
   md->hams.assign(hams, hams + ndet);
   md->ci.assign(reinterpret_cast<const c128*>(ci), reinterpret_cast<const c128*>(ci) + ndet);
+  DeviceGuard g(md->device);
+  // every determinant's PsiT stacked per spin, conj(ci) and log conj(ci) (a coefficient below
+  // 1e-12 in modulus enters the log overlap as 1e-12, NOMSD.cpp:303-316)
+  const long M = h0->M;
+  AFQMC_TRY(dalloc(&md->PsiTall, size_t(ndet) * (h0->nel_tot > 0 ? h0->nel_tot : 1) * M));
+  for (int sp = 0; sp < h0->nspin; ++sp) {
+    const long rows = long(h0->nel[sp]) * M;
+    for (int d = 0; d < ndet && rows > 0; ++d)
+      AFQMC_CUDA_TRY(cudaMemcpy(md->PsiTall + long(ndet) * h0->el_off[sp] * M + d * rows,
+                                hams[d]->PsiT + long(h0->el_off[sp]) * M, sizeof(c128) * rows,
+                                cudaMemcpyDeviceToDevice));
+  }
+  std::vector<c128> cc(ndet), lc(ndet);
+  for (int d = 0; d < ndet; ++d) {
+    cc[d] = cconj(md->ci[d]);
+    lc[d] = cabs(md->ci[d]) < 1e-12 ? clog(cmk(1e-12, 0)) : clog(cc[d]);
+  }
+  AFQMC_TRY(dalloc(&md->dcc, size_t(ndet)));
+  AFQMC_TRY(dalloc(&md->dlc, size_t(ndet)));
+  AFQMC_CUDA_TRY(cudaMemcpy(md->dcc, cc.data(), sizeof(c128) * ndet, cudaMemcpyHostToDevice));
+  AFQMC_CUDA_TRY(cudaMemcpy(md->dlc, lc.data(), sizeof(c128) * ndet, cudaMemcpyHostToDevice));
   *out = md.release();
   return AFQMC_OK;
 }
@@ -1338,13 +1412,8 @@ extern "C" int afqmc_nomsd_energy(afqmc_nomsd md, afqmc_wset ws, afqmc_c128* E, 
     AFQMC_TRY(ham_energy(h, s, md->Gc, ldG, md->Ed + size_t(d) * W * 3, W, true, true, true,
                          precision));
   }
-  std::vector<c128> cc(nd);
-  for (int d = 0; d < nd; ++d) cc[d] = cconj(md->ci[d]);
-  Scratch cd;
-  AFQMC_TRY(cd.get(sizeof(c128) * nd, s));
-  AFQMC_CUDA_TRY(cudaMemcpyAsync(cd.p, cc.data(), sizeof(c128) * nd, cudaMemcpyHostToDevice, s));
-  multidet_energy_kernel<<<ceil_div(W, 128), 128, 0, s>>>(md->Ed, md->ov, (const c128*)cd.p, nd,
-                                                          W, (c128*)E, (c128*)ovlp);
+  multidet_energy_kernel<<<ceil_div(W, 128), 128, 0, s>>>(md->Ed, md->ov, md->dcc, nd, W,
+                                                          (c128*)E, (c128*)ovlp);
   AFQMC_TRY(launch_status("multidet_energy_kernel"));
   return cudaStreamSynchronize(s) == cudaSuccess ? AFQMC_OK : AFQMC_ERR_CUDA;
 }

@@ -103,3 +103,44 @@ def test_multidet_propagation_vs_oracle(cuda, wt, nup, ndn):
     d = to_host(wset.properties())[:, O.OVLP] - ows.props[:, O.OVLP]
     assert np.max(np.abs(_wrap(d))) < 1e-9
     prop.set_trial(None)
+
+
+@pytest.mark.parametrize("wt,nup,ndn", [(1, 2, 2), (2, 2, 2)])
+def test_multidet_batched_walker_chunks(cuda, wt, nup, ndn):
+    """300 determinants: the batched step goes over the walkers in chunks of 65535 // 300 = 218
+    (the batched GEMM's grid limit), so 230 walkers take a full and a ragged chunk."""
+    from safire_b200 import afqmc as A
+    M, Nc, W, nd = 8, 6, 230, 300
+    h1, Likn = make_hamiltonian(M, Nc, 0.9, seed=5)
+    _, C = np.linalg.eigh(h1)
+    rs = np.random.default_rng(11)
+    PsiTs = []
+    for _ in range(nd):
+        P = [np.ascontiguousarray(C[:, np.sort(rs.choice(M, nup, replace=False))].T).astype(complex)]
+        if wt == A.COLLINEAR:
+            P.append(np.ascontiguousarray(
+                C[:, np.sort(rs.choice(M, ndn, replace=False))].T).astype(complex))
+        PsiTs.append(P)
+    ci = rs.standard_normal(nd) + 1j * rs.standard_normal(nd)
+    hij = h1[None].astype(complex)
+    hams = [A.HamiltonianOperations(wt, M, nup, ndn, Likn[None], hij, 0.1, P) for P in PsiTs]
+    ohams = [O.Real3IndexFactorization(wt, M, nup, ndn, Likn[None], hij, 0.1, P)
+             for P in PsiTs[:1]] * nd
+    md = A.NOMSDMulti(hams, ci)
+    omd = O.NOMSDMulti(ohams, PsiTs, ci)
+    SA = rs.standard_normal((W, M, nup)) + 1j * rs.standard_normal((W, M, nup))
+    SB = rs.standard_normal((W, M, ndn)) + 1j * rs.standard_normal((W, M, ndn)) \
+        if wt == A.COLLINEAR else None
+    wset = A.WalkerSet(wt, M, nup, ndn, W)
+    wset.init_from_trial(hams[0])
+    wset.SlaterMatrices(0).copy_(to_dev(SA))
+    if SB is not None:
+        wset.SlaterMatrices(1).copy_(to_dev(SB))
+    lo_o = omd.Log_Overlap(SA, SB)
+    lo = md.Log_Overlap(wset)
+    assert np.max(np.abs(_wrap(to_host(lo) - lo_o))) < 1e-10
+    wset.setProperty(A.capi.OVLP, lo_o)
+    G, ovG = md.MixedDensityMatrix(wset)
+    Go, ovGo = omd.MixedDensityMatrix(SA, SB, lo_o)
+    assert rel_err(to_host(G), Go) < 1e-10
+    assert rel_err(to_host(ovG), ovGo) < 1e-10
