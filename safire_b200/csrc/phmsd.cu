@@ -515,108 +515,83 @@ __global__ void __launch_bounds__(PH_THREADS) excited_1body_all_kernel(
 
 // The 2-body energy terms of one excited determinant at one Cholesky index n, from per-walker
 // tables instead of its R rows.  With t_j = T[j][n][:] (rows of the half-rotated Twina), the
-// determinant's holes h, particles p, reference orbitals r = refc[h], Q = INV (the inverse of
-// QQ0[p][h]) and the compact R_b[x] = sum_q Q[b][q] (delta(x, p_q) - sum_i delta(x, occ_i)
-// QQ0[p_q][i]):
-//   F[a][b] = t_{h_a} . R_b = sum_q Q[b][q] (t_{h_a}[p_q] - Y[h_a][p_q]
-//                                           - sum_e (t_{h_a}[p_e] - t_{h_a}[r_e]) QQ0[p_q][h_e])
-//   D[a]    = U[h_a] . R_a   (the same with U and Z in place of t and Y)
-// where U[h][x] = sum_j t_h[r_j] t_j[x], Y[h][x] = sum_i t_h[r_i] QQ0[x][i], Z = (t[:, r]) Y.
-// ex and kn are then the terms of ph_excited_2body_energy_dense_cholesky
-// (detail/phmsd_impl.hpp:33-153) summed in closed form: every sum over electrons reduces to the
-// tables U and f0 = sum_i t_i[r_i] plus corrections over the nex holes.
-// Table layout: Tn [nel][nact]; Yv [nel][nv] and Qv [nel][nv] (QQ0 transposed) on the virtual
-// columns c; Uh [nh][nact] and Zh [nh][nv] on the hole rows k.  e4 = the determinant's holes,
-// particles, hole rows k and particle columns c.
-template <int NEX, typename C>
+// reference orbitals r_i, the virtual orbitals v_c, the determinant's holes h_a (electrons),
+// their hole rows k_a and particle columns c_a (its particles p_a = v_{c_a}), Q = INV (the
+// inverse of the excitation block M[q][x] = QQ0[p_q][h_x]), and the compact
+// R_b[x] = sum_q Q[b][q] (delta(x, p_q) - sum_i delta(x, occ_i) QQ0[p_q][i]), the terms of
+// ph_excited_2body_energy_dense_cholesky (detail/phmsd_impl.hpp:33-153) summed in closed form
+// over the electrons are
+//   F[a][b] = t_{h_a} . R_b,  D[a] = U[h_a] . R_a  with U[h][x] = sum_j t_h[r_j] t_j[x],
+//   kn = f0 + sum_a (F[a][a] + t_{h_a}[p_a] - t_{h_a}[r_a]),  f0 = sum_i t_i[r_i],
+//   ex = sum_{a,b} F[a][b] F[b][a] + sum_{a,x} (t_{h_a}[p_x] t_{h_x}[p_a] - t_{h_a}[r_x] t_{h_x}[r_a])
+//        + 2 sum_a (D[a] + sum_x (t_{h_a}[p_x] - t_{h_a}[r_x]) F[x][a]
+//                   + U[h_a][p_a] - U[h_a][r_a] - sum_x t_{h_a}[r_x] (t_{h_x}[p_a] - t_{h_x}[r_a])).
+// Because Q M = 1, F = P - (t_{h_a}[p_b] - t_{h_a}[r_b]) with P[a][b] = sum_q Sf[h_a][c_q] Q[b][q],
+// and every term at the holes' reference columns cancels, which leaves
+//   kn = f0 + tr P,   ex = tr(P P) + 2 sum_{a,q} Q[a][q] SU[k_a][c_q],
+//   Sf[j][c] = t_j[v_c] - sum_i t_j[r_i] QQ0[v_c][i],   SU[k][c] = sum_j t_{h_k}[r_j] Sf[j][c].
+// Table layout: Sf [nel][nv] (all electrons' rows), SU [nh][nv] (hole rows), one pair per
+// Cholesky index g of the block's group (strides sfs, sus).  e4 = the determinant's holes,
+// particles, hole rows k and particle columns c.  The determinant's Q and indices are read once
+// for the ng indices of the group: exg[g], kng[g].
+template <int NEX, int NG, typename C>
 __device__ __forceinline__ void excited_terms(const int* __restrict__ e4,
-                                              const c128* __restrict__ Qg, const C* Tn,
-                                              const C* Yv, const C* Uh, const C* Zh, const C* Qv,
-                                              const int* refs, int nact, int nv, C f0, C& ex_out,
-                                              C& kn_out) {
-  using R = decltype(f0.x);
+                                              const c128* __restrict__ Qg, const C* Sf,
+                                              const C* SU, int nv, int sfs, int sus, int ng,
+                                              const C* f0, C* exg, C* kng) {
+  using R = decltype(f0[0].x);
   C Qi[NEX * NEX];  // the determinant's Woodbury inverse, in the working precision
 #pragma unroll
   for (int k = 0; k < NEX * NEX; ++k) Qi[k] = to_cx<C>(Qg[k]);
-  int h[NEX], p[NEX], r[NEX], hr[NEX], pc[NEX];
+  int so[NEX], uo[NEX], pc[NEX];
 #pragma unroll
   for (int a = 0; a < NEX; ++a) {
-    h[a] = e4[a];
-    p[a] = e4[NEX + a];
-    hr[a] = e4[2 * NEX + a];
+    so[a] = e4[a] * nv;
+    uo[a] = e4[2 * NEX + a] * nv;
     pc[a] = e4[3 * NEX + a];
-    r[a] = refs[h[a]];
   }
-  C F[NEX][NEX], D[NEX];
 #pragma unroll
-  for (int a = 0; a < NEX; ++a) {
-    const C* ta = Tn + h[a] * nact;
-    const C* ua = Uh + hr[a] * nact;
-    C dt[NEX], du[NEX];
+  for (int g = 0; g < NG; ++g) {
+    if (g >= ng) break;
+    const C* Sg = Sf + g * sfs;
+    const C* Ug = SU + g * sus;
+    C P[NEX][NEX];
+    C d = czero<C>();
 #pragma unroll
-    for (int x = 0; x < NEX; ++x) {
-      dt[x] = csub(ta[p[x]], ta[r[x]]);
-      du[x] = csub(ua[p[x]], ua[r[x]]);
-    }
-    C g[NEX], gu[NEX];
+    for (int a = 0; a < NEX; ++a) {
+      C sv[NEX];
 #pragma unroll
-    for (int q = 0; q < NEX; ++q) {
-      C ct = czero<C>(), cu = czero<C>();
-#pragma unroll
-      for (int x = 0; x < NEX; ++x) {
-        const C qv = Qv[h[x] * nv + pc[q]];  // QQ0[p_q][h_x]
-        ct = cadd(ct, cmul(dt[x], qv));
-        cu = cadd(cu, cmul(du[x], qv));
+      for (int q = 0; q < NEX; ++q) {
+        sv[q] = Sg[so[a] + pc[q]];
+        d = cadd(d, cmul(Qi[a * NEX + q], Ug[uo[a] + pc[q]]));
       }
-      g[q] = csub(csub(ta[p[q]], Yv[h[a] * nv + pc[q]]), ct);
-      gu[q] = csub(csub(ua[p[q]], Zh[hr[a] * nv + pc[q]]), cu);
+#pragma unroll
+      for (int b = 0; b < NEX; ++b) {
+        C acc = czero<C>();
+#pragma unroll
+        for (int q = 0; q < NEX; ++q) acc = cadd(acc, cmul(sv[q], Qi[b * NEX + q]));
+        P[a][b] = acc;
+      }
     }
+    C tr = czero<C>(), pp = czero<C>(), off = czero<C>();
 #pragma unroll
-    for (int b = 0; b < NEX; ++b) {
-      C f = czero<C>();
+    for (int a = 0; a < NEX; ++a) {
+      tr = cadd(tr, P[a][a]);
+      pp = cadd(pp, cmul(P[a][a], P[a][a]));
 #pragma unroll
-      for (int q = 0; q < NEX; ++q) f = cadd(f, cmul(Qi[b * NEX + q], g[q]));
-      F[a][b] = f;
+      for (int b = a + 1; b < NEX; ++b) off = cadd(off, cmul(P[a][b], P[b][a]));
     }
-    C dd = czero<C>();
-#pragma unroll
-    for (int q = 0; q < NEX; ++q) dd = cadd(dd, cmul(Qi[a * NEX + q], gu[q]));
-    D[a] = dd;
+    exg[g] = cadd(cadd(pp, cscale(off, R(2))), cscale(d, R(2)));
+    kng[g] = cadd(f0[g], tr);
   }
-  C ex = czero<C>(), kn = f0;
-#pragma unroll
-  for (int a = 0; a < NEX; ++a) {
-    const C* ta = Tn + h[a] * nact;
-    const C* ua = Uh + hr[a] * nact;
-    const C tpa = ta[p[a]], tra = ta[r[a]];
-    kn = cadd(kn, cadd(F[a][a], csub(tpa, tra)));
-    // f_a^2 and the changed electron's own diagonal term
-    ex = cadd(ex, cmul(F[a][a], F[a][a]));
-    ex = cadd(ex, csub(cmul(tpa, tpa), cmul(tra, tra)));
-    // B_a = sum_j t_{h_a}[occ_j] F(j, a);  C_a = sum over unchanged j of the pair term (i = h_a)
-    C B = D[a];
-    C Cc = csub(ua[p[a]], ua[r[a]]);
-#pragma unroll
-    for (int x = 0; x < NEX; ++x) {
-      const C* tx = Tn + h[x] * nact;
-      B = cadd(B, cmul(csub(ta[p[x]], ta[r[x]]), F[x][a]));
-      Cc = csub(Cc, cmul(ta[r[x]], csub(tx[p[a]], tx[r[a]])));
-      if (x != a) ex = cadd(ex, csub(cmul(ta[p[x]], tx[p[a]]), cmul(ta[r[x]], tx[r[a]])));
-      if (x > a) ex = cadd(ex, cscale(cmul(F[x][a], F[a][x]), R(2)));
-    }
-    ex = cadd(ex, cscale(cadd(B, Cc), R(2)));
-  }
-  ex_out = ex;
-  kn_out = kn;
 }
 
 // nex > 4 is rare: out of line, so that its larger frame stays out of the common path
-template <int NEX, typename C>
-__device__ __noinline__ void excited_terms_rare(const int* e4, const c128* Qi, const C* Tn,
-                                                const C* Yv, const C* Uh, const C* Zh,
-                                                const C* Qv, const int* refs, int nact, int nv,
-                                                C f0, C& ex, C& kn) {
-  excited_terms<NEX, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0, ex, kn);
+template <int NEX, int NG, typename C>
+__device__ __noinline__ void excited_terms_rare(const int* e4, const c128* Qi, const C* Sf,
+                                                const C* SU, int nv, int sfs, int sus, int ng,
+                                                const C* f0, C* exg, C* kng) {
+  excited_terms<NEX, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0, exg, kng);
 }
 
 // One product of the tables: out[k][c] = sum_j a[k][sel_j] b[j][c] over the rows k of `rows`
@@ -665,20 +640,21 @@ __device__ __forceinline__ void table_products(const TableProduct<C> (&P)[NP], c
   }
 }
 
-// Excited-determinant 2-body energies of one spin for walker blockIdx.y at Cholesky index
-// blockIdx.x, all unique excitations in one launch (the work of ph_excited_energies_first_step /
-// second_step, phmsd_helpers.hpp:401-527, for every shell): the per-(walker, n) tables in shared
-// memory, then one thread per excited determinant.  EXacc[w] -= wgt ex / 2,
-// EJacc[w] += wgt (kn^2 - f0^2) / 2; KE[u][w][n] = kn, or with `cross` E[w].EJ += cross . kn.
-// The reference determinant's terms come from the same tables (ph_reference_energy,
-// Real3IndexFactorization.hpp:212-233, 598-696): Kref[w][n] = f0, REF[w] += (sum_ij t_i[r_j]
-// t_j[r_i], f0^2).
+// Excited-determinant 2-body energies of one spin for walker blockIdx.y at the NG Cholesky
+// indices n = NG blockIdx.x + g, all unique excitations in one launch (the work of
+// ph_excited_energies_first_step / second_step, phmsd_helpers.hpp:401-527, for every shell): the
+// per-(walker, n) tables Sf and SU in shared memory, built one index at a time, then one thread
+// per excited determinant over the group's indices (its Q, indices and weight read once).
+// EXacc[w] -= wgt ex / 2, EJacc[w] += wgt (kn^2 - f0^2) / 2; KE[u][w][n] = kn, or with `cross`
+// E[w].EJ += cross . kn.  The reference determinant's terms come from the same tables
+// (ph_reference_energy, Real3IndexFactorization.hpp:212-233, 598-696): Kref[w][n] = f0,
+// REF[w] += (sum_ij t_i[r_j] t_j[r_i], f0^2).
 // R = double: complex128 tables and per-determinant sums (the reference's arithmetic); R = float:
 // complex64 tables and per-determinant sums, for the mixed-precision energy (half the shared
 // memory, twice the FP32 rate); the sums over determinants, the reference determinant's terms
 // and every output stay FP64.
 constexpr int PHX_THREADS = 256;
-template <typename R>
+template <typename R, int NG>
 __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_energy_tables_kernel(
     const c128* __restrict__ Twina, const c128* __restrict__ QQ0, const int* __restrict__ refc,
     const int* __restrict__ hl, const int* __restrict__ vl, int nh, int nv,
@@ -690,57 +666,77 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
     c128* __restrict__ REF) {
   using C = typename CxOf<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* Tn = reinterpret_cast<C*>(smem_raw);            // [nel][nact]
-  C* Qv = Tn + nel * nact;                           // [nel][nv]
-  C* Yv = Qv + nel * nv;                             // [nel][nv]
-  C* Uh = Yv + nel * nv;                             // [nh][nact]
-  C* Zh = Uh + nh * nact;                            // [nh][nv]
-  int* refs = reinterpret_cast<int*>(Zh + nh * nv);  // [nel]
-  int* hls = refs + nel;                             // [nh]
+  C* Tn = reinterpret_cast<C*>(smem_raw);                 // [nel][nact], one index at a time
+  C* Qv = Tn + nel * nact;                                // [nel][nv]
+  C* Sf = Qv + nel * nv;                                  // [NG][nel][nv]
+  C* SU = Sf + NG * nel * nv;                             // [NG][nh][nv]
+  int* refs = reinterpret_cast<int*>(SU + NG * nh * nv);  // [nel]
+  int* hls = refs + nel;                                  // [nh]
+  int* vls = hls + nh;                                    // [nv]
   __shared__ double red[PHX_THREADS / 32 * 6];
-  const int n = blockIdx.x, w = blockIdx.y;
+  const int n0 = blockIdx.x * NG, w = blockIdx.y;
+  const int ng = min(NG, nchol - n0);
+  const int sfs = nel * nv, sus = nh * nv;
   const c128* Tw = Twina + size_t(w) * nel * nchol * nact;
   const c128* Qw = QQ0 + size_t(w) * nact * nel;
-  for (int k = threadIdx.x; k < nel * nact; k += blockDim.x) {
-    const int j = k / nact, x = k - j * nact;
-    Tn[k] = to_cx<C>(Tw[(size_t(j) * nchol + n) * nact + x]);
-  }
   for (int k = threadIdx.x; k < nel * nv; k += blockDim.x) {
     const int i = k / nv, c = k - i * nv;
     Qv[k] = to_cx<C>(Qw[size_t(vl[c]) * nel + i]);
   }
   for (int i = threadIdx.x; i < nel; i += blockDim.x) refs[i] = refc[i];
   for (int k = threadIdx.x; k < nh; k += blockDim.x) hls[k] = hl[k];
-  __syncthreads();
-  // Y = t[:, r] Qv,  U = t[hole rows, r] t
-  {
-    const TableProduct<C> P[2] = {{Tn, nact, nullptr, nel, Qv, nv, nv, Yv, nv},
-                                  {Tn, nact, hls, nh, Tn, nact, nact, Uh, nact}};
-    table_products<2, C>(P, refs, nel);
-  }
-  // the reference determinant: f0 = sum_i t_i[r_i], ex0 = sum_ij t_i[r_j] t_j[r_i]
-  c128 ex0 = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0);
-  for (int k = threadIdx.x; k < nel * nel; k += blockDim.x) {
-    const int i = k / nel, j = k - i * nel;
-    ex0 = cadd(ex0, cmul(to_cx<c128>(Tn[i * nact + refs[j]]), to_cx<c128>(Tn[j * nact + refs[i]])));
-  }
-  __syncthreads();
-  // Z = t[hole rows, r] Y
-  {
-    const TableProduct<C> P[1] = {{Tn, nact, hls, nh, Yv, nv, nv, Zh, nv}};
-    table_products<1, C>(P, refs, nel);
-  }
-  c128 f0 = cmk(0, 0);
-  for (int i = 0; i < nel; ++i) f0 = cadd(f0, to_cx<c128>(Tn[i * nact + refs[i]]));
-  const C f0w = to_cx<C>(f0);
-  const c128 f00 = cmul(f0, f0);
-  block_sum3(ex0, z1, z2, red);  // ends with a barrier: Zh is complete after it
-  if (threadIdx.x == 0 && Kref) {
-    Kref[size_t(w) * nchol + n] = f0;
-    atomicAdd(&REF[2 * w].x, ex0.x);
-    atomicAdd(&REF[2 * w].y, ex0.y);
-    atomicAdd(&REF[2 * w + 1].x, f00.x);
-    atomicAdd(&REF[2 * w + 1].y, f00.y);
+  for (int c = threadIdx.x; c < nv; c += blockDim.x) vls[c] = vl[c];
+  C f0w[NG];
+  c128 f00[NG];
+#pragma unroll
+  for (int g = 0; g < NG; ++g) {
+    f0w[g] = czero<C>();
+    f00[g] = cmk(0, 0);
+    if (g >= ng) break;
+    const int n = n0 + g;
+    C* Sg = Sf + g * sfs;
+    C* Ug = SU + g * sus;
+    for (int k = threadIdx.x; k < nel * nact; k += blockDim.x) {
+      const int j = k / nact, x = k - j * nact;
+      Tn[k] = to_cx<C>(Tw[(size_t(j) * nchol + n) * nact + x]);
+    }
+    __syncthreads();
+    // Y = t[:, r] Qv (into Sf)
+    {
+      const TableProduct<C> P[1] = {{Tn, nact, nullptr, nel, Qv, nv, nv, Sg, nv}};
+      table_products<1, C>(P, refs, nel);
+    }
+    // the reference determinant: f0 = sum_i t_i[r_i], ex0 = sum_ij t_i[r_j] t_j[r_i]
+    c128 ex0 = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0);
+    for (int k = threadIdx.x; k < nel * nel; k += blockDim.x) {
+      const int i = k / nel, j = k - i * nel;
+      ex0 = cadd(ex0,
+                 cmul(to_cx<c128>(Tn[i * nact + refs[j]]), to_cx<c128>(Tn[j * nact + refs[i]])));
+    }
+    __syncthreads();
+    // Sf = t[:, v] - Y
+    for (int k = threadIdx.x; k < nel * nv; k += blockDim.x) {
+      const int j = k / nv, c = k - j * nv;
+      Sg[k] = csub(Tn[j * nact + vls[c]], Sg[k]);
+    }
+    __syncthreads();
+    // SU = t[hole rows, r] Sf
+    {
+      const TableProduct<C> P[1] = {{Tn, nact, hls, nh, Sg, nv, nv, Ug, nv}};
+      table_products<1, C>(P, refs, nel);
+    }
+    c128 f0 = cmk(0, 0);
+    for (int i = 0; i < nel; ++i) f0 = cadd(f0, to_cx<c128>(Tn[i * nact + refs[i]]));
+    f0w[g] = to_cx<C>(f0);
+    f00[g] = cmul(f0, f0);
+    block_sum3(ex0, z1, z2, red);  // ends with a barrier: SU is complete, Tn free after it
+    if (threadIdx.x == 0 && Kref) {
+      Kref[size_t(w) * nchol + n] = f0;
+      atomicAdd(&REF[2 * w].x, ex0.x);
+      atomicAdd(&REF[2 * w].y, ex0.y);
+      atomicAdd(&REF[2 * w + 1].x, f00[g].x);
+      atomicAdd(&REF[2 * w + 1].y, f00[g].y);
+    }
   }
   __syncthreads();
   c128 exs = cmk(0, 0), ejs = cmk(0, 0), ejc = cmk(0, 0);
@@ -749,26 +745,33 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
     const int nex = unex[u];
     const int* e4 = uexc4 + uoff4[u];
     const c128* Qi = Iw + uinv[u];
-    C exw, knw;
+    C exw[NG], knw[NG];
     switch (nex) {
-      case 1: excited_terms<1, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
-      case 2: excited_terms<2, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
-      case 3: excited_terms<3, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
-      case 4: excited_terms<4, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
-      case 5: excited_terms_rare<5, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
-      case 6: excited_terms_rare<6, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
-      case 7: excited_terms_rare<7, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
-      default: excited_terms_rare<8, C>(e4, Qi, Tn, Yv, Uh, Zh, Qv, refs, nact, nv, f0w, exw, knw); break;
+      case 1: excited_terms<1, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      case 2: excited_terms<2, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      case 3: excited_terms<3, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      case 4: excited_terms<4, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      case 5: excited_terms_rare<5, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      case 6: excited_terms_rare<6, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      case 7: excited_terms_rare<7, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      default: excited_terms_rare<8, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
     }
-    const c128 ex = to_cx<c128>(exw), kn = to_cx<c128>(knw);
+    c128 exu = cmk(0, 0), eju = cmk(0, 0);
+    const size_t o = (size_t(u) * W + w) * nchol + n0;
+#pragma unroll
+    for (int g = 0; g < NG; ++g) {
+      if (g >= ng) break;
+      const c128 kn = to_cx<c128>(knw[g]);
+      exu = cadd(exu, to_cx<c128>(exw[g]));
+      eju = cadd(eju, csub(cmul(kn, kn), f00[g]));
+      if (cross)
+        ejc = cadd(ejc, cmul(cross[o + g], kn));
+      else
+        KE[o + g] = kn;
+    }
     const c128 wu = wgt[size_t(u) * W + w];
-    exs = cadd(exs, cmul(wu, ex));
-    ejs = cadd(ejs, cmul(wu, csub(cmul(kn, kn), f00)));
-    const size_t o = (size_t(u) * W + w) * nchol + n;
-    if (cross)
-      ejc = cadd(ejc, cmul(cross[o], kn));
-    else
-      KE[o] = kn;
+    exs = cadd(exs, cmul(wu, exu));
+    ejs = cadd(ejs, cmul(wu, eju));
   }
   block_sum3(exs, ejs, ejc, red);
   if (threadIdx.x == 0) {
@@ -1681,9 +1684,10 @@ int phmsd_half_rotated(afqmc_phmsd h, cudaStream_t s, int sp, int nb) {
 // the excited determinants of spin sp, shell by shell: 1-body into el[0], 2-body into el[1..2],
 // KE of each determinant written to KEout + k0 * nb * Nc (cross = nullptr) or to KEl and
 // contracted with cross at once (the second step)
-size_t excited_tables_smem(afqmc_phmsd h, int sp, size_t elem = sizeof(c128)) {
+size_t excited_tables_smem(afqmc_phmsd h, int sp, size_t elem = sizeof(c128), int ng = 1) {
   const size_t N = h->nel[sp], na = h->nact[sp], nv = h->nv[sp], nh = h->nh[sp];
-  return (N * na + 2 * N * nv + nh * na + nh * nv) * elem + (N + nh) * sizeof(int);
+  return (N * na + N * nv + size_t(ng) * (N * nv + nh * nv)) * elem +
+         (N + nh + nv) * sizeof(int);
 }
 
 // The reference determinant's and the excited determinants' energies of spin sp
@@ -1746,10 +1750,20 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
       AFQMC_TRY(launch_status("excited_1body_all_kernel"));
     }
     c128* REF = h->el + 3 * nb;  // [nb][2]: sum_n ex0, sum_n f0^2
-    auto kern = mixed ? excited_energy_tables_kernel<float> : excited_energy_tables_kernel<double>;
+    // four Cholesky indices per CTA where their tables fit (each determinant's Q, indices and
+    // weight are then read once per four indices), else one
+    const size_t esz = mixed ? sizeof(c64) : sizeof(c128);
+    const size_t smem4 = excited_tables_smem(h, sp, esz, 4);
+    const bool g4 = smem4 <= (mixed ? 110 : 200) * 1024;
+    const int NGr = g4 ? 4 : 1;
+    const size_t smem = g4 ? smem4 : tsmem;
+    auto kern = mixed ? (g4 ? excited_energy_tables_kernel<float, 4>
+                            : excited_energy_tables_kernel<float, 1>)
+                      : (g4 ? excited_energy_tables_kernel<double, 4>
+                            : excited_energy_tables_kernel<double, 1>);
     AFQMC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        int(tsmem)));
-    kern<<<dim3(Nc, nb), PHX_THREADS, tsmem, s>>>(
+                                        int(smem)));
+    kern<<<dim3((Nc + NGr - 1) / NGr, nb), PHX_THREADS, smem, s>>>(
         h->Twina, h->eQ[sp], h->refc[sp], h->hl[sp], h->vl[sp], h->nh[sp], h->nv[sp],
         h->uoff4[sp], h->unex[sp], h->uexc4[sp], h->uinv[sp], h->INV, h->ninv[sp], h->wgt,
         h->nuniq[sp], nb, N, na, Nc, h->el + nb, h->el + 2 * nb, cross ? nullptr : KEout, cross,
