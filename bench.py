@@ -109,7 +109,7 @@ def run_profile_case(args):
         wl, trial = make_phmsd_workload(W=W)
         sim = Simulation.from_workload(wl, W=W, rp=rp, trial=trial, precision=prec)
         sim.prop.Propagate(sim.wset, sim.Eshift)
-        sim.wfn.Energy(sim.wset, set_properties=False)
+        sim.wfn.Energy(sim.wset, set_properties=False, precision=prec)
     else:
         W = args.walkers
         sim = Simulation.from_workload(make_workload("cfg2"), W=W, precision=prec, rp=rp)

@@ -57,6 +57,7 @@ struct TcParams {
   float* acc_split[4];  // optional split copy of the updated running sum (last Taylor term)
   c128* out_c;
   long outc_ld, outc_bs;
+  int outc_f32;         // EPI_C128: out_c holds complex64 (float2) elements instead
   int vhs_M;            // EPI_VHS: columns are (i, k) pairs of an M x M matrix
   // FP16 operands: the accumulator row r is multiplied by row_inv[r] (the A operand's row scale;
   // the B operand's scale is folded into alpha) before the epilogue uses it
@@ -430,7 +431,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_cgemm_kernel(const __grid_co
           if constexpr (EPI == EPI_C128 || EPI == EPI_S64) {
             const double dr = p.alpha.x * double(vr[j]) - p.alpha.y * double(vi[j]);
             const double di = p.alpha.x * double(vi[j]) + p.alpha.y * double(vr[j]);
-            p.out_c[long(z) * p.outc_bs + long(row) * p.outc_ld + col] = cmk(dr, di);
+            const long idx = long(z) * p.outc_bs + long(row) * p.outc_ld + col;
+            if (EPI == EPI_C128 && p.outc_f32)
+              reinterpret_cast<float2*>(p.out_c)[idx] = make_float2(float(dr), float(di));
+            else
+              p.out_c[idx] = cmk(dr, di);
           } else if constexpr (EPI == EPI_PLANES) {
             const long idx = long(z) * p.out_bs + long(row) * p.out_ld + col;
             split_store(xr, p.out[0], p.out[1], idx);
@@ -1787,7 +1792,7 @@ int tcgemm_rb_create(TcGemmRB** out, const c128* B, long rows_b, long K, long ld
 void tcgemm_rb_destroy(TcGemmRB* g) { delete g; }
 
 int tcgemm_rb_run(cudaStream_t s, TcGemmRB* g, const c128* A, long lda, int rows_a, c128* C,
-                  long ldc) {
+                  long ldc, bool c64_out) {
   if (rows_a <= 0) return AFQMC_OK;
   const long K = g->B.k;
   if (g->a_cap < rows_a) {
@@ -1816,6 +1821,7 @@ int tcgemm_rb_run(cudaStream_t s, TcGemmRB* g, const c128* A, long lda, int rows
   p.out_c = C;
   p.outc_ld = ldc;
   p.outc_bs = 0;
+  p.outc_f32 = c64_out ? 1 : 0;
   p.err = g->err;
   return launch_tc<true, false, 128, 2, EPI_C128, true>(s, p, 1);
 }

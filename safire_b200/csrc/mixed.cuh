@@ -60,7 +60,8 @@ int mixed_error_flag(MixedHam* m, unsigned* flag);
 struct TcGemmRB;
 int tcgemm_rb_create(TcGemmRB** out, const c128* B, long rows_b, long K, long ldb);
 void tcgemm_rb_destroy(TcGemmRB* g);
+// c64_out: C holds complex64 (float2) elements, ldc counted in them
 int tcgemm_rb_run(cudaStream_t s, TcGemmRB* g, const c128* A, long lda, int rows_a, c128* C,
-                  long ldc);
+                  long ldc, bool c64_out = false);
 
 }  // namespace afqmc

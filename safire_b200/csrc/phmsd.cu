@@ -452,7 +452,8 @@ __global__ void woodbury_inverses_kernel(const c128* __restrict__ QQ0, const int
                                          const int* __restrict__ unex,
                                          const int* __restrict__ uexc,
                                          const int* __restrict__ uinv, int nuniq, int W, int nact,
-                                         int nel, int ninv, c128* __restrict__ INV) {
+                                         int nel, int ninv, c128* __restrict__ INV,
+                                         float2* __restrict__ INV32) {
   const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= long(nuniq - 1) * W) return;
   const int w = int(t / (nuniq - 1)), u = 1 + int(t - long(w) * (nuniq - 1));
@@ -463,6 +464,13 @@ __global__ void woodbury_inverses_kernel(const c128* __restrict__ QQ0, const int
   c128* o = INV + size_t(w) * ninv + uinv[u];
   for (int p = 0; p < nex; ++p)
     for (int q = 0; q < nex; ++q) o[p * nex + q] = ok ? inv[p][q] : cmk(0.0, 0.0);
+  if (INV32) {
+    float2* o32 = INV32 + size_t(w) * ninv + uinv[u];
+    for (int p = 0; p < nex; ++p)
+      for (int q = 0; q < nex; ++q)
+        o32[p * nex + q] = ok ? make_float2(float(inv[p][q].x), float(inv[p][q].y))
+                              : make_float2(0.f, 0.f);
+  }
 }
 
 // The 1-body energies of every unique excitation u >= 1 for walker blockIdx.x, from the
@@ -536,13 +544,13 @@ __global__ void __launch_bounds__(PH_THREADS) excited_1body_all_kernel(
 // for the ng indices of the group: exg[g], kng[g].
 template <int NEX, int NG, typename C>
 __device__ __forceinline__ void excited_terms(const int* __restrict__ e4,
-                                              const c128* __restrict__ Qg, const C* Sf,
+                                              const C* __restrict__ Qg, const C* Sf,
                                               const C* SU, int nv, int sfs, int sus, int ng,
                                               const C* f0, C* exg, C* kng) {
   using R = decltype(f0[0].x);
   C Qi[NEX * NEX];  // the determinant's Woodbury inverse, in the working precision
 #pragma unroll
-  for (int k = 0; k < NEX * NEX; ++k) Qi[k] = to_cx<C>(Qg[k]);
+  for (int k = 0; k < NEX * NEX; ++k) Qi[k] = Qg[k];
   int so[NEX], uo[NEX], pc[NEX];
 #pragma unroll
   for (int a = 0; a < NEX; ++a) {
@@ -588,7 +596,7 @@ __device__ __forceinline__ void excited_terms(const int* __restrict__ e4,
 
 // nex > 4 is rare: out of line, so that its larger frame stays out of the common path
 template <int NEX, int NG, typename C>
-__device__ __noinline__ void excited_terms_rare(const int* e4, const c128* Qi, const C* Sf,
+__device__ __noinline__ void excited_terms_rare(const int* e4, const C* Qi, const C* Sf,
                                                 const C* SU, int nv, int sfs, int sus, int ng,
                                                 const C* f0, C* exg, C* kng) {
   excited_terms<NEX, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0, exg, kng);
@@ -654,20 +662,44 @@ __device__ __forceinline__ void table_products(const TableProduct<C> (&P)[NP], c
 // memory, twice the FP32 rate); the sums over determinants, the reference determinant's terms
 // and every output stay FP64.
 constexpr int PHX_THREADS = 256;
-template <typename R, int NG>
+
+// asynchronous global -> shared copies of 8 or 16 bytes (cp.async, completion per commit group)
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// TW: the element type of Twina (complex128, or complex64 from the mixed half rotation).  When
+// it is the working type C the rows t_j come in by asynchronous copies, the next index's while
+// the current one's tables are built (nbuf = 2), else by converting loads.  INVc holds the
+// Woodbury inverses in the working type; uhdr[u] = {nex, uoff4, uinv, 0}.
+template <typename R, int NG, typename TW>
 __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_energy_tables_kernel(
-    const c128* __restrict__ Twina, const c128* __restrict__ QQ0, const int* __restrict__ refc,
+    const TW* __restrict__ Twina, const c128* __restrict__ QQ0, const int* __restrict__ refc,
     const int* __restrict__ hl, const int* __restrict__ vl, int nh, int nv,
-    const int* __restrict__ uoff4, const int* __restrict__ unex, const int* __restrict__ uexc4,
-    const int* __restrict__ uinv, const c128* __restrict__ INV, int ninv,
-    const c128* __restrict__ wgt, int nuniq, int W, int nel, int nact, int nchol,
+    const int4* __restrict__ uhdr, const int* __restrict__ uexc4,
+    const typename CxOf<R>::T* __restrict__ INVc, int ninv,
+    const c128* __restrict__ wgt, int nuniq, int W, int nel, int nact, int nchol, int nbuf,
     c128* __restrict__ EXacc, c128* __restrict__ EJacc, c128* __restrict__ KE,
     const c128* __restrict__ cross, c128* __restrict__ E, c128* __restrict__ Kref,
     c128* __restrict__ REF) {
   using C = typename CxOf<R>::T;
+  constexpr bool ASYNC = sizeof(TW) == sizeof(C);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* Tn = reinterpret_cast<C*>(smem_raw);                 // [nel][nact], one index at a time
-  C* Qv = Tn + nel * nact;                                // [nel][nv]
+  C* Tb0 = reinterpret_cast<C*>(smem_raw);                // [nbuf][nel][nact]
+  C* Tb1 = Tb0 + (nbuf - 1) * nel * nact;
+  C* Qv = Tb0 + nbuf * nel * nact;                        // [nel][nv]
   C* Sf = Qv + nel * nv;                                  // [NG][nel][nv]
   C* SU = Sf + NG * nel * nv;                             // [NG][nh][nv]
   int* refs = reinterpret_cast<int*>(SU + NG * nh * nv);  // [nel]
@@ -677,8 +709,21 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
   const int n0 = blockIdx.x * NG, w = blockIdx.y;
   const int ng = min(NG, nchol - n0);
   const int sfs = nel * nv, sus = nh * nv;
-  const c128* Tw = Twina + size_t(w) * nel * nchol * nact;
+  const TW* Tw = Twina + size_t(w) * nel * nchol * nact;
   const c128* Qw = QQ0 + size_t(w) * nact * nel;
+  auto load_t = [&](int g, C* dst) {
+    const int n = n0 + g;
+    for (int k = threadIdx.x; k < nel * nact; k += blockDim.x) {
+      const int j = k / nact, x = k - j * nact;
+      const TW* src = Tw + (size_t(j) * nchol + n) * nact + x;
+      if constexpr (ASYNC)
+        cp_async<int(sizeof(C))>(dst + k, src);
+      else
+        dst[k] = to_cx<C>(*src);
+    }
+    if constexpr (ASYNC) cp_async_commit();
+  };
+  load_t(0, Tb0);
   for (int k = threadIdx.x; k < nel * nv; k += blockDim.x) {
     const int i = k / nv, c = k - i * nv;
     Qv[k] = to_cx<C>(Qw[size_t(vl[c]) * nel + i]);
@@ -694,11 +739,14 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
     f00[g] = cmk(0, 0);
     if (g >= ng) break;
     const int n = n0 + g;
+    C* Tn = (g & 1) ? Tb1 : Tb0;
     C* Sg = Sf + g * sfs;
     C* Ug = SU + g * sus;
-    for (int k = threadIdx.x; k < nel * nact; k += blockDim.x) {
-      const int j = k / nact, x = k - j * nact;
-      Tn[k] = to_cx<C>(Tw[(size_t(j) * nchol + n) * nact + x]);
+    if (nbuf == 2 && g + 1 < ng) {
+      load_t(g + 1, (g & 1) ? Tb0 : Tb1);  // the other buffer, free since the last barrier
+      if constexpr (ASYNC) cp_async_wait<1>();
+    } else {
+      if constexpr (ASYNC) cp_async_wait<0>();
     }
     __syncthreads();
     // Y = t[:, r] Qv (into Sf)
@@ -737,16 +785,18 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
       atomicAdd(&REF[2 * w + 1].x, f00[g].x);
       atomicAdd(&REF[2 * w + 1].y, f00[g].y);
     }
+    if (nbuf == 1 && g + 1 < ng) load_t(g + 1, Tb0);
   }
   __syncthreads();
   c128 exs = cmk(0, 0), ejs = cmk(0, 0), ejc = cmk(0, 0);
-  const c128* Iw = INV + size_t(w) * ninv;
+  const C* Iw = INVc + size_t(w) * ninv;
   for (int u = 1 + threadIdx.x; u < nuniq; u += blockDim.x) {
-    const int nex = unex[u];
-    const int* e4 = uexc4 + uoff4[u];
-    const c128* Qi = Iw + uinv[u];
+    const int4 hd = uhdr[u];
+    const c128 wu = wgt[size_t(u) * W + w];
+    const int* e4 = uexc4 + hd.y;
+    const C* Qi = Iw + hd.z;
     C exw[NG], knw[NG];
-    switch (nex) {
+    switch (hd.x) {
       case 1: excited_terms<1, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
       case 2: excited_terms<2, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
       case 3: excited_terms<3, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
@@ -769,7 +819,6 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
       else
         KE[o + g] = kn;
     }
-    const c128 wu = wgt[size_t(u) * W + w];
     exs = cadd(exs, cmul(wu, exu));
     ejs = cadd(ejs, cmul(wu, eju));
   }
@@ -1106,6 +1155,12 @@ struct afqmc_phmsd_s {
   int nkseg = 0;
   bool kseg_split = false;
   c128* INV = nullptr;
+  // mixed precision: the same inverses in complex64 (float2, half the bytes of INV's buffer)
+  c128* INV32 = nullptr;
+  // per unique excitation {nex, uoff4, uinv, 0} (one load in the energy tables kernel)
+  int4* uhdr[2] = {nullptr, nullptr};
+  // Twina holds complex64 elements (the mixed tensor-core half rotation feeding the tables)
+  bool twina64[2] = {false, false};
   // energy: the Hamiltonian half-rotated with the active orbitals
   bool has_ham = false;
   int Nc = 0;
@@ -1141,7 +1196,7 @@ struct afqmc_phmsd_s {
   }
   void free_core_scratch() {
     for (c128** q : {&eG[0], &eG[1], &eQ[0], &eQ[1], &eov[0], &eov[1], &eTMN, &eTNN, &elogov,
-                     &eOv, &wgt, &Rfull, &INV})
+                     &eOv, &wgt, &Rfull, &INV, &INV32})
       if (*q) {
         cudaFree(*q);
         *q = nullptr;
@@ -1169,6 +1224,7 @@ struct afqmc_phmsd_s {
       cudaFree(vl[s]);
       cudaFree(uexc4[s]);
       cudaFree(uoff4[s]);
+      cudaFree(uhdr[s]);
       cudaFree(lnak[s]);
       cudaFree(haj[s]);
       cudaFree(orbmat[s]);
@@ -1397,6 +1453,9 @@ extern "C" int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact
     AFQMC_TRY(to_device(&h->vl[s], vlv.data(), vlv.size()));
     AFQMC_TRY(to_device(&h->uexc4[s], e4.data(), e4.size()));
     AFQMC_TRY(to_device(&h->uoff4[s], o4.data(), o4.size()));
+    std::vector<int4> hd(nuniq[s], make_int4(0, 0, 0, 0));
+    for (int u = 1; u < nuniq[s]; ++u) hd[u] = make_int4(nex[s][u], o4[u], io[u], 0);
+    AFQMC_TRY(to_device(&h->uhdr[s], hd.data(), hd.size()));
   }
   *out = h.release();
   return AFQMC_OK;
@@ -1583,6 +1642,7 @@ int phmsd_core_scratch(afqmc_phmsd h, int Wb) {
   AFQMC_TRY(scratch_alloc(&h->wgt, nu * Wb));
   AFQMC_TRY(scratch_alloc(&h->Rfull, size_t(Wb) * ne * na));
   AFQMC_TRY(scratch_alloc(&h->INV, size_t(Wb) * std::max(h->ninv[0], h->ninv[1])));
+  AFQMC_TRY(scratch_alloc(&h->INV32, (size_t(Wb) * std::max(h->ninv[0], h->ninv[1]) + 1) / 2));
   h->capCore = Wb;
   return AFQMC_OK;
 }
@@ -1650,6 +1710,20 @@ int phmsd_spin_factors(afqmc_phmsd h, cudaStream_t s, int sp, const c128* S, lon
 }
 
 // Swia = G haj^T, Twina = G Lnak^T for spin sp
+// shared memory of excited_energy_tables_kernel: nbuf buffers of the rows t_j, Qv, and ng
+// pairs of tables Sf, SU, in elements of elem bytes
+size_t excited_tables_smem(afqmc_phmsd h, int sp, size_t elem, int ng, int nbuf) {
+  const size_t N = h->nel[sp], na = h->nact[sp], nv = h->nv[sp], nh = h->nh[sp];
+  return (size_t(nbuf) * N * na + N * nv + size_t(ng) * (N * nv + nh * nv)) * elem +
+         (N + nh + nv) * sizeof(int);
+}
+
+// the energy of spin sp runs the per-(walker, n) tables kernel (else the per-shell R rows)
+bool phmsd_tables(afqmc_phmsd h, int sp) {
+  const size_t esz = h->precision == AFQMC_PREC_MIXED ? sizeof(c64) : sizeof(c128);
+  return h->tables_ok[sp] && excited_tables_smem(h, sp, esz, 1, 1) <= 200 * 1024;
+}
+
 int phmsd_half_rotated(afqmc_phmsd h, cudaStream_t s, int sp, int nb) {
   const int N = h->nel[sp], na = h->nact[sp];
   GemmParams p{};
@@ -1668,10 +1742,14 @@ int phmsd_half_rotated(afqmc_phmsd h, cudaStream_t s, int sp, int nb) {
       if (st != AFQMC_OK && st != AFQMC_ERR_UNSUPPORTED) return st;
       h->tc_lnak_state[sp] = st == AFQMC_OK ? 1 : -1;
     }
-    if (h->tc_lnak_state[sp] == 1)
+    if (h->tc_lnak_state[sp] == 1) {
+      // complex64 output where only the tables kernel reads it
+      h->twina64[sp] = phmsd_tables(h, sp);
       return tcgemm_rb_run(s, h->tc_lnak[sp], h->eG[sp], h->M, nb * N, h->Twina,
-                           long(h->Nc) * na);
+                           long(h->Nc) * na, h->twina64[sp]);
+    }
   }
+  h->twina64[sp] = false;
   GemmParams q{};
   q.m = nb * N; q.n = h->Nc * na; q.k = h->M;
   q.A = h->eG[sp]; q.lda = h->M;
@@ -1679,15 +1757,6 @@ int phmsd_half_rotated(afqmc_phmsd h, cudaStream_t s, int sp, int nb) {
   q.C = h->Twina; q.ldc = long(h->Nc) * na;
   q.alpha = cmk(1, 0); q.beta = cmk(0, 0);
   return zgemm(s, 1, GN, false, GT, false, q);
-}
-
-// the excited determinants of spin sp, shell by shell: 1-body into el[0], 2-body into el[1..2],
-// KE of each determinant written to KEout + k0 * nb * Nc (cross = nullptr) or to KEl and
-// contracted with cross at once (the second step)
-size_t excited_tables_smem(afqmc_phmsd h, int sp, size_t elem = sizeof(c128), int ng = 1) {
-  const size_t N = h->nel[sp], na = h->nact[sp], nv = h->nv[sp], nh = h->nh[sp];
-  return (N * na + N * nv + size_t(ng) * (N * nv + nh * nv)) * elem +
-         (N + nh + nv) * sizeof(int);
 }
 
 // The reference determinant's and the excited determinants' energies of spin sp
@@ -1699,8 +1768,7 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
   // the 2-body terms from per-(walker, n) tables when they fit in shared memory, else per shell
   // from the R rows (the reference kernel's formulation)
   const bool mixed = h->precision == AFQMC_PREC_MIXED;
-  const size_t tsmem = excited_tables_smem(h, sp, mixed ? sizeof(c64) : sizeof(c128));
-  const bool tables = h->tables_ok[sp] && tsmem <= 200 * 1024;
+  const bool tables = phmsd_tables(h, sp);
   if (!tables) {
     ph_reference_kernel<<<nb, PH_THREADS, 0, s>>>(h->Swia, h->Twina, h->refc[sp], N, Nc, na, E0,
                                                   h->eOv, E, Kref);
@@ -1742,7 +1810,7 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
       const long nt = long(h->nuniq[sp] - 1) * nb;
       woodbury_inverses_kernel<<<unsigned((nt + 127) / 128), 128, 0, s>>>(
           h->eQ[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp], h->nuniq[sp], nb, na, N,
-          h->ninv[sp], h->INV);
+          h->ninv[sp], h->INV, mixed ? reinterpret_cast<float2*>(h->INV32) : nullptr);
       AFQMC_TRY(launch_status("woodbury_inverses_kernel"));
       excited_1body_all_kernel<<<nb, PH_THREADS, 0, s>>>(
           h->Swia, h->eQ[sp], h->refc[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp],
@@ -1751,23 +1819,35 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
     }
     c128* REF = h->el + 3 * nb;  // [nb][2]: sum_n ex0, sum_n f0^2
     // four Cholesky indices per CTA where their tables fit (each determinant's Q, indices and
-    // weight are then read once per four indices), else one
+    // weight are then read once per four indices), the next index's rows loaded while the
+    // current tables are built where a second row buffer fits
     const size_t esz = mixed ? sizeof(c64) : sizeof(c128);
-    const size_t smem4 = excited_tables_smem(h, sp, esz, 4);
-    const bool g4 = smem4 <= (mixed ? 110 : 200) * 1024;
-    const int NGr = g4 ? 4 : 1;
-    const size_t smem = g4 ? smem4 : tsmem;
-    auto kern = mixed ? (g4 ? excited_energy_tables_kernel<float, 4>
-                            : excited_energy_tables_kernel<float, 1>)
-                      : (g4 ? excited_energy_tables_kernel<double, 4>
-                            : excited_energy_tables_kernel<double, 1>);
-    AFQMC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        int(smem)));
-    kern<<<dim3((Nc + NGr - 1) / NGr, nb), PHX_THREADS, smem, s>>>(
-        h->Twina, h->eQ[sp], h->refc[sp], h->hl[sp], h->vl[sp], h->nh[sp], h->nv[sp],
-        h->uoff4[sp], h->unex[sp], h->uexc4[sp], h->uinv[sp], h->INV, h->ninv[sp], h->wgt,
-        h->nuniq[sp], nb, N, na, Nc, h->el + nb, h->el + 2 * nb, cross ? nullptr : KEout, cross,
-        E, Kref, REF);
+    const size_t lim = size_t(mixed ? 110 : 200) * 1024;
+    int ngr = 4, nbuf = 2;
+    if (excited_tables_smem(h, sp, esz, 4, 2) > lim) nbuf = 1;
+    if (excited_tables_smem(h, sp, esz, 4, nbuf) > lim) ngr = nbuf = 1;
+    const size_t smem = excited_tables_smem(h, sp, esz, ngr, nbuf);
+    const dim3 grid((Nc + ngr - 1) / ngr, nb);
+    auto go = [&](auto kern, const auto* tw, const auto* inv) -> int {
+      AFQMC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(smem)));
+      kern<<<grid, PHX_THREADS, smem, s>>>(
+          tw, h->eQ[sp], h->refc[sp], h->hl[sp], h->vl[sp], h->nh[sp], h->nv[sp], h->uhdr[sp],
+          h->uexc4[sp], inv, h->ninv[sp], h->wgt, h->nuniq[sp], nb, N, na, Nc, nbuf, h->el + nb,
+          h->el + 2 * nb, cross ? nullptr : KEout, cross, E, Kref, REF);
+      return AFQMC_OK;
+    };
+    const c64* inv32 = reinterpret_cast<const c64*>(h->INV32);
+    const c64* tw64 = reinterpret_cast<const c64*>(h->Twina);
+    if (mixed && h->twina64[sp])
+      AFQMC_TRY(ngr == 4 ? go(excited_energy_tables_kernel<float, 4, c64>, tw64, inv32)
+                         : go(excited_energy_tables_kernel<float, 1, c64>, tw64, inv32));
+    else if (mixed)
+      AFQMC_TRY(ngr == 4 ? go(excited_energy_tables_kernel<float, 4, c128>, h->Twina, inv32)
+                         : go(excited_energy_tables_kernel<float, 1, c128>, h->Twina, inv32));
+    else
+      AFQMC_TRY(ngr == 4 ? go(excited_energy_tables_kernel<double, 4, c128>, h->Twina, h->INV)
+                         : go(excited_energy_tables_kernel<double, 1, c128>, h->Twina, h->INV));
     AFQMC_TRY(launch_status("excited_energy_tables_kernel"));
     reference_from_tables_kernel<<<(nb + 127) / 128, 128, 0, s>>>(h->Swia, h->refc[sp], N, na, E0,
                                                                   h->eOv, REF, nb, E);
@@ -1907,7 +1987,7 @@ extern "C" int afqmc_phmsd_density_matrix(afqmc_phmsd h, const afqmc_c128* wbuf,
           const long ni = long(nu - 1) * nb;
           woodbury_inverses_kernel<<<unsigned((ni + 127) / 128), 128, 0, s>>>(
               h->eQ[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp], nu, nb, na, N,
-              h->ninv[sp], h->INV);
+              h->ninv[sp], h->INV, nullptr);
           AFQMC_TRY(launch_status("woodbury_inverses_kernel"));
         }
         const size_t rsm = 3 * size_t(N) * na * sizeof(c128);
