@@ -309,16 +309,26 @@ __global__ void couple_kernel(const int* __restrict__ rowptr, const int* __restr
                               const c128* __restrict__ v_other, int nu_other,
                               const c128* __restrict__ ov_self, int nu, int W,
                               c128* __restrict__ wgt) {
-  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  // one warp per (u, w): the row of the reference (u = 0) holds a large share of the
+  // determinants, so its entries are split over the lanes
+  const long t = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (t >= long(nu) * W) return;
   const int u = int(t / W), w = int(t - long(u) * W);
   c128 acc = cmk(0, 0);
-  for (int j = rowptr[u]; j < rowptr[u + 1]; ++j) {
+  for (int j = rowptr[u] + lane; j < rowptr[u + 1]; j += 32) {
     const int k = kidx[j];
     acc = cadd(acc, cmul(coef[k], v_other[size_t(w) * nu_other + det_other[k]]));
   }
-  if (ov_self) acc = cmul(acc, ov_self[size_t(w) * nu + u]);
-  wgt[t] = acc;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+  }
+  if (lane == 0) {
+    if (ov_self) acc = cmul(acc, ov_self[size_t(w) * nu + u]);
+    wgt[t] = acc;
+  }
 }
 
 // Ov[w] = sum_u wgt[u][w] ov[w][u]   (before the weights are scaled by the overlaps)
@@ -474,43 +484,48 @@ __global__ void woodbury_inverses_kernel(const c128* __restrict__ QQ0, const int
 }
 
 // The 1-body energies of every unique excitation u >= 1 for walker blockIdx.x, from the
-// Woodbury inverses Qi (INV, uinv) instead of R rows (ph_excited_1body_kernel over compact_R's
+// Woodbury inverses Qi (INV, uhdr) instead of R rows (ph_excited_1body_kernel over compact_R's
 // rows, PHMSD.cpp:376-546): with R_u[p] = sum_q Qi[p][q] (e_{part_q} - sum_i QQ0[part_q][i]
 // e_{o_u(i)}), o_u(i) the orbital of electron i in determinant u (its particle for a hole, else
 // refc[i]),
 //   e1_u = sum_p (S[i_p] . R_u[p] + S[i_p][part_p] - S[i_p][refc[i_p]]),
-// and E[w] += sum_u wgt[u][w] e1_u.  A singular block has Qi = 0, so R_u = 0 (as the reference).
+// and E[w] += sum_u wgt[u][w] e1_u.  Because Qi inverts M[q][x] = QQ0[part_q][i_x], the terms at
+// the holes' reference orbitals cancel and e1_u = sum_{p,q} Qi[p][q] Sf1[i_p][c_q] with the
+// per-walker table Sf1[i][c] = S[i][v_c] - sum_j S[i][refc_j] QQ0[v_c][j] (v_c the virtual
+// orbitals, c_q the particle columns).  A singular block has Qi = 0, so e1_u = 0 (as the
+// reference).  Grid (walkers, parts): each CTA builds Sf1 and takes every gridDim.y-th excitation.
 __global__ void __launch_bounds__(PH_THREADS) excited_1body_all_kernel(
     const c128* __restrict__ S, const c128* __restrict__ QQ0, const int* __restrict__ refc,
-    const int* __restrict__ uoff, const int* __restrict__ unex, const int* __restrict__ uexc,
-    const int* __restrict__ uinv, const c128* __restrict__ INV, int ninv,
+    const int* __restrict__ vl, int nv, const int4* __restrict__ uhdr,
+    const int* __restrict__ uexc4, const c128* __restrict__ INV, int ninv,
     const c128* __restrict__ wgt, int nuniq, int W, int nel, int nact, c128* __restrict__ E) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  c128* sf1 = reinterpret_cast<c128*>(smem_raw);  // [nel][nv]
   __shared__ double red[PH_THREADS / 32 * 6];
   const int w = blockIdx.x;
   const c128* Sw = S + size_t(w) * nel * nact;
   const c128* Q0 = QQ0 + size_t(w) * nact * nel;
   const c128* Iw = INV + size_t(w) * ninv;
+  for (int k = threadIdx.x; k < nel * nv; k += blockDim.x) {
+    const int i = k / nv, c = k - i * nv;
+    const c128* Si = Sw + size_t(i) * nact;
+    const c128* Qc = Q0 + size_t(vl[c]) * nel;
+    c128 t = Si[vl[c]];
+    for (int j = 0; j < nel; ++j) t = csub(t, cmul(Si[refc[j]], Qc[j]));
+    sf1[k] = t;
+  }
+  __syncthreads();
   c128 acc = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0);
-  for (int u = 1 + threadIdx.x; u < nuniq; u += blockDim.x) {
-    const int n = unex[u];
-    const int* e = uexc + uoff[u];  // holes e[0..n), particles e[n..2n)
-    const c128* Qi = Iw + uinv[u];
+  for (int u = 1 + blockIdx.y * blockDim.x + threadIdx.x; u < nuniq;
+       u += gridDim.y * blockDim.x) {
+    const int4 hd = uhdr[u];
+    const int n = hd.x;
+    const int* e4 = uexc4 + hd.y;  // holes, particles, hole rows, particle columns
+    const c128* Qi = Iw + hd.z;
     c128 e1 = cmk(0, 0);
     for (int p = 0; p < n; ++p) {
-      const c128* Sp = Sw + size_t(e[p]) * nact;
-      e1 = cadd(e1, csub(Sp[e[n + p]], Sp[refc[e[p]]]));
-      for (int q = 0; q < n; ++q) {
-        const c128* Tq = Q0 + size_t(e[n + q]) * nel;  // QQ0[part_q][:]
-        // S[i_p] . (e_{part_q} - sum_i QQ0[part_q][i] e_{o_u(i)})
-        c128 t = Sp[e[n + q]];
-        for (int i = 0; i < nel; ++i) {
-          int oi = refc[i];
-          for (int hh = 0; hh < n; ++hh)
-            if (e[hh] == i) oi = e[n + hh];
-          t = csub(t, cmul(Tq[i], Sp[oi]));
-        }
-        e1 = cadd(e1, cmul(Qi[p * n + q], t));
-      }
+      const c128* row = sf1 + e4[p] * nv;
+      for (int q = 0; q < n; ++q) e1 = cadd(e1, cmul(Qi[p * n + q], row[e4[3 * n + q]]));
     }
     acc = cadd(acc, cmul(wgt[size_t(u) * W + w], e1));
   }
@@ -602,49 +617,46 @@ __device__ __noinline__ void excited_terms_rare(const int* e4, const C* Qi, cons
   excited_terms<NEX, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0, exg, kng);
 }
 
-// One product of the tables: out[k][c] = sum_j a[k][sel_j] b[j][c] over the rows k of `rows`
-// (row index rows[k], or k when rows is null).
-template <typename C>
-struct TableProduct {
-  const C* a;
-  int lda;
-  const int* rows;
-  int nrows;
-  const C* b;
-  int ldb, ncol;
-  C* out;
-  int ldo;
-};
-
-// Runs products side by side over the block: a thread owns the columns t and t + nt (nt =
-// ceil(ncol / 2)) of one row, so that each shared-memory read of a feeds two products and
-// neighbouring threads read neighbouring columns of b.
-template <int NP, typename C>
-__device__ __forceinline__ void table_products(const TableProduct<C> (&P)[NP], const int* sel,
-                                               int nsum) {
-  int start[NP + 1];
-  start[0] = 0;
+// One product of the tables: out[k][c] = sum_j a[r_k][sel_j] b[j][c] over the rows k < nrows
+// (r_k = rows[k], or k when rows is null), c < ncol.  A thread owns RT rows and the columns
+// t and t + half (half = ceil(ncol / 2)) of them, so that every shared-memory read of a feeds
+// two products and every read of b feeds RT; neighbouring threads read neighbouring columns of b.
+template <int RT, typename C>
+__device__ __forceinline__ void table_product(const C* a, int lda, const int* rows, int nrows,
+                                              const int* sel, int nsum, const C* b, int ldb,
+                                              int ncol, C* out, int ldo) {
+  const int half = (ncol + 1) / 2;
+  const int nrt = (nrows + RT - 1) / RT;
+  for (int t = threadIdx.x; t < nrt * half; t += blockDim.x) {
+    const int rt = t / half, ct = t - rt * half;
+    const bool two = ct + half < ncol;
+    const C* ar[RT];
 #pragma unroll
-  for (int i = 0; i < NP; ++i) start[i + 1] = start[i] + P[i].nrows * ((P[i].ncol + 1) / 2);
-  for (int idx = threadIdx.x; idx < start[NP]; idx += blockDim.x) {
-    int i = 0;
-#pragma unroll
-    for (int q = 1; q < NP; ++q)
-      if (idx >= start[q]) i = q;
-    const TableProduct<C>& T = P[i];
-    const int nt = (T.ncol + 1) / 2, loc = idx - start[i];
-    const int k = loc / nt, t = loc - k * nt;
-    const bool two = t + nt < T.ncol;
-    const C* ak = T.a + (T.rows ? T.rows[k] : k) * T.lda;
-    C a0 = czero<C>(), a1 = czero<C>();
-    for (int j = 0; j < nsum; ++j) {
-      const C x = ak[sel[j]];
-      const C* bj = T.b + j * T.ldb + t;
-      a0 = cadd(a0, cmul(x, bj[0]));
-      if (two) a1 = cadd(a1, cmul(x, bj[nt]));
+    for (int r = 0; r < RT; ++r) {
+      const int k = rt * RT + r;
+      ar[r] = a + (k < nrows ? (rows ? rows[k] : k) : 0) * lda;  // a row past the end: row 0
     }
-    T.out[k * T.ldo + t] = a0;
-    if (two) T.out[k * T.ldo + t + nt] = a1;
+    C acc0[RT], acc1[RT];
+#pragma unroll
+    for (int r = 0; r < RT; ++r) acc0[r] = acc1[r] = czero<C>();
+    for (int j = 0; j < nsum; ++j) {
+      const int sj = sel[j];
+      const C b0 = b[j * ldb + ct];
+      const C b1 = two ? b[j * ldb + ct + half] : czero<C>();
+#pragma unroll
+      for (int r = 0; r < RT; ++r) {
+        const C x = ar[r][sj];
+        acc0[r] = cadd(acc0[r], cmul(x, b0));
+        acc1[r] = cadd(acc1[r], cmul(x, b1));
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < RT; ++r) {
+      const int k = rt * RT + r;
+      if (k >= nrows) break;
+      out[k * ldo + ct] = acc0[r];
+      if (two) out[k * ldo + ct + half] = acc1[r];
+    }
   }
 }
 
@@ -750,10 +762,7 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
     }
     __syncthreads();
     // Y = t[:, r] Qv (into Sf)
-    {
-      const TableProduct<C> P[1] = {{Tn, nact, nullptr, nel, Qv, nv, nv, Sg, nv}};
-      table_products<1, C>(P, refs, nel);
-    }
+    table_product<3, C>(Tn, nact, nullptr, nel, refs, nel, Qv, nv, nv, Sg, nv);
     // the reference determinant: f0 = sum_i t_i[r_i], ex0 = sum_ij t_i[r_j] t_j[r_i]
     c128 ex0 = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0);
     for (int k = threadIdx.x; k < nel * nel; k += blockDim.x) {
@@ -769,10 +778,7 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
     }
     __syncthreads();
     // SU = t[hole rows, r] Sf
-    {
-      const TableProduct<C> P[1] = {{Tn, nact, hls, nh, Sg, nv, nv, Ug, nv}};
-      table_products<1, C>(P, refs, nel);
-    }
+    table_product<3, C>(Tn, nact, hls, nh, refs, nel, Sg, nv, nv, Ug, nv);
     c128 f0 = cmk(0, 0);
     for (int i = 0; i < nel; ++i) f0 = cadd(f0, to_cx<c128>(Tn[i * nact + refs[i]]));
     f0w[g] = to_cx<C>(f0);
@@ -1812,8 +1818,11 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
           h->eQ[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp], h->nuniq[sp], nb, na, N,
           h->ninv[sp], h->INV, mixed ? reinterpret_cast<float2*>(h->INV32) : nullptr);
       AFQMC_TRY(launch_status("woodbury_inverses_kernel"));
-      excited_1body_all_kernel<<<nb, PH_THREADS, 0, s>>>(
-          h->Swia, h->eQ[sp], h->refc[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp],
+      const size_t sm1 = size_t(N) * h->nv[sp] * sizeof(c128);
+      AFQMC_CUDA_TRY(cudaFuncSetAttribute(excited_1body_all_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm1)));
+      excited_1body_all_kernel<<<dim3(nb, 4), PH_THREADS, sm1, s>>>(
+          h->Swia, h->eQ[sp], h->refc[sp], h->vl[sp], h->nv[sp], h->uhdr[sp], h->uexc4[sp],
           h->INV, h->ninv[sp], h->wgt, h->nuniq[sp], nb, N, na, h->el);
       AFQMC_TRY(launch_status("excited_1body_all_kernel"));
     }
@@ -1894,7 +1903,7 @@ extern "C" int afqmc_phmsd_energy(afqmc_phmsd h, const afqmc_c128* wbuf, long ld
       const int nu0 = h->nuniq[0], nu1 = h->nuniq[1];
       auto couple = [&](int sp, const c128* v_other, int nu_other, const c128* ov_self) -> int {
         const long nt = long(h->nuniq[sp]) * nb;
-        couple_kernel<<<unsigned((nt + 127) / 128), 128, 0, s>>>(
+        couple_kernel<<<unsigned((nt + 3) / 4), 128, 0, s>>>(
             h->rowptr[sp], h->kidx[sp], h->det[1 - sp], h->coef, v_other, nu_other, ov_self,
             h->nuniq[sp], nb, h->wgt);
         return launch_status("couple_kernel");
@@ -1970,14 +1979,14 @@ extern "C" int afqmc_phmsd_density_matrix(afqmc_phmsd h, const afqmc_c128* wbuf,
         const long nt = long(nu) * nb;
         // wgt[u][w] (PHMSD.cpp:717-724, 754-760)
         if (sp == 0) {
-          couple_kernel<<<unsigned((nt + 127) / 128), 128, 0, s>>>(
+          couple_kernel<<<unsigned((nt + 3) / 4), 128, 0, s>>>(
               h->rowptr[0], h->kidx[0], h->det[1], h->coef, h->eov[1], h->nuniq[1], nullptr, nu,
               nb, h->wgt);
           AFQMC_TRY(launch_status("couple_kernel"));
           total_overlap_kernel<<<nb, PH_THREADS, 0, s>>>(h->wgt, h->eov[0], nu, nb, h->eOv);
           AFQMC_TRY(launch_status("total_overlap_kernel"));
         }
-        couple_kernel<<<unsigned((nt + 127) / 128), 128, 0, s>>>(
+        couple_kernel<<<unsigned((nt + 3) / 4), 128, 0, s>>>(
             h->rowptr[sp], h->kidx[sp], h->det[1 - sp], h->coef, h->eov[1 - sp],
             h->nuniq[1 - sp], h->eov[sp], nu, nb, h->wgt);
         AFQMC_TRY(launch_status("couple_kernel"));
