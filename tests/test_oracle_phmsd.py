@@ -199,3 +199,51 @@ def test_excitations_from_occupation_lists():
         tot = sum(np.conj(coef[k]) * np.linalg.det(orb[0][occ[0][k]] @ Su[w]) *
                   np.linalg.det(orb[1][occ[1][k]] @ Sd[w]) for k in range(ndet))
         assert abs(np.exp(logov[w]) - tot) <= 1e-10 * abs(tot)
+
+
+@pytest.mark.parametrize("nex", [1, 2, 3, 4, 5])
+def test_reduced_closed_form_matches_the_reference_sums(nex):
+    """The reduced closed form the GPU tables kernels evaluate (phmsd.cu `excited_terms`,
+    `excited_1body_all_kernel`), restated in numpy, against the reference's per-determinant
+    sums (ph_excited_2body_energy_dense_cholesky / ph_excited_1body_energy over compact_R's
+    rows).  With Q the inverse of the excitation block M[q][x] = QQ0[p_q][h_x]:
+      Sf[j][c] = t_j[v_c] - sum_i t_j[r_i] QQ0[v_c][i],  SU[h][c] = sum_j t_h[r_j] Sf[j][c],
+      P[a][b] = sum_q Sf[h_a][c_q] Q[b][q],  Kn = f0 + tr P,
+      eX = sum_n (tr(P P) + 2 sum_{a,q} Q[a][q] SU[h_a][c_q]),
+      e1 = sum_{p,q} Q[p][q] Sf1[h_p][c_q],  Sf1 = S[:, v] - S[:, r] QQ0[v, :]^T."""
+    rs = np.random.default_rng(40 + nex)
+    nw, nel, nchol, nact = 2, 6, 5, 13
+    refc = np.arange(nel)
+    virt = np.arange(nel, nact)
+
+    def cx(*shape):
+        return rs.standard_normal(shape) + 1j * rs.standard_normal(shape)
+
+    T = cx(nw, nel, nchol, nact)
+    S = cx(nw, nel, nact)
+    QQ0 = cx(nw, nact, nel)
+    for _ in range(3):
+        holes = np.sort(rs.choice(nel, nex, replace=False))
+        parts = np.sort(rs.choice(virt, nex, replace=False))
+        iexcit = np.concatenate([holes, parts])[None]
+        R = P.compact_R(iexcit, refc, QQ0)
+        wgt = np.ones((1, nw), complex)
+        EX, EJ, KE = P.ph_excited_2body_energy_dense_cholesky(iexcit, refc, T, R, wgt)
+        E1 = P.ph_excited_1body_energy(iexcit, refc, S, R, wgt)
+        cols = parts - nel  # particle columns among the virtual orbitals
+        for w in range(nw):
+            Q = np.linalg.inv(QQ0[w][np.ix_(parts, holes)])
+            eX = 0j
+            Kn = np.zeros(nchol, complex)
+            for n in range(nchol):
+                t = T[w, :, n, :]
+                Sf = t[:, virt] - t[:, refc] @ QQ0[w][virt, :].T
+                SU = t[:, refc] @ Sf
+                Pm = Sf[np.ix_(holes, cols)] @ Q.T
+                eX += np.trace(Pm @ Pm) + 2 * np.sum(Q * SU[np.ix_(holes, cols)])
+                Kn[n] = sum(t[i, refc[i]] for i in range(nel)) + np.trace(Pm)
+            assert abs(-0.5 * eX - EX[w]) <= 1e-10 * abs(EX[w])
+            assert np.max(np.abs(Kn - KE[0, w])) <= 1e-10 * np.max(np.abs(KE[0, w]))
+            Sf1 = S[w][:, virt] - S[w][:, refc] @ QQ0[w][virt, :].T
+            e1 = np.sum(Q * Sf1[np.ix_(holes, cols)])
+            assert abs(e1 - E1[w]) <= 1e-10 * abs(E1[w])
