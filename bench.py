@@ -327,6 +327,8 @@ def tf32_peak_tflops(torch):
 
 
 SEGMENT_BLOCKS = 8  # blocks timed from one restart of the walkers at the trial
+# dense BF16 rate (the kind::f16 roofline denominator) when MEASURED_PEAKS.json is absent
+BF16_FALLBACK_TFLOPS = 1590.0
 
 
 def _segmented(sim, n_blocks, world, body, clocks=None):
@@ -509,6 +511,10 @@ def _roofline(sim, wl, W, prec, phases, args, torch, taylor_mode=1):
         if f16_top and peaks.get("bf16_tflops"):
             peak = float(peaks["bf16_tflops"])
             peak_src = "of measured: MEASURED_PEAKS.json bf16_tflops (dense kind::f16 rate)"
+        elif f16_top:
+            peak = BF16_FALLBACK_TFLOPS
+            peak_src = "of fallback: 1590 TFLOP/s dense BF16, an earlier measurement on this " \
+                       "GPU type (no MEASURED_PEAKS.json)"
         else:
             peak = tf32_peak_tflops(torch)
             peak_src = "cuBLAS TF32 GEMM 8192^3 measured in this run (no TF32 entry in the file " \

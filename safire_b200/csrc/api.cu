@@ -179,19 +179,19 @@ struct afqmc_host_rng_s {
 // PsiT stacked per spin ([nd][N_s][M] at nd * el_off[s] * M), so one GEMM per walker forms the
 // overlap matrices of all determinants, one Gauss-Jordan launch inverts them, and one GEMM
 // with K = nd * N_s sums the weighted full density matrices.  Walkers go in chunks of wchunk
-// (the batched GEMM's grid limit and a bounded workspace): Tb [wchunk][nd][N_s][N_s] and
-// Gcb [wchunk][nd][N_s][M] per spin, ovd / wdd [wchunk][nd].
+// (the batched launches' grid limit and a bounded workspace): Tb and Ttb
+// [wchunk][nd][N_s][N_s] and Gcb [wchunk][nd][N_s][M] per spin, ovd / wdd [wchunk][nd].
 struct afqmc_nomsd_s {
   int device = 0;
   std::vector<afqmc_ham_s*> hams;
   std::vector<c128> ci;
   c128 *PsiTall = nullptr, *dcc = nullptr, *dlc = nullptr;  // conj(ci), log conj(ci)
   c128 *Gc = nullptr, *ov = nullptr, *T = nullptr, *Ed = nullptr;  // energy (per determinant)
-  c128 *Tb = nullptr, *Gcb = nullptr, *ovd = nullptr, *wdd = nullptr;
+  c128 *Tb = nullptr, *Ttb = nullptr, *Gcb = nullptr, *ovd = nullptr, *wdd = nullptr;
   int capW = 0, wchunk = 0;
   void free_bufs() {
     dfree(Gc); dfree(ov); dfree(T); dfree(Ed);
-    dfree(Tb); dfree(Gcb); dfree(ovd); dfree(wdd);
+    dfree(Tb); dfree(Ttb); dfree(Gcb); dfree(ovd); dfree(wdd);
     capW = 0;
     wchunk = 0;
   }
@@ -1167,6 +1167,7 @@ int nomsd_bufs(afqmc_nomsd md, int W) {
   size_t wc = std::min<size_t>(size_t(W), 65535 / nd);
   wc = std::min(wc, std::max<size_t>(1, NOMSD_CHUNK_BYTES / per_walker));
   AFQMC_TRY(dalloc(&md->Tb, wc * nd * (nsq > 0 ? nsq : 1)));
+  AFQMC_TRY(dalloc(&md->Ttb, wc * nd * (nsq > 0 ? nsq : 1)));
   AFQMC_TRY(dalloc(&md->Gcb, wc * nd * size_t(ldG > 0 ? ldG : 1)));
   AFQMC_TRY(dalloc(&md->ovd, wc * nd));
   AFQMC_TRY(dalloc(&md->wdd, wc * nd));
@@ -1214,11 +1215,15 @@ __global__ void multidet_weights_kernel(const c128* __restrict__ ovd, const c128
   Ov[w] = cadd(sum, shift);
 }
 
-// T[b][:] *= wdd[b] for blocks of n elements
-__global__ void scale_blocks_kernel(c128* __restrict__ T, long n, long nb,
-                                    const c128* __restrict__ wdd) {
+// Tt[b] = wdd[b] T[b]^T for nb blocks of n x n elements
+__global__ void weight_transpose_blocks_kernel(const c128* __restrict__ T, c128* __restrict__ Tt,
+                                               int n, long nb, const c128* __restrict__ wdd) {
   const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t < n * nb) T[t] = cmul(T[t], wdd[t / n]);
+  const long nsq = long(n) * n;
+  if (t >= nsq * nb) return;
+  const long b = t / nsq;
+  const int e = int(t - b * nsq), i = e / n, j = e - i * n;
+  Tt[b * nsq + long(j) * n + i] = cmul(T[t], wdd[b]);
 }
 
 // Overlap matrices T[w][d] = PsiT_d S_w of every determinant for walkers w0 .. w0+wc-1 (one
@@ -1291,18 +1296,21 @@ int nomsd_density_matrix(afqmc_nomsd md, afqmc_wset_s* ws, cudaStream_t s, c128*
       }
       const long nsq = long(Ns) * Ns;
       c128* Tsp = md->Tb + toff;
+      c128* Ttsp = md->Ttb + toff;
       toff += long(md->wchunk) * nd * nsq;
       c128* Gcsp = md->Gcb + long(md->wchunk) * nd * h0->el_off[sp] * M;
-      scale_blocks_kernel<<<ceil_div(nsq * nb, 256), 256, 0, s>>>(Tsp, nsq, nb, md->wdd);
-      AFQMC_TRY(launch_status("scale_blocks_kernel"));
-      // Gc[w][d] = (wdd T^{-1})^T S_w^T  [N_s x M]  (the determinant's compact G, weighted)
+      weight_transpose_blocks_kernel<<<ceil_div(nsq * nb, 256), 256, 0, s>>>(Tsp, Ttsp, Ns, nb,
+                                                                            md->wdd);
+      AFQMC_TRY(launch_status("weight_transpose_blocks_kernel"));
+      // Gc[w] = [wdd_d (T_d^{-1})^T]_d S_w^T  [nd N_s x M]  (every determinant's compact G,
+      // weighted; one product per walker)
       GemmParams p{};
-      p.m = Ns; p.n = int(M); p.k = Ns;
-      p.A = Tsp; p.lda = Ns; p.strideA = nsq;
-      p.B = S0 + ws->offS(sp); p.ldb = Ns; p.strideB = ws->walker_size; p.bdiv = nd;
-      p.C = Gcsp; p.ldc = M; p.strideC = long(Ns) * M;
+      p.m = nd * Ns; p.n = int(M); p.k = Ns;
+      p.A = Ttsp; p.lda = Ns; p.strideA = long(nd) * nsq;
+      p.B = S0 + ws->offS(sp); p.ldb = Ns; p.strideB = ws->walker_size;
+      p.C = Gcsp; p.ldc = M; p.strideC = long(nd) * Ns * M;
       p.alpha = cmk(1, 0); p.beta = cmk(0, 0);
-      AFQMC_TRY(zgemm(s, int(nb), GT, false, GT, false, p));
+      AFQMC_TRY(zgemm(s, wc, GN, false, GT, false, p));
       // G[w][s] = PsiTall_s^T Gc[w]  (K = nd * N_s: the sum over determinants)
       GemmParams q{};
       q.m = int(M); q.n = int(M); q.k = nd * Ns;

@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(WM_WARPS* WN_WARPS * 32)
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
 
   const TA* Ag = reinterpret_cast<const TA*>(p.A) + b * p.strideA;
-  const TB* Bg = reinterpret_cast<const TB*>(p.B) + (p.bdiv > 1 ? b / p.bdiv : b) * p.strideB;
+  const TB* Bg = reinterpret_cast<const TB*>(p.B) + b * p.strideB;
 
   TA ra[K::A_PER_T];
   TB rb[K::B_PER_T];

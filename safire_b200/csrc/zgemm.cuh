@@ -22,7 +22,6 @@ struct GemmParams {
   c128 alpha, beta;
   c128* D; long ldd, strideD;  // optional second output (nullptr: none)
   bool d_store;                 // D = result (true) or D += result (false)
-  int bdiv;                     // problem b reads B at (b / bdiv) * strideB (0 or 1: b)
 };
 
 // op codes for the C++ launcher

@@ -108,7 +108,7 @@ def test_multidet_propagation_vs_oracle(cuda, wt, nup, ndn):
 @pytest.mark.parametrize("wt,nup,ndn", [(1, 2, 2), (2, 2, 2)])
 def test_multidet_batched_walker_chunks(cuda, wt, nup, ndn):
     """300 determinants: the batched step goes over the walkers in chunks of 65535 // 300 = 218
-    (the batched GEMM's grid limit), so 230 walkers take a full and a ragged chunk."""
+    (a bound on the batched launches' grids), so 230 walkers take a full and a ragged chunk."""
     from safire_b200 import afqmc as A
     M, Nc, W, nd = 8, 6, 230, 300
     h1, Likn = make_hamiltonian(M, Nc, 0.9, seed=5)
