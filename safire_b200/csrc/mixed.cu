@@ -37,6 +37,7 @@ enum Epi : int {
   EPI_VHS = 4,       // out planes [z=0][row][ (col/M)*ldv + col%M ] = split(alpha * acc)
   EPI_VHS_SYM = 5,   // symmetric L: tile nt = (i block, k block) of the upper triangle; out
                      // planes [row][i][k] and [row][k][i] = split(alpha * acc), alpha real
+  EPI_C64T = 6,      // out_c as complex64 [z][col][row] = alpha * col_inv[col] * acc
 };
 
 // Symmetric vHS tiles: the BN = 128 columns of a tile are the (i, k) pairs of an 8 x 16 block,
@@ -57,7 +58,7 @@ struct TcParams {
   float* acc_split[4];  // optional split copy of the updated running sum (last Taylor term)
   c128* out_c;
   long outc_ld, outc_bs;
-  int outc_f32;         // EPI_C128: out_c holds complex64 (float2) elements instead
+  const float* col_inv;  // EPI_C64T: per-column scale (the B operand's row scale)
   int vhs_M;            // EPI_VHS: columns are (i, k) pairs of an M x M matrix
   // FP16 operands: the accumulator row r is multiplied by row_inv[r] (the A operand's row scale;
   // the B operand's scale is folded into alpha) before the epilogue uses it
@@ -431,11 +432,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_cgemm_kernel(const __grid_co
           if constexpr (EPI == EPI_C128 || EPI == EPI_S64) {
             const double dr = p.alpha.x * double(vr[j]) - p.alpha.y * double(vi[j]);
             const double di = p.alpha.x * double(vi[j]) + p.alpha.y * double(vr[j]);
-            const long idx = long(z) * p.outc_bs + long(row) * p.outc_ld + col;
-            if (EPI == EPI_C128 && p.outc_f32)
-              reinterpret_cast<float2*>(p.out_c)[idx] = make_float2(float(dr), float(di));
-            else
-              p.out_c[idx] = cmk(dr, di);
+            p.out_c[long(z) * p.outc_bs + long(row) * p.outc_ld + col] = cmk(dr, di);
+          } else if constexpr (EPI == EPI_C64T) {
+            // lanes hold consecutive rows: consecutive addresses of the transposed output
+            const float f = p.col_inv ? p.col_inv[col] : 1.f;
+            reinterpret_cast<float2*>(p.out_c)[long(z) * p.outc_bs + long(col) * p.outc_ld + row] =
+                make_float2(xr * f, xi * f);
           } else if constexpr (EPI == EPI_PLANES) {
             const long idx = long(z) * p.out_bs + long(row) * p.out_ld + col;
             split_store(xr, p.out[0], p.out[1], idx);
@@ -1806,6 +1808,27 @@ int tcgemm_rb_run(cudaStream_t s, TcGemmRB* g, const c128* A, long lda, int rows
     g->a_cap = rows_a;
   }
   AFQMC_TRY(split_rows_f16(s, A, lda, rows_a, int(K), g->A, g->a_inv));
+  if (c64_out) {
+    // C^T = B A^T with B (real) as the MMA's A operand: the accumulator rows are C's columns,
+    // so the epilogue's lanes write consecutive complex64 elements of C
+    TcParams p{};
+    for (int q = 0; q < 2; ++q)
+      AFQMC_TRY(make_map_es(&p.a[q], g->B, q, 0, K, g->B.rows, g->B.ld, 1, g->B.bstride(), 128));
+    for (int q = 0; q < 4; ++q)
+      AFQMC_TRY(make_map_es(&p.b[q], g->A, q, 0, K, rows_a, g->A.ld, 1, long(rows_a) * g->A.ld,
+                            128));
+    p.m = int(g->B.rows);
+    p.n = rows_a;
+    p.k = int(K);
+    p.order = 1;  // a tile of B's rows stays in L2 while the tiles of A's rows stream past it
+    p.alpha = cmk(double(g->b_inv), 0);
+    p.col_inv = g->a_inv;
+    p.out_c = C;
+    p.outc_ld = ldc;
+    p.outc_bs = 0;
+    p.err = g->err;
+    return launch_tc<false, true, 128, 2, EPI_C64T, true>(s, p, 1);
+  }
   TcParams p{};
   for (int q = 0; q < 4; ++q)
     AFQMC_TRY(make_map_es(&p.a[q], g->A, q, 0, K, rows_a, g->A.ld, 1, long(rows_a) * g->A.ld,
@@ -1821,7 +1844,6 @@ int tcgemm_rb_run(cudaStream_t s, TcGemmRB* g, const c128* A, long lda, int rows
   p.out_c = C;
   p.outc_ld = ldc;
   p.outc_bs = 0;
-  p.outc_f32 = c64_out ? 1 : 0;
   p.err = g->err;
   return launch_tc<true, false, 128, 2, EPI_C128, true>(s, p, 1);
 }

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <type_traits>
 #include <memory>
 #include <vector>
 
@@ -55,6 +56,15 @@ template <> __device__ __forceinline__ c64 to_cx<c64>(c128 x) {
 template <typename C> __device__ __forceinline__ C to_cx(c64 x);
 template <> __device__ __forceinline__ c128 to_cx<c128>(c64 x) {
   return cmk(double(x.x), double(x.y));
+}
+// o += v, component-wise atomics in o's precision
+__device__ __forceinline__ void atomic_add_cx(c128* o, c128 v) {
+  atomicAdd(&o->x, v.x);
+  atomicAdd(&o->y, v.y);
+}
+__device__ __forceinline__ void atomic_add_cx(c64* o, c128 v) {
+  atomicAdd(&o->x, float(v.x));
+  atomicAdd(&o->y, float(v.y));
 }
 
 __device__ __forceinline__ c128 dot_row(const c128* __restrict__ t, const c128* __restrict__ r,
@@ -703,8 +713,8 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
     const int4* __restrict__ uhdr, const int* __restrict__ uexc4,
     const typename CxOf<R>::T* __restrict__ INVc, int ninv,
     const c128* __restrict__ wgt, int nuniq, int W, int nel, int nact, int nchol, int nbuf,
-    c128* __restrict__ EXacc, c128* __restrict__ EJacc, c128* __restrict__ KE,
-    const c128* __restrict__ cross, c128* __restrict__ E, c128* __restrict__ Kref,
+    c128* __restrict__ EXacc, c128* __restrict__ EJacc, TW* __restrict__ KE,
+    const TW* __restrict__ cross, c128* __restrict__ E, TW* __restrict__ Kref,
     c128* __restrict__ REF) {
   using C = typename CxOf<R>::T;
   constexpr bool ASYNC = sizeof(TW) == sizeof(C);
@@ -785,7 +795,7 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
     f00[g] = cmul(f0, f0);
     block_sum3(ex0, z1, z2, red);  // ends with a barrier: SU is complete, Tn free after it
     if (threadIdx.x == 0 && Kref) {
-      Kref[size_t(w) * nchol + n] = f0;
+      Kref[size_t(w) * nchol + n] = to_cx<TW>(f0);
       atomicAdd(&REF[2 * w].x, ex0.x);
       atomicAdd(&REF[2 * w].y, ex0.y);
       atomicAdd(&REF[2 * w + 1].x, f00[g].x);
@@ -821,9 +831,9 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
       exu = cadd(exu, to_cx<c128>(exw[g]));
       eju = cadd(eju, csub(cmul(kn, kn), f00[g]));
       if (cross)
-        ejc = cadd(ejc, cmul(cross[o + g], kn));
+        ejc = cadd(ejc, cmul(to_cx<c128>(cross[o + g]), kn));
       else
-        KE[o + g] = kn;
+        KE[o + g] = to_cx<TW>(kn);
     }
     exs = cadd(exs, cmul(wu, exu));
     ejs = cadd(ejs, cmul(wu, eju));
@@ -863,12 +873,14 @@ __global__ void reference_from_tables_kernel(const c128* __restrict__ Swia,
 // determinants, such as the reference down-spin excitation, would otherwise serialise one CTA);
 // segment g = (d, j0, j1).  A row of one segment stores its result, longer rows add into KEd,
 // which is zeroed first.
+// KT: the element type of the K vectors (complex64 in the mixed energy's tables path).
 constexpr int KE_SEG = 16;
+template <typename KT>
 __global__ void couple_ke_kernel(const int* __restrict__ seg, const int* __restrict__ kidx,
                                  const int* __restrict__ det_up, const c128* __restrict__ coef,
-                                 const c128* __restrict__ KEr, const c128* __restrict__ ov_up,
+                                 const KT* __restrict__ KEr, const c128* __restrict__ ov_up,
                                  int nu_up, const c128* __restrict__ ov_dn, int nu_dn, int W,
-                                 int nchol, c128* __restrict__ KEd) {
+                                 int nchol, KT* __restrict__ KEd) {
   __shared__ c128 f[KE_SEG];
   __shared__ int uu[KE_SEG];
   const int g = blockIdx.x, w = blockIdx.y;
@@ -883,20 +895,19 @@ __global__ void couple_ke_kernel(const int* __restrict__ seg, const int* __restr
   for (int n = threadIdx.x; n < nchol; n += blockDim.x) {
     c128 acc = cmk(0, 0);
     for (int j = 0; j < j1 - j0; ++j)
-      acc = cadd(acc, cmul(f[j], KEr[(size_t(uu[j]) * W + w) * nchol + n]));
-    c128* o = KEd + (size_t(d) * W + w) * nchol + n;
-    if (single) {
-      *o = acc;
-    } else {
-      atomicAdd(&o->x, acc.x);
-      atomicAdd(&o->y, acc.y);
-    }
+      acc = cadd(acc, cmul(f[j], to_cx<c128>(KEr[(size_t(uu[j]) * W + w) * nchol + n])));
+    KT* o = KEd + (size_t(d) * W + w) * nchol + n;
+    if (single)
+      *o = to_cx<KT>(acc);
+    else
+      atomic_add_cx(o, acc);
   }
 }
 
 // E[w][2] += sum_{d, n} A[d][w][n] B[d][w][n]  (the cross-spin Coulomb products)
-__global__ void __launch_bounds__(PH_THREADS) cross_ej_kernel(const c128* __restrict__ A,
-                                                              const c128* __restrict__ B, int nd,
+template <typename KT>
+__global__ void __launch_bounds__(PH_THREADS) cross_ej_kernel(const KT* __restrict__ A,
+                                                              const KT* __restrict__ B, int nd,
                                                               int W, int nchol,
                                                               c128* __restrict__ E) {
   __shared__ double red[PH_THREADS / 32 * 6];
@@ -905,7 +916,7 @@ __global__ void __launch_bounds__(PH_THREADS) cross_ej_kernel(const c128* __rest
   for (long k = threadIdx.x; k < long(nd) * nchol; k += blockDim.x) {
     const int d = int(k / nchol), n = int(k - long(d) * nchol);
     const size_t o = (size_t(d) * W + w) * nchol + n;
-    s = cadd(s, cmul(A[o], B[o]));
+    s = cadd(s, cmul(to_cx<c128>(A[o]), to_cx<c128>(B[o])));
   }
   block_sum3(s, z1, z2, red);
   if (threadIdx.x == 0) E[w * 3 + 2] = cadd(E[w * 3 + 2], s);
@@ -1167,6 +1178,8 @@ struct afqmc_phmsd_s {
   int4* uhdr[2] = {nullptr, nullptr};
   // Twina holds complex64 elements (the mixed tensor-core half rotation feeding the tables)
   bool twina64[2] = {false, false};
+  // the K vectors KEr, KEd, Kdn hold complex64 (the mixed tables path on both spins)
+  bool ke64 = false;
   // energy: the Hamiltonian half-rotated with the active orbitals
   bool has_ham = false;
   int Nc = 0;
@@ -1730,6 +1743,18 @@ bool phmsd_tables(afqmc_phmsd h, int sp) {
   return h->tables_ok[sp] && excited_tables_smem(h, sp, esz, 1, 1) <= 200 * 1024;
 }
 
+// the FP16 split planes of Lnak for the mixed half rotation, made at the first mixed energy
+// (state 1 ready, -1 Lnak complex or K not a multiple of 8: the complex128 GEMM runs)
+int phmsd_tc_prepare(afqmc_phmsd h, cudaStream_t s, int sp) {
+  if (h->tc_lnak_state[sp] != 0) return AFQMC_OK;
+  AFQMC_CUDA_TRY(cudaStreamSynchronize(s));
+  const int st = tcgemm_rb_create(&h->tc_lnak[sp], h->lnak[sp], long(h->Nc) * h->nact[sp],
+                                  h->M, h->M);
+  if (st != AFQMC_OK && st != AFQMC_ERR_UNSUPPORTED) return st;
+  h->tc_lnak_state[sp] = st == AFQMC_OK ? 1 : -1;
+  return AFQMC_OK;
+}
+
 int phmsd_half_rotated(afqmc_phmsd h, cudaStream_t s, int sp, int nb) {
   const int N = h->nel[sp], na = h->nact[sp];
   GemmParams p{};
@@ -1741,16 +1766,10 @@ int phmsd_half_rotated(afqmc_phmsd h, cudaStream_t s, int sp, int nb) {
   AFQMC_TRY(zgemm(s, 1, GN, false, GT, false, p));
   if (h->precision == AFQMC_PREC_MIXED) {
     // mixed precision: the FP16 split on the tensor cores when Lnak is real
-    if (h->tc_lnak_state[sp] == 0) {
-      AFQMC_CUDA_TRY(cudaStreamSynchronize(s));
-      const int st = tcgemm_rb_create(&h->tc_lnak[sp], h->lnak[sp], long(h->Nc) * na, h->M,
-                                      h->M);
-      if (st != AFQMC_OK && st != AFQMC_ERR_UNSUPPORTED) return st;
-      h->tc_lnak_state[sp] = st == AFQMC_OK ? 1 : -1;
-    }
+    AFQMC_TRY(phmsd_tc_prepare(h, s, sp));
     if (h->tc_lnak_state[sp] == 1) {
-      // complex64 output where only the tables kernel reads it
-      h->twina64[sp] = phmsd_tables(h, sp);
+      // complex64 output where only the tables kernels read it (both spins, h->ke64)
+      h->twina64[sp] = h->ke64;
       return tcgemm_rb_run(s, h->tc_lnak[sp], h->eG[sp], h->M, nb * N, h->Twina,
                            long(h->Nc) * na, h->twina64[sp]);
     }
@@ -1806,8 +1825,8 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
                                                           h->el + 2 * nb, KE);
     AFQMC_TRY(launch_status("ph_excited_2body_kernel"));
     if (cross) {
-      cross_ej_kernel<<<nb, PH_THREADS, 0, s>>>(cross + size_t(k0) * nb * Nc, h->KEl, nd, nb, Nc,
-                                                E);
+      cross_ej_kernel<c128><<<nb, PH_THREADS, 0, s>>>(cross + size_t(k0) * nb * Nc, h->KEl, nd,
+                                                      nb, Nc, E);
       AFQMC_TRY(launch_status("cross_ej_kernel"));
     }
   }
@@ -1837,13 +1856,16 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
     if (excited_tables_smem(h, sp, esz, 4, nbuf) > lim) ngr = nbuf = 1;
     const size_t smem = excited_tables_smem(h, sp, esz, ngr, nbuf);
     const dim3 grid((Nc + ngr - 1) / ngr, nb);
+    // the K vectors have Twina's element type (complex64 in the mixed energy's tables path)
     auto go = [&](auto kern, const auto* tw, const auto* inv) -> int {
+      using KT = std::remove_const_t<std::remove_pointer_t<decltype(tw)>>;
       AFQMC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(smem)));
       kern<<<grid, PHX_THREADS, smem, s>>>(
           tw, h->eQ[sp], h->refc[sp], h->hl[sp], h->vl[sp], h->nh[sp], h->nv[sp], h->uhdr[sp],
           h->uexc4[sp], inv, h->ninv[sp], h->wgt, h->nuniq[sp], nb, N, na, Nc, nbuf, h->el + nb,
-          h->el + 2 * nb, cross ? nullptr : KEout, cross, E, Kref, REF);
+          h->el + 2 * nb, cross ? nullptr : reinterpret_cast<KT*>(KEout),
+          reinterpret_cast<const KT*>(cross), E, reinterpret_cast<KT*>(Kref), REF);
       return AFQMC_OK;
     };
     const c64* inv32 = reinterpret_cast<const c64*>(h->INV32);
@@ -1892,6 +1914,14 @@ extern "C" int afqmc_phmsd_energy(afqmc_phmsd h, const afqmc_c128* wbuf, long ld
   c128* Eall = reinterpret_cast<c128*>(E_out);
   c128* Oall = reinterpret_cast<c128*>(ovlp);
   auto run = [&]() -> int {
+    // complex64 half-rotated rows and K vectors when both spins run the mixed tables kernels
+    h->ke64 = false;
+    if (h->precision == AFQMC_PREC_MIXED && phmsd_tables(h, 0) && phmsd_tables(h, 1)) {
+      AFQMC_TRY(phmsd_tc_prepare(h, s, 0));
+      AFQMC_TRY(phmsd_tc_prepare(h, s, 1));
+      h->ke64 = h->tc_lnak_state[0] == 1 && h->tc_lnak_state[1] == 1;
+    }
+    const size_t kesz = h->ke64 ? sizeof(c64) : sizeof(c128);
     for (int w0 = 0; w0 < W; w0 += Wb) {
       const int nb = (W - w0 < Wb) ? W - w0 : Wb;
       const c128* Sb = S + long(w0) * ldS;
@@ -1918,17 +1948,28 @@ extern "C" int afqmc_phmsd_energy(afqmc_phmsd h, const afqmc_c128* wbuf, long ld
       // K vectors coupled to the down-spin excitations (PHMSD.cpp:472-494)
       {
         if (h->kseg_split)
-          AFQMC_CUDA_TRY(cudaMemsetAsync(h->KEd, 0, sizeof(c128) * size_t(nu1) * nb * Nc, s));
+          AFQMC_CUDA_TRY(cudaMemsetAsync(h->KEd, 0, kesz * size_t(nu1) * nb * Nc, s));
         dim3 grid(h->nkseg, nb);
-        couple_ke_kernel<<<grid, 128, 0, s>>>(h->kseg, h->kidx[1], h->det[0], h->coef, h->KEr,
-                                              h->eov[0], nu0, h->eov[1], nu1, nb, Nc, h->KEd);
+        if (h->ke64)
+          couple_ke_kernel<c64><<<grid, 128, 0, s>>>(
+              h->kseg, h->kidx[1], h->det[0], h->coef, reinterpret_cast<const c64*>(h->KEr),
+              h->eov[0], nu0, h->eov[1], nu1, nb, Nc, reinterpret_cast<c64*>(h->KEd));
+        else
+          couple_ke_kernel<c128><<<grid, 128, 0, s>>>(h->kseg, h->kidx[1], h->det[0], h->coef,
+                                                      h->KEr, h->eov[0], nu0, h->eov[1], nu1, nb,
+                                                      Nc, h->KEd);
         AFQMC_TRY(launch_status("couple_ke_kernel"));
       }
       // spin down (PHMSD.cpp:497-531)
       AFQMC_TRY(couple(1, h->eov[0], nu0, h->eov[1]));
       AFQMC_TRY(phmsd_half_rotated(h, s, 1, nb));
       AFQMC_TRY(phmsd_reference_and_excited(h, s, 1, nb, 0.0, h->Kdn, nullptr, h->KEd, E));
-      cross_ej_kernel<<<nb, PH_THREADS, 0, s>>>(h->KEd, h->Kdn, 1, nb, Nc, E);
+      if (h->ke64)
+        cross_ej_kernel<c64><<<nb, PH_THREADS, 0, s>>>(reinterpret_cast<const c64*>(h->KEd),
+                                                       reinterpret_cast<const c64*>(h->Kdn), 1,
+                                                       nb, Nc, E);
+      else
+        cross_ej_kernel<c128><<<nb, PH_THREADS, 0, s>>>(h->KEd, h->Kdn, 1, nb, Nc, E);
       AFQMC_TRY(launch_status("cross_ej_kernel"));
       finish_energy_kernel<<<(nb + 127) / 128, 128, 0, s>>>(h->eOv, h->elogov, nb, E,
                                                             Oall + w0);
