@@ -473,7 +473,8 @@ __global__ void woodbury_inverses_kernel(const c128* __restrict__ QQ0, const int
                                          const int* __restrict__ uexc,
                                          const int* __restrict__ uinv, int nuniq, int W, int nact,
                                          int nel, int ninv, c128* __restrict__ INV,
-                                         float2* __restrict__ INV32) {
+                                         float2* __restrict__ INV32,
+                                         const int4* __restrict__ uhdrs) {
   const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= long(nuniq - 1) * W) return;
   const int w = int(t / (nuniq - 1)), u = 1 + int(t - long(w) * (nuniq - 1));
@@ -484,12 +485,13 @@ __global__ void woodbury_inverses_kernel(const c128* __restrict__ QQ0, const int
   c128* o = INV + size_t(w) * ninv + uinv[u];
   for (int p = 0; p < nex; ++p)
     for (int q = 0; q < nex; ++q) o[p * nex + q] = ok ? inv[p][q] : cmk(0.0, 0.0);
-  if (INV32) {
-    float2* o32 = INV32 + size_t(w) * ninv + uinv[u];
+  if (INV32) {  // structure-of-arrays within the shell: entry k at base + k cnt
+    const int4 hs = uhdrs[u];
+    float2* o32 = INV32 + size_t(w) * ninv + hs.z;
     for (int p = 0; p < nex; ++p)
       for (int q = 0; q < nex; ++q)
-        o32[p * nex + q] = ok ? make_float2(float(inv[p][q].x), float(inv[p][q].y))
-                              : make_float2(0.f, 0.f);
+        o32[size_t(p * nex + q) * hs.w] = ok ? make_float2(float(inv[p][q].x), float(inv[p][q].y))
+                                             : make_float2(0.f, 0.f);
   }
 }
 
@@ -569,19 +571,19 @@ __global__ void __launch_bounds__(PH_THREADS) excited_1body_all_kernel(
 // for the ng indices of the group: exg[g], kng[g].
 template <int NEX, int NG, typename C>
 __device__ __forceinline__ void excited_terms(const int* __restrict__ e4,
-                                              const C* __restrict__ Qg, const C* Sf,
+                                              const C* __restrict__ Qg, int es, const C* Sf,
                                               const C* SU, int nv, int sfs, int sus, int ng,
                                               const C* f0, C* exg, C* kng) {
   using R = decltype(f0[0].x);
   C Qi[NEX * NEX];  // the determinant's Woodbury inverse, in the working precision
 #pragma unroll
-  for (int k = 0; k < NEX * NEX; ++k) Qi[k] = Qg[k];
+  for (int k = 0; k < NEX * NEX; ++k) Qi[k] = Qg[k * es];
   int so[NEX], uo[NEX], pc[NEX];
 #pragma unroll
   for (int a = 0; a < NEX; ++a) {
-    so[a] = e4[a] * nv;
-    uo[a] = e4[2 * NEX + a] * nv;
-    pc[a] = e4[3 * NEX + a];
+    so[a] = e4[a * es] * nv;
+    uo[a] = e4[(2 * NEX + a) * es] * nv;
+    pc[a] = e4[(3 * NEX + a) * es];
   }
 #pragma unroll
   for (int g = 0; g < NG; ++g) {
@@ -621,20 +623,22 @@ __device__ __forceinline__ void excited_terms(const int* __restrict__ e4,
 
 // nex > 4 is rare: out of line, so that its larger frame stays out of the common path
 template <int NEX, int NG, typename C>
-__device__ __noinline__ void excited_terms_rare(const int* e4, const C* Qi, const C* Sf,
+__device__ __noinline__ void excited_terms_rare(const int* e4, const C* Qi, int es, const C* Sf,
                                                 const C* SU, int nv, int sfs, int sus, int ng,
                                                 const C* f0, C* exg, C* kng) {
-  excited_terms<NEX, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0, exg, kng);
+  excited_terms<NEX, NG, C>(e4, Qi, es, Sf, SU, nv, sfs, sus, ng, f0, exg, kng);
 }
 
 // One product of the tables: out[k][c] = sum_j a[r_k][sel_j] b[j][c] over the rows k < nrows
 // (r_k = rows[k], or k when rows is null), c < ncol.  A thread owns RT rows and the columns
 // t and t + half (half = ceil(ncol / 2)) of them, so that every shared-memory read of a feeds
 // two products and every read of b feeds RT; neighbouring threads read neighbouring columns of b.
+// With sub: out[k][c] = sub[k][subcols_c] - (the product) instead.
 template <int RT, typename C>
 __device__ __forceinline__ void table_product(const C* a, int lda, const int* rows, int nrows,
                                               const int* sel, int nsum, const C* b, int ldb,
-                                              int ncol, C* out, int ldo) {
+                                              int ncol, C* out, int ldo, const C* sub = nullptr,
+                                              int ldsub = 0, const int* subcols = nullptr) {
   const int half = (ncol + 1) / 2;
   const int nrt = (nrows + RT - 1) / RT;
   for (int t = threadIdx.x; t < nrt * half; t += blockDim.x) {
@@ -664,6 +668,10 @@ __device__ __forceinline__ void table_product(const C* a, int lda, const int* ro
     for (int r = 0; r < RT; ++r) {
       const int k = rt * RT + r;
       if (k >= nrows) break;
+      if (sub) {
+        acc0[r] = csub(sub[k * ldsub + subcols[ct]], acc0[r]);
+        if (two) acc1[r] = csub(sub[k * ldsub + subcols[ct + half]], acc1[r]);
+      }
       out[k * ldo + ct] = acc0[r];
       if (two) out[k * ldo + ct + half] = acc1[r];
     }
@@ -705,7 +713,9 @@ __device__ __forceinline__ void cp_async_wait() {
 // TW: the element type of Twina (complex128, or complex64 from the mixed half rotation).  When
 // it is the working type C the rows t_j come in by asynchronous copies, the next index's while
 // the current one's tables are built (nbuf = 2), else by converting loads.  INVc holds the
-// Woodbury inverses in the working type; uhdr[u] = {nex, uoff4, uinv, 0}.
+// Woodbury inverses in the working type; uhdr[u] = {nex, base of u in uexc4, base of u in INVc,
+// stride es}: field entry k of excitation u at base + k es (es = 1: one excitation's entries
+// together; es = the shell's size: structure-of-arrays, consecutive excitations adjacent).
 template <typename R, int NG, typename TW>
 __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_energy_tables_kernel(
     const TW* __restrict__ Twina, const c128* __restrict__ QQ0, const int* __restrict__ refc,
@@ -755,6 +765,7 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
   for (int c = threadIdx.x; c < nv; c += blockDim.x) vls[c] = vl[c];
   C f0w[NG];
   c128 f00[NG];
+  c128 ex0 = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0), f00s = cmk(0, 0);
 #pragma unroll
   for (int g = 0; g < NG; ++g) {
     f0w[g] = czero<C>();
@@ -771,20 +782,14 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
       if constexpr (ASYNC) cp_async_wait<0>();
     }
     __syncthreads();
-    // Y = t[:, r] Qv (into Sf)
-    table_product<3, C>(Tn, nact, nullptr, nel, refs, nel, Qv, nv, nv, Sg, nv);
-    // the reference determinant: f0 = sum_i t_i[r_i], ex0 = sum_ij t_i[r_j] t_j[r_i]
-    c128 ex0 = cmk(0, 0), z1 = cmk(0, 0), z2 = cmk(0, 0);
+    // Sf = t[:, v] - t[:, r] Qv
+    table_product<3, C>(Tn, nact, nullptr, nel, refs, nel, Qv, nv, nv, Sg, nv, Tn, nact, vls);
+    // the reference determinant: f0 = sum_i t_i[r_i], ex0 = sum_ij t_i[r_j] t_j[r_i] (summed
+    // over the group's indices, reduced over the block after the loop)
     for (int k = threadIdx.x; k < nel * nel; k += blockDim.x) {
       const int i = k / nel, j = k - i * nel;
       ex0 = cadd(ex0,
                  cmul(to_cx<c128>(Tn[i * nact + refs[j]]), to_cx<c128>(Tn[j * nact + refs[i]])));
-    }
-    __syncthreads();
-    // Sf = t[:, v] - Y
-    for (int k = threadIdx.x; k < nel * nv; k += blockDim.x) {
-      const int j = k / nv, c = k - j * nv;
-      Sg[k] = csub(Tn[j * nact + vls[c]], Sg[k]);
     }
     __syncthreads();
     // SU = t[hole rows, r] Sf
@@ -793,15 +798,19 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
     for (int i = 0; i < nel; ++i) f0 = cadd(f0, to_cx<c128>(Tn[i * nact + refs[i]]));
     f0w[g] = to_cx<C>(f0);
     f00[g] = cmul(f0, f0);
-    block_sum3(ex0, z1, z2, red);  // ends with a barrier: SU is complete, Tn free after it
     if (threadIdx.x == 0 && Kref) {
       Kref[size_t(w) * nchol + n] = to_cx<TW>(f0);
-      atomicAdd(&REF[2 * w].x, ex0.x);
-      atomicAdd(&REF[2 * w].y, ex0.y);
-      atomicAdd(&REF[2 * w + 1].x, f00[g].x);
-      atomicAdd(&REF[2 * w + 1].y, f00[g].y);
+      f00s = cadd(f00s, f00[g]);
     }
+    __syncthreads();  // SU complete; Tn free for the next index's rows
     if (nbuf == 1 && g + 1 < ng) load_t(g + 1, Tb0);
+  }
+  block_sum3(ex0, z1, z2, red);
+  if (threadIdx.x == 0 && Kref) {
+    atomicAdd(&REF[2 * w].x, ex0.x);
+    atomicAdd(&REF[2 * w].y, ex0.y);
+    atomicAdd(&REF[2 * w + 1].x, f00s.x);
+    atomicAdd(&REF[2 * w + 1].y, f00s.y);
   }
   __syncthreads();
   c128 exs = cmk(0, 0), ejs = cmk(0, 0), ejc = cmk(0, 0);
@@ -813,14 +822,14 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
     const C* Qi = Iw + hd.z;
     C exw[NG], knw[NG];
     switch (hd.x) {
-      case 1: excited_terms<1, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
-      case 2: excited_terms<2, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
-      case 3: excited_terms<3, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
-      case 4: excited_terms<4, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
-      case 5: excited_terms_rare<5, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
-      case 6: excited_terms_rare<6, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
-      case 7: excited_terms_rare<7, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
-      default: excited_terms_rare<8, NG, C>(e4, Qi, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      case 1: excited_terms<1, NG, C>(e4, Qi, hd.w, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      case 2: excited_terms<2, NG, C>(e4, Qi, hd.w, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      case 3: excited_terms<3, NG, C>(e4, Qi, hd.w, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      case 4: excited_terms<4, NG, C>(e4, Qi, hd.w, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      case 5: excited_terms_rare<5, NG, C>(e4, Qi, hd.w, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      case 6: excited_terms_rare<6, NG, C>(e4, Qi, hd.w, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      case 7: excited_terms_rare<7, NG, C>(e4, Qi, hd.w, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
+      default: excited_terms_rare<8, NG, C>(e4, Qi, hd.w, Sf, SU, nv, sfs, sus, ng, f0w, exw, knw); break;
     }
     c128 exu = cmk(0, 0), eju = cmk(0, 0);
     const size_t o = (size_t(u) * W + w) * nchol + n0;
@@ -1176,6 +1185,13 @@ struct afqmc_phmsd_s {
   c128* INV32 = nullptr;
   // per unique excitation {nex, uoff4, uinv, 0} (one load in the energy tables kernel)
   int4* uhdr[2] = {nullptr, nullptr};
+  // the tables kernel's view: within each run of equal nex (a shell of cnt excitations), the
+  // fields of uexc4 and the entries of the complex64 inverses INV32 are stored structure-of-
+  // arrays (element k of excitation u at base + k cnt + (u - u0)), so that the threads of a
+  // warp, which take consecutive excitations, read consecutive addresses; uhdrs[u] = {nex,
+  // uexc4s base of u, INV32 base of u, cnt}
+  int4* uhdrs[2] = {nullptr, nullptr};
+  int* uexc4s[2] = {nullptr, nullptr};
   // Twina holds complex64 elements (the mixed tensor-core half rotation feeding the tables)
   bool twina64[2] = {false, false};
   // the K vectors KEr, KEd, Kdn hold complex64 (the mixed tables path on both spins)
@@ -1244,6 +1260,8 @@ struct afqmc_phmsd_s {
       cudaFree(uexc4[s]);
       cudaFree(uoff4[s]);
       cudaFree(uhdr[s]);
+      cudaFree(uhdrs[s]);
+      cudaFree(uexc4s[s]);
       cudaFree(lnak[s]);
       cudaFree(haj[s]);
       cudaFree(orbmat[s]);
@@ -1473,8 +1491,25 @@ extern "C" int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact
     AFQMC_TRY(to_device(&h->uexc4[s], e4.data(), e4.size()));
     AFQMC_TRY(to_device(&h->uoff4[s], o4.data(), o4.size()));
     std::vector<int4> hd(nuniq[s], make_int4(0, 0, 0, 0));
-    for (int u = 1; u < nuniq[s]; ++u) hd[u] = make_int4(nex[s][u], o4[u], io[u], 0);
+    for (int u = 1; u < nuniq[s]; ++u) hd[u] = make_int4(nex[s][u], o4[u], io[u], 1);
     AFQMC_TRY(to_device(&h->uhdr[s], hd.data(), hd.size()));
+    // structure-of-arrays copies per shell (runs of equal nex, nex non-decreasing in u)
+    std::vector<int4> hs(nuniq[s], make_int4(0, 0, 0, 1));
+    std::vector<int> e4s(e4.size() > 0 ? e4.size() : 1, 0);
+    for (int u0 = 1; u0 < nuniq[s];) {
+      const int n = nex[s][u0];
+      int cnt = 0;
+      while (u0 + cnt < nuniq[s] && nex[s][u0 + cnt] == n) ++cnt;
+      const int ebase = o4[u0], qbase = io[u0];
+      for (int t = 0; t < cnt; ++t) {
+        const int u = u0 + t;
+        hs[u] = make_int4(n, ebase + t, qbase + t, cnt);
+        for (int f = 0; f < 4 * n; ++f) e4s[size_t(ebase) + size_t(f) * cnt + t] = e4[o4[u] + f];
+      }
+      u0 += cnt;
+    }
+    AFQMC_TRY(to_device(&h->uhdrs[s], hs.data(), hs.size()));
+    AFQMC_TRY(to_device(&h->uexc4s[s], e4s.data(), e4s.size()));
   }
   *out = h.release();
   return AFQMC_OK;
@@ -1835,7 +1870,8 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
       const long nt = long(h->nuniq[sp] - 1) * nb;
       woodbury_inverses_kernel<<<unsigned((nt + 127) / 128), 128, 0, s>>>(
           h->eQ[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp], h->nuniq[sp], nb, na, N,
-          h->ninv[sp], h->INV, mixed ? reinterpret_cast<float2*>(h->INV32) : nullptr);
+          h->ninv[sp], h->INV, mixed ? reinterpret_cast<float2*>(h->INV32) : nullptr,
+          h->uhdrs[sp]);
       AFQMC_TRY(launch_status("woodbury_inverses_kernel"));
       const size_t sm1 = size_t(N) * h->nv[sp] * sizeof(c128);
       AFQMC_CUDA_TRY(cudaFuncSetAttribute(excited_1body_all_kernel,
@@ -1862,8 +1898,9 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
       AFQMC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(smem)));
       kern<<<grid, PHX_THREADS, smem, s>>>(
-          tw, h->eQ[sp], h->refc[sp], h->hl[sp], h->vl[sp], h->nh[sp], h->nv[sp], h->uhdr[sp],
-          h->uexc4[sp], inv, h->ninv[sp], h->wgt, h->nuniq[sp], nb, N, na, Nc, nbuf, h->el + nb,
+          tw, h->eQ[sp], h->refc[sp], h->hl[sp], h->vl[sp], h->nh[sp], h->nv[sp],
+          mixed ? h->uhdrs[sp] : h->uhdr[sp], mixed ? h->uexc4s[sp] : h->uexc4[sp], inv,
+          h->ninv[sp], h->wgt, h->nuniq[sp], nb, N, na, Nc, nbuf, h->el + nb,
           h->el + 2 * nb, cross ? nullptr : reinterpret_cast<KT*>(KEout),
           reinterpret_cast<const KT*>(cross), E, reinterpret_cast<KT*>(Kref), REF);
       return AFQMC_OK;
@@ -2037,7 +2074,7 @@ extern "C" int afqmc_phmsd_density_matrix(afqmc_phmsd h, const afqmc_c128* wbuf,
           const long ni = long(nu - 1) * nb;
           woodbury_inverses_kernel<<<unsigned((ni + 127) / 128), 128, 0, s>>>(
               h->eQ[sp], h->uoff[sp], h->unex[sp], h->uexc[sp], h->uinv[sp], nu, nb, na, N,
-              h->ninv[sp], h->INV, nullptr);
+              h->ninv[sp], h->INV, nullptr, nullptr);
           AFQMC_TRY(launch_status("woodbury_inverses_kernel"));
         }
         const size_t rsm = 3 * size_t(N) * na * sizeof(c128);
