@@ -341,6 +341,15 @@ __global__ void couple_kernel(const int* __restrict__ rowptr, const int* __restr
   }
 }
 
+// out[w][u] = in[u][w]  (nu x W)
+__global__ void transpose_uw_kernel(const c128* __restrict__ in, int nu, int W,
+                                    c128* __restrict__ out) {
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= long(nu) * W) return;
+  const int w = int(t / nu), u = int(t - long(w) * nu);
+  out[t] = in[size_t(u) * W + w];
+}
+
 // Ov[w] = sum_u wgt[u][w] ov[w][u]   (before the weights are scaled by the overlaps)
 __global__ void __launch_bounds__(PH_THREADS) total_overlap_kernel(
     const c128* __restrict__ wgt, const c128* __restrict__ ov, int nu, int W,
@@ -722,7 +731,7 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
     const int* __restrict__ hl, const int* __restrict__ vl, int nh, int nv,
     const int4* __restrict__ uhdr, const int* __restrict__ uexc4,
     const typename CxOf<R>::T* __restrict__ INVc, int ninv,
-    const c128* __restrict__ wgt, int nuniq, int W, int nel, int nact, int nchol, int nbuf,
+    const c128* __restrict__ wgtT, int nuniq, int W, int nel, int nact, int nchol, int nbuf,
     c128* __restrict__ EXacc, c128* __restrict__ EJacc, TW* __restrict__ KE,
     const TW* __restrict__ cross, c128* __restrict__ E, TW* __restrict__ Kref,
     c128* __restrict__ REF) {
@@ -815,9 +824,10 @@ __global__ void __launch_bounds__(PHX_THREADS, sizeof(R) == 4 ? 2 : 1) excited_e
   __syncthreads();
   c128 exs = cmk(0, 0), ejs = cmk(0, 0), ejc = cmk(0, 0);
   const C* Iw = INVc + size_t(w) * ninv;
+  const c128* wgw = wgtT + size_t(w) * nuniq;  // this walker's weights, consecutive in u
   for (int u = 1 + threadIdx.x; u < nuniq; u += blockDim.x) {
     const int4 hd = uhdr[u];
-    const c128 wu = wgt[size_t(u) * W + w];
+    const c128 wu = wgw[u];
     const int* e4 = uexc4 + hd.y;
     const C* Qi = Iw + hd.z;
     C exw[NG], knw[NG];
@@ -911,6 +921,15 @@ __global__ void couple_ke_kernel(const int* __restrict__ seg, const int* __restr
     else
       atomic_add_cx(o, acc);
   }
+}
+
+// the KEd rows of the CSR rows split over several segments (krow) set to zero before their
+// segments add into them
+template <typename KT>
+__global__ void zero_k_rows_kernel(const int* __restrict__ krow, int W, int nchol,
+                                   KT* __restrict__ KEd) {
+  KT* o = KEd + (size_t(krow[blockIdx.x]) * W + blockIdx.y) * nchol;
+  for (int n = threadIdx.x; n < nchol; n += blockDim.x) o[n] = to_cx<KT>(cmk(0, 0));
 }
 
 // E[w][2] += sum_{d, n} A[d][w][n] B[d][w][n]  (the cross-spin Coulomb products)
@@ -1179,7 +1198,8 @@ struct afqmc_phmsd_s {
   // segments {d, j0, j1, single} of the down-spin CSR rows for couple_ke_kernel
   int* kseg = nullptr;
   int nkseg = 0;
-  bool kseg_split = false;
+  int* krow = nullptr;  // the CSR rows split over several segments (their KEd rows are zeroed)
+  int nkrow = 0;
   c128* INV = nullptr;
   // mixed precision: the same inverses in complex64 (float2, half the bytes of INV's buffer)
   c128* INV32 = nullptr;
@@ -1218,6 +1238,7 @@ struct afqmc_phmsd_s {
   c128 *eG[2] = {nullptr, nullptr}, *eQ[2] = {nullptr, nullptr}, *eov[2] = {nullptr, nullptr};
   c128 *eTMN = nullptr, *eTNN = nullptr, *elogov = nullptr, *eOv = nullptr;
   c128 *wgt = nullptr, *Swia = nullptr, *Twina = nullptr, *KEr = nullptr, *KEd = nullptr;
+  c128* wgtT = nullptr;  // wgt transposed, [w][u], for the tables kernel
   c128 *KEl = nullptr, *Kdn = nullptr, *R = nullptr, *el = nullptr;
   size_t R_elems = 0, KEl_elems = 0;
   int capCore = 0;  // walkers the Woodbury factors / density-matrix buffers hold
@@ -1231,7 +1252,7 @@ struct afqmc_phmsd_s {
   }
   void free_core_scratch() {
     for (c128** q : {&eG[0], &eG[1], &eQ[0], &eQ[1], &eov[0], &eov[1], &eTMN, &eTNN, &elogov,
-                     &eOv, &wgt, &Rfull, &INV, &INV32})
+                     &eOv, &wgt, &wgtT, &Rfull, &INV, &INV32})
       if (*q) {
         cudaFree(*q);
         *q = nullptr;
@@ -1273,6 +1294,7 @@ struct afqmc_phmsd_s {
     }
     cudaFree(coef);
     cudaFree(kseg);
+    cudaFree(krow);
   }
 };
 
@@ -1430,7 +1452,6 @@ extern "C" int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact
       std::vector<int> sg;
       for (int u = 0; u < nuniq[1]; ++u) {
         const bool single = rp[u + 1] - rp[u] <= KE_SEG;
-        h->kseg_split = h->kseg_split || !single;
         for (int j = rp[u]; j < rp[u + 1] || j == rp[u]; j += KE_SEG) {
           sg.insert(sg.end(), {u, j, std::min(j + KE_SEG, rp[u + 1]), single ? 1 : 0});
           if (rp[u + 1] == rp[u]) break;
@@ -1438,6 +1459,11 @@ extern "C" int afqmc_phmsd_create(int M, int nup, int ndn, int nact_up, int nact
       }
       h->nkseg = int(sg.size() / 4);
       AFQMC_TRY(to_device(&h->kseg, sg.data(), sg.size()));
+      std::vector<int> kr;
+      for (int u = 0; u < nuniq[1]; ++u)
+        if (rp[u + 1] - rp[u] > KE_SEG) kr.push_back(u);
+      h->nkrow = int(kr.size());
+      AFQMC_TRY(to_device(&h->krow, kr.data(), kr.size()));
     }
     // shells of equal excitation number
     for (int u = 1; u < nuniq[s]; ++u) {
@@ -1694,6 +1720,7 @@ int phmsd_core_scratch(afqmc_phmsd h, int Wb) {
   AFQMC_TRY(scratch_alloc(&h->elogov, Wb));
   AFQMC_TRY(scratch_alloc(&h->eOv, Wb));
   AFQMC_TRY(scratch_alloc(&h->wgt, nu * Wb));
+  AFQMC_TRY(scratch_alloc(&h->wgtT, nu * Wb));
   AFQMC_TRY(scratch_alloc(&h->Rfull, size_t(Wb) * ne * na));
   AFQMC_TRY(scratch_alloc(&h->INV, size_t(Wb) * std::max(h->ninv[0], h->ninv[1])));
   AFQMC_TRY(scratch_alloc(&h->INV32, (size_t(Wb) * std::max(h->ninv[0], h->ninv[1]) + 1) / 2));
@@ -1882,6 +1909,12 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
       AFQMC_TRY(launch_status("excited_1body_all_kernel"));
     }
     c128* REF = h->el + 3 * nb;  // [nb][2]: sum_n ex0, sum_n f0^2
+    {
+      const long nt = long(h->nuniq[sp]) * nb;
+      transpose_uw_kernel<<<unsigned((nt + 255) / 256), 256, 0, s>>>(h->wgt, h->nuniq[sp], nb,
+                                                                     h->wgtT);
+      AFQMC_TRY(launch_status("transpose_uw_kernel"));
+    }
     // four Cholesky indices per CTA where their tables fit (each determinant's Q, indices and
     // weight are then read once per four indices), the next index's rows loaded while the
     // current tables are built where a second row buffer fits
@@ -1900,7 +1933,7 @@ int phmsd_reference_and_excited(afqmc_phmsd h, cudaStream_t s, int sp, int nb, d
       kern<<<grid, PHX_THREADS, smem, s>>>(
           tw, h->eQ[sp], h->refc[sp], h->hl[sp], h->vl[sp], h->nh[sp], h->nv[sp],
           mixed ? h->uhdrs[sp] : h->uhdr[sp], mixed ? h->uexc4s[sp] : h->uexc4[sp], inv,
-          h->ninv[sp], h->wgt, h->nuniq[sp], nb, N, na, Nc, nbuf, h->el + nb,
+          h->ninv[sp], h->wgtT, h->nuniq[sp], nb, N, na, Nc, nbuf, h->el + nb,
           h->el + 2 * nb, cross ? nullptr : reinterpret_cast<KT*>(KEout),
           reinterpret_cast<const KT*>(cross), E, reinterpret_cast<KT*>(Kref), REF);
       return AFQMC_OK;
@@ -1958,7 +1991,6 @@ extern "C" int afqmc_phmsd_energy(afqmc_phmsd h, const afqmc_c128* wbuf, long ld
       AFQMC_TRY(phmsd_tc_prepare(h, s, 1));
       h->ke64 = h->tc_lnak_state[0] == 1 && h->tc_lnak_state[1] == 1;
     }
-    const size_t kesz = h->ke64 ? sizeof(c64) : sizeof(c128);
     for (int w0 = 0; w0 < W; w0 += Wb) {
       const int nb = (W - w0 < Wb) ? W - w0 : Wb;
       const c128* Sb = S + long(w0) * ldS;
@@ -1984,8 +2016,14 @@ extern "C" int afqmc_phmsd_energy(afqmc_phmsd h, const afqmc_c128* wbuf, long ld
       AFQMC_TRY(phmsd_reference_and_excited(h, s, 0, nb, h->E0, h->KEr, h->KEr, nullptr, E));
       // K vectors coupled to the down-spin excitations (PHMSD.cpp:472-494)
       {
-        if (h->kseg_split)
-          AFQMC_CUDA_TRY(cudaMemsetAsync(h->KEd, 0, kesz * size_t(nu1) * nb * Nc, s));
+        if (h->nkrow > 0) {
+          if (h->ke64)
+            zero_k_rows_kernel<c64><<<dim3(h->nkrow, nb), 256, 0, s>>>(
+                h->krow, nb, Nc, reinterpret_cast<c64*>(h->KEd));
+          else
+            zero_k_rows_kernel<c128><<<dim3(h->nkrow, nb), 256, 0, s>>>(h->krow, nb, Nc, h->KEd);
+          AFQMC_TRY(launch_status("zero_k_rows_kernel"));
+        }
         dim3 grid(h->nkseg, nb);
         if (h->ke64)
           couple_ke_kernel<c64><<<grid, 128, 0, s>>>(
